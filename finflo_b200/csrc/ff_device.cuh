@@ -1,0 +1,218 @@
+// Device-side numerics of the FINFLO hot path (sm_100a, FP64).
+//
+// Each function is the per-face or per-cell body of a reference routine; the
+// kernels in ff_kernels.cu decide the launch shape and data movement.
+// Reference citations are to the Fortran sources of mattipalin/finflo.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "../../include/finflo_types.h"
+
+#define FF_DI __device__ __forceinline__
+
+// Storage geometry of one block on one grid level.  a[] holds device
+// pointers to the FF_NSLOTS per-cell arrays (enum ff_slot).
+struct DevBlock {
+  int imax, jmax, kmax;
+  int is, il, ntot;
+  int npatch, pad;
+  const ff_patch* patch;   // device copy of the patch table
+  double* a[FF_NSLOTS];
+};
+
+FF_DI size_t ix(const DevBlock& b, int I, int J, int K) {
+  return (size_t)(K + 1) * b.il + (size_t)(J + 1) * b.is + (size_t)(I + 1);
+}
+
+template <typename T> FF_DI T dmax(T a, T b) { return a > b ? a : b; }
+template <typename T> FF_DI T dmin(T a, T b) { return a < b ? a : b; }
+
+// SURFVECTS base3c.f:12245: two tangent unit vectors completing the normal.
+template <typename T>
+FF_DI void surfvects(T a11, T a12, T a13, T& a21, T& a22, T& a23, T& a31, T& a32, T& a33) {
+  T am = fabs(a11);
+  int idir = 1;
+  if (fabs(a12) < am) { am = fabs(a12); idir = 2; }
+  if (fabs(a13) < am) idir = 3;
+  T b1, b2, b3;
+  if (idir == 1) { b1 = T(0); b2 = -a13; b3 = a12; }
+  else if (idir == 2) { b1 = a13; b2 = T(0); b3 = -a11; }
+  else { b1 = -a12; b2 = a11; b3 = T(0); }
+  T palpo = T(1) / sqrt(b1 * b1 + b2 * b2 + b3 * b3);
+  a21 = b1 * palpo; a22 = b2 * palpo; a23 = b3 * palpo;
+  a31 = a12 * a23 - a13 * a22;
+  a32 = a13 * a21 - a11 * a23;
+  a33 = a11 * a22 - a12 * a21;
+}
+
+// XXTRAP base3c.f:750 (kappa scheme, van Albada limiter); r0..r3 are the
+// cells I-2S, I-S, I, I+S of the face between I-S and I.
+FF_DI void xxtrap(double r0, double r1, double r2, double r3, int intem, double& rip, double& rim) {
+  int inter = intem < 0 ? -intem : intem;
+  int inte2 = inter < 1 ? 1 : (inter > 5 ? 5 : inter);
+  double rk1 = inte2 == 1 ? 0. : (inte2 == 2 ? 1. : (inte2 == 3 ? 1.3333333 : (inte2 == 4 ? 2. : 1.5)));
+  double rk2 = 2. - rk1;
+  double R1 = .25 * rk1, R2 = .25 * rk2;
+  double diff0 = r1 - r0, diff1 = r2 - r1, diff2 = r3 - r2;
+  if (intem <= 0 && intem >= -5) {
+    rip = r2 - (diff1 * R1 + diff2 * R2);
+    rim = r1 + (diff1 * R1 + diff0 * R2);
+  } else if (inter <= 4) {
+    double diff12 = diff1 * diff1 + 1.e-10;
+    double phibi = (diff12 + diff1 * diff0) / (diff12 + diff0 * diff0);
+    double phifi = (diff12 + diff1 * diff2) / (diff12 + diff2 * diff2);
+    rip = r2 - phifi * (diff1 * R1 + diff2 * R2);
+    rim = r1 + phibi * (diff1 * R1 + diff0 * R2);
+  } else {
+    rip = r2;
+    rim = r1;
+  }
+}
+
+// Roe flux-difference splitting for a general EOS (FLUXKE base3c.f:4753-5120)
+// at one face; laminar (k = omega = 0), UROT = 0.  q[v][m]: v = ro,u,v,w,p,
+// m = cells I-2S, I-S, I, I+S.  cr / cl2 = {DRDP, DRDH, RO, P} of cell I and of
+// the cell DERIV pairs it with (I-S, or I itself for the k direction,
+// base3c.f:4892 with IL > NTOT).  Returns the 5 flux components.
+FF_DI void roe_flux(const double q[5][4], double nx, double ny, double nz, double area,
+                    int intem, const ff_params& p, double c_r, double c_l,
+                    const double cr[4], const double cl2[4], double f[5]) {
+  double roip, roim, rmip, rmim, rnip, rnim, rwip, rwim, ppi, pmi;
+  xxtrap(q[0][0], q[0][1], q[0][2], q[0][3], intem, roip, roim);
+  xxtrap(q[1][0], q[1][1], q[1][2], q[1][3], intem, rmip, rmim);
+  xxtrap(q[2][0], q[2][1], q[2][2], q[2][3], intem, rnip, rnim);
+  xxtrap(q[3][0], q[3][1], q[3][2], q[3][3], intem, rwip, rwim);
+  xxtrap(q[4][0], q[4][1], q[4][2], q[4][3], intem, ppi, pmi);
+  roip = dmax(0.001 * p.frsden, roip);
+  ppi = dmax(0.001 * p.frspre, ppi);
+  roim = dmax(0.001 * p.frsden, roim);
+  pmi = dmax(0.001 * p.frspre, pmi);
+  const double gm1 = p.gamma - 1.;
+  // EFPRO state.f:620 (perfect gas)
+  double eip = ppi / (gm1 * roip) - p.e0ref;
+  double eim = pmi / (gm1 * roim) - p.e0ref;
+  double elr = ppi / (gm1 * roim) - p.e0ref;
+  double erl = pmi / (gm1 * roip) - p.e0ref;
+  // DERIV base3c.f:707 (Glaister hat derivatives)
+  double ypro1 = 1. / cr[2], ypro2 = 1. / cl2[2];
+  double dedph = 0.5 * ((-cr[0] / cr[1] - ypro1) + (-cl2[0] / cl2[1] - ypro2));
+  double dedrh = 0.5 * ((1. / cr[1] + cr[3] * (ypro1 * ypro1)) + (1. / cl2[1] + cl2[3] * (ypro2 * ypro2)));
+  {
+    double dpp = 2. * (ppi - pmi), drr = 2. * (roip - roim);
+    if (fabs(dpp) >= 1.e-2 * (ppi + pmi)) dedph = (eip + elr - eim - erl) / dpp;
+    if (fabs(drr) >= 1.e-2 * (roip + roim)) dedrh = (eip + erl - eim - elr) / drr;
+  }
+  double a21, a22, a23, a31, a32, a33;
+  surfvects(nx, ny, nz, a21, a22, a23, a31, a32, a33);
+  double ur = nx * rmip + ny * rnip + nz * rwip;
+  double vr = a21 * rmip + a22 * rnip + a23 * rwip;
+  double wr = a31 * rmip + a32 * rnip + a33 * rwip;
+  double ul = nx * rmim + ny * rnim + nz * rwim;
+  double vl = a21 * rmim + a22 * rnim + a23 * rwim;
+  double wl = a31 * rmim + a32 * rnim + a33 * rwim;
+  double ypror = 1. / roip, yprol = 1. / roim;
+  double eir = eip + .5 * (ur * ur + vr * vr + wr * wr);
+  double eil = eim + .5 * (ul * ul + vl * vl + wl * wl);
+  double pr = ppi, pl = pmi;
+  double hr = eir + pr * ypror, hl = eil + yprol * pl;
+  double rohat = sqrt(roip * roim), yproh = 1. / rohat;
+  double sqrl = 1. / (roim + rohat), cql = roim * sqrl, cqr = 1. - cql;
+  double uhat = cqr * ur + cql * ul, vhat = cqr * vr + cql * vl, what = cqr * wr + cql * wl;
+  double hhat = cqr * hr + cql * hl, ehat = cqr * eip + cql * eim;
+  double phat = rohat * (hhat - ehat - .5 * (uhat * uhat + vhat * vhat + what * what));
+  phat = dmin(dmax(pr, pl), phat);
+  phat = dmax(dmin(pr, pl), phat);
+  double drdhh = 1. / (dedrh - phat * (yproh * yproh));
+  double drdph = -drdhh * (dedph + yproh);
+  double chat2 = 1. / (drdhh * yproh + drdph);
+  double cmin = dmin(c_r, c_l), cmax = dmax(c_r, c_l);
+  chat2 = dmin(cmax * cmax, chat2);
+  chat2 = dmax(cmin * cmin, chat2);
+  double chat = sqrt(chat2);
+  double pdpde = dedph;
+  double dro = roip - roim, du = ur - ul;
+  double dp = pr - pl;
+  double pchat2 = 1. / (chat * chat);
+  double alfa1 = .5 * (dp + rohat * chat * du) * pchat2;
+  double alfa2 = .5 * (dp - rohat * chat * du) * pchat2;
+  double alfa3 = dro - dp * pchat2;
+  double alfa4 = rohat * (vr - vl), alfa5 = rohat * (wr - wl);
+  double rl1h = uhat + chat, rl2h = uhat - chat, rl3h = uhat;
+  double rl1 = fabs(rl1h), rl2 = fabs(rl2h), rl3 = fabs(rl3h);
+  if (p.entropy_fix) {
+    double e22;
+    e22 = 4. * dmax(dmax(1.e-10, rl1h - (ul + c_l)), (ur + c_r) - rl1h);
+    if (rl1 <= e22) rl1 = .5 * (rl1h * rl1h + e22 * e22) / e22;
+    e22 = 4. * dmax(dmax(1.e-10, rl2h - (ul - c_l)), (ur - c_r) - rl2h);
+    if (rl2 <= e22) rl2 = .5 * (rl2h * rl2h + e22 * e22) / e22;
+    e22 = 4. * dmax(dmax(1.e-10, rl3h - ul), ur - rl3h);
+    if (rl3 <= e22) rl3 = .5 * (rl3h * rl3h + e22 * e22) / e22;
+  }
+  double roucr = roip * ur, roucl = roim * ul;
+  double damp = rl1 * alfa1 + rl2 * alfa2 + rl3 * alfa3;
+  double ha = .5 * area;
+  double f1 = ha * (roucr + roucl - damp);
+  double f2 = ha * (roucr * ur + pr + roucl * ul + pl - (damp * uhat + (rl1 * alfa1 - rl2 * alfa2) * chat));
+  double f3 = ha * (roucr * vr + roucl * vl - damp * vhat - rl3 * alfa4);
+  double f4 = ha * (roucr * wr + roucl * wl - damp * what - rl3 * alfa5);
+  double f5 = ha * (roucr * hr + roucl * hl - damp * hhat
+                    - ((rl1 * alfa1 - rl2 * alfa2) * uhat * chat - rl3 * alfa3 * rohat * (chat * chat) * pdpde
+                       + rl3 * alfa4 * vhat + rl3 * alfa5 * what));
+  f[0] += f1;
+  f[1] += nx * f2 + a21 * f3 + a31 * f4;
+  f[2] += ny * f2 + a22 * f3 + a32 * f4;
+  f[3] += nz * f2 + a23 * f3 + a33 * f4;
+  f[4] += f5;
+}
+
+// SYI / SYM1I imps4.f:10/46 and the split-eigenvalue product of one
+// neighbour: SYM1I(diag(l1,l2,l1,l1,l5) * SYI(dw)).
+template <typename T>
+FF_DI void jac_product(T out[5], const T dw[5], T c, T ro, T nx, T ny, T nz, T l1, T l2, T l5) {
+  T a21, a22, a23, a31, a32, a33;
+  surfvects(nx, ny, nz, a21, a22, a23, a31, a32, a33);
+  T z2 = nx * dw[1] + ny * dw[2] + nz * dw[3];
+  T z3 = a21 * dw[1] + a22 * dw[2] + a23 * dw[3];
+  T z4 = a31 * dw[1] + a32 * dw[2] + a33 * dw[3];
+  T roc = ro * c;
+  T w1 = l1 * (dw[0] - dw[4] / ro);
+  T w2 = l2 * (roc * z2 + dw[4]);
+  T w3 = l1 * z3;
+  T w4 = l1 * z4;
+  T w5 = l5 * (-roc * z2 + dw[4]);
+  T ypro = T(1) / ro, pc2 = T(.5) * ypro, proc = pc2 / c;
+  out[0] = w1 + pc2 * (w2 + w5);
+  T x2i = proc * (w2 - w5);
+  out[4] = T(.5) * (w2 + w5);
+  out[1] = nx * x2i + a21 * w3 + a31 * w4;
+  out[2] = ny * x2i + a22 * w3 + a32 * w4;
+  out[3] = nz * x2i + a23 * w3 + a33 * w4;
+}
+
+// Bounded grid-wide barrier for a co-resident (cooperative) grid.  Every
+// spin has an iteration limit; on time-out the error word is set and all
+// blocks leave the kernel at their next barrier.
+FF_DI bool grid_barrier(unsigned* count, unsigned* gen, unsigned nblocks, int* err) {
+  __syncthreads();
+  if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
+    volatile unsigned* vg = gen;
+    unsigned g = *vg;
+    __threadfence();
+    unsigned arrived = atomicAdd(count, 1u);
+    if (arrived == nblocks - 1) {
+      atomicExch(count, 0u);
+      __threadfence();
+      atomicAdd(gen, 1u);
+    } else {
+      long it = 0;
+      while (*vg == g) {
+        if (++it > (1L << 24)) { atomicExch(err, 1); break; }
+        if (*((volatile int*)err)) break;
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return *((volatile int*)err) == 0;
+}

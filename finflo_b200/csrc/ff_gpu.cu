@@ -1,0 +1,488 @@
+// libfinflo_gpu.so: the C-ABI of the sm_100a FINFLO hot path.
+//
+// A context owns one CUDA stream and the device copies of the blocks; all
+// stage calls are asynchronous on that stream.  The per-cycle sequence of the
+// reference's CYCLES (ns3c.f:1354) for one grid level is available both as
+// separate stage calls (drop-in replacements of STATIM/RESIDU/IMPS/FIN/BOUNDI)
+// and as ff_cycles(), which captures one cycle in a CUDA graph and replays it.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+#include <vector>
+#include "ff_kernels.cuh"
+#include "../../include/finflo_gpu.h"
+
+using namespace ff;
+
+namespace {
+
+struct BlockCtx {
+  int imax = 0, jmax = 0, kmax = 0, ntot = 0, npatch = 0;
+  double* base = nullptr;       // FF_NSLOTS slots of ntot doubles
+  size_t slot_stride = 0;
+  ff_patch* d_patch = nullptr;
+  std::vector<ff_patch> h_patch;
+  ff_params prm{};
+  double* coef = nullptr;       // NCOEF x ntot (FP64 LU-SGS)
+  float* coef32 = nullptr;      // NCOEF x ntot (FP32 LU-SGS)
+  float* dw32 = nullptr;        // 5 x ntot
+  int coop_blocks = 0, coop_blocks32 = 0;
+  DevBlock db{};
+  cudaGraphExec_t graph = nullptr;
+  int graph_fp32 = -1;
+};
+
+struct Ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<BlockCtx*> blocks;
+  unsigned* d_bar = nullptr;            // grid barrier {count, generation}
+  int* d_err = nullptr;                 // sweep time-out flag
+  double* d_resi = nullptr;             // 5 sums of squares
+  unsigned long long* d_dromax = nullptr;
+  double* d_hist = nullptr;             // per-cycle {resi[5], dromax}
+  int* d_hist_pos = nullptr;
+  int hist_cap = 0;
+  int sm_count = 0;
+  char errmsg[256] = {0};
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+int fail(Ctx* c, int code, const char* what, cudaError_t e = cudaSuccess) {
+  if (c) snprintf(c->errmsg, sizeof(c->errmsg), "%s%s%s", what, e != cudaSuccess ? ": " : "",
+                  e != cudaSuccess ? cudaGetErrorString(e) : "");
+  return code;
+}
+#define CK(call)                                                   \
+  do {                                                             \
+    cudaError_t e_ = (call);                                       \
+    if (e_ != cudaSuccess) return fail(c, FF_ERR_CUDA, #call, e_); \
+  } while (0)
+
+inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
+
+BlockCtx* getb(Ctx* c, int blk) {
+  if (!c || blk < 0 || blk >= (int)c->blocks.size()) return nullptr;
+  return c->blocks[blk];
+}
+
+// __global__ helpers for the cycle history
+__global__ void k_reset_acc(double* resi, unsigned long long* dm) {
+  if (threadIdx.x < 5) resi[threadIdx.x] = 0.;
+  if (threadIdx.x == 0) *dm = 0ull;
+}
+__global__ void k_record(const double* resi, const unsigned long long* dm, double* hist, int* pos, int cap) {
+  int p = *pos;
+  if (p < cap) {
+    for (int v = 0; v < 5; v++) hist[6 * p + v] = resi[v];
+    hist[6 * p + 5] = __longlong_as_double((long long)*dm);
+  }
+  *pos = p + 1;
+}
+
+int launch_patch(Ctx* c, BlockCtx* b, void (*kern)(DevBlock, ff_params, int), int arg) {
+  if (b->npatch == 0) return 0;
+  int maxn = 1;
+  for (auto& p : b->h_patch) maxn = max(maxn, (p.r1b - p.r1a + 1) * (p.r2b - p.r2a + 1));
+  dim3 g(nblk(maxn, 128), b->npatch);
+  kern<<<g, 128, 0, c->stream>>>(b->db, b->prm, arg);
+  return 0;
+}
+
+// ---- stages -----------------------------------------------------------------
+int st_statim(Ctx* c, BlockCtx* b) {
+  k_state<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db, b->prm);
+  launch_patch(c, b, k_reflec, 0);
+  launch_patch(c, b, k_reflec, 1);
+  return 0;
+}
+
+int st_boundi(Ctx* c, BlockCtx* b) {
+  k_refcor<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db);
+  if (b->npatch) {
+    int maxn = 1;
+    for (auto& p : b->h_patch) maxn = max(maxn, (p.r1b - p.r1a + 1) * (p.r2b - p.r2a + 1));
+    k_mir<<<dim3(nblk(maxn, 128), b->npatch), 128, 0, c->stream>>>(b->db);
+  }
+  return st_statim(c, b);
+}
+
+int st_residu(Ctx* c, BlockCtx* b, int level, int icycle) {
+  if (level == 1) {
+    if (b->npatch) {
+      int maxn = 1;
+      for (auto& p : b->h_patch) maxn = max(maxn, (p.r1b - p.r1a + 1) * (p.r2b - p.r2a + 1));
+      k_refcen<<<dim3(nblk(maxn, 128), b->npatch), 128, 0, c->stream>>>(b->db, b->prm);
+    }
+  }
+  if (b->prm.fullns && level == 1) {
+    long ng = (long)(b->imax + 2) * (b->jmax + 2) * (b->kmax + 2);
+    k_grad<<<nblk(ng, 128), 128, 0, c->stream>>>(b->db, level);
+  }
+  if (level == 1) launch_patch(c, b, k_inlet_outlet, icycle);
+  dim3 g(nblk(b->imax, TI), nblk(b->jmax, TJ), nblk(b->kmax, TK));
+  k_residual<<<g, 128, 0, c->stream>>>(b->db, b->prm, level);
+  return 0;
+}
+
+int coop_sweep(Ctx* c, BlockCtx* b, int upper, bool fp32) {
+  int nb = fp32 ? b->coop_blocks32 : b->coop_blocks;
+  double* dw64 = b->base + (size_t)FF_DRO * b->slot_stride;
+  // the five increment slots are contiguous: DRO, DM, DN, DW, DE
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nb);
+  cfg.blockDim = dim3(256);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = c->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaError_t e;
+  if (!fp32) {
+    e = cudaLaunchKernelEx(&cfg, k_lusgs_sweep<double>, b->db, (const double*)b->coef, dw64, upper,
+                           c->d_bar, c->d_err);
+  } else {
+    e = cudaLaunchKernelEx(&cfg, k_lusgs_sweep<float>, b->db, (const float*)b->coef32, b->dw32, upper,
+                           c->d_bar, c->d_err);
+  }
+  if (e != cudaSuccess) return fail(c, FF_ERR_CUDA, "cooperative sweep launch", e);
+  return 0;
+}
+
+int st_imps(Ctx* c, BlockCtx* b, int level, bool divide_cp) {
+  int ncell = b->imax * b->jmax * b->kmax;
+  double cfl = level == 1 ? b->prm.cfl : b->prm.cfll;
+  k_time3_copr<<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, cfl);
+  bool fp32 = b->prm.lusgs_fp32 != 0;
+  int rc;
+  if (!fp32) {
+    k_lusgs_coef<double><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, b->coef, 1);
+    if ((rc = coop_sweep(c, b, 1, false))) return rc;
+    k_lusgs_coef<double><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, b->coef, 0);
+    if ((rc = coop_sweep(c, b, 0, false))) return rc;
+  } else {
+    k_copy_dw<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->dw32, 1);
+    k_lusgs_coef<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, b->coef32, 1);
+    if ((rc = coop_sweep(c, b, 1, true))) return rc;
+    k_lusgs_coef<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, b->coef32, 0);
+    if ((rc = coop_sweep(c, b, 0, true))) return rc;
+    k_copy_dw<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->dw32, 0);
+  }
+  if (divide_cp) {
+    // standalone IMPS: finish with DRO/CP (imps3.f:483); the fused cycle
+    // folds this division into the FIN kernel instead
+    k_fin_divide<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db);
+  }
+  return 0;
+}
+
+int st_fin(Ctx* c, BlockCtx* b, int divide_cp) {
+  k_fin<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db, b->prm, c->d_dromax, divide_cp);
+  return 0;
+}
+
+int one_cycle(Ctx* c, BlockCtx* b, int icycle) {
+  int rc;
+  k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi, c->d_dromax);
+  if ((rc = st_residu(c, b, 1, icycle))) return rc;
+  int ncell = b->imax * b->jmax * b->kmax;
+  k_resl2<<<min(nblk(ncell, 256), 4 * c->sm_count), 256, 0, c->stream>>>(b->db, c->d_resi);
+  if ((rc = st_imps(c, b, 1, false))) return rc;
+  if ((rc = st_fin(c, b, 1))) return rc;
+  if ((rc = st_boundi(c, b))) return rc;
+  k_record<<<1, 1, 0, c->stream>>>(c->d_resi, c->d_dromax, c->d_hist, c->d_hist_pos, c->hist_cap);
+  return 0;
+}
+
+int ensure_hist(Ctx* c, int n) {
+  if (n <= c->hist_cap) return 0;
+  if (c->d_hist) cudaFree(c->d_hist);
+  CK(cudaMalloc(&c->d_hist, sizeof(double) * 6 * n));
+  c->hist_cap = n;
+  for (auto* b : c->blocks)
+    if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+  return 0;
+}
+
+}  // namespace
+
+
+// ============================================================================
+extern "C" {
+
+int ff_abi_version(void) { return FF_ABI_VERSION; }
+
+const char* ff_last_error(void* ctx) { return ctx ? ((Ctx*)ctx)->errmsg : "no context"; }
+
+int ff_create(void** out, int device) {
+  Ctx* c = new Ctx();
+  c->device = device;
+  *out = nullptr;
+  CK(cudaSetDevice(device));
+  CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  CK(cudaMalloc(&c->d_bar, 2 * sizeof(unsigned)));
+  CK(cudaMemset(c->d_bar, 0, 2 * sizeof(unsigned)));
+  CK(cudaMalloc(&c->d_err, sizeof(int)));
+  CK(cudaMemset(c->d_err, 0, sizeof(int)));
+  CK(cudaMalloc(&c->d_resi, 8 * sizeof(double)));
+  CK(cudaMalloc(&c->d_dromax, sizeof(unsigned long long)));
+  CK(cudaMalloc(&c->d_hist_pos, sizeof(int)));
+  CK(cudaMemset(c->d_hist_pos, 0, sizeof(int)));
+  CK(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device));
+  CK(cudaEventCreate(&c->ev0));
+  CK(cudaEventCreate(&c->ev1));
+  *out = c;
+  return 0;
+}
+
+int ff_destroy(void* ctx) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return FF_ERR_ARG;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  for (auto* b : c->blocks) {
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    cudaFree(b->base); cudaFree(b->d_patch); cudaFree(b->coef); cudaFree(b->coef32); cudaFree(b->dw32);
+    delete b;
+  }
+  cudaFree(c->d_bar); cudaFree(c->d_err); cudaFree(c->d_resi); cudaFree(c->d_dromax);
+  cudaFree(c->d_hist); cudaFree(c->d_hist_pos);
+  cudaEventDestroy(c->ev0); cudaEventDestroy(c->ev1);
+  cudaStreamDestroy(c->stream);
+  delete c;
+  return 0;
+}
+
+int ff_block_add(void* ctx, int imax, int jmax, int kmax, int npatch, const ff_patch* patches,
+                 const ff_params* prm) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || imax < 2 || jmax < 2 || kmax < 1 || npatch < 0 || !prm) return fail(c, FF_ERR_ARG, "ff_block_add: bad dims");
+  BlockCtx* b = new BlockCtx();
+  b->imax = imax; b->jmax = jmax; b->kmax = kmax;
+  b->ntot = (imax + 4) * (jmax + 4) * (kmax + 4);
+  b->slot_stride = (size_t)b->ntot;   // DRO..DE stay contiguous (5 x ntot)
+  b->prm = *prm;
+  b->npatch = npatch;
+  b->h_patch.assign(patches, patches + npatch);
+  for (auto& p : b->h_patch) {
+    if (p.iface < 1 || p.iface > 6 || p.r1a < 1 || p.r2a < 1 || p.r1b < p.r1a || p.r2b < p.r2a) {
+      delete b;
+      return fail(c, FF_ERR_ARG, "ff_block_add: bad patch range");
+    }
+  }
+  CK(cudaMalloc(&b->base, sizeof(double) * b->slot_stride * FF_NSLOTS));
+  CK(cudaMemsetAsync(b->base, 0, sizeof(double) * b->slot_stride * FF_NSLOTS, c->stream));
+  if (npatch) {
+    CK(cudaMalloc(&b->d_patch, sizeof(ff_patch) * npatch));
+    CK(cudaMemcpyAsync(b->d_patch, patches, sizeof(ff_patch) * npatch, cudaMemcpyHostToDevice, c->stream));
+  }
+  CK(cudaMalloc(&b->coef, sizeof(double) * NCOEF * (size_t)b->ntot));
+  CK(cudaMalloc(&b->coef32, sizeof(float) * NCOEF * (size_t)b->ntot));
+  CK(cudaMalloc(&b->dw32, sizeof(float) * 5 * (size_t)b->ntot));
+  b->db.imax = imax; b->db.jmax = jmax; b->db.kmax = kmax;
+  b->db.is = imax + 4; b->db.il = (imax + 4) * (jmax + 4); b->db.ntot = b->ntot;
+  b->db.npatch = npatch; b->db.patch = b->d_patch;
+  for (int s = 0; s < FF_NSLOTS; s++) b->db.a[s] = b->base + (size_t)s * b->slot_stride;
+  // cooperative grid size: enough threads for the widest hyperplane
+  int per_sm = 0, per_sm32 = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lusgs_sweep<double>, 256, 0));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm32, k_lusgs_sweep<float>, 256, 0));
+  long widest = (long)jmax * kmax;
+  b->coop_blocks = (int)min((long)per_sm * c->sm_count, max(1L, (widest + 255) / 256));
+  b->coop_blocks32 = (int)min((long)per_sm32 * c->sm_count, max(1L, (widest + 255) / 256));
+  if (b->coop_blocks < 1 || b->coop_blocks32 < 1) return fail(c, FF_ERR_CUDA, "no cooperative occupancy");
+  c->blocks.push_back(b);
+  return (int)c->blocks.size() - 1;
+}
+
+int ff_block_params(void* ctx, int blk, const ff_params* prm) {
+  Ctx* c = (Ctx*)ctx;
+  BlockCtx* b = getb(c, blk);
+  if (!b || !prm) return fail(c, FF_ERR_ARG, "ff_block_params");
+  b->prm = *prm;
+  if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+  return 0;
+}
+
+int ff_upload(void* ctx, int blk, int slot, const double* host) {
+  Ctx* c = (Ctx*)ctx;
+  BlockCtx* b = getb(c, blk);
+  if (!b || slot < 0 || slot >= FF_NSLOTS || !host) return fail(c, FF_ERR_ARG, "ff_upload");
+  CK(cudaMemcpyAsync(b->db.a[slot], host, sizeof(double) * b->ntot, cudaMemcpyHostToDevice, c->stream));
+  return 0;
+}
+
+int ff_download(void* ctx, int blk, int slot, double* host) {
+  Ctx* c = (Ctx*)ctx;
+  BlockCtx* b = getb(c, blk);
+  if (!b || slot < 0 || slot >= FF_NSLOTS || !host) return fail(c, FF_ERR_ARG, "ff_download");
+  CK(cudaMemcpyAsync(host, b->db.a[slot], sizeof(double) * b->ntot, cudaMemcpyDeviceToHost, c->stream));
+  return 0;
+}
+
+void* ff_device_ptr(void* ctx, int blk, int slot) {
+  BlockCtx* b = getb((Ctx*)ctx, blk);
+  if (!b || slot < 0 || slot >= FF_NSLOTS) return nullptr;
+  return b->db.a[slot];
+}
+
+void* ff_stream(void* ctx) { return ctx ? (void*)((Ctx*)ctx)->stream : nullptr; }
+
+int ff_synchronize(void* ctx) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return FF_ERR_ARG;
+  CK(cudaStreamSynchronize(c->stream));
+  int err = 0;
+  CK(cudaMemcpy(&err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err) {
+    cudaMemset(c->d_err, 0, sizeof(int));
+    cudaMemset(c->d_bar, 0, 2 * sizeof(unsigned));
+    return fail(c, FF_ERR_TIMEOUT, "LU-SGS grid barrier timed out");
+  }
+  return 0;
+}
+
+int ff_statim(void* ctx, int blk) {
+  Ctx* c = (Ctx*)ctx;
+  BlockCtx* b = getb(c, blk);
+  if (!b) return fail(c, FF_ERR_ARG, "ff_statim");
+  st_statim(c, b);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int ff_boundi(void* ctx, int blk) {
+  Ctx* c = (Ctx*)ctx;
+  BlockCtx* b = getb(c, blk);
+  if (!b) return fail(c, FF_ERR_ARG, "ff_boundi");
+  st_boundi(c, b);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int ff_residu(void* ctx, int blk, int level, int icycle) {
+  Ctx* c = (Ctx*)ctx;
+  BlockCtx* b = getb(c, blk);
+  if (!b || level != 1) return fail(c, FF_ERR_ARG, "ff_residu (level 1 only)");
+  st_residu(c, b, level, icycle);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int ff_resl2(void* ctx, int blk, double* out5) {
+  Ctx* c = (Ctx*)ctx;
+  BlockCtx* b = getb(c, blk);
+  if (!b || !out5) return fail(c, FF_ERR_ARG, "ff_resl2");
+  k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi, c->d_dromax);
+  int ncell = b->imax * b->jmax * b->kmax;
+  k_resl2<<<min(nblk(ncell, 256), 4 * c->sm_count), 256, 0, c->stream>>>(b->db, c->d_resi);
+  CK(cudaMemcpyAsync(out5, c->d_resi, 5 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int ff_imps(void* ctx, int blk, int level) {
+  Ctx* c = (Ctx*)ctx;
+  BlockCtx* b = getb(c, blk);
+  if (!b || level != 1) return fail(c, FF_ERR_ARG, "ff_imps (level 1 only)");
+  int rc = st_imps(c, b, level, true);
+  if (rc) return rc;
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int ff_fin(void* ctx, int blk, double* dromax) {
+  Ctx* c = (Ctx*)ctx;
+  BlockCtx* b = getb(c, blk);
+  if (!b) return fail(c, FF_ERR_ARG, "ff_fin");
+  k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi, c->d_dromax);
+  st_fin(c, b, 0);
+  if (dromax) {
+    unsigned long long bits;
+    CK(cudaMemcpyAsync(&bits, c->d_dromax, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    memcpy(dromax, &bits, sizeof(double));
+  }
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int ff_cycles(void* ctx, int blk, int ncycles, int icycle0, double* hist, int use_graph) {
+  Ctx* c = (Ctx*)ctx;
+  BlockCtx* b = getb(c, blk);
+  if (!b || ncycles < 0) return fail(c, FF_ERR_ARG, "ff_cycles");
+  int rc;
+  if ((rc = ensure_hist(c, max(ncycles, 1)))) return rc;
+  CK(cudaMemsetAsync(c->d_hist_pos, 0, sizeof(int), c->stream));
+  int it = 0;
+  // the first cycle of a run (ICYCLE = 1) differs (INLET density), run it eagerly
+  while (it < ncycles && (icycle0 + it == 1 || !use_graph)) {
+    if ((rc = one_cycle(c, b, icycle0 + it))) return rc;
+    it++;
+  }
+  if (it < ncycles) {
+    int want = b->prm.lusgs_fp32 ? 1 : 0;
+    if (!b->graph || b->graph_fp32 != want) {
+      if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+      cudaGraph_t g;
+      CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      rc = one_cycle(c, b, 2);
+      cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+      if (rc) return rc;
+      if (e != cudaSuccess) return fail(c, FF_ERR_CUDA, "cycle capture", e);
+      CK(cudaGraphInstantiate(&b->graph, g, 0));
+      cudaGraphDestroy(g);
+      b->graph_fp32 = want;
+    }
+    for (; it < ncycles; it++) CK(cudaGraphLaunch(b->graph, c->stream));
+  }
+  CK(cudaGetLastError());
+  if (hist) {
+    CK(cudaMemcpyAsync(hist, c->d_hist, sizeof(double) * 6 * ncycles, cudaMemcpyDeviceToHost, c->stream));
+    rc = ff_synchronize(ctx);
+    if (rc) return rc;
+  }
+  return 0;
+}
+
+int ff_time_cycles(void* ctx, int blk, int ncycles, float* ms) {
+  Ctx* c = (Ctx*)ctx;
+  BlockCtx* b = getb(c, blk);
+  if (!b || !ms) return fail(c, FF_ERR_ARG, "ff_time_cycles");
+  CK(cudaEventRecord(c->ev0, c->stream));
+  int rc = ff_cycles(ctx, blk, ncycles, 2, nullptr, 1);
+  if (rc) return rc;
+  CK(cudaEventRecord(c->ev1, c->stream));
+  CK(cudaEventSynchronize(c->ev1));
+  CK(cudaEventElapsedTime(ms, c->ev0, c->ev1));
+  return ff_synchronize(ctx);
+}
+
+int ff_time_stage(void* ctx, int blk, int stage, int reps, float* ms) {
+  Ctx* c = (Ctx*)ctx;
+  BlockCtx* b = getb(c, blk);
+  if (!b || !ms || reps < 1) return fail(c, FF_ERR_ARG, "ff_time_stage");
+  CK(cudaEventRecord(c->ev0, c->stream));
+  for (int r = 0; r < reps; r++) {
+    if (stage == FF_STAGE_RESIDUAL) {
+      dim3 g(nblk(b->imax, TI), nblk(b->jmax, TJ), nblk(b->kmax, TK));
+      k_residual<<<g, 128, 0, c->stream>>>(b->db, b->prm, 1);
+    } else if (stage == FF_STAGE_GRAD) {
+      long ng = (long)(b->imax + 2) * (b->jmax + 2) * (b->kmax + 2);
+      k_grad<<<nblk(ng, 128), 128, 0, c->stream>>>(b->db, 1);
+    } else if (stage == FF_STAGE_STATE) {
+      k_state<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db, b->prm);
+    } else {
+      return fail(c, FF_ERR_ARG, "ff_time_stage: unknown stage");
+    }
+  }
+  CK(cudaEventRecord(c->ev1, c->stream));
+  CK(cudaEventSynchronize(c->ev1));
+  CK(cudaEventElapsedTime(ms, c->ev0, c->ev1));
+  *ms /= reps;
+  return 0;
+}
+
+}  // extern "C"

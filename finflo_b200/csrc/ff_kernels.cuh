@@ -1,0 +1,785 @@
+// sm_100a kernels of the FINFLO per-iteration hot path (FP64).
+//
+// Launch shapes:
+//   k_state / k_fin / k_time3_copr ...  element-wise, one thread per cell
+//   k_patch_*                         one grid row per boundary patch
+//   k_grad                            one thread per cell incl. ghost layer 1
+//   k_residual                        32x4x4-cell tiles, all three face
+//                                     directions fused, face fluxes staged
+//                                     in shared memory, residual written once
+//   k_lusgs_coef + k_lusgs_sweep      coefficient pass, then a cooperative
+//                                     persistent kernel marching the i+j+k
+//                                     hyperplanes with a bounded grid barrier
+#pragma once
+#include "ff_device.cuh"
+
+namespace ff {
+
+constexpr int TI = 32, TJ = 4, TK = 4;   // residual tile
+constexpr int NCOEF = 13;                 // LU-SGS coefficients per cell
+
+// ---------------------------------------------------------------------------
+// STATIM: PDTOP state.f:1690, PERFGA state.f:159, CONSVA base3c.f:489, and the
+// laminar TURBDI (ADJUIN res3c.f:9447: EPS2 = 1, VIST = 0 on interior cells).
+FF_DI void state_cell(const DevBlock& b, const ff_params& p, size_t n) {
+  double* a_P = b.a[FF_P];
+  double pd = b.a[FF_PDIFF][n], T = b.a[FF_TEMP][n];
+  double P = pd + p.frspre;
+  const double gm1 = p.gamma - 1., cp2 = p.gamma / gm1 * p.rgas;
+  double trgs = T * p.rgas;
+  double drdp = 1. / trgs;
+  double ro = P * drdp;
+  double vis = p.visu0 * T * sqrt(T) / (T + p.tsu0);
+  double e = trgs / gm1;
+  double drdh = -ro / e / p.gamma;
+  double u = b.a[FF_U][n], v = b.a[FF_V][n], w = b.a[FF_W][n];
+  double rkin = (u * u + v * v + w * w) * .5;
+  double c = sqrt(dmax(1. / (drdh / ro + drdp), 1.0));
+  a_P[n] = P;
+  b.a[FF_DRDP][n] = drdp;
+  b.a[FF_RO][n] = ro;
+  b.a[FF_VIS][n] = vis;
+  b.a[FF_DRDH][n] = drdh;
+  b.a[FF_CP][n] = cp2;
+  b.a[FF_CH][n] = vis * cp2 / p.pr;
+  b.a[FF_C][n] = c;
+  b.a[FF_E][n] = (e + rkin) * ro;
+  b.a[FF_RM][n] = ro * u;
+  b.a[FF_RN][n] = ro * v;
+  b.a[FF_RW][n] = ro * w;
+}
+
+__global__ void k_state(DevBlock b, ff_params p) {
+  size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= (size_t)b.ntot) return;
+  state_cell(b, p, n);
+  int i = (int)(n % b.is), j = (int)((n / b.is) % (b.jmax + 4)), k = (int)(n / b.il);
+  if (i >= 2 && i < b.imax + 2 && j >= 2 && j < b.jmax + 2 && k >= 2 && k < b.kmax + 2) {
+    b.a[FF_EPS2][n] = 1.0;
+    b.a[FF_VIST][n] = 0.0;
+  }
+}
+
+// Face description of a patch: direction, sign, normal stride, interior layer.
+struct FaceG { int dir, idir, s, layer; };
+FF_DI FaceG face_g(const DevBlock& b, int iface) {
+  FaceG f;
+  f.dir = (iface - 1) % 3 + 1;
+  f.idir = iface <= 3 ? 1 : -1;
+  f.s = f.dir == 1 ? 1 : (f.dir == 2 ? b.is : b.il);
+  int mx = f.dir == 1 ? b.imax : (f.dir == 2 ? b.jmax : b.kmax);
+  f.layer = iface <= 3 ? 1 : mx;
+  return f;
+}
+FF_DI size_t face_cell(const DevBlock& b, const FaceG& f, int a, int c) {
+  if (f.dir == 1) return ix(b, f.layer, a, c);
+  if (f.dir == 2) return ix(b, a, f.layer, c);
+  return ix(b, a, c, f.layer);
+}
+
+// Patch-cell iteration: blockIdx.y = patch, x covers r1 x r2.
+#define FF_PATCH_LOOP(b)                                                       \
+  const ff_patch& pa = (b).patch[blockIdx.y];                                  \
+  int n1 = pa.r1b - pa.r1a + 1, n2 = pa.r2b - pa.r2a + 1;                      \
+  int t = blockIdx.x * blockDim.x + threadIdx.x;                               \
+  if (t >= n1 * n2) return;                                                    \
+  int pa1 = pa.r1a + t % n1, pa2 = pa.r2a + t / n1;                            \
+  FaceG fg = face_g((b), pa.iface);                                            \
+  int ls = fg.idir * fg.s;                                                     \
+  size_t L = face_cell((b), fg, pa1, pa2);
+
+// REFLEC turb3.f:5294: solid walls (viscous, wall at rest) and the inlet
+// pressure extrapolation.  mode 0: REFLEC; mode 1: re-evaluate the equation of
+// state in the two ghost cells first (the second STATIM pass).
+__global__ void k_reflec(DevBlock b, ff_params p, int mode) {
+  FF_PATCH_LOOP(b)
+  size_t LB = L - ls, LT = L + ls, LC = L - 2 * ls;
+  bool wall = pa.ityp >= 7 && pa.ityp <= 10;
+  if (!wall && pa.ityp != FF_BC_INL) return;
+  if (mode == 1) { state_cell(b, p, LB); state_cell(b, p, LC); }
+  double* P = b.a[FF_P]; double* PD = b.a[FF_PDIFF];
+  if (pa.ityp == FF_BC_INL) {
+    P[LB] = P[L]; PD[LB] = PD[L]; P[LC] = P[L]; PD[LC] = PD[L];
+    return;
+  }
+  double *T = b.a[FF_TEMP], *RO = b.a[FF_RO];
+  int ihfl = pa.iheat == 1 ? 1 : 0;
+  double tsurf = pa.iheat == 1 ? pa.bount : 0.0;
+  double tb = (1 - ihfl) * T[L] + ihfl * (2. * tsurf - T[L]);
+  tb = dmax(dmin(tb, p.tuplim), p.tlolim);
+  T[LB] = tb; T[LC] = tb;
+  b.a[FF_VIS][LB] = b.a[FF_VIS][L]; b.a[FF_CH][LB] = b.a[FF_CH][L]; b.a[FF_C][LB] = b.a[FF_C][L];
+  b.a[FF_DRDP][LB] = b.a[FF_DRDP][L]; b.a[FF_DRDH][LB] = b.a[FF_DRDH][L];
+  double u = -b.a[FF_U][L], v = -b.a[FF_V][L], w = -b.a[FF_W][L];
+  b.a[FF_U][LB] = u; b.a[FF_V][LB] = v; b.a[FF_W][LB] = w;
+  b.a[FF_U][LC] = u; b.a[FF_V][LC] = v; b.a[FF_W][LC] = w;
+  double ro = dmax(0.001 * p.frsden, RO[L]);
+  double pb = dmax(0.001 * p.frspre, 2. * P[L] - P[LT]);
+  double pdb = dmax(-0.999 * p.frspre, 2. * PD[L] - PD[LT]);
+  RO[LB] = ro; RO[LC] = ro; P[LB] = pb; P[LC] = pb; PD[LB] = pdb; PD[LC] = pdb;
+  b.a[FF_EPS2][LB] = 1.; b.a[FF_VIST][LB] = 0.; b.a[FF_EPS2][LC] = 1.; b.a[FF_VIST][LC] = 0.;
+  b.a[FF_RM][LB] = ro * u; b.a[FF_RN][LB] = ro * v; b.a[FF_RW][LB] = ro * w;
+  b.a[FF_RM][LC] = ro * u; b.a[FF_RN][LC] = ro * v; b.a[FF_RW][LC] = ro * w;
+  b.a[FF_E][LB] = b.a[FF_E][L]; b.a[FF_E][LC] = b.a[FF_E][L];
+}
+
+// REFCEN turb3.f:5881: linear extrapolation into the first wall ghost.
+__global__ void k_refcen(DevBlock b, ff_params p) {
+  FF_PATCH_LOOP(b)
+  if (pa.ityp < 7 || pa.ityp > 10) return;
+  size_t LB = L - ls, LT = L + ls;
+  double* RO = b.a[FF_RO]; double* P = b.a[FF_P]; double* PD = b.a[FF_PDIFF];
+  RO[LB] = dmax(0.001 * p.frsden, 2. * RO[L] - RO[LT]);
+  P[LB] = dmax(0.001 * p.frspre, 2. * P[L] - P[LT]);
+  PD[LB] = dmax(-0.999 * p.frspre, 2. * PD[L] - PD[LT]);
+  const int sl[7] = {FF_E, FF_U, FF_V, FF_W, FF_RM, FF_RN, FF_RW};
+#pragma unroll
+  for (int s = 0; s < 7; s++) { double* q = b.a[sl[s]]; q[LB] = 2. * q[L] - q[LT]; }
+}
+
+// INLET base3c.f:9223 (INLOUT 4) and OUTLET base3c.f:9595 (INLOUT 2, 3): the
+// level-1 ghost update FLUCYC does before the fluxes (res3c.f:7730-7834).
+__global__ void k_inlet_outlet(DevBlock b, ff_params p, int icycle) {
+  FF_PATCH_LOOP(b)
+  bool inl = pa.ityp == FF_BC_INL && pa.ibtype == 4;
+  bool out = pa.ityp == FF_BC_OUT && (pa.ibtype == 2 || pa.ibtype == 3);
+  if (!inl && !out) return;
+  size_t II = L, II2 = L + ls, IM1 = L - ls, IM2 = IM1 - ls;
+  size_t IF1 = fg.idir == 1 ? II : II + fg.s;
+  double *U = b.a[FF_U], *V = b.a[FF_V], *W = b.a[FF_W], *T = b.a[FF_TEMP], *RO = b.a[FF_RO];
+  double *P = b.a[FF_P], *PD = b.a[FF_PDIFF], *E = b.a[FF_E], *RM = b.a[FF_RM], *RN = b.a[FF_RN];
+  double *RW = b.a[FF_RW], *EPS2 = b.a[FF_EPS2], *VIST = b.a[FF_VIST], *VIS = b.a[FF_VIS];
+  if (inl) {
+    double dpkoe = P[II], dpdif = PD[II];
+    EPS2[IM1] = EPS2[II]; EPS2[IM2] = EPS2[II];
+    VIST[IM1] = VIST[II]; VIST[IM2] = VIST[II];
+    double rm = pa.bounu * pa.bounr, rn = pa.bounv * pa.bounr, rw = pa.bounw * pa.bounr;
+    RM[IM1] = rm; RN[IM1] = rn; RW[IM1] = rw; RM[IM2] = rm; RN[IM2] = rn; RW[IM2] = rw;
+    if (icycle == 1) RO[IM1] = pa.bounr;
+    T[IM1] = pa.bount; T[IM2] = pa.bount;
+    P[IM1] = dpkoe; P[IM2] = dpkoe; PD[IM1] = dpdif; PD[IM2] = dpdif;
+    double e = p.rgas / (p.gamma - 1.) * pa.bount;
+    double r1 = RO[IM1], r2 = RO[IM2];
+    double u1 = rm / r1, v1 = rn / r1, w1 = rw / r1, u2 = rm / r2, v2 = rn / r2, w2 = rw / r2;
+    U[IM1] = u1; V[IM1] = v1; W[IM1] = w1; U[IM2] = u2; V[IM2] = v2; W[IM2] = w2;
+    E[IM1] = r1 * (e + .5 * (u1 * u1 + v1 * v1 + w1 * w1));
+    E[IM2] = r2 * (e + .5 * (u2 * u2 + v2 * v2 + w2 * w2));
+    return;
+  }
+  const double turlim = 1.e-6;   // FLUCYC's local TURLIM (res3c.f:7750)
+  double rk3 = pa.ibtype == 2 ? 0.7 : 1.0, rk4 = pa.ibtype == 2 ? 0.3 : 0.0;
+  const double* NX = b.a[FF_A1XA + 4 * (fg.dir - 1)];
+  const double* NY = b.a[FF_A1YA + 4 * (fg.dir - 1)];
+  const double* NZ = b.a[FF_A1ZA + 4 * (fg.dir - 1)];
+  double a11 = NX[IF1], a12 = NY[IF1], a13 = NZ[IF1], a21, a22, a23, a31, a32, a33;
+  surfvects(a11, a12, a13, a21, a22, a23, a31, a32, a33);
+  double veloc = .5 * (a11 * (U[II] + pa.bounu) + a12 * (V[II] + pa.bounv) + a13 * (W[II] + pa.bounw));
+  P[IM1] = pa.bounp; P[IM2] = pa.bounp; PD[IM1] = pa.bounpd; PD[IM2] = pa.bounpd;
+  double eps2 = dmin(EPS2[II], turlim), vist = dmin(VIST[II], turlim * VIS[IM2]);
+  EPS2[IM1] = eps2; EPS2[IM2] = eps2; VIST[IM1] = vist; VIST[IM2] = vist;
+  if (-veloc * fg.idir > 0.) {
+    double u = RO[II] * U[II] / RO[IM1], v = V[II], w = W[II];
+    U[IM1] = u; U[IM2] = u; V[IM1] = v; V[IM2] = v; W[IM1] = w; W[IM2] = w;
+    T[IM1] = T[II]; T[IM2] = T[II];
+    RM[IM1] = RO[IM1] * u; RM[IM2] = RO[IM2] * u;
+    RN[IM1] = RO[IM1] * v; RN[IM2] = RO[IM2] * v;
+    RW[IM1] = RO[IM1] * w; RW[IM2] = RO[IM2] * w;
+  } else {
+    double velc1 = a11 * U[II] + a12 * V[II] + a13 * W[II];
+    double velc2 = a21 * pa.bounu + a22 * pa.bounv + a23 * pa.bounw;
+    double velc3 = a31 * pa.bounu + a32 * pa.bounv + a33 * pa.bounw;
+    double uu = a11 * velc1 + a21 * velc2 + a31 * velc3;
+    double vv = a12 * velc1 + a22 * velc2 + a32 * velc3;
+    double ww = a13 * velc1 + a23 * velc2 + a33 * velc3;
+    double u = rk3 * U[IM1] + rk4 * uu, v = rk3 * V[IM1] + rk4 * vv, w = rk3 * W[IM1] + rk4 * ww;
+    U[IM1] = u; U[IM2] = u; V[IM1] = v; V[IM2] = v; W[IM1] = w; W[IM2] = w;
+    T[IM1] = pa.bount; T[IM2] = pa.bount;
+    RO[IM1] = pa.bounr; RO[IM2] = pa.bounr;
+  }
+}
+
+// MIR ns3c.f:9003 -> MIRROR gluebm.f:3911 for symmetry patches.
+__global__ void k_mir(DevBlock b) {
+  FF_PATCH_LOOP(b)
+  if (pa.ityp != FF_BC_MIR) return;
+  (void)ls;
+  int kdir = fg.idir == 1 ? -1 : 1, koff = fg.idir == 1 ? 0 : 1;
+  size_t IC1 = L, IT = IC1 + (size_t)koff * fg.s;
+  size_t IT1 = IC1 + kdir * fg.s, IT2 = IC1 + 2 * kdir * fg.s, IC2 = IC1 - kdir * fg.s;
+  double nx = b.a[FF_A1XA + 4 * (fg.dir - 1)][IT];
+  double ny = b.a[FF_A1YA + 4 * (fg.dir - 1)][IT];
+  double nz = b.a[FF_A1ZA + 4 * (fg.dir - 1)][IT];
+  double a11 = -2. * nx * nx + 1.0, a12 = -2. * nx * ny, a13 = -2. * nx * nz;
+  double a22 = -2. * ny * ny + 1.0, a23 = -2. * ny * nz, a33 = -2. * nz * nz + 1.0;
+  double *U = b.a[FF_U], *V = b.a[FF_V], *W = b.a[FF_W];
+  double u1 = U[IC1], v1 = V[IC1], w1 = W[IC1], u2 = U[IC2], v2 = V[IC2], w2 = W[IC2];
+  U[IT1] = a11 * u1 + a12 * v1 + a13 * w1;
+  V[IT1] = a12 * u1 + a22 * v1 + a23 * w1;
+  W[IT1] = a13 * u1 + a23 * v1 + a33 * w1;
+  U[IT2] = a11 * u2 + a12 * v2 + a13 * w2;
+  V[IT2] = a12 * u2 + a22 * v2 + a23 * w2;
+  W[IT2] = a13 * u2 + a23 * v2 + a33 * w2;
+  const int sc[6] = {FF_TEMP, FF_E, FF_P, FF_PDIFF, FF_EPS2, FF_VIST};
+#pragma unroll
+  for (int s = 0; s < 6; s++) { double* q = b.a[sc[s]]; q[IT1] = q[IC1]; q[IT2] = q[IC2]; }
+}
+
+// REFCOR turb3.f:6040: ghost cells with two or three ghost indices copy the
+// interior edge/corner cell next to them.
+__global__ void k_refcor(DevBlock b) {
+  size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= (size_t)b.ntot) return;
+  int i = (int)(n % b.is) - 1, j = (int)((n / b.is) % (b.jmax + 4)) - 1, k = (int)(n / b.il) - 1;
+  int gi = i < 1 || i > b.imax, gj = j < 1 || j > b.jmax, gk = k < 1 || k > b.kmax;
+  if (gi + gj + gk < 2) return;
+  int ic = i < 1 ? 1 : (i > b.imax ? b.imax : i);
+  int jc = j < 1 ? 1 : (j > b.jmax ? b.jmax : j);
+  int kc = k < 1 ? 1 : (k > b.kmax ? b.kmax : k);
+  size_t src = ix(b, ic, jc, kc);
+  const int sl[18] = {FF_RO, FF_RM, FF_RN, FF_RW, FF_E, FF_U, FF_V, FF_W, FF_P, FF_PDIFF,
+                      FF_EPS2, FF_VIST, FF_TEMP, FF_VIS, FF_CH, FF_C, FF_DRDP, FF_DRDH};
+#pragma unroll
+  for (int s = 0; s < 18; s++) b.a[sl[s]][n] = b.a[sl[s]][src];
+}
+
+// DERFUN turb3.f:2476 + TEMDER turb3.f:3456 (IDERI = 1), interior + first
+// ghost layer on level 1.
+__global__ void k_grad(DevBlock b, int level) {
+  int lo = level == 1 ? 0 : 1, hi = level == 1 ? 1 : 0;
+  int ni = b.imax + hi - lo + 1, nj = b.jmax + hi - lo + 1, nk = b.kmax + hi - lo + 1;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ni * nj * nk) return;
+  int I = lo + t % ni, J = lo + (t / ni) % nj, K = lo + t / (ni * nj);
+  const int IS = b.is, IL = b.il;
+  size_t L = ix(b, I, J, K);
+  const double *U = b.a[FF_U], *V = b.a[FF_V], *W = b.a[FF_W], *T = b.a[FF_TEMP];
+  const double *A1 = b.a[FF_A1], *A2 = b.a[FF_A2], *A3 = b.a[FF_A3];
+  const double *D1 = b.a[FF_D1], *D2 = b.a[FF_D2], *D3 = b.a[FF_D3];
+  double q[4][6];   // face-weighted values of u,v,w,T on the 6 faces (m/p per dir)
+  double aa[6];     // areas: 1m,1p,2m,2p,3m,3p
+  const double* Dd[3] = {D1, D2, D3};
+  const double* Ad[3] = {A1, A2, A3};
+  const int st[3] = {1, IS, IL};
+  const double* F[4] = {U, V, W, T};
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+#pragma unroll
+    for (int side = 0; side < 2; side++) {
+      size_t nb = side == 0 ? L - st[d] : L + st[d];
+      double w1 = 2.0 * (Dd[d][L] / (Dd[d][L] + Dd[d][nb])), w2 = 2.0 - w1;
+      aa[2 * d + side] = side == 0 ? Ad[d][L] : Ad[d][L + st[d]];
+#pragma unroll
+      for (int v = 0; v < 4; v++) q[v][2 * d + side] = w2 * F[v][L] + w1 * F[v][nb];
+    }
+  }
+  double pvol = .5 / b.a[FF_VOL][L];
+  double g[3][3];   // g[v][x] = d(u_v)/dx_x
+#pragma unroll
+  for (int x = 0; x < 3; x++) {
+    const double* N1 = b.a[FF_A1XA + x];
+    const double* N2 = b.a[FF_A2XA + x];
+    const double* N3 = b.a[FF_A3XA + x];
+    double n3p = N3[L + IL], n3m = N3[L], n2p = N2[L + IS], n2m = N2[L], n1p = N1[L + 1], n1m = N1[L];
+#pragma unroll
+    for (int v = 0; v < 3; v++)
+      g[v][x] = pvol * (n3p * (aa[5] * q[v][5]) - n3m * (aa[4] * q[v][4]) + n2p * (aa[3] * q[v][3])
+                        - n2m * (aa[2] * q[v][2]) + n1p * (aa[1] * q[v][1]) - n1m * (aa[0] * q[v][0]));
+    bool tk = !(level == 1 && (K == 0 || K == b.kmax + 1) && b.kmax <= 1);
+    if (tk)
+      b.a[FF_DTDX + x][L] = pvol * (aa[5] * n3p * q[3][5] - aa[4] * n3m * q[3][4] + aa[3] * n2p * q[3][3]
+                                    - aa[2] * n2m * q[3][2] + aa[1] * n1p * q[3][1] - aa[0] * n1m * q[3][0]);
+  }
+  double w12 = .5 * (g[0][1] - g[1][0]), w13 = .5 * (g[0][2] - g[2][0]), w23 = .5 * (g[1][2] - g[2][1]);
+  b.a[FF_W12][L] = w12; b.a[FF_W13][L] = w13; b.a[FF_W23][L] = w23;
+  b.a[FF_OHMI][L] = 2. * sqrt(w12 * w12 + w13 * w13 + w23 * w23);
+  double s11 = g[0][0], s22 = g[1][1], s33 = g[2][2];
+  double s12 = .5 * (g[0][1] + g[1][0]), s13 = .5 * (g[0][2] + g[2][0]), s23 = .5 * (g[1][2] + g[2][1]);
+  b.a[FF_S11][L] = s11; b.a[FF_S12][L] = s12; b.a[FF_S13][L] = s13;
+  b.a[FF_S22][L] = s22; b.a[FF_S23][L] = s23; b.a[FF_S33][L] = s33;
+  double stn = s11 * s11 + 2. * s12 * s12 + 2. * s13 * s13 + s22 * s22 + 2. * s23 * s23 + s33 * s33;
+  b.a[FF_STRAIN][L] = sqrt(2. * stn);
+}
+
+// FLUXBL base3c.f:4085 (IDIFF = 1) for the face between M = L-S and L; the
+// result is the viscous part of the face flux (FRO untouched).
+FF_DI void visc_flux(const DevBlock& b, const ff_params& p, size_t L, int S, int dir, double f[5]) {
+  size_t M = L - S;
+  const double* D = b.a[FF_D1 + dir - 1];
+  double w1 = 2.0 * (__ldg(D + L) / (__ldg(D + L) + __ldg(D + M))), w2 = 2.0 - w1;
+  double w1p = .5 * w1, w2p = .5 * w2;
+#define LD(s, n) __ldg(b.a[s] + (n))
+  double s11l = LD(FF_S11, L), s11m = LD(FF_S11, M), s22l = LD(FF_S22, L), s22m = LD(FF_S22, M);
+  double s33l = LD(FF_S33, L), s33m = LD(FF_S33, M), s12l = LD(FF_S12, L), s12m = LD(FF_S12, M);
+  double s13l = LD(FF_S13, L), s13m = LD(FF_S13, M), s23l = LD(FF_S23, L), s23m = LD(FF_S23, M);
+  double w12l = LD(FF_W12, L), w12m = LD(FF_W12, M), w13l = LD(FF_W13, L), w13m = LD(FF_W13, M);
+  double w23l = LD(FF_W23, L), w23m = LD(FF_W23, M);
+  double dudx = w2p * s11l + w1p * s11m, dvdy = w2p * s22l + w1p * s22m, dwdz = w2p * s33l + w1p * s33m;
+  double dudy = w2p * (s12l + w12l) + w1p * (s12m + w12m);
+  double dudz = w2p * (s13l + w13l) + w1p * (s13m + w13m);
+  double dvdx = w2p * (s12l - w12l) + w1p * (s12m - w12m);
+  double dvdz = w2p * (s23l + w23l) + w1p * (s23m + w23m);
+  double dwdx = w2p * (s13l - w13l) + w1p * (s13m - w13m);
+  double dwdy = w2p * (s23l - w23l) + w1p * (s23m - w23m);
+  double s11i = w2 * s11l + w1 * s11m, s12i = w2 * s12l + w1 * s12m, s13i = w2 * s13l + w1 * s13m;
+  double s22i = w2 * s22l + w1 * s22m, s23i = w2 * s23l + w1 * s23m, s33i = w2 * s33l + w1 * s33m;
+  double dtdxi = w2p * LD(FF_DTDX, L) + w1p * LD(FF_DTDX, M);
+  double dtdyi = w2p * LD(FF_DTDY, L) + w1p * LD(FF_DTDY, M);
+  double dtdzi = w2p * LD(FF_DTDZ, L) + w1p * LD(FF_DTDZ, M);
+  double sxi = LD(FF_XC, L) - LD(FF_XC, M), syi = LD(FF_YC, L) - LD(FF_YC, M), szi = LD(FF_ZC, L) - LD(FF_ZC, M);
+  double slen = sqrt(sxi * sxi + syi * syi + szi * szi) + 1.e-21;
+  sxi = sxi / slen; syi = syi / slen; szi = szi / slen;
+  double nx = LD(FF_A1XA + 4 * (dir - 1), L), ny = LD(FF_A1YA + 4 * (dir - 1), L), nz = LD(FF_A1ZA + 4 * (dir - 1), L);
+  double area = LD(FF_A1 + 4 * (dir - 1), L);
+  double alfa = sxi * nx + syi * ny + szi * nz;
+  double surf = 0.5 * area * (LD(FF_EPS2, L) * LD(FF_VIS, L) + LD(FF_EPS2, M) * LD(FF_VIS, M));
+  double surfe = 0.5 * area * (LD(FF_CP, L) * LD(FF_VIST, L) / p.prt + LD(FF_CH, L)
+                               + LD(FF_CP, M) * LD(FF_VIST, M) / p.prt + LD(FF_CH, M));
+  double ul = LD(FF_U, L), um = LD(FF_U, M), vl = LD(FF_V, L), vm = LD(FF_V, M), wl = LD(FF_W, L), wm = LD(FF_W, M);
+  double duvwsj = nx * (dudx * sxi + dudy * syi + dudz * szi) + ny * (dvdx * sxi + dvdy * syi + dvdz * szi)
+                + nz * (dwdx * sxi + dwdy * syi + dwdz * szi);
+  double f2 = nx * s11i + ny * s12i + nz * s13i;
+  double f3 = nx * s12i + ny * s22i + nz * s23i;
+  double f4 = nx * s13i + ny * s23i + nz * s33i;
+  if (alfa > 0.) {
+    double adotu = nx * (ul - um) + ny * (vl - vm) + nz * (wl - wm);
+    double cc = adotu / slen - duvwsj;
+    f2 = alfa * ((ul - um) / slen - (sxi * dudx + syi * dudy + szi * dudz)) + sxi * cc + f2;
+    f3 = alfa * ((vl - vm) / slen - (sxi * dvdx + syi * dvdy + szi * dvdz)) + syi * cc + f3;
+    f4 = alfa * ((wl - wm) / slen - (sxi * dwdx + syi * dwdy + szi * dwdz)) + szi * cc + f4;
+  }
+  const double R23 = .6666667;
+  double dv = dudx + dvdy + dwdz;
+  f2 = surf * (f2 - R23 * nx * dv);
+  f3 = surf * (f3 - R23 * ny * dv);
+  f4 = surf * (f4 - R23 * nz * dv);
+  double f5 = .5 * ((ul + um) * f2 + (vl + vm) * f3 + (wl + wm) * f4) + surfe * (dtdxi * nx + dtdyi * ny + dtdzi * nz);
+  if (alfa > 0.)
+    f5 = surfe * alfa * ((LD(FF_TEMP, L) - LD(FF_TEMP, M)) / slen - sxi * dtdxi - syi * dtdyi - szi * dtdzi) + f5;
+#undef LD
+  f[0] = 0.; f[1] = -f2; f[2] = -f3; f[3] = -f4; f[4] = -f5;
+}
+
+// BOTSKE base3c.f:6147 wall-face flux (laminar, TURCOR false as FLUCYC passes
+// it, wall at rest).  II = interior cell at the wall.
+FF_DI void wall_flux(const DevBlock& b, const ff_params& p, size_t II, int S, int idir, int dir,
+                     int iheat, int intem, double f[5]) {
+#define LD(s, n) __ldg(b.a[s] + (n))
+  double rc1 = intem == 6 ? 1. : 1.5, rc2 = rc1 - 1.;
+  const double prs = p.pr / p.prt, ymr = .166666667, eps = 1.e-3;
+  int lstrid = S * idir;
+  size_t II2 = II + lstrid, IF1 = idir == 1 ? II : II + S;
+  int ihfl = (iheat == 2 || iheat >= 12) ? 1 : 0;
+  int iht = (iheat == 0 || iheat == 15) ? 0 : 1;
+  const int ao = 4 * (dir - 1);
+  double a_f = LD(FF_A1 + ao, IF1);
+  double dist = (a_f + LD(FF_A1 + ao, IF1 + lstrid)) / LD(FF_VOL, II);
+  double surg = -dist * ymr;
+  double visb = dmax(0.01 * p.frsvis, rc1 * LD(FF_VIS, II) - rc2 * LD(FF_VIS, II2));
+  double chsb = dmax(eps, rc1 * LD(FF_CH, II) - rc2 * LD(FF_CH, II2));
+  double pb1 = dmax(0.01 * p.frspre, rc1 * LD(FF_P, II) - rc2 * LD(FF_P, II2));
+  double surf = surg * visb;
+  double surfe = surg * (prs * 0. / visb + 1.) * chsb;
+  double tempb = dmax(0.01 * p.frstem, rc1 * LD(FF_TEMP, II) - rc2 * LD(FF_TEMP, II2));
+  double tsurf = iheat == 3 ? tempb : p.frstem;
+  double cvii = iht * idir * (9.000 * LD(FF_TEMP, II) - 1.000 * LD(FF_TEMP, II2) - 8. * tsurf);
+  double uvii = idir * (9.000 * LD(FF_U, II) - 1.000 * LD(FF_U, II2));
+  double vvii = idir * (9.000 * LD(FF_V, II) - 1.000 * LD(FF_V, II2));
+  double wvii = idir * (9.000 * LD(FF_W, II) - 1.000 * LD(FF_W, II2));
+  double ax = LD(FF_A1XA + ao, IF1), ay = LD(FF_A1YA + ao, IF1), az = LD(FF_A1ZA + ao, IF1);
+  double duc = .33333 * (ay * vvii + az * wvii + ax * uvii);
+  double f2v = surf * (uvii + ax * duc);
+  double f3v = surf * (vvii + ay * duc);
+  double f4v = surf * (wvii + az * duc);
+  double f5v = (1 - ihfl) * surfe * cvii;
+  f[0] = 0.;
+  f[1] = a_f * (ax * pb1 + f2v);
+  f[2] = a_f * (ay * pb1 + f3v);
+  f[3] = a_f * (az * pb1 + f4v);
+  f[4] = a_f * f5v;
+#undef LD
+}
+
+// Flux of one face (dir, cell L on the high side, normal index m).
+FF_DI void face_flux(const DevBlock& b, const ff_params& p, int dir, size_t L, int m, int t1, int t2,
+                     int level, double f[5]) {
+  const int S = dir == 1 ? 1 : (dir == 2 ? b.is : b.il);
+  const int nmax = dir == 1 ? b.imax : (dir == 2 ? b.jmax : b.kmax);
+  int intem = dir == 1 ? p.interi : (dir == 2 ? p.interj : p.interk);
+  if (level > 1) intem = p.coarse_inter;
+  // wall face?  (BOTSKE overwrites, res3c.f:8092)
+  if (m == 1 || m == nmax + 1) {
+    int iface = m == 1 ? dir : dir + 3;
+    for (int ip = 0; ip < b.npatch; ip++) {
+      const ff_patch& pa = b.patch[ip];
+      if (pa.iface != iface || pa.ityp < 8 || pa.ityp > 10) continue;
+      if (t1 < pa.r1a || t1 > pa.r1b || t2 < pa.r2a || t2 > pa.r2b) continue;
+      int idir = m == 1 ? 1 : -1;
+      size_t II = m == 1 ? L : L - S;
+      wall_flux(b, p, II, S, idir, dir, pa.iheat, intem, f);
+      return;
+    }
+  }
+  f[0] = f[1] = f[2] = f[3] = f[4] = 0.;
+  if (level == 1 && p.fullns) visc_flux(b, p, L, S, dir, f);
+  double q[5][4];
+  const int sl[5] = {FF_RO, FF_U, FF_V, FF_W, FF_P};
+#pragma unroll
+  for (int v = 0; v < 5; v++) {
+    const double* a = b.a[sl[v]];
+    q[v][0] = __ldg(a + L - 2 * S); q[v][1] = __ldg(a + L - S); q[v][2] = __ldg(a + L); q[v][3] = __ldg(a + L + S);
+  }
+  size_t L2 = dir == 3 ? L : L - S;
+  double cr[4] = {__ldg(b.a[FF_DRDP] + L), __ldg(b.a[FF_DRDH] + L), q[0][2], q[4][2]};
+  double cl[4] = {__ldg(b.a[FF_DRDP] + L2), __ldg(b.a[FF_DRDH] + L2), __ldg(b.a[FF_RO] + L2), __ldg(b.a[FF_P] + L2)};
+  const int ao = 4 * (dir - 1);
+  roe_flux(q, __ldg(b.a[FF_A1XA + ao] + L), __ldg(b.a[FF_A1YA + ao] + L), __ldg(b.a[FF_A1ZA + ao] + L),
+           __ldg(b.a[FF_A1 + ao] + L), intem, p, __ldg(b.a[FF_C] + L), __ldg(b.a[FF_C] + L - S), cr, cl, f);
+}
+
+// RESIDU: fused k, i, j face fluxes and SWEEP res3c.f:992 for a 32x4x4 tile.
+__global__ void __launch_bounds__(128) k_residual(DevBlock b, ff_params p, int level) {
+  __shared__ double sF[5][TI * (TJ + 1) * TK];   // 640 faces x 5
+  const int tid = threadIdx.x;
+  const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ, k0 = blockIdx.z * TK;
+  const int ci = tid % TI, cj = tid / TI;
+  double acc[TK][5];
+#pragma unroll
+  for (int c = 0; c < TK; c++)
+#pragma unroll
+    for (int v = 0; v < 5; v++) acc[c][v] = 0.;
+  // ---- k faces (SWEEP with KSTRID = IL, res3c.f:355) ----
+  for (int f = tid; f < TI * TJ * (TK + 1); f += blockDim.x) {
+    int fi = f % TI, fj = (f / TI) % TJ, fk = f / (TI * TJ);
+    int I = i0 + fi + 1, J = j0 + fj + 1, m = k0 + fk + 1;
+    if (I > b.imax || J > b.jmax || m > b.kmax + 1) continue;
+    double fl[5];
+    face_flux(b, p, 3, ix(b, I, J, m), m, I, J, level, fl);
+#pragma unroll
+    for (int v = 0; v < 5; v++) sF[v][f] = fl[v];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int c = 0; c < TK; c++) {
+    int f0 = ci + TI * (cj + TJ * c), f1 = ci + TI * (cj + TJ * (c + 1));
+    if (i0 + ci < b.imax && j0 + cj < b.jmax && k0 + c < b.kmax)
+#pragma unroll
+      for (int v = 0; v < 5; v++) acc[c][v] = acc[c][v] - (sF[v][f1] - sF[v][f0]);
+  }
+  __syncthreads();
+  // ---- i faces ----
+  for (int f = tid; f < (TI + 1) * TJ * TK; f += blockDim.x) {
+    int fi = f % (TI + 1), fj = (f / (TI + 1)) % TJ, fk = f / ((TI + 1) * TJ);
+    int m = i0 + fi + 1, J = j0 + fj + 1, K = k0 + fk + 1;
+    if (m > b.imax + 1 || J > b.jmax || K > b.kmax) continue;
+    double fl[5];
+    face_flux(b, p, 1, ix(b, m, J, K), m, J, K, level, fl);
+#pragma unroll
+    for (int v = 0; v < 5; v++) sF[v][f] = fl[v];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int c = 0; c < TK; c++) {
+    int f0 = ci + (TI + 1) * (cj + TJ * c);
+    if (i0 + ci < b.imax && j0 + cj < b.jmax && k0 + c < b.kmax)
+#pragma unroll
+      for (int v = 0; v < 5; v++) acc[c][v] = acc[c][v] - (sF[v][f0 + 1] - sF[v][f0]);
+  }
+  __syncthreads();
+  // ---- j faces, then 1/VOL (SWEEP IDO = 1) ----
+  for (int f = tid; f < TI * (TJ + 1) * TK; f += blockDim.x) {
+    int fi = f % TI, fj = (f / TI) % (TJ + 1), fk = f / (TI * (TJ + 1));
+    int I = i0 + fi + 1, m = j0 + fj + 1, K = k0 + fk + 1;
+    if (I > b.imax || m > b.jmax + 1 || K > b.kmax) continue;
+    double fl[5];
+    face_flux(b, p, 2, ix(b, I, m, K), m, I, K, level, fl);
+#pragma unroll
+    for (int v = 0; v < 5; v++) sF[v][f] = fl[v];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int c = 0; c < TK; c++) {
+    int I = i0 + ci + 1, J = j0 + cj + 1, K = k0 + c + 1;
+    if (I > b.imax || J > b.jmax || K > b.kmax) continue;
+    int f0 = ci + TI * (cj + (TJ + 1) * c), f1 = ci + TI * (cj + 1 + (TJ + 1) * c);
+    size_t n = ix(b, I, J, K);
+    double rv = 1. / __ldg(b.a[FF_VOL] + n);
+#pragma unroll
+    for (int v = 0; v < 5; v++) b.a[FF_DRO + v][n] = (acc[c][v] - (sF[v][f1] - sF[v][f0])) * rv;
+  }
+}
+
+// Sum of squares (RESL2 res3c.f:8920) of the five residuals into out[0..4].
+__global__ void k_resl2(DevBlock b, double* out) {
+  __shared__ double red[5][8];
+  double s[5] = {0, 0, 0, 0, 0};
+  int n_int = b.imax * b.jmax * b.kmax;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n_int; t += gridDim.x * blockDim.x) {
+    int I = t % b.imax + 1, J = (t / b.imax) % b.jmax + 1, K = t / (b.imax * b.jmax) + 1;
+    size_t n = ix(b, I, J, K);
+#pragma unroll
+    for (int v = 0; v < 5; v++) { double d = b.a[FF_DRO + v][n]; s[v] += d * d; }
+  }
+#pragma unroll
+  for (int v = 0; v < 5; v++) {
+    double x = s[v];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) == 0) red[v][threadIdx.x >> 5] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < 5) {
+    double x = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) x += red[threadIdx.x][w];
+    atomicAdd(out + threadIdx.x, x);
+  }
+}
+
+// TIME3 base3c.f:79 + LOCDT imps3.f:784 + COPR imps3.f:891 (interior cells).
+__global__ void k_time3_copr(DevBlock b, ff_params p, double cfl) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= b.imax * b.jmax * b.kmax) return;
+  int I = t % b.imax + 1, J = (t / b.imax) % b.jmax + 1, K = t / (b.imax * b.jmax) + 1;
+  const int IS = b.is, IL = b.il;
+  size_t kk = ix(b, I, J, K);
+#define LD(s, n) __ldg(b.a[s] + (n))
+  double a1 = LD(FF_A1, kk), a1p = LD(FF_A1, kk + 1), a2 = LD(FF_A2, kk), a2p = LD(FF_A2, kk + IS);
+  double a3 = LD(FF_A3, kk), a3p = LD(FF_A3, kk + IL);
+  double zz = 0.;
+  if (p.idi1 != 0 && I <= min(p.idi1, b.imax)) zz = .5 * (a1 + a1p);
+  if (p.idi2 != 0 && J <= min(p.idi2, b.jmax)) zz = dmax(.5 * (a2 + a2p), zz);
+  if (p.idi3 != 0 && K <= min(p.idi3, b.kmax)) zz = dmax(.5 * (a3 + a3p), zz);
+  double ro = b.a[FF_RO][kk], u = b.a[FF_U][kk], v = b.a[FF_V][kk], w = b.a[FF_W][kk];
+  double c = b.a[FF_C][kk], P = b.a[FF_P][kk];
+  double pvol = 1. / LD(FF_VOL, kk), ypro = 1. / (ro + 1.e-10);
+  double a1k = .5 * (a1 + a1p), a2k = .5 * (a2 + a2p), a3k = .5 * (a3 + a3p);
+  double ucii = .5 * (LD(FF_A1XA, kk) * a1 + LD(FF_A1XA, kk + 1) * a1p) * u
+              + .5 * (LD(FF_A1YA, kk) * a1 + LD(FF_A1YA, kk + 1) * a1p) * v
+              + .5 * (LD(FF_A1ZA, kk) * a1 + LD(FF_A1ZA, kk + 1) * a1p) * w;
+  double vcii = .5 * (LD(FF_A2XA, kk) * a2 + LD(FF_A2XA, kk + IS) * a2p) * u
+              + .5 * (LD(FF_A2YA, kk) * a2 + LD(FF_A2YA, kk + IS) * a2p) * v
+              + .5 * (LD(FF_A2ZA, kk) * a2 + LD(FF_A2ZA, kk + IS) * a2p) * w;
+  double wcii = .5 * (LD(FF_A3XA, kk) * a3 + LD(FF_A3XA, kk + IL) * a3p) * u
+              + .5 * (LD(FF_A3YA, kk) * a3 + LD(FF_A3YA, kk + IL) * a3p) * v
+              + .5 * (LD(FF_A3ZA, kk) * a3 + LD(FF_A3ZA, kk + IL) * a3p) * w;
+#undef LD
+  double b1 = pvol * (fabs(ucii) + fabs(vcii) + fabs(wcii) + c * sqrt(a1k * a1k + a2k * a2k + a3k * a3k)) / cfl;
+  double rnum = zz * zz * (pvol * pvol) * ypro;
+  double tt = rnum * (b.a[FF_VIS][kk] + p.pr / p.prt * b.a[FF_VIST][kk]) / p.cdiff;
+  double b11 = dmax(b1, 2. * tt * p.pvisc);
+  double denlow = 1. + dmax(0., (p.frspre - 2. * P) / P);
+  double denmax = 1. + dmax(0., (ro - 2. * p.frsden) * ypro) * 5.;
+  double dtl = 1. / (b11 * dmax(denlow, denmax));
+  b.a[FF_DTL][kk] = dtl;
+  // LOCDT + COPR
+  double dri = dtl * b.a[FF_DRO][kk], dmi = dtl * b.a[FF_DM][kk], dni = dtl * b.a[FF_DN][kk];
+  double dwi = dtl * b.a[FF_DW][kk], dre = dtl * b.a[FF_DE][kk];
+  double yp = 1. / ro, drodh = b.a[FF_DRDH][kk], drodp = b.a[FF_DRDP][kk];
+  double beta = .5 * (u * u + v * v + w * w);
+  double dkin = u * dmi + v * dni + w * dwi;
+  b.a[FF_DM][kk] = yp * (-u * dri + dmi);
+  b.a[FF_DN][kk] = yp * (-v * dri + dni);
+  b.a[FF_DW][kk] = yp * (-w * dri + dwi);
+  double hi = yp * (b.a[FF_E][kk] + P);
+  double dei = dre - (hi - 2 * beta) * dri - dkin;
+  double dpi = c * c * (dri - drodh * yp * dei);
+  b.a[FF_DRO][kk] = (dri - drodp * dpi) / drodh;
+  b.a[FF_DE][kk] = dpi;
+}
+
+// LU-SGS coefficients of each interior cell (PREDGS imps4.f:388-470 for
+// upper=1, CORRGS imps4.f:120-200 + DIAGGS imps4.f:604 for upper=0).
+// Layout: coef[c*ntot + n], c = xi(3) xj(3) xk(3) dt1 scinv scinp fdiag.
+template <typename CT>
+__global__ void k_lusgs_coef(DevBlock b, ff_params p, CT* coef, int upper) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= b.imax * b.jmax * b.kmax) return;
+  int I = t % b.imax + 1, J = (t / b.imax) % b.jmax + 1, K = t / (b.imax * b.jmax) + 1;
+  const int IS = b.is, IL = b.il;
+  size_t N = ix(b, I, J, K);
+#define LD(s, n) __ldg(b.a[s] + (n))
+  double u = LD(FF_U, N), v = LD(FF_V, N), w = LD(FF_W, N), c = LD(FF_C, N), ro = LD(FF_RO, N);
+  double vol = LD(FF_VOL, N), mu = LD(FF_VIST, N) + LD(FF_VIS, N);
+  const int st[3] = {1, IS, IL};
+  const int idi[3] = {p.idi1, p.idi2, p.idi3};
+  const int idx[3] = {I, J, K};
+  double xa[3], rmax_lo[3];
+  double x[3][3];
+  for (int d = 0; d < 3; d++) {
+    const int ao = 4 * d;
+    size_t fN = upper ? N : N + st[d];          // face normal used for the eigenvalue
+    size_t nb = upper ? N - st[d] : N + st[d];  // cell across that face
+    double ff = 2.;
+    if (upper && idx[d] == 1) ff = 4.;
+    if (idx[d] > idi[d]) ff = 0.;
+    double rl1 = LD(FF_A1XA + ao, fN) * u + LD(FF_A1YA + ao, fN) * v + LD(FF_A1ZA + ao, fN) * w;
+    double rnum = (vol + LD(FF_VOL, nb)) * (ro + LD(FF_RO, nb));
+    double tt = (ff * 2.) * LD(FF_A1 + ao, N) / rnum * (mu + LD(FF_VIST, nb) + LD(FF_VIS, nb));
+    double rmax = fabs(rl1) + c;
+    double sg = upper ? -1. : 1.;
+    x[d][0] = (rl1 + sg * rmax) * .5 + sg * tt;
+    x[d][1] = (rl1 + c + sg * rmax) * .5 + sg * tt;
+    x[d][2] = (rl1 - c + sg * rmax) * .5 + sg * tt;
+    xa[d] = rmax + tt;
+    // SCINP uses the low-face spectral radius in both sweeps
+    double rl1lo = LD(FF_A1XA + ao, N) * u + LD(FF_A1YA + ao, N) * v + LD(FF_A1ZA + ao, N) * w;
+    rmax_lo[d] = upper ? rmax : (fabs(rl1) + c);
+    (void)rl1lo;
+  }
+  double dt1 = p.theta * LD(FF_DTL, N);
+  double a1 = LD(FF_A1, N), a2 = LD(FF_A2, N), a3 = LD(FF_A3, N);
+  double a1p = LD(FF_A1, N + 1), a2p = LD(FF_A2, N + IS), a3p = LD(FF_A3, N + IL);
+  double scinv = upper ? 1. / (vol + dt1 * (xa[0] * a1 + xa[1] * a2 + xa[2] * a3))
+                       : 1. / (vol + dt1 * (xa[0] * a1p + xa[1] * a2p + xa[2] * a3p));
+  double scinp = 1. / (vol + dt1 * (rmax_lo[0] * a1 + rmax_lo[1] * a2 + rmax_lo[2] * a3));
+  double fdiag = 1.;
+  if (!upper) {   // DIAGGS imps4.f:614-660
+    double r[6];
+    for (int d = 0; d < 3; d++) {
+      const int ao = 4 * d;
+      size_t fp = N + st[d];
+      r[2 * d] = fabs(LD(FF_A1XA + ao, N) * u + LD(FF_A1YA + ao, N) * v + LD(FF_A1ZA + ao, N) * w) + c;
+      r[2 * d + 1] = fabs(LD(FF_A1XA + ao, fp) * u + LD(FF_A1YA + ao, fp) * v + LD(FF_A1ZA + ao, fp) * w) + c;
+    }
+    double sc = .5 * (a1 * r[0] + a1p * r[1] + a2 * r[2] + a2p * r[3] + a3 * r[4] + a3p * r[5]);
+    fdiag = 1. + p.theta * LD(FF_DTL, N) / vol * sc;
+  }
+#undef LD
+  size_t nt = b.ntot;
+  for (int d = 0; d < 3; d++)
+    for (int e = 0; e < 3; e++) coef[(3 * d + e) * nt + N] = (CT)x[d][e];
+  coef[9 * nt + N] = (CT)dt1;
+  coef[10 * nt + N] = (CT)scinv;
+  coef[11 * nt + N] = (CT)scinp;
+  coef[12 * nt + N] = (CT)fdiag;
+}
+
+// One LU-SGS sweep as i+j+k hyperplanes (cooperative, persistent).  The
+// triangular system is the reference's (PREDGS: neighbours i+1, j+1, k+1 with
+// the reference's dropped i+1 coupling in row J = JMAX, imps4.f:547-559;
+// CORRGS: i-1, j-1, k-1), so the result equals its slab-by-slab order.
+// dw: increment arrays (5 x ntot) of type CT; read through L2 (__ldcg)
+// because other blocks write them during the sweep.
+template <typename CT>
+__global__ void k_lusgs_sweep(DevBlock b, const CT* __restrict__ coef, CT* dw, int upper,
+                              unsigned* bar, int* err) {
+  const int IMAX = b.imax, JMAX = b.jmax, KMAX = b.kmax, IS = b.is, IL = b.il;
+  const size_t nt = b.ntot;
+  const int nthreads = gridDim.x * blockDim.x;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nplanes = IMAX + JMAX + KMAX - 2;
+  for (int s = 0; s < nplanes; s++) {
+    int m = upper ? IMAX + JMAX + KMAX - s : 3 + s;
+    int klo = max(1, m - IMAX - JMAX), khi = min(KMAX, m - 2);
+    int npairs = (khi - klo + 1) * JMAX;
+    for (int q = tid; q < npairs; q += nthreads) {
+      int K = klo + q / JMAX, J = q % JMAX + 1, I = m - J - K;
+      if (I < 1 || I > IMAX) continue;
+      size_t N = ix(b, I, J, K);
+      CT dt1 = coef[9 * nt + N];
+      CT vol = (CT)__ldg(b.a[FF_VOL] + N);
+      CT cd[5];
+      CT fd = upper ? CT(1) : coef[12 * nt + N];
+#pragma unroll
+      for (int v = 0; v < 5; v++) cd[v] = __ldcg(dw + v * nt + N) * fd;
+      // the three neighbours: k first (reference order), then i and j
+      CT ck[5] = {0, 0, 0, 0, 0}, yd[5] = {0, 0, 0, 0, 0}, bd[5] = {0, 0, 0, 0, 0};
+      const int st[3] = {1, IS, IL};
+      const bool has[3] = {upper ? (I < IMAX && J < JMAX) : (I > 1), upper ? (J < JMAX) : (J > 1),
+                           upper ? (K < KMAX) : (K > 1)};
+#pragma unroll
+      for (int d = 2; d >= 0; d--) {
+        if (!has[d]) continue;
+        size_t nb = upper ? N + st[d] : N - st[d];
+        size_t fN = upper ? nb : N;              // shared face
+        const int ao = 4 * d;
+        CT x[5];
+#pragma unroll
+        for (int v = 0; v < 5; v++) x[v] = __ldcg(dw + v * nt + nb);
+        CT out[5];
+        jac_product<CT>(out, x, (CT)__ldg(b.a[FF_C] + nb), (CT)__ldg(b.a[FF_RO] + nb),
+                        (CT)__ldg(b.a[FF_A1XA + ao] + fN), (CT)__ldg(b.a[FF_A1YA + ao] + fN),
+                        (CT)__ldg(b.a[FF_A1ZA + ao] + fN), coef[(3 * d) * nt + nb],
+                        coef[(3 * d + 1) * nt + nb], coef[(3 * d + 2) * nt + nb]);
+        CT* dst = d == 2 ? ck : (d == 0 ? yd : bd);
+#pragma unroll
+        for (int v = 0; v < 5; v++) dst[v] = out[v];
+      }
+      CT a3 = (CT)__ldg(b.a[FF_A3] + (upper ? N + IL : N));
+      CT a1 = (CT)__ldg(b.a[FF_A1] + (upper ? N + 1 : N));
+      CT a2 = (CT)__ldg(b.a[FF_A2] + (upper ? N + IS : N));
+      CT scinv = coef[10 * nt + N], scinp = coef[11 * nt + N];
+      CT res[5];
+#pragma unroll
+      for (int v = 0; v < 5; v++) {
+        CT x = upper ? (-dt1 * a3 * ck[v] + vol * cd[v]) : (dt1 * a3 * ck[v] + vol * cd[v]);
+        x = upper ? x - dt1 * (a1 * yd[v] + a2 * bd[v]) : x + dt1 * (a1 * yd[v] + a2 * bd[v]);
+        res[v] = x * (v < 4 ? scinv : scinp);
+      }
+#pragma unroll
+      for (int v = 0; v < 5; v++) __stcg(dw + v * nt + N, res[v]);
+    }
+    if (!grid_barrier(bar, bar + 1, gridDim.x, err)) return;
+  }
+}
+
+// Copy between the FP64 increment arrays and a CT work copy (FP32 LU-SGS).
+template <typename CT>
+__global__ void k_copy_dw(DevBlock b, CT* dw, int to_work) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= b.imax * b.jmax * b.kmax) return;
+  int I = t % b.imax + 1, J = (t / b.imax) % b.jmax + 1, K = t / (b.imax * b.jmax) + 1;
+  size_t n = ix(b, I, J, K);
+  for (int v = 0; v < 5; v++) {
+    if (to_work) dw[v * (size_t)b.ntot + n] = (CT)b.a[FF_DRO + v][n];
+    else b.a[FF_DRO + v][n] = (double)dw[v * (size_t)b.ntot + n];
+  }
+}
+
+// DRO/CP (imps3.f:483), FIN res3c.f:1077, the limits of CYCLES
+// (ns3c.f:1553-1596: UPLIM/LOLIM res3c.f:3314-3401, PDTOP, LOLIMP), the
+// interior *OLD copies of SUBIN and the max|dp| monitor (DROMXX, IDRXX=6).
+__global__ void k_fin(DevBlock b, ff_params p, unsigned long long* dromax_bits, int divide_cp) {
+  size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double amax = 0.;
+  if (n < (size_t)b.ntot) {
+    int i = (int)(n % b.is), j = (int)((n / b.is) % (b.jmax + 4)), k = (int)(n / b.il);
+    bool kin = k >= 2 && k < b.kmax + 2, jin = j >= 2 && j < b.jmax + 2;
+    bool interior = kin && jin && i >= 2 && i < b.imax + 2;
+    double T = b.a[FF_TEMP][n], U = b.a[FF_U][n], V = b.a[FF_V][n], W = b.a[FF_W][n], PD = b.a[FF_PDIFF][n];
+    if (interior) {
+      double dt = b.a[FF_DRO][n];
+      if (divide_cp) { dt = dt / b.a[FF_CP][n]; b.a[FF_DRO][n] = dt; }
+      T = b.a[FF_TOLD][n] + dt;
+      U = b.a[FF_UOLD][n] + b.a[FF_DM][n];
+      V = b.a[FF_VOLD][n] + b.a[FF_DN][n];
+      W = b.a[FF_WOLD][n] + b.a[FF_DW][n];
+      PD = b.a[FF_POLD][n] + b.a[FF_DE][n];
+      amax = fabs(b.a[FF_DE][n]);
+    }
+    if (kin && jin) {   // UPLIM range: interior k-planes, interior rows
+      T = dmin(T, p.tuplim); U = dmin(U, 5000.); V = dmin(V, 5000.); W = dmin(W, 5000.);
+    }
+    T = dmax(T, p.tlolim); U = dmax(U, -5000.); V = dmax(V, -5000.); W = dmax(W, -5000.);
+    double P = PD + p.frspre;
+    double prelim = dmin(0., P - 0.01 * p.frspre);
+    P = P - prelim; PD = PD - prelim;
+    b.a[FF_TEMP][n] = T; b.a[FF_U][n] = U; b.a[FF_V][n] = V; b.a[FF_W][n] = W;
+    b.a[FF_PDIFF][n] = PD; b.a[FF_P][n] = P;
+    if (interior) {
+      b.a[FF_TOLD][n] = T; b.a[FF_UOLD][n] = U; b.a[FF_VOLD][n] = V; b.a[FF_WOLD][n] = W;
+      b.a[FF_POLD][n] = PD;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) amax = dmax(amax, __shfl_down_sync(0xffffffffu, amax, o));
+  if ((threadIdx.x & 31) == 0 && amax > 0.) atomicMax(dromax_bits, (unsigned long long)__double_as_longlong(amax));
+}
+
+// Standalone DRO/CP that ends IMPS (imps3.f:483) when it is called as a stage.
+__global__ void k_fin_divide(DevBlock b) {
+  size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= (size_t)b.ntot) return;
+  int i = (int)(n % b.is), j = (int)((n / b.is) % (b.jmax + 4)), k = (int)(n / b.il);
+  if (i >= 2 && i < b.imax + 2 && j >= 2 && j < b.jmax + 2 && k >= 2 && k < b.kmax + 2)
+    b.a[FF_DRO][n] = b.a[FF_DRO][n] / b.a[FF_CP][n];
+}
+
+}  // namespace ff

@@ -1,0 +1,195 @@
+"""Python front end of libfinflo_gpu.so (ctypes over the C-ABI of
+include/finflo_gpu.h).
+
+This is the host-side mirror of the reference's block-routine interface: a
+``GpuSolver`` owns one device context and exposes the stage calls STATIM,
+RESIDU, RESL2, IMPS, FIN, BOUNDI (ns3c.f:10318, 2355, res3c.f:8920,
+ns3c.f:2683, res3c.f:1077, ns3c.f:10608) and the fused cycle loop of NS3D /
+CYCLES (ns3c.f:467-663).  There is no CPU fallback: if the CUDA library is
+missing or a device call fails, an exception is raised.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+from .case import FFPatch, FFParams, SLOT, SLOTS, Block
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfinflo_gpu.so")
+_SRC = [os.path.join(_HERE, "csrc", f) for f in ("ff_gpu.cu", "ff_kernels.cuh", "ff_device.cuh")]
+NVCC_FLAGS = ["-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
+              "-Xcompiler", "-fPIC", "-shared", "-std=c++17"]
+
+FF_STAGE_RESIDUAL, FF_STAGE_GRAD, FF_STAGE_STATE = 1, 2, 3
+
+
+class FinfloGpuError(RuntimeError):
+    pass
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile libfinflo_gpu.so in-tree for sm_100a (nvcc cross-compiles
+    without a GPU)."""
+    newest = max(os.path.getmtime(p) for p in _SRC + [os.path.join(_HERE, "..", "include", "finflo_gpu.h"),
+                                                      os.path.join(_HERE, "..", "include", "finflo_types.h")])
+    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < newest:
+        cmd = ["nvcc"] + NVCC_FLAGS + ["-o", LIB_PATH, _SRC[0]]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.check_call(cmd, cwd=os.path.join(_HERE, "csrc"))
+    return LIB_PATH
+
+
+_LIB = None
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise FinfloGpuError(f"{LIB_PATH} is missing: run __graft_entry__.build() first")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, ci, cd = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+        L.ff_last_error.restype = ctypes.c_char_p
+        L.ff_last_error.argtypes = [vp]
+        L.ff_create.argtypes = [ctypes.POINTER(vp), ci]
+        L.ff_destroy.argtypes = [vp]
+        L.ff_block_add.argtypes = [vp, ci, ci, ci, ci, ctypes.POINTER(FFPatch), ctypes.POINTER(FFParams)]
+        L.ff_block_params.argtypes = [vp, ci, ctypes.POINTER(FFParams)]
+        L.ff_upload.argtypes = [vp, ci, ci, ctypes.POINTER(cd)]
+        L.ff_download.argtypes = [vp, ci, ci, ctypes.POINTER(cd)]
+        L.ff_device_ptr.restype = vp
+        L.ff_device_ptr.argtypes = [vp, ci, ci]
+        L.ff_stream.restype = vp
+        L.ff_stream.argtypes = [vp]
+        L.ff_synchronize.argtypes = [vp]
+        for n in ("ff_statim", "ff_boundi"):
+            getattr(L, n).argtypes = [vp, ci]
+        L.ff_residu.argtypes = [vp, ci, ci, ci]
+        L.ff_resl2.argtypes = [vp, ci, ctypes.POINTER(cd)]
+        L.ff_imps.argtypes = [vp, ci, ci]
+        L.ff_fin.argtypes = [vp, ci, ctypes.POINTER(cd)]
+        L.ff_cycles.argtypes = [vp, ci, ci, ci, ctypes.POINTER(cd), ci]
+        L.ff_time_cycles.argtypes = [vp, ci, ci, ctypes.POINTER(ctypes.c_float)]
+        L.ff_time_stage.argtypes = [vp, ci, ci, ci, ctypes.POINTER(ctypes.c_float)]
+        _LIB = L
+    return _LIB
+
+
+def _dptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class GpuSolver:
+    """One device context holding one or more blocks."""
+
+    def __init__(self, device: int = 0):
+        self.L = lib()
+        h = ctypes.c_void_p()
+        self._check(self.L.ff_create(ctypes.byref(h), device), None)
+        self.ctx = h
+        self.blocks = []
+
+    def _check(self, rc, ctx="self"):
+        if rc != 0:
+            msg = self.L.ff_last_error(self.ctx if ctx == "self" else None)
+            raise FinfloGpuError(f"libfinflo_gpu error {rc}: {msg.decode() if msg else ''}")
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.L.ff_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- blocks --------------------------------------------------------
+    def add_block(self, blk: Block, prm: FFParams) -> int:
+        pats = blk.patch_array()
+        bid = self.L.ff_block_add(self.ctx, blk.imax, blk.jmax, blk.kmax, len(blk.patches),
+                                  ctypes.cast(pats, ctypes.POINTER(FFPatch)), ctypes.byref(prm))
+        if bid < 0:
+            self._check(-bid)
+        self.blocks.append((blk, prm))
+        return bid
+
+    def set_params(self, bid: int, prm: FFParams):
+        self._check(self.L.ff_block_params(self.ctx, bid, ctypes.byref(prm)))
+
+    def upload(self, bid: int, names=None):
+        blk = self.blocks[bid][0]
+        for n in names or SLOTS:
+            self._check(self.L.ff_upload(self.ctx, bid, SLOT[n], _dptr(blk.arrays[n])))
+        self.sync()
+
+    def download(self, bid: int, names=None, into=None) -> dict:
+        blk = self.blocks[bid][0]
+        out = {}
+        for n in names or SLOTS:
+            a = into[n] if into is not None else np.empty(blk.ntot)
+            self._check(self.L.ff_download(self.ctx, bid, SLOT[n], _dptr(a)))
+            out[n] = a
+        self.sync()
+        return out
+
+    def device_ptr(self, bid: int, name: str) -> int:
+        return self.L.ff_device_ptr(self.ctx, bid, SLOT[name])
+
+    def sync(self):
+        self._check(self.L.ff_synchronize(self.ctx))
+
+    # ---- stages (reference routine names) -------------------------------
+    def statim(self, bid=0):
+        self._check(self.L.ff_statim(self.ctx, bid))
+
+    def boundi(self, bid=0):
+        self._check(self.L.ff_boundi(self.ctx, bid))
+
+    def residu(self, bid=0, level=1, icycle=1):
+        self._check(self.L.ff_residu(self.ctx, bid, level, icycle))
+
+    def resl2(self, bid=0) -> np.ndarray:
+        r = (ctypes.c_double * 5)()
+        self._check(self.L.ff_resl2(self.ctx, bid, r))
+        return np.array(r[:])
+
+    def imps(self, bid=0, level=1):
+        self._check(self.L.ff_imps(self.ctx, bid, level))
+
+    def fin(self, bid=0) -> float:
+        d = ctypes.c_double()
+        self._check(self.L.ff_fin(self.ctx, bid, ctypes.byref(d)))
+        return d.value
+
+    def cycles(self, n, bid=0, icycle0=1, use_graph=True) -> np.ndarray:
+        hist = np.zeros((max(n, 1), 6))
+        self._check(self.L.ff_cycles(self.ctx, bid, n, icycle0, _dptr(hist), int(use_graph)))
+        return hist[:n]
+
+    def time_cycles(self, n, bid=0) -> float:
+        ms = ctypes.c_float()
+        self._check(self.L.ff_time_cycles(self.ctx, bid, n, ctypes.byref(ms)))
+        return ms.value
+
+    def time_stage(self, stage, reps=10, bid=0) -> float:
+        ms = ctypes.c_float()
+        self._check(self.L.ff_time_stage(self.ctx, bid, stage, reps, ctypes.byref(ms)))
+        return ms.value
+
+    def start(self, bid=0):
+        """NS3D start-up (ns3c.f:378-379): BOUNDI, then the *OLD copies."""
+        blk = self.blocks[bid][0]
+        self.boundi(bid)
+        self.sync()
+        st = self.download(bid, ["TEMP", "U", "V", "W", "PDIFF"])
+        for a, b2 in (("TOLD", "TEMP"), ("UOLD", "U"), ("VOLD", "V"), ("WOLD", "W"), ("POLD", "PDIFF")):
+            blk.arrays[a][:] = st[b2]
+        self.upload(bid, ["TOLD", "UOLD", "VOLD", "WOLD", "POLD"])

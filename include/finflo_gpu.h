@@ -1,0 +1,71 @@
+/*
+ * libfinflo_gpu.so -- C-ABI of the sm_100a FINFLO per-iteration hot path.
+ *
+ * One context = one CUDA device + one stream.  Blocks are stored on the
+ * device in the reference's own layout (finflo_types.h): every per-cell array
+ * is FP64, NTOT = (IMAX+4)*(JMAX+4)*(KMAX+4), i fastest, two ghost layers.
+ * Stage calls are asynchronous on the context's stream; ff_synchronize()
+ * waits and reports device-side time-outs.  Every function returns 0 on
+ * success or one of the FF_ERR_* codes (ff_last_error() has the message); no
+ * function aborts the process (the reference STOPs, e.g. ns3c.f:2209-2217).
+ *
+ * Reference interfaces replaced (Fortran, every argument by reference):
+ *   ff_statim    STATIM  ns3c.f:10318  (PDTOP, STATE/PERFGA, CONSVA, REFLEC)
+ *   ff_residu    RESIDI  ns3c.f:2355 -> RESIDU res3c.f:6 (level 1, laminar)
+ *   ff_resl2     RESL2   res3c.f:8920
+ *   ff_imps      IMPSDI  ns3c.f:2683 -> IMPS imps3.f:6 (LUSGS = 1)
+ *   ff_fin       FIN     res3c.f:1077 + the limits of CYCLES ns3c.f:1553-1596
+ *   ff_boundi    BOUNDI  ns3c.f:10608 (REFCOR, MIR, STATIM; single block)
+ *   ff_cycles    CYCLES  ns3c.f:1354 + BOUNDI + SUBIN per cycle, graph-replayed
+ */
+#ifndef FINFLO_GPU_H
+#define FINFLO_GPU_H
+#include "finflo_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FF_ABI_VERSION 1
+
+enum { FF_OK = 0, FF_ERR_CUDA = 1, FF_ERR_ARG = 2, FF_ERR_TIMEOUT = 3 };
+enum { FF_STAGE_RESIDUAL = 1, FF_STAGE_GRAD = 2, FF_STAGE_STATE = 3 };
+
+int ff_abi_version(void);
+const char *ff_last_error(void *ctx);
+
+int ff_create(void **ctx, int device);
+int ff_destroy(void *ctx);
+
+/* Add a block (one multigrid level); returns the block id (>= 0) or -code. */
+int ff_block_add(void *ctx, int imax, int jmax, int kmax, int npatch,
+                 const ff_patch *patches, const ff_params *prm);
+int ff_block_params(void *ctx, int blk, const ff_params *prm);
+
+/* Host <-> device copy of one per-cell array slot (enum ff_slot), NTOT doubles. */
+int ff_upload(void *ctx, int blk, int slot, const double *host);
+int ff_download(void *ctx, int blk, int slot, double *host);
+void *ff_device_ptr(void *ctx, int blk, int slot);
+void *ff_stream(void *ctx);
+int ff_synchronize(void *ctx);
+
+/* Stages (drop-in replacements of the reference routines listed above). */
+int ff_statim(void *ctx, int blk);
+int ff_boundi(void *ctx, int blk);
+int ff_residu(void *ctx, int blk, int level, int icycle);
+int ff_resl2(void *ctx, int blk, double *out5);
+int ff_imps(void *ctx, int blk, int level);
+int ff_fin(void *ctx, int blk, double *dromax);
+
+/* ncycles full cycles (RESIDU, RESL2, IMPS, FIN, BOUNDI, SUBIN); hist
+ * (nullable) receives ncycles x {RESI(31..35) sums of squares, DROMAX}. */
+int ff_cycles(void *ctx, int blk, int ncycles, int icycle0, double *hist, int use_graph);
+
+/* Timing helpers (CUDA events on the context stream). */
+int ff_time_cycles(void *ctx, int blk, int ncycles, float *ms);
+int ff_time_stage(void *ctx, int blk, int stage, int reps, float *ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

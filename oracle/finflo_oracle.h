@@ -1,0 +1,57 @@
+/*
+ * CPU oracle for the FINFLO per-iteration hot path (test infrastructure only).
+ *
+ * A restatement in C, FP64, of the reference Fortran routines on the path,
+ * in their loop and accumulation order.  It is the checker for the sm_100a
+ * library: only the tests, the smoke check and the bench's CPU-baseline leg
+ * call it.  PARITY UNPINNED: the reference has no tests, fixtures or golden
+ * vectors and no Fortran compiler exists on these machines, so the oracle is
+ * pinned only by the analytic invariants in tests/ (free-stream preservation,
+ * Roe consistency, rotational invariance, conservation).
+ */
+#ifndef FINFLO_ORACLE_H
+#define FINFLO_ORACLE_H
+#include "../include/finflo_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct orc_block {
+  int imax, jmax, kmax, npatch;
+  const ff_patch *patch;
+  double *a[FF_NSLOTS];
+} orc_block;
+
+int  orc_version(void);
+void orc_statim(orc_block *b, const ff_params *p);
+void orc_adjuin_laminar(orc_block *b);
+void orc_refcen(orc_block *b, const ff_params *p);
+void orc_gradients(orc_block *b, int level);
+void orc_inlet_outlet(orc_block *b, const ff_params *p, int dir, int icycle);
+void orc_flux_dir(orc_block *b, const ff_params *p, int dir, int level);
+void orc_sweep(orc_block *b, int dir, int ido);
+void orc_residu(orc_block *b, const ff_params *p, int level, int icycle);
+void orc_resl2(const orc_block *b, double *resi5);
+void orc_time3(orc_block *b, const ff_params *p, double cfl);
+void orc_locdt_copr(orc_block *b);
+void orc_predgs(orc_block *b, const ff_params *p);
+void orc_diaggs(orc_block *b, const ff_params *p);
+void orc_corrgs(orc_block *b, const ff_params *p);
+void orc_imps(orc_block *b, const ff_params *p, int level);
+void orc_fin_limits(orc_block *b, const ff_params *p);
+void orc_refcor(orc_block *b);
+void orc_mir(orc_block *b);
+void orc_subin(orc_block *b, double *dromax);
+void orc_boundi(orc_block *b, const ff_params *p);
+void orc_cycle(orc_block *b, const ff_params *p, int icycle, double *resi5, double *dromax);
+
+/* single-face kernels exposed for the invariant tests */
+void orc_roe_face(const double *qr, const double *ql, const double *qrr, const double *qll,
+                  const double *nrm, double area, int intem, const ff_params *p,
+                  const double *cell_r, const double *cell_l, int kquirk, double *f5);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

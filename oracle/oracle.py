@@ -1,0 +1,135 @@
+"""ctypes front end of the CPU oracle (test infrastructure only).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use
+this module, as the checker of the CUDA path.  PARITY UNPINNED (see
+finflo_oracle.h).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+from finflo_b200.case import FFPatch, FFParams, SLOTS
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+def build(force=False):
+    so = os.path.join(_HERE, "liboracle.so")
+    src = os.path.join(_HERE, "finflo_oracle.c")
+    if force or not os.path.exists(so) or os.path.getmtime(so) < os.path.getmtime(src):
+        subprocess.check_call(["make", "-s", "-C", _HERE, "liboracle.so", "CC=gcc"])
+    return so
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        _LIB = ctypes.CDLL(build())
+        L = _LIB
+        vp = ctypes.c_void_p
+        for name in ("orc_statim", "orc_refcen", "orc_time3", "orc_predgs", "orc_diaggs",
+                     "orc_corrgs", "orc_fin_limits", "orc_boundi"):
+            getattr(L, name).restype = None
+        L.orc_roe_face.restype = None
+    return _LIB
+
+
+class OrcBlock(ctypes.Structure):
+    _fields_ = [("imax", ctypes.c_int), ("jmax", ctypes.c_int), ("kmax", ctypes.c_int),
+                ("npatch", ctypes.c_int), ("patch", ctypes.POINTER(FFPatch)),
+                ("a", ctypes.c_void_p * len(SLOTS))]
+
+
+class Oracle:
+    """Wraps one block's numpy arrays (modified in place by the oracle)."""
+
+    def __init__(self, blk, prm: FFParams):
+        self.blk = blk
+        self.prm = prm
+        self._patches = blk.patch_array()
+        ob = OrcBlock()
+        ob.imax, ob.jmax, ob.kmax = blk.imax, blk.jmax, blk.kmax
+        ob.npatch = len(blk.patches)
+        ob.patch = ctypes.cast(self._patches, ctypes.POINTER(FFPatch))
+        for i, n in enumerate(SLOTS):
+            arr = blk.arrays[n]
+            assert arr.dtype == np.float64 and arr.flags.c_contiguous
+            ob.a[i] = arr.ctypes.data
+        self.ob = ob
+        self.L = lib()
+
+    def _b(self):
+        return ctypes.byref(self.ob)
+
+    def _p(self):
+        return ctypes.byref(self.prm)
+
+    def statim(self):
+        self.L.orc_statim(self._b(), self._p())
+
+    def boundi(self):
+        self.L.orc_boundi(self._b(), self._p())
+
+    def subin(self):
+        d = ctypes.c_double()
+        self.L.orc_subin(self._b(), ctypes.byref(d))
+        return d.value
+
+    def adjuin(self):
+        self.L.orc_adjuin_laminar(self._b())
+
+    def residu(self, level=1, icycle=1):
+        self.L.orc_residu(self._b(), self._p(), level, icycle)
+
+    def resl2(self):
+        r = (ctypes.c_double * 5)()
+        self.L.orc_resl2(self._b(), r)
+        return np.array(r[:])
+
+    def imps(self, level=1):
+        self.L.orc_imps(self._b(), self._p(), level)
+
+    def time3(self, cfl):
+        self.L.orc_time3(self._b(), self._p(), ctypes.c_double(cfl))
+
+    def locdt_copr(self):
+        self.L.orc_locdt_copr(self._b())
+
+    def predgs(self):
+        self.L.orc_predgs(self._b(), self._p())
+
+    def diaggs(self):
+        self.L.orc_diaggs(self._b(), self._p())
+
+    def corrgs(self):
+        self.L.orc_corrgs(self._b(), self._p())
+
+    def fin_limits(self):
+        self.L.orc_fin_limits(self._b(), self._p())
+
+    def cycle(self, icycle):
+        r = (ctypes.c_double * 5)()
+        d = ctypes.c_double()
+        self.L.orc_cycle(self._b(), self._p(), icycle, r, ctypes.byref(d))
+        return np.array(r[:]), d.value
+
+    def start(self):
+        """NS3D start-up: SUBIN(0), BOUNDI(1) (ns3c.f:378-379), then SUBIN copies."""
+        self.subin()
+        self.boundi()
+        self.subin()
+
+
+def roe_face(qr, ql, qrr, qll, nrm, area, intem, prm, cell_r, cell_l, kquirk=False):
+    L = lib()
+    D5 = ctypes.c_double * 5
+    f = D5(0, 0, 0, 0, 0)
+    L.orc_roe_face(D5(*qr), D5(*ql), D5(*qrr), D5(*qll), (ctypes.c_double * 3)(*nrm),
+                   ctypes.c_double(area), intem, ctypes.byref(prm), D5(*cell_r), D5(*cell_l),
+                   int(kquirk), f)
+    return np.array(f[:])

@@ -1,0 +1,156 @@
+"""Parity of the sm_100a path with the CPU oracle (needs a B200).
+
+Criteria: residual per cell within 1e-12 of the oracle,
+relative to max(|R|, S) with S = sum of |face flux|/VOL of the cell; stage
+outputs and fields after many cycles within the tolerances written per test.
+"""
+import numpy as np
+import pytest
+
+from finflo_b200.gpu import GpuSolver
+from oracle.oracle import Oracle
+from tests.util import flux_scale, interior, make_pair
+
+pytestmark = pytest.mark.gpu
+
+RES = ("DRO", "DM", "DN", "DW", "DE")
+
+
+def _setup(ni=17, nj=9, nk=9, **kw):
+    bg, bc, prm, fs = make_pair(ni, nj, nk, **kw)
+    o = Oracle(bc, prm)
+    o.start()
+    g = GpuSolver(0)
+    bid = g.add_block(bg, prm)
+    g.upload(bid)
+    g.start(bid)
+    return g, bid, bg, o, bc, prm
+
+
+def _cmp_state(g, bid, bg, bc, names, rtol):
+    d = g.download(bid, names)
+    for n in names:
+        ref, got = bc.arrays[n], d[n]
+        scale = np.abs(ref).max() + 1e-300
+        err = np.abs(got - ref).max() / scale
+        assert err <= rtol, (n, err)
+
+
+@pytest.mark.parametrize("dims", [(17, 9, 9), (33, 17, 9)])
+def test_statim_boundi(gpu_lib, dims):
+    g, bid, bg, o, bc, prm = _setup(*dims)
+    g.sync()
+    _cmp_state(g, bid, bg, bc, ["RO", "P", "PDIFF", "TEMP", "U", "V", "W", "C", "E", "VIS", "CH",
+                                 "DRDP", "DRDH", "RM", "RN", "RW", "EPS2", "VIST"], 1e-14)
+    g.close()
+
+
+@pytest.mark.parametrize("dims,inter", [((17, 9, 9), 3), ((33, 17, 9), 3), ((17, 9, 5), -3), ((17, 9, 9), 55)])
+def test_residual(gpu_lib, dims, inter):
+    g, bid, bg, o, bc, prm = _setup(*dims, inter=inter)
+    o.statim(); o.adjuin(); o.residu(1, 1)
+    g.residu(bid, 1, 1)
+    g.sync()
+    d = g.download(bid, list(RES) + ["S11", "S12", "W12", "DTDX", "DTDZ"])
+    S = flux_scale(o, bc)
+    for n in RES:
+        ref = interior(bc, bc.arrays[n]); got = interior(bg, d[n])
+        den = np.maximum(np.abs(ref), S[n]) + 1e-300
+        err = (np.abs(got - ref) / den).max()
+        assert err <= 1e-12, (n, err)
+    # gradients: interior + first ghost layer
+    for n in ("S11", "S12", "W12", "DTDX", "DTDZ"):
+        ref = bc.arrays[n].reshape(bc.kmax + 4, bc.jmax + 4, bc.imax + 4)[1:-1, 1:-1, 1:-1]
+        got = d[n].reshape(bc.kmax + 4, bc.jmax + 4, bc.imax + 4)[1:-1, 1:-1, 1:-1]
+        err = np.abs(got - ref).max() / (np.abs(ref).max() + 1e-300)
+        assert err <= 1e-12, (n, err)
+    g.close()
+
+
+def test_resl2(gpu_lib):
+    g, bid, bg, o, bc, prm = _setup()
+    o.statim(); o.adjuin(); o.residu(1, 1)
+    g.residu(bid, 1, 1)
+    r_g = g.resl2(bid)
+    r_c = o.resl2()
+    np.testing.assert_allclose(r_g, r_c, rtol=1e-10, atol=1e-300)
+    g.close()
+
+
+@pytest.mark.parametrize("dims", [(17, 9, 9), (25, 13, 7)])
+def test_imps_lusgs(gpu_lib, dims):
+    """The GPU hyperplane LU-SGS solves the reference's triangular systems
+    (incl. the dropped i+1 coupling in the last j row of PREDGS)."""
+    g, bid, bg, o, bc, prm = _setup(*dims)
+    o.statim(); o.adjuin(); o.residu(1, 1)
+    g.residu(bid, 1, 1)
+    # same residual on both sides, then IMPS
+    g.sync()
+    bg_res = g.download(bid, list(RES))
+    for n in RES:
+        bc.arrays[n][:] = bg_res[n]
+    o.imps(1)
+    g.imps(bid, 1)
+    g.sync()
+    d = g.download(bid, list(RES) + ["DTL"])
+    for n in list(RES) + ["DTL"]:
+        ref = interior(bc, bc.arrays[n]); got = interior(bg, d[n])
+        err = np.abs(got - ref).max() / (np.abs(ref).max() + 1e-300)
+        assert err <= 1e-11, (n, err)
+    g.close()
+
+
+def test_fin(gpu_lib):
+    g, bid, bg, o, bc, prm = _setup()
+    o.statim(); o.adjuin(); o.residu(1, 1); o.imps(1)
+    g.sync()
+    for n in RES:
+        bg.arrays[n][:] = bc.arrays[n]
+    g.upload(bid, list(RES))
+    dm_g = g.fin(bid)
+    o.fin_limits()
+    _cmp_state(g, bid, bg, bc, ["TEMP", "U", "V", "W", "PDIFF", "P"], 1e-15)
+    dm_c = np.abs(interior(bc, bc.arrays["DE"])).max()
+    assert abs(dm_g - dm_c) <= 1e-15 * dm_c
+    g.close()
+
+
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_cycles_match_oracle(gpu_lib, use_graph):
+    """30 full cycles: fields and residual history against the oracle."""
+    g, bid, bg, o, bc, prm = _setup(17, 9, 9)
+    n = 30
+    hist = g.cycles(n, bid, icycle0=1, use_graph=use_graph)
+    ref = np.array([o.cycle(i + 1)[0] for i in range(n)])
+    np.testing.assert_allclose(hist[:, :5], ref, rtol=1e-8)
+    d = g.download(bid, ["TEMP", "U", "V", "W", "PDIFF"])
+    for nme in d:
+        a = interior(bg, d[nme]); b = interior(bc, bc.arrays[nme])
+        rel = np.linalg.norm(a - b) / (np.linalg.norm(b) + 1e-300)
+        assert rel <= 1e-10, (nme, rel)
+    g.close()
+
+
+def test_fp32_lusgs_converges_to_fp64_answer(gpu_lib):
+    """FP32 implicit operator: the residual stays FP64, so the fixed point is
+    the FP64 one; after the same cycles the fields differ by a bounded amount."""
+    g, bid, bg, o, bc, prm = _setup(17, 9, 9)
+    prm32 = type(prm).from_buffer_copy(prm)
+    prm32.lusgs_fp32 = 1
+    g2 = GpuSolver(0)
+    bg2 = make_pair(17, 9, 9)[0]
+    b2 = g2.add_block(bg2, prm32)
+    g2.upload(b2)
+    g2.start(b2)
+    h64 = g.cycles(150, bid)
+    h32 = g2.cycles(150, b2)
+    assert np.isfinite(h32).all()
+    d64 = g.download(bid, ["TEMP", "U", "PDIFF"])
+    d32 = g2.download(b2, ["TEMP", "U", "PDIFF"])
+    for n in d64:
+        a, b = interior(bg, d64[n]), interior(bg2, d32[n])
+        rel = np.linalg.norm(a - b) / np.linalg.norm(b)
+        assert rel < 1e-3, (n, rel)
+    # both runs must be converging
+    assert h32[-1, 0] < h32[0, 0] and h64[-1, 0] < h64[0, 0]
+    g.close(); g2.close()

@@ -1,0 +1,32 @@
+"""Shared helpers of the parity tests."""
+import numpy as np
+
+from finflo_b200 import case
+
+
+def interior(blk, a):
+    return a.reshape(blk.kmax + 4, blk.jmax + 4, blk.imax + 4)[2:-2, 2:-2, 2:-2]
+
+
+def flux_scale(o, blk):
+    """S = sum over the six faces of |F|/VOL per cell and variable (the
+    normalisation of the 1e-12 residual parity criterion)."""
+    import ctypes
+    L = o.L
+    nt = blk.ntot
+    S = np.zeros((5, nt))
+    istr = blk.imax + 4
+    il = istr * (blk.jmax + 4)
+    for d, st in ((1, 1), (2, istr), (3, il)):
+        L.orc_flux_dir(o._b(), o._p(), d, 1)
+        for v, n in enumerate(("F1R", "F1RM", "F1RN", "F1RW", "F1E")):
+            F = np.abs(blk.arrays[n])
+            S[v, :nt - st] += F[:nt - st] + F[st:]
+    vol = blk.arrays["VOL"]
+    return {n: interior(blk, S[v] / vol) for v, n in enumerate(("DRO", "DM", "DN", "DW", "DE"))}
+
+
+def make_pair(ni=17, nj=9, nk=9, **kw):
+    bg, prm, fs = case.bump_case(ni, nj, nk, **kw)
+    bc, _, _ = case.bump_case(ni, nj, nk, **kw)
+    return bg, bc, prm, fs
