@@ -101,12 +101,12 @@ def box_nodes(x, y, z):
     return X.copy(), Y.copy(), Z.copy()
 
 
-def _extend(a: np.ndarray) -> np.ndarray:
-    """Add NG ghost node layers per side by mirror extrapolation x[-m] = 2x[0]-x[m]."""
+def _extend(a: np.ndarray, ng: int = NG) -> np.ndarray:
+    """Add ng ghost node layers per side by mirror extrapolation x[-m] = 2x[0]-x[m]."""
     for ax in range(3):
         n = a.shape[ax]
-        lo = [2 * np.take(a, 0, axis=ax) - np.take(a, m, axis=ax) for m in (2, 1)]
-        hi = [2 * np.take(a, n - 1, axis=ax) - np.take(a, n - 1 - m, axis=ax) for m in (1, 2)]
+        lo = [2 * np.take(a, 0, axis=ax) - np.take(a, m, axis=ax) for m in range(ng, 0, -1)]
+        hi = [2 * np.take(a, n - 1, axis=ax) - np.take(a, n - 1 - m, axis=ax) for m in range(1, ng + 1)]
         a = np.concatenate([np.expand_dims(t, ax) for t in lo] + [a]
                            + [np.expand_dims(t, ax) for t in hi], axis=ax)
     return a
@@ -129,12 +129,12 @@ METRIC_NAMES = ("A1", "A1XA", "A1YA", "A1ZA", "A2", "A2XA", "A2YA", "A2ZA",
                 "D1", "D2", "D3")
 
 
-def compute_metrics(X, Y, Z) -> Metrics:
-    """Metrics of all cells (ghosts included) from interior node arrays (nk,nj,ni)."""
+def compute_metrics(X, Y, Z, ng: int = NG, raw: bool = False):
+    """Metrics of all cells (ng ghost layers) from interior node arrays (nk,nj,ni)."""
     nk, nj, ni = X.shape
     imax, jmax, kmax = ni - 1, nj - 1, nk - 1
-    P = np.stack([_extend(X), _extend(Y), _extend(Z)], axis=-1)  # (kmax+5, jmax+5, imax+5, 3)
-    ks, js, is_ = kmax + 4, jmax + 4, imax + 4
+    P = np.stack([_extend(X, ng), _extend(Y, ng), _extend(Z, ng)], axis=-1)
+    ks, js, is_ = kmax + 2 * ng, jmax + 2 * ng, imax + 2 * ng
 
     def face_vec(c00, c11, c01, c10):
         return 0.5 * np.cross(c11 - c00, c01 - c10)
@@ -187,15 +187,78 @@ def compute_metrics(X, Y, Z) -> Metrics:
     out["D1"] = np.minimum(1e4, (vol + eps) / (out["A1"] + a1h + eps) * 2.0)
     out["D2"] = np.minimum(1e4, (vol + eps) / (out["A2"] + a2h + eps) * 2.0)
     out["D3"] = np.minimum(1e4, (vol + eps) / (out["A3"] + a3h + eps) * 2.0)
+    if raw:
+        return dict(S1=Si, S2=Sj, S3=Sk, S1h=Si_hi, S2h=Sj_hi, S3h=Sk_hi, VOL=vol, C=cen,
+                    dims=(imax, jmax, kmax), ng=ng)
     m = Metrics(imax, jmax, kmax)
     for k2 in METRIC_NAMES:
         m.arrays[k2] = np.ascontiguousarray(out[k2], dtype=np.float64).reshape(-1)
     return m
 
 
-def lump_metrics(fine: Metrics, X, Y, Z) -> Metrics:
-    """Coarse-level metrics from every second fine node (face vectors of the
-    coarse cell are sums of the fine sub-faces for planar faces; here the
-    coarse level is rebuilt from the coarse node subset, the standard
-    vertex-lumping of GRID1B/LUMPA1, gluebm.f:1492-1496)."""
-    return compute_metrics(X[::2, ::2, ::2], Y[::2, ::2, ::2], Z[::2, ::2, ::2])
+def _finish(S1, S2, S3, S1h, S2h, S3h, vol, cen, dims, ng):
+    """Metrics arrays (2 ghost layers) from face vectors, volumes and centres
+    given with ng >= 2 ghost layers."""
+    imax, jmax, kmax = dims
+    c = ng - NG
+    sl = (slice(c, c + kmax + 2 * NG), slice(c, c + jmax + 2 * NG), slice(c, c + imax + 2 * NG))
+    out = {}
+    for name, S in (("A1", S1), ("A2", S2), ("A3", S3)):
+        S = S[sl]
+        mag = np.sqrt(np.sum(S * S, -1))
+        safe = np.where(mag > 0, mag, 1.0)
+        out[name] = mag
+        out[name + "XA"] = S[..., 0] / safe
+        out[name + "YA"] = S[..., 1] / safe
+        out[name + "ZA"] = S[..., 2] / safe
+    v = vol[sl]
+    out["VOL"] = v
+    cc = cen[sl]
+    out["XC"], out["YC"], out["ZC"] = cc[..., 0], cc[..., 1], cc[..., 2]
+    eps = 1e-20
+    for d, Sh in (("1", S1h), ("2", S2h), ("3", S3h)):
+        ah = np.sqrt(np.sum(Sh[sl] ** 2, -1))
+        out["D" + d] = np.minimum(1e4, (v + eps) / (out["A" + d] + ah + eps) * 2.0)
+    m = Metrics(imax, jmax, kmax)
+    for k2 in METRIC_NAMES:
+        m.arrays[k2] = np.ascontiguousarray(out[k2], dtype=np.float64).reshape(-1)
+    return m
+
+
+def _lump(r):
+    """One coarsening step (GRID1B/LUMPA1 gluebm.f:1492-1496): coarse volumes
+    are sums of the 8 children, coarse face vectors sums of the 4 child
+    faces, centres volume-weighted; ng halves."""
+    ng = r["ng"]
+    imax, jmax, kmax = r["dims"]
+    assert ng % 2 == 0 and imax % 2 == 0 and jmax % 2 == 0 and kmax % 2 == 0
+    vol, cen = r["VOL"], r["C"]
+
+    def csum(a):  # sum over 2x2x2 children (k, j, i axes)
+        return (a[0::2, 0::2, 0::2] + a[0::2, 0::2, 1::2] + a[0::2, 1::2, 0::2] + a[0::2, 1::2, 1::2]
+                + a[1::2, 0::2, 0::2] + a[1::2, 0::2, 1::2] + a[1::2, 1::2, 0::2] + a[1::2, 1::2, 1::2])
+    vc = csum(vol)
+    cc = csum(cen * vol[..., None]) / vc[..., None]
+    S1 = r["S1"][0::2, 0::2, 0::2] + r["S1"][0::2, 1::2, 0::2] + r["S1"][1::2, 0::2, 0::2] + r["S1"][1::2, 1::2, 0::2]
+    S2 = r["S2"][0::2, 0::2, 0::2] + r["S2"][0::2, 0::2, 1::2] + r["S2"][1::2, 0::2, 0::2] + r["S2"][1::2, 0::2, 1::2]
+    S3 = r["S3"][0::2, 0::2, 0::2] + r["S3"][0::2, 0::2, 1::2] + r["S3"][0::2, 1::2, 0::2] + r["S3"][0::2, 1::2, 1::2]
+    S1h = r["S1h"][0::2, 0::2, 1::2] + r["S1h"][0::2, 1::2, 1::2] + r["S1h"][1::2, 0::2, 1::2] + r["S1h"][1::2, 1::2, 1::2]
+    S2h = r["S2h"][0::2, 1::2, 0::2] + r["S2h"][0::2, 1::2, 1::2] + r["S2h"][1::2, 1::2, 0::2] + r["S2h"][1::2, 1::2, 1::2]
+    S3h = r["S3h"][1::2, 0::2, 0::2] + r["S3h"][1::2, 0::2, 1::2] + r["S3h"][1::2, 1::2, 0::2] + r["S3h"][1::2, 1::2, 1::2]
+    return dict(S1=S1, S2=S2, S3=S3, S1h=S1h, S2h=S2h, S3h=S3h, VOL=vc, C=cc,
+                dims=(imax // 2, jmax // 2, kmax // 2), ng=ng // 2)
+
+
+def mg_metrics(X, Y, Z, nlev: int):
+    """Metrics of every multigrid level (level 1 first), coarse levels
+    lumped from the fine cells so that the 8 children of a coarse cell fill
+    it exactly (volumes and face vectors add up)."""
+    ng = NG * 2 ** (nlev - 1)
+    r = compute_metrics(X, Y, Z, ng=ng, raw=True)
+    levels = []
+    for lev in range(nlev):
+        levels.append(_finish(r["S1"], r["S2"], r["S3"], r["S1h"], r["S2h"], r["S3h"], r["VOL"], r["C"],
+                              r["dims"], r["ng"]))
+        if lev + 1 < nlev:
+            r = _lump(r)
+    return levels

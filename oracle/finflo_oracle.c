@@ -143,14 +143,10 @@ static void reflec(orc_block *b, const ff_params *p) {
   }
 }
 
-/* STATIM is applied twice per cycle by the reference (BOUNDI ns3c.f:10896,
- * 10905, then CYCLES ns3c.f:1450); the second application sees the ghost
- * pressures REFLEC wrote.  Two passes reproduce that fixed point. */
+/* One STATIM call: equation of state on every cell, then REFLEC. */
 void orc_statim(orc_block *b, const ff_params *p) {
-  for (int pass = 0; pass < 2; pass++) {
-    state_cells(b, p);
-    reflec(b, p);
-  }
+  state_cells(b, p);
+  reflec(b, p);
 }
 
 /* TURBDI laminar branch: ADJUIN EPS2=1, VIST=0 on internal cells (res3c.f:9447). */
@@ -614,6 +610,28 @@ static void fluxbl_face(const orc_block *b, const ff_params *p, size_t L, int S,
   F[0] = 0.; F[1] = -f2; F[2] = -f3; F[3] = -f4; F[4] = 0. - f5;
 }
 
+/* FLUXDO base3c.f:3677 (thin layer, IDIFF=1): the viscous flux on coarse
+ * levels and whenever FULLNS is off. */
+static void fluxdo_face(const orc_block *b, const ff_params *p, size_t L, int S, int dir, double *F) {
+  const double *A = b->a[FF_A1 + 4 * (dir - 1)], *NX = b->a[FF_A1XA + 4 * (dir - 1)];
+  const double *NY = b->a[FF_A1YA + 4 * (dir - 1)], *NZ = b->a[FF_A1ZA + 4 * (dir - 1)];
+  const double *VOL = b->a[FF_VOL], *U = b->a[FF_U], *V = b->a[FF_V], *W = b->a[FF_W], *T = b->a[FF_TEMP];
+  const double *VIS = b->a[FF_VIS], *EPS2 = b->a[FF_EPS2], *VIST = b->a[FF_VIST];
+  const double *CP = b->a[FF_CP], *CH = b->a[FF_CH];
+  size_t M = L - S;
+  double ypd2 = A[L] / (VOL[L] + VOL[M]);
+  double surg = -A[L] * ypd2;
+  double surf = surg * (EPS2[L] * VIS[L] + EPS2[M] * VIS[M]);
+  double surfe = surg * (CP[L] * VIST[L] / p->prt + CH[L] + CP[M] * VIST[M] / p->prt + CH[M]);
+  double duc = .333333 * (NX[L] * (U[L] - U[M]) + NY[L] * (V[L] - V[M]) + NZ[L] * (W[L] - W[M]));
+  double f2 = surf * (U[L] - U[M] + NX[L] * duc);
+  double f3 = surf * (V[L] - V[M] + NY[L] * duc);
+  double f4 = surf * (W[L] - W[M] + NZ[L] * duc);
+  double f5 = .5 * ((U[L] + U[M]) * f2 + (V[L] + V[M]) * f3 + (W[L] + W[M]) * f4);
+  F[0] = 0.; F[1] = f2; F[2] = f3; F[3] = f4;
+  F[4] = 0. + f5 + surfe * (T[L] - T[M]);
+}
+
 /* BOTSKE base3c.f:6147-6760: solid-wall face flux on level 1, laminar,
  * TURCOR=.FALSE. (the value FLUCYC passes, res3c.f:8107), wall at rest. */
 static void botske_face(const orc_block *b, const ff_params *p, size_t II, int S, int idir,
@@ -697,6 +715,7 @@ void orc_flux_dir(orc_block *b, const ff_params *p, int dir, int level) {
         size_t L = dir == 1 ? IX(d, m, t1, t2) : (dir == 2 ? IX(d, t1, m, t2) : IX(d, t1, t2, m));
         double f[5] = {0, 0, 0, 0, 0};
         if (level == 1 && p->fullns) fluxbl_face(b, p, L, S, dir, f);
+        else fluxdo_face(b, p, L, S, dir, f);
         double q[5][4];
         const double *arr[5] = {RO, U, V, W, P};
         for (int v = 0; v < 5; v++) {
@@ -711,7 +730,7 @@ void orc_flux_dir(orc_block *b, const ff_params *p, int dir, int level) {
         for (int v = 0; v < 5; v++) F[v][L] = f[v];
       }
   /* wall faces: BOTSKE overwrites (res3c.f:8092, only where IDIM > KBOT) */
-  if (level == 1) {
+  {
     for (int ip = 0; ip < b->npatch; ip++) {
       const ff_patch *pa = &b->patch[ip];
       if (pa->ityp < 8 || pa->ityp > 10) continue;
@@ -757,7 +776,7 @@ void orc_residu(orc_block *b, const ff_params *p, int level, int icycle) {
   for (int s = FF_W12; s <= FF_W23; s++) memset(b->a[s], 0, sizeof(double) * d.ntot);
   for (int s = FF_DTDX; s <= FF_DTDZ; s++) memset(b->a[s], 0, sizeof(double) * d.ntot);
   if (level == 1) orc_refcen(b, p);
-  if (p->fullns) orc_gradients(b, level);
+  if (p->fullns && level == 1) orc_gradients(b, level);
   const int order[3] = {3, 1, 2};
   for (int o = 0; o < 3; o++) {
     int dir = order[o];
@@ -1277,11 +1296,13 @@ void orc_subin(orc_block *b, double *dromax) {
   memcpy(b->a[FF_POLD], b->a[FF_PDIFF], sizeof(double) * d.ntot);
 }
 
-/* BOUNDI ns3c.f:10608 for one block without 1:1 connections:
- * REFCOR, MIR, STATIM. */
+/* BOUNDI ns3c.f:10608 for one block without 1:1 connections: REFCOR, MIR,
+ * and STATIM before and after CONNEC (ns3c.f:10896, 10905); the second
+ * STATIM sees the ghost pressures the first REFLEC wrote. */
 void orc_boundi(orc_block *b, const ff_params *p) {
   orc_refcor(b);
   orc_mir(b);
+  orc_statim(b, p);
   orc_statim(b, p);
 }
 
@@ -1295,5 +1316,168 @@ void orc_cycle(orc_block *b, const ff_params *p, int icycle, double *resi5, doub
   orc_imps(b, p, 1);
   orc_fin_limits(b, p);
   orc_boundi(b, p);
+  orc_subin(b, dromax);
+}
+
+/* ---------------------------------------------------------------------- */
+/* Multigrid (FAS V-cycle of CYCLES ns3c.f:1607-2170)                      */
+/* ---------------------------------------------------------------------- */
+
+/* TRANSF multi.f:156: volume-weighted 8 -> 1 restriction of TEMP,U,V,W,PD,
+ * EPS2,VIST and of the residuals into the coarse forcing P2H, the coarse
+ * *OLD copies, and the coarse ghost rings (multi.f:250-432). */
+void orc_transf(orc_block *f, orc_block *c) {
+  dims_t df = dims_of(f), dc = dims_of(c);
+  static const int vs[7] = {FF_TEMP, FF_U, FF_V, FF_W, FF_PDIFF, FF_EPS2, FF_VIST};
+  static const int rs[5] = {FF_DRO, FF_DM, FF_DN, FF_DW, FF_DE};
+  static const int ps[5] = {FF_ROP2H, FF_RMP2H, FF_RNP2H, FF_RWP2H, FF_EP2H};
+  const double *VOL = f->a[FF_VOL], *VOL2 = c->a[FF_VOL];
+  for (int K = 0; K <= dc.kmax + 1; K++)
+    for (int J = 0; J <= dc.jmax + 1; J++)
+      for (int I = 0; I <= dc.imax + 1; I++) {
+        size_t N = IX(dc, I, J, K);
+        size_t ijk = IX(df, 2 * I - 1, 2 * J - 1, 2 * K - 1);
+        size_t ipjk = ijk + 1, ijpk = ijk + df.is, ipjpk = ijk + df.is + 1;
+        size_t ijkp = ijk + df.il, ipjpkp = ipjpk + df.il, ijpkp = ijpk + df.il, ipjkp = ipjk + df.il;
+        double pvol = 1. / VOL2[N];
+#define R8(X) ((VOL[ipjpk] * X[ipjpk] + VOL[ijk] * X[ijk] + VOL[ipjk] * X[ipjk] + VOL[ijpk] * X[ijpk] + \
+                VOL[ipjpkp] * X[ipjpkp] + VOL[ijkp] * X[ijkp] + VOL[ipjkp] * X[ipjkp] + VOL[ijpkp] * X[ijpkp]) * pvol)
+        for (int v = 0; v < 7; v++) { const double *X = f->a[vs[v]]; c->a[vs[v]][N] = R8(X); }
+        for (int v = 0; v < 5; v++) { const double *X = f->a[rs[v]]; c->a[ps[v]][N] = R8(X); }
+#undef R8
+      }
+  for (int K = 1; K <= dc.kmax; K++)
+    for (int J = 1; J <= dc.jmax; J++)
+      for (int I = 1; I <= dc.imax; I++) {
+        size_t N = IX(dc, I, J, K);
+        c->a[FF_TOLD][N] = c->a[FF_TEMP][N];
+        c->a[FF_UOLD][N] = c->a[FF_U][N];
+        c->a[FF_VOLD][N] = c->a[FF_V][N];
+        c->a[FF_WOLD][N] = c->a[FF_W][N];
+        c->a[FF_POLD][N] = c->a[FF_PDIFF][N];
+      }
+  /* ghost rings: P2H zero on both ghost layers, state copied outward from
+   * the first ghost layer (order of multi.f: low i, high i, high j, low j,
+   * low k, high k) */
+  #define RING(N0, OFF)                                                          \
+    do {                                                                         \
+      size_t n0 = (N0);                                                          \
+      for (int v = 0; v < 5; v++) { c->a[ps[v]][n0] = 0.; c->a[ps[v]][n0 + (OFF)] = 0.; } \
+      for (int v = 0; v < 7; v++) c->a[vs[v]][n0 + (OFF)] = c->a[vs[v]][n0];     \
+    } while (0)
+  for (int K = -1; K <= dc.kmax + 2; K++)
+    for (int J = -1; J <= dc.jmax + 2; J++) RING(IX(dc, 0, J, K), -1);
+  for (int K = -1; K <= dc.kmax + 2; K++)
+    for (int J = -1; J <= dc.jmax + 2; J++) RING(IX(dc, dc.imax + 1, J, K), 1);
+  for (int K = -1; K <= dc.kmax + 2; K++)
+    for (int I = -1; I <= dc.imax + 2; I++) RING(IX(dc, I, dc.jmax + 1, K), dc.is);
+  for (int K = -1; K <= dc.kmax + 2; K++)
+    for (int I = -1; I <= dc.imax + 2; I++) RING(IX(dc, I, 0, K), -dc.is);
+  for (int J = -1; J <= dc.jmax + 2; J++)
+    for (int I = -1; I <= dc.imax + 2; I++) RING(IX(dc, I, J, 0), -dc.il);
+  for (int J = -1; J <= dc.jmax + 2; J++)
+    for (int I = -1; I <= dc.imax + 2; I++) RING(IX(dc, I, J, dc.kmax + 1), dc.il);
+  #undef RING
+}
+
+/* FORCFU multi.f:1609: P2H -= R (every cell of the level). */
+void orc_forcfu(orc_block *c) {
+  dims_t d = dims_of(c);
+  for (int v = 0; v < 5; v++)
+    for (int n = 0; n < d.ntot; n++) c->a[FF_ROP2H + v][n] = c->a[FF_ROP2H + v][n] - c->a[FF_DRO + v][n];
+}
+
+/* ADDRES multi.f:1686: R = P2H + R. */
+void orc_addres(orc_block *c) {
+  dims_t d = dims_of(c);
+  for (int v = 0; v < 5; v++)
+    for (int n = 0; n < d.ntot; n++) c->a[FF_DRO + v][n] = c->a[FF_ROP2H + v][n] + c->a[FF_DRO + v][n];
+}
+
+/* INTERP multi.f:1763: inject the coarse correction into the 8 children. */
+void orc_interp(orc_block *c, orc_block *f) {
+  dims_t dc = dims_of(c), df = dims_of(f);
+  for (int K = 1; K <= df.kmax; K++)
+    for (int J = 1; J <= df.jmax; J++)
+      for (int I = 1; I <= df.imax; I++) {
+        size_t N = IX(dc, (I + 1) / 2, (J + 1) / 2, (K + 1) / 2), F = IX(df, I, J, K);
+        double dto = c->a[FF_TEMP][N] - c->a[FF_TOLD][N];
+        double du = c->a[FF_U][N] - c->a[FF_UOLD][N];
+        double dv = c->a[FF_V][N] - c->a[FF_VOLD][N];
+        double dw = c->a[FF_W][N] - c->a[FF_WOLD][N];
+        double dp = c->a[FF_PDIFF][N] - c->a[FF_POLD][N];
+        f->a[FF_TEMP][F] = f->a[FF_TEMP][F] + dto;
+        f->a[FF_U][F] = f->a[FF_U][F] + du;
+        f->a[FF_V][F] = f->a[FF_V][F] + dv;
+        f->a[FF_W][F] = f->a[FF_W][F] + dw;
+        f->a[FF_P][F] = f->a[FF_P][F] + dp;
+        f->a[FF_PDIFF][F] = f->a[FF_PDIFF][F] + dp;
+      }
+}
+
+/* FIN on a coarse level and the limits after it (ns3c.f:1935-1990) or after
+ * INTERP (ns3c.f:2059-2125): UPLIM/LOLIM of TEMP and LOLIMP, without PDTOP. */
+static void temp_p_limits(orc_block *b, const ff_params *p) {
+  dims_t d = dims_of(b);
+  double *T = b->a[FF_TEMP], *P = b->a[FF_P], *PD = b->a[FF_PDIFF];
+  for (int K = 1; K <= d.kmax; K++) {
+    size_t ia = (size_t)(K + 1) * d.il + 2 * d.is;
+    for (int i = 0; i < d.jmax * d.is; i++) T[ia + i] = MIND(T[ia + i], p->tuplim);
+  }
+  for (int n = 0; n < d.ntot; n++) T[n] = MAXD(T[n], p->tlolim);
+  for (int n = 0; n < d.ntot; n++) {
+    double prelim = MIND(0., P[n] - 0.01 * p->frspre);
+    P[n] = P[n] - prelim;
+    PD[n] = PD[n] - prelim;
+  }
+}
+
+void orc_fin_coarse(orc_block *b, const ff_params *p) {
+  dims_t d = dims_of(b);
+  for (int K = 1; K <= d.kmax; K++)
+    for (int J = 1; J <= d.jmax; J++)
+      for (int I = 1; I <= d.imax; I++) {
+        size_t n = IX(d, I, J, K);
+        b->a[FF_TEMP][n] = b->a[FF_TOLD][n] + b->a[FF_DRO][n];
+        b->a[FF_U][n] = b->a[FF_UOLD][n] + b->a[FF_DM][n];
+        b->a[FF_V][n] = b->a[FF_VOLD][n] + b->a[FF_DN][n];
+        b->a[FF_W][n] = b->a[FF_WOLD][n] + b->a[FF_DW][n];
+        b->a[FF_PDIFF][n] = b->a[FF_POLD][n] + b->a[FF_DE][n];
+      }
+  temp_p_limits(b, p);
+}
+
+void orc_interp_limits(orc_block *c, orc_block *f, const ff_params *pf) {
+  orc_interp(c, f);
+  temp_p_limits(f, pf);
+}
+
+/* One multigrid cycle of CYCLES (ns3c.f:1400-2170) with BOUNDI and SUBIN.
+ * lv[0] is the fine level; prm[m] are the level's parameters (IDM1..3). */
+void orc_mg_cycle(orc_block **lv, int nlev, const ff_params *prm, int icycle, double *resi5, double *dromax) {
+  orc_block *b = lv[0];
+  orc_statim(b, &prm[0]);
+  orc_adjuin_laminar(b);
+  orc_residu(b, &prm[0], 1, icycle);
+  orc_resl2(b, resi5);
+  orc_imps(b, &prm[0], 1);
+  orc_fin_limits(b, &prm[0]);
+  for (int m = 1; m < nlev; m++) {          /* down: level m (0-based) */
+    orc_block *f = lv[m - 1], *c = lv[m];
+    orc_statim(f, &prm[m - 1]);
+    orc_residu(f, &prm[m - 1], m, icycle);
+    if (m == 1) orc_resl2(f, resi5);
+    if (m > 1) orc_addres(f);
+    orc_transf(f, c);
+    orc_statim(c, &prm[m]);
+    orc_residu(c, &prm[m], m + 1, icycle);
+    orc_forcfu(c);
+    orc_addres(c);
+    orc_imps(c, &prm[m], m + 1);
+    orc_fin_coarse(c, &prm[m]);
+  }
+  for (int m = nlev - 1; m >= 1; m--) orc_interp_limits(lv[m], lv[m - 1], &prm[m - 1]);
+  reflec(b, &prm[0]);
+  orc_boundi(b, &prm[0]);
   orc_subin(b, dromax);
 }

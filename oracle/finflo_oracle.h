@@ -45,6 +45,13 @@ void orc_mir(orc_block *b);
 void orc_subin(orc_block *b, double *dromax);
 void orc_boundi(orc_block *b, const ff_params *p);
 void orc_cycle(orc_block *b, const ff_params *p, int icycle, double *resi5, double *dromax);
+void orc_transf(orc_block *f, orc_block *c);
+void orc_forcfu(orc_block *c);
+void orc_addres(orc_block *c);
+void orc_interp(orc_block *c, orc_block *f);
+void orc_fin_coarse(orc_block *b, const ff_params *p);
+void orc_interp_limits(orc_block *c, orc_block *f, const ff_params *pf);
+void orc_mg_cycle(orc_block **lv, int nlev, const ff_params *prm, int icycle, double *resi5, double *dromax);
 
 /* single-face kernels exposed for the invariant tests */
 void orc_roe_face(const double *qr, const double *ql, const double *qrr, const double *qll,

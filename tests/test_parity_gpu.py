@@ -103,6 +103,7 @@ def test_imps_lusgs(gpu_lib, dims):
 def test_fin(gpu_lib):
     g, bid, bg, o, bc, prm = _setup()
     o.statim(); o.adjuin(); o.residu(1, 1); o.imps(1)
+    g.residu(bid, 1, 1)    # same ghost updates (REFCEN, INLET/OUTLET) on both sides
     g.sync()
     for n in RES:
         bg.arrays[n][:] = bc.arrays[n]
