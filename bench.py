@@ -172,7 +172,10 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     from finflo_b200 import case
     from finflo_b200.gpu import GpuSolver, FF_STAGE_RESIDUAL
-    blk, prm, fs = case.bump_case(WORKLOAD["ni"], WORKLOAD["nj"], WORKLOAD["nk"])
+    wl = dict(WORKLOAD)
+    if args.grid:
+        wl["ni"], wl["nj"], wl["nk"] = (int(x) for x in args.grid.split(","))
+    blk, prm, fs = case.bump_case(wl["ni"], wl["nj"], wl["nk"])
     g = GpuSolver(local)
     bid = g.add_block(blk, prm)
     g.upload(bid)
@@ -194,13 +197,13 @@ def run_ours(args):
     bytes_per_cell = 288.0   # algorithmic bytes of the laminar FP64 residual
     achieved = bytes_per_cell * ncell / (ms_res * 1e-3) / 1e9
     peak, kind = _peaks()
+    launches = g.cycle_launches(bid) * args.steps
     # ---- end to end through the C-ABI with host buffers ----------------
-    import ctypes
     names_in = ["TEMP", "U", "V", "W", "PDIFF"]
     host = {n: blk.arrays[n] for n in names_in}
     h2d = d2h = 0
     t0 = time.perf_counter()
-    for s in range(args.steps):
+    for s in range(0 if args.no_e2e else args.steps):
         g.upload(bid, names_in)
         h2d += 8 * blk.ntot * len(names_in)
         hist = g.cycles(1, bid, icycle0=2)
@@ -209,23 +212,24 @@ def run_ours(args):
     g.sync()
     e2e_s = time.perf_counter() - t0
     e2e_s = _allreduce_max(e2e_s, ws)
-    e2e = ncell * args.steps * ws / e2e_s
+    e2e = ncell * args.steps * ws / e2e_s if not args.no_e2e else None
     line = {
         "metric": "cell-iters/s", "value": value, "unit": "cell-iters/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded bump-channel grid and noisy free stream)",
-        "config": {"workload": WORKLOAD_NAME, "cells_per_gpu": ncell, "parallelism": f"replicas x{ws}",
+        "config": {"workload": WORKLOAD_NAME if not args.grid else f"bump channel {blk.imax}x{blk.jmax}x{blk.kmax} cells (profiling size)",
+                   "cells_per_gpu": ncell, "parallelism": f"replicas x{ws}",
                    "l2": "working set < L2 (cycle state resident)"},
-        "gpu_launches": None,
+        "gpu_launches": launches,
         "roofline": {"bound": "hbm", "kernel": "k_residual", "achieved": achieved, "peak": peak,
                      "peak_kind": kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
                      "ms_per_launch": ms_res, "bytes_per_cell": bytes_per_cell},
-        "e2e": {"value": e2e, "unit": "cell-iters/s", "h2d_bytes_per_step": h2d // args.steps,
-                "d2h_bytes_per_step": d2h // args.steps},
+        "e2e": {"value": e2e, "unit": "cell-iters/s", "h2d_bytes_per_step": h2d // max(1, args.steps),
+                "d2h_bytes_per_step": d2h // max(1, args.steps)},
         "clocks": clocks,
     }
-    if rank == 0 and not args.no_cpu:
+    if rank == 0 and not args.no_cpu and not args.grid:
         rate, ncyc = cpu_oracle_rate(seconds=min(15.0, max(3.0, args.cpu_seconds)))
         line["cpu_baseline"] = {"value": rate, "unit": "cell-iters/s", "cores": 1, "kind": "port",
                                 "sample": f"{ncyc} oracle cycles on the same 64x32x32 workload"}
@@ -246,6 +250,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--grid", default="", help="node counts ni,nj,nk (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -30,6 +30,7 @@ struct BlockCtx {
   DevBlock db{};
   cudaGraphExec_t graph = nullptr;
   int graph_fp32 = -1;
+  int cycle_launches = 0;       // kernel launches in one captured cycle
 };
 
 struct Ctx {
@@ -46,6 +47,7 @@ struct Ctx {
   int sm_count = 0;
   char errmsg[256] = {0};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  long nlaunch = 0;                     // kernel launches issued so far
 };
 
 int fail(Ctx* c, int code, const char* what, cudaError_t e = cudaSuccess) {
@@ -86,12 +88,14 @@ int launch_patch(Ctx* c, BlockCtx* b, void (*kern)(DevBlock, ff_params, int), in
   for (auto& p : b->h_patch) maxn = max(maxn, (p.r1b - p.r1a + 1) * (p.r2b - p.r2a + 1));
   dim3 g(nblk(maxn, 128), b->npatch);
   kern<<<g, 128, 0, c->stream>>>(b->db, b->prm, arg);
+  c->nlaunch++;
   return 0;
 }
 
 // ---- stages -----------------------------------------------------------------
 int st_statim(Ctx* c, BlockCtx* b) {
   k_state<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db, b->prm);
+  c->nlaunch++;
   launch_patch(c, b, k_reflec, 0);
   launch_patch(c, b, k_reflec, 1);
   return 0;
@@ -99,10 +103,12 @@ int st_statim(Ctx* c, BlockCtx* b) {
 
 int st_boundi(Ctx* c, BlockCtx* b) {
   k_refcor<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db);
+  c->nlaunch++;
   if (b->npatch) {
     int maxn = 1;
     for (auto& p : b->h_patch) maxn = max(maxn, (p.r1b - p.r1a + 1) * (p.r2b - p.r2a + 1));
     k_mir<<<dim3(nblk(maxn, 128), b->npatch), 128, 0, c->stream>>>(b->db);
+    c->nlaunch++;
   }
   return st_statim(c, b);
 }
@@ -113,15 +119,18 @@ int st_residu(Ctx* c, BlockCtx* b, int level, int icycle) {
       int maxn = 1;
       for (auto& p : b->h_patch) maxn = max(maxn, (p.r1b - p.r1a + 1) * (p.r2b - p.r2a + 1));
       k_refcen<<<dim3(nblk(maxn, 128), b->npatch), 128, 0, c->stream>>>(b->db, b->prm);
+      c->nlaunch++;
     }
   }
   if (b->prm.fullns && level == 1) {
     long ng = (long)(b->imax + 2) * (b->jmax + 2) * (b->kmax + 2);
     k_grad<<<nblk(ng, 128), 128, 0, c->stream>>>(b->db, level);
+    c->nlaunch++;
   }
   if (level == 1) launch_patch(c, b, k_inlet_outlet, icycle);
   dim3 g(nblk(b->imax, TI), nblk(b->jmax, TJ), nblk(b->kmax, TK));
   k_residual<<<g, 128, 0, c->stream>>>(b->db, b->prm, level);
+  c->nlaunch++;
   return 0;
 }
 
@@ -148,6 +157,7 @@ int coop_sweep(Ctx* c, BlockCtx* b, int upper, bool fp32) {
                            c->d_bar, c->d_err);
   }
   if (e != cudaSuccess) return fail(c, FF_ERR_CUDA, "cooperative sweep launch", e);
+  c->nlaunch++;
   return 0;
 }
 
@@ -155,44 +165,56 @@ int st_imps(Ctx* c, BlockCtx* b, int level, bool divide_cp) {
   int ncell = b->imax * b->jmax * b->kmax;
   double cfl = level == 1 ? b->prm.cfl : b->prm.cfll;
   k_time3_copr<<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, cfl);
+  c->nlaunch++;
   bool fp32 = b->prm.lusgs_fp32 != 0;
   int rc;
   if (!fp32) {
     k_lusgs_coef<double><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, b->coef, 1);
+    c->nlaunch++;
     if ((rc = coop_sweep(c, b, 1, false))) return rc;
     k_lusgs_coef<double><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, b->coef, 0);
+    c->nlaunch++;
     if ((rc = coop_sweep(c, b, 0, false))) return rc;
   } else {
     k_copy_dw<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->dw32, 1);
+    c->nlaunch++;
     k_lusgs_coef<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, b->coef32, 1);
+    c->nlaunch++;
     if ((rc = coop_sweep(c, b, 1, true))) return rc;
     k_lusgs_coef<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, b->coef32, 0);
+    c->nlaunch++;
     if ((rc = coop_sweep(c, b, 0, true))) return rc;
     k_copy_dw<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->dw32, 0);
+    c->nlaunch++;
   }
   if (divide_cp) {
     // standalone IMPS: finish with DRO/CP (imps3.f:483); the fused cycle
     // folds this division into the FIN kernel instead
     k_fin_divide<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db);
+    c->nlaunch++;
   }
   return 0;
 }
 
 int st_fin(Ctx* c, BlockCtx* b, int divide_cp) {
   k_fin<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db, b->prm, c->d_dromax, divide_cp);
+  c->nlaunch++;
   return 0;
 }
 
 int one_cycle(Ctx* c, BlockCtx* b, int icycle) {
   int rc;
   k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi, c->d_dromax);
+  c->nlaunch++;
   if ((rc = st_residu(c, b, 1, icycle))) return rc;
   int ncell = b->imax * b->jmax * b->kmax;
   k_resl2<<<min(nblk(ncell, 256), 4 * c->sm_count), 256, 0, c->stream>>>(b->db, c->d_resi);
+  c->nlaunch++;
   if ((rc = st_imps(c, b, 1, false))) return rc;
   if ((rc = st_fin(c, b, 1))) return rc;
   if ((rc = st_boundi(c, b))) return rc;
   k_record<<<1, 1, 0, c->stream>>>(c->d_resi, c->d_dromax, c->d_hist, c->d_hist_pos, c->hist_cap);
+  c->nlaunch++;
   return 0;
 }
 
@@ -376,8 +398,10 @@ int ff_resl2(void* ctx, int blk, double* out5) {
   BlockCtx* b = getb(c, blk);
   if (!b || !out5) return fail(c, FF_ERR_ARG, "ff_resl2");
   k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi, c->d_dromax);
+  c->nlaunch++;
   int ncell = b->imax * b->jmax * b->kmax;
   k_resl2<<<min(nblk(ncell, 256), 4 * c->sm_count), 256, 0, c->stream>>>(b->db, c->d_resi);
+  c->nlaunch++;
   CK(cudaMemcpyAsync(out5, c->d_resi, 5 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return 0;
@@ -398,6 +422,7 @@ int ff_fin(void* ctx, int blk, double* dromax) {
   BlockCtx* b = getb(c, blk);
   if (!b) return fail(c, FF_ERR_ARG, "ff_fin");
   k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi, c->d_dromax);
+  c->nlaunch++;
   st_fin(c, b, 0);
   if (dromax) {
     unsigned long long bits;
@@ -428,7 +453,9 @@ int ff_cycles(void* ctx, int blk, int ncycles, int icycle0, double* hist, int us
       if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
       cudaGraph_t g;
       CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      long n0 = c->nlaunch;
       rc = one_cycle(c, b, 2);
+      b->cycle_launches = (int)(c->nlaunch - n0);
       cudaError_t e = cudaStreamEndCapture(c->stream, &g);
       if (rc) return rc;
       if (e != cudaSuccess) return fail(c, FF_ERR_CUDA, "cycle capture", e);
@@ -445,6 +472,11 @@ int ff_cycles(void* ctx, int blk, int ncycles, int icycle0, double* hist, int us
     if (rc) return rc;
   }
   return 0;
+}
+
+int ff_cycle_launches(void* ctx, int blk) {
+  BlockCtx* b = getb((Ctx*)ctx, blk);
+  return b ? b->cycle_launches : -FF_ERR_ARG;
 }
 
 int ff_time_cycles(void* ctx, int blk, int ncycles, float* ms) {
@@ -469,11 +501,14 @@ int ff_time_stage(void* ctx, int blk, int stage, int reps, float* ms) {
     if (stage == FF_STAGE_RESIDUAL) {
       dim3 g(nblk(b->imax, TI), nblk(b->jmax, TJ), nblk(b->kmax, TK));
       k_residual<<<g, 128, 0, c->stream>>>(b->db, b->prm, 1);
+      c->nlaunch++;
     } else if (stage == FF_STAGE_GRAD) {
       long ng = (long)(b->imax + 2) * (b->jmax + 2) * (b->kmax + 2);
       k_grad<<<nblk(ng, 128), 128, 0, c->stream>>>(b->db, 1);
+      c->nlaunch++;
     } else if (stage == FF_STAGE_STATE) {
       k_state<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db, b->prm);
+      c->nlaunch++;
     } else {
       return fail(c, FF_ERR_ARG, "ff_time_stage: unknown stage");
     }

@@ -76,6 +76,7 @@ def lib():
         L.ff_cycles.argtypes = [vp, ci, ci, ci, ctypes.POINTER(cd), ci]
         L.ff_time_cycles.argtypes = [vp, ci, ci, ctypes.POINTER(ctypes.c_float)]
         L.ff_time_stage.argtypes = [vp, ci, ci, ci, ctypes.POINTER(ctypes.c_float)]
+        L.ff_cycle_launches.argtypes = [vp, ci]
         _LIB = L
     return _LIB
 
@@ -178,6 +179,9 @@ class GpuSolver:
         ms = ctypes.c_float()
         self._check(self.L.ff_time_cycles(self.ctx, bid, n, ctypes.byref(ms)))
         return ms.value
+
+    def cycle_launches(self, bid=0) -> int:
+        return self.L.ff_cycle_launches(self.ctx, bid)
 
     def time_stage(self, stage, reps=10, bid=0) -> float:
         ms = ctypes.c_float()

@@ -61,7 +61,9 @@ int ff_fin(void *ctx, int blk, double *dromax);
  * (nullable) receives ncycles x {RESI(31..35) sums of squares, DROMAX}. */
 int ff_cycles(void *ctx, int blk, int ncycles, int icycle0, double *hist, int use_graph);
 
-/* Timing helpers (CUDA events on the context stream). */
+/* Timing helpers (CUDA events on the context stream); ff_cycle_launches is
+ * the number of kernel launches in one graph-captured cycle. */
+int ff_cycle_launches(void *ctx, int blk);
 int ff_time_cycles(void *ctx, int blk, int ncycles, float *ms);
 int ff_time_stage(void *ctx, int blk, int stage, int reps, float *ms);
 
