@@ -521,3 +521,6 @@ int ff_time_stage(void* ctx, int blk, int stage, int reps, float* ms) {
 }
 
 }  // extern "C"
+
+// The allocation-free implicit stage shares this translation unit's kernels.
+#include "ff_noalloc.cu"

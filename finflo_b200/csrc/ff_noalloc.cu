@@ -1,0 +1,123 @@
+// Allocation-free variant of the LU-SGS implicit stage (ff_imps_noalloc).
+//
+// Who needs it: callers that must not allocate device memory while they run.
+// Examples are a host code that has already handed all device memory to its
+// own pool allocator and forbids further cudaMalloc calls, an application
+// that runs under a hard per-process memory cap fixed at start-up, or a code
+// path that is not allowed to synchronise the device (cudaMalloc and cudaFree
+// can synchronise).  Such a caller owns the block's arrays itself and passes
+// their device addresses in; this entry point then runs TIME3, LOCDT, COPR,
+// PREDGS, DIAGGS, CORRGS and DRO/CP (the same kernels as ff_imps) without
+// creating a context and without calling cudaMalloc, cudaFree or any
+// allocating library routine.
+//
+// The LU-SGS coefficients and the grid-barrier words that ff_imps keeps in
+// per-context buffers live here in one file-scope __device__ array of fixed
+// size.  Every GPU that loads the library holds that array (about 10 MB)
+// until the process exits.  Its maximum block size is FF_NOALLOC_MAX_NTOT
+// cells including the two ghost layers; larger blocks are rejected with
+// FF_ERR_SIZE before any work is queued.
+//
+// This file is compiled as part of ff_gpu.cu's translation unit (included at
+// its end), so it shares the kernels with the context-based entry points.
+
+#define FF_NOALLOC_BAR_WORDS 64   // doubles reserved for the barrier words
+
+// Scratch: NCOEF coefficient arrays of FF_NOALLOC_MAX_NTOT doubles, then the
+// barrier words {count, generation, error}.  In host code the name below is
+// only a host-side stand-in for the array; its device address comes from
+// cudaGetSymbolAddress in noalloc_setup().
+static __device__ __align__(256) double ff_noalloc_scratch[ff::NCOEF * (size_t)FF_NOALLOC_MAX_NTOT + FF_NOALLOC_BAR_WORDS];
+
+namespace {
+
+struct NoallocDevice {
+  int ready;
+  double* scratch;   // device address of ff_noalloc_scratch on this device
+  int sm_count;
+  int coop_per_sm;
+};
+constexpr int kMaxDevices = 64;
+NoallocDevice g_noalloc[kMaxDevices];
+
+// Once per device, with that device current: resolve the device address of
+// the scratch array and the cooperative occupancy of the sweep kernel.
+int noalloc_setup(int dev) {
+  NoallocDevice& d = g_noalloc[dev];
+  if (d.ready) return 0;
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, ff_noalloc_scratch) != cudaSuccess || !p) return FF_ERR_CUDA;
+  int sms = 0, per_sm = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return FF_ERR_CUDA;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ff::k_lusgs_sweep<double>, 256, 0) != cudaSuccess ||
+      per_sm < 1)
+    return FF_ERR_CUDA;
+  d.scratch = (double*)p;
+  d.sm_count = sms;
+  d.coop_per_sm = per_sm;
+  d.ready = 1;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" int ff_imps_noalloc(int imax, int jmax, int kmax, const ff_params* prm,
+                               double* const* slots, int level, void* stream) {
+  if (imax < 2 || jmax < 2 || kmax < 1 || !prm || !slots || (level != 1 && level != 2 && level != 3))
+    return FF_ERR_ARG;
+  long ntot = (long)(imax + 4) * (jmax + 4) * (kmax + 4);
+  if (ntot > FF_NOALLOC_MAX_NTOT) return FF_ERR_SIZE;
+  static const int needed[] = {FF_RO, FF_E, FF_P, FF_U, FF_V, FF_W, FF_C, FF_VIS, FF_CP, FF_DRDP, FF_DRDH,
+                               FF_VIST, FF_DRO, FF_DM, FF_DN, FF_DW, FF_DE, FF_DTL, FF_A1, FF_A1XA,
+                               FF_A1YA, FF_A1ZA, FF_A2, FF_A2XA, FF_A2YA, FF_A2ZA, FF_A3, FF_A3XA,
+                               FF_A3YA, FF_A3ZA, FF_VOL};
+  for (int s : needed)
+    if (!slots[s]) return FF_ERR_ARG;
+  // the five increment arrays must be back to back (ntot apart), as the
+  // sweep kernel addresses them from DRO
+  for (int v = 1; v < 5; v++)
+    if (slots[FF_DRO + v] != slots[FF_DRO] + (size_t)v * ntot) return FF_ERR_ARG;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return FF_ERR_CUDA;
+  int rc = noalloc_setup(dev);
+  if (rc) return rc;
+  const NoallocDevice& nd = g_noalloc[dev];
+  cudaStream_t st = (cudaStream_t)stream;
+
+  DevBlock db{};
+  db.imax = imax; db.jmax = jmax; db.kmax = kmax;
+  db.is = imax + 4; db.il = (imax + 4) * (jmax + 4); db.ntot = (int)ntot;
+  db.npatch = 0; db.patch = nullptr;
+  for (int s = 0; s < FF_NSLOTS; s++) db.a[s] = slots[s];
+
+  double* coef = nd.scratch;
+  unsigned* bar = (unsigned*)(nd.scratch + ff::NCOEF * (size_t)FF_NOALLOC_MAX_NTOT);
+  int* err = (int*)(bar + 2);
+  // every call shares the array: the barrier words must start at zero
+  if (cudaMemsetAsync(bar, 0, 4 * sizeof(unsigned), st) != cudaSuccess) return FF_ERR_CUDA;
+
+  int ncell = imax * jmax * kmax;
+  ff_params p = *prm;
+  double cfl = level == 1 ? p.cfl : p.cfll;
+  k_time3_copr<<<(ncell + 127) / 128, 128, 0, st>>>(db, p, cfl);
+  long widest = (long)jmax * kmax;
+  int nb = (int)min((long)nd.coop_per_sm * nd.sm_count, max(1L, (widest + 255) / 256));
+  double* dw = slots[FF_DRO];
+  for (int upper = 1; upper >= 0; upper--) {
+    k_lusgs_coef<double><<<(ncell + 127) / 128, 128, 0, st>>>(db, p, coef, upper);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(nb);
+    cfg.blockDim = dim3(256);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (cudaLaunchKernelEx(&cfg, k_lusgs_sweep<double>, db, (const double*)coef, dw, upper, bar, err) != cudaSuccess)
+      return FF_ERR_CUDA;
+  }
+  k_fin_divide<<<(int)((ntot + 255) / 256), 256, 0, st>>>(db);
+  if (cudaGetLastError() != cudaSuccess) return FF_ERR_CUDA;
+  return 0;
+}

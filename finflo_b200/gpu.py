@@ -20,7 +20,8 @@ from .case import FFPatch, FFParams, SLOT, SLOTS, Block
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libfinflo_gpu.so")
-_SRC = [os.path.join(_HERE, "csrc", f) for f in ("ff_gpu.cu", "ff_kernels.cuh", "ff_device.cuh")]
+_SRC = [os.path.join(_HERE, "csrc", f) for f in ("ff_gpu.cu", "ff_kernels.cuh", "ff_device.cuh",
+                                                 "ff_noalloc.cu")]
 NVCC_FLAGS = ["-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC", "-shared", "-std=c++17"]
 
@@ -77,6 +78,7 @@ def lib():
         L.ff_time_cycles.argtypes = [vp, ci, ci, ctypes.POINTER(ctypes.c_float)]
         L.ff_time_stage.argtypes = [vp, ci, ci, ci, ctypes.POINTER(ctypes.c_float)]
         L.ff_cycle_launches.argtypes = [vp, ci]
+        L.ff_imps_noalloc.argtypes = [ci, ci, ci, ctypes.POINTER(FFParams), ctypes.POINTER(vp), ci, vp]
         _LIB = L
     return _LIB
 

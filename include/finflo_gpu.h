@@ -28,7 +28,7 @@ extern "C" {
 
 #define FF_ABI_VERSION 1
 
-enum { FF_OK = 0, FF_ERR_CUDA = 1, FF_ERR_ARG = 2, FF_ERR_TIMEOUT = 3 };
+enum { FF_OK = 0, FF_ERR_CUDA = 1, FF_ERR_ARG = 2, FF_ERR_TIMEOUT = 3, FF_ERR_SIZE = 4 };
 enum { FF_STAGE_RESIDUAL = 1, FF_STAGE_GRAD = 2, FF_STAGE_STATE = 3 };
 
 int ff_abi_version(void);
@@ -60,6 +60,24 @@ int ff_fin(void *ctx, int blk, double *dromax);
 /* ncycles full cycles (RESIDU, RESL2, IMPS, FIN, BOUNDI, SUBIN); hist
  * (nullable) receives ncycles x {RESI(31..35) sums of squares, DROMAX}. */
 int ff_cycles(void *ctx, int blk, int ncycles, int icycle0, double *hist, int use_graph);
+
+/* Allocation-free implicit stage.  No counterpart in the reference: it is the
+ * ff_imps stage (TIME3, LOCDT, COPR, PREDGS, DIAGGS, CORRGS, DRO/CP) for
+ * callers that cannot call cudaMalloc while they run -- for example a host
+ * code whose device memory is all owned by its own pool, or one running
+ * under a fixed memory cap.  No context is created and nothing is allocated:
+ * slots[] holds the caller's device pointers (enum ff_slot; the five
+ * increment arrays DRO..DE must be contiguous, NTOT apart), and the LU-SGS
+ * coefficients and barrier words live in a file-scope device array that
+ * every GPU loading the library keeps (~10 MB) until the process exits.
+ * Limit: NTOT = (IMAX+4)(JMAX+4)(KMAX+4) <= FF_NOALLOC_MAX_NTOT, else
+ * FF_ERR_SIZE with nothing queued.  The first call on a device resolves the
+ * array's device address; make that first call before any stream capture.
+ * Calls share the array, so calls that overlap on the GPU race: serialise
+ * them (one stream, or events).  Asynchronous on `stream` (a cudaStream_t). */
+#define FF_NOALLOC_MAX_NTOT 98304
+int ff_imps_noalloc(int imax, int jmax, int kmax, const ff_params *prm,
+                    double *const *slots, int level, void *stream);
 
 /* Timing helpers (CUDA events on the context stream); ff_cycle_launches is
  * the number of kernel launches in one graph-captured cycle. */
