@@ -7,6 +7,7 @@
 // and as ff_cycles(), which captures one cycle in a CUDA graph and replays it.
 #include <cuda_runtime.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 #include <vector>
 #include "ff_kernels.cuh"
@@ -27,6 +28,9 @@ struct BlockCtx {
   float* coef32 = nullptr;      // NCOEF x ntot (FP32 LU-SGS)
   float* dw32 = nullptr;        // 5 x ntot
   int coop_blocks = 0, coop_blocks32 = 0;
+  int use_lines = 0;            // 1: cluster line-wavefront LU-SGS
+  LineGeom lg{};
+  size_t lines_smem = 0, lines_smem32 = 0;
   DevBlock db{};
   cudaGraphExec_t graph = nullptr;
   int graph_fp32 = -1;
@@ -161,6 +165,75 @@ int coop_sweep(Ctx* c, BlockCtx* b, int upper, bool fp32) {
   return 0;
 }
 
+int lines_sweep(Ctx* c, BlockCtx* b, int upper, bool fp32) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(b->lg.cs);
+  cfg.blockDim = dim3(LTHREADS);
+  cfg.dynamicSmemBytes = fp32 ? b->lines_smem32 : b->lines_smem;
+  cfg.stream = c->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = b->lg.cs;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  double* dw64 = b->base + (size_t)FF_DRO * b->slot_stride;
+  cudaError_t e = fp32 ? cudaLaunchKernelEx(&cfg, k_lusgs_lines<float>, b->db, (const float*)b->coef32, b->dw32, upper, b->lg)
+                       : cudaLaunchKernelEx(&cfg, k_lusgs_lines<double>, b->db, (const double*)b->coef, dw64, upper, b->lg);
+  if (e != cudaSuccess) return fail(c, FF_ERR_CUDA, "cluster sweep launch", e);
+  c->nlaunch++;
+  return 0;
+}
+
+// Choose the LU-SGS sweep kernel of a block: the cluster line wavefront
+// when the (j,k) line tiles fit one cluster, else the cooperative hyperplane
+// kernel.
+int setup_lines(Ctx* c, BlockCtx* b) {
+  LineGeom lg{};
+  lg.ntj = (b->jmax + LTJ - 1) / LTJ;
+  lg.ntk = (b->kmax + LTK - 1) / LTK;
+  lg.ntiles = lg.ntj * lg.ntk;
+  for (int cs = 16; cs >= 1; cs /= 2) {
+    int csz = min(cs, lg.ntiles);
+    int tpc = (lg.ntiles + csz - 1) / csz;
+    size_t sm64 = (size_t)25 * tpc * LTHREADS * sizeof(double);
+    size_t sm32 = (size_t)25 * tpc * LTHREADS * sizeof(float);
+    if (sm64 > 200 * 1024) continue;
+    CK(cudaFuncSetAttribute(k_lusgs_lines<double>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    CK(cudaFuncSetAttribute(k_lusgs_lines<float>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    CK(cudaFuncSetAttribute(k_lusgs_lines<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm64));
+    CK(cudaFuncSetAttribute(k_lusgs_lines<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm32));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(csz);
+    cfg.blockDim = dim3(LTHREADS);
+    cfg.dynamicSmemBytes = sm64;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = csz; attr[0].val.clusterDim.y = 1; attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, k_lusgs_lines<double>, &cfg) != cudaSuccess || nclusters < 1) {
+      cudaGetLastError();
+      continue;
+    }
+    lg.cs = csz;
+    lg.tpc = tpc;
+    b->lg = lg;
+    b->lines_smem = sm64;
+    b->lines_smem32 = sm32;
+    b->use_lines = 1;
+    return 0;
+  }
+  b->use_lines = 0;
+  return 0;
+}
+
+int sweep(Ctx* c, BlockCtx* b, int upper, bool fp32) {
+  return b->use_lines ? lines_sweep(c, b, upper, fp32) : coop_sweep(c, b, upper, fp32);
+}
+
 int st_imps(Ctx* c, BlockCtx* b, int level, bool divide_cp) {
   int ncell = b->imax * b->jmax * b->kmax;
   double cfl = level == 1 ? b->prm.cfl : b->prm.cfll;
@@ -171,19 +244,19 @@ int st_imps(Ctx* c, BlockCtx* b, int level, bool divide_cp) {
   if (!fp32) {
     k_lusgs_coef<double><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, b->coef, 1);
     c->nlaunch++;
-    if ((rc = coop_sweep(c, b, 1, false))) return rc;
+    if ((rc = sweep(c, b, 1, false))) return rc;
     k_lusgs_coef<double><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, b->coef, 0);
     c->nlaunch++;
-    if ((rc = coop_sweep(c, b, 0, false))) return rc;
+    if ((rc = sweep(c, b, 0, false))) return rc;
   } else {
     k_copy_dw<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->dw32, 1);
     c->nlaunch++;
     k_lusgs_coef<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, b->coef32, 1);
     c->nlaunch++;
-    if ((rc = coop_sweep(c, b, 1, true))) return rc;
+    if ((rc = sweep(c, b, 1, true))) return rc;
     k_lusgs_coef<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, b->coef32, 0);
     c->nlaunch++;
-    if ((rc = coop_sweep(c, b, 0, true))) return rc;
+    if ((rc = sweep(c, b, 0, true))) return rc;
     k_copy_dw<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->dw32, 0);
     c->nlaunch++;
   }
@@ -315,6 +388,12 @@ int ff_block_add(void* ctx, int imax, int jmax, int kmax, int npatch, const ff_p
   b->coop_blocks = (int)min((long)per_sm * c->sm_count, max(1L, (widest + 255) / 256));
   b->coop_blocks32 = (int)min((long)per_sm32 * c->sm_count, max(1L, (widest + 255) / 256));
   if (b->coop_blocks < 1 || b->coop_blocks32 < 1) return fail(c, FF_ERR_CUDA, "no cooperative occupancy");
+  {
+    int rc = setup_lines(c, b);
+    if (rc) return rc;
+    const char* env = getenv("FINFLO_LUSGS");
+    if (env && strcmp(env, "hyperplane") == 0) b->use_lines = 0;
+  }
   c->blocks.push_back(b);
   return (int)c->blocks.size() - 1;
 }
@@ -472,6 +551,11 @@ int ff_cycles(void* ctx, int blk, int ncycles, int icycle0, double* hist, int us
     if (rc) return rc;
   }
   return 0;
+}
+
+int ff_lusgs_kind(void* ctx, int blk) {
+  BlockCtx* b = getb((Ctx*)ctx, blk);
+  return b ? (b->use_lines ? 1 + b->lg.cs * 100 : 0) : -FF_ERR_ARG;
 }
 
 int ff_cycle_launches(void* ctx, int blk) {

@@ -12,6 +12,7 @@
 //                                     hyperplanes with a bounded grid barrier
 #pragma once
 #include "ff_device.cuh"
+#include <cooperative_groups.h>
 
 namespace ff {
 
@@ -783,3 +784,125 @@ __global__ void k_fin_divide(DevBlock b) {
 }
 
 }  // namespace ff
+
+// ---------------------------------------------------------------------------
+// LU-SGS sweep as a line wavefront inside one thread-block cluster.
+//
+// Thread (lj, lk) of tile t owns the i-line (J, K); at hyperplane m it
+// handles the cell I = m - J - K of its line.  Like the reference (PREDGS
+// imps4.f:345 / CORRGS imps4.f:76) each cell, once solved, produces the
+// split-Jacobian products for its three downstream neighbours: the i
+// neighbour is on the same line (kept in shared memory), the j and k
+// neighbours are the lines (J -/+ 1, K) and (J, K -/+ 1), read at the next
+// plane from shared memory -- from another CTA's shared memory (DSMEM) when
+// the line belongs to another tile.  One cluster barrier per plane; the
+// published values are double-buffered so a plane reads only the previous
+// plane's outputs.  The triangular system is the reference's (incl. the
+// dropped i+1 coupling in row J = JMAX of PREDGS), so the result equals the
+// hyperplane and slab orders up to rounding.
+// ---------------------------------------------------------------------------
+constexpr int LTJ = 16, LTK = 8, LTHREADS = LTJ * LTK;
+
+struct LineGeom {
+  int ntj, ntk, ntiles, cs, tpc;   // tiles in j/k, cluster size, tiles per CTA
+};
+
+template <typename CT>
+__global__ void __launch_bounds__(LTHREADS) k_lusgs_lines(DevBlock b, const CT* __restrict__ coef, CT* dw,
+                                                          int upper, LineGeom lg) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  CT* pub = reinterpret_cast<CT*>(smem_raw);   // [2][tpc][10][LTHREADS]: bd(5), ck(5)
+  CT* ydb = pub + 2 * lg.tpc * 10 * LTHREADS;   // [tpc][5][LTHREADS]
+  const int IMAX = b.imax, JMAX = b.jmax, KMAX = b.kmax, IS = b.is, IL = b.il;
+  const size_t nt = b.ntot;
+  const int rank = (int)cluster.block_rank();
+  const int lane = threadIdx.x, lj = lane % LTJ, lk = lane / LTJ;
+  const int nplanes = IMAX + JMAX + KMAX - 2;
+  for (int q = 0; q < lg.tpc; q++)
+    for (int v = 0; v < 5; v++) ydb[(q * 5 + v) * LTHREADS + lane] = CT(0);
+  cluster.sync();
+  for (int s = 0; s < nplanes; s++) {
+    const int m = upper ? IMAX + JMAX + KMAX - s : 3 + s;
+    const int bin = s & 1, bout = bin ^ 1;
+    for (int q = 0; q < lg.tpc; q++) {
+      int t = q * lg.cs + rank;
+      if (t >= lg.ntiles) break;
+      int tj = t % lg.ntj, tk = t / lg.ntj;
+      int J = tj * LTJ + lj + 1, K = tk * LTK + lk + 1;
+      if (J > JMAX || K > KMAX) continue;
+      int I = m - J - K;
+      if (I < 1 || I > IMAX) continue;
+      size_t N = ix(b, I, J, K);
+      // ---- consume: neighbour contributions of the previous plane ----
+      CT yd[5], bd[5], ck[5];
+      bool hy = upper ? (I < IMAX && J < JMAX) : (I > 1);
+      bool hj = upper ? (J < JMAX) : (J > 1);
+      bool hk = upper ? (K < KMAX) : (K > 1);
+#pragma unroll
+      for (int v = 0; v < 5; v++) yd[v] = hy ? ydb[(q * 5 + v) * LTHREADS + lane] : CT(0);
+      {
+        int Jn = upper ? J + 1 : J - 1;       // line across the j face
+        int Kn = upper ? K + 1 : K - 1;       // line across the k face
+        // source of bd: line (Jn, K); of ck: line (J, Kn)
+        const CT* src;
+        int tjn = (Jn - 1) / LTJ, ljn = (Jn - 1) % LTJ, tn = tk * lg.ntj + tjn;
+        if (hj) {
+          src = cluster.map_shared_rank(pub, tn % lg.cs);
+          int ln = lk * LTJ + ljn, qn = tn / lg.cs;
+#pragma unroll
+          for (int v = 0; v < 5; v++) bd[v] = src[((bin * lg.tpc + qn) * 10 + v) * LTHREADS + ln];
+        } else {
+#pragma unroll
+          for (int v = 0; v < 5; v++) bd[v] = CT(0);
+        }
+        int tkn = (Kn - 1) / LTK, lkn = (Kn - 1) % LTK, tn2 = tkn * lg.ntj + tj;
+        if (hk) {
+          src = cluster.map_shared_rank(pub, tn2 % lg.cs);
+          int ln = lkn * LTJ + lj, qn = tn2 / lg.cs;
+#pragma unroll
+          for (int v = 0; v < 5; v++) ck[v] = src[((bin * lg.tpc + qn) * 10 + 5 + v) * LTHREADS + ln];
+        } else {
+#pragma unroll
+          for (int v = 0; v < 5; v++) ck[v] = CT(0);
+        }
+      }
+      // ---- solve the cell ----
+      CT dt1 = coef[9 * nt + N], scinv = coef[10 * nt + N], scinp = coef[11 * nt + N];
+      CT fd = upper ? CT(1) : coef[12 * nt + N];
+      CT vol = (CT)__ldg(b.a[FF_VOL] + N);
+      CT a3 = (CT)__ldg(b.a[FF_A3] + (upper ? N + IL : N));
+      CT a1 = (CT)__ldg(b.a[FF_A1] + (upper ? N + 1 : N));
+      CT a2 = (CT)__ldg(b.a[FF_A2] + (upper ? N + IS : N));
+      CT res[5];
+#pragma unroll
+      for (int v = 0; v < 5; v++) {
+        CT x = upper ? (-dt1 * a3 * ck[v] + vol * (dw[v * nt + N] * fd)) : (dt1 * a3 * ck[v] + vol * (dw[v * nt + N] * fd));
+        x = upper ? x - dt1 * (a1 * yd[v] + a2 * bd[v]) : x + dt1 * (a1 * yd[v] + a2 * bd[v]);
+        res[v] = x * (v < 4 ? scinv : scinp);
+        dw[v * nt + N] = res[v];
+      }
+      // ---- produce: contributions to the three downstream neighbours ----
+      CT c = (CT)__ldg(b.a[FF_C] + N), ro = (CT)__ldg(b.a[FF_RO] + N);
+      const int st[3] = {1, IS, IL};
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        size_t fN = upper ? N : N + st[d];
+        const int ao = 4 * d;
+        CT out[5];
+        jac_product<CT>(out, res, c, ro, (CT)__ldg(b.a[FF_A1XA + ao] + fN), (CT)__ldg(b.a[FF_A1YA + ao] + fN),
+                        (CT)__ldg(b.a[FF_A1ZA + ao] + fN), coef[(3 * d) * nt + N], coef[(3 * d + 1) * nt + N],
+                        coef[(3 * d + 2) * nt + N]);
+        if (d == 0) {
+#pragma unroll
+          for (int v = 0; v < 5; v++) ydb[(q * 5 + v) * LTHREADS + lane] = out[v];
+        } else {
+#pragma unroll
+          for (int v = 0; v < 5; v++) pub[((bout * lg.tpc + q) * 10 + (d == 1 ? 0 : 5) + v) * LTHREADS + lane] = out[v];
+        }
+      }
+    }
+    cluster.sync();
+  }
+}

@@ -78,6 +78,7 @@ def lib():
         L.ff_time_cycles.argtypes = [vp, ci, ci, ctypes.POINTER(ctypes.c_float)]
         L.ff_time_stage.argtypes = [vp, ci, ci, ci, ctypes.POINTER(ctypes.c_float)]
         L.ff_cycle_launches.argtypes = [vp, ci]
+        L.ff_lusgs_kind.argtypes = [vp, ci]
         L.ff_imps_noalloc.argtypes = [ci, ci, ci, ctypes.POINTER(FFParams), ctypes.POINTER(vp), ci, vp]
         _LIB = L
     return _LIB
@@ -181,6 +182,9 @@ class GpuSolver:
         ms = ctypes.c_float()
         self._check(self.L.ff_time_cycles(self.ctx, bid, n, ctypes.byref(ms)))
         return ms.value
+
+    def lusgs_kind(self, bid=0) -> int:
+        return self.L.ff_lusgs_kind(self.ctx, bid)
 
     def cycle_launches(self, bid=0) -> int:
         return self.L.ff_cycle_launches(self.ctx, bid)

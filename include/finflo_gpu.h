@@ -82,6 +82,9 @@ int ff_imps_noalloc(int imax, int jmax, int kmax, const ff_params *prm,
 /* Timing helpers (CUDA events on the context stream); ff_cycle_launches is
  * the number of kernel launches in one graph-captured cycle. */
 int ff_cycle_launches(void *ctx, int blk);
+/* LU-SGS sweep kernel of a block: 0 = cooperative hyperplane kernel,
+ * 1 + 100*cluster_size = cluster line wavefront. */
+int ff_lusgs_kind(void *ctx, int blk);
 int ff_time_cycles(void *ctx, int blk, int ncycles, float *ms);
 int ff_time_stage(void *ctx, int blk, int stage, int reps, float *ms);
 

@@ -77,7 +77,7 @@ def test_resl2(gpu_lib):
     g.close()
 
 
-@pytest.mark.parametrize("dims", [(17, 9, 9), (25, 13, 7)])
+@pytest.mark.parametrize("dims", [(17, 9, 9), (25, 13, 7), (17, 65, 65), (9, 41, 19)])
 def test_imps_lusgs(gpu_lib, dims):
     """The GPU hyperplane LU-SGS solves the reference's triangular systems
     (incl. the dropped i+1 coupling in the last j row of PREDGS)."""
@@ -155,3 +155,28 @@ def test_fp32_lusgs_converges_to_fp64_answer(gpu_lib):
     # both runs must be converging
     assert h32[-1, 0] < h32[0, 0] and h64[-1, 0] < h64[0, 0]
     g.close(); g2.close()
+
+
+@pytest.mark.parametrize("dims", [(33, 33, 33), (17, 65, 65)])
+def test_line_and_hyperplane_sweeps_agree(gpu_lib, dims, monkeypatch):
+    """The cluster line-wavefront LU-SGS and the cooperative hyperplane kernel
+    solve the same triangular systems."""
+    g1, b1, bg1, o, bc, prm = _setup(*dims)
+    assert g1.lusgs_kind(b1) % 100 == 1
+    monkeypatch.setenv("FINFLO_LUSGS", "hyperplane")
+    g2 = GpuSolver(0)
+    bg2 = make_pair(*dims)[0]
+    b2 = g2.add_block(bg2, prm)
+    assert g2.lusgs_kind(b2) == 0
+    g2.upload(b2)
+    g2.start(b2)
+    for g, b in ((g1, b1), (g2, b2)):
+        g.residu(b, 1, 1)
+        g.imps(b, 1)
+    d1 = g1.download(b1, list(RES))
+    d2 = g2.download(b2, list(RES))
+    for n in RES:
+        a, c = interior(bg1, d1[n]), interior(bg2, d2[n])
+        err = np.abs(a - c).max() / (np.abs(c).max() + 1e-300)
+        assert err <= 1e-12, (n, err)
+    g1.close(); g2.close()
