@@ -186,6 +186,13 @@ def new_block(X, Y, Z, patches) -> Block:
     return Block(m.imax, m.jmax, m.kmax, arrays, patches, nodes=(X, Y, Z))
 
 
+def block_from_metrics(m, patches, nodes=None) -> Block:
+    arrays = {n: np.zeros(m.ntot) for n in SLOTS}
+    for n in METRIC_SLOTS:
+        arrays[n][:] = m.arrays[n]
+    return Block(m.imax, m.jmax, m.kmax, arrays, patches, nodes=nodes)
+
+
 def init_freestream(b: Block, fs, *, noise=1e-3, seed=0):
     """Uniform free stream plus seeded Gaussian noise on the density of the
     interior cells, held at constant pressure (T = p/(R rho))."""
@@ -216,3 +223,100 @@ def bump_case(ni=65, nj=33, nk=33, *, h1=1e-3, amp=0.1, mach=0.5, reynolds=1e4,
     init_freestream(blk, fs, noise=noise, seed=seed)
     prm = make_params(fc, blk.dims, cfl=cfl, inter=inter)
     return blk, prm, fs
+
+
+def bump_case_mg(ni=65, nj=33, nk=33, nlev=3, *, h1=1e-3, amp=0.1, mach=0.5, reynolds=1e4,
+                 zlen=0.5, noise=1e-3, seed=0, cfl=2.0, cfll=2.0, inter=3, span_amp=0.0):
+    """The bump channel with nlev multigrid levels (finest first); coarse
+    metrics are lumped from the fine cells, patch ranges follow each level."""
+    fc = FlowConditions(mach=mach, reynolds=reynolds)
+    fs = fc.freestream()
+    X, Y, Z = grid.bump_nodes(ni, nj, nk, h1=h1, amp=amp, zlen=zlen, span_amp=span_amp)
+    levels = []
+    for lev, m in enumerate(grid.mg_metrics(X, Y, Z, nlev)):
+        blk = block_from_metrics(m, channel_patches(m.imax, m.jmax, m.kmax, fs), nodes=(X, Y, Z) if lev == 0 else None)
+        init_freestream(blk, fs, noise=noise if lev == 0 else 0.0, seed=seed)
+        levels.append(blk)
+    prm = make_params(fc, levels[0].dims, cfl=cfl, cfll=cfll, inter=inter)
+    prms = [level_params(prm, lev + 1) for lev in range(nlev)]
+    return levels, prms, fs
+
+
+# ---- multi-block periodic box (1:1 patched blocks) -----------------------
+
+_OPP = {1: 4, 2: 5, 3: 6, 4: 1, 5: 2, 6: 3}
+
+
+def _face_ranges(iface, imax, jmax, kmax):
+    d = (iface - 1) % 3
+    if d == 0:
+        return (1, jmax), (1, kmax)
+    if d == 1:
+        return (1, imax), (1, kmax)
+    return (1, imax), (1, jmax)
+
+
+def box_block_sizes(nb=(4, 3, 2), lo=17, hi=97, seed=36):
+    """Cells per block along each direction, drawn uniformly from {lo..hi}
+    with the seed; block (a, b, c) of the Cartesian arrangement has
+    (ni[a], nj[b], nk[c]) cells, so every interface is 1:1."""
+    rng = np.random.default_rng(seed)
+    return tuple([int(v) for v in rng.integers(lo, hi + 1, size=n)] for n in nb)
+
+
+def periodic_box_case(nb=(4, 3, 2), sizes=None, *, seed=36, lo=17, hi=97, mach=0.3,
+                      amp=1e-2, cfl=2.0, inter=3, lusgs_fp32=False, wave=(1, 1, 1)):
+    """The unit box split into nb[0] x nb[1] x nb[2] blocks with 1:1 patches on
+    every interface, periodic in all three directions (the outer faces are
+    1:1 patched to the opposite blocks).  Inviscid (viscous face fluxes off,
+    IDI1..3 = 0) uniform flow at the given Mach number along the diagonal,
+    with an entropy wave rho = rho0 (1 + amp sin(2 pi k.x + phi)) at constant
+    pressure; phi comes from the seed.  Returns blocks, params, free stream."""
+    if sizes is None:
+        sizes = box_block_sizes(nb, lo, hi, seed)
+    ni, nj, nk = sizes
+    fc = FlowConditions(mach=mach, reynolds=0.0)
+    fs = fc.freestream()
+    phi = 2 * math.pi * np.random.default_rng(seed + 1000).random()
+    cut = [np.concatenate([[0], np.cumsum(n)]) for n in (ni, nj, nk)]
+    tot = [c[-1] for c in cut]
+    ids = {}
+    for c in range(len(nk)):
+        for b in range(len(nj)):
+            for a in range(len(ni)):
+                ids[a, b, c] = len(ids)
+    blocks, prms = [], []
+    u = fs["u"] / math.sqrt(3.0)
+    for (a, b, c), bid in ids.items():
+        x = cut[0][a:a + 2]; y = cut[1][b:b + 2]; z = cut[2][c:c + 2]
+        X, Y, Z = grid.box_nodes(np.arange(x[0], x[1] + 1) / tot[0],
+                                 np.arange(y[0], y[1] + 1) / tot[1],
+                                 np.arange(z[0], z[1] + 1) / tot[2])
+        imax, jmax, kmax = ni[a], nj[b], nk[c]
+        pats = []
+        for iface in range(1, 7):
+            d = (iface - 1) % 3
+            step = -1 if iface <= 3 else 1
+            nbr = [a, b, c]
+            nbr[d] = (nbr[d] + step) % len(sizes[d])
+            r1, r2 = _face_ranges(iface, imax, jmax, kmax)
+            pa = _patch(grid.BC_CON, iface, r1, r2, ibtype=ids[tuple(nbr)])
+            pa.nface = _OPP[iface]
+            pa.n1a = pa.n2a = 1
+            pats.append(pa)
+        blk = new_block(X, Y, Z, pats)
+        ar = blk.arrays
+        ar["TEMP"][:] = fs["t"]
+        ar["U"][:] = u; ar["V"][:] = u; ar["W"][:] = u
+        ar["PDIFF"][:] = 0.0
+        ar["EPS2"][:] = 1.0
+        ar["VIST"][:] = 0.0
+        xc, yc, zc = (blk.interior(n) for n in ("XC", "YC", "ZC"))
+        arg = 2 * math.pi * (wave[0] * xc + wave[1] * yc + wave[2] * zc) + phi
+        rho = fs["rho"] * (1.0 + amp * np.sin(arg))
+        blk.interior("TEMP")[:] = fs["p"] / (fc.rgas * rho)
+        prm = make_params(fc, blk.dims, cfl=cfl, inter=inter, fullns=False, lusgs_fp32=lusgs_fp32)
+        prm.idi1 = prm.idi2 = prm.idi3 = 0
+        blocks.append(blk)
+        prms.append(prm)
+    return blocks, prms, fs

@@ -35,6 +35,8 @@ struct BlockCtx {
   cudaGraphExec_t graph = nullptr;
   int graph_fp32 = -1;
   int cycle_launches = 0;       // kernel launches in one captured cycle
+  BlockCtx* coarse = nullptr;   // next multigrid level (MGRID > 1)
+  int level = 1;
 };
 
 struct Ctx {
@@ -52,6 +54,17 @@ struct Ctx {
   char errmsg[256] = {0};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   long nlaunch = 0;                     // kernel launches issued so far
+  // multi-block: per-block streams for the concurrent chains inside a
+  // captured cycle, the device block table and the connection work-list
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> side_ev;
+  cudaEvent_t fork_ev = nullptr;
+  DevBlock* d_blocks = nullptr;
+  ConnItem* d_conn = nullptr;
+  int nconn = 0, maxconn = 1, conn_blocks = -1;
+  cudaGraphExec_t mb_graph = nullptr;
+  int mb_graph_n = -1;
+  int mb_launches = 0;
 };
 
 int fail(Ctx* c, int code, const char* what, cudaError_t e = cudaSuccess) {
@@ -97,11 +110,13 @@ int launch_patch(Ctx* c, BlockCtx* b, void (*kern)(DevBlock, ff_params, int), in
 }
 
 // ---- stages -----------------------------------------------------------------
-int st_statim(Ctx* c, BlockCtx* b) {
+// STATIM: equation of state and REFLEC; npass = 2 repeats them on the patch
+// ghosts (BOUNDI calls STATIM twice, ns3c.f:10896, 10905).
+int st_statim(Ctx* c, BlockCtx* b, int npass = 2) {
   k_state<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db, b->prm);
   c->nlaunch++;
   launch_patch(c, b, k_reflec, 0);
-  launch_patch(c, b, k_reflec, 1);
+  if (npass > 1) launch_patch(c, b, k_reflec, 1);
   return 0;
 }
 
@@ -291,6 +306,196 @@ int one_cycle(Ctx* c, BlockCtx* b, int icycle) {
   return 0;
 }
 
+// One multigrid cycle of CYCLES (ns3c.f:1400-2170): fine-level update, then
+// for each coarser level STATIM/RESIDI of the finer level, TRANSF, STATIM,
+// RESIDI, FORCFU, ADDRES, IMPSDI, FIN; then INTERP back up, REFLEC, BOUNDI.
+int mg_cycle(Ctx* c, BlockCtx* b, int icycle) {
+  int rc;
+  k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi, c->d_dromax);
+  c->nlaunch++;
+  if ((rc = st_residu(c, b, 1, icycle))) return rc;
+  if ((rc = st_imps(c, b, 1, false))) return rc;
+  if ((rc = st_fin(c, b, 1))) return rc;
+  std::vector<BlockCtx*> lv;
+  for (BlockCtx* x = b; x; x = x->coarse) lv.push_back(x);
+  for (size_t m = 1; m < lv.size(); m++) {
+    BlockCtx *f = lv[m - 1], *cc = lv[m];
+    st_statim(c, f, 1);
+    if ((rc = st_residu(c, f, (int)m, icycle))) return rc;
+    if (m == 1) {   // RESL2 of the level-1 residual after the fine update
+      k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi, c->d_dromax);
+      c->nlaunch++;
+      int ncell = f->imax * f->jmax * f->kmax;
+      k_resl2<<<min(nblk(ncell, 256), 4 * c->sm_count), 256, 0, c->stream>>>(f->db, c->d_resi);
+      c->nlaunch++;
+    } else {
+      k_forcing<<<nblk(f->ntot, 256), 256, 0, c->stream>>>(f->db, 1);
+      c->nlaunch++;
+    }
+    long nc = (long)(cc->imax + 2) * (cc->jmax + 2) * (cc->kmax + 2);
+    k_transf<<<nblk(nc, 128), 128, 0, c->stream>>>(f->db, cc->db);
+    c->nlaunch++;
+    k_transf_ring<<<nblk(cc->ntot, 256), 256, 0, c->stream>>>(cc->db);
+    c->nlaunch++;
+    st_statim(c, cc, 1);
+    if ((rc = st_residu(c, cc, (int)m + 1, icycle))) return rc;
+    k_forcing<<<nblk(cc->ntot, 256), 256, 0, c->stream>>>(cc->db, 0);
+    c->nlaunch++;
+    k_forcing<<<nblk(cc->ntot, 256), 256, 0, c->stream>>>(cc->db, 1);
+    c->nlaunch++;
+    if ((rc = st_imps(c, cc, (int)m + 1, true))) return rc;
+    k_fin_coarse<<<nblk(cc->ntot, 256), 256, 0, c->stream>>>(cc->db, cc->prm, 1);
+    c->nlaunch++;
+  }
+  for (size_t m = lv.size() - 1; m >= 1; m--) {
+    BlockCtx *f = lv[m - 1], *cc = lv[m];
+    int nf = f->imax * f->jmax * f->kmax;
+    k_interp<<<nblk(nf, 256), 256, 0, c->stream>>>(cc->db, f->db);
+    c->nlaunch++;
+    k_fin_coarse<<<nblk(f->ntot, 256), 256, 0, c->stream>>>(f->db, f->prm, 0);
+    c->nlaunch++;
+  }
+  launch_patch(c, b, k_reflec, 0);
+  if ((rc = st_boundi(c, b))) return rc;
+  // SUBIN's *OLD copies (INTERP changed the level-1 state after FIN)
+  k_subin_copy<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db);
+  c->nlaunch++;
+  // SUBIN's max|DE| sees the level-1 residual of the second RESIDI
+  k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi + 6, c->d_dromax);
+  c->nlaunch++;
+  int ncell = b->imax * b->jmax * b->kmax;
+  k_maxabs_de<<<min(nblk(ncell, 256), 4 * c->sm_count), 256, 0, c->stream>>>(b->db, c->d_dromax);
+  c->nlaunch++;
+  k_record<<<1, 1, 0, c->stream>>>(c->d_resi, c->d_dromax, c->d_hist, c->d_hist_pos, c->hist_cap);
+  c->nlaunch++;
+  return 0;
+}
+
+// Device block table and connection work-list of all blocks of the context.
+int ensure_conn(Ctx* c) {
+  int nb = (int)c->blocks.size();
+  if (c->conn_blocks == nb) return 0;
+  std::vector<DevBlock> tab(nb);
+  std::vector<ConnItem> items;
+  int maxn = 1;
+  for (int n = 0; n < nb; n++) {
+    tab[n] = c->blocks[n]->db;
+    for (auto& pa : c->blocks[n]->h_patch) {
+      if (pa.ityp != FF_BC_CON) continue;
+      if (pa.ibtype < 0 || pa.ibtype >= nb) return fail(c, FF_ERR_ARG, "connection to an unknown block");
+      ConnItem it;
+      it.dst = n; it.src = pa.ibtype; it.pa = pa;
+      items.push_back(it);
+      maxn = max(maxn, (pa.r1b - pa.r1a + 1) * (pa.r2b - pa.r2a + 1));
+    }
+  }
+  if (c->d_blocks) cudaFree(c->d_blocks);
+  if (c->d_conn) cudaFree(c->d_conn);
+  c->d_blocks = nullptr; c->d_conn = nullptr;
+  CK(cudaMalloc(&c->d_blocks, sizeof(DevBlock) * max(1, nb)));
+  CK(cudaMemcpy(c->d_blocks, tab.data(), sizeof(DevBlock) * nb, cudaMemcpyHostToDevice));
+  c->nconn = (int)items.size();
+  c->maxconn = maxn;
+  if (c->nconn) {
+    CK(cudaMalloc(&c->d_conn, sizeof(ConnItem) * c->nconn));
+    CK(cudaMemcpy(c->d_conn, items.data(), sizeof(ConnItem) * c->nconn, cudaMemcpyHostToDevice));
+  }
+  while ((int)c->side.size() < nb) {
+    cudaStream_t s; cudaEvent_t e;
+    CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    c->side.push_back(s); c->side_ev.push_back(e);
+  }
+  if (!c->fork_ev) CK(cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming));
+  c->conn_blocks = nb;
+  return 0;
+}
+
+int st_connec(Ctx* c) {
+  if (!c->nconn) return 0;
+  k_connec<<<dim3(nblk(c->maxconn, 128), c->nconn), 128, 0, c->stream>>>(c->d_blocks, c->d_conn);
+  c->nlaunch++;
+  return 0;
+}
+
+// Run fn(block) for every block on its own stream, forked from and joined
+// back into the context stream (captured as parallel graph branches).
+// Blocks whose sweep is the cooperative hyperplane kernel share the context's
+// grid barrier and need the whole GPU, so their chains run one after another.
+template <typename F>
+int fork_join(Ctx* c, int nb, F fn) {
+  bool concurrent = nb > 1;
+  for (int n = 0; n < nb; n++) concurrent = concurrent && c->blocks[n]->use_lines;
+  if (!concurrent) {
+    for (int n = 0; n < nb; n++) {
+      int rc = fn(n);
+      if (rc) return rc;
+    }
+    return 0;
+  }
+  cudaStream_t main = c->stream;
+  CK(cudaEventRecord(c->fork_ev, main));
+  int rc = 0;
+  for (int n = 0; n < nb && !rc; n++) {
+    CK(cudaStreamWaitEvent(c->side[n], c->fork_ev, 0));
+    c->stream = c->side[n];
+    rc = fn(n);
+    c->stream = main;
+    CK(cudaEventRecord(c->side_ev[n], c->side[n]));
+  }
+  c->stream = main;
+  for (int n = 0; n < nb; n++) CK(cudaStreamWaitEvent(main, c->side_ev[n], 0));
+  return rc;
+}
+
+// BOUNDI ns3c.f:10608 over all blocks: REFCOR, MIR and STATIM per block,
+// CONNEC of every 1:1 patch in one launch, STATIM again.
+int mb_boundi(Ctx* c) {
+  int nb = (int)c->blocks.size(), rc;
+  rc = fork_join(c, nb, [&](int n) {
+    BlockCtx* b = c->blocks[n];
+    k_refcor<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db);
+    c->nlaunch++;
+    if (b->npatch) {
+      int maxn = 1;
+      for (auto& p : b->h_patch) maxn = max(maxn, (p.r1b - p.r1a + 1) * (p.r2b - p.r2a + 1));
+      k_mir<<<dim3(nblk(maxn, 128), b->npatch), 128, 0, c->stream>>>(b->db);
+      c->nlaunch++;
+    }
+    return st_statim(c, b, 1);
+  });
+  if (rc) return rc;
+  if ((rc = st_connec(c))) return rc;
+  return fork_join(c, nb, [&](int n) { return st_statim(c, c->blocks[n], 1); });
+}
+
+// One NS3D cycle over all single-grid blocks: CYCLES per block (concurrent
+// branches), then the all-block BOUNDI and SUBIN.
+int mb_cycle(Ctx* c, int icycle) {
+  int nb = (int)c->blocks.size(), rc;
+  k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi, c->d_dromax);
+  c->nlaunch++;
+  rc = fork_join(c, nb, [&](int n) {
+    BlockCtx* b = c->blocks[n];
+    int r;
+    if ((r = st_residu(c, b, 1, icycle))) return r;
+    int ncell = b->imax * b->jmax * b->kmax;
+    k_resl2<<<min(nblk(ncell, 256), 4 * c->sm_count), 256, 0, c->stream>>>(b->db, c->d_resi);
+    c->nlaunch++;
+    if ((r = st_imps(c, b, 1, false))) return r;
+    return st_fin(c, b, 1);
+  });
+  if (rc) return rc;
+  if ((rc = mb_boundi(c))) return rc;
+  k_record<<<1, 1, 0, c->stream>>>(c->d_resi, c->d_dromax, c->d_hist, c->d_hist_pos, c->hist_cap);
+  c->nlaunch++;
+  return 0;
+}
+
+int run_cycle(Ctx* c, BlockCtx* b, int icycle) {
+  return b->coarse ? mg_cycle(c, b, icycle) : one_cycle(c, b, icycle);
+}
+
 int ensure_hist(Ctx* c, int n) {
   if (n <= c->hist_cap) return 0;
   if (c->d_hist) cudaFree(c->d_hist);
@@ -321,7 +526,7 @@ int ff_create(void** out, int device) {
   CK(cudaMemset(c->d_bar, 0, 2 * sizeof(unsigned)));
   CK(cudaMalloc(&c->d_err, sizeof(int)));
   CK(cudaMemset(c->d_err, 0, sizeof(int)));
-  CK(cudaMalloc(&c->d_resi, 8 * sizeof(double)));
+  CK(cudaMalloc(&c->d_resi, 16 * sizeof(double)));
   CK(cudaMalloc(&c->d_dromax, sizeof(unsigned long long)));
   CK(cudaMalloc(&c->d_hist_pos, sizeof(int)));
   CK(cudaMemset(c->d_hist_pos, 0, sizeof(int)));
@@ -342,6 +547,10 @@ int ff_destroy(void* ctx) {
     cudaFree(b->base); cudaFree(b->d_patch); cudaFree(b->coef); cudaFree(b->coef32); cudaFree(b->dw32);
     delete b;
   }
+  if (c->mb_graph) cudaGraphExecDestroy(c->mb_graph);
+  for (size_t n = 0; n < c->side.size(); n++) { cudaStreamDestroy(c->side[n]); cudaEventDestroy(c->side_ev[n]); }
+  if (c->fork_ev) cudaEventDestroy(c->fork_ev);
+  cudaFree(c->d_blocks); cudaFree(c->d_conn);
   cudaFree(c->d_bar); cudaFree(c->d_err); cudaFree(c->d_resi); cudaFree(c->d_dromax);
   cudaFree(c->d_hist); cudaFree(c->d_hist_pos);
   cudaEventDestroy(c->ev0); cudaEventDestroy(c->ev1);
@@ -398,12 +607,24 @@ int ff_block_add(void* ctx, int imax, int jmax, int kmax, int npatch, const ff_p
   return (int)c->blocks.size() - 1;
 }
 
+int ff_mg_link(void* ctx, int fine, int coarse) {
+  Ctx* c = (Ctx*)ctx;
+  BlockCtx *f = getb(c, fine), *cc = getb(c, coarse);
+  if (!f || !cc || f == cc || f->imax != 2 * cc->imax || f->jmax != 2 * cc->jmax || f->kmax != 2 * cc->kmax)
+    return fail(c, FF_ERR_ARG, "ff_mg_link: the coarse block must halve every dimension");
+  f->coarse = cc;
+  cc->level = f->level + 1;
+  if (f->graph) { cudaGraphExecDestroy(f->graph); f->graph = nullptr; }
+  return 0;
+}
+
 int ff_block_params(void* ctx, int blk, const ff_params* prm) {
   Ctx* c = (Ctx*)ctx;
   BlockCtx* b = getb(c, blk);
   if (!b || !prm) return fail(c, FF_ERR_ARG, "ff_block_params");
   b->prm = *prm;
   if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+  if (c->mb_graph) { cudaGraphExecDestroy(c->mb_graph); c->mb_graph = nullptr; }
   return 0;
 }
 
@@ -523,7 +744,7 @@ int ff_cycles(void* ctx, int blk, int ncycles, int icycle0, double* hist, int us
   int it = 0;
   // the first cycle of a run (ICYCLE = 1) differs (INLET density), run it eagerly
   while (it < ncycles && (icycle0 + it == 1 || !use_graph)) {
-    if ((rc = one_cycle(c, b, icycle0 + it))) return rc;
+    if ((rc = run_cycle(c, b, icycle0 + it))) return rc;
     it++;
   }
   if (it < ncycles) {
@@ -533,7 +754,7 @@ int ff_cycles(void* ctx, int blk, int ncycles, int icycle0, double* hist, int us
       cudaGraph_t g;
       CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
       long n0 = c->nlaunch;
-      rc = one_cycle(c, b, 2);
+      rc = run_cycle(c, b, 2);
       b->cycle_launches = (int)(c->nlaunch - n0);
       cudaError_t e = cudaStreamEndCapture(c->stream, &g);
       if (rc) return rc;
@@ -561,6 +782,72 @@ int ff_lusgs_kind(void* ctx, int blk) {
 int ff_cycle_launches(void* ctx, int blk) {
   BlockCtx* b = getb((Ctx*)ctx, blk);
   return b ? b->cycle_launches : -FF_ERR_ARG;
+}
+
+int ff_boundi_all(void* ctx) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || c->blocks.empty()) return fail(c, FF_ERR_ARG, "ff_boundi_all");
+  for (auto* b : c->blocks)
+    if (b->level != 1) return fail(c, FF_ERR_ARG, "ff_boundi_all: finest-level blocks only");
+  int rc;
+  if ((rc = ensure_conn(c))) return rc;
+  if ((rc = mb_boundi(c))) return rc;
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int ff_cycles_all(void* ctx, int ncycles, int icycle0, double* hist, int use_graph) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || ncycles < 0 || c->blocks.empty()) return fail(c, FF_ERR_ARG, "ff_cycles_all");
+  for (auto* b : c->blocks)
+    if (b->coarse || b->level != 1) return fail(c, FF_ERR_ARG, "ff_cycles_all: single-grid blocks only");
+  int rc;
+  if ((rc = ensure_conn(c))) return rc;
+  if ((rc = ensure_hist(c, max(ncycles, 1)))) return rc;
+  CK(cudaMemsetAsync(c->d_hist_pos, 0, sizeof(int), c->stream));
+  int it = 0;
+  while (it < ncycles && (icycle0 + it == 1 || !use_graph)) {
+    if ((rc = mb_cycle(c, icycle0 + it))) return rc;
+    it++;
+  }
+  if (it < ncycles) {
+    int nb = (int)c->blocks.size();
+    if (!c->mb_graph || c->mb_graph_n != nb) {
+      if (c->mb_graph) { cudaGraphExecDestroy(c->mb_graph); c->mb_graph = nullptr; }
+      cudaGraph_t g;
+      CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      long n0 = c->nlaunch;
+      rc = mb_cycle(c, 2);
+      c->mb_launches = (int)(c->nlaunch - n0);
+      cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+      if (rc) return rc;
+      if (e != cudaSuccess) return fail(c, FF_ERR_CUDA, "multi-block cycle capture", e);
+      CK(cudaGraphInstantiate(&c->mb_graph, g, 0));
+      cudaGraphDestroy(g);
+      c->mb_graph_n = nb;
+    }
+    for (; it < ncycles; it++) CK(cudaGraphLaunch(c->mb_graph, c->stream));
+  }
+  CK(cudaGetLastError());
+  if (hist) {
+    CK(cudaMemcpyAsync(hist, c->d_hist, sizeof(double) * 6 * ncycles, cudaMemcpyDeviceToHost, c->stream));
+    rc = ff_synchronize(ctx);
+    if (rc) return rc;
+  }
+  return 0;
+}
+
+int ff_time_cycles_all(void* ctx, int ncycles, float* ms, int* launches_per_cycle) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !ms) return fail(c, FF_ERR_ARG, "ff_time_cycles_all");
+  CK(cudaEventRecord(c->ev0, c->stream));
+  int rc = ff_cycles_all(ctx, ncycles, 2, nullptr, 1);
+  if (rc) return rc;
+  CK(cudaEventRecord(c->ev1, c->stream));
+  CK(cudaEventSynchronize(c->ev1));
+  CK(cudaEventElapsedTime(ms, c->ev0, c->ev1));
+  if (launches_per_cycle) *launches_per_cycle = c->mb_launches;
+  return ff_synchronize(ctx);
 }
 
 int ff_time_cycles(void* ctx, int blk, int ncycles, float* ms) {

@@ -360,6 +360,29 @@ FF_DI void visc_flux(const DevBlock& b, const ff_params& p, size_t L, int S, int
   f[0] = 0.; f[1] = -f2; f[2] = -f3; f[3] = -f4; f[4] = -f5;
 }
 
+// FLUXDO base3c.f:3677 (thin layer, IDIFF = 1): the viscous flux on coarse
+// levels and whenever FULLNS is off.
+FF_DI void visc_flux_thin(const DevBlock& b, const ff_params& p, size_t L, int S, int dir, double f[5]) {
+#define LD(s, n) __ldg(b.a[s] + (n))
+  size_t M = L - S;
+  const int ao = 4 * (dir - 1);
+  double area = LD(FF_A1 + ao, L);
+  double nx = LD(FF_A1XA + ao, L), ny = LD(FF_A1YA + ao, L), nz = LD(FF_A1ZA + ao, L);
+  double surg = -area * (area / (LD(FF_VOL, L) + LD(FF_VOL, M)));
+  double surf = surg * (LD(FF_EPS2, L) * LD(FF_VIS, L) + LD(FF_EPS2, M) * LD(FF_VIS, M));
+  double surfe = surg * (LD(FF_CP, L) * LD(FF_VIST, L) / p.prt + LD(FF_CH, L)
+                         + LD(FF_CP, M) * LD(FF_VIST, M) / p.prt + LD(FF_CH, M));
+  double ul = LD(FF_U, L), um = LD(FF_U, M), vl = LD(FF_V, L), vm = LD(FF_V, M), wl = LD(FF_W, L), wm = LD(FF_W, M);
+  double duc = .333333 * (nx * (ul - um) + ny * (vl - vm) + nz * (wl - wm));
+  double f2 = surf * (ul - um + nx * duc);
+  double f3 = surf * (vl - vm + ny * duc);
+  double f4 = surf * (wl - wm + nz * duc);
+  double f5 = .5 * ((ul + um) * f2 + (vl + vm) * f3 + (wl + wm) * f4);
+  f[0] = 0.; f[1] = f2; f[2] = f3; f[3] = f4;
+  f[4] = f5 + surfe * (LD(FF_TEMP, L) - LD(FF_TEMP, M));
+#undef LD
+}
+
 // BOTSKE base3c.f:6147 wall-face flux (laminar, TURCOR false as FLUCYC passes
 // it, wall at rest).  II = interior cell at the wall.
 FF_DI void wall_flux(const DevBlock& b, const ff_params& p, size_t II, int S, int idir, int dir,
@@ -420,8 +443,13 @@ FF_DI void face_flux(const DevBlock& b, const ff_params& p, int dir, size_t L, i
       return;
     }
   }
-  f[0] = f[1] = f[2] = f[3] = f[4] = 0.;
-  if (level == 1 && p.fullns) visc_flux(b, p, L, S, dir, f);
+  const int idi = dir == 1 ? p.idi1 : (dir == 2 ? p.idi2 : p.idi3);
+  if (m <= min(idi, nmax + 1)) {   // SINVIS base3c.f:3876: viscous faces
+    if (level == 1 && p.fullns) visc_flux(b, p, L, S, dir, f);
+    else visc_flux_thin(b, p, L, S, dir, f);
+  } else {
+    f[0] = f[1] = f[2] = f[3] = f[4] = 0.;
+  }
   double q[5][4];
   const int sl[5] = {FF_RO, FF_U, FF_V, FF_W, FF_P};
 #pragma unroll
@@ -781,6 +809,179 @@ __global__ void k_fin_divide(DevBlock b) {
   int i = (int)(n % b.is), j = (int)((n / b.is) % (b.jmax + 4)), k = (int)(n / b.il);
   if (i >= 2 && i < b.imax + 2 && j >= 2 && j < b.jmax + 2 && k >= 2 && k < b.kmax + 2)
     b.a[FF_DRO][n] = b.a[FF_DRO][n] / b.a[FF_CP][n];
+}
+
+// ---------------------------------------------------------------------------
+// Multigrid transfers (FAS V-cycle of CYCLES ns3c.f:1607-2170)
+// ---------------------------------------------------------------------------
+
+// TRANSF multi.f:156: volume-weighted restriction of TEMP,U,V,W,PDIFF,EPS2,
+// VIST and of the residuals (into P2H) for coarse cells 0..MAX+1, and the
+// interior *OLD copies.
+__global__ void k_transf(DevBlock f, DevBlock c) {
+  int ni = c.imax + 2, nj = c.jmax + 2, nk = c.kmax + 2;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ni * nj * nk) return;
+  int I = t % ni, J = (t / ni) % nj, K = t / (ni * nj);
+  size_t N = ix(c, I, J, K);
+  size_t ijk = ix(f, 2 * I - 1, 2 * J - 1, 2 * K - 1);
+  size_t o[8] = {ijk + f.is + 1, ijk, ijk + 1, ijk + f.is,
+                 ijk + f.is + 1 + f.il, ijk + f.il, ijk + 1 + f.il, ijk + f.is + f.il};
+  const double* VOL = f.a[FF_VOL];
+  double vv[8];
+#pragma unroll
+  for (int q = 0; q < 8; q++) vv[q] = VOL[o[q]];
+  double pvol = 1. / c.a[FF_VOL][N];
+  const int vs[12] = {FF_TEMP, FF_U, FF_V, FF_W, FF_PDIFF, FF_EPS2, FF_VIST, FF_DRO, FF_DM, FF_DN, FF_DW, FF_DE};
+  const int ds[12] = {FF_TEMP, FF_U, FF_V, FF_W, FF_PDIFF, FF_EPS2, FF_VIST, FF_ROP2H, FF_RMP2H, FF_RNP2H, FF_RWP2H, FF_EP2H};
+#pragma unroll
+  for (int v = 0; v < 12; v++) {
+    const double* X = f.a[vs[v]];
+    double s = 0.;
+#pragma unroll
+    for (int q = 0; q < 8; q++) s += vv[q] * X[o[q]];
+    c.a[ds[v]][N] = s * pvol;
+  }
+  if (I >= 1 && I <= c.imax && J >= 1 && J <= c.jmax && K >= 1 && K <= c.kmax) {
+    c.a[FF_TOLD][N] = c.a[FF_TEMP][N];
+    c.a[FF_UOLD][N] = c.a[FF_U][N];
+    c.a[FF_VOLD][N] = c.a[FF_V][N];
+    c.a[FF_WOLD][N] = c.a[FF_W][N];
+    c.a[FF_POLD][N] = c.a[FF_PDIFF][N];
+  }
+}
+
+// Coarse ghost rings of TRANSF (multi.f:250-432): P2H = 0 in both ghost
+// layers; the second ghost layer of each face copies the first one.
+__global__ void k_transf_ring(DevBlock c) {
+  size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= (size_t)c.ntot) return;
+  int i = (int)(n % c.is) - 1, j = (int)((n / c.is) % (c.jmax + 4)) - 1, k = (int)(n / c.il) - 1;
+  bool gi = i < 1 || i > c.imax, gj = j < 1 || j > c.jmax, gk = k < 1 || k > c.kmax;
+  if (!(gi || gj || gk)) return;
+#pragma unroll
+  for (int v = 0; v < 5; v++) c.a[FF_ROP2H + v][n] = 0.;
+  // second-layer face ghosts copy the first layer along the face normal
+  // (cells in the second layer of two directions are not used on coarse
+  // levels and are left alone)
+  int second = (i == -1 || i == c.imax + 2) + (j == -1 || j == c.jmax + 2) + (k == -1 || k == c.kmax + 2);
+  if (second != 1) return;
+  int src_off = 0;
+  if (i == -1) src_off = 1; else if (i == c.imax + 2) src_off = -1;
+  else if (j == -1) src_off = c.is; else if (j == c.jmax + 2) src_off = -c.is;
+  else if (k == -1) src_off = c.il; else if (k == c.kmax + 2) src_off = -c.il;
+  if (src_off == 0) return;
+  const int vs[7] = {FF_TEMP, FF_U, FF_V, FF_W, FF_PDIFF, FF_EPS2, FF_VIST};
+#pragma unroll
+  for (int v = 0; v < 7; v++) c.a[vs[v]][n] = c.a[vs[v]][n + src_off];
+}
+
+// FORCFU multi.f:1609 (mode 0: P2H -= R) and ADDRES multi.f:1686 (mode 1:
+// R = P2H + R), every cell of the level.
+__global__ void k_forcing(DevBlock b, int mode) {
+  size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= (size_t)b.ntot) return;
+#pragma unroll
+  for (int v = 0; v < 5; v++) {
+    double* P2 = b.a[FF_ROP2H + v];
+    double* R = b.a[FF_DRO + v];
+    if (mode == 0) P2[n] = P2[n] - R[n];
+    else R[n] = P2[n] + R[n];
+  }
+}
+
+// INTERP multi.f:1763: inject the coarse correction into the 8 children.
+__global__ void k_interp(DevBlock c, DevBlock f) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= f.imax * f.jmax * f.kmax) return;
+  int I = t % f.imax + 1, J = (t / f.imax) % f.jmax + 1, K = t / (f.imax * f.jmax) + 1;
+  size_t N = ix(c, (I + 1) / 2, (J + 1) / 2, (K + 1) / 2), F = ix(f, I, J, K);
+  double dp = c.a[FF_PDIFF][N] - c.a[FF_POLD][N];
+  f.a[FF_TEMP][F] = f.a[FF_TEMP][F] + (c.a[FF_TEMP][N] - c.a[FF_TOLD][N]);
+  f.a[FF_U][F] = f.a[FF_U][F] + (c.a[FF_U][N] - c.a[FF_UOLD][N]);
+  f.a[FF_V][F] = f.a[FF_V][F] + (c.a[FF_V][N] - c.a[FF_VOLD][N]);
+  f.a[FF_W][F] = f.a[FF_W][F] + (c.a[FF_W][N] - c.a[FF_WOLD][N]);
+  f.a[FF_P][F] = f.a[FF_P][F] + dp;
+  f.a[FF_PDIFF][F] = f.a[FF_PDIFF][F] + dp;
+}
+
+// FIN on a coarse level (update = 1) and the TEMP / pressure limits that
+// follow it or INTERP (ns3c.f:1948-1990, 2059-2125): UPLIM/LOLIM TEMP,
+// LOLIMP (no PDTOP there).
+__global__ void k_fin_coarse(DevBlock b, ff_params p, int update) {
+  size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= (size_t)b.ntot) return;
+  int i = (int)(n % b.is), j = (int)((n / b.is) % (b.jmax + 4)), k = (int)(n / b.il);
+  bool kin = k >= 2 && k < b.kmax + 2, jin = j >= 2 && j < b.jmax + 2;
+  bool interior = kin && jin && i >= 2 && i < b.imax + 2;
+  double T = b.a[FF_TEMP][n];
+  if (update && interior) {
+    T = b.a[FF_TOLD][n] + b.a[FF_DRO][n];
+    b.a[FF_U][n] = b.a[FF_UOLD][n] + b.a[FF_DM][n];
+    b.a[FF_V][n] = b.a[FF_VOLD][n] + b.a[FF_DN][n];
+    b.a[FF_W][n] = b.a[FF_WOLD][n] + b.a[FF_DW][n];
+    b.a[FF_PDIFF][n] = b.a[FF_POLD][n] + b.a[FF_DE][n];
+  }
+  if (kin && jin) T = dmin(T, p.tuplim);
+  T = dmax(T, p.tlolim);
+  b.a[FF_TEMP][n] = T;
+  double P = b.a[FF_P][n];
+  double prelim = dmin(0., P - 0.01 * p.frspre);
+  b.a[FF_P][n] = P - prelim;
+  b.a[FF_PDIFF][n] = b.a[FF_PDIFF][n] - prelim;
+}
+
+// CONNEC ns3c.f:8605 (EXPTOT/IMPVO2 gluebm.f:6819/6964) for aligned 1:1
+// patches of all blocks in one launch: blockIdx.y = connection item; the two
+// interior layers of the source block fill the two ghost layers of the
+// destination patch (TEMP,U,V,W,E,EPS2,VIST,CH,P,PDIFF, as BOUNDI passes).
+struct ConnItem { int dst, src; ff_patch pa; };
+
+__global__ void k_connec(const DevBlock* __restrict__ blocks, const ConnItem* __restrict__ items) {
+  const ConnItem& it = items[blockIdx.y];
+  const ff_patch& pa = it.pa;
+  int n1 = pa.r1b - pa.r1a + 1, n2 = pa.r2b - pa.r2a + 1;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n1 * n2) return;
+  int a = pa.r1a + t % n1, c = pa.r2a + t / n1;
+  const DevBlock& d = blocks[it.dst];
+  const DevBlock& s = blocks[it.src];
+  FaceG fd = face_g(d, pa.iface), fs = face_g(s, pa.nface);
+  size_t L = face_cell(d, fd, a, c);
+  size_t S = face_cell(s, fs, a - pa.r1a + pa.n1a, c - pa.r2a + pa.n2a);
+  const int vs[10] = {FF_TEMP, FF_U, FF_V, FF_W, FF_E, FF_EPS2, FF_VIST, FF_CH, FF_P, FF_PDIFF};
+  int lsd = fd.idir * fd.s, lss = fs.idir * fs.s;
+#pragma unroll
+  for (int g = 1; g <= 2; g++) {
+    size_t G = L - g * lsd, Q = S + (g - 1) * lss;
+#pragma unroll
+    for (int v = 0; v < 10; v++) d.a[vs[v]][G] = s.a[vs[v]][Q];
+  }
+}
+
+// SUBIN ns3c.f:9742: the *OLD copies of the interior cells.
+__global__ void k_subin_copy(DevBlock b) {
+  size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= (size_t)b.ntot) return;
+  int i = (int)(n % b.is), j = (int)((n / b.is) % (b.jmax + 4)), k = (int)(n / b.il);
+  if (!(i >= 2 && i < b.imax + 2 && j >= 2 && j < b.jmax + 2 && k >= 2 && k < b.kmax + 2)) return;
+  b.a[FF_TOLD][n] = b.a[FF_TEMP][n];
+  b.a[FF_UOLD][n] = b.a[FF_U][n];
+  b.a[FF_VOLD][n] = b.a[FF_V][n];
+  b.a[FF_WOLD][n] = b.a[FF_W][n];
+  b.a[FF_POLD][n] = b.a[FF_PDIFF][n];
+}
+
+// max |DE| over the interior (DROMXX, IDRXX = 6) into dm_bits.
+__global__ void k_maxabs_de(DevBlock b, unsigned long long* dm_bits) {
+  double amax = 0.;
+  int ncell = b.imax * b.jmax * b.kmax;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ncell; t += gridDim.x * blockDim.x) {
+    int I = t % b.imax + 1, J = (t / b.imax) % b.jmax + 1, K = t / (b.imax * b.jmax) + 1;
+    amax = dmax(amax, fabs(b.a[FF_DE][ix(b, I, J, K)]));
+  }
+  for (int o = 16; o > 0; o >>= 1) amax = dmax(amax, __shfl_down_sync(0xffffffffu, amax, o));
+  if ((threadIdx.x & 31) == 0 && amax > 0.) atomicMax(dm_bits, (unsigned long long)__double_as_longlong(amax));
 }
 
 }  // namespace ff

@@ -61,6 +61,10 @@ def lib():
         L.ff_destroy.argtypes = [vp]
         L.ff_block_add.argtypes = [vp, ci, ci, ci, ci, ctypes.POINTER(FFPatch), ctypes.POINTER(FFParams)]
         L.ff_block_params.argtypes = [vp, ci, ctypes.POINTER(FFParams)]
+        L.ff_mg_link.argtypes = [vp, ci, ci]
+        L.ff_boundi_all.argtypes = [vp]
+        L.ff_cycles_all.argtypes = [vp, ci, ci, ctypes.POINTER(cd), ci]
+        L.ff_time_cycles_all.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ci)]
         L.ff_upload.argtypes = [vp, ci, ci, ctypes.POINTER(cd)]
         L.ff_download.argtypes = [vp, ci, ci, ctypes.POINTER(cd)]
         L.ff_device_ptr.restype = vp
@@ -125,6 +129,14 @@ class GpuSolver:
         self.blocks.append((blk, prm))
         return bid
 
+    def add_levels(self, levels, prms) -> int:
+        """Add the multigrid levels of one block (finest first) and link
+        them; returns the id of the finest level."""
+        ids = [self.add_block(b, p) for b, p in zip(levels, prms)]
+        for f, c in zip(ids[:-1], ids[1:]):
+            self._check(self.L.ff_mg_link(self.ctx, f, c))
+        return ids[0]
+
     def set_params(self, bid: int, prm: FFParams):
         self._check(self.L.ff_block_params(self.ctx, bid, ctypes.byref(prm)))
 
@@ -178,6 +190,29 @@ class GpuSolver:
         self._check(self.L.ff_cycles(self.ctx, bid, n, icycle0, _dptr(hist), int(use_graph)))
         return hist[:n]
 
+    def boundi_all(self):
+        self._check(self.L.ff_boundi_all(self.ctx))
+
+    def start_all(self):
+        """NS3D start-up over every block: BOUNDI(1) with the 1:1
+        connections, then the *OLD copies of each block."""
+        self.boundi_all()
+        self.sync()
+        for bid in range(len(self.blocks)):
+            self._old_copies(bid)
+
+    def cycles_all(self, n, icycle0=1, use_graph=True) -> np.ndarray:
+        """n cycles over every block (multi-block NS3D with 1:1 CONNEC)."""
+        hist = np.zeros((max(n, 1), 6))
+        self._check(self.L.ff_cycles_all(self.ctx, n, icycle0, _dptr(hist), int(use_graph)))
+        return hist[:n]
+
+    def time_cycles_all(self, n):
+        ms = ctypes.c_float()
+        nl = ctypes.c_int()
+        self._check(self.L.ff_time_cycles_all(self.ctx, n, ctypes.byref(ms), ctypes.byref(nl)))
+        return ms.value, nl.value
+
     def time_cycles(self, n, bid=0) -> float:
         ms = ctypes.c_float()
         self._check(self.L.ff_time_cycles(self.ctx, bid, n, ctypes.byref(ms)))
@@ -196,9 +231,12 @@ class GpuSolver:
 
     def start(self, bid=0):
         """NS3D start-up (ns3c.f:378-379): BOUNDI, then the *OLD copies."""
-        blk = self.blocks[bid][0]
         self.boundi(bid)
         self.sync()
+        self._old_copies(bid)
+
+    def _old_copies(self, bid):
+        blk = self.blocks[bid][0]
         st = self.download(bid, ["TEMP", "U", "V", "W", "PDIFF"])
         for a, b2 in (("TOLD", "TEMP"), ("UOLD", "U"), ("VOLD", "V"), ("WOLD", "W"), ("POLD", "PDIFF")):
             blk.arrays[a][:] = st[b2]

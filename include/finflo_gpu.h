@@ -41,6 +41,10 @@ int ff_destroy(void *ctx);
 int ff_block_add(void *ctx, int imax, int jmax, int kmax, int npatch,
                  const ff_patch *patches, const ff_params *prm);
 int ff_block_params(void *ctx, int blk, const ff_params *prm);
+/* Make `coarse` the next multigrid level of `fine` (every dimension halved;
+ * MGRID levels, main.f:4613-4630).  ff_cycles on the finest block then runs
+ * the FAS V-cycle of CYCLES (ns3c.f:1607-2170) over the chain. */
+int ff_mg_link(void *ctx, int fine, int coarse);
 
 /* Host <-> device copy of one per-cell array slot (enum ff_slot), NTOT doubles. */
 int ff_upload(void *ctx, int blk, int slot, const double *host);
@@ -78,6 +82,16 @@ int ff_cycles(void *ctx, int blk, int ncycles, int icycle0, double *hist, int us
 #define FF_NOALLOC_MAX_NTOT 98304
 int ff_imps_noalloc(int imax, int jmax, int kmax, const ff_params *prm,
                     double *const *slots, int level, void *stream);
+
+/* ncycles cycles of NS3D over every (single-grid) block of the context:
+ * CYCLES per block as concurrent graph branches, then BOUNDI with the 1:1
+ * connections (CONNEC ns3c.f:8605) of all blocks in one launch, and SUBIN.
+ * Connection patches have ityp = FF_BC_CON, ibtype = source block id,
+ * nface = source face, n1a/n2a = source range start (aligned patches). */
+int ff_cycles_all(void *ctx, int ncycles, int icycle0, double *hist, int use_graph);
+/* BOUNDI(1) ns3c.f:10608 over every block, 1:1 connections included. */
+int ff_boundi_all(void *ctx);
+int ff_time_cycles_all(void *ctx, int ncycles, float *ms, int *launches_per_cycle);
 
 /* Timing helpers (CUDA events on the context stream); ff_cycle_launches is
  * the number of kernel launches in one graph-captured cycle. */

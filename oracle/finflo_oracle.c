@@ -714,8 +714,11 @@ void orc_flux_dir(orc_block *b, const ff_params *p, int dir, int level) {
       for (int m = 1; m <= nmax + 1; m++) {
         size_t L = dir == 1 ? IX(d, m, t1, t2) : (dir == 2 ? IX(d, t1, m, t2) : IX(d, t1, t2, m));
         double f[5] = {0, 0, 0, 0, 0};
-        if (level == 1 && p->fullns) fluxbl_face(b, p, L, S, dir, f);
-        else fluxdo_face(b, p, L, S, dir, f);
+        int idi = dir == 1 ? p->idi1 : (dir == 2 ? p->idi2 : p->idi3);
+        if (m <= MIND(idi, nmax + 1)) {          /* SINVIS: viscous faces */
+          if (level == 1 && p->fullns) fluxbl_face(b, p, L, S, dir, f);
+          else fluxdo_face(b, p, L, S, dir, f);
+        }
         double q[5][4];
         const double *arr[5] = {RO, U, V, W, P};
         for (int v = 0; v < 5; v++) {
@@ -1480,4 +1483,70 @@ void orc_mg_cycle(orc_block **lv, int nlev, const ff_params *prm, int icycle, do
   reflec(b, &prm[0]);
   orc_boundi(b, &prm[0]);
   orc_subin(b, dromax);
+}
+
+/* ---------------------------------------------------------------------- */
+/* Multi-block: 1:1 connections (CONNEC ns3c.f:8605 -> EXPTOT gluebm.f:6819 */
+/* / IMPVO2 gluebm.f:6964) for aligned patches (ICON(14) = 0).             */
+/* ---------------------------------------------------------------------- */
+
+/* Copy the two interior layers next to the source face of block `src` into
+ * the two ghost layers of patch `pa` of block `dst`.  BOUNDI passes TEMP in
+ * the RO position and U,V,W in RM,RN,RW (ns3c.f:10900), so the exchanged
+ * variables are TEMP,U,V,W,E,EPS2,VIST,CH,P,PDIFF. */
+void orc_connec_patch(orc_block *dst, const ff_patch *pa, const orc_block *src) {
+  static const int vs[10] = {FF_TEMP, FF_U, FF_V, FF_W, FF_E, FF_EPS2, FF_VIST, FF_CH, FF_P, FF_PDIFF};
+  dims_t dd = dims_of(dst), ds = dims_of((orc_block *)src);
+  face_t fd = face_geom(&dd, pa->iface), fs = face_geom(&ds, pa->nface);
+  int lsd = fd.idir * fd.s, lss = fs.idir * fs.s;
+  for (int bb = pa->r2a; bb <= pa->r2b; bb++)
+    for (int a = pa->r1a; a <= pa->r1b; a++) {
+      size_t L = face_cell(&dd, &fd, a, bb);
+      size_t S = face_cell(&ds, &fs, a - pa->r1a + pa->n1a, bb - pa->r2a + pa->n2a);
+      for (int g = 1; g <= 2; g++) {
+        size_t G = L - g * lsd, Q = S + (g - 1) * lss;
+        for (int v = 0; v < 10; v++) dst->a[vs[v]][G] = src->a[vs[v]][Q];
+      }
+    }
+}
+
+void orc_connec(orc_block **blk, int nblk) {
+  for (int n = 0; n < nblk; n++)
+    for (int ip = 0; ip < blk[n]->npatch; ip++) {
+      const ff_patch *pa = &blk[n]->patch[ip];
+      if (pa->ityp != FF_BC_CON) continue;
+      orc_connec_patch(blk[n], pa, blk[pa->ibtype]);
+    }
+}
+
+/* BOUNDI ns3c.f:10608 for several blocks: REFCOR, MIR, STATIM per block
+ * (ns3c.f:10660-10700), CONNEC of the 1:1 patches, STATIM again. */
+void orc_mb_boundi(orc_block **blk, int nblk, const ff_params *prm) {
+  for (int n = 0; n < nblk; n++) { orc_refcor(blk[n]); orc_mir(blk[n]); orc_statim(blk[n], &prm[n]); }
+  orc_connec(blk, nblk);
+  for (int n = 0; n < nblk; n++) orc_statim(blk[n], &prm[n]);
+}
+
+/* One cycle of NS3D for several single-grid blocks: CYCLES per block, then
+ * BOUNDI over all blocks (REFCOR, MIR, STATIM, CONNEC, STATIM) and SUBIN. */
+void orc_mb_cycle(orc_block **blk, int nblk, const ff_params *prm, int icycle, double *resi5, double *dromax) {
+  for (int v = 0; v < 5; v++) resi5[v] = 0.;
+  double dm = 0.;
+  for (int n = 0; n < nblk; n++) {
+    double r[5];
+    orc_statim(blk[n], &prm[n]);
+    orc_adjuin_laminar(blk[n]);
+    orc_residu(blk[n], &prm[n], 1, icycle);
+    orc_resl2(blk[n], r);
+    for (int v = 0; v < 5; v++) resi5[v] += r[v];
+    orc_imps(blk[n], &prm[n], 1);
+    orc_fin_limits(blk[n], &prm[n]);
+  }
+  orc_mb_boundi(blk, nblk, prm);
+  for (int n = 0; n < nblk; n++) {
+    double d;
+    orc_subin(blk[n], &d);
+    if (d > dm) dm = d;
+  }
+  *dromax = dm;
 }

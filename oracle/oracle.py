@@ -133,3 +133,51 @@ def roe_face(qr, ql, qrr, qll, nrm, area, intem, prm, cell_r, cell_l, kquirk=Fal
                    ctypes.c_double(area), intem, ctypes.byref(prm), D5(*cell_r), D5(*cell_l),
                    int(kquirk), f)
     return np.array(f[:])
+
+
+class OracleMG:
+    """Multigrid levels of one block (finest first) for orc_mg_cycle."""
+
+    def __init__(self, levels, prms):
+        self.levels = [Oracle(b, p) for b, p in zip(levels, prms)]
+        n = len(levels)
+        self._ptrs = (ctypes.POINTER(OrcBlock) * n)(*[ctypes.pointer(o.ob) for o in self.levels])
+        self._prms = (FFParams * n)(*prms)
+        self.L = lib()
+
+    def start(self):
+        self.levels[0].start()
+
+    def cycle(self, icycle):
+        r = (ctypes.c_double * 5)()
+        d = ctypes.c_double()
+        self.L.orc_mg_cycle(self._ptrs, len(self.levels), self._prms, icycle, r, ctypes.byref(d))
+        return np.array(r[:]), d.value
+
+
+class OracleMB:
+    """Single-grid blocks joined by 1:1 patches, for orc_mb_cycle."""
+
+    def __init__(self, blocks, prms):
+        self.blocks = [Oracle(b, p) for b, p in zip(blocks, prms)]
+        n = len(blocks)
+        self._ptrs = (ctypes.POINTER(OrcBlock) * n)(*[ctypes.pointer(o.ob) for o in self.blocks])
+        self._prms = (FFParams * n)(*prms)
+        self.L = lib()
+
+    def boundi(self):
+        self.L.orc_mb_boundi(self._ptrs, len(self.blocks), self._prms)
+
+    def start(self):
+        """NS3D start-up over all blocks: SUBIN, BOUNDI(1), SUBIN."""
+        for o in self.blocks:
+            o.subin()
+        self.boundi()
+        for o in self.blocks:
+            o.subin()
+
+    def cycle(self, icycle):
+        r = (ctypes.c_double * 5)()
+        d = ctypes.c_double()
+        self.L.orc_mb_cycle(self._ptrs, len(self.blocks), self._prms, icycle, r, ctypes.byref(d))
+        return np.array(r[:]), d.value
