@@ -42,6 +42,12 @@ class FFParams(ctypes.Structure):
             "idi1", "idi2", "idi3", "coarse_inter", "lusgs_fp32", "pad0")]
 
 
+class FFHaloItem(ctypes.Structure):
+    """ff_halo_item of include/finflo_gpu.h."""
+    _fields_ = [("blk", ctypes.c_int), ("mode", ctypes.c_int), ("offset", ctypes.c_longlong),
+                ("pa", FFPatch)]
+
+
 # enum ff_slot (include/finflo_types.h), in order
 SLOTS = ["RO", "RM", "RN", "RW", "E", "P", "PDIFF", "U", "V", "W", "C",
          "TEMP", "VIS", "CH", "CP", "DRDP", "DRDH", "EPS2", "VIST",

@@ -65,6 +65,12 @@ struct Ctx {
   cudaGraphExec_t mb_graph = nullptr;
   int mb_graph_n = -1;
   int mb_launches = 0;
+  // halo exchange with blocks on other GPUs
+  HaloItem* d_halo = nullptr;
+  int nhalo = 0, halo_maxn = 1;
+  bool halo_pack = false, halo_unpack = false;
+  double *halo_send = nullptr, *halo_recv = nullptr;
+  cudaGraphExec_t phase_graph[2] = {nullptr, nullptr};
 };
 
 int fail(Ctx* c, int code, const char* what, cudaError_t e = cudaSuccess) {
@@ -371,18 +377,21 @@ int mg_cycle(Ctx* c, BlockCtx* b, int icycle) {
   return 0;
 }
 
+void drop_phase_graphs(Ctx* c);
+
 // Device block table and connection work-list of all blocks of the context.
 int ensure_conn(Ctx* c) {
   int nb = (int)c->blocks.size();
   if (c->conn_blocks == nb) return 0;
+  drop_phase_graphs(c);
   std::vector<DevBlock> tab(nb);
   std::vector<ConnItem> items;
   int maxn = 1;
   for (int n = 0; n < nb; n++) {
     tab[n] = c->blocks[n]->db;
     for (auto& pa : c->blocks[n]->h_patch) {
-      if (pa.ityp != FF_BC_CON) continue;
-      if (pa.ibtype < 0 || pa.ibtype >= nb) return fail(c, FF_ERR_ARG, "connection to an unknown block");
+      if (pa.ityp != FF_BC_CON || pa.ibtype < 0) continue;   // negative: remote source
+      if (pa.ibtype >= nb) return fail(c, FF_ERR_ARG, "connection to an unknown block");
       ConnItem it;
       it.dst = n; it.src = pa.ibtype; it.pa = pa;
       items.push_back(it);
@@ -492,6 +501,67 @@ int mb_cycle(Ctx* c, int icycle) {
   return 0;
 }
 
+int st_halo(Ctx* c, int mode) {
+  if (!c->nhalo || !(mode == 0 ? c->halo_pack : c->halo_unpack)) return 0;
+  k_halo<<<dim3(nblk(c->halo_maxn, 128), c->nhalo), 128, 0, c->stream>>>(c->d_blocks, c->d_halo, mode,
+                                                                          c->halo_send, c->halo_recv);
+  c->nlaunch++;
+  return 0;
+}
+
+// Multi-GPU phases (see ff_mb_phase in the header).
+int mb_phase(Ctx* c, int phase, int icycle) {
+  int nb = (int)c->blocks.size(), rc;
+  if (phase == FF_PHASE_CYCLE_A) {
+    k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi, c->d_dromax);
+    c->nlaunch++;
+    rc = fork_join(c, nb, [&](int n) {
+      BlockCtx* b = c->blocks[n];
+      int r;
+      if ((r = st_residu(c, b, 1, icycle))) return r;
+      int ncell = b->imax * b->jmax * b->kmax;
+      k_resl2<<<min(nblk(ncell, 256), 4 * c->sm_count), 256, 0, c->stream>>>(b->db, c->d_resi);
+      c->nlaunch++;
+      if ((r = st_imps(c, b, 1, false))) return r;
+      return st_fin(c, b, 1);
+    });
+    if (rc) return rc;
+  }
+  if (phase == FF_PHASE_CYCLE_A || phase == FF_PHASE_BOUNDI_A) {
+    rc = fork_join(c, nb, [&](int n) {
+      BlockCtx* b = c->blocks[n];
+      k_refcor<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db);
+      c->nlaunch++;
+      if (b->npatch) {
+        int maxn = 1;
+        for (auto& p : b->h_patch) maxn = max(maxn, (p.r1b - p.r1a + 1) * (p.r2b - p.r2a + 1));
+        k_mir<<<dim3(nblk(maxn, 128), b->npatch), 128, 0, c->stream>>>(b->db);
+        c->nlaunch++;
+      }
+      return st_statim(c, b, 1);
+    });
+    if (rc) return rc;
+    if ((rc = st_connec(c))) return rc;
+    return st_halo(c, 0);
+  }
+  if (phase == FF_PHASE_B) {
+    if ((rc = st_halo(c, 1))) return rc;
+    return fork_join(c, nb, [&](int n) { return st_statim(c, c->blocks[n], 1); });
+  }
+  if (phase == FF_PHASE_RECORD) {
+    k_record<<<1, 1, 0, c->stream>>>(c->d_resi, c->d_dromax, c->d_hist, c->d_hist_pos, c->hist_cap);
+    c->nlaunch++;
+    return 0;
+  }
+  return fail(c, FF_ERR_ARG, "ff_mb_phase: unknown phase");
+}
+
+void drop_phase_graphs(Ctx* c) {
+  for (auto& g : c->phase_graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  if (c->mb_graph) { cudaGraphExecDestroy(c->mb_graph); c->mb_graph = nullptr; }
+}
+
 int run_cycle(Ctx* c, BlockCtx* b, int icycle) {
   return b->coarse ? mg_cycle(c, b, icycle) : one_cycle(c, b, icycle);
 }
@@ -503,6 +573,7 @@ int ensure_hist(Ctx* c, int n) {
   c->hist_cap = n;
   for (auto* b : c->blocks)
     if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+  drop_phase_graphs(c);
   return 0;
 }
 
@@ -547,7 +618,8 @@ int ff_destroy(void* ctx) {
     cudaFree(b->base); cudaFree(b->d_patch); cudaFree(b->coef); cudaFree(b->coef32); cudaFree(b->dw32);
     delete b;
   }
-  if (c->mb_graph) cudaGraphExecDestroy(c->mb_graph);
+  drop_phase_graphs(c);
+  cudaFree(c->d_halo);
   for (size_t n = 0; n < c->side.size(); n++) { cudaStreamDestroy(c->side[n]); cudaEventDestroy(c->side_ev[n]); }
   if (c->fork_ev) cudaEventDestroy(c->fork_ev);
   cudaFree(c->d_blocks); cudaFree(c->d_conn);
@@ -624,7 +696,7 @@ int ff_block_params(void* ctx, int blk, const ff_params* prm) {
   if (!b || !prm) return fail(c, FF_ERR_ARG, "ff_block_params");
   b->prm = *prm;
   if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
-  if (c->mb_graph) { cudaGraphExecDestroy(c->mb_graph); c->mb_graph = nullptr; }
+  drop_phase_graphs(c);
   return 0;
 }
 
@@ -782,6 +854,88 @@ int ff_lusgs_kind(void* ctx, int blk) {
 int ff_cycle_launches(void* ctx, int blk) {
   BlockCtx* b = getb((Ctx*)ctx, blk);
   return b ? b->cycle_launches : -FF_ERR_ARG;
+}
+
+int ff_halo_plan(void* ctx, int nitems, const ff_halo_item* items, double* send_buf, double* recv_buf) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || nitems < 0 || (nitems && !items)) return fail(c, FF_ERR_ARG, "ff_halo_plan");
+  int nb = (int)c->blocks.size();
+  std::vector<HaloItem> h(nitems);
+  bool pk = false, up = false;
+  int maxn = 1;
+  for (int i = 0; i < nitems; i++) {
+    const ff_halo_item& it = items[i];
+    if (it.blk < 0 || it.blk >= nb || (it.mode != 0 && it.mode != 1) || it.offset < 0)
+      return fail(c, FF_ERR_ARG, "ff_halo_plan: bad item");
+    BlockCtx* b = c->blocks[it.blk];
+    const ff_patch& pa = it.pa;
+    int face = it.mode == 0 ? pa.nface : pa.iface;
+    int n1 = pa.r1b - pa.r1a + 1, n2 = pa.r2b - pa.r2a + 1;
+    int d = (face - 1) % 3;
+    int e1 = d == 0 ? b->jmax : b->imax, e2 = d == 2 ? b->jmax : b->kmax;
+    int s1 = it.mode == 0 ? pa.n1a : pa.r1a, s2 = it.mode == 0 ? pa.n2a : pa.r2a;
+    if (face < 1 || face > 6 || n1 < 1 || n2 < 1 || s1 < 1 || s2 < 1 || s1 + n1 - 1 > e1 || s2 + n2 - 1 > e2)
+      return fail(c, FF_ERR_ARG, "ff_halo_plan: patch range outside the block");
+    if (it.mode == 0 ? !send_buf : !recv_buf) return fail(c, FF_ERR_ARG, "ff_halo_plan: missing buffer");
+    h[i].blk = it.blk; h[i].mode = it.mode; h[i].offset = it.offset; h[i].pa = pa;
+    pk = pk || it.mode == 0; up = up || it.mode == 1;
+    maxn = max(maxn, n1 * n2);
+  }
+  int rc;
+  if ((rc = ensure_conn(c))) return rc;
+  if (c->d_halo) cudaFree(c->d_halo);
+  c->d_halo = nullptr;
+  if (nitems) {
+    CK(cudaMalloc(&c->d_halo, sizeof(HaloItem) * nitems));
+    CK(cudaMemcpy(c->d_halo, h.data(), sizeof(HaloItem) * nitems, cudaMemcpyHostToDevice));
+  }
+  c->nhalo = nitems; c->halo_maxn = maxn; c->halo_pack = pk; c->halo_unpack = up;
+  c->halo_send = send_buf; c->halo_recv = recv_buf;
+  drop_phase_graphs(c);
+  return 0;
+}
+
+int ff_mb_phase(void* ctx, int phase, int icycle, int use_graph) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || c->blocks.empty()) return fail(c, FF_ERR_ARG, "ff_mb_phase");
+  for (auto* b : c->blocks)
+    if (b->coarse || b->level != 1) return fail(c, FF_ERR_ARG, "ff_mb_phase: single-grid blocks only");
+  int rc;
+  if ((rc = ensure_conn(c))) return rc;
+  if (phase == FF_PHASE_RECORD && (rc = ensure_hist(c, 1))) return rc;
+  int gi = phase == FF_PHASE_CYCLE_A ? 0 : (phase == FF_PHASE_B ? 1 : -1);
+  if (!use_graph || icycle <= 1 || gi < 0) {
+    if ((rc = mb_phase(c, phase, icycle))) return rc;
+  } else {
+    if (!c->phase_graph[gi]) {
+      cudaGraph_t g;
+      CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      rc = mb_phase(c, phase, 2);
+      cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+      if (rc) return rc;
+      if (e != cudaSuccess) return fail(c, FF_ERR_CUDA, "phase capture", e);
+      CK(cudaGraphInstantiate(&c->phase_graph[gi], g, 0));
+      cudaGraphDestroy(g);
+    }
+    CK(cudaGraphLaunch(c->phase_graph[gi], c->stream));
+  }
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int ff_history(void* ctx, int n, double* hist, int reset) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || n < 0) return fail(c, FF_ERR_ARG, "ff_history");
+  if (!hist) {
+    int rc = ensure_hist(c, max(n, 1));
+    if (rc) return rc;
+    if (reset) CK(cudaMemsetAsync(c->d_hist_pos, 0, sizeof(int), c->stream));
+    return 0;
+  }
+  if (n > c->hist_cap) return fail(c, FF_ERR_ARG, "ff_history: more rows than recorded");
+  if (n) CK(cudaMemcpyAsync(hist, c->d_hist, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost, c->stream));
+  if (reset && c->d_hist_pos) CK(cudaMemsetAsync(c->d_hist_pos, 0, sizeof(int), c->stream));
+  return ff_synchronize(ctx);
 }
 
 int ff_boundi_all(void* ctx) {

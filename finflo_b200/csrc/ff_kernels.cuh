@@ -959,6 +959,42 @@ __global__ void k_connec(const DevBlock* __restrict__ blocks, const ConnItem* __
   }
 }
 
+// Halo pack (mode 0, from the source block) / unpack (mode 1, into the
+// destination's ghost layers) of remote 1:1 patches; blockIdx.y = item.
+struct HaloItem { int blk, mode; long long offset; ff_patch pa; };
+
+__global__ void k_halo(const DevBlock* __restrict__ blocks, const HaloItem* __restrict__ items,
+                       int mode, double* __restrict__ sbuf, const double* __restrict__ rbuf) {
+  const HaloItem& it = items[blockIdx.y];
+  if (it.mode != mode) return;
+  const ff_patch& pa = it.pa;
+  int n1 = pa.r1b - pa.r1a + 1, n2 = pa.r2b - pa.r2a + 1, n = n1 * n2;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  int a = t % n1, c = t / n1;
+  const DevBlock& b = blocks[it.blk];
+  const int vs[10] = {FF_TEMP, FF_U, FF_V, FF_W, FF_E, FF_EPS2, FF_VIST, FF_CH, FF_P, FF_PDIFF};
+  if (mode == 0) {
+    FaceG fs = face_g(b, pa.nface);
+    size_t S = face_cell(b, fs, a + pa.n1a, c + pa.n2a);
+    int lss = fs.idir * fs.s;
+    double* o = sbuf + it.offset;
+#pragma unroll
+    for (int g = 0; g < 2; g++)
+#pragma unroll
+      for (int v = 0; v < 10; v++) o[(size_t)(g * 10 + v) * n + t] = b.a[vs[v]][S + g * lss];
+  } else {
+    FaceG fd = face_g(b, pa.iface);
+    size_t L = face_cell(b, fd, a + pa.r1a, c + pa.r2a);
+    int lsd = fd.idir * fd.s;
+    const double* o = rbuf + it.offset;
+#pragma unroll
+    for (int g = 0; g < 2; g++)
+#pragma unroll
+      for (int v = 0; v < 10; v++) b.a[vs[v]][L - (g + 1) * lsd] = o[(size_t)(g * 10 + v) * n + t];
+  }
+}
+
 // SUBIN ns3c.f:9742: the *OLD copies of the interior cells.
 __global__ void k_subin_copy(DevBlock b) {
   size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;

@@ -16,7 +16,7 @@ import subprocess
 
 import numpy as np
 
-from .case import FFPatch, FFParams, SLOT, SLOTS, Block
+from .case import FFHaloItem, FFPatch, FFParams, SLOT, SLOTS, Block
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libfinflo_gpu.so")
@@ -26,6 +26,7 @@ NVCC_FLAGS = ["-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC", "-shared", "-std=c++17"]
 
 FF_STAGE_RESIDUAL, FF_STAGE_GRAD, FF_STAGE_STATE = 1, 2, 3
+FF_PHASE_CYCLE_A, FF_PHASE_BOUNDI_A, FF_PHASE_B, FF_PHASE_RECORD = 0, 1, 2, 3
 
 
 class FinfloGpuError(RuntimeError):
@@ -63,6 +64,9 @@ def lib():
         L.ff_block_params.argtypes = [vp, ci, ctypes.POINTER(FFParams)]
         L.ff_mg_link.argtypes = [vp, ci, ci]
         L.ff_boundi_all.argtypes = [vp]
+        L.ff_halo_plan.argtypes = [vp, ci, ctypes.POINTER(FFHaloItem), vp, vp]
+        L.ff_mb_phase.argtypes = [vp, ci, ci, ci]
+        L.ff_history.argtypes = [vp, ci, ctypes.POINTER(cd), ci]
         L.ff_cycles_all.argtypes = [vp, ci, ci, ctypes.POINTER(cd), ci]
         L.ff_time_cycles_all.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ci)]
         L.ff_upload.argtypes = [vp, ci, ci, ctypes.POINTER(cd)]
@@ -189,6 +193,27 @@ class GpuSolver:
         hist = np.zeros((max(n, 1), 6))
         self._check(self.L.ff_cycles(self.ctx, bid, n, icycle0, _dptr(hist), int(use_graph)))
         return hist[:n]
+
+    def halo_plan(self, items, send_ptr, recv_ptr):
+        """Remote 1:1 patches: items (FFHaloItem list) and the device
+        addresses of the packed send / receive buffers."""
+        arr = (FFHaloItem * max(1, len(items)))(*items)
+        self._check(self.L.ff_halo_plan(self.ctx, len(items), arr, ctypes.c_void_p(send_ptr or None),
+                                        ctypes.c_void_p(recv_ptr or None)))
+
+    def mb_phase(self, phase, icycle=2, use_graph=True):
+        self._check(self.L.ff_mb_phase(self.ctx, phase, icycle, int(use_graph)))
+
+    def reserve_history(self, n, reset=True):
+        self._check(self.L.ff_history(self.ctx, n, None, int(reset)))
+
+    def history(self, n, reset=False) -> np.ndarray:
+        h = np.zeros((max(n, 1), 6))
+        self._check(self.L.ff_history(self.ctx, n, _dptr(h), int(reset)))
+        return h[:n]
+
+    def stream_handle(self) -> int:
+        return self.L.ff_stream(self.ctx) or 0
 
     def boundi_all(self):
         self._check(self.L.ff_boundi_all(self.ctx))

@@ -91,6 +91,44 @@ int ff_imps_noalloc(int imax, int jmax, int kmax, const ff_params *prm,
 int ff_cycles_all(void *ctx, int ncycles, int icycle0, double *hist, int use_graph);
 /* BOUNDI(1) ns3c.f:10608 over every block, 1:1 connections included. */
 int ff_boundi_all(void *ctx);
+
+/* Blocks spread over several GPUs (one context per GPU).  A 1:1 patch whose
+ * source block lives on another GPU keeps ityp = FF_BC_CON with a negative
+ * ibtype in this context; the host moves its ghost data between contexts
+ * (e.g. NCCL send/recv) as packed halo buffers.  One item per remote patch:
+ * mode 0 packs the two interior layers of local block `blk` behind the
+ * source face pa.nface (pa is the destination block's patch), mode 1 unpacks
+ * them into the ghost layers of local block `blk` behind pa.iface.  Packed
+ * layout at `offset` (doubles): [layer 0..1][var 0..9][cell of the patch],
+ * vars TEMP,U,V,W,E,EPS2,VIST,CH,P,PDIFF, cells in r1-fastest order
+ * (EXPTOT/IMPVO2 gluebm.f:6819/6964 send the same ten variables). */
+typedef struct {
+  int blk;
+  int mode;
+  long long offset;
+  ff_patch pa;
+} ff_halo_item;
+int ff_halo_plan(void *ctx, int nitems, const ff_halo_item *items, double *send_buf,
+                 double *recv_buf);
+
+/* A multi-GPU cycle, in phases with the host's exchange in between:
+ *   FF_PHASE_CYCLE_A   CYCLES of every local block, then BOUNDI part one
+ *                      (REFCOR, MIR, STATIM), local CONNEC and the halo pack;
+ *   FF_PHASE_BOUNDI_A  BOUNDI part one, local CONNEC and the pack only;
+ *   FF_PHASE_B         halo unpack and the second STATIM of every block;
+ *   FF_PHASE_RECORD    append this context's {sum of squares[5], max|dp|}
+ *                      to the history (sums add, maxima max over GPUs).
+ * Cycle phases A and B are replayed as CUDA graphs when use_graph is set
+ * and icycle > 1. */
+#define FF_PHASE_CYCLE_A 0
+#define FF_PHASE_BOUNDI_A 1
+#define FF_PHASE_B 2
+#define FF_PHASE_RECORD 3
+int ff_mb_phase(void *ctx, int phase, int icycle, int use_graph);
+/* Copy the first n history rows (6 doubles each) to the host; with
+ * hist == NULL reserve room for n rows instead.  reset != 0 restarts the
+ * history at row 0. */
+int ff_history(void *ctx, int n, double *hist, int reset);
 int ff_time_cycles_all(void *ctx, int ncycles, float *ms, int *launches_per_cycle);
 
 /* Timing helpers (CUDA events on the context stream); ff_cycle_launches is

@@ -1550,3 +1550,35 @@ void orc_mb_cycle(orc_block **blk, int nblk, const ff_params *prm, int icycle, d
   }
   *dromax = dm;
 }
+
+/* Remote 1:1 patch: the ten CONNEC variables of the two source layers
+ * packed as [layer][var][cell, r1 fastest] (the library's halo layout), and
+ * their unpacking into the destination ghosts; together they equal
+ * orc_connec_patch. */
+void orc_halo_pack(const orc_block *src, const ff_patch *pa, double *out) {
+  static const int vs[10] = {FF_TEMP, FF_U, FF_V, FF_W, FF_E, FF_EPS2, FF_VIST, FF_CH, FF_P, FF_PDIFF};
+  dims_t ds = dims_of((orc_block *)src);
+  face_t fs = face_geom(&ds, pa->nface);
+  int lss = fs.idir * fs.s;
+  int n1 = pa->r1b - pa->r1a + 1, n2 = pa->r2b - pa->r2a + 1, n = n1 * n2;
+  for (int c = 0; c < n2; c++)
+    for (int a = 0; a < n1; a++) {
+      size_t S = face_cell(&ds, &fs, a + pa->n1a, c + pa->n2a);
+      for (int g = 0; g < 2; g++)
+        for (int v = 0; v < 10; v++) out[(size_t)(g * 10 + v) * n + c * n1 + a] = src->a[vs[v]][S + g * lss];
+    }
+}
+
+void orc_halo_unpack(orc_block *dst, const ff_patch *pa, const double *in) {
+  static const int vs[10] = {FF_TEMP, FF_U, FF_V, FF_W, FF_E, FF_EPS2, FF_VIST, FF_CH, FF_P, FF_PDIFF};
+  dims_t dd = dims_of(dst);
+  face_t fd = face_geom(&dd, pa->iface);
+  int lsd = fd.idir * fd.s;
+  int n1 = pa->r1b - pa->r1a + 1, n2 = pa->r2b - pa->r2a + 1, n = n1 * n2;
+  for (int c = 0; c < n2; c++)
+    for (int a = 0; a < n1; a++) {
+      size_t L = face_cell(&dd, &fd, a + pa->r1a, c + pa->r2a);
+      for (int g = 0; g < 2; g++)
+        for (int v = 0; v < 10; v++) dst->a[vs[v]][L - (g + 1) * lsd] = in[(size_t)(g * 10 + v) * n + c * n1 + a];
+    }
+}

@@ -53,6 +53,8 @@ void orc_fin_coarse(orc_block *b, const ff_params *p);
 void orc_interp_limits(orc_block *c, orc_block *f, const ff_params *pf);
 void orc_connec_patch(orc_block *dst, const ff_patch *pa, const orc_block *src);
 void orc_connec(orc_block **blk, int nblk);
+void orc_halo_pack(const orc_block *src, const ff_patch *pa, double *out);
+void orc_halo_unpack(orc_block *dst, const ff_patch *pa, const double *in);
 void orc_mb_boundi(orc_block **blk, int nblk, const ff_params *prm);
 void orc_mb_cycle(orc_block **blk, int nblk, const ff_params *prm, int icycle, double *resi5, double *dromax);
 void orc_mg_cycle(orc_block **lv, int nlev, const ff_params *prm, int icycle, double *resi5, double *dromax);
