@@ -232,9 +232,13 @@ def bump_case(ni=65, nj=33, nk=33, *, h1=1e-3, amp=0.1, mach=0.5, reynolds=1e4,
 
 
 def bump_case_mg(ni=65, nj=33, nk=33, nlev=3, *, h1=1e-3, amp=0.1, mach=0.5, reynolds=1e4,
-                 zlen=0.5, noise=1e-3, seed=0, cfl=2.0, cfll=2.0, inter=3, span_amp=0.0):
+                 zlen=0.5, noise=1e-3, seed=0, cfl=2.0, cfll=2.0, inter=3, span_amp=0.0,
+                 lusgs_fp32=False, coarse_fp32=False):
     """The bump channel with nlev multigrid levels (finest first); coarse
-    metrics are lumped from the fine cells, patch ranges follow each level."""
+    metrics are lumped from the fine cells, patch ranges follow each level.
+    lusgs_fp32 runs the fine level's implicit operator in FP32, coarse_fp32
+    the coarse levels' (their correction reaches the fine level through
+    INTERP; residuals and updates stay FP64)."""
     fc = FlowConditions(mach=mach, reynolds=reynolds)
     fs = fc.freestream()
     X, Y, Z = grid.bump_nodes(ni, nj, nk, h1=h1, amp=amp, zlen=zlen, span_amp=span_amp)
@@ -245,6 +249,9 @@ def bump_case_mg(ni=65, nj=33, nk=33, nlev=3, *, h1=1e-3, amp=0.1, mach=0.5, rey
         levels.append(blk)
     prm = make_params(fc, levels[0].dims, cfl=cfl, cfll=cfll, inter=inter)
     prms = [level_params(prm, lev + 1) for lev in range(nlev)]
+    prms[0].lusgs_fp32 = int(lusgs_fp32)
+    for q in prms[1:]:
+        q.lusgs_fp32 = int(coarse_fp32)
     return levels, prms, fs
 
 
@@ -262,15 +269,23 @@ def _face_ranges(iface, imax, jmax, kmax):
     return (1, imax), (1, jmax)
 
 
-def box_block_sizes(nb=(4, 3, 2), lo=17, hi=97, seed=36):
-    """Cells per block along each direction, drawn uniformly from {lo..hi}
-    with the seed; block (a, b, c) of the Cartesian arrangement has
-    (ni[a], nj[b], nk[c]) cells, so every interface is 1:1."""
+def box_block_sizes(nb=(4, 3, 2), seed=2, target=6.0e6, tol=0.10, nodes=tuple(range(17, 98, 4))):
+    """Cells per block along each direction of the Cartesian block
+    arrangement: node counts drawn with the seed from {17, 21, ..., 97} (one
+    more than a multiple of 4, so every block has three multigrid levels),
+    redrawn until the total is within tol of target cells.  Block (a, b, c)
+    has (ni[a], nj[b], nk[c]) cells, so every interface is 1:1."""
     rng = np.random.default_rng(seed)
-    return tuple([int(v) for v in rng.integers(lo, hi + 1, size=n)] for n in nb)
+    nodes = np.asarray(nodes)
+    for _ in range(100000):
+        s = tuple([int(v) - 1 for v in rng.choice(nodes, size=n)] for n in nb)
+        cells = sum(s[0]) * sum(s[1]) * sum(s[2])
+        if abs(cells - target) <= tol * target:
+            return s
+    raise RuntimeError("no block split within the target size")
 
 
-def periodic_box_case(nb=(4, 3, 2), sizes=None, *, seed=36, lo=17, hi=97, mach=0.3,
+def periodic_box_case(nb=(4, 3, 2), sizes=None, *, seed=2, mach=0.3, target=None,
                       amp=1e-2, cfl=2.0, inter=3, lusgs_fp32=False, wave=(1, 1, 1)):
     """The unit box split into nb[0] x nb[1] x nb[2] blocks with 1:1 patches on
     every interface, periodic in all three directions (the outer faces are
@@ -279,7 +294,9 @@ def periodic_box_case(nb=(4, 3, 2), sizes=None, *, seed=36, lo=17, hi=97, mach=0
     with an entropy wave rho = rho0 (1 + amp sin(2 pi k.x + phi)) at constant
     pressure; phi comes from the seed.  Returns blocks, params, free stream."""
     if sizes is None:
-        sizes = box_block_sizes(nb, lo, hi, seed)
+        # 6M cells for the 24-block arrangement, proportionally fewer otherwise
+        tgt = target if target is not None else 6.0e6 * nb[0] * nb[1] * nb[2] / 24
+        sizes = box_block_sizes(nb, seed, target=tgt)
     ni, nj, nk = sizes
     fc = FlowConditions(mach=mach, reynolds=0.0)
     fs = fc.freestream()

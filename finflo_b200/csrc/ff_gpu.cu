@@ -695,7 +695,9 @@ int ff_block_params(void* ctx, int blk, const ff_params* prm) {
   BlockCtx* b = getb(c, blk);
   if (!b || !prm) return fail(c, FF_ERR_ARG, "ff_block_params");
   b->prm = *prm;
-  if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+  // captured cycles of any block may include this one (multigrid levels)
+  for (auto* x : c->blocks)
+    if (x->graph) { cudaGraphExecDestroy(x->graph); x->graph = nullptr; }
   drop_phase_graphs(c);
   return 0;
 }

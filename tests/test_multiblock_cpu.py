@@ -50,10 +50,10 @@ def test_periodic_box_conserves_and_preserves_free_stream():
 def test_box_block_sizes_are_seeded_and_in_range():
     s = case.box_block_sizes()
     assert s == case.box_block_sizes()
-    assert all(17 <= v <= 97 for d in s for v in d)
+    assert all(16 <= v <= 96 and v % 4 == 0 for d in s for v in d)
     assert [len(d) for d in s] == [4, 3, 2]
     cells = sum(a * b * c for a in s[0] for b in s[1] for c in s[2])
-    assert 5.5e6 < cells < 6.5e6
+    assert 5.4e6 <= cells <= 6.6e6
 
 
 def test_multiblock_cycles_converge():
