@@ -198,6 +198,8 @@ def run_ours(args):
     achieved = bytes_per_cell * ncell / (ms_res * 1e-3) / 1e9
     peak, kind = _peaks()
     launches = g.cycle_launches(bid) * args.steps
+    lk = g.lusgs_kind(bid)
+    sweep = dict(g.sweep_tuning(bid), chosen="cluster lines" if lk % 100 == 1 else "cooperative hyperplane")
     # ---- end to end through the C-ABI with host buffers ----------------
     names_in = ["TEMP", "U", "V", "W", "PDIFF"]
     host = {n: blk.arrays[n] for n in names_in}
@@ -220,7 +222,7 @@ def run_ours(args):
         "data": "synthetic (seeded bump-channel grid and noisy free stream)",
         "config": {"workload": WORKLOAD_NAME if not args.grid else f"bump channel {blk.imax}x{blk.jmax}x{blk.kmax} cells (profiling size)",
                    "cells_per_gpu": ncell, "parallelism": f"replicas x{ws}",
-                   "l2": "working set < L2 (cycle state resident)"},
+                   "l2": "working set < L2 (cycle state resident)", "lusgs_sweep": sweep},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "kernel": "k_residual", "achieved": achieved, "peak": peak,
                      "peak_kind": kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,

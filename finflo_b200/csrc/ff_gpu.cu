@@ -29,6 +29,8 @@ struct BlockCtx {
   float* dw32 = nullptr;        // 5 x ntot
   int coop_blocks = 0, coop_blocks32 = 0;
   int use_lines = 0;            // 1: cluster line-wavefront LU-SGS
+  int tuned = 0;                // sweep kind chosen by tune_sweep
+  float sweep_ms[2] = {0.f, 0.f};   // measured lower sweep: lines, hyperplane
   LineGeom lg{};
   size_t lines_smem = 0, lines_smem32 = 0;
   DevBlock db{};
@@ -207,6 +209,9 @@ int lines_sweep(Ctx* c, BlockCtx* b, int upper, bool fp32) {
   return 0;
 }
 
+constexpr int kMaxDev = 64;
+int g_lines_smem[kMaxDev][2];   // dynamic shared memory granted to k_lusgs_lines<f64|f32>
+
 // Choose the LU-SGS sweep kernel of a block: the cluster line wavefront
 // when the (j,k) line tiles fit one cluster, else the cooperative hyperplane
 // kernel.
@@ -221,10 +226,18 @@ int setup_lines(Ctx* c, BlockCtx* b) {
     size_t sm64 = (size_t)25 * tpc * LTHREADS * sizeof(double);
     size_t sm32 = (size_t)25 * tpc * LTHREADS * sizeof(float);
     if (sm64 > 200 * 1024) continue;
+    // kernel attributes are per device, shared by all blocks: only raise them
+    if (c->device < 0 || c->device >= kMaxDev) return fail(c, FF_ERR_ARG, "device id");
     CK(cudaFuncSetAttribute(k_lusgs_lines<double>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     CK(cudaFuncSetAttribute(k_lusgs_lines<float>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    CK(cudaFuncSetAttribute(k_lusgs_lines<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm64));
-    CK(cudaFuncSetAttribute(k_lusgs_lines<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm32));
+    if ((int)sm64 > g_lines_smem[c->device][0]) {
+      CK(cudaFuncSetAttribute(k_lusgs_lines<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm64));
+      g_lines_smem[c->device][0] = (int)sm64;
+    }
+    if ((int)sm32 > g_lines_smem[c->device][1]) {
+      CK(cudaFuncSetAttribute(k_lusgs_lines<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm32));
+      g_lines_smem[c->device][1] = (int)sm32;
+    }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(csz);
     cfg.blockDim = dim3(LTHREADS);
@@ -248,6 +261,63 @@ int setup_lines(Ctx* c, BlockCtx* b) {
     return 0;
   }
   b->use_lines = 0;
+  return 0;
+}
+
+// Sweep autotuner: a cluster line sweep uses at most 16 SMs per block, the
+// cooperative hyperplane sweep the whole GPU with a barrier per plane; which
+// is faster depends on the block's shape.  Time both (lower sweep, on the
+// block's current coefficients, into a scratch increment buffer so the
+// block's data is untouched) and keep the faster.  Blocks that run side by
+// side in a multi-block cycle keep the line sweep (see fork_join).
+int tune_sweep(Ctx* c, BlockCtx* b) {
+  if (b->tuned) return 0;
+  b->tuned = 1;
+  const char* env = getenv("FINFLO_LUSGS");
+  if (!b->use_lines || (env && (!strcmp(env, "hyperplane") || !strcmp(env, "lines")))) return 0;
+  int ncell = b->imax * b->jmax * b->kmax;
+  double* scratch = nullptr;
+  CK(cudaMalloc(&scratch, sizeof(double) * 5 * (size_t)b->ntot));
+  CK(cudaMemsetAsync(scratch, 0, sizeof(double) * 5 * (size_t)b->ntot, c->stream));
+  k_lusgs_coef<double><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, b->coef, 1);
+  float best[2] = {0.f, 0.f};
+  int rc = 0;
+  for (int kind = 0; kind < 2 && !rc; kind++) {
+    for (int rep = 0; rep < 4 && !rc; rep++) {   // rep 0 warms up
+      cudaEventRecord(c->ev0, c->stream);
+      cudaError_t e;
+      if (kind == 0) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(b->lg.cs); cfg.blockDim = dim3(LTHREADS);
+        cfg.dynamicSmemBytes = b->lines_smem; cfg.stream = c->stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = b->lg.cs; attr[0].val.clusterDim.y = 1; attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr; cfg.numAttrs = 1;
+        e = cudaLaunchKernelEx(&cfg, k_lusgs_lines<double>, b->db, (const double*)b->coef, scratch, 1, b->lg);
+      } else {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(b->coop_blocks); cfg.blockDim = dim3(256); cfg.stream = c->stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative; attr[0].val.cooperative = 1;
+        cfg.attrs = attr; cfg.numAttrs = 1;
+        e = cudaLaunchKernelEx(&cfg, k_lusgs_sweep<double>, b->db, (const double*)b->coef, scratch, 1,
+                               c->d_bar, c->d_err);
+      }
+      if (e != cudaSuccess) { rc = fail(c, FF_ERR_CUDA, "sweep autotune launch", e); break; }
+      cudaEventRecord(c->ev1, c->stream);
+      cudaError_t s2 = cudaEventSynchronize(c->ev1);
+      if (s2 != cudaSuccess) { rc = fail(c, FF_ERR_CUDA, "sweep autotune", s2); break; }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+      if (rep > 0) best[kind] = rep == 1 ? ms : fminf(best[kind], ms);
+    }
+  }
+  cudaFree(scratch);
+  if (rc) return rc;
+  b->sweep_ms[0] = best[0];
+  b->sweep_ms[1] = best[1];
+  if (best[1] < best[0]) b->use_lines = 0;
   return 0;
 }
 
@@ -675,6 +745,7 @@ int ff_block_add(void* ctx, int imax, int jmax, int kmax, int npatch, const ff_p
     const char* env = getenv("FINFLO_LUSGS");
     if (env && strcmp(env, "hyperplane") == 0) b->use_lines = 0;
   }
+  b->tuned = 0;
   c->blocks.push_back(b);
   return (int)c->blocks.size() - 1;
 }
@@ -813,6 +884,12 @@ int ff_cycles(void* ctx, int blk, int ncycles, int icycle0, double* hist, int us
   BlockCtx* b = getb(c, blk);
   if (!b || ncycles < 0) return fail(c, FF_ERR_ARG, "ff_cycles");
   int rc;
+  for (BlockCtx* x = b; x; x = x->coarse) {
+    if (!x->tuned) {
+      if ((rc = tune_sweep(c, x))) return rc;
+      if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+    }
+  }
   if ((rc = ensure_hist(c, max(ncycles, 1)))) return rc;
   CK(cudaMemsetAsync(c->d_hist_pos, 0, sizeof(int), c->stream));
   int it = 0;
@@ -845,6 +922,14 @@ int ff_cycles(void* ctx, int blk, int ncycles, int icycle0, double* hist, int us
     rc = ff_synchronize(ctx);
     if (rc) return rc;
   }
+  return 0;
+}
+
+int ff_sweep_tuning(void* ctx, int blk, float* ms2) {
+  BlockCtx* b = getb((Ctx*)ctx, blk);
+  if (!b || !ms2) return FF_ERR_ARG;
+  ms2[0] = b->sweep_ms[0];
+  ms2[1] = b->sweep_ms[1];
   return 0;
 }
 

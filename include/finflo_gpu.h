@@ -136,6 +136,9 @@ int ff_time_cycles_all(void *ctx, int ncycles, float *ms, int *launches_per_cycl
 int ff_cycle_launches(void *ctx, int blk);
 /* LU-SGS sweep kernel of a block: 0 = cooperative hyperplane kernel,
  * 1 + 100*cluster_size = cluster line wavefront. */
+/* The autotuner's measured lower-sweep times in ms {cluster lines, cooperative
+ * hyperplane} of a block (zeros until its first ff_cycles call). */
+int ff_sweep_tuning(void *ctx, int blk, float *ms2);
 int ff_lusgs_kind(void *ctx, int blk);
 int ff_time_cycles(void *ctx, int blk, int ncycles, float *ms);
 int ff_time_stage(void *ctx, int blk, int stage, int reps, float *ms);
