@@ -29,14 +29,16 @@ class FFPatch(ctypes.Structure):
                 ("bounr", ctypes.c_double), ("bounu", ctypes.c_double),
                 ("bounv", ctypes.c_double), ("bounw", ctypes.c_double),
                 ("bount", ctypes.c_double), ("bounp", ctypes.c_double),
-                ("bounpd", ctypes.c_double)]
+                ("bounpd", ctypes.c_double), ("bounrk", ctypes.c_double),
+                ("bounep", ctypes.c_double)]
 
 
 class FFParams(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in (
         "gamma", "rgas", "pr", "prt", "visu0", "expsu", "tsu0", "e0ref", "t0ref",
         "frsden", "frspre", "frsvel", "frsvis", "frstem", "cfl", "cfll", "theta",
-        "cdiff", "pvisc", "tlolim", "tuplim", "cmgk", "cmgeps")] + [
+        "cdiff", "pvisc", "tlolim", "tuplim", "cmgk", "cmgeps",
+        "rklim", "epslim", "turlim", "csimps", "re")] + [
         (n, ctypes.c_int) for n in (
             "interi", "interj", "interk", "entropy_fix", "iturb", "fullns",
             "idi1", "idi2", "idi3", "coarse_inter", "lusgs_fp32", "pad0")]
@@ -51,14 +53,17 @@ class FFHaloItem(ctypes.Structure):
 # enum ff_slot (include/finflo_types.h), in order
 SLOTS = ["RO", "RM", "RN", "RW", "E", "P", "PDIFF", "U", "V", "W", "C",
          "TEMP", "VIS", "CH", "CP", "DRDP", "DRDH", "EPS2", "VIST",
-         "DRO", "DM", "DN", "DW", "DE", "DTL",
+         "DRO", "DM", "DN", "DW", "DE", "DRK", "DEPS", "DTL",
          "TOLD", "UOLD", "VOLD", "WOLD", "POLD",
          "A1", "A1XA", "A1YA", "A1ZA", "A2", "A2XA", "A2YA", "A2ZA",
          "A3", "A3XA", "A3YA", "A3ZA", "VOL", "XC", "YC", "ZC", "D1", "D2", "D3",
          "W12", "W13", "W23", "S11", "S12", "S13", "S22", "S23", "S33",
          "DTDX", "DTDY", "DTDZ", "OHMI", "STRAIN",
          "F1R", "F1RM", "F1RN", "F1RW", "F1E",
-         "ROP2H", "RMP2H", "RNP2H", "RWP2H", "EP2H"]
+         "ROP2H", "RMP2H", "RNP2H", "RWP2H", "EP2H",
+         "RK", "REPS", "DISTW", "FUN1", "SRK", "SEPS", "PTUR",
+         "DKDX", "DKDY", "DKDZ", "DEDX", "DEDY", "DEDZ",
+         "RKOLD", "EPSOLD", "F1RK", "F1EPS", "RKP2H", "EPP2H"]
 SLOT = {n: i for i, n in enumerate(SLOTS)}
 STATE_SLOTS = SLOTS[:19]
 METRIC_SLOTS = list(grid.METRIC_NAMES)
@@ -102,6 +107,8 @@ def make_params(fc: FlowConditions, dims, *, cfl=2.0, cfll=2.0, inter=3,
     p.theta, p.cdiff, p.pvisc = 1.5, 2.0, 1.8
     p.tlolim, p.tuplim = 0.05 * fs["t"], 6.0 * fs["t"]
     p.cmgk, p.cmgeps = 0.1, 0.2
+    p.turlim, p.csimps = 5000.0, 5.0
+    p.re = fs["rho"] * fs["u"] / fs["mu"]     # per unit reference length
     p.interi = p.interj = p.interk = inter
     p.entropy_fix = int(entropy_fix)
     p.iturb = iturb
@@ -218,9 +225,45 @@ def init_freestream(b: Block, fs, *, noise=1e-3, seed=0):
     return b
 
 
+def wall_distance(blk: Block):
+    """DISTW: distance of every cell centre (ghosts included) to the nearest
+    face centre of the block's solid-wall patches (set-up data, like the
+    reference's DISTANCES pass before the iteration loop)."""
+    from scipy.spatial import cKDTree
+    X, Y, Z = blk.nodes
+    pts = []
+    for pa in blk.patches:
+        if not (7 <= pa.ityp <= 10):
+            continue
+        d = (pa.iface - 1) % 3
+        idx = 0 if pa.iface <= 3 else (X.shape[2 - d] - 1)
+        sl = [slice(None)] * 3
+        sl[2 - d] = idx
+        fx, fy, fz = (np.asarray(a[tuple(sl)]) for a in (X, Y, Z))
+        c = [0.25 * (f[:-1, :-1] + f[1:, :-1] + f[:-1, 1:] + f[1:, 1:]) for f in (fx, fy, fz)]
+        pts.append(np.stack([c[0].ravel(), c[1].ravel(), c[2].ravel()], axis=1))
+    if not pts:
+        return np.full(blk.ntot, 1.0e3)
+    tree = cKDTree(np.concatenate(pts))
+    q = np.stack([blk.arrays["XC"], blk.arrays["YC"], blk.arrays["ZC"]], axis=1)
+    dist, _ = tree.query(q)
+    return dist
+
+
+def sst_freestream(fs, tu=1.0e-3, mut_ratio=0.1):
+    """Free-stream rho*k and rho*omega from the turbulence intensity and
+    mu_t/mu (main.f:3770-3790, IDIS=2): rho*k = 1.5 rho (Tu U)^2,
+    rho*omega = rho (rho*k) / mu_t."""
+    rk = 1.5 * fs["rho"] * (tu * fs["u"]) ** 2
+    mut = mut_ratio * fs["mu"]
+    return rk, fs["rho"] * rk / mut
+
+
 def bump_case(ni=65, nj=33, nk=33, *, h1=1e-3, amp=0.1, mach=0.5, reynolds=1e4,
-              zlen=0.5, noise=1e-3, seed=0, cfl=2.0, inter=3, span_amp=0.0):
-    """The single-block laminar bump channel (node counts ni x nj x nk)."""
+              zlen=0.5, noise=1e-3, seed=0, cfl=2.0, inter=3, span_amp=0.0,
+              turbulence=None, tu=1.0e-3, mut_ratio=0.1):
+    """The single-block bump channel (node counts ni x nj x nk); laminar, or
+    k-omega SST with turbulence="sst" (free-stream Tu and mu_t/mu)."""
     fc = FlowConditions(mach=mach, reynolds=reynolds)
     fs = fc.freestream()
     X, Y, Z = grid.bump_nodes(ni, nj, nk, h1=h1, amp=amp, zlen=zlen, span_amp=span_amp)
@@ -228,7 +271,28 @@ def bump_case(ni=65, nj=33, nk=33, *, h1=1e-3, amp=0.1, mach=0.5, reynolds=1e4,
     blk = new_block(X, Y, Z, channel_patches(imax, jmax, kmax, fs))
     init_freestream(blk, fs, noise=noise, seed=seed)
     prm = make_params(fc, blk.dims, cfl=cfl, inter=inter)
+    if turbulence == "sst":
+        setup_sst(blk, prm, fs, tu=tu, mut_ratio=mut_ratio)
     return blk, prm, fs
+
+
+def setup_sst(blk: Block, prm: FFParams, fs, tu=1.0e-3, mut_ratio=0.1):
+    """Switch a case to k-omega SST: ITURB=6, the free-stream limits RKLIM /
+    EPSLIM, inlet BOUNRK/BOUNEP, DISTW, and rho*k, rho*omega, mu_t of the
+    free stream in every cell."""
+    rk, re = sst_freestream(fs, tu, mut_ratio)
+    prm.iturb = 6
+    prm.rklim, prm.epslim = rk, re
+    for pa in blk.patches:
+        pa.bounrk, pa.bounep = rk, re
+    blk.arrays["DISTW"][:] = wall_distance(blk)
+    blk.arrays["RK"][:] = rk
+    blk.arrays["REPS"][:] = re
+    blk.arrays["EPS2"][:] = 1.0 + mut_ratio
+    blk.arrays["VIST"][:] = mut_ratio * fs["mu"]
+    blk.arrays["RKOLD"][:] = rk
+    blk.arrays["EPSOLD"][:] = re
+    return blk
 
 
 def bump_case_mg(ni=65, nj=33, nk=33, nlev=3, *, h1=1e-3, amp=0.1, mach=0.5, reynolds=1e4,

@@ -189,6 +189,48 @@ FF_DI void jac_product(T out[5], const T dw[5], T c, T ro, T nx, T ny, T nz, T l
   out[3] = nz * x2i + a23 * w3 + a33 * w4;
 }
 
+// SYIKE / SYM1KE imps4.f:982/1034: the seven-equation product of PRKEGS /
+// COKEGS, SYM1KE(diag(l1,l2,l1,l1,l5,l1,l1) * SYIKE(dw)).
+template <typename T>
+FF_DI void jac_product_ke(T out[7], const T dw[7], T rk, T c, T ro, T drdp, T drdh, T nx, T ny, T nz, T l1,
+                          T l2, T l5) {
+  T a21, a22, a23, a31, a32, a33;
+  surfvects(nx, ny, nz, a21, a22, a23, a31, a32, a33);
+  T z2 = nx * dw[1] + ny * dw[2] + nz * dw[3];
+  T z3 = a21 * dw[1] + a22 * dw[2] + a23 * dw[3];
+  T z4 = a31 * dw[1] + a32 * dw[2] + a33 * dw[3];
+  T roc = ro * c, pc2 = T(1) / ro, dpres = dw[4];
+  T w1 = l1 * (dw[0] - pc2 * dpres);
+  T w2 = l2 * (roc * z2 + dpres);
+  T w3 = l1 * z3, w4 = l1 * z4;
+  T w5 = l5 * (-roc * z2 + dpres);
+  T w6 = l1 * dw[5], w7 = l1 * dw[6];
+  T ypro = T(1) / ro, pc2b = T(.5) * ypro, proc = pc2b / c;
+  T drh = T(.667) * rk * (ypro * ypro) * drdh;
+  T ydrp = T(1) / (T(1) + T(.667) * rk * ypro * drdp);
+  T dh = w1 + pc2b * (w2 + w5);
+  out[0] = dh;
+  T x2i = proc * (w2 - w5);
+  out[4] = ydrp * (T(.5) * (w2 + w5) - drh * ro * dh - T(.667) * ro * w6);
+  out[5] = w6;
+  out[6] = w7;
+  out[1] = nx * x2i + a21 * w3 + a31 * w4;
+  out[2] = ny * x2i + a22 * w3 + a32 * w4;
+  out[3] = nz * x2i + a23 * w3 + a33 * w4;
+}
+
+// One neighbour's product for NV = 5 (laminar) or 7 (k-omega) equations.
+template <typename T, int NV>
+FF_DI void nb_product(T* out, const T* dw, const DevBlock& b, size_t n, T c, T ro, T nx, T ny, T nz, T l1, T l2,
+                      T l5) {
+  if constexpr (NV == 5) {
+    jac_product<T>(out, dw, c, ro, nx, ny, nz, l1, l2, l5);
+  } else {
+    jac_product_ke<T>(out, dw, (T)__ldg(b.a[FF_RK] + n), c, ro, (T)__ldg(b.a[FF_DRDP] + n),
+                      (T)__ldg(b.a[FF_DRDH] + n), nx, ny, nz, l1, l2, l5);
+  }
+}
+
 // Bounded grid-wide barrier for a co-resident (cooperative) grid.  Every
 // spin has an iteration limit; on time-out the error word is set and all
 // blocks leave the kernel at their next barrier.

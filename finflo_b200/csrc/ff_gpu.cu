@@ -26,7 +26,8 @@ struct BlockCtx {
   ff_params prm{};
   double* coef = nullptr;       // NCOEF x ntot (FP64 LU-SGS)
   float* coef32 = nullptr;      // NCOEF x ntot (FP32 LU-SGS)
-  float* dw32 = nullptr;        // 5 x ntot
+  float* dw32 = nullptr;        // 7 x ntot
+  unsigned long long* d_red = nullptr;   // per-block reduction word (FUN1KO CDMAX)
   int coop_blocks = 0, coop_blocks32 = 0;
   int use_lines = 0;            // 1: cluster line-wavefront LU-SGS
   int tuned = 0;                // sweep kind chosen by tune_sweep
@@ -140,7 +141,41 @@ int st_boundi(Ctx* c, BlockCtx* b) {
   return st_statim(c, b);
 }
 
+// TURBEQ res3c.f:5845 and RESIKE res3c.f:3423 (k-omega SST, level 1).
+int st_residu_sst(Ctx* c, BlockCtx* b, int icycle) {
+  int ncell = b->imax * b->jmax * b->kmax;
+  long ng = (long)(b->imax + 2) * (b->jmax + 2) * (b->kmax + 2);
+  k_grad<<<nblk(ng, 128), 128, 0, c->stream>>>(b->db, 1);              // DERFUN (+ TEMDER of T)
+  k_eps2ko<<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm);
+  k_crosko<<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db);
+  k_rk_roundtrip<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db);
+  CK(cudaMemsetAsync(b->d_red, 0, sizeof(unsigned long long), c->stream));
+  k_cdmax<<<min(nblk(b->ntot, 256), 4 * c->sm_count), 256, 0, c->stream>>>(b->db, b->d_red);
+  k_fun1ko<<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, b->d_red);
+  c->nlaunch += 6;
+  if (b->npatch) {
+    int maxn = 1;
+    for (auto& p : b->h_patch) maxn = max(maxn, (p.r1b - p.r1a + 1) * (p.r2b - p.r2a + 1));
+    k_refcen<<<dim3(nblk(maxn, 128), b->npatch), 128, 0, c->stream>>>(b->db, b->prm);
+    c->nlaunch++;
+  }
+  k_prodke<<<nblk((long)b->jmax * b->db.is * b->kmax, 128), 128, 0, c->stream>>>(b->db);
+  long nt3 = (long)(b->imax + 2) * (b->jmax + 2) * (b->kmax > 1 ? b->kmax + 2 : b->kmax);
+  k_temder_ke<<<nblk(nt3, 128), 128, 0, c->stream>>>(b->db);
+  c->nlaunch += 2;
+  launch_patch(c, b, k_inlet_outlet, icycle);
+  dim3 g(nblk(b->imax, TI), nblk(b->jmax, TJ), nblk(b->kmax, TK));
+  k_residual_sst<<<g, 128, 0, c->stream>>>(b->db, b->prm);
+  k_sourko_addske<<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db);
+  c->nlaunch += 2;
+  return 0;
+}
+
 int st_residu(Ctx* c, BlockCtx* b, int level, int icycle) {
+  if (b->prm.iturb >= 3) {
+    if (level != 1) return fail(c, FF_ERR_ARG, "k-omega SST runs on the finest level only");
+    return st_residu_sst(c, b, icycle);
+  }
   if (level == 1) {
     if (b->npatch) {
       int maxn = 1;
@@ -164,7 +199,7 @@ int st_residu(Ctx* c, BlockCtx* b, int level, int icycle) {
 int coop_sweep(Ctx* c, BlockCtx* b, int upper, bool fp32) {
   int nb = fp32 ? b->coop_blocks32 : b->coop_blocks;
   double* dw64 = b->base + (size_t)FF_DRO * b->slot_stride;
-  // the five increment slots are contiguous: DRO, DM, DN, DW, DE
+  // the increment slots are contiguous: DRO, DM, DN, DW, DE (, DRK, DEPS)
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(nb);
   cfg.blockDim = dim3(256);
@@ -176,12 +211,17 @@ int coop_sweep(Ctx* c, BlockCtx* b, int upper, bool fp32) {
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   cudaError_t e;
+  const bool ke = b->prm.iturb >= 3;   // seven equations (k-omega)
   if (!fp32) {
-    e = cudaLaunchKernelEx(&cfg, k_lusgs_sweep<double>, b->db, (const double*)b->coef, dw64, upper,
-                           c->d_bar, c->d_err);
+    e = ke ? cudaLaunchKernelEx(&cfg, k_lusgs_sweep<double, 7>, b->db, (const double*)b->coef, dw64, upper,
+                                c->d_bar, c->d_err)
+           : cudaLaunchKernelEx(&cfg, k_lusgs_sweep<double, 5>, b->db, (const double*)b->coef, dw64, upper,
+                                c->d_bar, c->d_err);
   } else {
-    e = cudaLaunchKernelEx(&cfg, k_lusgs_sweep<float>, b->db, (const float*)b->coef32, b->dw32, upper,
-                           c->d_bar, c->d_err);
+    e = ke ? cudaLaunchKernelEx(&cfg, k_lusgs_sweep<float, 7>, b->db, (const float*)b->coef32, b->dw32, upper,
+                                c->d_bar, c->d_err)
+           : cudaLaunchKernelEx(&cfg, k_lusgs_sweep<float, 5>, b->db, (const float*)b->coef32, b->dw32, upper,
+                                c->d_bar, c->d_err);
   }
   if (e != cudaSuccess) return fail(c, FF_ERR_CUDA, "cooperative sweep launch", e);
   c->nlaunch++;
@@ -202,42 +242,57 @@ int lines_sweep(Ctx* c, BlockCtx* b, int upper, bool fp32) {
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   double* dw64 = b->base + (size_t)FF_DRO * b->slot_stride;
-  cudaError_t e = fp32 ? cudaLaunchKernelEx(&cfg, k_lusgs_lines<float>, b->db, (const float*)b->coef32, b->dw32, upper, b->lg)
-                       : cudaLaunchKernelEx(&cfg, k_lusgs_lines<double>, b->db, (const double*)b->coef, dw64, upper, b->lg);
+  cudaError_t e;
+  if (b->prm.iturb >= 3)
+    e = fp32 ? cudaLaunchKernelEx(&cfg, k_lusgs_lines<float, 7>, b->db, (const float*)b->coef32, b->dw32, upper, b->lg)
+             : cudaLaunchKernelEx(&cfg, k_lusgs_lines<double, 7>, b->db, (const double*)b->coef, dw64, upper, b->lg);
+  else
+    e = fp32 ? cudaLaunchKernelEx(&cfg, k_lusgs_lines<float, 5>, b->db, (const float*)b->coef32, b->dw32, upper, b->lg)
+             : cudaLaunchKernelEx(&cfg, k_lusgs_lines<double, 5>, b->db, (const double*)b->coef, dw64, upper, b->lg);
   if (e != cudaSuccess) return fail(c, FF_ERR_CUDA, "cluster sweep launch", e);
   c->nlaunch++;
   return 0;
 }
 
 constexpr int kMaxDev = 64;
-int g_lines_smem[kMaxDev][2];   // dynamic shared memory granted to k_lusgs_lines<f64|f32>
+int g_lines_smem[kMaxDev][4];   // dynamic shared memory granted to k_lusgs_lines<f64|f32, 5|7>
 
 // Choose the LU-SGS sweep kernel of a block: the cluster line wavefront
 // when the (j,k) line tiles fit one cluster, else the cooperative hyperplane
 // kernel.
+template <int NV>
+int lines_attrs(Ctx* c, size_t sm64, size_t sm32) {
+  int* g = g_lines_smem[c->device] + (NV == 7 ? 2 : 0);
+  CK(cudaFuncSetAttribute(k_lusgs_lines<double, NV>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  CK(cudaFuncSetAttribute(k_lusgs_lines<float, NV>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  if ((int)sm64 > g[0]) {
+    CK(cudaFuncSetAttribute(k_lusgs_lines<double, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm64));
+    g[0] = (int)sm64;
+  }
+  if ((int)sm32 > g[1]) {
+    CK(cudaFuncSetAttribute(k_lusgs_lines<float, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm32));
+    g[1] = (int)sm32;
+  }
+  return 0;
+}
+
 int setup_lines(Ctx* c, BlockCtx* b) {
   LineGeom lg{};
   lg.ntj = (b->jmax + LTJ - 1) / LTJ;
   lg.ntk = (b->kmax + LTK - 1) / LTK;
   lg.ntiles = lg.ntj * lg.ntk;
+  const int nv = b->prm.iturb >= 3 ? 7 : 5;
+  if (c->device < 0 || c->device >= kMaxDev) return fail(c, FF_ERR_ARG, "device id");
   for (int cs = 16; cs >= 1; cs /= 2) {
     int csz = min(cs, lg.ntiles);
     int tpc = (lg.ntiles + csz - 1) / csz;
-    size_t sm64 = (size_t)25 * tpc * LTHREADS * sizeof(double);
-    size_t sm32 = (size_t)25 * tpc * LTHREADS * sizeof(float);
+    // pub [2][tpc][2 NV] + ydb [tpc][NV] values per thread
+    size_t sm64 = (size_t)5 * nv * tpc * LTHREADS * sizeof(double);
+    size_t sm32 = (size_t)5 * nv * tpc * LTHREADS * sizeof(float);
     if (sm64 > 200 * 1024) continue;
     // kernel attributes are per device, shared by all blocks: only raise them
-    if (c->device < 0 || c->device >= kMaxDev) return fail(c, FF_ERR_ARG, "device id");
-    CK(cudaFuncSetAttribute(k_lusgs_lines<double>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    CK(cudaFuncSetAttribute(k_lusgs_lines<float>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    if ((int)sm64 > g_lines_smem[c->device][0]) {
-      CK(cudaFuncSetAttribute(k_lusgs_lines<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm64));
-      g_lines_smem[c->device][0] = (int)sm64;
-    }
-    if ((int)sm32 > g_lines_smem[c->device][1]) {
-      CK(cudaFuncSetAttribute(k_lusgs_lines<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm32));
-      g_lines_smem[c->device][1] = (int)sm32;
-    }
+    int rc = nv == 7 ? lines_attrs<7>(c, sm64, sm32) : lines_attrs<5>(c, sm64, sm32);
+    if (rc) return rc;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(csz);
     cfg.blockDim = dim3(LTHREADS);
@@ -248,7 +303,9 @@ int setup_lines(Ctx* c, BlockCtx* b) {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     int nclusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&nclusters, k_lusgs_lines<double>, &cfg) != cudaSuccess || nclusters < 1) {
+    cudaError_t e = nv == 7 ? cudaOccupancyMaxActiveClusters(&nclusters, k_lusgs_lines<double, 7>, &cfg)
+                            : cudaOccupancyMaxActiveClusters(&nclusters, k_lusgs_lines<double, 5>, &cfg);
+    if (e != cudaSuccess || nclusters < 1) {
       cudaGetLastError();
       continue;
     }
@@ -277,8 +334,8 @@ int tune_sweep(Ctx* c, BlockCtx* b) {
   if (!b->use_lines || (env && (!strcmp(env, "hyperplane") || !strcmp(env, "lines")))) return 0;
   int ncell = b->imax * b->jmax * b->kmax;
   double* scratch = nullptr;
-  CK(cudaMalloc(&scratch, sizeof(double) * 5 * (size_t)b->ntot));
-  CK(cudaMemsetAsync(scratch, 0, sizeof(double) * 5 * (size_t)b->ntot, c->stream));
+  CK(cudaMalloc(&scratch, sizeof(double) * 7 * (size_t)b->ntot));
+  CK(cudaMemsetAsync(scratch, 0, sizeof(double) * 7 * (size_t)b->ntot, c->stream));
   k_lusgs_coef<double><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, b->coef, 1);
   float best[2] = {0.f, 0.f};
   int rc = 0;
@@ -294,15 +351,19 @@ int tune_sweep(Ctx* c, BlockCtx* b) {
         attr[0].id = cudaLaunchAttributeClusterDimension;
         attr[0].val.clusterDim.x = b->lg.cs; attr[0].val.clusterDim.y = 1; attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr; cfg.numAttrs = 1;
-        e = cudaLaunchKernelEx(&cfg, k_lusgs_lines<double>, b->db, (const double*)b->coef, scratch, 1, b->lg);
+        e = b->prm.iturb >= 3
+                ? cudaLaunchKernelEx(&cfg, k_lusgs_lines<double, 7>, b->db, (const double*)b->coef, scratch, 1, b->lg)
+                : cudaLaunchKernelEx(&cfg, k_lusgs_lines<double, 5>, b->db, (const double*)b->coef, scratch, 1, b->lg);
       } else {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(b->coop_blocks); cfg.blockDim = dim3(256); cfg.stream = c->stream;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeCooperative; attr[0].val.cooperative = 1;
         cfg.attrs = attr; cfg.numAttrs = 1;
-        e = cudaLaunchKernelEx(&cfg, k_lusgs_sweep<double>, b->db, (const double*)b->coef, scratch, 1,
-                               c->d_bar, c->d_err);
+        e = b->prm.iturb >= 3 ? cudaLaunchKernelEx(&cfg, k_lusgs_sweep<double, 7>, b->db, (const double*)b->coef,
+                                                   scratch, 1, c->d_bar, c->d_err)
+                              : cudaLaunchKernelEx(&cfg, k_lusgs_sweep<double, 5>, b->db, (const double*)b->coef,
+                                                   scratch, 1, c->d_bar, c->d_err);
       }
       if (e != cudaSuccess) { rc = fail(c, FF_ERR_CUDA, "sweep autotune launch", e); break; }
       cudaEventRecord(c->ev1, c->stream);
@@ -328,8 +389,14 @@ int sweep(Ctx* c, BlockCtx* b, int upper, bool fp32) {
 int st_imps(Ctx* c, BlockCtx* b, int level, bool divide_cp) {
   int ncell = b->imax * b->jmax * b->kmax;
   double cfl = level == 1 ? b->prm.cfl : b->prm.cfll;
-  k_time3_copr<<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, cfl);
-  c->nlaunch++;
+  if (b->prm.iturb >= 3) {   // TIME3, then LOCDTK + IMSOKO + COPRKE
+    k_time3_copr<<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, cfl, 1);
+    k_locdtk_imsoko_coprke<<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm);
+    c->nlaunch += 2;
+  } else {
+    k_time3_copr<<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, cfl);
+    c->nlaunch++;
+  }
   bool fp32 = b->prm.lusgs_fp32 != 0;
   int rc;
   if (!fp32) {
@@ -340,7 +407,7 @@ int st_imps(Ctx* c, BlockCtx* b, int level, bool divide_cp) {
     c->nlaunch++;
     if ((rc = sweep(c, b, 0, false))) return rc;
   } else {
-    k_copy_dw<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->dw32, 1);
+    k_copy_dw<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->dw32, 1, b->prm.iturb >= 3 ? 7 : 5);
     c->nlaunch++;
     k_lusgs_coef<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, b->coef32, 1);
     c->nlaunch++;
@@ -348,13 +415,13 @@ int st_imps(Ctx* c, BlockCtx* b, int level, bool divide_cp) {
     k_lusgs_coef<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, b->coef32, 0);
     c->nlaunch++;
     if ((rc = sweep(c, b, 0, true))) return rc;
-    k_copy_dw<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->dw32, 0);
+    k_copy_dw<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->dw32, 0, b->prm.iturb >= 3 ? 7 : 5);
     c->nlaunch++;
   }
   if (divide_cp) {
     // standalone IMPS: finish with DRO/CP (imps3.f:483); the fused cycle
     // folds this division into the FIN kernel instead
-    k_fin_divide<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db);
+    k_fin_divide<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db, b->prm.iturb >= 3);
     c->nlaunch++;
   }
   return 0;
@@ -368,8 +435,12 @@ int st_fin(Ctx* c, BlockCtx* b, int divide_cp) {
 
 int one_cycle(Ctx* c, BlockCtx* b, int icycle) {
   int rc;
+  const bool sst = b->prm.iturb >= 3;
   k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi, c->d_dromax);
   c->nlaunch++;
+  // STATIM at the start of CYCLES: after the previous BOUNDI it only matters
+  // where SUBIN capped k (E includes k)
+  if (sst && (rc = st_statim(c, b, 1))) return rc;
   if ((rc = st_residu(c, b, 1, icycle))) return rc;
   int ncell = b->imax * b->jmax * b->kmax;
   k_resl2<<<min(nblk(ncell, 256), 4 * c->sm_count), 256, 0, c->stream>>>(b->db, c->d_resi);
@@ -377,6 +448,10 @@ int one_cycle(Ctx* c, BlockCtx* b, int icycle) {
   if ((rc = st_imps(c, b, 1, false))) return rc;
   if ((rc = st_fin(c, b, 1))) return rc;
   if ((rc = st_boundi(c, b))) return rc;
+  if (sst) {   // SUBIN: k cap, RKOLD / EPSOLD
+    k_subin_sst<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db, b->prm);
+    c->nlaunch++;
+  }
   k_record<<<1, 1, 0, c->stream>>>(c->d_resi, c->d_dromax, c->d_hist, c->d_hist_pos, c->hist_cap);
   c->nlaunch++;
   return 0;
@@ -557,6 +632,7 @@ int mb_cycle(Ctx* c, int icycle) {
   rc = fork_join(c, nb, [&](int n) {
     BlockCtx* b = c->blocks[n];
     int r;
+    if (b->prm.iturb >= 3 && (r = st_statim(c, b, 1))) return r;
     if ((r = st_residu(c, b, 1, icycle))) return r;
     int ncell = b->imax * b->jmax * b->kmax;
     k_resl2<<<min(nblk(ncell, 256), 4 * c->sm_count), 256, 0, c->stream>>>(b->db, c->d_resi);
@@ -566,6 +642,11 @@ int mb_cycle(Ctx* c, int icycle) {
   });
   if (rc) return rc;
   if ((rc = mb_boundi(c))) return rc;
+  for (auto* b : c->blocks)
+    if (b->prm.iturb >= 3) {
+      k_subin_sst<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db, b->prm);
+      c->nlaunch++;
+    }
   k_record<<<1, 1, 0, c->stream>>>(c->d_resi, c->d_dromax, c->d_hist, c->d_hist_pos, c->hist_cap);
   c->nlaunch++;
   return 0;
@@ -686,6 +767,7 @@ int ff_destroy(void* ctx) {
   for (auto* b : c->blocks) {
     if (b->graph) cudaGraphExecDestroy(b->graph);
     cudaFree(b->base); cudaFree(b->d_patch); cudaFree(b->coef); cudaFree(b->coef32); cudaFree(b->dw32);
+    cudaFree(b->d_red);
     delete b;
   }
   drop_phase_graphs(c);
@@ -726,15 +808,23 @@ int ff_block_add(void* ctx, int imax, int jmax, int kmax, int npatch, const ff_p
   }
   CK(cudaMalloc(&b->coef, sizeof(double) * NCOEF * (size_t)b->ntot));
   CK(cudaMalloc(&b->coef32, sizeof(float) * NCOEF * (size_t)b->ntot));
-  CK(cudaMalloc(&b->dw32, sizeof(float) * 5 * (size_t)b->ntot));
+  CK(cudaMalloc(&b->dw32, sizeof(float) * 7 * (size_t)b->ntot));
+  CK(cudaMalloc(&b->d_red, sizeof(unsigned long long) * 2));
   b->db.imax = imax; b->db.jmax = jmax; b->db.kmax = kmax;
   b->db.is = imax + 4; b->db.il = (imax + 4) * (jmax + 4); b->db.ntot = b->ntot;
   b->db.npatch = npatch; b->db.patch = b->d_patch;
   for (int s = 0; s < FF_NSLOTS; s++) b->db.a[s] = b->base + (size_t)s * b->slot_stride;
   // cooperative grid size: enough threads for the widest hyperplane
   int per_sm = 0, per_sm32 = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lusgs_sweep<double>, 256, 0));
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm32, k_lusgs_sweep<float>, 256, 0));
+  {   // the seven-equation instantiations use more registers: size for them
+    int a = 0, a7 = 0, f = 0, f7 = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_lusgs_sweep<double, 5>, 256, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a7, k_lusgs_sweep<double, 7>, 256, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&f, k_lusgs_sweep<float, 5>, 256, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&f7, k_lusgs_sweep<float, 7>, 256, 0));
+    per_sm = min(a, a7);
+    per_sm32 = min(f, f7);
+  }
   long widest = (long)jmax * kmax;
   b->coop_blocks = (int)min((long)per_sm * c->sm_count, max(1L, (widest + 255) / 256));
   b->coop_blocks32 = (int)min((long)per_sm32 * c->sm_count, max(1L, (widest + 255) / 256));
@@ -755,6 +845,8 @@ int ff_mg_link(void* ctx, int fine, int coarse) {
   BlockCtx *f = getb(c, fine), *cc = getb(c, coarse);
   if (!f || !cc || f == cc || f->imax != 2 * cc->imax || f->jmax != 2 * cc->jmax || f->kmax != 2 * cc->kmax)
     return fail(c, FF_ERR_ARG, "ff_mg_link: the coarse block must halve every dimension");
+  if (f->prm.iturb >= 3 || cc->prm.iturb >= 3)
+    return fail(c, FF_ERR_ARG, "ff_mg_link: multigrid with k-omega SST is not available");
   f->coarse = cc;
   cc->level = f->level + 1;
   if (f->graph) { cudaGraphExecDestroy(f->graph); f->graph = nullptr; }
@@ -765,7 +857,13 @@ int ff_block_params(void* ctx, int blk, const ff_params* prm) {
   Ctx* c = (Ctx*)ctx;
   BlockCtx* b = getb(c, blk);
   if (!b || !prm) return fail(c, FF_ERR_ARG, "ff_block_params");
+  bool nv_changed = (b->prm.iturb >= 3) != (prm->iturb >= 3);
   b->prm = *prm;
+  if (nv_changed) {   // the line sweep's shared memory depends on the equation count
+    int rc = setup_lines(c, b);
+    if (rc) return rc;
+    b->tuned = 0;
+  }
   // captured cycles of any block may include this one (multigrid levels)
   for (auto* x : c->blocks)
     if (x->graph) { cudaGraphExecDestroy(x->graph); x->graph = nullptr; }
@@ -815,7 +913,7 @@ int ff_statim(void* ctx, int blk) {
   Ctx* c = (Ctx*)ctx;
   BlockCtx* b = getb(c, blk);
   if (!b) return fail(c, FF_ERR_ARG, "ff_statim");
-  st_statim(c, b);
+  st_statim(c, b, 1);   // one STATIM call: equation of state + REFLEC
   CK(cudaGetLastError());
   return 0;
 }

@@ -35,7 +35,15 @@ FF_DI void state_cell(const DevBlock& b, const ff_params& p, size_t n) {
   double drdh = -ro / e / p.gamma;
   double u = b.a[FF_U][n], v = b.a[FF_V][n], w = b.a[FF_W][n];
   double rkin = (u * u + v * v + w * w) * .5;
-  double c = sqrt(dmax(1. / (drdh / ro + drdp), 1.0));
+  double c, rk = 0.;
+  if (p.iturb < 3) {
+    c = sqrt(dmax(1. / (drdh / ro + drdp), 1.0));
+  } else {   // CONSVA two-equation branch: k in the sound speed and E
+    rk = b.a[FF_RK][n];
+    double ypro = 1. / ro;
+    double xturb = 1. + (2. / 3.) * rk * ypro * drdp;
+    c = sqrt(dmax(xturb / (drdh * ypro + drdp), 1.0));
+  }
   a_P[n] = P;
   b.a[FF_DRDP][n] = drdp;
   b.a[FF_RO][n] = ro;
@@ -44,7 +52,7 @@ FF_DI void state_cell(const DevBlock& b, const ff_params& p, size_t n) {
   b.a[FF_CP][n] = cp2;
   b.a[FF_CH][n] = vis * cp2 / p.pr;
   b.a[FF_C][n] = c;
-  b.a[FF_E][n] = (e + rkin) * ro;
+  b.a[FF_E][n] = p.iturb < 3 ? (e + rkin) * ro : (e + rkin) * ro + rk;
   b.a[FF_RM][n] = ro * u;
   b.a[FF_RN][n] = ro * v;
   b.a[FF_RW][n] = ro * w;
@@ -122,6 +130,10 @@ __global__ void k_reflec(DevBlock b, ff_params p, int mode) {
   b.a[FF_RM][LB] = ro * u; b.a[FF_RN][LB] = ro * v; b.a[FF_RW][LB] = ro * w;
   b.a[FF_RM][LC] = ro * u; b.a[FF_RN][LC] = ro * v; b.a[FF_RW][LC] = ro * w;
   b.a[FF_E][LB] = b.a[FF_E][L]; b.a[FF_E][LC] = b.a[FF_E][L];
+  if (p.iturb >= 3) {   // turb3.f:5646-5658 (ITURB = 6)
+    b.a[FF_RK][LB] = -b.a[FF_RK][L];
+    b.a[FF_REPS][LB] = dmax(0., 2. * b.a[FF_REPS][L] - b.a[FF_REPS][LT]);
+  }
 }
 
 // REFCEN turb3.f:5881: linear extrapolation into the first wall ghost.
@@ -136,6 +148,11 @@ __global__ void k_refcen(DevBlock b, ff_params p) {
   const int sl[7] = {FF_E, FF_U, FF_V, FF_W, FF_RM, FF_RN, FF_RW};
 #pragma unroll
   for (int s = 0; s < 7; s++) { double* q = b.a[sl[s]]; q[LB] = 2. * q[L] - q[LT]; }
+  if (p.iturb >= 3) {   // turb3.f:6013-6027
+    double *RK = b.a[FF_RK], *RE = b.a[FF_REPS];
+    RK[LB] = dmax(p.rklim, 2. * RK[L] - 1. * RK[LT]);
+    RE[LB] = dmax(p.epslim, 2. * RE[L] - 1. * RE[LT]);
+  }
 }
 
 // INLET base3c.f:9223 (INLOUT 4) and OUTLET base3c.f:9595 (INLOUT 2, 3): the
@@ -165,9 +182,16 @@ __global__ void k_inlet_outlet(DevBlock b, ff_params p, int icycle) {
     U[IM1] = u1; V[IM1] = v1; W[IM1] = w1; U[IM2] = u2; V[IM2] = v2; W[IM2] = w2;
     E[IM1] = r1 * (e + .5 * (u1 * u1 + v1 * v1 + w1 * w1));
     E[IM2] = r2 * (e + .5 * (u2 * u2 + v2 * v2 + w2 * w2));
+    if (p.iturb >= 3) {   // base3c.f:9534-9541
+      b.a[FF_RK][IM1] = pa.bounrk; b.a[FF_RK][IM2] = pa.bounrk;
+      b.a[FF_REPS][IM1] = pa.bounep; b.a[FF_REPS][IM2] = pa.bounep;
+      E[IM1] = E[IM1] + pa.bounrk;
+      E[IM2] = E[IM2] + pa.bounrk;
+    }
     return;
   }
-  const double turlim = 1.e-6;   // FLUCYC's local TURLIM (res3c.f:7750)
+  // FLUCYC's local TURLIM (res3c.f:7750); FLXCYC passes the real one
+  const double turlim = p.iturb >= 3 ? p.turlim : 1.e-6;
   double rk3 = pa.ibtype == 2 ? 0.7 : 1.0, rk4 = pa.ibtype == 2 ? 0.3 : 0.0;
   const double* NX = b.a[FF_A1XA + 4 * (fg.dir - 1)];
   const double* NY = b.a[FF_A1YA + 4 * (fg.dir - 1)];
@@ -197,6 +221,13 @@ __global__ void k_inlet_outlet(DevBlock b, ff_params p, int icycle) {
     T[IM1] = pa.bount; T[IM2] = pa.bount;
     RO[IM1] = pa.bounr; RO[IM2] = pa.bounr;
   }
+  if (p.iturb >= 3 && -veloc * fg.idir > 0.) {   // base3c.f:10134-10146
+    double rk = b.a[FF_RK][II], re = b.a[FF_REPS][II];
+    b.a[FF_RK][IM1] = rk; b.a[FF_RK][IM2] = rk;
+    b.a[FF_REPS][IM1] = re; b.a[FF_REPS][IM2] = re;
+    E[IM1] = E[IM1] + rk;
+    E[IM2] = E[IM2] + rk;
+  }
 }
 
 // MIR ns3c.f:9003 -> MIRROR gluebm.f:3911 for symmetry patches.
@@ -220,9 +251,9 @@ __global__ void k_mir(DevBlock b) {
   U[IT2] = a11 * u2 + a12 * v2 + a13 * w2;
   V[IT2] = a12 * u2 + a22 * v2 + a23 * w2;
   W[IT2] = a13 * u2 + a23 * v2 + a33 * w2;
-  const int sc[6] = {FF_TEMP, FF_E, FF_P, FF_PDIFF, FF_EPS2, FF_VIST};
+  const int sc[8] = {FF_TEMP, FF_E, FF_P, FF_PDIFF, FF_EPS2, FF_VIST, FF_RK, FF_REPS};
 #pragma unroll
-  for (int s = 0; s < 6; s++) { double* q = b.a[sc[s]]; q[IT1] = q[IC1]; q[IT2] = q[IC2]; }
+  for (int s = 0; s < 8; s++) { double* q = b.a[sc[s]]; q[IT1] = q[IC1]; q[IT2] = q[IC2]; }
 }
 
 // REFCOR turb3.f:6040: ghost cells with two or three ghost indices copy the
@@ -237,10 +268,10 @@ __global__ void k_refcor(DevBlock b) {
   int jc = j < 1 ? 1 : (j > b.jmax ? b.jmax : j);
   int kc = k < 1 ? 1 : (k > b.kmax ? b.kmax : k);
   size_t src = ix(b, ic, jc, kc);
-  const int sl[18] = {FF_RO, FF_RM, FF_RN, FF_RW, FF_E, FF_U, FF_V, FF_W, FF_P, FF_PDIFF,
-                      FF_EPS2, FF_VIST, FF_TEMP, FF_VIS, FF_CH, FF_C, FF_DRDP, FF_DRDH};
+  const int sl[20] = {FF_RO, FF_RM, FF_RN, FF_RW, FF_E, FF_U, FF_V, FF_W, FF_P, FF_PDIFF,
+                      FF_EPS2, FF_VIST, FF_TEMP, FF_VIS, FF_CH, FF_C, FF_DRDP, FF_DRDH, FF_RK, FF_REPS};
 #pragma unroll
-  for (int s = 0; s < 18; s++) b.a[sl[s]][n] = b.a[sl[s]][src];
+  for (int s = 0; s < 20; s++) b.a[sl[s]][n] = b.a[sl[s]][src];
 }
 
 // DERFUN turb3.f:2476 + TEMDER turb3.f:3456 (IDERI = 1), interior + first
@@ -563,7 +594,8 @@ __global__ void k_resl2(DevBlock b, double* out) {
 }
 
 // TIME3 base3c.f:79 + LOCDT imps3.f:784 + COPR imps3.f:891 (interior cells).
-__global__ void k_time3_copr(DevBlock b, ff_params p, double cfl) {
+// mode 1: TIME3 only (the two-equation path converts in k_locdtk_imsoko_coprke).
+__global__ void k_time3_copr(DevBlock b, ff_params p, double cfl, int mode = 0) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= b.imax * b.jmax * b.kmax) return;
   int I = t % b.imax + 1, J = (t / b.imax) % b.jmax + 1, K = t / (b.imax * b.jmax) + 1;
@@ -598,6 +630,7 @@ __global__ void k_time3_copr(DevBlock b, ff_params p, double cfl) {
   double denmax = 1. + dmax(0., (ro - 2. * p.frsden) * ypro) * 5.;
   double dtl = 1. / (b11 * dmax(denlow, denmax));
   b.a[FF_DTL][kk] = dtl;
+  if (mode == 1) return;
   // LOCDT + COPR
   double dri = dtl * b.a[FF_DRO][kk], dmi = dtl * b.a[FF_DM][kk], dni = dtl * b.a[FF_DN][kk];
   double dwi = dtl * b.a[FF_DW][kk], dre = dtl * b.a[FF_DE][kk];
@@ -687,7 +720,7 @@ __global__ void k_lusgs_coef(DevBlock b, ff_params p, CT* coef, int upper) {
 // CORRGS: i-1, j-1, k-1), so the result equals its slab-by-slab order.
 // dw: increment arrays (5 x ntot) of type CT; read through L2 (__ldcg)
 // because other blocks write them during the sweep.
-template <typename CT>
+template <typename CT, int NV>
 __global__ void k_lusgs_sweep(DevBlock b, const CT* __restrict__ coef, CT* dw, int upper,
                               unsigned* bar, int* err) {
   const int IMAX = b.imax, JMAX = b.jmax, KMAX = b.kmax, IS = b.is, IL = b.il;
@@ -705,14 +738,17 @@ __global__ void k_lusgs_sweep(DevBlock b, const CT* __restrict__ coef, CT* dw, i
       size_t N = ix(b, I, J, K);
       CT dt1 = coef[9 * nt + N];
       CT vol = (CT)__ldg(b.a[FF_VOL] + N);
-      CT cd[5];
+      CT cd[NV];
       CT fd = upper ? CT(1) : coef[12 * nt + N];
 #pragma unroll
-      for (int v = 0; v < 5; v++) cd[v] = __ldcg(dw + v * nt + N) * fd;
+      for (int v = 0; v < NV; v++) cd[v] = __ldcg(dw + v * nt + N) * fd;
       // the three neighbours: k first (reference order), then i and j
-      CT ck[5] = {0, 0, 0, 0, 0}, yd[5] = {0, 0, 0, 0, 0}, bd[5] = {0, 0, 0, 0, 0};
+      CT ck[NV], yd[NV], bd[NV];
+#pragma unroll
+      for (int v = 0; v < NV; v++) { ck[v] = 0; yd[v] = 0; bd[v] = 0; }
       const int st[3] = {1, IS, IL};
-      const bool has[3] = {upper ? (I < IMAX && J < JMAX) : (I > 1), upper ? (J < JMAX) : (J > 1),
+      // PREDGS drops the i+1 coupling of row J = JMAX; PRKEGS does not
+      const bool has[3] = {upper ? (I < IMAX && (NV == 7 || J < JMAX)) : (I > 1), upper ? (J < JMAX) : (J > 1),
                            upper ? (K < KMAX) : (K > 1)};
 #pragma unroll
       for (int d = 2; d >= 0; d--) {
@@ -720,31 +756,31 @@ __global__ void k_lusgs_sweep(DevBlock b, const CT* __restrict__ coef, CT* dw, i
         size_t nb = upper ? N + st[d] : N - st[d];
         size_t fN = upper ? nb : N;              // shared face
         const int ao = 4 * d;
-        CT x[5];
+        CT x[NV];
 #pragma unroll
-        for (int v = 0; v < 5; v++) x[v] = __ldcg(dw + v * nt + nb);
-        CT out[5];
-        jac_product<CT>(out, x, (CT)__ldg(b.a[FF_C] + nb), (CT)__ldg(b.a[FF_RO] + nb),
-                        (CT)__ldg(b.a[FF_A1XA + ao] + fN), (CT)__ldg(b.a[FF_A1YA + ao] + fN),
-                        (CT)__ldg(b.a[FF_A1ZA + ao] + fN), coef[(3 * d) * nt + nb],
-                        coef[(3 * d + 1) * nt + nb], coef[(3 * d + 2) * nt + nb]);
+        for (int v = 0; v < NV; v++) x[v] = __ldcg(dw + v * nt + nb);
+        CT out[NV];
+        nb_product<CT, NV>(out, x, b, nb, (CT)__ldg(b.a[FF_C] + nb), (CT)__ldg(b.a[FF_RO] + nb),
+                           (CT)__ldg(b.a[FF_A1XA + ao] + fN), (CT)__ldg(b.a[FF_A1YA + ao] + fN),
+                           (CT)__ldg(b.a[FF_A1ZA + ao] + fN), coef[(3 * d) * nt + nb],
+                           coef[(3 * d + 1) * nt + nb], coef[(3 * d + 2) * nt + nb]);
         CT* dst = d == 2 ? ck : (d == 0 ? yd : bd);
 #pragma unroll
-        for (int v = 0; v < 5; v++) dst[v] = out[v];
+        for (int v = 0; v < NV; v++) dst[v] = out[v];
       }
       CT a3 = (CT)__ldg(b.a[FF_A3] + (upper ? N + IL : N));
       CT a1 = (CT)__ldg(b.a[FF_A1] + (upper ? N + 1 : N));
       CT a2 = (CT)__ldg(b.a[FF_A2] + (upper ? N + IS : N));
       CT scinv = coef[10 * nt + N], scinp = coef[11 * nt + N];
-      CT res[5];
+      CT res[NV];
 #pragma unroll
-      for (int v = 0; v < 5; v++) {
+      for (int v = 0; v < NV; v++) {
         CT x = upper ? (-dt1 * a3 * ck[v] + vol * cd[v]) : (dt1 * a3 * ck[v] + vol * cd[v]);
         x = upper ? x - dt1 * (a1 * yd[v] + a2 * bd[v]) : x + dt1 * (a1 * yd[v] + a2 * bd[v]);
-        res[v] = x * (v < 4 ? scinv : scinp);
+        res[v] = x * (v == 4 ? scinp : scinv);
       }
 #pragma unroll
-      for (int v = 0; v < 5; v++) __stcg(dw + v * nt + N, res[v]);
+      for (int v = 0; v < NV; v++) __stcg(dw + v * nt + N, res[v]);
     }
     if (!grid_barrier(bar, bar + 1, gridDim.x, err)) return;
   }
@@ -752,12 +788,12 @@ __global__ void k_lusgs_sweep(DevBlock b, const CT* __restrict__ coef, CT* dw, i
 
 // Copy between the FP64 increment arrays and a CT work copy (FP32 LU-SGS).
 template <typename CT>
-__global__ void k_copy_dw(DevBlock b, CT* dw, int to_work) {
+__global__ void k_copy_dw(DevBlock b, CT* dw, int to_work, int nv) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= b.imax * b.jmax * b.kmax) return;
   int I = t % b.imax + 1, J = (t / b.imax) % b.jmax + 1, K = t / (b.imax * b.jmax) + 1;
   size_t n = ix(b, I, J, K);
-  for (int v = 0; v < 5; v++) {
+  for (int v = 0; v < nv; v++) {
     if (to_work) dw[v * (size_t)b.ntot + n] = (CT)b.a[FF_DRO + v][n];
     else b.a[FF_DRO + v][n] = (double)dw[v * (size_t)b.ntot + n];
   }
@@ -774,9 +810,19 @@ __global__ void k_fin(DevBlock b, ff_params p, unsigned long long* dromax_bits, 
     bool kin = k >= 2 && k < b.kmax + 2, jin = j >= 2 && j < b.jmax + 2;
     bool interior = kin && jin && i >= 2 && i < b.imax + 2;
     double T = b.a[FF_TEMP][n], U = b.a[FF_U][n], V = b.a[FF_V][n], W = b.a[FF_W][n], PD = b.a[FF_PDIFF][n];
+    const bool sst = p.iturb >= 3;
     if (interior) {
       double dt = b.a[FF_DRO][n];
       if (divide_cp) { dt = dt / b.a[FF_CP][n]; b.a[FF_DRO][n] = dt; }
+      if (sst) {   // imps3.f:488-492, then FIN res3c.f:1190-1198
+        double ro = b.a[FF_RO][n], drk = b.a[FF_DRK][n], deps = b.a[FF_DEPS][n];
+        if (divide_cp) { drk = drk * ro; deps = deps * ro; b.a[FF_DRK][n] = drk; b.a[FF_DEPS][n] = deps; }
+        double rkold = b.a[FF_RKOLD][n], epold = b.a[FF_EPSOLD][n];
+        double rk = rkold + drk / (1. + fabs(drk) / (.45 * rkold));
+        double re = epold + deps / (1. + fabs(deps) / (.90 * epold));
+        b.a[FF_RK][n] = rk;
+        b.a[FF_REPS][n] = re;
+      }
       T = b.a[FF_TOLD][n] + dt;
       U = b.a[FF_UOLD][n] + b.a[FF_DM][n];
       V = b.a[FF_VOLD][n] + b.a[FF_DN][n];
@@ -793,6 +839,10 @@ __global__ void k_fin(DevBlock b, ff_params p, unsigned long long* dromax_bits, 
     P = P - prelim; PD = PD - prelim;
     b.a[FF_TEMP][n] = T; b.a[FF_U][n] = U; b.a[FF_V][n] = V; b.a[FF_W][n] = W;
     b.a[FF_PDIFF][n] = PD; b.a[FF_P][n] = P;
+    if (sst) {   // LOLIM of RK and REPS over every cell (FIN, then CYCLES)
+      b.a[FF_RK][n] = dmax(b.a[FF_RK][n], p.rklim);
+      b.a[FF_REPS][n] = dmax(b.a[FF_REPS][n], p.epslim);
+    }
     if (interior) {
       b.a[FF_TOLD][n] = T; b.a[FF_UOLD][n] = U; b.a[FF_VOLD][n] = V; b.a[FF_WOLD][n] = W;
       b.a[FF_POLD][n] = PD;
@@ -803,12 +853,17 @@ __global__ void k_fin(DevBlock b, ff_params p, unsigned long long* dromax_bits, 
 }
 
 // Standalone DRO/CP that ends IMPS (imps3.f:483) when it is called as a stage.
-__global__ void k_fin_divide(DevBlock b) {
+__global__ void k_fin_divide(DevBlock b, int sst) {
   size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= (size_t)b.ntot) return;
   int i = (int)(n % b.is), j = (int)((n / b.is) % (b.jmax + 4)), k = (int)(n / b.il);
-  if (i >= 2 && i < b.imax + 2 && j >= 2 && j < b.jmax + 2 && k >= 2 && k < b.kmax + 2)
+  if (i >= 2 && i < b.imax + 2 && j >= 2 && j < b.jmax + 2 && k >= 2 && k < b.kmax + 2) {
     b.a[FF_DRO][n] = b.a[FF_DRO][n] / b.a[FF_CP][n];
+    if (sst) {   // imps3.f:488-492
+      b.a[FF_DRK][n] = b.a[FF_DRK][n] * b.a[FF_RO][n];
+      b.a[FF_DEPS][n] = b.a[FF_DEPS][n] * b.a[FF_RO][n];
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -934,7 +989,7 @@ __global__ void k_fin_coarse(DevBlock b, ff_params p, int update) {
 // CONNEC ns3c.f:8605 (EXPTOT/IMPVO2 gluebm.f:6819/6964) for aligned 1:1
 // patches of all blocks in one launch: blockIdx.y = connection item; the two
 // interior layers of the source block fill the two ghost layers of the
-// destination patch (TEMP,U,V,W,E,EPS2,VIST,CH,P,PDIFF, as BOUNDI passes).
+// destination patch (TEMP,U,V,W,E,EPS2,VIST,CH,P,PDIFF,RK,REPS, as BOUNDI passes).
 struct ConnItem { int dst, src; ff_patch pa; };
 
 __global__ void k_connec(const DevBlock* __restrict__ blocks, const ConnItem* __restrict__ items) {
@@ -949,13 +1004,13 @@ __global__ void k_connec(const DevBlock* __restrict__ blocks, const ConnItem* __
   FaceG fd = face_g(d, pa.iface), fs = face_g(s, pa.nface);
   size_t L = face_cell(d, fd, a, c);
   size_t S = face_cell(s, fs, a - pa.r1a + pa.n1a, c - pa.r2a + pa.n2a);
-  const int vs[10] = {FF_TEMP, FF_U, FF_V, FF_W, FF_E, FF_EPS2, FF_VIST, FF_CH, FF_P, FF_PDIFF};
+  const int vs[12] = {FF_TEMP, FF_U, FF_V, FF_W, FF_E, FF_EPS2, FF_VIST, FF_CH, FF_P, FF_PDIFF, FF_RK, FF_REPS};
   int lsd = fd.idir * fd.s, lss = fs.idir * fs.s;
 #pragma unroll
   for (int g = 1; g <= 2; g++) {
     size_t G = L - g * lsd, Q = S + (g - 1) * lss;
 #pragma unroll
-    for (int v = 0; v < 10; v++) d.a[vs[v]][G] = s.a[vs[v]][Q];
+    for (int v = 0; v < 12; v++) d.a[vs[v]][G] = s.a[vs[v]][Q];
   }
 }
 
@@ -973,7 +1028,7 @@ __global__ void k_halo(const DevBlock* __restrict__ blocks, const HaloItem* __re
   if (t >= n) return;
   int a = t % n1, c = t / n1;
   const DevBlock& b = blocks[it.blk];
-  const int vs[10] = {FF_TEMP, FF_U, FF_V, FF_W, FF_E, FF_EPS2, FF_VIST, FF_CH, FF_P, FF_PDIFF};
+  const int vs[12] = {FF_TEMP, FF_U, FF_V, FF_W, FF_E, FF_EPS2, FF_VIST, FF_CH, FF_P, FF_PDIFF, FF_RK, FF_REPS};
   if (mode == 0) {
     FaceG fs = face_g(b, pa.nface);
     size_t S = face_cell(b, fs, a + pa.n1a, c + pa.n2a);
@@ -982,7 +1037,7 @@ __global__ void k_halo(const DevBlock* __restrict__ blocks, const HaloItem* __re
 #pragma unroll
     for (int g = 0; g < 2; g++)
 #pragma unroll
-      for (int v = 0; v < 10; v++) o[(size_t)(g * 10 + v) * n + t] = b.a[vs[v]][S + g * lss];
+      for (int v = 0; v < 12; v++) o[(size_t)(g * 12 + v) * n + t] = b.a[vs[v]][S + g * lss];
   } else {
     FaceG fd = face_g(b, pa.iface);
     size_t L = face_cell(b, fd, a + pa.r1a, c + pa.r2a);
@@ -991,7 +1046,7 @@ __global__ void k_halo(const DevBlock* __restrict__ blocks, const HaloItem* __re
 #pragma unroll
     for (int g = 0; g < 2; g++)
 #pragma unroll
-      for (int v = 0; v < 10; v++) b.a[vs[v]][L - (g + 1) * lsd] = o[(size_t)(g * 10 + v) * n + t];
+      for (int v = 0; v < 12; v++) b.a[vs[v]][L - (g + 1) * lsd] = o[(size_t)(g * 12 + v) * n + t];
   }
 }
 
@@ -1020,6 +1075,8 @@ __global__ void k_maxabs_de(DevBlock b, unsigned long long* dm_bits) {
   if ((threadIdx.x & 31) == 0 && amax > 0.) atomicMax(dm_bits, (unsigned long long)__double_as_longlong(amax));
 }
 
+#include "ff_sst.cuh"
+
 }  // namespace ff
 
 // ---------------------------------------------------------------------------
@@ -1044,21 +1101,21 @@ struct LineGeom {
   int ntj, ntk, ntiles, cs, tpc;   // tiles in j/k, cluster size, tiles per CTA
 };
 
-template <typename CT>
+template <typename CT, int NV>
 __global__ void __launch_bounds__(LTHREADS) k_lusgs_lines(DevBlock b, const CT* __restrict__ coef, CT* dw,
                                                           int upper, LineGeom lg) {
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  CT* pub = reinterpret_cast<CT*>(smem_raw);   // [2][tpc][10][LTHREADS]: bd(5), ck(5)
-  CT* ydb = pub + 2 * lg.tpc * 10 * LTHREADS;   // [tpc][5][LTHREADS]
+  CT* pub = reinterpret_cast<CT*>(smem_raw);        // [2][tpc][2*NV][LTHREADS]: bd(NV), ck(NV)
+  CT* ydb = pub + 2 * lg.tpc * 2 * NV * LTHREADS;   // [tpc][NV][LTHREADS]
   const int IMAX = b.imax, JMAX = b.jmax, KMAX = b.kmax, IS = b.is, IL = b.il;
   const size_t nt = b.ntot;
   const int rank = (int)cluster.block_rank();
   const int lane = threadIdx.x, lj = lane % LTJ, lk = lane / LTJ;
   const int nplanes = IMAX + JMAX + KMAX - 2;
   for (int q = 0; q < lg.tpc; q++)
-    for (int v = 0; v < 5; v++) ydb[(q * 5 + v) * LTHREADS + lane] = CT(0);
+    for (int v = 0; v < NV; v++) ydb[(q * NV + v) * LTHREADS + lane] = CT(0);
   cluster.sync();
   for (int s = 0; s < nplanes; s++) {
     const int m = upper ? IMAX + JMAX + KMAX - s : 3 + s;
@@ -1073,12 +1130,13 @@ __global__ void __launch_bounds__(LTHREADS) k_lusgs_lines(DevBlock b, const CT* 
       if (I < 1 || I > IMAX) continue;
       size_t N = ix(b, I, J, K);
       // ---- consume: neighbour contributions of the previous plane ----
-      CT yd[5], bd[5], ck[5];
-      bool hy = upper ? (I < IMAX && J < JMAX) : (I > 1);
+      CT yd[NV], bd[NV], ck[NV];
+      // PREDGS drops the i+1 coupling of row J = JMAX; PRKEGS does not
+      bool hy = upper ? (I < IMAX && (NV == 7 || J < JMAX)) : (I > 1);
       bool hj = upper ? (J < JMAX) : (J > 1);
       bool hk = upper ? (K < KMAX) : (K > 1);
 #pragma unroll
-      for (int v = 0; v < 5; v++) yd[v] = hy ? ydb[(q * 5 + v) * LTHREADS + lane] : CT(0);
+      for (int v = 0; v < NV; v++) yd[v] = hy ? ydb[(q * NV + v) * LTHREADS + lane] : CT(0);
       {
         int Jn = upper ? J + 1 : J - 1;       // line across the j face
         int Kn = upper ? K + 1 : K - 1;       // line across the k face
@@ -1089,20 +1147,20 @@ __global__ void __launch_bounds__(LTHREADS) k_lusgs_lines(DevBlock b, const CT* 
           src = cluster.map_shared_rank(pub, tn % lg.cs);
           int ln = lk * LTJ + ljn, qn = tn / lg.cs;
 #pragma unroll
-          for (int v = 0; v < 5; v++) bd[v] = src[((bin * lg.tpc + qn) * 10 + v) * LTHREADS + ln];
+          for (int v = 0; v < NV; v++) bd[v] = src[((bin * lg.tpc + qn) * 2 * NV + v) * LTHREADS + ln];
         } else {
 #pragma unroll
-          for (int v = 0; v < 5; v++) bd[v] = CT(0);
+          for (int v = 0; v < NV; v++) bd[v] = CT(0);
         }
         int tkn = (Kn - 1) / LTK, lkn = (Kn - 1) % LTK, tn2 = tkn * lg.ntj + tj;
         if (hk) {
           src = cluster.map_shared_rank(pub, tn2 % lg.cs);
           int ln = lkn * LTJ + lj, qn = tn2 / lg.cs;
 #pragma unroll
-          for (int v = 0; v < 5; v++) ck[v] = src[((bin * lg.tpc + qn) * 10 + 5 + v) * LTHREADS + ln];
+          for (int v = 0; v < NV; v++) ck[v] = src[((bin * lg.tpc + qn) * 2 * NV + NV + v) * LTHREADS + ln];
         } else {
 #pragma unroll
-          for (int v = 0; v < 5; v++) ck[v] = CT(0);
+          for (int v = 0; v < NV; v++) ck[v] = CT(0);
         }
       }
       // ---- solve the cell ----
@@ -1112,12 +1170,12 @@ __global__ void __launch_bounds__(LTHREADS) k_lusgs_lines(DevBlock b, const CT* 
       CT a3 = (CT)__ldg(b.a[FF_A3] + (upper ? N + IL : N));
       CT a1 = (CT)__ldg(b.a[FF_A1] + (upper ? N + 1 : N));
       CT a2 = (CT)__ldg(b.a[FF_A2] + (upper ? N + IS : N));
-      CT res[5];
+      CT res[NV];
 #pragma unroll
-      for (int v = 0; v < 5; v++) {
+      for (int v = 0; v < NV; v++) {
         CT x = upper ? (-dt1 * a3 * ck[v] + vol * (dw[v * nt + N] * fd)) : (dt1 * a3 * ck[v] + vol * (dw[v * nt + N] * fd));
         x = upper ? x - dt1 * (a1 * yd[v] + a2 * bd[v]) : x + dt1 * (a1 * yd[v] + a2 * bd[v]);
-        res[v] = x * (v < 4 ? scinv : scinp);
+        res[v] = x * (v == 4 ? scinp : scinv);
         dw[v * nt + N] = res[v];
       }
       // ---- produce: contributions to the three downstream neighbours ----
@@ -1127,16 +1185,16 @@ __global__ void __launch_bounds__(LTHREADS) k_lusgs_lines(DevBlock b, const CT* 
       for (int d = 0; d < 3; d++) {
         size_t fN = upper ? N : N + st[d];
         const int ao = 4 * d;
-        CT out[5];
-        jac_product<CT>(out, res, c, ro, (CT)__ldg(b.a[FF_A1XA + ao] + fN), (CT)__ldg(b.a[FF_A1YA + ao] + fN),
-                        (CT)__ldg(b.a[FF_A1ZA + ao] + fN), coef[(3 * d) * nt + N], coef[(3 * d + 1) * nt + N],
-                        coef[(3 * d + 2) * nt + N]);
+        CT out[NV];
+        nb_product<CT, NV>(out, res, b, N, c, ro, (CT)__ldg(b.a[FF_A1XA + ao] + fN),
+                           (CT)__ldg(b.a[FF_A1YA + ao] + fN), (CT)__ldg(b.a[FF_A1ZA + ao] + fN),
+                           coef[(3 * d) * nt + N], coef[(3 * d + 1) * nt + N], coef[(3 * d + 2) * nt + N]);
         if (d == 0) {
 #pragma unroll
-          for (int v = 0; v < 5; v++) ydb[(q * 5 + v) * LTHREADS + lane] = out[v];
+          for (int v = 0; v < NV; v++) ydb[(q * NV + v) * LTHREADS + lane] = out[v];
         } else {
 #pragma unroll
-          for (int v = 0; v < 5; v++) pub[((bout * lg.tpc + q) * 10 + (d == 1 ? 0 : 5) + v) * LTHREADS + lane] = out[v];
+          for (int v = 0; v < NV; v++) pub[((bout * lg.tpc + q) * 2 * NV + (d == 1 ? 0 : NV) + v) * LTHREADS + lane] = out[v];
         }
       }
     }

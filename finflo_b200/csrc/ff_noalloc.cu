@@ -49,7 +49,7 @@ int noalloc_setup(int dev) {
   if (cudaGetSymbolAddress(&p, ff_noalloc_scratch) != cudaSuccess || !p) return FF_ERR_CUDA;
   int sms = 0, per_sm = 0;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return FF_ERR_CUDA;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ff::k_lusgs_sweep<double>, 256, 0) != cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (ff::k_lusgs_sweep<double, 5>), 256, 0) != cudaSuccess ||
       per_sm < 1)
     return FF_ERR_CUDA;
   d.scratch = (double*)p;
@@ -65,6 +65,7 @@ extern "C" int ff_imps_noalloc(int imax, int jmax, int kmax, const ff_params* pr
                                double* const* slots, int level, void* stream) {
   if (imax < 2 || jmax < 2 || kmax < 1 || !prm || !slots || (level != 1 && level != 2 && level != 3))
     return FF_ERR_ARG;
+  if (prm->iturb >= 3) return FF_ERR_ARG;   // five-equation (laminar) implicit stage only
   long ntot = (long)(imax + 4) * (jmax + 4) * (kmax + 4);
   if (ntot > FF_NOALLOC_MAX_NTOT) return FF_ERR_SIZE;
   static const int needed[] = {FF_RO, FF_E, FF_P, FF_U, FF_V, FF_W, FF_C, FF_VIS, FF_CP, FF_DRDP, FF_DRDH,
@@ -114,10 +115,10 @@ extern "C" int ff_imps_noalloc(int imax, int jmax, int kmax, const ff_params* pr
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (cudaLaunchKernelEx(&cfg, k_lusgs_sweep<double>, db, (const double*)coef, dw, upper, bar, err) != cudaSuccess)
+    if (cudaLaunchKernelEx(&cfg, k_lusgs_sweep<double, 5>, db, (const double*)coef, dw, upper, bar, err) != cudaSuccess)
       return FF_ERR_CUDA;
   }
-  k_fin_divide<<<(int)((ntot + 255) / 256), 256, 0, st>>>(db);
+  k_fin_divide<<<(int)((ntot + 255) / 256), 256, 0, st>>>(db, 0);
   if (cudaGetLastError() != cudaSuccess) return FF_ERR_CUDA;
   return 0;
 }

@@ -1,0 +1,580 @@
+// k-omega SST (ITURB=6, KOVER=0, IDIS=2) on the device, level 1.
+//
+// The per-cycle steps of the reference's two-equation path: TURBEQ
+// (res3c.f:5845: DERFUN + EPS2KO turb3.f:7454), RESIKE (res3c.f:3423:
+// CROSKO turb3.f:7790, FUN1KO 7385, MAKE_EPS 7905, PRODKE 4687, TEMDER of k
+// and omega, FLXCYC res3c.f:6424 faces with FLKEBL base3c.f:5727, FLUXBL,
+// FLUXKE base3c.f:4753 and BOTSKE base3c.f:6147, SWEEPK 1342, SOURKO
+// turb3.f:7624, ADDSKE res3c.f:1473), the point-implicit and conversion
+// steps of IMPS (LOCDTK imps3.f:807, IMSOKO 972, COPRKE 1113) and the k cap
+// of SUBIN (ns3c.f:9742).  Included by ff_kernels.cuh inside namespace ff.
+
+// COEFKO turb3.f:8068 (ITURB=6, KOVER<5)
+constexpr double SST_A1KLEB = 0.31, SST_BSTAR = 0.09, SST_CKAPPA = 0.41, SST_BETA1 = 0.075;
+constexpr double SST_SIGRK1 = 0.85, SST_SIGOM1 = 0.5, SST_BETA2 = 0.0828, SST_SIGRK2 = 1.0,
+                 SST_SIGOM2 = 0.856;
+
+// ---- TURBEQ: EPS2KO with STRAIN (res3c.f:6338), interior cells ----------
+__global__ void k_eps2ko(DevBlock b, ff_params p) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= b.imax * b.jmax * b.kmax) return;
+  int I = t % b.imax + 1, J = (t / b.imax) % b.jmax + 1, K = t / (b.imax * b.jmax) + 1;
+  size_t L = ix(b, I, J, K);
+  const double eps = 1.e-20, frsmut = 1.e-3 * p.frsvis;
+  double ro = b.a[FF_RO][L], rk = b.a[FF_RK][L], rom = b.a[FF_REPS][L], dw = b.a[FF_DISTW][L];
+  double vis = b.a[FF_VIS][L], st = b.a[FF_STRAIN][L];
+  double prol = 1. / ro;
+  double rkl = dmax(rk * prol, 0.0);
+  double oml = rom * prol;
+  double dis2 = dw * dw;
+  double arg21 = 2. * sqrt(rkl) / dmax(eps, SST_BSTAR * oml * dw);
+  double auxvi = vis / dmax(eps, rom * dis2);
+  double arg2 = dmax(arg21, 500. * auxvi);
+  double arg4 = 150. * auxvi;
+  double fun2 = tanh(arg2 * arg2);
+  double fun3 = 1. - tanh(arg4 * arg4 * arg4 * arg4);
+  double rmubas = rk / oml;
+  double rmumen = SST_A1KLEB * rk / dmax(eps, st * fun2 * fun3);
+  double rmutrb = dmin(rmubas, rmumen);
+  rmutrb = dmax(rmutrb, frsmut);
+  rmutrb = dmin(rmutrb, p.turlim * vis);
+  b.a[FF_VIST][L] = rmutrb;
+  b.a[FF_EPS2][L] = 1.0 + rmutrb / vis;
+}
+
+// ---- CROSKO: cross diffusion into SEPS (interior).  k and omega of every
+// stencil cell are RK/RO and REPS/RO as the reference's in-place division
+// leaves them; k_rk_roundtrip then applies its RK = (RK/RO)*RO round trip.
+__global__ void k_crosko(DevBlock b) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= b.imax * b.jmax * b.kmax) return;
+  int I = t % b.imax + 1, J = (t / b.imax) % b.jmax + 1, K = t / (b.imax * b.jmax) + 1;
+  const int IS = b.is, IL = b.il;
+  size_t L = ix(b, I, J, K);
+  const double *RK = b.a[FF_RK], *RE = b.a[FF_REPS], *RO = b.a[FF_RO];
+#define KV(n) (RK[n] * (1. / RO[n]))
+#define OV(n) (RE[n] * (1. / RO[n]))
+#define LD(s, n) __ldg(b.a[s] + (n))
+  double k0 = KV(L), o0 = OV(L);
+  double rk1m = LD(FF_A1, L) * (k0 + KV(L - 1)), rk1p = LD(FF_A1, L + 1) * (k0 + KV(L + 1));
+  double om1m = LD(FF_A1, L) * (o0 + OV(L - 1)), om1p = LD(FF_A1, L + 1) * (o0 + OV(L + 1));
+  double rk2m = LD(FF_A2, L) * (k0 + KV(L - IS)), rk2p = LD(FF_A2, L + IS) * (k0 + KV(L + IS));
+  double om2m = LD(FF_A2, L) * (o0 + OV(L - IS)), om2p = LD(FF_A2, L + IS) * (o0 + OV(L + IS));
+  double rk3m = LD(FF_A3, L) * (k0 + KV(L - IL)), rk3p = LD(FF_A3, L + IL) * (k0 + KV(L + IL));
+  double om3m = LD(FF_A3, L) * (o0 + OV(L - IL)), om3p = LD(FF_A3, L + IL) * (o0 + OV(L + IL));
+  double pvol = 0.5 / LD(FF_VOL, L);
+#define CSUM(c, p3, m3, p2, m2, p1, m1)                                                                   \
+  (pvol * (LD(FF_A3##c, L + IL) * p3 - LD(FF_A3##c, L) * m3 + LD(FF_A2##c, L + IS) * p2 -               \
+           LD(FF_A2##c, L) * m2 + LD(FF_A1##c, L + 1) * p1 - LD(FF_A1##c, L) * m1))
+  double dkdx = CSUM(XA, rk3p, rk3m, rk2p, rk2m, rk1p, rk1m);
+  double dkdy = CSUM(YA, rk3p, rk3m, rk2p, rk2m, rk1p, rk1m);
+  double dkdz = CSUM(ZA, rk3p, rk3m, rk2p, rk2m, rk1p, rk1m);
+  double dodx = CSUM(XA, om3p, om3m, om2p, om2m, om1p, om1m);
+  double dody = CSUM(YA, om3p, om3m, om2p, om2m, om1p, om1m);
+  double dodz = CSUM(ZA, om3p, om3m, om2p, om2m, om1p, om1m);
+#undef CSUM
+#undef LD
+#undef KV
+#undef OV
+  double divdot = dkdx * dodx + dkdy * dody + dkdz * dodz;
+  b.a[FF_SEPS][L] = 2.0 * SST_SIGOM2 * RO[L] * divdot / o0;
+}
+
+__global__ void k_rk_roundtrip(DevBlock b) {
+  size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= (size_t)b.ntot) return;
+  double ro = b.a[FF_RO][n], prol = 1. / ro;
+  b.a[FF_RK][n] = (b.a[FF_RK][n] * prol) * ro;
+  b.a[FF_REPS][n] = (b.a[FF_REPS][n] * prol) * ro;
+}
+
+// CDMAX of FUN1KO: max(0, CROSSD) over the storage range from cell (1,1,1)
+// to (IMAX,JMAX,KMAX); non-negative doubles order like their bit patterns.
+__global__ void k_cdmax(DevBlock b, unsigned long long* out) {
+  size_t lbeg = ix(b, 1, 1, 1), lend = ix(b, b.imax, b.jmax, b.kmax);
+  double m = 0.;
+  for (size_t n = lbeg + (size_t)blockIdx.x * blockDim.x + threadIdx.x; n <= lend;
+       n += (size_t)gridDim.x * blockDim.x)
+    m = dmax(b.a[FF_SEPS][n], m);
+  for (int o = 16; o > 0; o >>= 1) m = dmax(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m > 0.) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+__global__ void k_fun1ko(DevBlock b, ff_params p, const unsigned long long* cdmax_bits) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= b.imax * b.jmax * b.kmax) return;
+  int I = t % b.imax + 1, J = (t / b.imax) % b.jmax + 1, K = t / (b.imax * b.jmax) + 1;
+  size_t L = ix(b, I, J, K);
+  const double eps = 1.e-20;
+  double cdmin = 1e-8 * __longlong_as_double((long long)*cdmax_bits);
+  double ro = b.a[FF_RO][L], rk = b.a[FF_RK][L], rom = b.a[FF_REPS][L], dw = b.a[FF_DISTW][L];
+  double prol = 1. / ro;
+  double rkl = dmax(rk * prol, 0.0);
+  double oml = rom * prol;
+  double dis2 = dw * dw;
+  double cdkom = dmax(b.a[FF_SEPS][L], cdmin);
+  double arg11 = sqrt(rkl) / dmax(eps, SST_BSTAR * oml * dw);
+  double arg12 = 500. * b.a[FF_VIS][L] / dmax(eps, rom * dis2);
+  double arg13 = dmax(arg11, arg12);
+  double arg14 = 4. * SST_SIGOM2 * rk / dmax(eps, cdkom * dis2);
+  double arg1 = dmin(arg13, arg14);
+  double f1 = tanh(arg1 * arg1 * arg1 * arg1);
+  if (dw < .40559E-7 * sqrt(p.re)) f1 = 1.;
+  b.a[FF_FUN1][L] = f1;
+}
+
+// MAKE_EPS + PRODKE (Kato-Launder): rows J = 1..JMAX of the interior
+// k-planes, i ghosts included, as the reference loops.
+__global__ void k_prodke(DevBlock b) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int per = b.jmax * b.is;
+  if (t >= per * b.kmax) return;
+  int K = t / per + 1, jj = t % per;
+  size_t L = (size_t)(K + 1) * b.il + 2 * b.is + jj;
+#define A(s) b.a[s][L]
+  double s11 = A(FF_S11), s12 = A(FF_S12), s13 = A(FF_S13), s22 = A(FF_S22), s23 = A(FF_S23), s33 = A(FF_S33);
+  double strain = s11 * s11 + s12 * s12 + s13 * s13 + s12 * s12 + s22 * s22 + s23 * s23 + s13 * s13 + s23 * s23 +
+                  s33 * s33;
+  strain = sqrt(2. * strain);
+  double trueps = 0.09 * A(FF_REPS) * A(FF_RK) / A(FF_RO);
+  double pt = (A(FF_EPS2) - 1.) * A(FF_VIS) * strain * A(FF_OHMI);
+  b.a[FF_PTUR][L] = dmin(pt, 20. * trueps);
+#undef A
+}
+
+// TEMDER of k = RK/RO and omega = REPS/RO (DIVV12 + TEMDER, res3c.f:3994-4006)
+// over the TEMDER range of level 1.
+__global__ void k_temder_ke(DevBlock b) {
+  int ni = b.imax + 2, nj = b.jmax + 2;
+  int klo = b.kmax > 1 ? 0 : 1, nk = b.kmax > 1 ? b.kmax + 2 : b.kmax;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ni * nj * nk) return;
+  int I = t % ni, J = (t / ni) % nj, K = t / (ni * nj) + klo;
+  const int IS = b.is, IL = b.il;
+  size_t L = ix(b, I, J, K);
+  const double *RO = b.a[FF_RO];
+#define LD(s, n) __ldg(b.a[s] + (n))
+  const size_t nb[6] = {L - 1, L + 1, L - (size_t)IS, L + IS, L - (size_t)IL, L + IL};
+  const int dslot[6] = {FF_D1, FF_D1, FF_D2, FF_D2, FF_D3, FF_D3};
+  double w1[6], w2[6];
+#pragma unroll
+  for (int q = 0; q < 6; q++) {
+    double dl = LD(dslot[q], L);
+    w1[q] = 2.0 * (dl / (dl + LD(dslot[q], nb[q])));
+    w2[q] = 2.0 - w1[q];
+  }
+  double pvol = .5 / LD(FF_VOL, L);
+#pragma unroll
+  for (int f = 0; f < 2; f++) {
+    const double* PH = b.a[f == 0 ? FF_RK : FF_REPS];
+    double ph0 = PH[L] / RO[L];
+    double t_[6];
+#pragma unroll
+    for (int q = 0; q < 6; q++) t_[q] = w2[q] * ph0 + w1[q] * (PH[nb[q]] / RO[nb[q]]);
+    // t_: 1m, 1p, 2m, 2p, 3m, 3p
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const int x1 = FF_A1XA + c, x2 = FF_A2XA + c, x3 = FF_A3XA + c;
+      double g = pvol * (LD(FF_A3, L + IL) * LD(x3, L + IL) * t_[5] - LD(FF_A3, L) * LD(x3, L) * t_[4] +
+                         LD(FF_A2, L + IS) * LD(x2, L + IS) * t_[3] - LD(FF_A2, L) * LD(x2, L) * t_[2] +
+                         LD(FF_A1, L + 1) * LD(x1, L + 1) * t_[1] - LD(FF_A1, L) * LD(x1, L) * t_[0]);
+      b.a[(f == 0 ? FF_DKDX : FF_DEDX) + c][L] = g;
+    }
+  }
+#undef LD
+}
+
+// ---- face fluxes of the seven equations ---------------------------------
+
+// FLUXKE base3c.f:4753-5120 with k and omega (UROT = 0); q[v][m], v = ro, u,
+// v, w, p, rk, reps; m = cells I-2S..I+S.  Adds to f[7].
+FF_DI void roe_flux_ke(const double q[7][4], double nx, double ny, double nz, double area, int intem,
+                       int intet, const ff_params& p, double c_r, double c_l, const double cr[4],
+                       const double cl2[4], double f[7]) {
+  double roip, roim, rmip, rmim, rnip, rnim, rwip, rwim, ppi, pmi, rkip, rkim, reip, reim;
+  xxtrap(q[0][0], q[0][1], q[0][2], q[0][3], intem, roip, roim);
+  xxtrap(q[1][0], q[1][1], q[1][2], q[1][3], intem, rmip, rmim);
+  xxtrap(q[2][0], q[2][1], q[2][2], q[2][3], intem, rnip, rnim);
+  xxtrap(q[3][0], q[3][1], q[3][2], q[3][3], intem, rwip, rwim);
+  xxtrap(q[4][0], q[4][1], q[4][2], q[4][3], intem, ppi, pmi);
+  xxtrap(q[5][0], q[5][1], q[5][2], q[5][3], intet, rkip, rkim);
+  xxtrap(q[6][0], q[6][1], q[6][2], q[6][3], intet, reip, reim);
+  roip = dmax(0.001 * p.frsden, roip);
+  ppi = dmax(0.001 * p.frspre, ppi);
+  roim = dmax(0.001 * p.frsden, roim);
+  pmi = dmax(0.001 * p.frspre, pmi);
+  const double gm1 = p.gamma - 1.;
+  double eip = ppi / (gm1 * roip) - p.e0ref;
+  double eim = pmi / (gm1 * roim) - p.e0ref;
+  double elr = ppi / (gm1 * roim) - p.e0ref;
+  double erl = pmi / (gm1 * roip) - p.e0ref;
+  double ypro1 = 1. / cr[2], ypro2 = 1. / cl2[2];
+  double dedph = 0.5 * ((-cr[0] / cr[1] - ypro1) + (-cl2[0] / cl2[1] - ypro2));
+  double dedrh = 0.5 * ((1. / cr[1] + cr[3] * (ypro1 * ypro1)) + (1. / cl2[1] + cl2[3] * (ypro2 * ypro2)));
+  {
+    double dpp = 2. * (ppi - pmi), drr = 2. * (roip - roim);
+    if (fabs(dpp) >= 1.e-2 * (ppi + pmi)) dedph = (eip + elr - eim - erl) / dpp;
+    if (fabs(drr) >= 1.e-2 * (roip + roim)) dedrh = (eip + erl - eim - elr) / drr;
+  }
+  double a21, a22, a23, a31, a32, a33;
+  surfvects(nx, ny, nz, a21, a22, a23, a31, a32, a33);
+  double ur = nx * rmip + ny * rnip + nz * rwip;
+  double vr = a21 * rmip + a22 * rnip + a23 * rwip;
+  double wr = a31 * rmip + a32 * rnip + a33 * rwip;
+  double ul = nx * rmim + ny * rnim + nz * rwim;
+  double vl = a21 * rmim + a22 * rnim + a23 * rwim;
+  double wl = a31 * rmim + a32 * rnim + a33 * rwim;
+  double rkipi = dmax(0.001 * p.rklim, rkip), reipi = dmax(0.001 * p.epslim, reip);
+  double rkimi = dmax(0.001 * p.rklim, rkim), reimi = dmax(0.001 * p.epslim, reim);
+  double ypror = 1. / roip, yprol = 1. / roim;
+  double rkr = rkipi * ypror, rkl = rkimi * yprol;
+  double eir = eip + .5 * (ur * ur + vr * vr + wr * wr) + rkr;
+  double eil = eim + .5 * (ul * ul + vl * vl + wl * wl) + rkl;
+  double pr = ppi, pl = pmi, pkr = .6667 * rkipi, pkl = .6667 * rkimi;
+  double epsr = reipi * ypror, epsl = reimi * yprol;
+  double hr = eir + pr * ypror, hl = eil + yprol * pl;
+  double rohat = sqrt(roip * roim), yproh = 1. / rohat;
+  double sqrl = 1. / (roim + rohat), cql = roim * sqrl, cqr = 1. - cql;
+  double uhat = cqr * ur + cql * ul, vhat = cqr * vr + cql * vl, what = cqr * wr + cql * wl;
+  double hhat = cqr * hr + cql * hl, ehat = cqr * eip + cql * eim;
+  double rkhat = cqr * rkr + cql * rkl, epshat = cqr * epsr + cql * epsl;
+  double phat = rohat * (hhat - ehat - .5 * (uhat * uhat + vhat * vhat + what * what) - rkhat);
+  phat = dmin(dmax(pr, pl), phat);
+  phat = dmax(dmin(pr, pl), phat);
+  double drdhh = 1. / (dedrh - phat * (yproh * yproh));
+  double drdph = -drdhh * (dedph + yproh);
+  double xturb = 1. + .6667 * rkhat * yproh * drdph;
+  double chat2 = xturb / (drdhh * yproh + drdph);
+  double cmin = dmin(c_r, c_l), cmax = dmax(c_r, c_l);
+  chat2 = dmin(cmax * cmax, chat2);
+  chat2 = dmax(cmin * cmin, chat2);
+  double chat = sqrt(chat2);
+  double pdpde = dedph;
+  double dro = roip - roim, du = ur - ul, dk = rkr - rkl;
+  double dp = pr - pl + .6667 * (rkhat * dro + rohat * dk);
+  double pchat2 = 1. / (chat * chat);
+  double alfa1 = .5 * (dp + rohat * chat * du) * pchat2;
+  double alfa2 = .5 * (dp - rohat * chat * du) * pchat2;
+  double alfa3 = dro - dp * pchat2;
+  double alfa4 = rohat * (vr - vl), alfa5 = rohat * (wr - wl), alfa6 = rohat * dk, alfa7 = rohat * (epsr - epsl);
+  double rl1h = uhat + chat, rl2h = uhat - chat, rl3h = uhat;
+  double rl1 = fabs(rl1h), rl2 = fabs(rl2h), rl3 = fabs(rl3h);
+  if (p.entropy_fix) {
+    double e22;
+    e22 = 4. * dmax(dmax(1.e-10, rl1h - (ul + c_l)), (ur + c_r) - rl1h);
+    if (rl1 <= e22) rl1 = .5 * (rl1h * rl1h + e22 * e22) / e22;
+    e22 = 4. * dmax(dmax(1.e-10, rl2h - (ul - c_l)), (ur - c_r) - rl2h);
+    if (rl2 <= e22) rl2 = .5 * (rl2h * rl2h + e22 * e22) / e22;
+    e22 = 4. * dmax(dmax(1.e-10, rl3h - ul), ur - rl3h);
+    if (rl3 <= e22) rl3 = .5 * (rl3h * rl3h + e22 * e22) / e22;
+  }
+  double roucr = roip * ur, roucl = roim * ul;
+  double damp = rl1 * alfa1 + rl2 * alfa2 + rl3 * alfa3;
+  double ha = .5 * area;
+  double f1 = ha * (roucr + roucl - damp);
+  double f2 = ha * (roucr * ur + pr + pkr + roucl * ul + pl + pkl - (damp * uhat + (rl1 * alfa1 - rl2 * alfa2) * chat));
+  double f3 = ha * (roucr * vr + roucl * vl - damp * vhat - rl3 * alfa4);
+  double f4 = ha * (roucr * wr + roucl * wl - damp * what - rl3 * alfa5);
+  double f5 = ha * (roucr * (hr + pkr * ypror) + roucl * (hl + pkl * yprol) - damp * hhat -
+                    ((rl1 * alfa1 - rl2 * alfa2) * uhat * chat - rl3 * alfa3 * rohat * (chat * chat) * pdpde +
+                     rl3 * alfa4 * vhat + rl3 * alfa5 * what) +
+                    rl3 * alfa6 * (1. - .6667 * rohat * pdpde));
+  double f6 = ha * (roucr * rkr + roucl * rkl - damp * rkhat - rl3 * alfa6);
+  double f7 = ha * (roucr * epsr + roucl * epsl - damp * epshat - rl3 * alfa7);
+  f[0] += f1;
+  f[1] += nx * f2 + a21 * f3 + a31 * f4;
+  f[2] += ny * f2 + a22 * f3 + a32 * f4;
+  f[3] += nz * f2 + a23 * f3 + a33 * f4;
+  f[4] += f5;
+  f[5] += f6;
+  f[6] += f7;
+}
+
+// FLKEBL: k and omega diffusion of one face (I = high-side cell).
+FF_DI void flkebl_face(const DevBlock& b, size_t I, int S, int dir, double& frk, double& feps) {
+#define LD(s, n) __ldg(b.a[s] + (n))
+  size_t M = I - S;
+  const int ao = 4 * (dir - 1);
+  double f1 = LD(FF_FUN1, I), onemf1 = dmax(0.0, 1.0 - f1);
+  double psigk = f1 * SST_SIGRK1 + onemf1 * SST_SIGRK2;
+  double psige = f1 * SST_SIGOM1 + onemf1 * SST_SIGOM2;
+  const double* D = b.a[FF_D1 + dir - 1];
+  double w1 = 2.0 * (__ldg(D + I) / (__ldg(D + I) + __ldg(D + M))), w2 = 2.0 - w1;
+  double dkdxi = 0.5 * (w2 * LD(FF_DKDX, I) + w1 * LD(FF_DKDX, M));
+  double dkdyi = 0.5 * (w2 * LD(FF_DKDY, I) + w1 * LD(FF_DKDY, M));
+  double dkdzi = 0.5 * (w2 * LD(FF_DKDZ, I) + w1 * LD(FF_DKDZ, M));
+  double dedxi = 0.5 * (w2 * LD(FF_DEDX, I) + w1 * LD(FF_DEDX, M));
+  double dedyi = 0.5 * (w2 * LD(FF_DEDY, I) + w1 * LD(FF_DEDY, M));
+  double dedzi = 0.5 * (w2 * LD(FF_DEDZ, I) + w1 * LD(FF_DEDZ, M));
+  double sxi = LD(FF_XC, I) - LD(FF_XC, M), syi = LD(FF_YC, I) - LD(FF_YC, M), szi = LD(FF_ZC, I) - LD(FF_ZC, M);
+  double slen = sqrt(sxi * sxi + syi * syi + szi * szi) + 1.E-21;
+  sxi = sxi / slen; syi = syi / slen; szi = szi / slen;
+  double nx = LD(FF_A1XA + ao, I), ny = LD(FF_A1YA + ao, I), nz = LD(FF_A1ZA + ao, I);
+  double alfa = dmax(sxi * nx + syi * ny + szi * nz, 0.);
+  double rmut2 = LD(FF_VIST, I) + LD(FF_VIST, M);
+  double vv = LD(FF_VIS, I) + LD(FF_VIS, M), area = LD(FF_A1 + ao, I);
+  double surfk = 0.5 * area * (vv + rmut2 * psigk);
+  double surfep = 0.5 * area * (vv + rmut2 * psige);
+  double ypro1 = 1. / LD(FF_RO, I), ypro2 = 1. / LD(FF_RO, M);
+  frk = -surfk * (alfa * (LD(FF_RK, I) * ypro1 - LD(FF_RK, M) * ypro2) / slen + dkdxi * (nx - alfa * sxi) +
+                  dkdyi * (ny - alfa * syi) + dkdzi * (nz - alfa * szi));
+  feps = -surfep * (alfa * (LD(FF_REPS, I) * ypro1 - LD(FF_REPS, M) * ypro2) / slen + dedxi * (nx - alfa * sxi) +
+                    dedyi * (ny - alfa * syi) + dedzi * (nz - alfa * szi));
+#undef LD
+}
+
+// BOTSKE with k and omega (smooth wall, IDIS=2): seven wall fluxes.
+FF_DI void wall_flux_ke(const DevBlock& b, const ff_params& p, size_t II, int S, int idir, int dir, int iheat,
+                        int intem, double f[7]) {
+#define LD(s, n) __ldg(b.a[s] + (n))
+  double rc1 = intem == 6 ? 1. : 1.5, rc2 = rc1 - 1.;
+  const double prs = p.pr / p.prt, ymr = .166666667, eps = 1.e-3;
+  int lstrid = S * idir;
+  size_t II2 = II + lstrid, IF1 = idir == 1 ? II : II + S;
+  int ihfl = (iheat == 2 || iheat >= 12) ? 1 : 0;
+  int iht = (iheat == 0 || iheat == 15) ? 0 : 1;
+  const int ao = 4 * (dir - 1);
+  double a_f = LD(FF_A1 + ao, IF1);
+  double dist = (a_f + LD(FF_A1 + ao, IF1 + lstrid)) / LD(FF_VOL, II);
+  double surg = -dist * ymr;
+  double visb = dmax(0.01 * p.frsvis, rc1 * LD(FF_VIS, II) - rc2 * LD(FF_VIS, II2));
+  double chsb = dmax(eps, rc1 * LD(FF_CH, II) - rc2 * LD(FF_CH, II2));
+  double straib = dmax(eps, rc1 * LD(FF_STRAIN, II) - rc2 * LD(FF_STRAIN, II2));
+  double pb1 = dmax(0.01 * p.frspre, rc1 * LD(FF_P, II) - rc2 * LD(FF_P, II2));
+  double rob = dmax(0.001 * p.frsden, rc1 * LD(FF_RO, II) - rc2 * LD(FF_RO, II2));
+  double surf = surg * visb;
+  double surfe = surg * (prs * 0. / visb + 1.) * chsb;
+  double rapub = 1.0E-20;
+  double surfrk = surg * (1.0 + SST_SIGRK1 * rapub) * visb;
+  double surfep = surg * (1.0 + SST_SIGOM1 * rapub) * visb;
+  double ypro1 = 1. / LD(FF_RO, II), ypro2 = 1. / LD(FF_RO, II2);
+  double rnub = visb / rob;
+  double plusfc = sqrt(rnub * straib) / rnub;
+  double yplus1 = 2.0 * plusfc / dist;
+  double skpmin = dmax(dmin(2.4 * pow(yplus1, 0.85), 8.0), 1.e-3);
+  double skplus = dmax(0.0 * plusfc, skpmin);
+  double pskp = 1.0 / skplus;
+  double omsurf = straib * dmax(2500.0 * pskp * pskp, 100.0 * pskp);
+  double tempb = dmax(0.01 * p.frstem, rc1 * LD(FF_TEMP, II) - rc2 * LD(FF_TEMP, II2));
+  double tsurf = iheat == 3 ? tempb : p.frstem;
+  double cvii = iht * idir * (9.000 * LD(FF_TEMP, II) - 1.000 * LD(FF_TEMP, II2) - 8. * tsurf);
+  double uvii = idir * (9.000 * LD(FF_U, II) - 1.000 * LD(FF_U, II2));
+  double vvii = idir * (9.000 * LD(FF_V, II) - 1.000 * LD(FF_V, II2));
+  double wvii = idir * (9.000 * LD(FF_W, II) - 1.000 * LD(FF_W, II2));
+  double ax = LD(FF_A1XA + ao, IF1), ay = LD(FF_A1YA + ao, IF1), az = LD(FF_A1ZA + ao, IF1);
+  double duc = .33333 * (ay * vvii + az * wvii + ax * uvii);
+  double f2v = surf * (uvii + ax * duc);
+  double f3v = surf * (vvii + ay * duc);
+  double f4v = surf * (wvii + az * duc);
+  double f5v = (1 - ihfl) * surfe * cvii;
+  double evii = idir * (9.0 * LD(FF_REPS, II) * ypro1 - 1.0 * LD(FF_REPS, II2) * ypro2 - 8. * omsurf);
+  double rkii = idir * (9.000 * LD(FF_RK, II) * ypro1 - 1.000 * LD(FF_RK, II2) * ypro2);
+  rkii = idir * dmax(idir * rkii, 0.0);
+  double f6v = surfrk * rkii;
+  double f7v = surfep * evii;
+  f[0] = 0.;
+  f[1] = a_f * (ax * pb1 + f2v);
+  f[2] = a_f * (ay * pb1 + f3v);
+  f[3] = a_f * (az * pb1 + f4v);
+  f[4] = a_f * (f5v + f6v);
+  f[5] = a_f * f6v;
+  f[6] = a_f * f7v;
+#undef LD
+}
+
+// Flux of one face with k and omega (FLXCYC order: FLKEBL, SETV12, FLUXBL,
+// FLUXKE; BOTSKE on walls).
+FF_DI void face_flux_ke(const DevBlock& b, const ff_params& p, int dir, size_t L, int m, int t1, int t2,
+                        double f[7]) {
+  const int S = dir == 1 ? 1 : (dir == 2 ? b.is : b.il);
+  const int nmax = dir == 1 ? b.imax : (dir == 2 ? b.jmax : b.kmax);
+  int intem = dir == 1 ? p.interi : (dir == 2 ? p.interj : p.interk);
+  int intet = (intem > -5 && intem < 5) ? 1 : intem;
+  if (m == 1 || m == nmax + 1) {
+    int iface = m == 1 ? dir : dir + 3;
+    for (int ip = 0; ip < b.npatch; ip++) {
+      const ff_patch& pa = b.patch[ip];
+      if (pa.iface != iface || pa.ityp < 8 || pa.ityp > 10) continue;
+      if (t1 < pa.r1a || t1 > pa.r1b || t2 < pa.r2a || t2 > pa.r2b) continue;
+      int idir = m == 1 ? 1 : -1;
+      size_t II = m == 1 ? L : L - S;
+      wall_flux_ke(b, p, II, S, idir, dir, pa.iheat, intem, f);
+      return;
+    }
+  }
+  const int idi = dir == 1 ? p.idi1 : (dir == 2 ? p.idi2 : p.idi3);
+#pragma unroll
+  for (int v = 0; v < 7; v++) f[v] = 0.;
+  if (m <= min(idi, nmax + 1)) {
+    double frk, feps, fv[5];
+    flkebl_face(b, L, S, dir, frk, feps);
+    visc_flux(b, p, L, S, dir, fv);
+    f[1] = fv[1]; f[2] = fv[2]; f[3] = fv[3];
+    f[4] = frk + fv[4];
+    f[5] = frk; f[6] = feps;
+  }
+  double q[7][4];
+  const int sl[7] = {FF_RO, FF_U, FF_V, FF_W, FF_P, FF_RK, FF_REPS};
+#pragma unroll
+  for (int v = 0; v < 7; v++) {
+    const double* a = b.a[sl[v]];
+    q[v][0] = __ldg(a + L - 2 * S); q[v][1] = __ldg(a + L - S); q[v][2] = __ldg(a + L); q[v][3] = __ldg(a + L + S);
+  }
+  size_t L2 = dir == 3 ? L : L - S;
+  double cr[4] = {__ldg(b.a[FF_DRDP] + L), __ldg(b.a[FF_DRDH] + L), q[0][2], q[4][2]};
+  double cl[4] = {__ldg(b.a[FF_DRDP] + L2), __ldg(b.a[FF_DRDH] + L2), __ldg(b.a[FF_RO] + L2), __ldg(b.a[FF_P] + L2)};
+  const int ao = 4 * (dir - 1);
+  roe_flux_ke(q, __ldg(b.a[FF_A1XA + ao] + L), __ldg(b.a[FF_A1YA + ao] + L), __ldg(b.a[FF_A1ZA + ao] + L),
+              __ldg(b.a[FF_A1 + ao] + L), intem, intet, p, __ldg(b.a[FF_C] + L), __ldg(b.a[FF_C] + L - S), cr, cl, f);
+}
+
+// RESIKE face cycles + SWEEPK for a 32x4x4 tile (k, i, j, then 1/VOL).
+__global__ void __launch_bounds__(128) k_residual_sst(DevBlock b, ff_params p) {
+  __shared__ double sF[7][TI * (TJ + 1) * TK];
+  const int tid = threadIdx.x;
+  const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ, k0 = blockIdx.z * TK;
+  const int ci = tid % TI, cj = tid / TI;
+  double acc[TK][7];
+#pragma unroll
+  for (int c = 0; c < TK; c++)
+#pragma unroll
+    for (int v = 0; v < 7; v++) acc[c][v] = 0.;
+  for (int f = tid; f < TI * TJ * (TK + 1); f += blockDim.x) {
+    int fi = f % TI, fj = (f / TI) % TJ, fk = f / (TI * TJ);
+    int I = i0 + fi + 1, J = j0 + fj + 1, m = k0 + fk + 1;
+    if (I > b.imax || J > b.jmax || m > b.kmax + 1) continue;
+    double fl[7];
+    face_flux_ke(b, p, 3, ix(b, I, J, m), m, I, J, fl);
+#pragma unroll
+    for (int v = 0; v < 7; v++) sF[v][f] = fl[v];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int c = 0; c < TK; c++) {
+    int f0 = ci + TI * (cj + TJ * c), f1 = ci + TI * (cj + TJ * (c + 1));
+    if (i0 + ci < b.imax && j0 + cj < b.jmax && k0 + c < b.kmax)
+#pragma unroll
+      for (int v = 0; v < 7; v++) acc[c][v] = acc[c][v] - (sF[v][f1] - sF[v][f0]);
+  }
+  __syncthreads();
+  for (int f = tid; f < (TI + 1) * TJ * TK; f += blockDim.x) {
+    int fi = f % (TI + 1), fj = (f / (TI + 1)) % TJ, fk = f / ((TI + 1) * TJ);
+    int m = i0 + fi + 1, J = j0 + fj + 1, K = k0 + fk + 1;
+    if (m > b.imax + 1 || J > b.jmax || K > b.kmax) continue;
+    double fl[7];
+    face_flux_ke(b, p, 1, ix(b, m, J, K), m, J, K, fl);
+#pragma unroll
+    for (int v = 0; v < 7; v++) sF[v][f] = fl[v];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int c = 0; c < TK; c++) {
+    int f0 = ci + (TI + 1) * (cj + TJ * c);
+    if (i0 + ci < b.imax && j0 + cj < b.jmax && k0 + c < b.kmax)
+#pragma unroll
+      for (int v = 0; v < 7; v++) acc[c][v] = acc[c][v] - (sF[v][f0 + 1] - sF[v][f0]);
+  }
+  __syncthreads();
+  for (int f = tid; f < TI * (TJ + 1) * TK; f += blockDim.x) {
+    int fi = f % TI, fj = (f / TI) % (TJ + 1), fk = f / (TI * (TJ + 1));
+    int I = i0 + fi + 1, m = j0 + fj + 1, K = k0 + fk + 1;
+    if (I > b.imax || m > b.jmax + 1 || K > b.kmax) continue;
+    double fl[7];
+    face_flux_ke(b, p, 2, ix(b, I, m, K), m, I, K, fl);
+#pragma unroll
+    for (int v = 0; v < 7; v++) sF[v][f] = fl[v];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int c = 0; c < TK; c++) {
+    int I = i0 + ci + 1, J = j0 + cj + 1, K = k0 + c + 1;
+    if (I > b.imax || J > b.jmax || K > b.kmax) continue;
+    int f0 = ci + TI * (cj + (TJ + 1) * c), f1 = ci + TI * (cj + 1 + (TJ + 1) * c);
+    size_t n = ix(b, I, J, K);
+    double rv = 1. / __ldg(b.a[FF_VOL] + n);
+#pragma unroll
+    for (int v = 0; v < 7; v++) b.a[FF_DRO + v][n] = (acc[c][v] - (sF[v][f1] - sF[v][f0])) * rv;
+  }
+}
+
+// SOURKO (KOVER=0, RANS, no rotation correction) + ADDSKE, interior cells.
+__global__ void k_sourko_addske(DevBlock b) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= b.imax * b.jmax * b.kmax) return;
+  int I = t % b.imax + 1, J = (t / b.imax) % b.jmax + 1, K = t / (b.imax * b.jmax) + 1;
+  size_t L = ix(b, I, J, K);
+  const double pbstar = 1.0 / SST_BSTAR, persbs = 1.0 / sqrt(SST_BSTAR), eps = 1.0E-10;
+  double f1 = b.a[FF_FUN1][L], onemf1 = dmax(0.0, 1.0 - f1);
+  double beta = f1 * SST_BETA1 + onemf1 * SST_BETA2;
+  double sigom = f1 * SST_SIGOM1 + onemf1 * SST_SIGOM2;
+  double gamkom = beta * pbstar - sigom * (SST_CKAPPA * SST_CKAPPA) * persbs;
+  double rmutrb = dmax(eps, b.a[FF_EPS2][L] - 1.0) * b.a[FF_VIS][L];
+  double ro = b.a[FF_RO][L], rom = b.a[FF_REPS][L], pt = b.a[FF_PTUR][L];
+  double prol = 1.0 / ro;
+  double som = onemf1 * b.a[FF_SEPS][L];
+  double srk = pt - SST_BSTAR * b.a[FF_RK][L] * rom * prol;
+  double omepro = gamkom * ro * pt / (rmutrb * rom);
+  double omedis = 1.0 * beta * prol * rom;
+  som = som + rom * (omepro - omedis);
+  b.a[FF_SRK][L] = srk;
+  b.a[FF_SEPS][L] = som;
+  b.a[FF_DRK][L] = b.a[FF_DRK][L] + srk;
+  b.a[FF_DEPS][L] = b.a[FF_DEPS][L] + som;
+}
+
+// LOCDTK (DTURB=1) + IMSOKO + COPRKE, after TIME3 wrote DTL (interior).
+__global__ void k_locdtk_imsoko_coprke(DevBlock b, ff_params p) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= b.imax * b.jmax * b.kmax) return;
+  int I = t % b.imax + 1, J = (t / b.imax) % b.jmax + 1, K = t / (b.imax * b.jmax) + 1;
+  size_t i = ix(b, I, J, K);
+  double dtl = b.a[FF_DTL][i];
+  double dri = dtl * b.a[FF_DRO][i], dmi = dtl * b.a[FF_DM][i], dni = dtl * b.a[FF_DN][i];
+  double dwi = dtl * b.a[FF_DW][i], dre = dtl * b.a[FF_DE][i];
+  double drk = 1. * dtl * b.a[FF_DRK][i], deps = 1. * dtl * b.a[FF_DEPS][i];
+  // IMSOKO imps3.f:972
+  const double gamkom = SST_BETA1 / SST_BSTAR - SST_SIGOM1 * (SST_CKAPPA * SST_CKAPPA) / sqrt(SST_BSTAR);
+  const double ckmax = 1.0 / (2.0 * p.csimps), eps = 1.0E-10;
+  double E = b.a[FF_E][i], rk = b.a[FF_RK][i], rom = b.a[FF_REPS][i], ro = b.a[FF_RO][i];
+  double emeanf = E - rk;
+  double drkmax = dmax(ckmax * dmin(rk, fabs(0.1 * emeanf - 0.9 * rk)), eps);
+  double dommax = ckmax * rom;
+  double prol = 1. / ro;
+  double atprod = fabs(b.a[FF_PTUR][i]);
+  double rnutrb = dmax(b.a[FF_EPS2][i] - 1.0, eps) * b.a[FF_VIS][i] * prol;
+  double drkden = 1.0 + dtl * (atprod / drkmax + prol * SST_BSTAR * rom);
+  double domden = 1.0 + dtl * (gamkom * atprod / (rnutrb * dommax) + 2. * SST_BETA1 * rom);
+  drk = drk / drkden;
+  deps = deps / domden;
+  // COPRKE imps3.f:1113
+  double u = b.a[FF_U][i], v = b.a[FF_V][i], w = b.a[FF_W][i];
+  double vel2 = u * u + v * v + w * w;
+  double drodh = b.a[FF_DRDH][i], drodp = b.a[FF_DRDP][i];
+  double ypro = 1. / ro, rki = rk * ypro;
+  double dkin = u * dmi + v * dni + w * dwi + drk;
+  b.a[FF_DM][i] = ypro * (-u * dri + dmi);
+  b.a[FF_DN][i] = ypro * (-v * dri + dni);
+  b.a[FF_DW][i] = ypro * (-w * dri + dwi);
+  b.a[FF_DRK][i] = ypro * (-rki * dri + drk);
+  b.a[FF_DEPS][i] = ypro * (-rom * ypro * dri + deps);
+  double hi = ypro * (E + b.a[FF_P][i]);
+  double dei = dre - (hi - vel2 - rki) * dri - dkin;
+  double c = b.a[FF_C][i];
+  double dpi = c * c * (dri - drodh * ypro * dei);
+  b.a[FF_DRO][i] = (dri - drodp * dpi) / drodh;
+  b.a[FF_DE][i] = dpi + .667 * drk;
+}
+
+// SUBIN for SST: the k cap (RKMAX = FRSDEN*FRSVEL^2) and RKOLD/EPSOLD over
+// all cells.
+__global__ void k_subin_sst(DevBlock b, ff_params p) {
+  size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= (size_t)b.ntot) return;
+  double rkmax = .5 * p.frsden * p.frsvel * p.frsvel * 2.;
+  double rk = b.a[FF_RK][n];
+  rk = dmin(rk, dmax(0.1 * b.a[FF_E][n], rkmax));
+  rk = dmin(rk, rkmax);
+  b.a[FF_RK][n] = rk;
+  b.a[FF_RKOLD][n] = rk;
+  b.a[FF_EPSOLD][n] = b.a[FF_REPS][n];
+}

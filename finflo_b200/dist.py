@@ -9,7 +9,7 @@ summed over processes for the convergence monitor.  Here:
   loaded rank), so each GPU holds whole blocks in its HBM;
 * ``HaloPlan`` lists, per peer rank, the remote patches in one canonical
   order that both sides derive from the global block list, with the offsets
-  of their packed ghost data ([layer][var][cell], 20 doubles per patch cell);
+  of their packed ghost data ([layer][var][cell], 24 doubles per patch cell);
 * ``DistributedBlocks`` drives one cycle as: device phase A (CYCLES of the
   local blocks, BOUNDI part one, local CONNEC, halo pack) -> one grouped
   send/recv per peer (NCCL over NVLink, or gloo on CPU) -> phase B (unpack,
@@ -32,7 +32,7 @@ from .case import Block, FFHaloItem, FFPatch
 from . import grid
 
 PHASE_CYCLE_A, PHASE_BOUNDI_A, PHASE_B, PHASE_RECORD = 0, 1, 2, 3
-HALO_VARS = 10
+HALO_VARS = 12
 HALO_LAYERS = 2
 
 

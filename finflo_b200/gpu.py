@@ -269,6 +269,10 @@ class GpuSolver:
     def _old_copies(self, bid):
         blk = self.blocks[bid][0]
         st = self.download(bid, ["TEMP", "U", "V", "W", "PDIFF"])
-        for a, b2 in (("TOLD", "TEMP"), ("UOLD", "U"), ("VOLD", "V"), ("WOLD", "W"), ("POLD", "PDIFF")):
+        pairs = [("TOLD", "TEMP"), ("UOLD", "U"), ("VOLD", "V"), ("WOLD", "W"), ("POLD", "PDIFF")]
+        if self.blocks[bid][1].iturb >= 3:
+            pairs += [("RKOLD", "RK"), ("EPSOLD", "REPS")]
+            st.update(self.download(bid, ["RK", "REPS"]))
+        for a, b2 in pairs:
             blk.arrays[a][:] = st[b2]
-        self.upload(bid, ["TOLD", "UOLD", "VOLD", "WOLD", "POLD"])
+        self.upload(bid, [a for a, _ in pairs])

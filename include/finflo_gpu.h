@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define FF_ABI_VERSION 1
+#define FF_ABI_VERSION 2
 
 enum { FF_OK = 0, FF_ERR_CUDA = 1, FF_ERR_ARG = 2, FF_ERR_TIMEOUT = 3, FF_ERR_SIZE = 4 };
 enum { FF_STAGE_RESIDUAL = 1, FF_STAGE_GRAD = 2, FF_STAGE_STATE = 3 };
@@ -61,6 +61,12 @@ int ff_resl2(void *ctx, int blk, double *out5);
 int ff_imps(void *ctx, int blk, int level);
 int ff_fin(void *ctx, int blk, double *dromax);
 
+/* With ff_params.iturb = 6 (k-omega SST, single grid level) ff_residu is
+ * TURBEQ res3c.f:5845 + RESIKE res3c.f:3423, ff_imps the seven-equation
+ * IMPS (LOCDTK, IMSOKO, COPRKE, PRKEGS/DIKEGS/COKEGS) and ff_fin also
+ * updates RK, REPS; ff_cycles adds the cycle-start STATIM and the k cap of
+ * SUBIN.  ff_mg_link refuses SST blocks. */
+
 /* ncycles full cycles (RESIDU, RESL2, IMPS, FIN, BOUNDI, SUBIN); hist
  * (nullable) receives ncycles x {RESI(31..35) sums of squares, DROMAX}. */
 int ff_cycles(void *ctx, int blk, int ncycles, int icycle0, double *hist, int use_graph);
@@ -78,7 +84,8 @@ int ff_cycles(void *ctx, int blk, int ncycles, int icycle0, double *hist, int us
  * FF_ERR_SIZE with nothing queued.  The first call on a device resolves the
  * array's device address; make that first call before any stream capture.
  * Calls share the array, so calls that overlap on the GPU race: serialise
- * them (one stream, or events).  Asynchronous on `stream` (a cudaStream_t). */
+ * them (one stream, or events).  Laminar (five-equation) blocks only:
+ * prm->iturb >= 3 gives FF_ERR_ARG.  Asynchronous on `stream` (a cudaStream_t). */
 #define FF_NOALLOC_MAX_NTOT 98304
 int ff_imps_noalloc(int imax, int jmax, int kmax, const ff_params *prm,
                     double *const *slots, int level, void *stream);

@@ -36,6 +36,8 @@ typedef struct ff_patch {
   int n1a, n2a;  /* start of the matching range in the neighbour face (CON)   */
   /* BOUNR/BOUNU/BOUNV/BOUNW/BOUNT/BOUNP/BOUNPD, uniform over the patch       */
   double bounr, bounu, bounv, bounw, bount, bounp, bounpd;
+  /* BOUNRK/BOUNEP: inlet rho*k and rho*omega (two-equation models)          */
+  double bounrk, bounep;
 } ff_patch;
 
 /* Flow, gas and solver constants (defaults: main.f:5234-5440, 3499, 3827). */
@@ -50,9 +52,14 @@ typedef struct ff_params {
   double pvisc;                         /* PVISC = 1.8 (imps3.f:110)          */
   double tlolim, tuplim;                /* 0.05*FRSTEM, 6*FRSTEM              */
   double cmgk, cmgeps;                  /* 0.1, 0.2 (main.f:5343-5344)        */
+  /* two-equation (k-omega SST) constants, main.f:3770-3830, 5338-5346      */
+  double rklim, epslim;                 /* free-stream rho*k, rho*omega        */
+  double turlim;                        /* mu_t / mu cap (5000)               */
+  double csimps;                        /* point-implicit source factor (5)   */
+  double re;                            /* Reynolds number (FUN1KO DISLIM)    */
   int interi, interj, interk;           /* XXTRAP INTEM per direction         */
   int entropy_fix;                      /* ENTROPY_FIX (0 default)            */
-  int iturb;                            /* 0 laminar (6 SST: next)            */
+  int iturb;                            /* 0 laminar, 6 k-omega SST (KOVER=0) */
   int fullns;                           /* 1: FLUXBL on level 1, else FLUXDO  */
   int idi1, idi2, idi3;                 /* viscous extents IDI1..3 (nodes)    */
   int coarse_inter;                     /* INTEM on coarse levels (55)        */
@@ -68,7 +75,7 @@ enum ff_slot {
   FF_RO, FF_RM, FF_RN, FF_RW, FF_E, FF_P, FF_PDIFF, FF_U, FF_V, FF_W, FF_C,
   FF_TEMP, FF_VIS, FF_CH, FF_CP, FF_DRDP, FF_DRDH, FF_EPS2, FF_VIST,
   /* residual / increments (RESIDU -> IMPS -> FIN) and local time step */
-  FF_DRO, FF_DM, FF_DN, FF_DW, FF_DE, FF_DTL,
+  FF_DRO, FF_DM, FF_DN, FF_DW, FF_DE, FF_DRK, FF_DEPS, FF_DTL,
   /* values at the start of the cycle (SUBIN ns3c.f:9742) */
   FF_TOLD, FF_UOLD, FF_VOLD, FF_WOLD, FF_POLD,
   /* metrics */
@@ -82,6 +89,13 @@ enum ff_slot {
   FF_F1R, FF_F1RM, FF_F1RN, FF_F1RW, FF_F1E,
   /* multigrid forcing P2H (TRANSF/FORCFU, multi.f:156, 1609) */
   FF_ROP2H, FF_RMP2H, FF_RNP2H, FF_RWP2H, FF_EP2H,
+  /* two-equation model: rho*k, rho*omega, wall distance (DISTW), blending
+   * F1 (FUN1), sources SRK/SEPS, production PTUR, gradients of k and omega
+   * (GRADK/GREPS), their start-of-cycle copies and face fluxes (F1RK,
+   * F1EPS), multigrid forcing of k and omega */
+  FF_RK, FF_REPS, FF_DISTW, FF_FUN1, FF_SRK, FF_SEPS, FF_PTUR,
+  FF_DKDX, FF_DKDY, FF_DKDZ, FF_DEDX, FF_DEDY, FF_DEDZ,
+  FF_RKOLD, FF_EPSOLD, FF_F1RK, FF_F1EPS, FF_RKP2H, FF_EPP2H,
   FF_NSLOTS
 };
 

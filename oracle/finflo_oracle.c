@@ -42,7 +42,7 @@ int orc_version(void) { return 1; }
 
 /* ---------------------------------------------------------------------- */
 /* STATIM (ns3c.f:10318): PDTOP state.f:1690, PERFGA state.f:159 (EXPSU=1.5 */
-/* branch, IUPPTL=0), CONSVA base3c.f:489 (ITURB<3 branch), REFLEC          */
+/* branch, IUPPTL=0), CONSVA base3c.f:489 (ITURB<3 and two-equation), REFLEC*/
 /* turb3.f:5294 (solid walls and the inlet-pressure extrapolation).         */
 /* ---------------------------------------------------------------------- */
 static void state_cells(orc_block *b, const ff_params *p) {
@@ -52,6 +52,7 @@ static void state_cells(orc_block *b, const ff_params *p) {
   double *DRDP = b->a[FF_DRDP], *DRDH = b->a[FF_DRDH], *C = b->a[FF_C];
   double *U = b->a[FF_U], *V = b->a[FF_V], *W = b->a[FF_W];
   double *RM = b->a[FF_RM], *RN = b->a[FF_RN], *RW = b->a[FF_RW];
+  const double *RK = b->a[FF_RK];
   const double gm1 = p->gamma - 1.0, cp2 = p->gamma / gm1 * p->rgas;
   for (int n = 0; n < d.ntot; n++) {
     P[n] = PD[n] + p->frspre;                      /* PDTOP, g = 0 */
@@ -64,8 +65,15 @@ static void state_cells(orc_block *b, const ff_params *p) {
     CP[n] = cp2;
     CH[n] = VIS[n] * cp2 / p->pr;
     double rkin = (U[n] * U[n] + V[n] * V[n] + W[n] * W[n]) * .5;   /* CONSVA */
-    C[n] = sqrt(MAXD(1.0 / (DRDH[n] / RO[n] + DRDP[n]), 1.0));
-    E[n] = (E[n] + rkin + 0.0) * RO[n];
+    if (p->iturb < 3) {
+      C[n] = sqrt(MAXD(1.0 / (DRDH[n] / RO[n] + DRDP[n]), 1.0));
+      E[n] = (E[n] + rkin + 0.0) * RO[n];
+    } else {                                        /* two-equation branch */
+      double ypro = 1. / RO[n];
+      double xturb = 1. + (2. / 3.) * RK[n] * ypro * DRDP[n];
+      C[n] = sqrt(MAXD(xturb / (DRDH[n] * ypro + DRDP[n]), 1.0));
+      E[n] = (E[n] + rkin + 0.0) * RO[n] + RK[n];
+    }
     RM[n] = RO[n] * U[n];
     RN[n] = RO[n] * V[n];
     RW[n] = RO[n] * W[n];
@@ -139,6 +147,11 @@ static void reflec(orc_block *b, const ff_params *p) {
         E[LB] = E[L];
         RM[LC] = RM[LB]; RN[LC] = RN[LB]; RW[LC] = RW[LB]; E[LC] = E[LB];
         EPS2[LC] = EPS2[LB]; VIST[LC] = VIST[LB]; PD[LC] = PD[LB]; P[LC] = P[LB]; RO[LC] = RO[LB];
+        if (p->iturb >= 3) {                        /* turb3.f:5646-5658, ITURB=6 */
+          double *RK = b->a[FF_RK], *REPS = b->a[FF_REPS];
+          RK[LB] = -RK[L];
+          REPS[LB] = MAXD(0., 2. * REPS[L] - REPS[LT]);
+        }
       }
   }
 }
@@ -186,6 +199,15 @@ void orc_refcen(orc_block *b, const ff_params *p) {
         RN[LB] = 2. * RN[L] - RN[LT];
         RW[LB] = 2. * RW[L] - RW[LT];
       }
+    if (p->iturb >= 3) {                            /* turb3.f:6013-6027 */
+      double *RK = b->a[FF_RK], *REPS = b->a[FF_REPS];
+      for (int bb = pa->r2a; bb <= pa->r2b; bb++)
+        for (int a = pa->r1a; a <= pa->r1b; a++) {
+          size_t L = face_cell(&d, &f, a, bb), LB = L - ls, LT = L + ls;
+          RK[LB] = MAXD(p->rklim, 2. * RK[L] - 1. * RK[LT]);
+          REPS[LB] = MAXD(p->epslim, 2. * REPS[L] - 1. * REPS[LT]);
+        }
+    }
   }
 }
 
@@ -298,7 +320,9 @@ void orc_inlet_outlet(orc_block *b, const ff_params *p, int dir, int icycle) {
   double *RO = b->a[FF_RO], *P = b->a[FF_P], *PD = b->a[FF_PDIFF], *E = b->a[FF_E];
   double *RM = b->a[FF_RM], *RN = b->a[FF_RN], *RW = b->a[FF_RW];
   double *EPS2 = b->a[FF_EPS2], *VIST = b->a[FF_VIST], *VIS = b->a[FF_VIS];
-  const double turlim = 1.e-6;
+  double *RK = b->a[FF_RK], *REPS = b->a[FF_REPS];
+  /* FLUCYC's local TURLIM (res3c.f:7750); FLXCYC passes the real one */
+  const double turlim = p->iturb >= 3 ? p->turlim : 1.e-6;
   for (int ip = 0; ip < b->npatch; ip++) {
     const ff_patch *pa = &b->patch[ip];
     face_t f = face_geom(&d, pa->iface);
@@ -335,6 +359,12 @@ void orc_inlet_outlet(orc_block *b, const ff_params *p, int dir, int icycle) {
           W[IM1] = RW[IM1] / RO[IM1]; W[IM2] = RW[IM2] / RO[IM2];
           E[IM1] = RO[IM1] * (E[IM1] + .5 * (U[IM1] * U[IM1] + V[IM1] * V[IM1] + W[IM1] * W[IM1]));
           E[IM2] = RO[IM2] * (E[IM2] + .5 * (U[IM2] * U[IM2] + V[IM2] * V[IM2] + W[IM2] * W[IM2]));
+          if (p->iturb >= 3) {                      /* base3c.f:9534-9541 */
+            RK[IM1] = pa->bounrk; RK[IM2] = RK[IM1];
+            REPS[IM1] = pa->bounep; REPS[IM2] = REPS[IM1];
+            E[IM1] = E[IM1] + RK[IM1];
+            E[IM2] = E[IM2] + RK[IM2];
+          }
         } else if (out && (pa->ibtype == 2 || pa->ibtype == 3)) {
           double rk3 = pa->ibtype == 2 ? 0.7 : 1.0, rk4 = pa->ibtype == 2 ? 0.3 : 0.0;
           double a11 = AX[IF1], a12 = AY[IF1], a13 = AZ[IF1], a21, a22, a23, a31, a32, a33;
@@ -375,6 +405,12 @@ void orc_inlet_outlet(orc_block *b, const ff_params *p, int dir, int icycle) {
             EPS2[IM1] = EPS2[IM2]; VIST[IM1] = VIST[IM2];
             T[IM1] = pa->bount; T[IM2] = T[IM1];
             RO[IM1] = pa->bounr; RO[IM2] = RO[IM1];
+          }
+          if (p->iturb >= 3 && -veloc * f.idir > 0.) {   /* base3c.f:10134-10146 */
+            RK[IM1] = 1. * RK[II] + 0. * RK[II2]; RK[IM2] = RK[IM1];
+            REPS[IM1] = 1. * REPS[II] + 0. * REPS[II2]; REPS[IM2] = REPS[IM1];
+            E[IM1] = E[IM1] + RK[IM1];
+            E[IM2] = E[IM2] + RK[IM2];
           }
         }
       }
@@ -1229,7 +1265,8 @@ void orc_fin_limits(orc_block *b, const ff_params *p) {
 void orc_refcor(orc_block *b) {
   dims_t d = dims_of(b);
   static const int slots[] = {FF_RO, FF_RM, FF_RN, FF_RW, FF_E, FF_U, FF_V, FF_W, FF_P, FF_PDIFF,
-                              FF_EPS2, FF_VIST, FF_TEMP, FF_VIS, FF_CH, FF_C, FF_DRDP, FF_DRDH};
+                              FF_EPS2, FF_VIST, FF_TEMP, FF_VIS, FF_CH, FF_C, FF_DRDP, FF_DRDH,
+                              FF_RK, FF_REPS};
   for (int K = -1; K <= d.kmax + 2; K++)
     for (int J = -1; J <= d.jmax + 2; J++)
       for (int I = -1; I <= d.imax + 2; I++) {
@@ -1271,8 +1308,8 @@ void orc_mir(orc_block *b) {
         U[IT2] = a11 * u2 + a12 * v2 + a13 * w2;
         V[IT2] = a21 * u2 + a22 * v2 + a23 * w2;
         W[IT2] = a31 * u2 + a32 * v2 + a33 * w2;
-        static const int sc[] = {FF_TEMP, FF_E, FF_P, FF_PDIFF, FF_EPS2, FF_VIST};
-        for (int s = 0; s < 6; s++) {
+        static const int sc[] = {FF_TEMP, FF_E, FF_P, FF_PDIFF, FF_EPS2, FF_VIST, FF_RK, FF_REPS};
+        for (int s = 0; s < 8; s++) {   /* RK, REPS: gluebm.f:4104-4125 */
           b->a[sc[s]][IT1] = b->a[sc[s]][IC1];
           b->a[sc[s]][IT2] = b->a[sc[s]][IC2];
         }
@@ -1495,7 +1532,8 @@ void orc_mg_cycle(orc_block **lv, int nlev, const ff_params *prm, int icycle, do
  * the RO position and U,V,W in RM,RN,RW (ns3c.f:10900), so the exchanged
  * variables are TEMP,U,V,W,E,EPS2,VIST,CH,P,PDIFF. */
 void orc_connec_patch(orc_block *dst, const ff_patch *pa, const orc_block *src) {
-  static const int vs[10] = {FF_TEMP, FF_U, FF_V, FF_W, FF_E, FF_EPS2, FF_VIST, FF_CH, FF_P, FF_PDIFF};
+  static const int vs[12] = {FF_TEMP, FF_U, FF_V, FF_W, FF_E, FF_EPS2, FF_VIST, FF_CH, FF_P, FF_PDIFF,
+                             FF_RK, FF_REPS};
   dims_t dd = dims_of(dst), ds = dims_of((orc_block *)src);
   face_t fd = face_geom(&dd, pa->iface), fs = face_geom(&ds, pa->nface);
   int lsd = fd.idir * fd.s, lss = fs.idir * fs.s;
@@ -1505,7 +1543,7 @@ void orc_connec_patch(orc_block *dst, const ff_patch *pa, const orc_block *src) 
       size_t S = face_cell(&ds, &fs, a - pa->r1a + pa->n1a, bb - pa->r2a + pa->n2a);
       for (int g = 1; g <= 2; g++) {
         size_t G = L - g * lsd, Q = S + (g - 1) * lss;
-        for (int v = 0; v < 10; v++) dst->a[vs[v]][G] = src->a[vs[v]][Q];
+        for (int v = 0; v < 12; v++) dst->a[vs[v]][G] = src->a[vs[v]][Q];
       }
     }
 }
@@ -1556,7 +1594,8 @@ void orc_mb_cycle(orc_block **blk, int nblk, const ff_params *prm, int icycle, d
  * their unpacking into the destination ghosts; together they equal
  * orc_connec_patch. */
 void orc_halo_pack(const orc_block *src, const ff_patch *pa, double *out) {
-  static const int vs[10] = {FF_TEMP, FF_U, FF_V, FF_W, FF_E, FF_EPS2, FF_VIST, FF_CH, FF_P, FF_PDIFF};
+  static const int vs[12] = {FF_TEMP, FF_U, FF_V, FF_W, FF_E, FF_EPS2, FF_VIST, FF_CH, FF_P, FF_PDIFF,
+                             FF_RK, FF_REPS};
   dims_t ds = dims_of((orc_block *)src);
   face_t fs = face_geom(&ds, pa->nface);
   int lss = fs.idir * fs.s;
@@ -1565,12 +1604,13 @@ void orc_halo_pack(const orc_block *src, const ff_patch *pa, double *out) {
     for (int a = 0; a < n1; a++) {
       size_t S = face_cell(&ds, &fs, a + pa->n1a, c + pa->n2a);
       for (int g = 0; g < 2; g++)
-        for (int v = 0; v < 10; v++) out[(size_t)(g * 10 + v) * n + c * n1 + a] = src->a[vs[v]][S + g * lss];
+        for (int v = 0; v < 12; v++) out[(size_t)(g * 12 + v) * n + c * n1 + a] = src->a[vs[v]][S + g * lss];
     }
 }
 
 void orc_halo_unpack(orc_block *dst, const ff_patch *pa, const double *in) {
-  static const int vs[10] = {FF_TEMP, FF_U, FF_V, FF_W, FF_E, FF_EPS2, FF_VIST, FF_CH, FF_P, FF_PDIFF};
+  static const int vs[12] = {FF_TEMP, FF_U, FF_V, FF_W, FF_E, FF_EPS2, FF_VIST, FF_CH, FF_P, FF_PDIFF,
+                             FF_RK, FF_REPS};
   dims_t dd = dims_of(dst);
   face_t fd = face_geom(&dd, pa->iface);
   int lsd = fd.idir * fd.s;
@@ -1579,6 +1619,8 @@ void orc_halo_unpack(orc_block *dst, const ff_patch *pa, const double *in) {
     for (int a = 0; a < n1; a++) {
       size_t L = face_cell(&dd, &fd, a + pa->r1a, c + pa->r2a);
       for (int g = 0; g < 2; g++)
-        for (int v = 0; v < 10; v++) dst->a[vs[v]][L - (g + 1) * lsd] = in[(size_t)(g * 10 + v) * n + c * n1 + a];
+        for (int v = 0; v < 12; v++) dst->a[vs[v]][L - (g + 1) * lsd] = in[(size_t)(g * 12 + v) * n + c * n1 + a];
     }
 }
+
+#include "finflo_oracle_sst.c"

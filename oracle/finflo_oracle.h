@@ -53,6 +53,14 @@ void orc_fin_coarse(orc_block *b, const ff_params *p);
 void orc_interp_limits(orc_block *c, orc_block *f, const ff_params *pf);
 void orc_connec_patch(orc_block *dst, const ff_patch *pa, const orc_block *src);
 void orc_connec(orc_block **blk, int nblk);
+/* k-omega SST (ITURB=6), single grid level: finflo_oracle_sst.c */
+void orc_turbeq_sst(orc_block *b, const ff_params *p);
+void orc_residu_sst(orc_block *b, const ff_params *p, int icycle);
+void orc_flux_dir_sst(orc_block *b, const ff_params *p, int dir);
+void orc_imps_sst(orc_block *b, const ff_params *p);
+void orc_fin_limits_sst(orc_block *b, const ff_params *p);
+void orc_subin_sst(orc_block *b, const ff_params *p, double *dromax);
+void orc_cycle_sst(orc_block *b, const ff_params *p, int icycle, double *resi5, double *dromax);
 void orc_halo_pack(const orc_block *src, const ff_patch *pa, double *out);
 void orc_halo_unpack(orc_block *dst, const ff_patch *pa, const double *in);
 void orc_mb_boundi(orc_block **blk, int nblk, const ff_params *prm);

@@ -115,14 +115,31 @@ class Oracle:
     def cycle(self, icycle):
         r = (ctypes.c_double * 5)()
         d = ctypes.c_double()
-        self.L.orc_cycle(self._b(), self._p(), icycle, r, ctypes.byref(d))
+        fn = self.L.orc_cycle_sst if self.prm.iturb >= 3 else self.L.orc_cycle
+        fn(self._b(), self._p(), icycle, r, ctypes.byref(d))
         return np.array(r[:]), d.value
+
+    def turbeq(self):
+        self.L.orc_turbeq_sst(self._b(), self._p())
+
+    def residu_sst(self, icycle=1):
+        self.L.orc_residu_sst(self._b(), self._p(), icycle)
+
+    def imps_sst(self):
+        self.L.orc_imps_sst(self._b(), self._p())
+
+    def fin_limits_sst(self):
+        self.L.orc_fin_limits_sst(self._b(), self._p())
 
     def start(self):
         """NS3D start-up: SUBIN(0), BOUNDI(1) (ns3c.f:378-379), then SUBIN copies."""
         self.subin()
         self.boundi()
         self.subin()
+        if self.prm.iturb >= 3:
+            a = self.blk.arrays
+            a["RKOLD"][:] = a["RK"]
+            a["EPSOLD"][:] = a["REPS"]
 
 
 def roe_face(qr, ql, qrr, qll, nrm, area, intem, prm, cell_r, cell_l, kquirk=False):

@@ -185,4 +185,4 @@ def test_abi_exports_every_declared_symbol():
     assert len(names) >= 15
     for n in names:
         assert hasattr(L, n), n
-    assert L.ff_abi_version() == 1
+    assert L.ff_abi_version() == 2

@@ -26,6 +26,27 @@ def flux_scale(o, blk):
     return {n: interior(blk, S[v] / vol) for v, n in enumerate(("DRO", "DM", "DN", "DW", "DE"))}
 
 
+def flux_scale_sst(o, blk):
+    """S of the seven k-omega equations: face fluxes as in flux_scale plus
+    the k and omega source terms."""
+    L = o.L
+    nt = blk.ntot
+    names = ("F1R", "F1RM", "F1RN", "F1RW", "F1E", "F1RK", "F1EPS")
+    S = np.zeros((7, nt))
+    istr = blk.imax + 4
+    il = istr * (blk.jmax + 4)
+    for d, st in ((1, 1), (2, istr), (3, il)):
+        L.orc_flux_dir_sst(o._b(), o._p(), d)
+        for v, n in enumerate(names):
+            F = np.abs(blk.arrays[n])
+            S[v, :nt - st] += F[:nt - st] + F[st:]
+    vol = blk.arrays["VOL"]
+    out = {n: interior(blk, S[v] / vol) for v, n in enumerate(("DRO", "DM", "DN", "DW", "DE", "DRK", "DEPS"))}
+    out["DRK"] = out["DRK"] + np.abs(interior(blk, blk.arrays["SRK"]))
+    out["DEPS"] = out["DEPS"] + np.abs(interior(blk, blk.arrays["SEPS"]))
+    return out
+
+
 def make_pair(ni=17, nj=9, nk=9, **kw):
     bg, prm, fs = case.bump_case(ni, nj, nk, **kw)
     bc, _, _ = case.bump_case(ni, nj, nk, **kw)
