@@ -225,29 +225,75 @@ def init_freestream(b: Block, fs, *, noise=1e-3, seed=0):
     return b
 
 
-def wall_distance(blk: Block):
+def _closest_on_triangles(p, a, b, c):
+    """Distance from points p (n,3) to triangles (a,b,c) (n,3 each): the
+    closest-point regions of a triangle (vertex, edge, face), vectorised."""
+    ab, ac, ap = b - a, c - a, p - a
+    d1, d2 = np.einsum("ij,ij->i", ab, ap), np.einsum("ij,ij->i", ac, ap)
+    bp = p - b
+    d3, d4 = np.einsum("ij,ij->i", ab, bp), np.einsum("ij,ij->i", ac, bp)
+    cp = p - c
+    d5, d6 = np.einsum("ij,ij->i", ab, cp), np.einsum("ij,ij->i", ac, cp)
+    va = d3 * d6 - d5 * d4
+    vb = d5 * d2 - d1 * d6
+    vc = d1 * d4 - d3 * d2
+    den = np.where(va + vb + vc == 0, 1.0, va + vb + vc)
+    v, w = vb / den, vc / den
+    q = a + ab * v[:, None] + ac * w[:, None]                      # inside the face
+    with np.errstate(divide="ignore", invalid="ignore"):
+        t_ab = np.clip(np.where(d1 - d3 != 0, d1 / (d1 - d3), 0), 0, 1)
+        t_ac = np.clip(np.where(d2 - d6 != 0, d2 / (d2 - d6), 0), 0, 1)
+        t_bc = np.clip(np.where((d4 - d3) + (d5 - d6) != 0, (d4 - d3) / ((d4 - d3) + (d5 - d6)), 0), 0, 1)
+    e_ab = a + ab * t_ab[:, None]
+    e_ac = a + ac * t_ac[:, None]
+    e_bc = b + (c - b) * t_bc[:, None]
+    cand = [q, a, b, c, e_ab, e_ac, e_bc]
+    inside = (va >= 0) & (vb >= 0) & (vc >= 0)
+    dist = np.full(len(p), np.inf)
+    for k, x in enumerate(cand):
+        dk = np.linalg.norm(p - x, axis=1)
+        if k == 0:
+            dk = np.where(inside, dk, np.inf)
+        dist = np.minimum(dist, dk)
+    return dist
+
+
+def wall_distance(blk: Block, wall_block: Block = None, nnear: int = 8):
     """DISTW: distance of every cell centre (ghosts included) to the nearest
-    face centre of the block's solid-wall patches (set-up data, like the
-    reference's DISTANCES pass before the iteration loop)."""
+    point of the solid-wall surface of wall_block (default: blk itself;
+    coarse multigrid levels pass the finest level, whose nodes they lack),
+    each wall face split into two triangles -- set-up data, like the
+    reference's DISTANCES pass before the iteration loop."""
     from scipy.spatial import cKDTree
-    X, Y, Z = blk.nodes
-    pts = []
-    for pa in blk.patches:
+    wb = wall_block if wall_block is not None else blk
+    X, Y, Z = wb.nodes
+    P = np.stack([X, Y, Z], axis=-1)
+    tri_a, tri_b, tri_c = [], [], []
+    for pa in wb.patches:
         if not (7 <= pa.ityp <= 10):
             continue
         d = (pa.iface - 1) % 3
-        idx = 0 if pa.iface <= 3 else (X.shape[2 - d] - 1)
+        idx = 0 if pa.iface <= 3 else (P.shape[2 - d] - 1)
         sl = [slice(None)] * 3
         sl[2 - d] = idx
-        fx, fy, fz = (np.asarray(a[tuple(sl)]) for a in (X, Y, Z))
-        c = [0.25 * (f[:-1, :-1] + f[1:, :-1] + f[:-1, 1:] + f[1:, 1:]) for f in (fx, fy, fz)]
-        pts.append(np.stack([c[0].ravel(), c[1].ravel(), c[2].ravel()], axis=1))
-    if not pts:
+        F = P[tuple(sl)]                                    # 2-D node array of the face
+        n00, n10, n01, n11 = F[:-1, :-1], F[1:, :-1], F[:-1, 1:], F[1:, 1:]
+        for a, b, c in ((n00, n10, n11), (n00, n11, n01)):
+            tri_a.append(a.reshape(-1, 3)); tri_b.append(b.reshape(-1, 3)); tri_c.append(c.reshape(-1, 3))
+    if not tri_a:
         return np.full(blk.ntot, 1.0e3)
-    tree = cKDTree(np.concatenate(pts))
+    A, B, C = (np.concatenate(t) for t in (tri_a, tri_b, tri_c))
+    cen = (A + B + C) / 3.0
+    tree = cKDTree(cen)
     q = np.stack([blk.arrays["XC"], blk.arrays["YC"], blk.arrays["ZC"]], axis=1)
-    dist, _ = tree.query(q)
-    return dist
+    k = min(nnear, len(cen))
+    _, idx = tree.query(q, k=k)
+    idx = idx.reshape(len(q), k)
+    best = np.full(len(q), np.inf)
+    for j in range(k):
+        t = idx[:, j]
+        best = np.minimum(best, _closest_on_triangles(q, A[t], B[t], C[t]))
+    return best
 
 
 def sst_freestream(fs, tu=1.0e-3, mut_ratio=0.1):
@@ -276,7 +322,7 @@ def bump_case(ni=65, nj=33, nk=33, *, h1=1e-3, amp=0.1, mach=0.5, reynolds=1e4,
     return blk, prm, fs
 
 
-def setup_sst(blk: Block, prm: FFParams, fs, tu=1.0e-3, mut_ratio=0.1):
+def setup_sst(blk: Block, prm: FFParams, fs, tu=1.0e-3, mut_ratio=0.1, wall_block: Block = None):
     """Switch a case to k-omega SST: ITURB=6, the free-stream limits RKLIM /
     EPSLIM, inlet BOUNRK/BOUNEP, DISTW, and rho*k, rho*omega, mu_t of the
     free stream in every cell."""
@@ -285,7 +331,7 @@ def setup_sst(blk: Block, prm: FFParams, fs, tu=1.0e-3, mut_ratio=0.1):
     prm.rklim, prm.epslim = rk, re
     for pa in blk.patches:
         pa.bounrk, pa.bounep = rk, re
-    blk.arrays["DISTW"][:] = wall_distance(blk)
+    blk.arrays["DISTW"][:] = wall_distance(blk, wall_block)
     blk.arrays["RK"][:] = rk
     blk.arrays["REPS"][:] = re
     blk.arrays["EPS2"][:] = 1.0 + mut_ratio
@@ -297,7 +343,7 @@ def setup_sst(blk: Block, prm: FFParams, fs, tu=1.0e-3, mut_ratio=0.1):
 
 def bump_case_mg(ni=65, nj=33, nk=33, nlev=3, *, h1=1e-3, amp=0.1, mach=0.5, reynolds=1e4,
                  zlen=0.5, noise=1e-3, seed=0, cfl=2.0, cfll=2.0, inter=3, span_amp=0.0,
-                 lusgs_fp32=False, coarse_fp32=False):
+                 lusgs_fp32=False, coarse_fp32=False, turbulence=None, tu=1.0e-3, mut_ratio=0.1):
     """The bump channel with nlev multigrid levels (finest first); coarse
     metrics are lumped from the fine cells, patch ranges follow each level.
     lusgs_fp32 runs the fine level's implicit operator in FP32, coarse_fp32
@@ -312,6 +358,10 @@ def bump_case_mg(ni=65, nj=33, nk=33, nlev=3, *, h1=1e-3, amp=0.1, mach=0.5, rey
         init_freestream(blk, fs, noise=noise if lev == 0 else 0.0, seed=seed)
         levels.append(blk)
     prm = make_params(fc, levels[0].dims, cfl=cfl, cfll=cfll, inter=inter)
+    if turbulence == "sst":
+        for lev, blk in enumerate(levels):
+            setup_sst(blk, prm if lev == 0 else FFParams.from_buffer_copy(prm), fs, tu=tu,
+                      mut_ratio=mut_ratio, wall_block=levels[0])
     prms = [level_params(prm, lev + 1) for lev in range(nlev)]
     prms[0].lusgs_fp32 = int(lusgs_fp32)
     for q in prms[1:]:

@@ -141,41 +141,50 @@ int st_boundi(Ctx* c, BlockCtx* b) {
   return st_statim(c, b);
 }
 
-// TURBEQ res3c.f:5845 and RESIKE res3c.f:3423 (k-omega SST, level 1).
-int st_residu_sst(Ctx* c, BlockCtx* b, int icycle) {
+// TURBEQ res3c.f:5845 (level 1 at the start of the cycle, m2 = 1) and
+// RESIKE res3c.f:3423 (k-omega SST) on a level; for m2 >= 2 RESIKE
+// recomputes the velocity gradients of the level itself.
+int st_residu_sst(Ctx* c, BlockCtx* b, int level, int m2, int icycle) {
   int ncell = b->imax * b->jmax * b->kmax;
-  long ng = (long)(b->imax + 2) * (b->jmax + 2) * (b->kmax + 2);
-  k_grad<<<nblk(ng, 128), 128, 0, c->stream>>>(b->db, 1);              // DERFUN (+ TEMDER of T)
-  k_eps2ko<<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm);
+  int gg = level == 1 ? 2 : 0;
+  long ng = (long)(b->imax + gg) * (b->jmax + gg) * (b->kmax + gg);
+  if (m2 >= 2 || level == 1) {   // DERFUN (+ TEMDER of T) of this level
+    k_grad<<<nblk(ng, 128), 128, 0, c->stream>>>(b->db, level);
+    c->nlaunch++;
+  }
+  if (level == 1 && m2 == 1) {
+    k_eps2ko<<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm);
+    c->nlaunch++;
+  }
   k_crosko<<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db);
   k_rk_roundtrip<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db);
   CK(cudaMemsetAsync(b->d_red, 0, sizeof(unsigned long long), c->stream));
   k_cdmax<<<min(nblk(b->ntot, 256), 4 * c->sm_count), 256, 0, c->stream>>>(b->db, b->d_red);
   k_fun1ko<<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, b->d_red);
-  c->nlaunch += 6;
-  if (b->npatch) {
+  c->nlaunch += 4;
+  if (b->npatch && level == 1) {
     int maxn = 1;
     for (auto& p : b->h_patch) maxn = max(maxn, (p.r1b - p.r1a + 1) * (p.r2b - p.r2a + 1));
     k_refcen<<<dim3(nblk(maxn, 128), b->npatch), 128, 0, c->stream>>>(b->db, b->prm);
     c->nlaunch++;
   }
   k_prodke<<<nblk((long)b->jmax * b->db.is * b->kmax, 128), 128, 0, c->stream>>>(b->db);
-  long nt3 = (long)(b->imax + 2) * (b->jmax + 2) * (b->kmax > 1 ? b->kmax + 2 : b->kmax);
-  k_temder_ke<<<nblk(nt3, 128), 128, 0, c->stream>>>(b->db);
-  c->nlaunch += 2;
-  launch_patch(c, b, k_inlet_outlet, icycle);
+  c->nlaunch++;
+  if (b->prm.fullns) {
+    long nt3 = (long)(b->imax + gg) * (b->jmax + gg) * ((level == 1 && b->kmax > 1) ? b->kmax + 2 : b->kmax);
+    k_temder_ke<<<nblk(nt3, 128), 128, 0, c->stream>>>(b->db, level);
+    c->nlaunch++;
+  }
+  if (level == 1) launch_patch(c, b, k_inlet_outlet, icycle);
   dim3 g(nblk(b->imax, TI), nblk(b->jmax, TJ), nblk(b->kmax, TK));
-  k_residual_sst<<<g, 128, 0, c->stream>>>(b->db, b->prm);
+  k_residual_sst<<<g, 128, 0, c->stream>>>(b->db, b->prm, level);
   k_sourko_addske<<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db);
   c->nlaunch += 2;
   return 0;
 }
 
-int st_residu(Ctx* c, BlockCtx* b, int level, int icycle) {
-  if (b->prm.iturb >= 3) {
-    if (level != 1) return fail(c, FF_ERR_ARG, "k-omega SST runs on the finest level only");
-    return st_residu_sst(c, b, icycle);
-  }
+int st_residu(Ctx* c, BlockCtx* b, int level, int icycle, int m2 = 1) {
+  if (b->prm.iturb >= 3) return st_residu_sst(c, b, level, m2, icycle);
   if (level == 1) {
     if (b->npatch) {
       int maxn = 1;
@@ -462,8 +471,10 @@ int one_cycle(Ctx* c, BlockCtx* b, int icycle) {
 // RESIDI, FORCFU, ADDRES, IMPSDI, FIN; then INTERP back up, REFLEC, BOUNDI.
 int mg_cycle(Ctx* c, BlockCtx* b, int icycle) {
   int rc;
+  const int sst = b->prm.iturb >= 3;
   k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi, c->d_dromax);
   c->nlaunch++;
+  if (sst && (rc = st_statim(c, b, 1))) return rc;
   if ((rc = st_residu(c, b, 1, icycle))) return rc;
   if ((rc = st_imps(c, b, 1, false))) return rc;
   if ((rc = st_fin(c, b, 1))) return rc;
@@ -472,7 +483,7 @@ int mg_cycle(Ctx* c, BlockCtx* b, int icycle) {
   for (size_t m = 1; m < lv.size(); m++) {
     BlockCtx *f = lv[m - 1], *cc = lv[m];
     st_statim(c, f, 1);
-    if ((rc = st_residu(c, f, (int)m, icycle))) return rc;
+    if ((rc = st_residu(c, f, (int)m, icycle, (int)m + 1))) return rc;
     if (m == 1) {   // RESL2 of the level-1 residual after the fine update
       k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi, c->d_dromax);
       c->nlaunch++;
@@ -480,19 +491,19 @@ int mg_cycle(Ctx* c, BlockCtx* b, int icycle) {
       k_resl2<<<min(nblk(ncell, 256), 4 * c->sm_count), 256, 0, c->stream>>>(f->db, c->d_resi);
       c->nlaunch++;
     } else {
-      k_forcing<<<nblk(f->ntot, 256), 256, 0, c->stream>>>(f->db, 1);
+      k_forcing<<<nblk(f->ntot, 256), 256, 0, c->stream>>>(f->db, 1, sst);
       c->nlaunch++;
     }
     long nc = (long)(cc->imax + 2) * (cc->jmax + 2) * (cc->kmax + 2);
-    k_transf<<<nblk(nc, 128), 128, 0, c->stream>>>(f->db, cc->db);
+    k_transf<<<nblk(nc, 128), 128, 0, c->stream>>>(f->db, cc->db, sst);
     c->nlaunch++;
-    k_transf_ring<<<nblk(cc->ntot, 256), 256, 0, c->stream>>>(cc->db);
+    k_transf_ring<<<nblk(cc->ntot, 256), 256, 0, c->stream>>>(cc->db, sst);
     c->nlaunch++;
     st_statim(c, cc, 1);
-    if ((rc = st_residu(c, cc, (int)m + 1, icycle))) return rc;
-    k_forcing<<<nblk(cc->ntot, 256), 256, 0, c->stream>>>(cc->db, 0);
+    if ((rc = st_residu(c, cc, (int)m + 1, icycle, (int)m + 1))) return rc;
+    k_forcing<<<nblk(cc->ntot, 256), 256, 0, c->stream>>>(cc->db, 0, sst);
     c->nlaunch++;
-    k_forcing<<<nblk(cc->ntot, 256), 256, 0, c->stream>>>(cc->db, 1);
+    k_forcing<<<nblk(cc->ntot, 256), 256, 0, c->stream>>>(cc->db, 1, sst);
     c->nlaunch++;
     if ((rc = st_imps(c, cc, (int)m + 1, true))) return rc;
     k_fin_coarse<<<nblk(cc->ntot, 256), 256, 0, c->stream>>>(cc->db, cc->prm, 1);
@@ -503,6 +514,10 @@ int mg_cycle(Ctx* c, BlockCtx* b, int icycle) {
     int nf = f->imax * f->jmax * f->kmax;
     k_interp<<<nblk(nf, 256), 256, 0, c->stream>>>(cc->db, f->db);
     c->nlaunch++;
+    if (sst) {
+      k_intert<<<nblk(nf, 256), 256, 0, c->stream>>>(cc->db, f->db, f->prm);
+      c->nlaunch++;
+    }
     k_fin_coarse<<<nblk(f->ntot, 256), 256, 0, c->stream>>>(f->db, f->prm, 0);
     c->nlaunch++;
   }
@@ -511,6 +526,10 @@ int mg_cycle(Ctx* c, BlockCtx* b, int icycle) {
   // SUBIN's *OLD copies (INTERP changed the level-1 state after FIN)
   k_subin_copy<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db);
   c->nlaunch++;
+  if (sst) {   // SUBIN: k cap, RKOLD / EPSOLD
+    k_subin_sst<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db, b->prm);
+    c->nlaunch++;
+  }
   // SUBIN's max|DE| sees the level-1 residual of the second RESIDI
   k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi + 6, c->d_dromax);
   c->nlaunch++;
@@ -845,8 +864,6 @@ int ff_mg_link(void* ctx, int fine, int coarse) {
   BlockCtx *f = getb(c, fine), *cc = getb(c, coarse);
   if (!f || !cc || f == cc || f->imax != 2 * cc->imax || f->jmax != 2 * cc->jmax || f->kmax != 2 * cc->kmax)
     return fail(c, FF_ERR_ARG, "ff_mg_link: the coarse block must halve every dimension");
-  if (f->prm.iturb >= 3 || cc->prm.iturb >= 3)
-    return fail(c, FF_ERR_ARG, "ff_mg_link: multigrid with k-omega SST is not available");
   f->coarse = cc;
   cc->level = f->level + 1;
   if (f->graph) { cudaGraphExecDestroy(f->graph); f->graph = nullptr; }

@@ -62,6 +62,7 @@ __global__ void k_state(DevBlock b, ff_params p) {
   size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= (size_t)b.ntot) return;
   state_cell(b, p, n);
+  if (p.iturb >= 3) return;   // TURBEQ, not ADJUIN, sets EPS2 and VIST
   int i = (int)(n % b.is), j = (int)((n / b.is) % (b.jmax + 4)), k = (int)(n / b.il);
   if (i >= 2 && i < b.imax + 2 && j >= 2 && j < b.jmax + 2 && k >= 2 && k < b.kmax + 2) {
     b.a[FF_EPS2][n] = 1.0;
@@ -393,7 +394,8 @@ FF_DI void visc_flux(const DevBlock& b, const ff_params& p, size_t L, int S, int
 
 // FLUXDO base3c.f:3677 (thin layer, IDIFF = 1): the viscous flux on coarse
 // levels and whenever FULLNS is off.
-FF_DI void visc_flux_thin(const DevBlock& b, const ff_params& p, size_t L, int S, int dir, double f[5]) {
+FF_DI void visc_flux_thin(const DevBlock& b, const ff_params& p, size_t L, int S, int dir, double f[5],
+                          double fe0 = 0.) {
 #define LD(s, n) __ldg(b.a[s] + (n))
   size_t M = L - S;
   const int ao = 4 * (dir - 1);
@@ -410,7 +412,7 @@ FF_DI void visc_flux_thin(const DevBlock& b, const ff_params& p, size_t L, int S
   double f4 = surf * (wl - wm + nz * duc);
   double f5 = .5 * ((ul + um) * f2 + (vl + vm) * f3 + (wl + wm) * f4);
   f[0] = 0.; f[1] = f2; f[2] = f3; f[3] = f4;
-  f[4] = f5 + surfe * (LD(FF_TEMP, L) - LD(FF_TEMP, M));
+  f[4] = fe0 + f5 + surfe * (LD(FF_TEMP, L) - LD(FF_TEMP, M));
 #undef LD
 }
 
@@ -873,7 +875,7 @@ __global__ void k_fin_divide(DevBlock b, int sst) {
 // TRANSF multi.f:156: volume-weighted restriction of TEMP,U,V,W,PDIFF,EPS2,
 // VIST and of the residuals (into P2H) for coarse cells 0..MAX+1, and the
 // interior *OLD copies.
-__global__ void k_transf(DevBlock f, DevBlock c) {
+__global__ void k_transf(DevBlock f, DevBlock c, int sst) {
   int ni = c.imax + 2, nj = c.jmax + 2, nk = c.kmax + 2;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ni * nj * nk) return;
@@ -897,18 +899,30 @@ __global__ void k_transf(DevBlock f, DevBlock c) {
     for (int q = 0; q < 8; q++) s += vv[q] * X[o[q]];
     c.a[ds[v]][N] = s * pvol;
   }
+  if (sst) {   // TRANKE multi.f:434: RK, REPS and DRK, DEPS into RKP2H, EPP2H
+    const int vk[4] = {FF_RK, FF_REPS, FF_DRK, FF_DEPS}, dk[4] = {FF_RK, FF_REPS, FF_RKP2H, FF_EPP2H};
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+      const double* X = f.a[vk[v]];
+      double s = 0.;
+#pragma unroll
+      for (int q = 0; q < 8; q++) s += vv[q] * X[o[q]];
+      c.a[dk[v]][N] = s * pvol;
+    }
+  }
   if (I >= 1 && I <= c.imax && J >= 1 && J <= c.jmax && K >= 1 && K <= c.kmax) {
     c.a[FF_TOLD][N] = c.a[FF_TEMP][N];
     c.a[FF_UOLD][N] = c.a[FF_U][N];
     c.a[FF_VOLD][N] = c.a[FF_V][N];
     c.a[FF_WOLD][N] = c.a[FF_W][N];
     c.a[FF_POLD][N] = c.a[FF_PDIFF][N];
+    if (sst) { c.a[FF_RKOLD][N] = c.a[FF_RK][N]; c.a[FF_EPSOLD][N] = c.a[FF_REPS][N]; }
   }
 }
 
 // Coarse ghost rings of TRANSF (multi.f:250-432): P2H = 0 in both ghost
 // layers; the second ghost layer of each face copies the first one.
-__global__ void k_transf_ring(DevBlock c) {
+__global__ void k_transf_ring(DevBlock c, int sst) {
   size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= (size_t)c.ntot) return;
   int i = (int)(n % c.is) - 1, j = (int)((n / c.is) % (c.jmax + 4)) - 1, k = (int)(n / c.il) - 1;
@@ -916,6 +930,7 @@ __global__ void k_transf_ring(DevBlock c) {
   if (!(gi || gj || gk)) return;
 #pragma unroll
   for (int v = 0; v < 5; v++) c.a[FF_ROP2H + v][n] = 0.;
+  if (sst) { c.a[FF_RKP2H][n] = 0.; c.a[FF_EPP2H][n] = 0.; }
   // second-layer face ghosts copy the first layer along the face normal
   // (cells in the second layer of two directions are not used on coarse
   // levels and are left alone)
@@ -926,22 +941,40 @@ __global__ void k_transf_ring(DevBlock c) {
   else if (j == -1) src_off = c.is; else if (j == c.jmax + 2) src_off = -c.is;
   else if (k == -1) src_off = c.il; else if (k == c.kmax + 2) src_off = -c.il;
   if (src_off == 0) return;
-  const int vs[7] = {FF_TEMP, FF_U, FF_V, FF_W, FF_PDIFF, FF_EPS2, FF_VIST};
-#pragma unroll
-  for (int v = 0; v < 7; v++) c.a[vs[v]][n] = c.a[vs[v]][n + src_off];
+  const int vs[9] = {FF_TEMP, FF_U, FF_V, FF_W, FF_PDIFF, FF_EPS2, FF_VIST, FF_RK, FF_REPS};
+  const int nv = sst ? 9 : 7;
+  for (int v = 0; v < nv; v++) c.a[vs[v]][n] = c.a[vs[v]][n + src_off];
 }
 
 // FORCFU multi.f:1609 (mode 0: P2H -= R) and ADDRES multi.f:1686 (mode 1:
 // R = P2H + R), every cell of the level.
-__global__ void k_forcing(DevBlock b, int mode) {
+__global__ void k_forcing(DevBlock b, int mode, int sst) {
   size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= (size_t)b.ntot) return;
-#pragma unroll
-  for (int v = 0; v < 5; v++) {
-    double* P2 = b.a[FF_ROP2H + v];
+  const int ps[7] = {FF_ROP2H, FF_RMP2H, FF_RNP2H, FF_RWP2H, FF_EP2H, FF_RKP2H, FF_EPP2H};
+  const int nv = sst ? 7 : 5;
+  for (int v = 0; v < nv; v++) {
+    double* P2 = b.a[ps[v]];
     double* R = b.a[FF_DRO + v];
     if (mode == 0) P2[n] = P2[n] - R[n];
     else R[n] = P2[n] + R[n];
+  }
+}
+
+// INTERT multi.f:2051 -> INTERO 2007: damped injection of the coarse k and
+// omega corrections (CMGK, CMGEPS) into the fine interior.
+__global__ void k_intert(DevBlock c, DevBlock f, ff_params p) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= f.imax * f.jmax * f.kmax) return;
+  int I = t % f.imax + 1, J = (t / f.imax) % f.jmax + 1, K = t / (f.imax * f.jmax) + 1;
+  size_t N = ix(c, (I + 1) / 2, (J + 1) / 2, (K + 1) / 2), F = ix(f, I, J, K);
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+    const double cc1 = q == 0 ? p.cmgk : p.cmgeps, cc2 = cc1 + 1.E-7;
+    double drok = c.a[q == 0 ? FF_RK : FF_REPS][N] - c.a[q == 0 ? FF_RKOLD : FF_EPSOLD][N];
+    double* R = f.a[q == 0 ? FF_RK : FF_REPS];
+    double r = R[F];
+    R[F] = r + cc1 * r * drok / (cc2 * r + fabs(drok));
   }
 }
 
@@ -960,15 +993,16 @@ __global__ void k_interp(DevBlock c, DevBlock f) {
   f.a[FF_PDIFF][F] = f.a[FF_PDIFF][F] + dp;
 }
 
-// FIN on a coarse level (update = 1) and the TEMP / pressure limits that
-// follow it or INTERP (ns3c.f:1948-1990, 2059-2125): UPLIM/LOLIM TEMP,
-// LOLIMP (no PDTOP there).
+// FIN on a coarse level (update = 1: UPLIM/LOLIM TEMP, LOLIMP, no PDTOP,
+// ns3c.f:1935-1990) and the limits after INTERP (update = 0, ns3c.f:2059-2125:
+// LOLIMP; the two-equation branch also limits TEMP, RK and REPS).
 __global__ void k_fin_coarse(DevBlock b, ff_params p, int update) {
   size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= (size_t)b.ntot) return;
   int i = (int)(n % b.is), j = (int)((n / b.is) % (b.jmax + 4)), k = (int)(n / b.il);
   bool kin = k >= 2 && k < b.kmax + 2, jin = j >= 2 && j < b.jmax + 2;
   bool interior = kin && jin && i >= 2 && i < b.imax + 2;
+  const bool sst = p.iturb >= 3;
   double T = b.a[FF_TEMP][n];
   if (update && interior) {
     T = b.a[FF_TOLD][n] + b.a[FF_DRO][n];
@@ -976,10 +1010,23 @@ __global__ void k_fin_coarse(DevBlock b, ff_params p, int update) {
     b.a[FF_V][n] = b.a[FF_VOLD][n] + b.a[FF_DN][n];
     b.a[FF_W][n] = b.a[FF_WOLD][n] + b.a[FF_DW][n];
     b.a[FF_PDIFF][n] = b.a[FF_POLD][n] + b.a[FF_DE][n];
+    if (sst) {   // FIN res3c.f:1190-1198
+      double drk = b.a[FF_DRK][n], deps = b.a[FF_DEPS][n];
+      double rkold = b.a[FF_RKOLD][n], epold = b.a[FF_EPSOLD][n];
+      b.a[FF_RK][n] = rkold + drk / (1. + fabs(drk) / (.45 * rkold));
+      b.a[FF_REPS][n] = epold + deps / (1. + fabs(deps) / (.90 * epold));
+    }
   }
-  if (kin && jin) T = dmin(T, p.tuplim);
-  T = dmax(T, p.tlolim);
-  b.a[FF_TEMP][n] = T;
+  if (sst) {   // LOLIM of RK, REPS over every cell (FIN; after INTERP, CYCLES)
+    b.a[FF_RK][n] = dmax(b.a[FF_RK][n], p.rklim);
+    b.a[FF_REPS][n] = dmax(b.a[FF_REPS][n], p.epslim);
+  }
+  // TEMP limits after a coarse FIN, and after INTERP on the two-equation branch
+  if (update || sst) {
+    if (kin && jin) T = dmin(T, p.tuplim);
+    T = dmax(T, p.tlolim);
+    b.a[FF_TEMP][n] = T;
+  }
   double P = b.a[FF_P][n];
   double prelim = dmin(0., P - 0.01 * p.frspre);
   b.a[FF_P][n] = P - prelim;

@@ -144,12 +144,13 @@ __global__ void k_prodke(DevBlock b) {
 
 // TEMDER of k = RK/RO and omega = REPS/RO (DIVV12 + TEMDER, res3c.f:3994-4006)
 // over the TEMDER range of level 1.
-__global__ void k_temder_ke(DevBlock b) {
-  int ni = b.imax + 2, nj = b.jmax + 2;
-  int klo = b.kmax > 1 ? 0 : 1, nk = b.kmax > 1 ? b.kmax + 2 : b.kmax;
+__global__ void k_temder_ke(DevBlock b, int level) {
+  const int lo = level == 1 ? 0 : 1, g = level == 1 ? 2 : 0;
+  int ni = b.imax + g, nj = b.jmax + g;
+  int klo = (level == 1 && b.kmax > 1) ? 0 : 1, nk = (level == 1 && b.kmax > 1) ? b.kmax + 2 : b.kmax;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ni * nj * nk) return;
-  int I = t % ni, J = (t / ni) % nj, K = t / (ni * nj) + klo;
+  int I = t % ni + lo, J = (t / ni) % nj + lo, K = t / (ni * nj) + klo;
   const int IS = b.is, IL = b.il;
   size_t L = ix(b, I, J, K);
   const double *RO = b.a[FF_RO];
@@ -323,6 +324,24 @@ FF_DI void flkebl_face(const DevBlock& b, size_t I, int S, int dir, double& frk,
 #undef LD
 }
 
+// FLUDKE base3c.f:5547: thin-layer k and omega diffusion (coarse levels).
+FF_DI void fludke_face(const DevBlock& b, size_t I, int S, int dir, double& frk, double& feps) {
+#define LD(s, n) __ldg(b.a[s] + (n))
+  size_t M = I - S;
+  double f1 = LD(FF_FUN1, I), onemf1 = dmax(0.0, 1.0 - f1);
+  double psigk = f1 * SST_SIGRK1 + onemf1 * SST_SIGRK2;
+  double psige = f1 * SST_SIGOM1 + onemf1 * SST_SIGOM2;
+  double area = LD(FF_A1 + 4 * (dir - 1), I);
+  double ypd2 = area / (LD(FF_VOL, I) + LD(FF_VOL, M));
+  double surg = -area * ypd2;
+  double rmut2 = (LD(FF_EPS2, I) - 1.) * LD(FF_VIS, I) + (LD(FF_EPS2, M) - 1.) * LD(FF_VIS, M);
+  double vv = LD(FF_VIS, I) + LD(FF_VIS, M);
+  double ypro1 = 1. / LD(FF_RO, I), ypro2 = 1. / LD(FF_RO, M);
+  frk = surg * (vv + rmut2 * psigk) * (LD(FF_RK, I) * ypro1 - LD(FF_RK, M) * ypro2);
+  feps = surg * (vv + rmut2 * psige) * (LD(FF_REPS, I) * ypro1 - LD(FF_REPS, M) * ypro2);
+#undef LD
+}
+
 // BOTSKE with k and omega (smooth wall, IDIS=2): seven wall fluxes.
 FF_DI void wall_flux_ke(const DevBlock& b, const ff_params& p, size_t II, int S, int idir, int dir, int iheat,
                         int intem, double f[7]) {
@@ -385,10 +404,11 @@ FF_DI void wall_flux_ke(const DevBlock& b, const ff_params& p, size_t II, int S,
 // Flux of one face with k and omega (FLXCYC order: FLKEBL, SETV12, FLUXBL,
 // FLUXKE; BOTSKE on walls).
 FF_DI void face_flux_ke(const DevBlock& b, const ff_params& p, int dir, size_t L, int m, int t1, int t2,
-                        double f[7]) {
+                        int level, double f[7]) {
   const int S = dir == 1 ? 1 : (dir == 2 ? b.is : b.il);
   const int nmax = dir == 1 ? b.imax : (dir == 2 ? b.jmax : b.kmax);
   int intem = dir == 1 ? p.interi : (dir == 2 ? p.interj : p.interk);
+  if (level > 1) intem = p.coarse_inter;
   int intet = (intem > -5 && intem < 5) ? 1 : intem;
   if (m == 1 || m == nmax + 1) {
     int iface = m == 1 ? dir : dir + 3;
@@ -407,10 +427,16 @@ FF_DI void face_flux_ke(const DevBlock& b, const ff_params& p, int dir, size_t L
   for (int v = 0; v < 7; v++) f[v] = 0.;
   if (m <= min(idi, nmax + 1)) {
     double frk, feps, fv[5];
-    flkebl_face(b, L, S, dir, frk, feps);
-    visc_flux(b, p, L, S, dir, fv);
+    if (level == 1 && p.fullns) {   // FLKEBL, SETV12, FLUXBL
+      flkebl_face(b, L, S, dir, frk, feps);
+      visc_flux(b, p, L, S, dir, fv);
+      f[4] = frk + fv[4];
+    } else {                        // FLUDKE, FLUXDO
+      fludke_face(b, L, S, dir, frk, feps);
+      visc_flux_thin(b, p, L, S, dir, fv, frk);
+      f[4] = fv[4];
+    }
     f[1] = fv[1]; f[2] = fv[2]; f[3] = fv[3];
-    f[4] = frk + fv[4];
     f[5] = frk; f[6] = feps;
   }
   double q[7][4];
@@ -429,7 +455,7 @@ FF_DI void face_flux_ke(const DevBlock& b, const ff_params& p, int dir, size_t L
 }
 
 // RESIKE face cycles + SWEEPK for a 32x4x4 tile (k, i, j, then 1/VOL).
-__global__ void __launch_bounds__(128) k_residual_sst(DevBlock b, ff_params p) {
+__global__ void __launch_bounds__(128) k_residual_sst(DevBlock b, ff_params p, int level) {
   __shared__ double sF[7][TI * (TJ + 1) * TK];
   const int tid = threadIdx.x;
   const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ, k0 = blockIdx.z * TK;
@@ -444,7 +470,7 @@ __global__ void __launch_bounds__(128) k_residual_sst(DevBlock b, ff_params p) {
     int I = i0 + fi + 1, J = j0 + fj + 1, m = k0 + fk + 1;
     if (I > b.imax || J > b.jmax || m > b.kmax + 1) continue;
     double fl[7];
-    face_flux_ke(b, p, 3, ix(b, I, J, m), m, I, J, fl);
+    face_flux_ke(b, p, 3, ix(b, I, J, m), m, I, J, level, fl);
 #pragma unroll
     for (int v = 0; v < 7; v++) sF[v][f] = fl[v];
   }
@@ -462,7 +488,7 @@ __global__ void __launch_bounds__(128) k_residual_sst(DevBlock b, ff_params p) {
     int m = i0 + fi + 1, J = j0 + fj + 1, K = k0 + fk + 1;
     if (m > b.imax + 1 || J > b.jmax || K > b.kmax) continue;
     double fl[7];
-    face_flux_ke(b, p, 1, ix(b, m, J, K), m, J, K, fl);
+    face_flux_ke(b, p, 1, ix(b, m, J, K), m, J, K, level, fl);
 #pragma unroll
     for (int v = 0; v < 7; v++) sF[v][f] = fl[v];
   }
@@ -480,7 +506,7 @@ __global__ void __launch_bounds__(128) k_residual_sst(DevBlock b, ff_params p) {
     int I = i0 + fi + 1, m = j0 + fj + 1, K = k0 + fk + 1;
     if (I > b.imax || m > b.jmax + 1 || K > b.kmax) continue;
     double fl[7];
-    face_flux_ke(b, p, 2, ix(b, I, m, K), m, I, K, fl);
+    face_flux_ke(b, p, 2, ix(b, I, m, K), m, I, K, level, fl);
 #pragma unroll
     for (int v = 0; v < 7; v++) sF[v][f] = fl[v];
   }

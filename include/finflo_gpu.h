@@ -61,11 +61,12 @@ int ff_resl2(void *ctx, int blk, double *out5);
 int ff_imps(void *ctx, int blk, int level);
 int ff_fin(void *ctx, int blk, double *dromax);
 
-/* With ff_params.iturb = 6 (k-omega SST, single grid level) ff_residu is
+/* With ff_params.iturb = 6 (k-omega SST) ff_residu is
  * TURBEQ res3c.f:5845 + RESIKE res3c.f:3423, ff_imps the seven-equation
  * IMPS (LOCDTK, IMSOKO, COPRKE, PRKEGS/DIKEGS/COKEGS) and ff_fin also
  * updates RK, REPS; ff_cycles adds the cycle-start STATIM and the k cap of
- * SUBIN.  ff_mg_link refuses SST blocks. */
+ * SUBIN; linked multigrid levels run TRANKE, the k-omega forcing, the
+ * coarse-level RESIKE (FLUDKE, first-order Roe) and INTERT. */
 
 /* ncycles full cycles (RESIDU, RESL2, IMPS, FIN, BOUNDI, SUBIN); hist
  * (nullable) receives ncycles x {RESI(31..35) sums of squares, DROMAX}. */

@@ -646,9 +646,19 @@ static void fluxbl_face(const orc_block *b, const ff_params *p, size_t L, int S,
   F[0] = 0.; F[1] = -f2; F[2] = -f3; F[3] = -f4; F[4] = 0. - f5;
 }
 
+static void fluxdo_face_fe(const orc_block *b, const ff_params *p, size_t L, int S, int dir, double fe0,
+                           double *F);
+
 /* FLUXDO base3c.f:3677 (thin layer, IDIFF=1): the viscous flux on coarse
  * levels and whenever FULLNS is off. */
 static void fluxdo_face(const orc_block *b, const ff_params *p, size_t L, int S, int dir, double *F) {
+  fluxdo_face_fe(b, p, L, S, dir, 0., F);
+}
+
+/* FLUXDO with the energy flux already holding fe0 (FLUDKE's k diffusion on
+ * two-equation coarse levels): FE = fe0 + F5VIG + SURFE*(T(I)-T(I-IL)). */
+static void fluxdo_face_fe(const orc_block *b, const ff_params *p, size_t L, int S, int dir, double fe0,
+                           double *F) {
   const double *A = b->a[FF_A1 + 4 * (dir - 1)], *NX = b->a[FF_A1XA + 4 * (dir - 1)];
   const double *NY = b->a[FF_A1YA + 4 * (dir - 1)], *NZ = b->a[FF_A1ZA + 4 * (dir - 1)];
   const double *VOL = b->a[FF_VOL], *U = b->a[FF_U], *V = b->a[FF_V], *W = b->a[FF_W], *T = b->a[FF_TEMP];
@@ -665,7 +675,7 @@ static void fluxdo_face(const orc_block *b, const ff_params *p, size_t L, int S,
   double f4 = surf * (W[L] - W[M] + NZ[L] * duc);
   double f5 = .5 * ((U[L] + U[M]) * f2 + (V[L] + V[M]) * f3 + (W[L] + W[M]) * f4);
   F[0] = 0.; F[1] = f2; F[2] = f3; F[3] = f4;
-  F[4] = 0. + f5 + surfe * (T[L] - T[M]);
+  F[4] = fe0 + f5 + surfe * (T[L] - T[M]);
 }
 
 /* BOTSKE base3c.f:6147-6760: solid-wall face flux on level 1, laminar,
@@ -1487,9 +1497,29 @@ void orc_fin_coarse(orc_block *b, const ff_params *p) {
   temp_p_limits(b, p);
 }
 
+void orc_intert(orc_block *c, orc_block *f, const ff_params *pf);
+
+/* After INTERP (ns3c.f:2016-2120): the two-equation branch limits T, RK,
+ * REPS (UPLIM/LOLIM); LOLIMP always. */
 void orc_interp_limits(orc_block *c, orc_block *f, const ff_params *pf) {
   orc_interp(c, f);
-  temp_p_limits(f, pf);
+  dims_t d = dims_of(f);
+  double *T = f->a[FF_TEMP], *P = f->a[FF_P], *PD = f->a[FF_PDIFF];
+  if (pf->iturb >= 3) {
+    orc_intert(c, f, pf);
+    for (int K = 1; K <= d.kmax; K++) {
+      size_t ia = (size_t)(K + 1) * d.il + 2 * d.is;
+      for (int i = 0; i < d.jmax * d.is; i++) T[ia + i] = MIND(T[ia + i], pf->tuplim);
+    }
+    for (int n = 0; n < d.ntot; n++) T[n] = MAXD(T[n], pf->tlolim);
+    for (int n = 0; n < d.ntot; n++) f->a[FF_RK][n] = MAXD(f->a[FF_RK][n], pf->rklim);
+    for (int n = 0; n < d.ntot; n++) f->a[FF_REPS][n] = MAXD(f->a[FF_REPS][n], pf->epslim);
+  }
+  for (int n = 0; n < d.ntot; n++) {
+    double prelim = MIND(0., P[n] - 0.01 * pf->frspre);
+    P[n] = P[n] - prelim;
+    PD[n] = PD[n] - prelim;
+  }
 }
 
 /* One multigrid cycle of CYCLES (ns3c.f:1400-2170) with BOUNDI and SUBIN.

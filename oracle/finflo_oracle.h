@@ -60,6 +60,14 @@ void orc_flux_dir_sst(orc_block *b, const ff_params *p, int dir);
 void orc_imps_sst(orc_block *b, const ff_params *p);
 void orc_fin_limits_sst(orc_block *b, const ff_params *p);
 void orc_subin_sst(orc_block *b, const ff_params *p, double *dromax);
+void orc_residu_sst_lev(orc_block *b, const ff_params *p, int lev, int m2, int icycle);
+void orc_imps_sst_lev(orc_block *b, const ff_params *p, int lev);
+void orc_tranke(orc_block *f, orc_block *c);
+void orc_forcfu_ke(orc_block *c);
+void orc_addres_ke(orc_block *c);
+void orc_intert(orc_block *c, orc_block *f, const ff_params *pf);
+void orc_fin_coarse_sst(orc_block *b, const ff_params *p);
+void orc_mg_cycle_sst(orc_block **lv, int nlev, const ff_params *prm, int icycle, double *resi5, double *dromax);
 void orc_cycle_sst(orc_block *b, const ff_params *p, int icycle, double *resi5, double *dromax);
 void orc_halo_pack(const orc_block *src, const ff_patch *pa, double *out);
 void orc_halo_unpack(orc_block *dst, const ff_patch *pa, const double *in);

@@ -571,35 +571,130 @@ static void sourko_addske(orc_block *b) {
       }
 }
 
-/* RESIKE res3c.f:3423 on level 1 for SST: zero the increments and sources,
- * CROSKO + FUN1KO, REFCEN, MAKE_EPS + PRODKE, TEMDER of T, k, omega, the
- * k, i, j direction cycles with SWEEPK, then SOURKO + ADDSKE.  The velocity
+/* FLUDKE base3c.f:5547: thin-layer k and omega diffusion of one face
+ * (coarse levels, or FULLNS off). */
+static void fludke_face(const orc_block *b, size_t I, int S, int dir, double *frk, double *feps) {
+  const double *A = b->a[FF_A1 + 4 * (dir - 1)], *VOL = b->a[FF_VOL], *FUN1 = b->a[FF_FUN1];
+  const double *VIS = b->a[FF_VIS], *EPS2 = b->a[FF_EPS2], *RO = b->a[FF_RO];
+  const double *RK = b->a[FF_RK], *REPS = b->a[FF_REPS];
+  size_t M = I - S;
+  double onemf1 = MAXD(0.0, (1.0 - FUN1[I]));
+  double psigk = FUN1[I] * SST_SIGRK1 + onemf1 * SST_SIGRK2;
+  double psige = FUN1[I] * SST_SIGOM1 + onemf1 * SST_SIGOM2;
+  double ypd2 = A[I] / (VOL[I] + VOL[M]);
+  double surg = -A[I] * ypd2;
+  double rmut2 = (EPS2[I] - 1.) * VIS[I] + (EPS2[M] - 1.) * VIS[M];
+  double surfk = surg * (VIS[I] + VIS[M] + rmut2 * psigk);
+  double surfep = surg * (VIS[I] + VIS[M] + rmut2 * psige);
+  double ypro1 = 1. / RO[I], ypro2 = 1. / RO[M];
+  *frk = surfk * (RK[I] * ypro1 - RK[M] * ypro2);
+  *feps = surfep * (REPS[I] * ypro1 - REPS[M] * ypro2);
+}
+
+/* FLXCYC on a coarse level (M > 1): FLUDKE + FLUXDO, first-order Roe
+ * (INTERI/J/K = INTET = 55), BOTSKE walls; no inlet/outlet update. */
+static void flux_dir_sst_coarse(orc_block *b, const ff_params *p, int dir) {
+  dims_t d = dims_of(b);
+  int S = dir == 1 ? 1 : (dir == 2 ? d.is : d.il);
+  int nmax = dir == 1 ? d.imax : (dir == 2 ? d.jmax : d.kmax);
+  int intem = p->coarse_inter, intet = (intem > -5 && intem < 5) ? 1 : intem;
+  double *F[7] = {b->a[FF_F1R], b->a[FF_F1RM], b->a[FF_F1RN], b->a[FF_F1RW], b->a[FF_F1E],
+                  b->a[FF_F1RK], b->a[FF_F1EPS]};
+  for (int v = 0; v < 7; v++) memset(F[v], 0, sizeof(double) * d.ntot);
+  const double *A = b->a[FF_A1 + 4 * (dir - 1)], *NX = b->a[FF_A1XA + 4 * (dir - 1)];
+  const double *NY = b->a[FF_A1YA + 4 * (dir - 1)], *NZ = b->a[FF_A1ZA + 4 * (dir - 1)];
+  const double *RO = b->a[FF_RO], *U = b->a[FF_U], *V = b->a[FF_V], *W = b->a[FF_W];
+  const double *P = b->a[FF_P], *C = b->a[FF_C], *DRDP = b->a[FF_DRDP], *DRDH = b->a[FF_DRDH];
+  const double *RK = b->a[FF_RK], *REPS = b->a[FF_REPS];
+  int t1max = dir == 1 ? d.jmax : d.imax, t2max = dir == 3 ? d.jmax : d.kmax;
+  int idi = dir == 1 ? p->idi1 : (dir == 2 ? p->idi2 : p->idi3);
+  for (int t2 = 1; t2 <= t2max; t2++)
+    for (int t1 = 1; t1 <= t1max; t1++)
+      for (int m = 1; m <= nmax + 1; m++) {
+        size_t L = dir == 1 ? IX(d, m, t1, t2) : (dir == 2 ? IX(d, t1, m, t2) : IX(d, t1, t2, m));
+        double f[7] = {0, 0, 0, 0, 0, 0, 0};
+        if (m <= MIND(idi, nmax + 1)) {
+          double frk, feps, fv[5];
+          fludke_face(b, L, S, dir, &frk, &feps);
+          f[5] = frk; f[6] = feps;
+          fluxdo_face_fe(b, p, L, S, dir, frk, fv);
+          f[0] = 0.; f[1] = fv[1]; f[2] = fv[2]; f[3] = fv[3]; f[4] = fv[4];
+        }
+        double q[7][4];
+        const double *arr[7] = {RO, U, V, W, P, RK, REPS};
+        for (int v = 0; v < 7; v++) {
+          q[v][0] = arr[v][L - 2 * S]; q[v][1] = arr[v][L - S];
+          q[v][2] = arr[v][L]; q[v][3] = arr[v][L + S];
+        }
+        double nrm[3] = {NX[L], NY[L], NZ[L]};
+        double cr[5] = {C[L], DRDP[L], DRDH[L], RO[L], P[L]};
+        size_t L2 = dir == 3 ? L : L - S;
+        double cl[5] = {C[L2], DRDP[L2], DRDH[L2], RO[L2], P[L2]};
+        roe_face_ke(q, nrm, A[L], intem, intet, p, C[L], C[L - S], cr, cl, f);
+        for (int v = 0; v < 7; v++) F[v][L] = f[v];
+      }
+  for (int ip = 0; ip < b->npatch; ip++) {
+    const ff_patch *pa = &b->patch[ip];
+    if (pa->ityp < 8 || pa->ityp > 10) continue;
+    face_t f = face_geom(&d, pa->iface);
+    if (f.dir != dir) continue;
+    for (int bb = pa->r2a; bb <= pa->r2b; bb++)
+      for (int a = pa->r1a; a <= pa->r1b; a++) {
+        size_t II = face_cell(&d, &f, a, bb);
+        double fw[7];
+        botske_face_ke(b, p, II, S, f.idir, dir, pa->iheat, intem, fw);
+        size_t IF1 = f.idir == 1 ? II : II + S;
+        for (int v = 0; v < 7; v++) F[v][IF1] = fw[v];
+      }
+  }
+}
+
+/* RESIKE res3c.f:3423 for SST on level lev (1 = finest) with CYCLES at
+ * multigrid depth m2: zero the increments and sources; for m2 >= 2 zero and
+ * recompute the velocity gradients (DERFUN at this level); CROSKO + FUN1KO;
+ * REFCEN on level 1; MAKE_EPS + PRODKE; TEMDER of T, k, omega; the k, i, j
+ * direction cycles with SWEEPK; SOURKO + ADDSKE.  For m2 = 1 the velocity
  * gradients are the ones TURBEQ computed this cycle. */
-void orc_residu_sst(orc_block *b, const ff_params *p, int icycle) {
+void orc_residu_sst_lev(orc_block *b, const ff_params *p, int lev, int m2, int icycle) {
   dims_t d = dims_of(b);
   for (int s = FF_DRO; s <= FF_DEPS; s++) memset(b->a[s], 0, sizeof(double) * d.ntot);
   memset(b->a[FF_SRK], 0, sizeof(double) * d.ntot);
   memset(b->a[FF_FUN1], 0, sizeof(double) * d.ntot);
+  if (m2 >= 2) {
+    static const int z[] = {FF_OHMI, FF_W12, FF_W13, FF_W23, FF_DTDX, FF_DTDY, FF_DTDZ, FF_DKDX, FF_DKDY,
+                            FF_DKDZ, FF_DEDX, FF_DEDY, FF_DEDZ, FF_S11, FF_S12, FF_S13, FF_S22, FF_S23, FF_S33};
+    for (size_t q = 0; q < sizeof(z) / sizeof(z[0]); q++) memset(b->a[z[q]], 0, sizeof(double) * d.ntot);
+    orc_gradients(b, lev);
+  }
   crosko(b);
   fun1ko(b, p);
-  orc_refcen(b, p);
+  if (lev == 1) orc_refcen(b, p);
   double *tmp = calloc((size_t)d.ntot, sizeof(double));
   prodke(b, tmp);
-  for (int s = FF_DTDX; s <= FF_DTDZ; s++) memset(b->a[s], 0, sizeof(double) * d.ntot);
-  temder_field(b, 1, b->a[FF_TEMP], b->a[FF_DTDX], b->a[FF_DTDY], b->a[FF_DTDZ]);
-  for (int L = 0; L < d.ntot; L++) tmp[L] = b->a[FF_RK][L] / b->a[FF_RO][L];     /* DIVV12 */
-  temder_field(b, 1, tmp, b->a[FF_DKDX], b->a[FF_DKDY], b->a[FF_DKDZ]);
-  for (int L = 0; L < d.ntot; L++) tmp[L] = b->a[FF_REPS][L] / b->a[FF_RO][L];
-  temder_field(b, 1, tmp, b->a[FF_DEDX], b->a[FF_DEDY], b->a[FF_DEDZ]);
+  if (p->fullns) {
+    temder_field(b, lev, b->a[FF_TEMP], b->a[FF_DTDX], b->a[FF_DTDY], b->a[FF_DTDZ]);
+    for (int L = 0; L < d.ntot; L++) tmp[L] = b->a[FF_RK][L] / b->a[FF_RO][L];     /* DIVV12 */
+    temder_field(b, lev, tmp, b->a[FF_DKDX], b->a[FF_DKDY], b->a[FF_DKDZ]);
+    for (int L = 0; L < d.ntot; L++) tmp[L] = b->a[FF_REPS][L] / b->a[FF_RO][L];
+    temder_field(b, lev, tmp, b->a[FF_DEDX], b->a[FF_DEDY], b->a[FF_DEDZ]);
+  }
   free(tmp);
   const int order[3] = {3, 1, 2};
   for (int o = 0; o < 3; o++) {
     int dir = order[o];
-    orc_inlet_outlet(b, p, dir, icycle);
-    orc_flux_dir_sst(b, p, dir);
+    if (lev == 1) {
+      orc_inlet_outlet(b, p, dir, icycle);
+      orc_flux_dir_sst(b, p, dir);
+    } else {
+      flux_dir_sst_coarse(b, p, dir);
+    }
     sweepk(b, dir, dir == 2);
   }
   sourko_addske(b);
+}
+
+void orc_residu_sst(orc_block *b, const ff_params *p, int icycle) {
+  orc_residu_sst_lev(b, p, 1, 1, icycle);
 }
 
 /* LOCDTK imps3.f:807 (DTURB=1), IMSOKO imps3.f:972 and COPRKE imps3.f:1113
@@ -948,9 +1043,9 @@ static void cokegs(orc_block *b, const ff_params *p) {
 
 /* IMPS imps3.f:6 for SST (LUSGS=1, JRIMP=0): TIME3, LOCDTK, IMSOKO, COPRKE,
  * PRKEGS, DIKEGS, COKEGS, DRO/CP, DRK and DEPS times RO. */
-void orc_imps_sst(orc_block *b, const ff_params *p) {
+void orc_imps_sst_lev(orc_block *b, const ff_params *p, int lev) {
   dims_t d = dims_of(b);
-  orc_time3(b, p, p->cfl);
+  orc_time3(b, p, lev == 1 ? p->cfl : p->cfll);
   locdtk_imsoko_coprke(b, p);
   prkegs(b, p);
   dikegs(b, p);
@@ -965,9 +1060,11 @@ void orc_imps_sst(orc_block *b, const ff_params *p) {
       }
 }
 
+void orc_imps_sst(orc_block *b, const ff_params *p) { orc_imps_sst_lev(b, p, 1); }
+
 /* FIN res3c.f:1077-1208 (ITURB>=3, single phase) and the CYCLES limits
  * (ns3c.f:1553-1596, LOLIM(REPS,EPSLIM) included). */
-void orc_fin_limits_sst(orc_block *b, const ff_params *p) {
+static void fin_sst_core(orc_block *b, const ff_params *p) {
   dims_t d = dims_of(b);
   double *RK = b->a[FF_RK], *REPS = b->a[FF_REPS];
   for (int K = 1; K <= d.kmax; K++)
@@ -987,6 +1084,12 @@ void orc_fin_limits_sst(orc_block *b, const ff_params *p) {
       }
   for (int n = 0; n < d.ntot; n++) RK[n] = MAXD(RK[n], p->rklim);
   for (int n = 0; n < d.ntot; n++) REPS[n] = MAXD(REPS[n], p->epslim);
+}
+
+void orc_fin_limits_sst(orc_block *b, const ff_params *p) {
+  dims_t d = dims_of(b);
+  double *REPS = b->a[FF_REPS];
+  fin_sst_core(b, p);
   double *T = b->a[FF_TEMP], *U = b->a[FF_U], *V = b->a[FF_V], *W = b->a[FF_W], *PD = b->a[FF_PDIFF];
   double *P = b->a[FF_P];
   for (int K = 1; K <= d.kmax; K++) {
@@ -1037,4 +1140,131 @@ void orc_cycle_sst(orc_block *b, const ff_params *p, int icycle, double *resi5, 
   orc_fin_limits_sst(b, p);
   orc_boundi(b, p);
   orc_subin_sst(b, p, dromax);
+}
+
+/* ---- multigrid with k and omega (CYCLES ns3c.f:1607-2120) -------------- */
+
+/* TRANKE multi.f:434: restriction of RK, REPS (into RO2/RM2), EPS2, VIST and
+ * of DRK, DEPS into the forcing RKP2H/EPP2H over coarse cells 0..MAX+1, the
+ * interior RKOLD/EPSOLD copies and the ghost rings (same order as TRANSF). */
+void orc_tranke(orc_block *f, orc_block *c) {
+  dims_t df = dims_of(f), dc = dims_of(c);
+  static const int vs[4] = {FF_RK, FF_REPS, FF_EPS2, FF_VIST};
+  static const int rs[2] = {FF_DRK, FF_DEPS};
+  static const int ps[2] = {FF_RKP2H, FF_EPP2H};
+  const double *VOL = f->a[FF_VOL], *VOL2 = c->a[FF_VOL];
+  int kind = df.kmax == 1 ? 1 : 2;
+  for (int K = 0; K <= dc.kmax + 1; K++)
+    for (int J = 0; J <= dc.jmax + 1; J++)
+      for (int I = 0; I <= dc.imax + 1; I++) {
+        size_t N = IX(dc, I, J, K);
+        size_t ijk = IX(df, 2 * I - 1, 2 * J - 1, kind * K - kind + 1);
+        size_t imjm2 = df.kmax == 1 ? 0 : df.il;
+        size_t ipjk = ijk + 1, ijpk = ijk + df.is, ipjpk = ijk + df.is + 1;
+        size_t ijkp = ijk + imjm2, ipjpkp = ipjpk + imjm2, ijpkp = ijpk + imjm2, ipjkp = ipjk + imjm2;
+        double pvol = 1. / VOL2[N];
+#define R8(X) ((VOL[ipjpk] * X[ipjpk] + VOL[ijk] * X[ijk] + VOL[ipjk] * X[ipjk] + VOL[ijpk] * X[ijpk] + \
+                VOL[ipjpkp] * X[ipjpkp] + VOL[ijkp] * X[ijkp] + VOL[ipjkp] * X[ipjkp] + VOL[ijpkp] * X[ijpkp]) * pvol)
+        for (int v = 0; v < 4; v++) c->a[vs[v]][N] = R8(f->a[vs[v]]);
+        for (int v = 0; v < 2; v++) c->a[ps[v]][N] = R8(f->a[rs[v]]);
+#undef R8
+      }
+  for (int K = 1; K <= dc.kmax; K++)
+    for (int J = 1; J <= dc.jmax; J++)
+      for (int I = 1; I <= dc.imax; I++) {
+        size_t N = IX(dc, I, J, K);
+        c->a[FF_RKOLD][N] = c->a[FF_RK][N];
+        c->a[FF_EPSOLD][N] = c->a[FF_REPS][N];
+      }
+#define RING(N0, OFF)                                                            \
+  do {                                                                           \
+    size_t n0 = (N0);                                                            \
+    for (int v = 0; v < 2; v++) { c->a[ps[v]][n0] = 0.; c->a[ps[v]][n0 + (OFF)] = 0.; } \
+    for (int v = 0; v < 4; v++) c->a[vs[v]][n0 + (OFF)] = c->a[vs[v]][n0];       \
+  } while (0)
+  for (int K = -1; K <= dc.kmax + 2; K++)
+    for (int J = -1; J <= dc.jmax + 2; J++) RING(IX(dc, 0, J, K), -1);
+  for (int K = -1; K <= dc.kmax + 2; K++)
+    for (int J = -1; J <= dc.jmax + 2; J++) RING(IX(dc, dc.imax + 1, J, K), 1);
+  for (int K = -1; K <= dc.kmax + 2; K++)
+    for (int I = -1; I <= dc.imax + 2; I++) RING(IX(dc, I, dc.jmax + 1, K), dc.is);
+  for (int K = -1; K <= dc.kmax + 2; K++)
+    for (int I = -1; I <= dc.imax + 2; I++) RING(IX(dc, I, 0, K), -dc.is);
+  for (int J = -1; J <= dc.jmax + 2; J++)
+    for (int I = -1; I <= dc.imax + 2; I++) RING(IX(dc, I, J, 0), -dc.il);
+  for (int J = -1; J <= dc.jmax + 2; J++)
+    for (int I = -1; I <= dc.imax + 2; I++) RING(IX(dc, I, J, dc.kmax + 1), dc.il);
+#undef RING
+}
+
+/* FORCFU / ADDRES multi.f:1609/1686 for k and omega (ITURB>=3 branch). */
+void orc_forcfu_ke(orc_block *c) {
+  dims_t d = dims_of(c);
+  orc_forcfu(c);
+  for (int n = 0; n < d.ntot; n++) c->a[FF_RKP2H][n] = c->a[FF_RKP2H][n] - c->a[FF_DRK][n];
+  for (int n = 0; n < d.ntot; n++) c->a[FF_EPP2H][n] = c->a[FF_EPP2H][n] - c->a[FF_DEPS][n];
+}
+
+void orc_addres_ke(orc_block *c) {
+  dims_t d = dims_of(c);
+  orc_addres(c);
+  for (int n = 0; n < d.ntot; n++) c->a[FF_DRK][n] = c->a[FF_RKP2H][n] + c->a[FF_DRK][n];
+  for (int n = 0; n < d.ntot; n++) c->a[FF_DEPS][n] = c->a[FF_EPP2H][n] + c->a[FF_DEPS][n];
+}
+
+/* INTERT multi.f:2051 -> INTERO 2007: damped injection of the coarse k and
+ * omega corrections, RO += CC1*RO*DROK/(CC2*RO + |DROK|). */
+void orc_intert(orc_block *c, orc_block *f, const ff_params *pf) {
+  dims_t dc = dims_of(c), df = dims_of(f);
+  const int ss[2] = {FF_RK, FF_REPS}, so[2] = {FF_RKOLD, FF_EPSOLD};
+  const double cc[2] = {pf->cmgk, pf->cmgeps};
+  for (int q = 0; q < 2; q++) {
+    const double cc1 = cc[q], cc2 = cc1 + 1.E-7;
+    for (int K = 1; K <= df.kmax; K++)
+      for (int J = 1; J <= df.jmax; J++)
+        for (int I = 1; I <= df.imax; I++) {
+          size_t N = IX(dc, (I + 1) / 2, (J + 1) / 2, (K + 1) / 2), F = IX(df, I, J, K);
+          double drok = c->a[ss[q]][N] - c->a[so[q]][N];
+          double alpo = fabs(drok);
+          double *R = f->a[ss[q]];
+          R[F] = R[F] + cc1 * R[F] * drok / (cc2 * R[F] + alpo);
+        }
+  }
+}
+
+/* Coarse-level FIN (ns3c.f:1935-1990): FIN with k and omega, then UPLIM /
+ * LOLIM of T and LOLIMP (no PDTOP, as there). */
+void orc_fin_coarse_sst(orc_block *b, const ff_params *p) {
+  fin_sst_core(b, p);
+  temp_p_limits(b, p);
+}
+
+/* One multigrid SST cycle of CYCLES (same order as orc_mg_cycle). */
+void orc_mg_cycle_sst(orc_block **lv, int nlev, const ff_params *prm, int icycle, double *resi5, double *dromax) {
+  orc_block *b = lv[0];
+  orc_statim(b, &prm[0]);
+  orc_turbeq_sst(b, &prm[0]);
+  orc_residu_sst_lev(b, &prm[0], 1, 1, icycle);
+  orc_resl2(b, resi5);
+  orc_imps_sst_lev(b, &prm[0], 1);
+  orc_fin_limits_sst(b, &prm[0]);
+  for (int m = 1; m < nlev; m++) {
+    orc_block *f = lv[m - 1], *c = lv[m];
+    orc_statim(f, &prm[m - 1]);
+    orc_residu_sst_lev(f, &prm[m - 1], m, m + 1, icycle);
+    if (m == 1) orc_resl2(f, resi5);
+    if (m > 1) orc_addres_ke(f);
+    orc_transf(f, c);
+    orc_tranke(f, c);
+    orc_statim(c, &prm[m]);
+    orc_residu_sst_lev(c, &prm[m], m + 1, m + 1, icycle);
+    orc_forcfu_ke(c);
+    orc_addres_ke(c);
+    orc_imps_sst_lev(c, &prm[m], m + 1);
+    orc_fin_coarse_sst(c, &prm[m]);
+  }
+  for (int m = nlev - 1; m >= 1; m--) orc_interp_limits(lv[m], lv[m - 1], &prm[m - 1]);
+  reflec(b, &prm[0]);
+  orc_boundi(b, &prm[0]);
+  orc_subin_sst(b, &prm[0], dromax);
 }

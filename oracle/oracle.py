@@ -168,7 +168,8 @@ class OracleMG:
     def cycle(self, icycle):
         r = (ctypes.c_double * 5)()
         d = ctypes.c_double()
-        self.L.orc_mg_cycle(self._ptrs, len(self.levels), self._prms, icycle, r, ctypes.byref(d))
+        fn = self.L.orc_mg_cycle_sst if self._prms[0].iturb >= 3 else self.L.orc_mg_cycle
+        fn(self._ptrs, len(self.levels), self._prms, icycle, r, ctypes.byref(d))
         return np.array(r[:]), d.value
 
 

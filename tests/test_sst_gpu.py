@@ -136,3 +136,30 @@ def test_sst_fp32_lusgs_tracks_fp64(gpu_lib):
         a, b = interior(bg, d64[n]), interior(bg2, d32[n])
         assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-3, n
     g.close(); g2.close()
+
+
+@pytest.mark.parametrize("nlev,dims", [(2, (17, 9, 9)), (3, (33, 17, 17))])
+def test_sst_multigrid_cycles_match_oracle(gpu_lib, nlev, dims):
+    """SST FAS V-cycles (TRANKE, k-omega forcing, coarse RESIKE with FLUDKE
+    and first-order Roe, seven-equation coarse LU-SGS, INTERT)."""
+    from finflo_b200 import case
+    from oracle.oracle import OracleMG
+    lv_g, prms, fs = case.bump_case_mg(*dims, nlev=nlev, **SST)
+    lv_c, _, _ = case.bump_case_mg(*dims, nlev=nlev, **SST)
+    om = OracleMG(lv_c, prms)
+    om.start()
+    g = GpuSolver(0)
+    bid = g.add_levels(lv_g, prms)
+    for b in range(len(lv_g)):
+        g.upload(bid + b)
+    g.start(bid)
+    n = 12
+    hist = g.cycles(n, bid, icycle0=1, use_graph=True)
+    ref = np.array([om.cycle(i + 1)[0] for i in range(n)])
+    np.testing.assert_allclose(hist[:, :5], ref, rtol=1e-7)
+    d = g.download(bid, ["TEMP", "U", "V", "RK", "REPS"])
+    for nme in d:
+        a = interior(lv_g[0], d[nme]); b = interior(lv_c[0], lv_c[0].arrays[nme])
+        rel = np.linalg.norm(a - b) / (np.linalg.norm(b) + 1e-300)
+        assert rel <= 1e-9, (nme, rel)
+    g.close()
