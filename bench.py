@@ -1,17 +1,22 @@
 #!/usr/bin/env python
 """Benchmark of the FINFLO per-iteration hot path on B200.
 
-One step = one full single-grid iteration of the reference's CYCLES on one
-block (STATIM/BOUNDI, RESIDU + RESL2, IMPS with LU-SGS, FIN + limits, SUBIN).
-Metric: cell-iters/s = interior cells x completed cycles / seconds (device
+One step = one full cycle of the reference's CYCLES on the workload: for the
+default workload (the bump channel 128x64x64 with k-omega SST and a 3-level
+V-cycle) one FAS V-cycle -- STATIM, TURBEQ, RESIKE + RESL2, IMPS (LU-SGS),
+FIN on the fine level, the coarse-level TRANSF/TRANKE, RESIKE, FORCFU,
+ADDRES, IMPS, FIN, the INTERP/INTERT prolongation, BOUNDI and SUBIN.
+Metric: cell-iters/s = fine-grid cells x completed cycles / seconds (device
 time from CUDA events on the library's stream, max over ranks).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload sst-mg|bump|box]
 
-N > 1 runs as N independent replicas (one block per GPU, no data-path
-collective; the batched multi-block exchange is a separate path), reported as
-weak scaling.  The reference arm times the CPU restatement of the reference
-routines (the Fortran reference has no compiler here) on the host cores.
+N > 1 runs N independent replicas of the single-block workloads (no
+data-path collective), reported as weak scaling; the multi-block box
+workload spreads its blocks over the GPUs (strong scaling).  The reference
+arm times the CPU restatement of the reference routines (the Fortran
+reference has no compiler here) on the host cores.
 """
 from __future__ import annotations
 
@@ -27,9 +32,72 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = dict(ni=65, nj=33, nk=33)   # node counts -> 64 x 32 x 32 cells
-WORKLOAD_NAME = ("bump channel 64x32x32 cells, laminar Re=1e4 M=0.5, Roe+MUSCL(INTER=3), "
-                 "full NS, LU-SGS, single grid, FP64")
+WORKLOADS = {
+    "sst-mg": dict(
+        name=("bump channel 128x64x64 cells, k-omega SST (Re=1e6 per unit length, M=0.6, Tu=0.1%, "
+              "mu_t/mu=0.1, first cell 2e-6), 3-level V-cycle, Roe+MUSCL(INTER=3), LU-SGS, FP64"),
+        kind="mg", nodes=(129, 65, 65), nlev=3, bytes_per_cell=328.0, dtype="f64",
+        kw=dict(turbulence="sst", reynolds=1e6, mach=0.6, h1=2e-6, noise=1e-3, seed=1),
+        state=["TEMP", "U", "V", "W", "PDIFF", "RK", "REPS"]),
+    "bump": dict(
+        name=("bump channel 64x32x32 cells, laminar Re=1e4 M=0.5, Roe+MUSCL(INTER=3), full NS, LU-SGS, "
+              "single grid, FP64"),
+        kind="single", nodes=(65, 33, 33), nlev=1, bytes_per_cell=288.0, dtype="f64",
+        kw=dict(), state=["TEMP", "U", "V", "W", "PDIFF"]),
+}
+
+
+def build_case(wl, nodes=None):
+    """Blocks (finest first) and parameters of a single-block workload."""
+    from finflo_b200 import case
+    ni, nj, nk = nodes or wl["nodes"]
+    if wl["kind"] == "mg":
+        levels, prms, fs = case.bump_case_mg(ni, nj, nk, nlev=wl["nlev"], **wl["kw"])
+        return levels, prms
+    blk, prm, fs = case.bump_case(ni, nj, nk, **wl["kw"])
+    return [blk], [prm]
+
+
+def cpu_oracle_rate(seconds, wl):
+    """Cell-iters/s of the CPU oracle on the workload (a bounded sample:
+    whole cycles until `seconds` have passed, at least two)."""
+    from oracle.oracle import Oracle, OracleMG
+    levels, prms = build_case(wl)
+    o = OracleMG(levels, prms) if len(levels) > 1 else Oracle(levels[0], prms[0])
+    o.start()
+    o.cycle(1)
+    n = 0
+    t0 = time.perf_counter()
+    while True:
+        o.cycle(n + 2)
+        n += 1
+        el = time.perf_counter() - t0
+        if el > seconds and n >= 2:
+            break
+    return levels[0].interior_cells * n / el, n
+
+
+def _cpu_worker(args):
+    seconds, wname = args
+    sys.path.insert(0, ROOT)
+    return cpu_oracle_rate(seconds, WORKLOADS[wname])
+
+
+def cpu_all_cores(seconds, wname):
+    """The oracle as independent replica processes on the host cores (as many
+    as the cores and the free memory allow)."""
+    import multiprocessing as mp
+    ncores = os.cpu_count() or 1
+    try:
+        import psutil
+        per = 1.5e9 if WORKLOADS[wname]["kind"] == "mg" else 0.3e9
+        ncores = max(1, min(ncores, int(psutil.virtual_memory().available * 0.6 // per)))
+    except Exception:
+        pass
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(ncores) as pool:
+        res = pool.map(_cpu_worker, [(seconds, wname)] * ncores)
+    return sum(r for r, _ in res), ncores, sum(n for _, n in res)
 
 
 def _peaks():
@@ -107,53 +175,35 @@ def _barrier(ws):
         dist.barrier()
 
 
-def cpu_oracle_rate(seconds=15.0, wl=WORKLOAD, procs=1):
-    """Cell-iters/s of the CPU oracle on the bench workload (bounded sample)."""
-    from finflo_b200 import case
-    from oracle.oracle import Oracle
-    blk, prm, fs = case.bump_case(wl["ni"], wl["nj"], wl["nk"])
-    o = Oracle(blk, prm)
-    o.start()
-    o.cycle(1)
-    n = 0
-    t0 = time.perf_counter()
-    while True:
-        o.cycle(n + 2)
-        n += 1
-        el = time.perf_counter() - t0
-        if el > seconds:
-            break
-    return blk.interior_cells * n / el, n
-
-
-def _cpu_worker(args):
-    seconds, wl = args
-    sys.path.insert(0, ROOT)
-    r, n = cpu_oracle_rate(seconds, wl)
-    return r, n
-
-
-def cpu_all_cores(seconds=15.0, wl=WORKLOAD):
-    import multiprocessing as mp
-    ncores = os.cpu_count() or 1
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(ncores) as pool:
-        res = pool.map(_cpu_worker, [(seconds, wl)] * ncores)
-    return sum(r for r, _ in res), ncores, sum(n for _, n in res)
-
-
 def run_reference(args):
     ws, rank, local = _dist()
     if rank != 0:
         return 0
-    seconds = max(5.0, min(20.0, 2.0 * args.steps))
-    rate, cores, ncyc = cpu_all_cores(seconds)
+    seconds = max(10.0, min(40.0, 2.0 * args.steps))
+    if args.workload == "box":   # one process: the 24 blocks hold several GB of host memory
+        from finflo_b200 import case
+        from oracle.oracle import OracleMB
+        nb = tuple(int(x) for x in args.blocks.split(","))
+        blocks, prms, _ = case.periodic_box_case(nb=nb, lusgs_fp32=False)
+        om = OracleMB(blocks, prms)
+        om.start()
+        om.cycle(1)
+        ncyc, t0 = 0, time.perf_counter()
+        while ncyc < 1 or time.perf_counter() - t0 < seconds:
+            om.cycle(ncyc + 2)
+            ncyc += 1
+        rate = sum(b.interior_cells for b in blocks) * ncyc / (time.perf_counter() - t0)
+        cores = 1
+        wl = dict(name=BOX_NAME + " (oracle: FP64 LU-SGS)", dtype="f64")
+    else:
+        wl = WORKLOADS[args.workload]
+        rate, cores, ncyc = cpu_all_cores(seconds, args.workload)
     line = {
         "metric": "cell-iters/s", "value": rate, "unit": "cell-iters/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": wl["dtype"],
         "data": "synthetic (seeded bump-channel grid and noisy free stream)",
-        "config": {"workload": WORKLOAD_NAME, "parallelism": f"{cores} host processes (replicas)"},
+        "config": {"workload": wl["name"], "parallelism": f"{cores} host processes (replicas)"},
         "impl": "reference",
         "cpu_baseline": {"value": rate, "unit": "cell-iters/s", "cores": cores, "kind": "port",
                          "sample": f"{ncyc} cycles total over {cores} replica processes, ~{seconds:.0f}s each"},
@@ -170,17 +220,17 @@ def run_ours(args):
         import torch.distributed as dist
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-    from finflo_b200 import case
-    from finflo_b200.gpu import GpuSolver, FF_STAGE_RESIDUAL
-    wl = dict(WORKLOAD)
-    if args.grid:
-        wl["ni"], wl["nj"], wl["nk"] = (int(x) for x in args.grid.split(","))
-    blk, prm, fs = case.bump_case(wl["ni"], wl["nj"], wl["nk"])
+    from finflo_b200.gpu import GpuSolver, FF_STAGE_RESIDUAL, FF_STAGE_SWEEP
+    wl = WORKLOADS[args.workload]
+    nodes = tuple(int(x) for x in args.grid.split(",")) if args.grid else None
+    levels, prms = build_case(wl, nodes)
+    blk = levels[0]
     g = GpuSolver(local)
-    bid = g.add_block(blk, prm)
-    g.upload(bid)
+    bid = g.add_levels(levels, prms) if len(levels) > 1 else g.add_block(blk, prms[0])
+    for q in range(len(levels)):
+        g.upload(bid + q)
     g.start(bid)
-    g.cycles(1 + args.warmup, bid, icycle0=1)   # warm-up incl. graph capture
+    g.cycles(1 + args.warmup, bid, icycle0=1)   # warm-up incl. the sweep autotuner and graph capture
     g.sync()
     ncell = blk.interior_cells
     # ---- device-timed cycles -------------------------------------------
@@ -192,16 +242,19 @@ def run_ours(args):
     _barrier(ws)
     ms = _allreduce_max(ms, ws)
     value = ncell * args.steps * ws / (ms * 1e-3)
-    # ---- dominant kernel: the fused residual ---------------------------
+    # ---- dominant kernels: the fused residual and one LU-SGS sweep -------
     ms_res = g.time_stage(FF_STAGE_RESIDUAL, reps=20, bid=bid)
-    bytes_per_cell = 288.0   # algorithmic bytes of the laminar FP64 residual
+    bytes_per_cell = wl["bytes_per_cell"]   # algorithmic bytes of the FP64 residual
     achieved = bytes_per_cell * ncell / (ms_res * 1e-3) / 1e9
-    peak, kind = _peaks()
+    ms_sweep = g.time_stage(FF_STAGE_SWEEP, reps=5, bid=bid)
+    g.cycles(1, bid, icycle0=2)   # the sweep timing overwrote the increments
+    peak, pkind = _peaks()
     launches = g.cycle_launches(bid) * args.steps
     lk = g.lusgs_kind(bid)
-    sweep = dict(g.sweep_tuning(bid), chosen="cluster lines" if lk % 100 == 1 else "cooperative hyperplane")
+    sweep = dict(g.sweep_tuning(bid), chosen="cluster lines" if lk % 100 == 1 else "cooperative hyperplane",
+                 ms_per_sweep=ms_sweep)
     # ---- end to end through the C-ABI with host buffers ----------------
-    names_in = ["TEMP", "U", "V", "W", "PDIFF"]
+    names_in = wl["state"]
     host = {n: blk.arrays[n] for n in names_in}
     h2d = d2h = 0
     t0 = time.perf_counter()
@@ -218,23 +271,26 @@ def run_ours(args):
     line = {
         "metric": "cell-iters/s", "value": value, "unit": "cell-iters/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": wl["dtype"],
         "data": "synthetic (seeded bump-channel grid and noisy free stream)",
-        "config": {"workload": WORKLOAD_NAME if not args.grid else f"bump channel {blk.imax}x{blk.jmax}x{blk.kmax} cells (profiling size)",
-                   "cells_per_gpu": ncell, "parallelism": f"replicas x{ws}",
-                   "l2": "working set < L2 (cycle state resident)", "lusgs_sweep": sweep},
+        "config": {"workload": wl["name"] if not args.grid else
+                   f"{args.workload} at {blk.imax}x{blk.jmax}x{blk.kmax} cells (profiling size)",
+                   "cells_per_gpu": ncell, "levels": len(levels), "parallelism": f"replicas x{ws}",
+                   "l2": "state resident in HBM; per-cycle working set above L2 at the default size",
+                   "lusgs_sweep": sweep},
         "gpu_launches": launches,
-        "roofline": {"bound": "hbm", "kernel": "k_residual", "achieved": achieved, "peak": peak,
-                     "peak_kind": kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
-                     "ms_per_launch": ms_res, "bytes_per_cell": bytes_per_cell},
+        "roofline": {"bound": "hbm", "kernel": "k_residual_sst" if prms[0].iturb >= 3 else "k_residual",
+                     "achieved": achieved, "peak": peak, "peak_kind": pkind, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "ms_per_launch": ms_res,
+                     "bytes_per_cell": bytes_per_cell},
         "e2e": {"value": e2e, "unit": "cell-iters/s", "h2d_bytes_per_step": h2d // max(1, args.steps),
                 "d2h_bytes_per_step": d2h // max(1, args.steps)},
         "clocks": clocks,
     }
     if rank == 0 and not args.no_cpu and not args.grid:
-        rate, ncyc = cpu_oracle_rate(seconds=min(15.0, max(3.0, args.cpu_seconds)))
+        rate, ncyc = cpu_oracle_rate(max(3.0, args.cpu_seconds), wl)
         line["cpu_baseline"] = {"value": rate, "unit": "cell-iters/s", "cores": 1, "kind": "port",
-                                "sample": f"{ncyc} oracle cycles on the same 64x32x32 workload"}
+                                "sample": f"{ncyc} oracle cycles of the same workload on one core"}
     if rank == 0:
         print(json.dumps(line))
     g.close()
@@ -344,7 +400,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--grid", default="", help="node counts ni,nj,nk (profiling runs)")
-    ap.add_argument("--workload", default="bump", choices=["bump", "box"])
+    ap.add_argument("--workload", default="sst-mg", choices=["sst-mg", "bump", "box"])
     ap.add_argument("--blocks", default="4,3,2", help="block arrangement of the box workload")
     args = ap.parse_args()
     if args.warmup < 3:

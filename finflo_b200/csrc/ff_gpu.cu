@@ -1227,8 +1227,14 @@ int ff_time_stage(void* ctx, int blk, int stage, int reps, float* ms) {
   for (int r = 0; r < reps; r++) {
     if (stage == FF_STAGE_RESIDUAL) {
       dim3 g(nblk(b->imax, TI), nblk(b->jmax, TJ), nblk(b->kmax, TK));
-      k_residual<<<g, 128, 0, c->stream>>>(b->db, b->prm, 1);
+      if (b->prm.iturb >= 3)
+        k_residual_sst<<<g, 128, 0, c->stream>>>(b->db, b->prm, 1);
+      else
+        k_residual<<<g, 128, 0, c->stream>>>(b->db, b->prm, 1);
       c->nlaunch++;
+    } else if (stage == FF_STAGE_SWEEP) {
+      int rc = sweep(c, b, 1, b->prm.lusgs_fp32 != 0);
+      if (rc) return rc;
     } else if (stage == FF_STAGE_GRAD) {
       long ng = (long)(b->imax + 2) * (b->jmax + 2) * (b->kmax + 2);
       k_grad<<<nblk(ng, 128), 128, 0, c->stream>>>(b->db, 1);

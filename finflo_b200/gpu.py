@@ -25,7 +25,7 @@ _SRC = [os.path.join(_HERE, "csrc", f) for f in ("ff_gpu.cu", "ff_kernels.cuh", 
 NVCC_FLAGS = ["-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC", "-shared", "-std=c++17"]
 
-FF_STAGE_RESIDUAL, FF_STAGE_GRAD, FF_STAGE_STATE = 1, 2, 3
+FF_STAGE_RESIDUAL, FF_STAGE_GRAD, FF_STAGE_STATE, FF_STAGE_SWEEP = 1, 2, 3, 4
 FF_PHASE_CYCLE_A, FF_PHASE_BOUNDI_A, FF_PHASE_B, FF_PHASE_RECORD = 0, 1, 2, 3
 
 

@@ -29,7 +29,7 @@ extern "C" {
 #define FF_ABI_VERSION 2
 
 enum { FF_OK = 0, FF_ERR_CUDA = 1, FF_ERR_ARG = 2, FF_ERR_TIMEOUT = 3, FF_ERR_SIZE = 4 };
-enum { FF_STAGE_RESIDUAL = 1, FF_STAGE_GRAD = 2, FF_STAGE_STATE = 3 };
+enum { FF_STAGE_RESIDUAL = 1, FF_STAGE_GRAD = 2, FF_STAGE_STATE = 3, FF_STAGE_SWEEP = 4 };
 
 int ff_abi_version(void);
 const char *ff_last_error(void *ctx);
