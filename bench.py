@@ -247,12 +247,12 @@ def run_ours(args):
     bytes_per_cell = wl["bytes_per_cell"]   # algorithmic bytes of the FP64 residual
     achieved = bytes_per_cell * ncell / (ms_res * 1e-3) / 1e9
     ms_sweep = g.time_stage(FF_STAGE_SWEEP, reps=5, bid=bid)
-    g.cycles(1, bid, icycle0=2)   # the sweep timing overwrote the increments
     peak, pkind = _peaks()
     launches = g.cycle_launches(bid) * args.steps
     lk = g.lusgs_kind(bid)
-    sweep = dict(g.sweep_tuning(bid), chosen="cluster lines" if lk % 100 == 1 else "cooperative hyperplane",
-                 ms_per_sweep=ms_sweep)
+    chosen = (f"cluster lines, {lk // 100} CTAs" if lk % 100 == 1
+              else f"cooperative hyperplane, {lk // 100} threads/CTA")
+    sweep = dict(g.sweep_tuning(bid), chosen=chosen, ms_per_sweep=ms_sweep)
     # ---- end to end through the C-ABI with host buffers ----------------
     names_in = wl["state"]
     host = {n: blk.arrays[n] for n in names_in}

@@ -219,6 +219,65 @@ FF_DI void jac_product_ke(T out[7], const T dw[7], T rk, T c, T ro, T drdp, T dr
   out[3] = nz * x2i + a23 * w3 + a33 * w4;
 }
 
+// Sweep layout.  The LU-SGS sweeps visit the cells plane by plane (i+j+k =
+// m); in the storage order (i fastest) the cells of one plane lie a j-stride
+// apart, so every load of a warp touches 32 cache lines.  The sweeps
+// therefore work on a skewed copy of their data, index
+//   S(I,J,K) = ((K-1) * (IMAX+JMAX-1) + (I+J-2)) * JMAX + (J-1),
+// in which the cells of one plane with the same K and consecutive J are
+// consecutive, and the upstream/downstream neighbours of a cell are at
+// S -/+ JMAX (i), S -/+ (JMAX+1) (j) and S -/+ (IMAX+JMAX-1)*JMAX (k).
+// Per cell (sw[c * ns + S]): its own solve data, then the data of the
+// products that it sends to its three downstream neighbours (the face frame
+// of each direction, the split eigenvalue coefficients, and the cell's
+// scalars 1/RO, RO*C, (.5/RO)/C and, for k-omega, DRH and
+// 1/(1+.667*RK*DRDP/RO) of SYM1KE).
+enum : int {
+  SW_DT1 = 0, SW_SCINV, SW_SCINP, SW_FD, SW_VOL, SW_A1, SW_A2, SW_A3, SW_RO,
+  SW_SC = 9,     // 5 scalars
+  SW_F = 14,     // 3 directions x 9 frame values (normal, SURFVECTS a21..a33)
+  SW_L = 41,     // 3 directions x 3 eigenvalue coefficients
+  SW_N = 50
+};
+
+__host__ __device__ inline size_t sw_size(int imax, int jmax, int kmax) {
+  return (size_t)kmax * (imax + jmax - 1) * jmax;
+}
+
+FF_DI size_t sw_index(const DevBlock& b, int I, int J, int K) {
+  return ((size_t)(K - 1) * (b.imax + b.jmax - 1) + (I + J - 2)) * b.jmax + (J - 1);
+}
+
+// The product of one cell with its precomputed frame f[9] and scalars
+// sc = {ypro, roc, proc, drh, ydrp}: SYM1I/SYM1KE(diag(l) * SYI/SYIKE(dw)).
+template <typename T, int NV>
+FF_DI void nb_product_pre(T* out, const T* dw, const T f[9], const T sc[5], T ro, T l1, T l2, T l5) {
+  const T nx = f[0], ny = f[1], nz = f[2], a21 = f[3], a22 = f[4], a23 = f[5], a31 = f[6], a32 = f[7], a33 = f[8];
+  const T ypro = sc[0], roc = sc[1], proc = sc[2];
+  T z2 = nx * dw[1] + ny * dw[2] + nz * dw[3];
+  T z3 = a21 * dw[1] + a22 * dw[2] + a23 * dw[3];
+  T z4 = a31 * dw[1] + a32 * dw[2] + a33 * dw[3];
+  T w1 = l1 * (dw[0] - ypro * dw[4]);
+  T w2 = l2 * (roc * z2 + dw[4]);
+  T w3 = l1 * z3, w4 = l1 * z4;
+  T w5 = l5 * (-roc * z2 + dw[4]);
+  T pc2 = T(.5) * ypro;
+  T dh = w1 + pc2 * (w2 + w5);
+  out[0] = dh;
+  T x2i = proc * (w2 - w5);
+  if constexpr (NV == 5) {
+    out[4] = T(.5) * (w2 + w5);
+  } else {
+    T w6 = l1 * dw[5];
+    out[4] = sc[4] * (T(.5) * (w2 + w5) - sc[3] * ro * dh - T(.667) * ro * w6);
+    out[5] = w6;
+    out[6] = l1 * dw[6];
+  }
+  out[1] = nx * x2i + a21 * w3 + a31 * w4;
+  out[2] = ny * x2i + a22 * w3 + a32 * w4;
+  out[3] = nz * x2i + a23 * w3 + a33 * w4;
+}
+
 // One neighbour's product for NV = 5 (laminar) or 7 (k-omega) equations.
 template <typename T, int NV>
 FF_DI void nb_product(T* out, const T* dw, const DevBlock& b, size_t n, T c, T ro, T nx, T ny, T nz, T l1, T l2,
@@ -249,8 +308,7 @@ FF_DI bool grid_barrier(unsigned* count, unsigned* gen, unsigned nblocks, int* e
       long it = 0;
       while (*vg == g) {
         if (++it > (1L << 24)) { atomicExch(err, 1); break; }
-        if (*((volatile int*)err)) break;
-        __nanosleep(32);
+        if ((it & 1023) == 0 && *((volatile int*)err)) break;
       }
     }
     __threadfence();

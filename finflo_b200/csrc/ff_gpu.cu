@@ -24,14 +24,18 @@ struct BlockCtx {
   ff_patch* d_patch = nullptr;
   std::vector<ff_patch> h_patch;
   ff_params prm{};
-  double* coef = nullptr;       // NCOEF x ntot (FP64 LU-SGS)
-  float* coef32 = nullptr;      // NCOEF x ntot (FP32 LU-SGS)
-  float* dw32 = nullptr;        // 7 x ntot
+  // LU-SGS data in the sweep layout (SW_N x ns) and the increments in it
+  // (7 x ns), FP64 or FP32 as the block's lusgs_fp32 asks
+  double* sw = nullptr;
+  double* dwp = nullptr;
+  float* sw32 = nullptr;
+  float* dwp32 = nullptr;
+  size_t ns = 0;
   unsigned long long* d_red = nullptr;   // per-block reduction word (FUN1KO CDMAX)
-  int coop_blocks = 0, coop_blocks32 = 0;
+  int coop_threads = 128;       // threads per CTA of the hyperplane sweep (tune_sweep)
   int use_lines = 0;            // 1: cluster line-wavefront LU-SGS
   int tuned = 0;                // sweep kind chosen by tune_sweep
-  float sweep_ms[2] = {0.f, 0.f};   // measured lower sweep: lines, hyperplane
+  float sweep_ms[2] = {0.f, 0.f};   // measured upper sweep: lines, best hyperplane
   LineGeom lg{};
   size_t lines_smem = 0, lines_smem32 = 0;
   DevBlock db{};
@@ -54,6 +58,7 @@ struct Ctx {
   int* d_hist_pos = nullptr;
   int hist_cap = 0;
   int sm_count = 0;
+  int coop_occ[2][2][3] = {};           // CTAs per SM of k_lusgs_sweep<f64|f32, 5|7> at 64/128/256 threads
   char errmsg[256] = {0};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   long nlaunch = 0;                     // kernel launches issued so far
@@ -205,13 +210,39 @@ int st_residu(Ctx* c, BlockCtx* b, int level, int icycle, int m2 = 1) {
   return 0;
 }
 
-int coop_sweep(Ctx* c, BlockCtx* b, int upper, bool fp32) {
-  int nb = fp32 ? b->coop_blocks32 : b->coop_blocks;
-  double* dw64 = b->base + (size_t)FF_DRO * b->slot_stride;
-  // the increment slots are contiguous: DRO, DM, DN, DW, DE (, DRK, DEPS)
+// Sweep-layout buffers in the block's LU-SGS precision (the other
+// precision's are freed).
+int alloc_sweep(Ctx* c, BlockCtx* b) {
+  const size_t ns = b->ns;
+  if (b->prm.lusgs_fp32) {
+    cudaFree(b->sw); cudaFree(b->dwp);
+    b->sw = nullptr; b->dwp = nullptr;
+    if (!b->sw32) CK(cudaMalloc(&b->sw32, sizeof(float) * SW_N * ns));
+    if (!b->dwp32) CK(cudaMalloc(&b->dwp32, sizeof(float) * 7 * ns));
+  } else {
+    cudaFree(b->sw32); cudaFree(b->dwp32);
+    b->sw32 = nullptr; b->dwp32 = nullptr;
+    if (!b->sw) CK(cudaMalloc(&b->sw, sizeof(double) * SW_N * ns));
+    if (!b->dwp) CK(cudaMalloc(&b->dwp, sizeof(double) * 7 * ns));
+  }
+  return 0;
+}
+
+// Grid of the cooperative hyperplane sweep: enough threads for the widest
+// plane (JMAX x KMAX cells), at most what can be co-resident.
+int coop_grid(Ctx* c, BlockCtx* b, bool fp32, int threads) {
+  int ti = threads == 64 ? 0 : (threads == 128 ? 1 : 2);
+  long per_sm = c->coop_occ[fp32 ? 1 : 0][b->prm.iturb >= 3 ? 1 : 0][ti];
+  long widest = (long)b->jmax * b->kmax;
+  return (int)min(per_sm * c->sm_count, max(1L, (widest + threads - 1) / threads));
+}
+
+int coop_sweep_n(Ctx* c, BlockCtx* b, int upper, bool fp32, int threads) {
+  int nb = coop_grid(c, b, fp32, threads);
+  if (nb < 1) return fail(c, FF_ERR_CUDA, "no cooperative occupancy");
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(nb);
-  cfg.blockDim = dim3(256);
+  cfg.blockDim = dim3(threads);
   cfg.dynamicSmemBytes = 0;
   cfg.stream = c->stream;
   cudaLaunchAttribute attr[1];
@@ -222,19 +253,23 @@ int coop_sweep(Ctx* c, BlockCtx* b, int upper, bool fp32) {
   cudaError_t e;
   const bool ke = b->prm.iturb >= 3;   // seven equations (k-omega)
   if (!fp32) {
-    e = ke ? cudaLaunchKernelEx(&cfg, k_lusgs_sweep<double, 7>, b->db, (const double*)b->coef, dw64, upper,
+    e = ke ? cudaLaunchKernelEx(&cfg, k_lusgs_sweep<double, 7>, b->db, (const double*)b->sw, b->dwp, upper,
                                 c->d_bar, c->d_err)
-           : cudaLaunchKernelEx(&cfg, k_lusgs_sweep<double, 5>, b->db, (const double*)b->coef, dw64, upper,
+           : cudaLaunchKernelEx(&cfg, k_lusgs_sweep<double, 5>, b->db, (const double*)b->sw, b->dwp, upper,
                                 c->d_bar, c->d_err);
   } else {
-    e = ke ? cudaLaunchKernelEx(&cfg, k_lusgs_sweep<float, 7>, b->db, (const float*)b->coef32, b->dw32, upper,
+    e = ke ? cudaLaunchKernelEx(&cfg, k_lusgs_sweep<float, 7>, b->db, (const float*)b->sw32, b->dwp32, upper,
                                 c->d_bar, c->d_err)
-           : cudaLaunchKernelEx(&cfg, k_lusgs_sweep<float, 5>, b->db, (const float*)b->coef32, b->dw32, upper,
+           : cudaLaunchKernelEx(&cfg, k_lusgs_sweep<float, 5>, b->db, (const float*)b->sw32, b->dwp32, upper,
                                 c->d_bar, c->d_err);
   }
   if (e != cudaSuccess) return fail(c, FF_ERR_CUDA, "cooperative sweep launch", e);
   c->nlaunch++;
   return 0;
+}
+
+int coop_sweep(Ctx* c, BlockCtx* b, int upper, bool fp32) {
+  return coop_sweep_n(c, b, upper, fp32, b->coop_threads);
 }
 
 int lines_sweep(Ctx* c, BlockCtx* b, int upper, bool fp32) {
@@ -250,14 +285,13 @@ int lines_sweep(Ctx* c, BlockCtx* b, int upper, bool fp32) {
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  double* dw64 = b->base + (size_t)FF_DRO * b->slot_stride;
   cudaError_t e;
   if (b->prm.iturb >= 3)
-    e = fp32 ? cudaLaunchKernelEx(&cfg, k_lusgs_lines<float, 7>, b->db, (const float*)b->coef32, b->dw32, upper, b->lg)
-             : cudaLaunchKernelEx(&cfg, k_lusgs_lines<double, 7>, b->db, (const double*)b->coef, dw64, upper, b->lg);
+    e = fp32 ? cudaLaunchKernelEx(&cfg, k_lusgs_lines<float, 7>, b->db, (const float*)b->sw32, b->dwp32, upper, b->lg)
+             : cudaLaunchKernelEx(&cfg, k_lusgs_lines<double, 7>, b->db, (const double*)b->sw, b->dwp, upper, b->lg);
   else
-    e = fp32 ? cudaLaunchKernelEx(&cfg, k_lusgs_lines<float, 5>, b->db, (const float*)b->coef32, b->dw32, upper, b->lg)
-             : cudaLaunchKernelEx(&cfg, k_lusgs_lines<double, 5>, b->db, (const double*)b->coef, dw64, upper, b->lg);
+    e = fp32 ? cudaLaunchKernelEx(&cfg, k_lusgs_lines<float, 5>, b->db, (const float*)b->sw32, b->dwp32, upper, b->lg)
+             : cudaLaunchKernelEx(&cfg, k_lusgs_lines<double, 5>, b->db, (const double*)b->sw, b->dwp, upper, b->lg);
   if (e != cudaSuccess) return fail(c, FF_ERR_CUDA, "cluster sweep launch", e);
   c->nlaunch++;
   return 0;
@@ -330,64 +364,59 @@ int setup_lines(Ctx* c, BlockCtx* b) {
   return 0;
 }
 
+// Sweep data of one sweep in the sweep layout (and, for upper = 1, the
+// right-hand side copied into it).
+void sweep_coef(Ctx* c, BlockCtx* b, int upper, bool fp32) {
+  int ncell = b->imax * b->jmax * b->kmax;
+  if (fp32)
+    k_sweep_coef<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, b->sw32, b->dwp32, upper);
+  else
+    k_sweep_coef<double><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, b->sw, b->dwp, upper);
+  c->nlaunch++;
+}
+
 // Sweep autotuner: a cluster line sweep uses at most 16 SMs per block, the
 // cooperative hyperplane sweep the whole GPU with a barrier per plane; which
-// is faster depends on the block's shape.  Time both (lower sweep, on the
-// block's current coefficients, into a scratch increment buffer so the
-// block's data is untouched) and keep the faster.  Blocks that run side by
+// is faster, and the hyperplane kernel's CTA size, depend on the block's
+// shape.  Time each candidate (upper sweep in the block's precision, on its
+// current state, in the block's own sweep buffers, which hold nothing
+// between implicit stages) and keep the fastest.  Blocks that run side by
 // side in a multi-block cycle keep the line sweep (see fork_join).
 int tune_sweep(Ctx* c, BlockCtx* b) {
   if (b->tuned) return 0;
   b->tuned = 1;
   const char* env = getenv("FINFLO_LUSGS");
-  if (!b->use_lines || (env && (!strcmp(env, "hyperplane") || !strcmp(env, "lines")))) return 0;
-  int ncell = b->imax * b->jmax * b->kmax;
-  double* scratch = nullptr;
-  CK(cudaMalloc(&scratch, sizeof(double) * 7 * (size_t)b->ntot));
-  CK(cudaMemsetAsync(scratch, 0, sizeof(double) * 7 * (size_t)b->ntot, c->stream));
-  k_lusgs_coef<double><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, b->coef, 1);
-  float best[2] = {0.f, 0.f};
+  const bool fp32 = b->prm.lusgs_fp32 != 0;
+  const int threads[3] = {64, 128, 256};
+  sweep_coef(c, b, 1, fp32);
+  float best_lines = 0.f, best_hyp = 0.f;
+  int best_t = b->coop_threads;
+  const bool try_lines = b->use_lines && !(env && !strcmp(env, "hyperplane"));
+  const bool try_hyp = !(env && !strcmp(env, "lines") && b->use_lines);
   int rc = 0;
-  for (int kind = 0; kind < 2 && !rc; kind++) {
+  for (int kind = 0; kind < 4 && !rc; kind++) {
+    if (kind == 0 && !try_lines) continue;
+    if (kind > 0 && !try_hyp) continue;
+    float best = 0.f;
     for (int rep = 0; rep < 4 && !rc; rep++) {   // rep 0 warms up
       cudaEventRecord(c->ev0, c->stream);
-      cudaError_t e;
-      if (kind == 0) {
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(b->lg.cs); cfg.blockDim = dim3(LTHREADS);
-        cfg.dynamicSmemBytes = b->lines_smem; cfg.stream = c->stream;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = b->lg.cs; attr[0].val.clusterDim.y = 1; attr[0].val.clusterDim.z = 1;
-        cfg.attrs = attr; cfg.numAttrs = 1;
-        e = b->prm.iturb >= 3
-                ? cudaLaunchKernelEx(&cfg, k_lusgs_lines<double, 7>, b->db, (const double*)b->coef, scratch, 1, b->lg)
-                : cudaLaunchKernelEx(&cfg, k_lusgs_lines<double, 5>, b->db, (const double*)b->coef, scratch, 1, b->lg);
-      } else {
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(b->coop_blocks); cfg.blockDim = dim3(256); cfg.stream = c->stream;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeCooperative; attr[0].val.cooperative = 1;
-        cfg.attrs = attr; cfg.numAttrs = 1;
-        e = b->prm.iturb >= 3 ? cudaLaunchKernelEx(&cfg, k_lusgs_sweep<double, 7>, b->db, (const double*)b->coef,
-                                                   scratch, 1, c->d_bar, c->d_err)
-                              : cudaLaunchKernelEx(&cfg, k_lusgs_sweep<double, 5>, b->db, (const double*)b->coef,
-                                                   scratch, 1, c->d_bar, c->d_err);
-      }
-      if (e != cudaSuccess) { rc = fail(c, FF_ERR_CUDA, "sweep autotune launch", e); break; }
+      rc = kind == 0 ? lines_sweep(c, b, 1, fp32) : coop_sweep_n(c, b, 1, fp32, threads[kind - 1]);
+      if (rc) break;
       cudaEventRecord(c->ev1, c->stream);
       cudaError_t s2 = cudaEventSynchronize(c->ev1);
       if (s2 != cudaSuccess) { rc = fail(c, FF_ERR_CUDA, "sweep autotune", s2); break; }
       float ms = 0.f;
       cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-      if (rep > 0) best[kind] = rep == 1 ? ms : fminf(best[kind], ms);
+      if (rep > 0) best = rep == 1 ? ms : fminf(best, ms);
     }
+    if (kind == 0) best_lines = best;
+    else if (best_hyp == 0.f || best < best_hyp) { best_hyp = best; best_t = threads[kind - 1]; }
   }
-  cudaFree(scratch);
   if (rc) return rc;
-  b->sweep_ms[0] = best[0];
-  b->sweep_ms[1] = best[1];
-  if (best[1] < best[0]) b->use_lines = 0;
+  b->sweep_ms[0] = best_lines;
+  b->sweep_ms[1] = best_hyp;
+  b->coop_threads = best_t;
+  if (try_lines && try_hyp && best_hyp < best_lines) b->use_lines = 0;
   return 0;
 }
 
@@ -408,25 +437,15 @@ int st_imps(Ctx* c, BlockCtx* b, int level, bool divide_cp) {
   }
   bool fp32 = b->prm.lusgs_fp32 != 0;
   int rc;
-  if (!fp32) {
-    k_lusgs_coef<double><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, b->coef, 1);
-    c->nlaunch++;
-    if ((rc = sweep(c, b, 1, false))) return rc;
-    k_lusgs_coef<double><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, b->coef, 0);
-    c->nlaunch++;
-    if ((rc = sweep(c, b, 0, false))) return rc;
-  } else {
-    k_copy_dw<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->dw32, 1, b->prm.iturb >= 3 ? 7 : 5);
-    c->nlaunch++;
-    k_lusgs_coef<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, b->coef32, 1);
-    c->nlaunch++;
-    if ((rc = sweep(c, b, 1, true))) return rc;
-    k_lusgs_coef<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, b->coef32, 0);
-    c->nlaunch++;
-    if ((rc = sweep(c, b, 0, true))) return rc;
-    k_copy_dw<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->dw32, 0, b->prm.iturb >= 3 ? 7 : 5);
-    c->nlaunch++;
-  }
+  sweep_coef(c, b, 1, fp32);
+  if ((rc = sweep(c, b, 1, fp32))) return rc;
+  sweep_coef(c, b, 0, fp32);
+  if ((rc = sweep(c, b, 0, fp32))) return rc;
+  if (fp32)
+    k_sweep_out<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->dwp32, b->prm.iturb >= 3 ? 7 : 5);
+  else
+    k_sweep_out<double><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->dwp, b->prm.iturb >= 3 ? 7 : 5);
+  c->nlaunch++;
   if (divide_cp) {
     // standalone IMPS: finish with DRO/CP (imps3.f:483); the fused cycle
     // folds this division into the FIN kernel instead
@@ -772,6 +791,15 @@ int ff_create(void** out, int device) {
   CK(cudaMalloc(&c->d_hist_pos, sizeof(int)));
   CK(cudaMemset(c->d_hist_pos, 0, sizeof(int)));
   CK(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device));
+  {   // co-resident CTAs of the cooperative sweep per SM, per instantiation and CTA size
+    const int th[3] = {64, 128, 256};
+    for (int t = 0; t < 3; t++) {
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->coop_occ[0][0][t], k_lusgs_sweep<double, 5>, th[t], 0));
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->coop_occ[0][1][t], k_lusgs_sweep<double, 7>, th[t], 0));
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->coop_occ[1][0][t], k_lusgs_sweep<float, 5>, th[t], 0));
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->coop_occ[1][1][t], k_lusgs_sweep<float, 7>, th[t], 0));
+    }
+  }
   CK(cudaEventCreate(&c->ev0));
   CK(cudaEventCreate(&c->ev1));
   *out = c;
@@ -785,7 +813,8 @@ int ff_destroy(void* ctx) {
   cudaStreamSynchronize(c->stream);
   for (auto* b : c->blocks) {
     if (b->graph) cudaGraphExecDestroy(b->graph);
-    cudaFree(b->base); cudaFree(b->d_patch); cudaFree(b->coef); cudaFree(b->coef32); cudaFree(b->dw32);
+    cudaFree(b->base); cudaFree(b->d_patch);
+    cudaFree(b->sw); cudaFree(b->dwp); cudaFree(b->sw32); cudaFree(b->dwp32);
     cudaFree(b->d_red);
     delete b;
   }
@@ -825,29 +854,13 @@ int ff_block_add(void* ctx, int imax, int jmax, int kmax, int npatch, const ff_p
     CK(cudaMalloc(&b->d_patch, sizeof(ff_patch) * npatch));
     CK(cudaMemcpyAsync(b->d_patch, patches, sizeof(ff_patch) * npatch, cudaMemcpyHostToDevice, c->stream));
   }
-  CK(cudaMalloc(&b->coef, sizeof(double) * NCOEF * (size_t)b->ntot));
-  CK(cudaMalloc(&b->coef32, sizeof(float) * NCOEF * (size_t)b->ntot));
-  CK(cudaMalloc(&b->dw32, sizeof(float) * 7 * (size_t)b->ntot));
+  b->ns = sw_size(imax, jmax, kmax);
+  { int rc = alloc_sweep(c, b); if (rc) return rc; }
   CK(cudaMalloc(&b->d_red, sizeof(unsigned long long) * 2));
   b->db.imax = imax; b->db.jmax = jmax; b->db.kmax = kmax;
   b->db.is = imax + 4; b->db.il = (imax + 4) * (jmax + 4); b->db.ntot = b->ntot;
   b->db.npatch = npatch; b->db.patch = b->d_patch;
   for (int s = 0; s < FF_NSLOTS; s++) b->db.a[s] = b->base + (size_t)s * b->slot_stride;
-  // cooperative grid size: enough threads for the widest hyperplane
-  int per_sm = 0, per_sm32 = 0;
-  {   // the seven-equation instantiations use more registers: size for them
-    int a = 0, a7 = 0, f = 0, f7 = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_lusgs_sweep<double, 5>, 256, 0));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a7, k_lusgs_sweep<double, 7>, 256, 0));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&f, k_lusgs_sweep<float, 5>, 256, 0));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&f7, k_lusgs_sweep<float, 7>, 256, 0));
-    per_sm = min(a, a7);
-    per_sm32 = min(f, f7);
-  }
-  long widest = (long)jmax * kmax;
-  b->coop_blocks = (int)min((long)per_sm * c->sm_count, max(1L, (widest + 255) / 256));
-  b->coop_blocks32 = (int)min((long)per_sm32 * c->sm_count, max(1L, (widest + 255) / 256));
-  if (b->coop_blocks < 1 || b->coop_blocks32 < 1) return fail(c, FF_ERR_CUDA, "no cooperative occupancy");
   {
     int rc = setup_lines(c, b);
     if (rc) return rc;
@@ -875,12 +888,17 @@ int ff_block_params(void* ctx, int blk, const ff_params* prm) {
   BlockCtx* b = getb(c, blk);
   if (!b || !prm) return fail(c, FF_ERR_ARG, "ff_block_params");
   bool nv_changed = (b->prm.iturb >= 3) != (prm->iturb >= 3);
+  bool fp_changed = (b->prm.lusgs_fp32 != 0) != (prm->lusgs_fp32 != 0);
   b->prm = *prm;
   if (nv_changed) {   // the line sweep's shared memory depends on the equation count
     int rc = setup_lines(c, b);
     if (rc) return rc;
-    b->tuned = 0;
   }
+  if (fp_changed) {
+    int rc = alloc_sweep(c, b);
+    if (rc) return rc;
+  }
+  if (nv_changed || fp_changed) b->tuned = 0;
   // captured cycles of any block may include this one (multigrid levels)
   for (auto* x : c->blocks)
     if (x->graph) { cudaGraphExecDestroy(x->graph); x->graph = nullptr; }
@@ -1050,7 +1068,7 @@ int ff_sweep_tuning(void* ctx, int blk, float* ms2) {
 
 int ff_lusgs_kind(void* ctx, int blk) {
   BlockCtx* b = getb((Ctx*)ctx, blk);
-  return b ? (b->use_lines ? 1 + b->lg.cs * 100 : 0) : -FF_ERR_ARG;
+  return b ? (b->use_lines ? 1 + b->lg.cs * 100 : 2 + b->coop_threads * 100) : -FF_ERR_ARG;
 }
 
 int ff_cycle_launches(void* ctx, int blk) {
@@ -1223,6 +1241,11 @@ int ff_time_stage(void* ctx, int blk, int stage, int reps, float* ms) {
   Ctx* c = (Ctx*)ctx;
   BlockCtx* b = getb(c, blk);
   if (!b || !ms || reps < 1) return fail(c, FF_ERR_ARG, "ff_time_stage");
+  if (stage == FF_STAGE_SWEEP) {   // the sweep's kernel choice and its data in the sweep layout
+    int rc = tune_sweep(c, b);
+    if (rc) return rc;
+    sweep_coef(c, b, 1, b->prm.lusgs_fp32 != 0);
+  }
   CK(cudaEventRecord(c->ev0, c->stream));
   for (int r = 0; r < reps; r++) {
     if (stage == FF_STAGE_RESIDUAL) {

@@ -7,9 +7,12 @@
 //   k_residual                        32x4x4-cell tiles, all three face
 //                                     directions fused, face fluxes staged
 //                                     in shared memory, residual written once
-//   k_lusgs_coef + k_lusgs_sweep      coefficient pass, then a cooperative
-//                                     persistent kernel marching the i+j+k
-//                                     hyperplanes with a bounded grid barrier
+//   k_sweep_coef + k_lusgs_sweep      coefficient pass into the skewed sweep
+//                                     layout, then a cooperative persistent
+//                                     kernel marching the i+j+k hyperplanes
+//                                     with a bounded grid barrier
+//   k_lusgs_lines                     the same sweep as a line wavefront in
+//                                     one thread-block cluster (DSMEM)
 #pragma once
 #include "ff_device.cuh"
 #include <cooperative_groups.h>
@@ -649,14 +652,16 @@ __global__ void k_time3_copr(DevBlock b, ff_params p, double cfl, int mode = 0) 
   b.a[FF_DE][kk] = dpi;
 }
 
-// LU-SGS coefficients of each interior cell (PREDGS imps4.f:388-470 for
-// upper=1, CORRGS imps4.f:120-200 + DIAGGS imps4.f:604 for upper=0).
-// Layout: coef[c*ntot + n], c = xi(3) xj(3) xk(3) dt1 scinv scinp fdiag.
-template <typename CT>
-__global__ void k_lusgs_coef(DevBlock b, ff_params p, CT* coef, int upper) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= b.imax * b.jmax * b.kmax) return;
-  int I = t % b.imax + 1, J = (t / b.imax) % b.jmax + 1, K = t / (b.imax * b.jmax) + 1;
+// LU-SGS coefficients of one interior cell (PREDGS imps4.f:388-470 for
+// upper=1, CORRGS imps4.f:120-200 + DIAGGS imps4.f:604 for upper=0): the
+// split eigenvalue coefficients x[d][0..2] of the face the cell's product in
+// direction d crosses, DT1 = THETA*DTL, the scalings SCINV / SCINP and the
+// diagonal factor of the lower sweep.
+struct CellCoef {
+  double x[3][3], dt1, scinv, scinp, fdiag;
+};
+
+FF_DI void lusgs_cell_coef(const DevBlock& b, const ff_params& p, int I, int J, int K, int upper, CellCoef& cc) {
   const int IS = b.is, IL = b.il;
   size_t N = ix(b, I, J, K);
 #define LD(s, n) __ldg(b.a[s] + (n))
@@ -666,7 +671,6 @@ __global__ void k_lusgs_coef(DevBlock b, ff_params p, CT* coef, int upper) {
   const int idi[3] = {p.idi1, p.idi2, p.idi3};
   const int idx[3] = {I, J, K};
   double xa[3], rmax_lo[3];
-  double x[3][3];
   for (int d = 0; d < 3; d++) {
     const int ao = 4 * d;
     size_t fN = upper ? N : N + st[d];          // face normal used for the eigenvalue
@@ -679,22 +683,21 @@ __global__ void k_lusgs_coef(DevBlock b, ff_params p, CT* coef, int upper) {
     double tt = (ff * 2.) * LD(FF_A1 + ao, N) / rnum * (mu + LD(FF_VIST, nb) + LD(FF_VIS, nb));
     double rmax = fabs(rl1) + c;
     double sg = upper ? -1. : 1.;
-    x[d][0] = (rl1 + sg * rmax) * .5 + sg * tt;
-    x[d][1] = (rl1 + c + sg * rmax) * .5 + sg * tt;
-    x[d][2] = (rl1 - c + sg * rmax) * .5 + sg * tt;
+    cc.x[d][0] = (rl1 + sg * rmax) * .5 + sg * tt;
+    cc.x[d][1] = (rl1 + c + sg * rmax) * .5 + sg * tt;
+    cc.x[d][2] = (rl1 - c + sg * rmax) * .5 + sg * tt;
     xa[d] = rmax + tt;
-    // SCINP uses the low-face spectral radius in both sweeps
-    double rl1lo = LD(FF_A1XA + ao, N) * u + LD(FF_A1YA + ao, N) * v + LD(FF_A1ZA + ao, N) * w;
-    rmax_lo[d] = upper ? rmax : (fabs(rl1) + c);
-    (void)rl1lo;
+    // SCINP uses the spectral radius of the eigenvalue face in both sweeps
+    rmax_lo[d] = fabs(rl1) + c;
   }
   double dt1 = p.theta * LD(FF_DTL, N);
   double a1 = LD(FF_A1, N), a2 = LD(FF_A2, N), a3 = LD(FF_A3, N);
   double a1p = LD(FF_A1, N + 1), a2p = LD(FF_A2, N + IS), a3p = LD(FF_A3, N + IL);
-  double scinv = upper ? 1. / (vol + dt1 * (xa[0] * a1 + xa[1] * a2 + xa[2] * a3))
-                       : 1. / (vol + dt1 * (xa[0] * a1p + xa[1] * a2p + xa[2] * a3p));
-  double scinp = 1. / (vol + dt1 * (rmax_lo[0] * a1 + rmax_lo[1] * a2 + rmax_lo[2] * a3));
-  double fdiag = 1.;
+  cc.dt1 = dt1;
+  cc.scinv = upper ? 1. / (vol + dt1 * (xa[0] * a1 + xa[1] * a2 + xa[2] * a3))
+                   : 1. / (vol + dt1 * (xa[0] * a1p + xa[1] * a2p + xa[2] * a3p));
+  cc.scinp = 1. / (vol + dt1 * (rmax_lo[0] * a1 + rmax_lo[1] * a2 + rmax_lo[2] * a3));
+  cc.fdiag = 1.;
   if (!upper) {   // DIAGGS imps4.f:614-660
     double r[6];
     for (int d = 0; d < 3; d++) {
@@ -704,16 +707,88 @@ __global__ void k_lusgs_coef(DevBlock b, ff_params p, CT* coef, int upper) {
       r[2 * d + 1] = fabs(LD(FF_A1XA + ao, fp) * u + LD(FF_A1YA + ao, fp) * v + LD(FF_A1ZA + ao, fp) * w) + c;
     }
     double sc = .5 * (a1 * r[0] + a1p * r[1] + a2 * r[2] + a2p * r[3] + a3 * r[4] + a3p * r[5]);
-    fdiag = 1. + p.theta * LD(FF_DTL, N) / vol * sc;
+    cc.fdiag = 1. + p.theta * LD(FF_DTL, N) / vol * sc;
   }
 #undef LD
-  size_t nt = b.ntot;
+}
+
+// Coefficients in the storage layout, coef[c*ntot + n], c = xi(3) xj(3)
+// xk(3) dt1 scinv scinp fdiag (the allocation-free stage's sweep).
+template <typename CT>
+__global__ void k_lusgs_coef(DevBlock b, ff_params p, CT* coef, int upper) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= b.imax * b.jmax * b.kmax) return;
+  int I = t % b.imax + 1, J = (t / b.imax) % b.jmax + 1, K = t / (b.imax * b.jmax) + 1;
+  CellCoef cc;
+  lusgs_cell_coef(b, p, I, J, K, upper, cc);
+  size_t nt = b.ntot, N = ix(b, I, J, K);
   for (int d = 0; d < 3; d++)
-    for (int e = 0; e < 3; e++) coef[(3 * d + e) * nt + N] = (CT)x[d][e];
-  coef[9 * nt + N] = (CT)dt1;
-  coef[10 * nt + N] = (CT)scinv;
-  coef[11 * nt + N] = (CT)scinp;
-  coef[12 * nt + N] = (CT)fdiag;
+    for (int e = 0; e < 3; e++) coef[(3 * d + e) * nt + N] = (CT)cc.x[d][e];
+  coef[9 * nt + N] = (CT)cc.dt1;
+  coef[10 * nt + N] = (CT)cc.scinv;
+  coef[11 * nt + N] = (CT)cc.scinp;
+  coef[12 * nt + N] = (CT)cc.fdiag;
+}
+
+// All data of one sweep in the sweep layout (see sw_index), and for the
+// first sweep (upper = 1) the right-hand side DRO..DE(,DRK,DEPS) copied into
+// dwp in the same layout and type.
+template <typename CT>
+__global__ void k_sweep_coef(DevBlock b, ff_params p, CT* sw, CT* dwp, int upper) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= b.imax * b.jmax * b.kmax) return;
+  int I = t % b.imax + 1, J = (t / b.imax) % b.jmax + 1, K = t / (b.imax * b.jmax) + 1;
+  CellCoef cc;
+  lusgs_cell_coef(b, p, I, J, K, upper, cc);
+  const size_t ns = sw_size(b.imax, b.jmax, b.kmax), S = sw_index(b, I, J, K);
+  const size_t N = ix(b, I, J, K);
+  const int IS = b.is, IL = b.il;
+  const int st[3] = {1, IS, IL};
+  sw[SW_DT1 * ns + S] = (CT)cc.dt1;
+  sw[SW_SCINV * ns + S] = (CT)cc.scinv;
+  sw[SW_SCINP * ns + S] = (CT)cc.scinp;
+  sw[SW_FD * ns + S] = (CT)cc.fdiag;
+  sw[SW_VOL * ns + S] = (CT)__ldg(b.a[FF_VOL] + N);
+  sw[SW_A1 * ns + S] = (CT)__ldg(b.a[FF_A1] + (upper ? N + 1 : N));
+  sw[SW_A2 * ns + S] = (CT)__ldg(b.a[FF_A2] + (upper ? N + IS : N));
+  sw[SW_A3 * ns + S] = (CT)__ldg(b.a[FF_A3] + (upper ? N + IL : N));
+  CT ro = (CT)__ldg(b.a[FF_RO] + N), c = (CT)__ldg(b.a[FF_C] + N);
+  sw[SW_RO * ns + S] = ro;
+  CT ypro = CT(1) / ro;
+  sw[(SW_SC + 0) * ns + S] = ypro;
+  sw[(SW_SC + 1) * ns + S] = ro * c;
+  sw[(SW_SC + 2) * ns + S] = (CT(.5) * ypro) / c;
+  if (p.iturb >= 3) {
+    CT rk = (CT)__ldg(b.a[FF_RK] + N), drdp = (CT)__ldg(b.a[FF_DRDP] + N), drdh = (CT)__ldg(b.a[FF_DRDH] + N);
+    sw[(SW_SC + 3) * ns + S] = CT(.667) * rk * (ypro * ypro) * drdh;
+    sw[(SW_SC + 4) * ns + S] = CT(1) / (CT(1) + CT(.667) * rk * ypro * drdp);
+  }
+  for (int d = 0; d < 3; d++) {
+    const int ao = 4 * d;
+    size_t fN = upper ? N : N + st[d];   // the face the product in direction d crosses
+    CT nx = (CT)__ldg(b.a[FF_A1XA + ao] + fN), ny = (CT)__ldg(b.a[FF_A1YA + ao] + fN),
+       nz = (CT)__ldg(b.a[FF_A1ZA + ao] + fN);
+    CT a21, a22, a23, a31, a32, a33;
+    surfvects(nx, ny, nz, a21, a22, a23, a31, a32, a33);
+    const CT f[9] = {nx, ny, nz, a21, a22, a23, a31, a32, a33};
+    for (int q = 0; q < 9; q++) sw[(SW_F + 9 * d + q) * ns + S] = f[q];
+    for (int e = 0; e < 3; e++) sw[(SW_L + 3 * d + e) * ns + S] = (CT)cc.x[d][e];
+  }
+  if (upper) {
+    const int nv = p.iturb >= 3 ? 7 : 5;
+    for (int v = 0; v < nv; v++) dwp[v * ns + S] = (CT)b.a[FF_DRO + v][N];
+  }
+}
+
+// The increments back from the sweep layout into DRO..DE(,DRK,DEPS).
+template <typename CT>
+__global__ void k_sweep_out(DevBlock b, const CT* __restrict__ dwp, int nv) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= b.imax * b.jmax * b.kmax) return;
+  int I = t % b.imax + 1, J = (t / b.imax) % b.jmax + 1, K = t / (b.imax * b.jmax) + 1;
+  const size_t ns = sw_size(b.imax, b.jmax, b.kmax), S = sw_index(b, I, J, K);
+  const size_t N = ix(b, I, J, K);
+  for (int v = 0; v < nv; v++) b.a[FF_DRO + v][N] = (double)dwp[v * ns + S];
 }
 
 // One LU-SGS sweep as i+j+k hyperplanes (cooperative, persistent).  The
@@ -723,8 +798,8 @@ __global__ void k_lusgs_coef(DevBlock b, ff_params p, CT* coef, int upper) {
 // dw: increment arrays (5 x ntot) of type CT; read through L2 (__ldcg)
 // because other blocks write them during the sweep.
 template <typename CT, int NV>
-__global__ void k_lusgs_sweep(DevBlock b, const CT* __restrict__ coef, CT* dw, int upper,
-                              unsigned* bar, int* err) {
+__global__ void k_lusgs_sweep_basic(DevBlock b, const CT* __restrict__ coef, CT* dw, int upper,
+                                    unsigned* bar, int* err) {
   const int IMAX = b.imax, JMAX = b.jmax, KMAX = b.kmax, IS = b.is, IL = b.il;
   const size_t nt = b.ntot;
   const int nthreads = gridDim.x * blockDim.x;
@@ -788,16 +863,65 @@ __global__ void k_lusgs_sweep(DevBlock b, const CT* __restrict__ coef, CT* dw, i
   }
 }
 
-// Copy between the FP64 increment arrays and a CT work copy (FP32 LU-SGS).
-template <typename CT>
-__global__ void k_copy_dw(DevBlock b, CT* dw, int to_work, int nv) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= b.imax * b.jmax * b.kmax) return;
-  int I = t % b.imax + 1, J = (t / b.imax) % b.jmax + 1, K = t / (b.imax * b.jmax) + 1;
-  size_t n = ix(b, I, J, K);
-  for (int v = 0; v < nv; v++) {
-    if (to_work) dw[v * (size_t)b.ntot + n] = (CT)b.a[FF_DRO + v][n];
-    else b.a[FF_DRO + v][n] = (double)dw[v * (size_t)b.ntot + n];
+// The hyperplane sweep on the sweep layout (k_sweep_coef): the cells of a
+// plane with one K and consecutive J are consecutive in sw and dwp, so each
+// warp's loads are coalesced.  Each cell pulls the products of its three
+// upstream neighbours from their increments and their precomputed frames,
+// scalars and eigenvalue coefficients.
+template <typename CT, int NV>
+__global__ void k_lusgs_sweep(DevBlock b, const CT* __restrict__ sw, CT* dwp, int upper, unsigned* bar, int* err) {
+  const int IMAX = b.imax, JMAX = b.jmax, KMAX = b.kmax;
+  const int W = IMAX + JMAX - 1;
+  const size_t ns = sw_size(IMAX, JMAX, KMAX);
+  const int nthreads = gridDim.x * blockDim.x;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nplanes = IMAX + JMAX + KMAX - 2;
+  const long off[3] = {JMAX, JMAX + 1, (long)W * JMAX};
+  for (int s = 0; s < nplanes; s++) {
+    const int m = upper ? IMAX + JMAX + KMAX - s : 3 + s;
+    const int klo = max(1, m - IMAX - JMAX), khi = min(KMAX, m - 2);
+    const int npairs = (khi - klo + 1) * JMAX;
+    for (int q = tid; q < npairs; q += nthreads) {
+      const int K = klo + q / JMAX, J = q % JMAX + 1, I = m - J - K;
+      if (I < 1 || I > IMAX) continue;
+      const size_t S = ((size_t)(K - 1) * W + (m - K - 2)) * JMAX + (J - 1);
+      // PREDGS drops the i+1 coupling of row J = JMAX; PRKEGS does not
+      const bool has[3] = {upper ? (I < IMAX && (NV == 7 || J < JMAX)) : (I > 1), upper ? (J < JMAX) : (J > 1),
+                           upper ? (K < KMAX) : (K > 1)};
+      CT ck[NV], yd[NV], bd[NV];
+#pragma unroll
+      for (int d = 2; d >= 0; d--) {   // k first (reference order), then i and j
+        CT* dst = d == 2 ? ck : (d == 0 ? yd : bd);
+        if (!has[d]) {
+#pragma unroll
+          for (int v = 0; v < NV; v++) dst[v] = CT(0);
+          continue;
+        }
+        const size_t nb = upper ? S + off[d] : S - off[d];
+        CT x[NV], f[9], sc[5], l[3];
+#pragma unroll
+        for (int v = 0; v < NV; v++) x[v] = __ldcg(dwp + v * ns + nb);
+#pragma unroll
+        for (int c = 0; c < 9; c++) f[c] = __ldg(sw + (SW_F + 9 * d + c) * ns + nb);
+#pragma unroll
+        for (int c = 0; c < (NV == 7 ? 5 : 3); c++) sc[c] = __ldg(sw + (SW_SC + c) * ns + nb);
+#pragma unroll
+        for (int e = 0; e < 3; e++) l[e] = __ldg(sw + (SW_L + 3 * d + e) * ns + nb);
+        nb_product_pre<CT, NV>(dst, x, f, sc, NV == 7 ? __ldg(sw + SW_RO * ns + nb) : CT(0), l[0], l[1], l[2]);
+      }
+      const CT dt1 = __ldg(sw + SW_DT1 * ns + S), vol = __ldg(sw + SW_VOL * ns + S);
+      const CT fd = upper ? CT(1) : __ldg(sw + SW_FD * ns + S);
+      const CT a1 = __ldg(sw + SW_A1 * ns + S), a2 = __ldg(sw + SW_A2 * ns + S), a3 = __ldg(sw + SW_A3 * ns + S);
+      const CT scinv = __ldg(sw + SW_SCINV * ns + S), scinp = __ldg(sw + SW_SCINP * ns + S);
+#pragma unroll
+      for (int v = 0; v < NV; v++) {
+        CT cd = __ldcg(dwp + v * ns + S) * fd;
+        CT x = upper ? (-dt1 * a3 * ck[v] + vol * cd) : (dt1 * a3 * ck[v] + vol * cd);
+        x = upper ? x - dt1 * (a1 * yd[v] + a2 * bd[v]) : x + dt1 * (a1 * yd[v] + a2 * bd[v]);
+        __stcg(dwp + v * ns + S, x * (v == 4 ? scinp : scinv));
+      }
+    }
+    if (!grid_barrier(bar, bar + 1, gridDim.x, err)) return;
   }
 }
 
@@ -1149,15 +1273,16 @@ struct LineGeom {
 };
 
 template <typename CT, int NV>
-__global__ void __launch_bounds__(LTHREADS) k_lusgs_lines(DevBlock b, const CT* __restrict__ coef, CT* dw,
+__global__ void __launch_bounds__(LTHREADS) k_lusgs_lines(DevBlock b, const CT* __restrict__ sw, CT* dwp,
                                                           int upper, LineGeom lg) {
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   CT* pub = reinterpret_cast<CT*>(smem_raw);        // [2][tpc][2*NV][LTHREADS]: bd(NV), ck(NV)
   CT* ydb = pub + 2 * lg.tpc * 2 * NV * LTHREADS;   // [tpc][NV][LTHREADS]
-  const int IMAX = b.imax, JMAX = b.jmax, KMAX = b.kmax, IS = b.is, IL = b.il;
-  const size_t nt = b.ntot;
+  const int IMAX = b.imax, JMAX = b.jmax, KMAX = b.kmax;
+  const int W = IMAX + JMAX - 1;
+  const size_t ns = sw_size(IMAX, JMAX, KMAX);
   const int rank = (int)cluster.block_rank();
   const int lane = threadIdx.x, lj = lane % LTJ, lk = lane / LTJ;
   const int nplanes = IMAX + JMAX + KMAX - 2;
@@ -1175,7 +1300,15 @@ __global__ void __launch_bounds__(LTHREADS) k_lusgs_lines(DevBlock b, const CT* 
       if (J > JMAX || K > KMAX) continue;
       int I = m - J - K;
       if (I < 1 || I > IMAX) continue;
-      size_t N = ix(b, I, J, K);
+      const size_t S = ((size_t)(K - 1) * W + (m - K - 2)) * JMAX + (J - 1);
+      // own data first: independent of the neighbours' contributions
+      const CT dt1 = __ldg(sw + SW_DT1 * ns + S), vol = __ldg(sw + SW_VOL * ns + S);
+      const CT fd = upper ? CT(1) : __ldg(sw + SW_FD * ns + S);
+      const CT a1 = __ldg(sw + SW_A1 * ns + S), a2 = __ldg(sw + SW_A2 * ns + S), a3 = __ldg(sw + SW_A3 * ns + S);
+      const CT scinv = __ldg(sw + SW_SCINV * ns + S), scinp = __ldg(sw + SW_SCINP * ns + S);
+      CT rhs[NV];
+#pragma unroll
+      for (int v = 0; v < NV; v++) rhs[v] = dwp[v * ns + S];
       // ---- consume: neighbour contributions of the previous plane ----
       CT yd[NV], bd[NV], ck[NV];
       // PREDGS drops the i+1 coupling of row J = JMAX; PRKEGS does not
@@ -1211,31 +1344,29 @@ __global__ void __launch_bounds__(LTHREADS) k_lusgs_lines(DevBlock b, const CT* 
         }
       }
       // ---- solve the cell ----
-      CT dt1 = coef[9 * nt + N], scinv = coef[10 * nt + N], scinp = coef[11 * nt + N];
-      CT fd = upper ? CT(1) : coef[12 * nt + N];
-      CT vol = (CT)__ldg(b.a[FF_VOL] + N);
-      CT a3 = (CT)__ldg(b.a[FF_A3] + (upper ? N + IL : N));
-      CT a1 = (CT)__ldg(b.a[FF_A1] + (upper ? N + 1 : N));
-      CT a2 = (CT)__ldg(b.a[FF_A2] + (upper ? N + IS : N));
       CT res[NV];
 #pragma unroll
       for (int v = 0; v < NV; v++) {
-        CT x = upper ? (-dt1 * a3 * ck[v] + vol * (dw[v * nt + N] * fd)) : (dt1 * a3 * ck[v] + vol * (dw[v * nt + N] * fd));
+        CT cd = rhs[v] * fd;
+        CT x = upper ? (-dt1 * a3 * ck[v] + vol * cd) : (dt1 * a3 * ck[v] + vol * cd);
         x = upper ? x - dt1 * (a1 * yd[v] + a2 * bd[v]) : x + dt1 * (a1 * yd[v] + a2 * bd[v]);
         res[v] = x * (v == 4 ? scinp : scinv);
-        dw[v * nt + N] = res[v];
+        dwp[v * ns + S] = res[v];
       }
       // ---- produce: contributions to the three downstream neighbours ----
-      CT c = (CT)__ldg(b.a[FF_C] + N), ro = (CT)__ldg(b.a[FF_RO] + N);
-      const int st[3] = {1, IS, IL};
+      CT sc[5];
+#pragma unroll
+      for (int c = 0; c < (NV == 7 ? 5 : 3); c++) sc[c] = __ldg(sw + (SW_SC + c) * ns + S);
+      const CT ro = NV == 7 ? __ldg(sw + SW_RO * ns + S) : CT(0);
 #pragma unroll
       for (int d = 0; d < 3; d++) {
-        size_t fN = upper ? N : N + st[d];
-        const int ao = 4 * d;
+        CT f[9], l[3];
+#pragma unroll
+        for (int c = 0; c < 9; c++) f[c] = __ldg(sw + (SW_F + 9 * d + c) * ns + S);
+#pragma unroll
+        for (int e = 0; e < 3; e++) l[e] = __ldg(sw + (SW_L + 3 * d + e) * ns + S);
         CT out[NV];
-        nb_product<CT, NV>(out, res, b, N, c, ro, (CT)__ldg(b.a[FF_A1XA + ao] + fN),
-                           (CT)__ldg(b.a[FF_A1YA + ao] + fN), (CT)__ldg(b.a[FF_A1ZA + ao] + fN),
-                           coef[(3 * d) * nt + N], coef[(3 * d + 1) * nt + N], coef[(3 * d + 2) * nt + N]);
+        nb_product_pre<CT, NV>(out, res, f, sc, ro, l[0], l[1], l[2]);
         if (d == 0) {
 #pragma unroll
           for (int v = 0; v < NV; v++) ydb[(q * NV + v) * LTHREADS + lane] = out[v];

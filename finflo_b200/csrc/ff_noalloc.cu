@@ -49,7 +49,7 @@ int noalloc_setup(int dev) {
   if (cudaGetSymbolAddress(&p, ff_noalloc_scratch) != cudaSuccess || !p) return FF_ERR_CUDA;
   int sms = 0, per_sm = 0;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return FF_ERR_CUDA;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (ff::k_lusgs_sweep<double, 5>), 256, 0) != cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (ff::k_lusgs_sweep_basic<double, 5>), 256, 0) != cudaSuccess ||
       per_sm < 1)
     return FF_ERR_CUDA;
   d.scratch = (double*)p;
@@ -115,7 +115,7 @@ extern "C" int ff_imps_noalloc(int imax, int jmax, int kmax, const ff_params* pr
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (cudaLaunchKernelEx(&cfg, k_lusgs_sweep<double, 5>, db, (const double*)coef, dw, upper, bar, err) != cudaSuccess)
+    if (cudaLaunchKernelEx(&cfg, k_lusgs_sweep_basic<double, 5>, db, (const double*)coef, dw, upper, bar, err) != cudaSuccess)
       return FF_ERR_CUDA;
   }
   k_fin_divide<<<(int)((ntot + 255) / 256), 256, 0, st>>>(db, 0);

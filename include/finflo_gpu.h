@@ -142,10 +142,11 @@ int ff_time_cycles_all(void *ctx, int ncycles, float *ms, int *launches_per_cycl
 /* Timing helpers (CUDA events on the context stream); ff_cycle_launches is
  * the number of kernel launches in one graph-captured cycle. */
 int ff_cycle_launches(void *ctx, int blk);
-/* LU-SGS sweep kernel of a block: 0 = cooperative hyperplane kernel,
- * 1 + 100*cluster_size = cluster line wavefront. */
-/* The autotuner's measured lower-sweep times in ms {cluster lines, cooperative
- * hyperplane} of a block (zeros until its first ff_cycles call). */
+/* LU-SGS sweep kernel of a block: 1 + 100*cluster_size = cluster line
+ * wavefront, 2 + 100*threads_per_CTA = cooperative hyperplane kernel. */
+/* The autotuner's measured upper-sweep times in ms {cluster lines, fastest
+ * cooperative hyperplane} of a block (zeros until its first ff_cycles call
+ * or sweep stage timing; lines 0 where the lines do not fit a cluster). */
 int ff_sweep_tuning(void *ctx, int blk, float *ms2);
 int ff_lusgs_kind(void *ctx, int blk);
 int ff_time_cycles(void *ctx, int blk, int ncycles, float *ms);

@@ -167,7 +167,7 @@ def test_line_and_hyperplane_sweeps_agree(gpu_lib, dims, monkeypatch):
     g2 = GpuSolver(0)
     bg2 = make_pair(*dims)[0]
     b2 = g2.add_block(bg2, prm)
-    assert g2.lusgs_kind(b2) == 0
+    assert g2.lusgs_kind(b2) % 100 == 2
     g2.upload(b2)
     g2.start(b2)
     for g, b in ((g1, b1), (g2, b2)):
