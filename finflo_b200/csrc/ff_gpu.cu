@@ -37,7 +37,7 @@ struct BlockCtx {
   int tuned = 0;                // sweep kind chosen by tune_sweep
   float sweep_ms[2] = {0.f, 0.f};   // measured upper sweep: lines, best hyperplane
   LineGeom lg{};
-  size_t lines_smem = 0, lines_smem32 = 0;
+  bool lines_stage = false;     // the staged line sweep fits (one tile per thread group)
   DevBlock db{};
   cudaGraphExec_t graph = nullptr;
   int graph_fp32 = -1;
@@ -58,10 +58,12 @@ struct Ctx {
   int* d_hist_pos = nullptr;
   int hist_cap = 0;
   int sm_count = 0;
+  int smem_optin = 0;                   // shared memory a CTA may opt in to
   int coop_occ[2][2][3] = {};           // CTAs per SM of k_lusgs_sweep<f64|f32, 5|7> at 64/128/256 threads
   char errmsg[256] = {0};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   long nlaunch = 0;                     // kernel launches issued so far
+  bool side_by_side = false;            // inside fork_join's concurrent chains
   // multi-block: per-block streams for the concurrent chains inside a
   // captured cycle, the device block table and the connection work-list
   std::vector<cudaStream_t> side;
@@ -272,11 +274,21 @@ int coop_sweep(Ctx* c, BlockCtx* b, int upper, bool fp32) {
   return coop_sweep_n(c, b, upper, fp32, b->coop_threads);
 }
 
+template <typename CT, int NV>
+cudaError_t launch_lines(cudaLaunchConfig_t* cfg, BlockCtx* b, const CT* sw, CT* dwp, int upper, bool stage) {
+  return stage ? cudaLaunchKernelEx(cfg, k_lusgs_lines<CT, NV, true>, b->db, sw, dwp, upper, b->lg)
+               : cudaLaunchKernelEx(cfg, k_lusgs_lines<CT, NV, false>, b->db, sw, dwp, upper, b->lg);
+}
+
+// The staged line sweep for a block swept alone; the unstaged one when
+// several blocks' sweeps run side by side (fork_join).
 int lines_sweep(Ctx* c, BlockCtx* b, int upper, bool fp32) {
+  const bool stage = b->lines_stage && !c->side_by_side;
+  const int nv = b->prm.iturb >= 3 ? 7 : 5;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(b->lg.cs);
-  cfg.blockDim = dim3(LTHREADS);
-  cfg.dynamicSmemBytes = fp32 ? b->lines_smem32 : b->lines_smem;
+  cfg.blockDim = dim3(LTHREADS * b->lg.ng);
+  cfg.dynamicSmemBytes = lines_smem_bytes(nv, b->lg.tpc, fp32 ? sizeof(float) : sizeof(double), stage);
   cfg.stream = c->stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -286,39 +298,50 @@ int lines_sweep(Ctx* c, BlockCtx* b, int upper, bool fp32) {
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   cudaError_t e;
-  if (b->prm.iturb >= 3)
-    e = fp32 ? cudaLaunchKernelEx(&cfg, k_lusgs_lines<float, 7>, b->db, (const float*)b->sw32, b->dwp32, upper, b->lg)
-             : cudaLaunchKernelEx(&cfg, k_lusgs_lines<double, 7>, b->db, (const double*)b->sw, b->dwp, upper, b->lg);
+  if (nv == 7)
+    e = fp32 ? launch_lines<float, 7>(&cfg, b, b->sw32, b->dwp32, upper, stage)
+             : launch_lines<double, 7>(&cfg, b, b->sw, b->dwp, upper, stage);
   else
-    e = fp32 ? cudaLaunchKernelEx(&cfg, k_lusgs_lines<float, 5>, b->db, (const float*)b->sw32, b->dwp32, upper, b->lg)
-             : cudaLaunchKernelEx(&cfg, k_lusgs_lines<double, 5>, b->db, (const double*)b->sw, b->dwp, upper, b->lg);
+    e = fp32 ? launch_lines<float, 5>(&cfg, b, b->sw32, b->dwp32, upper, stage)
+             : launch_lines<double, 5>(&cfg, b, b->sw, b->dwp, upper, stage);
   if (e != cudaSuccess) return fail(c, FF_ERR_CUDA, "cluster sweep launch", e);
   c->nlaunch++;
   return 0;
 }
 
 constexpr int kMaxDev = 64;
-int g_lines_smem[kMaxDev][4];   // dynamic shared memory granted to k_lusgs_lines<f64|f32, 5|7>
+int g_lines_smem[kMaxDev][4];   // dynamic shared memory granted to k_lusgs_lines<f64|f32, 5|7, *>
 
-// Choose the LU-SGS sweep kernel of a block: the cluster line wavefront
-// when the (j,k) line tiles fit one cluster, else the cooperative hyperplane
-// kernel.
+template <typename CT, int NV>
+int lines_attr_set(Ctx* c, size_t smem) {
+  CK(cudaFuncSetAttribute(k_lusgs_lines<CT, NV, true>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  CK(cudaFuncSetAttribute(k_lusgs_lines<CT, NV, false>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  CK(cudaFuncSetAttribute(k_lusgs_lines<CT, NV, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CK(cudaFuncSetAttribute(k_lusgs_lines<CT, NV, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  return 0;
+}
+
+// Kernel attributes are per device, shared by all blocks: only raise them.
 template <int NV>
 int lines_attrs(Ctx* c, size_t sm64, size_t sm32) {
   int* g = g_lines_smem[c->device] + (NV == 7 ? 2 : 0);
-  CK(cudaFuncSetAttribute(k_lusgs_lines<double, NV>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-  CK(cudaFuncSetAttribute(k_lusgs_lines<float, NV>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   if ((int)sm64 > g[0]) {
-    CK(cudaFuncSetAttribute(k_lusgs_lines<double, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm64));
+    int rc = lines_attr_set<double, NV>(c, sm64);
+    if (rc) return rc;
     g[0] = (int)sm64;
   }
   if ((int)sm32 > g[1]) {
-    CK(cudaFuncSetAttribute(k_lusgs_lines<float, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm32));
+    int rc = lines_attr_set<float, NV>(c, sm32);
+    if (rc) return rc;
     g[1] = (int)sm32;
   }
   return 0;
 }
 
+// Choose the LU-SGS sweep kernel of a block: the cluster line wavefront
+// when the (j,k) line tiles fit one cluster, else the cooperative hyperplane
+// kernel.  The largest cluster that fits is taken; a smaller cluster only
+// means more tiles per CTA.
 int setup_lines(Ctx* c, BlockCtx* b) {
   LineGeom lg{};
   lg.ntj = (b->jmax + LTJ - 1) / LTJ;
@@ -329,16 +352,18 @@ int setup_lines(Ctx* c, BlockCtx* b) {
   for (int cs = 16; cs >= 1; cs /= 2) {
     int csz = min(cs, lg.ntiles);
     int tpc = (lg.ntiles + csz - 1) / csz;
-    // pub [2][tpc][2 NV] + ydb [tpc][NV] values per thread
-    size_t sm64 = (size_t)5 * nv * tpc * LTHREADS * sizeof(double);
-    size_t sm32 = (size_t)5 * nv * tpc * LTHREADS * sizeof(float);
-    if (sm64 > 200 * 1024) continue;
-    // kernel attributes are per device, shared by all blocks: only raise them
+    int ng = min(tpc, LMAX_TPC);
+    // staging needs one tile per thread group and room for the stage
+    bool stage = tpc == ng && tpc <= LMAX_TPC_STAGE &&
+                 lines_smem_bytes(nv, tpc, sizeof(double), true) <= (size_t)c->smem_optin;
+    size_t sm64 = lines_smem_bytes(nv, tpc, sizeof(double), stage);
+    size_t sm32 = lines_smem_bytes(nv, tpc, sizeof(float), stage);
+    if (sm64 > (size_t)c->smem_optin) continue;
     int rc = nv == 7 ? lines_attrs<7>(c, sm64, sm32) : lines_attrs<5>(c, sm64, sm32);
     if (rc) return rc;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(csz);
-    cfg.blockDim = dim3(LTHREADS);
+    cfg.blockDim = dim3(LTHREADS * ng);
     cfg.dynamicSmemBytes = sm64;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -346,24 +371,28 @@ int setup_lines(Ctx* c, BlockCtx* b) {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     int nclusters = 0;
-    cudaError_t e = nv == 7 ? cudaOccupancyMaxActiveClusters(&nclusters, k_lusgs_lines<double, 7>, &cfg)
-                            : cudaOccupancyMaxActiveClusters(&nclusters, k_lusgs_lines<double, 5>, &cfg);
+    cudaError_t e;
+    if (nv == 7)
+      e = stage ? cudaOccupancyMaxActiveClusters(&nclusters, k_lusgs_lines<double, 7, true>, &cfg)
+                : cudaOccupancyMaxActiveClusters(&nclusters, k_lusgs_lines<double, 7, false>, &cfg);
+    else
+      e = stage ? cudaOccupancyMaxActiveClusters(&nclusters, k_lusgs_lines<double, 5, true>, &cfg)
+                : cudaOccupancyMaxActiveClusters(&nclusters, k_lusgs_lines<double, 5, false>, &cfg);
     if (e != cudaSuccess || nclusters < 1) {
       cudaGetLastError();
       continue;
     }
     lg.cs = csz;
     lg.tpc = tpc;
+    lg.ng = ng;
     b->lg = lg;
-    b->lines_smem = sm64;
-    b->lines_smem32 = sm32;
+    b->lines_stage = stage;
     b->use_lines = 1;
     return 0;
   }
   b->use_lines = 0;
   return 0;
 }
-
 // Sweep data of one sweep in the sweep layout (and, for upper = 1, the
 // right-hand side copied into it).
 void sweep_coef(Ctx* c, BlockCtx* b, int upper, bool fp32) {
@@ -628,6 +657,7 @@ int fork_join(Ctx* c, int nb, F fn) {
   cudaStream_t main = c->stream;
   CK(cudaEventRecord(c->fork_ev, main));
   int rc = 0;
+  c->side_by_side = true;
   for (int n = 0; n < nb && !rc; n++) {
     CK(cudaStreamWaitEvent(c->side[n], c->fork_ev, 0));
     c->stream = c->side[n];
@@ -635,6 +665,7 @@ int fork_join(Ctx* c, int nb, F fn) {
     c->stream = main;
     CK(cudaEventRecord(c->side_ev[n], c->side[n]));
   }
+  c->side_by_side = false;
   c->stream = main;
   for (int n = 0; n < nb; n++) CK(cudaStreamWaitEvent(main, c->side_ev[n], 0));
   return rc;
@@ -791,6 +822,7 @@ int ff_create(void** out, int device) {
   CK(cudaMalloc(&c->d_hist_pos, sizeof(int)));
   CK(cudaMemset(c->d_hist_pos, 0, sizeof(int)));
   CK(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device));
+  CK(cudaDeviceGetAttribute(&c->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
   {   // co-resident CTAs of the cooperative sweep per SM, per instantiation and CTA size
     const int th[3] = {64, 128, 256};
     for (int t = 0; t < 3; t++) {

@@ -1260,94 +1260,174 @@ __global__ void k_maxabs_de(DevBlock b, unsigned long long* dm_bits) {
 // neighbour is on the same line (kept in shared memory), the j and k
 // neighbours are the lines (J -/+ 1, K) and (J, K -/+ 1), read at the next
 // plane from shared memory -- from another CTA's shared memory (DSMEM) when
-// the line belongs to another tile.  One cluster barrier per plane; the
-// published values are double-buffered so a plane reads only the previous
-// plane's outputs.  The triangular system is the reference's (incl. the
-// dropped i+1 coupling in row J = JMAX of PREDGS), so the result equals the
-// hyperplane and slab orders up to rounding.
+// the line belongs to another tile.  The triangular system is the
+// reference's (incl. the dropped i+1 coupling in row J = JMAX of PREDGS), so
+// the result equals the hyperplane and slab orders up to rounding.
+//
+// A CTA of the cluster holds tpc tiles, ng = min(tpc, 4) of them side by
+// side (ng x 128 threads; a thread group takes every ng-th tile).  One split
+// cluster barrier per plane: a thread arrives once its products are
+// published and waits only before the next plane.  With STAGE (one tile per
+// thread group) the thread starts, between arrive and wait, the
+// asynchronous copy (cp.async) of its next cell's sweep data (the SW_N
+// values of the sweep layout and the right-hand side) into its own
+// shared-memory slots, so the memory latency of the next plane overlaps the
+// barrier.  Without STAGE the cell data is read from global memory where it
+// is used: the variant for many blocks' sweeps running side by side, where
+// the other blocks' warps hide the latency and the smaller shared-memory
+// footprint keeps more CTAs resident.  The published values are
+// double-buffered, so a plane reads only the previous plane's outputs.
 // ---------------------------------------------------------------------------
 constexpr int LTJ = 16, LTK = 8, LTHREADS = LTJ * LTK;
+constexpr int LMAX_TPC = 4;          // tile groups per CTA (threads per CTA <= 512)
+constexpr int LMAX_TPC_STAGE = 2;    // staged: <= 256 threads, so up to 255 registers a thread
+constexpr int LSTAGE = SW_N + 7;     // staged values per thread: sweep data + right-hand side
 
 struct LineGeom {
   int ntj, ntk, ntiles, cs, tpc;   // tiles in j/k, cluster size, tiles per CTA
+  int ng;                          // thread groups of 128 per CTA (tiles in parallel)
+};
+
+// Shared memory of k_lusgs_lines: pub [2][tpc][2*NV][128] (j and k
+// products), ydb [tpc][NV][128] (i products), with STAGE (one tile per
+// thread group, ng == tpc) stage [LSTAGE][tpc*128].
+__host__ __device__ inline size_t lines_smem_bytes(int nv, int tpc, size_t elem, bool stage) {
+  return ((size_t)5 * nv + (stage ? LSTAGE : 0)) * tpc * LTHREADS * elem;
+}
+
+FF_DI void cp_async_ca(void* smem, const double* g) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(g) : "memory");
+}
+FF_DI void cp_async_ca(void* smem, const float* g) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(g) : "memory");
+}
+FF_DI void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+FF_DI void cluster_arrive_release() { asm volatile("barrier.cluster.arrive.release;\n" ::: "memory"); }
+FF_DI void cluster_wait_acquire() { asm volatile("barrier.cluster.wait.acquire;\n" ::: "memory"); }
+
+// Start the copy of one cell's sweep data into the thread's stage slots
+// (stride = threads per CTA).
+template <typename CT, int NV>
+FF_DI void lines_stage(CT* stg, int stride, const CT* __restrict__ sw, const CT* dwp, size_t ns, size_t S,
+                       int upper) {
+#pragma unroll
+  for (int c = 0; c < SW_N; c++) {
+    if (c == SW_FD && upper) continue;
+    if (NV == 5 && (c == SW_RO || c == SW_SC + 3 || c == SW_SC + 4)) continue;
+    cp_async_ca(stg + c * stride, sw + c * ns + S);
+  }
+#pragma unroll
+  for (int v = 0; v < NV; v++) cp_async_ca(stg + (SW_N + v) * stride, dwp + v * ns + S);
+}
+
+// A lane's line in one tile slot of its CTA, with the DSMEM sources of its
+// j and k neighbours' products (offsets within one pub buffer).
+template <typename CT>
+struct LineDesc {
+  bool ok, hj, hk;
+  int J, K;
+  const CT* srcj;
+  const CT* srck;
 };
 
 template <typename CT, int NV>
-__global__ void __launch_bounds__(LTHREADS) k_lusgs_lines(DevBlock b, const CT* __restrict__ sw, CT* dwp,
-                                                          int upper, LineGeom lg) {
+FF_DI LineDesc<CT> line_desc(const cooperative_groups::cluster_group& cluster, CT* pub, const LineGeom& lg,
+                             int JMAX, int KMAX, int upper, int rank, int q, int lj, int lk) {
+  LineDesc<CT> d;
+  d.ok = false;
+  d.hj = d.hk = false;
+  d.J = d.K = 0;
+  d.srcj = d.srck = pub;
+  const int t = q * lg.cs + rank;
+  if (t >= lg.ntiles) return d;
+  const int tj = t % lg.ntj, tk = t / lg.ntj;
+  d.J = tj * LTJ + lj + 1;
+  d.K = tk * LTK + lk + 1;
+  d.ok = d.J <= JMAX && d.K <= KMAX;
+  d.hj = upper ? (d.J < JMAX) : (d.J > 1);
+  d.hk = upper ? (d.K < KMAX) : (d.K > 1);
+  if (d.ok && d.hj) {   // line (J -/+ 1, K)
+    const int Jn = upper ? d.J + 1 : d.J - 1;
+    const int tn = tk * lg.ntj + (Jn - 1) / LTJ, ln = lk * LTJ + (Jn - 1) % LTJ;
+    d.srcj = cluster.map_shared_rank(pub, tn % lg.cs) + (tn / lg.cs) * 2 * NV * LTHREADS + ln;
+  }
+  if (d.ok && d.hk) {   // line (J, K -/+ 1)
+    const int Kn = upper ? d.K + 1 : d.K - 1;
+    const int tn = ((Kn - 1) / LTK) * lg.ntj + tj, ln = ((Kn - 1) % LTK) * LTJ + lj;
+    d.srck = cluster.map_shared_rank(pub, tn % lg.cs) + ((tn / lg.cs) * 2 * NV + NV) * LTHREADS + ln;
+  }
+  return d;
+}
+
+template <typename CT, int NV, bool STAGE>
+__global__ void __launch_bounds__(LTHREADS * (STAGE ? LMAX_TPC_STAGE : LMAX_TPC))
+    k_lusgs_lines(DevBlock b, const CT* __restrict__ sw, CT* dwp, int upper, LineGeom lg) {
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int tpc = lg.tpc, ng = lg.ng, nthr = ng * LTHREADS;
   CT* pub = reinterpret_cast<CT*>(smem_raw);        // [2][tpc][2*NV][LTHREADS]: bd(NV), ck(NV)
-  CT* ydb = pub + 2 * lg.tpc * 2 * NV * LTHREADS;   // [tpc][NV][LTHREADS]
+  CT* ydb = pub + 2 * tpc * 2 * NV * LTHREADS;      // [tpc][NV][LTHREADS]
+  CT* my = ydb + tpc * NV * LTHREADS + threadIdx.x; // stage [LSTAGE][nthr] (STAGE: ng == tpc)
   const int IMAX = b.imax, JMAX = b.jmax, KMAX = b.kmax;
   const int W = IMAX + JMAX - 1;
   const size_t ns = sw_size(IMAX, JMAX, KMAX);
   const int rank = (int)cluster.block_rank();
-  const int lane = threadIdx.x, lj = lane % LTJ, lk = lane / LTJ;
+  const int g0 = threadIdx.x / LTHREADS, lane = threadIdx.x % LTHREADS, lj = lane % LTJ, lk = lane / LTJ;
   const int nplanes = IMAX + JMAX + KMAX - 2;
-  for (int q = 0; q < lg.tpc; q++)
+  const int pstride = tpc * 2 * NV * LTHREADS;   // one buffer of pub
+  auto plane_cell = [&](int s, int J, int K, int& I, size_t& S) {
+    const int m = upper ? IMAX + JMAX + KMAX - s : 3 + s;
+    I = m - J - K;
+    S = ((size_t)(K - 1) * W + (m - K - 2)) * JMAX + (J - 1);
+    return I >= 1 && I <= IMAX;
+  };
+  for (int q = g0; q < tpc; q += ng)
+#pragma unroll
     for (int v = 0; v < NV; v++) ydb[(q * NV + v) * LTHREADS + lane] = CT(0);
+  // the thread group's first tile (its only one with STAGE), computed once
+  const LineDesc<CT> d0 = line_desc<CT, NV>(cluster, pub, lg, JMAX, KMAX, upper, rank, g0, lj, lk);
+  if (STAGE) {
+    int I;
+    size_t S;
+    if (d0.ok && plane_cell(0, d0.J, d0.K, I, S)) lines_stage<CT, NV>(my, nthr, sw, dwp, ns, S, upper);
+  }
   cluster.sync();
   for (int s = 0; s < nplanes; s++) {
-    const int m = upper ? IMAX + JMAX + KMAX - s : 3 + s;
     const int bin = s & 1, bout = bin ^ 1;
-    for (int q = 0; q < lg.tpc; q++) {
-      int t = q * lg.cs + rank;
-      if (t >= lg.ntiles) break;
-      int tj = t % lg.ntj, tk = t / lg.ntj;
-      int J = tj * LTJ + lj + 1, K = tk * LTK + lk + 1;
-      if (J > JMAX || K > KMAX) continue;
-      int I = m - J - K;
-      if (I < 1 || I > IMAX) continue;
-      const size_t S = ((size_t)(K - 1) * W + (m - K - 2)) * JMAX + (J - 1);
-      // own data first: independent of the neighbours' contributions
-      const CT dt1 = __ldg(sw + SW_DT1 * ns + S), vol = __ldg(sw + SW_VOL * ns + S);
-      const CT fd = upper ? CT(1) : __ldg(sw + SW_FD * ns + S);
-      const CT a1 = __ldg(sw + SW_A1 * ns + S), a2 = __ldg(sw + SW_A2 * ns + S), a3 = __ldg(sw + SW_A3 * ns + S);
-      const CT scinv = __ldg(sw + SW_SCINV * ns + S), scinp = __ldg(sw + SW_SCINP * ns + S);
-      CT rhs[NV];
-#pragma unroll
-      for (int v = 0; v < NV; v++) rhs[v] = dwp[v * ns + S];
+    for (int q = g0; q < (STAGE ? g0 + 1 : tpc); q += ng) {
+      const LineDesc<CT> ld =
+          STAGE || q == g0 ? d0 : line_desc<CT, NV>(cluster, pub, lg, JMAX, KMAX, upper, rank, q, lj, lk);
+      const int J = ld.J;
+      int I;
+      size_t S;
+      if (!ld.ok || !plane_cell(s, J, ld.K, I, S)) continue;
+      if (STAGE) cp_async_wait_all();
+      // value c of the cell's sweep data (c >= SW_N: right-hand side)
+      auto cd_ = [&](int c) -> CT {
+        if (STAGE) return my[c * nthr];
+        return c < SW_N ? __ldg(sw + c * ns + S) : dwp[(c - SW_N) * ns + S];
+      };
+      // PREDGS drops the i+1 coupling of row J = JMAX; PRKEGS does not
+      const bool hy = upper ? (I < IMAX && (NV == 7 || J < JMAX)) : (I > 1);
       // ---- consume: neighbour contributions of the previous plane ----
       CT yd[NV], bd[NV], ck[NV];
-      // PREDGS drops the i+1 coupling of row J = JMAX; PRKEGS does not
-      bool hy = upper ? (I < IMAX && (NV == 7 || J < JMAX)) : (I > 1);
-      bool hj = upper ? (J < JMAX) : (J > 1);
-      bool hk = upper ? (K < KMAX) : (K > 1);
 #pragma unroll
-      for (int v = 0; v < NV; v++) yd[v] = hy ? ydb[(q * NV + v) * LTHREADS + lane] : CT(0);
-      {
-        int Jn = upper ? J + 1 : J - 1;       // line across the j face
-        int Kn = upper ? K + 1 : K - 1;       // line across the k face
-        // source of bd: line (Jn, K); of ck: line (J, Kn)
-        const CT* src;
-        int tjn = (Jn - 1) / LTJ, ljn = (Jn - 1) % LTJ, tn = tk * lg.ntj + tjn;
-        if (hj) {
-          src = cluster.map_shared_rank(pub, tn % lg.cs);
-          int ln = lk * LTJ + ljn, qn = tn / lg.cs;
-#pragma unroll
-          for (int v = 0; v < NV; v++) bd[v] = src[((bin * lg.tpc + qn) * 2 * NV + v) * LTHREADS + ln];
-        } else {
-#pragma unroll
-          for (int v = 0; v < NV; v++) bd[v] = CT(0);
-        }
-        int tkn = (Kn - 1) / LTK, lkn = (Kn - 1) % LTK, tn2 = tkn * lg.ntj + tj;
-        if (hk) {
-          src = cluster.map_shared_rank(pub, tn2 % lg.cs);
-          int ln = lkn * LTJ + lj, qn = tn2 / lg.cs;
-#pragma unroll
-          for (int v = 0; v < NV; v++) ck[v] = src[((bin * lg.tpc + qn) * 2 * NV + NV + v) * LTHREADS + ln];
-        } else {
-#pragma unroll
-          for (int v = 0; v < NV; v++) ck[v] = CT(0);
-        }
+      for (int v = 0; v < NV; v++) {
+        yd[v] = hy ? ydb[(q * NV + v) * LTHREADS + lane] : CT(0);
+        bd[v] = ld.hj ? ld.srcj[bin * pstride + v * LTHREADS] : CT(0);
+        ck[v] = ld.hk ? ld.srck[bin * pstride + v * LTHREADS] : CT(0);
       }
       // ---- solve the cell ----
+      const CT dt1 = cd_(SW_DT1), vol = cd_(SW_VOL), fd = upper ? CT(1) : cd_(SW_FD);
+      const CT a1 = cd_(SW_A1), a2 = cd_(SW_A2), a3 = cd_(SW_A3);
+      const CT scinv = cd_(SW_SCINV), scinp = cd_(SW_SCINP);
       CT res[NV];
 #pragma unroll
       for (int v = 0; v < NV; v++) {
-        CT cd = rhs[v] * fd;
+        CT cd = cd_(SW_N + v) * fd;
         CT x = upper ? (-dt1 * a3 * ck[v] + vol * cd) : (dt1 * a3 * ck[v] + vol * cd);
         x = upper ? x - dt1 * (a1 * yd[v] + a2 * bd[v]) : x + dt1 * (a1 * yd[v] + a2 * bd[v]);
         res[v] = x * (v == 4 ? scinp : scinv);
@@ -1356,15 +1436,15 @@ __global__ void __launch_bounds__(LTHREADS) k_lusgs_lines(DevBlock b, const CT* 
       // ---- produce: contributions to the three downstream neighbours ----
       CT sc[5];
 #pragma unroll
-      for (int c = 0; c < (NV == 7 ? 5 : 3); c++) sc[c] = __ldg(sw + (SW_SC + c) * ns + S);
-      const CT ro = NV == 7 ? __ldg(sw + SW_RO * ns + S) : CT(0);
+      for (int c = 0; c < (NV == 7 ? 5 : 3); c++) sc[c] = cd_(SW_SC + c);
+      const CT ro = NV == 7 ? cd_(SW_RO) : CT(0);
 #pragma unroll
       for (int d = 0; d < 3; d++) {
         CT f[9], l[3];
 #pragma unroll
-        for (int c = 0; c < 9; c++) f[c] = __ldg(sw + (SW_F + 9 * d + c) * ns + S);
+        for (int c = 0; c < 9; c++) f[c] = cd_(SW_F + 9 * d + c);
 #pragma unroll
-        for (int e = 0; e < 3; e++) l[e] = __ldg(sw + (SW_L + 3 * d + e) * ns + S);
+        for (int e = 0; e < 3; e++) l[e] = cd_(SW_L + 3 * d + e);
         CT out[NV];
         nb_product_pre<CT, NV>(out, res, f, sc, ro, l[0], l[1], l[2]);
         if (d == 0) {
@@ -1372,10 +1452,18 @@ __global__ void __launch_bounds__(LTHREADS) k_lusgs_lines(DevBlock b, const CT* 
           for (int v = 0; v < NV; v++) ydb[(q * NV + v) * LTHREADS + lane] = out[v];
         } else {
 #pragma unroll
-          for (int v = 0; v < NV; v++) pub[((bout * lg.tpc + q) * 2 * NV + (d == 1 ? 0 : NV) + v) * LTHREADS + lane] = out[v];
+          for (int v = 0; v < NV; v++)
+            pub[bout * pstride + (q * 2 * NV + (d == 1 ? 0 : NV) + v) * LTHREADS + lane] = out[v];
         }
       }
     }
-    cluster.sync();
+    cluster_arrive_release();
+    // the next plane's sweep data, in flight while the other CTAs finish
+    if (STAGE && s + 1 < nplanes && d0.ok) {
+      int I;
+      size_t S;
+      if (plane_cell(s + 1, d0.J, d0.K, I, S)) lines_stage<CT, NV>(my, nthr, sw, dwp, ns, S, upper);
+    }
+    cluster_wait_acquire();
   }
 }
