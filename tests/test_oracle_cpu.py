@@ -186,3 +186,16 @@ def test_abi_exports_every_declared_symbol():
     for n in names:
         assert hasattr(L, n), n
     assert L.ff_abi_version() == 2
+
+
+def test_nn_abi_exports_every_declared_symbol():
+    """libfinflo_nn.so (the warm start's tensor-core kernels) loads without a
+    GPU and exports every function that include/finflo_nn.h declares."""
+    from finflo_b200 import nn
+    nn.build()
+    L = ctypes.CDLL(nn.LIB_PATH)
+    hdr = open(os.path.join(ROOT, "include", "finflo_nn.h")).read()
+    names = re.findall(r"^\s*int\s+(ffnn_\w+)\s*\(", hdr, re.M)
+    assert sorted(names) == sorted(nn.SYMBOLS)
+    for n in names:
+        assert hasattr(L, n), n
