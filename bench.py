@@ -179,6 +179,11 @@ def run_reference(args):
     ws, rank, local = _dist()
     if rank != 0:
         return 0
+    if args.workload == "warmstart":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned warm start; its "
+                          "plain method (FP64 solver from the free stream) is timed in our line as "
+                          "plain_fp64_free_stream_s"}))
+        return 0
     seconds = max(10.0, min(40.0, 2.0 * args.steps))
     if args.workload == "box":   # one process: the 24 blocks hold several GB of host memory
         from finflo_b200 import case
@@ -390,6 +395,44 @@ def run_box(args):
     return 0
 
 
+WARM_NAME = ("learned warm start: bump channel 64x32x32 cells, laminar Re=1e4, Mach U[0.3,0.8] x bump "
+             "amplitude U[0.05,0.15]; 64 solver solutions (seed 3) train a 4-layer MLP encoder + 3-D "
+             "transposed-conv decoder (32 channels, BF16 weights, tcgen05 GEMMs); 16 held-out points (seed 4)")
+
+
+def run_warmstart(args):
+    """The learned warm start: wall time to the same residual tolerance from
+    the free stream (plain FP64 solver) and from the network's prediction
+    (FP32 implicit stage), summed over the held-out points.  Replicas only:
+    with N > 1 every rank runs the same study and rank 0 reports."""
+    ws_, rank, local = _dist()
+    import torch
+    torch.cuda.set_device(local)
+    from finflo_b200 import warmstart as wsm
+    logs = []
+    r = wsm.run_config(ntrain=args.ws_train, ntest=args.ws_test, cycles=args.ws_cycles, steps=args.ws_steps,
+                       tol_decades=args.ws_decades, log=logs.append)
+    if rank != 0:
+        return 0
+    line = {
+        "metric": f"time to a {args.ws_decades:g}-decade density-residual drop (sum over {args.ws_test} held-out cases)",
+        "value": r["warm_s"], "unit": "s", "n_gpus": ws_, "steps": args.ws_steps, "warmup": 0,
+        "ms_per_step": 1e3 * r["t_train"] / args.ws_steps, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16 network / f32 LU-SGS / f64 residual",
+        "data": "synthetic (seeded parameter points; training fields generated by the solver)",
+        "config": {"workload": WARM_NAME, "ntrain": args.ws_train, "ntest": args.ws_test,
+                   "training_cycles": args.ws_cycles, "training_steps": args.ws_steps,
+                   "parallelism": f"replicas x{ws_}"},
+        "plain_fp64_free_stream_s": r["base_s"], "speedup": r["speedup"],
+        "cycles": {"plain_fp64_free_stream": r["base_cycles"], "fp32_lusgs_warm_start": r["warm_cycles"]},
+        "training": {"data_s": r["t_data"], "train_s": r["t_train"], "loss": r["loss"]},
+        "cases": r["cases"],
+        "e2e": {"value": r["warm_s"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -400,7 +443,12 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--grid", default="", help="node counts ni,nj,nk (profiling runs)")
-    ap.add_argument("--workload", default="sst-mg", choices=["sst-mg", "bump", "box"])
+    ap.add_argument("--workload", default="sst-mg", choices=["sst-mg", "bump", "box", "warmstart"])
+    ap.add_argument("--ws-train", type=int, default=64)
+    ap.add_argument("--ws-test", type=int, default=16)
+    ap.add_argument("--ws-cycles", type=int, default=2000)
+    ap.add_argument("--ws-steps", type=int, default=6000)
+    ap.add_argument("--ws-decades", type=float, default=2.0)
     ap.add_argument("--blocks", default="4,3,2", help="block arrangement of the box workload")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -409,6 +457,8 @@ def main():
         return run_reference(args)
     if args.workload == "box":
         return run_box(args)
+    if args.workload == "warmstart":
+        return run_warmstart(args)
     return run_ours(args)
 
 

@@ -278,9 +278,9 @@ __global__ void k_f32_to_bf16(const float* __restrict__ in, long n, __nv_bfloat1
 
 // Mean-squared error of pred [rows, ld] (first cols columns) against
 // target [rows, cols]: loss += sum((p - t)^2) / count, grad = 2 (p - t) / count
-// as BF16 [rows, ld] with zero padding columns.
+// as BF16 [rows, ld] with zero padding columns (and as FP32 when gradf is set).
 __global__ void k_mse(const float* __restrict__ pred, int ld, const float* __restrict__ tgt, int rows, int cols,
-                      float inv_count, __nv_bfloat16* grad, float* loss) {
+                      float inv_count, __nv_bfloat16* grad, float* gradf, float* loss) {
   float s = 0.f;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < (long)rows * ld; i += (long)gridDim.x * blockDim.x) {
     const long r = i / ld;
@@ -292,6 +292,7 @@ __global__ void k_mse(const float* __restrict__ pred, int ld, const float* __res
       g = 2.f * d * inv_count;
     }
     grad[i] = __float2bfloat16_rn(g);
+    if (gradf) gradf[i] = g;
   }
   for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
   if ((threadIdx.x & 31) == 0) atomicAdd(loss, s * inv_count);
@@ -386,11 +387,12 @@ int ffnn_to_bf16(const float* in, long n, void* out, void* stream) {
   return cudaGetLastError() == cudaSuccess ? 0 : FFNN_ERR_CUDA;
 }
 
-int ffnn_mse(const float* pred, int ld, const float* tgt, int rows, int cols, void* grad, float* loss, void* stream) {
+int ffnn_mse(const float* pred, int ld, const float* tgt, int rows, int cols, void* grad, float* gradf, float* loss,
+             void* stream) {
   if (rows <= 0 || cols <= 0 || ld < cols) return FFNN_ERR_ARG;
   long n = (long)rows * ld;
   k_mse<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(pred, ld, tgt, rows, cols, 1.f / ((float)rows * cols),
-                                                              (__nv_bfloat16*)grad, loss);
+                                                              (__nv_bfloat16*)grad, gradf, loss);
   return cudaGetLastError() == cudaSuccess ? 0 : FFNN_ERR_CUDA;
 }
 

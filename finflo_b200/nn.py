@@ -48,7 +48,7 @@ def lib():
         L.ffnn_colsum.argtypes = [vp, ci, ci, ci, vp, vp]
         L.ffnn_transpose.argtypes = [vp, ci, ci, ci, vp, ci, ci, vp]
         L.ffnn_to_bf16.argtypes = [vp, cl, vp, vp]
-        L.ffnn_mse.argtypes = [vp, ci, vp, ci, ci, vp, vp, vp]
+        L.ffnn_mse.argtypes = [vp, ci, vp, ci, ci, vp, vp, vp, vp]
         L.ffnn_adam.argtypes = [vp, vp, vp, vp, cl, cf, cf, cf, cf, ci, cf, vp, vp, ci, vp]
         L.ffnn_error.argtypes = [ci]
         _LIB = L
@@ -118,11 +118,11 @@ def to_bf16(x, out):
     _check(lib().ffnn_to_bf16(x.data_ptr(), x.numel(), out.data_ptr(), _stream()), "ffnn_to_bf16")
 
 
-def mse(pred, tgt, grad, loss):
+def mse(pred, tgt, grad, loss, gradf=None):
     rows, ld = pred.shape
     cols = tgt.shape[1]
-    _check(lib().ffnn_mse(pred.data_ptr(), ld, tgt.data_ptr(), rows, cols, grad.data_ptr(), loss.data_ptr(),
-                          _stream()), "ffnn_mse")
+    _check(lib().ffnn_mse(pred.data_ptr(), ld, tgt.data_ptr(), rows, cols, grad.data_ptr(), _ptr(gradf),
+                          loss.data_ptr(), _stream()), "ffnn_mse")
 
 
 def adam(w, g, m, v, step, lr, b1=0.9, b2=0.999, eps=1e-8, wd=0.0, w16=None, w16t=None, rows=0):

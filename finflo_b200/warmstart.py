@@ -1,0 +1,484 @@
+"""Learned warm start: a small network predicts the flow field of a bump
+channel from its parameters (free-stream Mach number, bump amplitude); the
+solver then iterates from that prediction instead of from the free stream,
+to the same residual tolerance, and stays the judge of the prediction.
+
+Network (BF16 weights, FP32 accumulation, every product on the tensor cores
+through libfinflo_nn.so):
+
+* encoder: a 4-layer MLP on the normalised parameters (2 -> 64 -> 128 ->
+  256 -> 512), SiLU between layers; the 512 outputs are a 4x2x2 grid of
+  32-channel root voxels;
+* decoder: four levels of a 3-D transposed convolution with kernel 2 and
+  stride 2 (each voxel -> its 2x2x2 children, 32 -> 8 x 32 channels, SiLU)
+  followed by a 1x1x1 convolution (32 -> 32, SiLU), then a 1x1x1 output
+  convolution to the 5 conservative variables of each of the 64x32x32
+  cells.  Voxels are kept in octree order (child index = 8 x parent +
+  octant), so each transposed convolution is one GEMM whose output rows are
+  already the next level's voxels.
+
+Targets are the conservative variables (RO, RM, RN, RW, E) of converged
+solver runs, scaled by each case's free-stream values, minus their mean over
+the training set per cell, divided by one spread per variable (the
+spanwise momentum, numerical noise in these spanwise-uniform cases, shares
+the normal momentum's spread so that it does not weigh in the loss).
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+CH = 32                # decoder channels
+ROOT = (4, 2, 2)       # root voxels in i, j, k
+LEVELS = 4             # 2x refinements: 4x2x2 -> 64x32x32
+NVAR = 5               # RO, RM, RN, RW, E
+OUT_PAD = 16           # output channels padded to the GEMM's N step
+IN_PAD = 16            # parameters padded to the GEMM's K step
+ENC = [IN_PAD, 64, 128, 256, CH * ROOT[0] * ROOT[1] * ROOT[2]]
+GRID = tuple(r << LEVELS for r in ROOT)   # cells: 64, 32, 32
+
+
+def octree_order(root=ROOT, levels=LEVELS):
+    """Interior cell index (i fastest, [k][j][i]) of each finest-level voxel
+    in decoder order.  Root r = (rk * Rj + rj) * Ri + ri; a child's index is
+    8 x parent + (di + 2 dj + 4 dk)."""
+    ri, rj, rk = np.meshgrid(np.arange(root[0]), np.arange(root[1]), np.arange(root[2]), indexing="ij")
+    # voxel coordinates at level 0, in root order
+    order = np.argsort((rk * root[1] + rj) * root[0] + ri, axis=None, kind="stable")
+    I, J, K = ri.ravel()[order], rj.ravel()[order], rk.ravel()[order]
+    for _ in range(levels):
+        c = np.arange(8)
+        di, dj, dk = c & 1, (c >> 1) & 1, (c >> 2) & 1
+        I = (2 * I[:, None] + di[None, :]).ravel()
+        J = (2 * J[:, None] + dj[None, :]).ravel()
+        K = (2 * K[:, None] + dk[None, :]).ravel()
+    ni, nj = root[0] << levels, root[1] << levels
+    return (K * nj + J) * ni + I
+
+
+def conservative(blk):
+    """Interior (RO, RM, RN, RW, E) of a block as [cells, 5], i fastest."""
+    return np.stack([blk.interior(n).ravel() for n in ("RO", "RM", "RN", "RW", "E")], axis=1)
+
+
+def freestream_scales(fs, gamma=1.4, rgas=287.05287):
+    """Per-variable scales of a case (fs: the free-stream dict of
+    FlowConditions): rho, rho U, rho U, rho U, E."""
+    ru = fs["rho"] * fs["u"]
+    e = fs["rho"] * (rgas * fs["t"] / (gamma - 1.0) + 0.5 * fs["u"] ** 2)
+    return np.array([fs["rho"], ru, ru, ru, e])
+
+
+def state_from_conservative(q, fs, gamma=1.4, rgas=287.05287):
+    """Solver state (TEMP, U, V, W, PDIFF) of conservative values q [cells, 5]
+    for a perfect gas (PERFGA: e = R T / (gamma - 1), p = rho R T), with the
+    density and temperature kept above a fraction of the free stream's;
+    PDIFF is the pressure minus the free stream's (FRSPRE)."""
+    ro = np.maximum(q[:, 0], 0.2 * fs["rho"])
+    u, v, w = q[:, 1] / ro, q[:, 2] / ro, q[:, 3] / ro
+    e = q[:, 4] / ro - 0.5 * (u * u + v * v + w * w)
+    T = np.maximum(e * (gamma - 1.0) / rgas, 0.2 * fs["t"])
+    p = ro * rgas * T
+    return {"TEMP": T, "U": u, "V": v, "W": w, "PDIFF": p - fs["p"]}
+
+
+def normalise_params(mach, amp, mach_range=(0.3, 0.8), amp_range=(0.05, 0.15)):
+    x = np.zeros((len(mach), IN_PAD), dtype=np.float32)
+    x[:, 0] = 2.0 * (np.asarray(mach) - mach_range[0]) / (mach_range[1] - mach_range[0]) - 1.0
+    x[:, 1] = 2.0 * (np.asarray(amp) - amp_range[0]) / (amp_range[1] - amp_range[0]) - 1.0
+    return x
+
+
+def _r16(n):
+    return (n + 15) // 16 * 16
+
+
+@dataclass
+class Layer:
+    name: str
+    n: int            # outputs
+    k: int            # inputs
+    act: int          # 1: SiLU after the layer
+    off: int = 0      # weight offset in the flat parameter buffer
+    boff: int = 0     # bias offset
+
+
+def layers():
+    L = [Layer(f"enc{i + 1}", ENC[i + 1], ENC[i], 1 if i < 3 else 0) for i in range(4)]
+    for lv in range(LEVELS):
+        L.append(Layer(f"up{lv + 1}", 8 * CH, CH, 1))
+        L.append(Layer(f"mix{lv + 1}", CH, CH, 1))
+    L.append(Layer("out", OUT_PAD, CH, 0))
+    off = 0
+    for l in L:
+        l.off = off
+        off += l.n * l.k
+    for l in L:
+        l.boff = off
+        off += l.n
+    return L, off
+
+
+class WarmStartNet:
+    """Parameters, activations and the training step of the network.  torch
+    holds the memory; every GEMM, activation gradient, reduction and the
+    Adam update run in libfinflo_nn.so."""
+
+    def __init__(self, device="cuda", seed=0):
+        import torch
+        from . import nn
+        self.torch, self.nn = torch, nn
+        self.dev = torch.device(device)
+        self.L, self.nparam = layers()
+        g = torch.Generator().manual_seed(seed)
+        w = torch.zeros(self.nparam)
+        for l in self.L:   # Kaiming-uniform weights for SiLU layers, zero biases
+            bound = math.sqrt(6.0 / l.k) if l.act else math.sqrt(3.0 / l.k)
+            if l.name == "enc1":
+                bound = math.sqrt(6.0 / 2)   # two real inputs, the rest is padding
+            w[l.off:l.off + l.n * l.k] = (torch.rand(l.n * l.k, generator=g) * 2 - 1) * bound
+        self.w = w.to(self.dev)
+        self.g = torch.zeros_like(self.w)
+        self.m = torch.zeros_like(self.w)
+        self.v = torch.zeros_like(self.w)
+        self.w16 = torch.empty(self.nparam, dtype=torch.bfloat16, device=self.dev)
+        self.w16t = torch.empty(self.nparam, dtype=torch.bfloat16, device=self.dev)
+        self.step_n = 0
+        self._sync_bf16()
+        self.B = 0
+
+    # -- parameter views ----------------------------------------------------
+    def W(self, l):
+        return self.w16[l.off:l.off + l.n * l.k].view(l.n, l.k)
+
+    def WT(self, l):
+        return self.w16t[l.off:l.off + l.n * l.k].view(l.k, l.n)
+
+    def bias(self, l):
+        return self.w[l.boff:l.boff + l.n]
+
+    def gW(self, l):
+        return self.g[l.off:l.off + l.n * l.k].view(l.n, l.k)
+
+    def gb(self, l):
+        return self.g[l.boff:l.boff + l.n]
+
+    def _sync_bf16(self):
+        nn = self.nn
+        nn.to_bf16(self.w, self.w16)
+        for l in self.L:
+            nn.transpose(self.W(l), self.WT(l))
+
+    # -- buffers ----------------------------------------------------------------
+    def _alloc(self, B):
+        if B == self.B:
+            return
+        torch = self.torch
+        f32, b16, d = torch.float32, torch.bfloat16, self.dev
+        self.B = B
+        self.x0 = torch.zeros(B, IN_PAD, dtype=b16, device=d)
+        self.z, self.h = {}, {"enc0": self.x0}
+        for l in self.L[:4]:
+            self.z[l.name] = torch.empty(B, l.n, dtype=f32, device=d)
+            self.h[l.name] = torch.empty(B, l.n, dtype=b16, device=d)
+        V = B * ROOT[0] * ROOT[1] * ROOT[2]
+        self.rows = {}
+        prev = self.h["enc4"].view(V, CH)
+        self.inp = {}
+        for lv in range(LEVELS):
+            up, mix = f"up{lv + 1}", f"mix{lv + 1}"
+            self.inp[up] = prev
+            self.z[up] = torch.empty(V, 8 * CH, dtype=f32, device=d)
+            self.h[up] = torch.empty(V, 8 * CH, dtype=b16, device=d)
+            self.rows[up] = V
+            V *= 8
+            self.inp[mix] = self.h[up].view(V, CH)
+            self.z[mix] = torch.empty(V, CH, dtype=f32, device=d)
+            self.h[mix] = torch.empty(V, CH, dtype=b16, device=d)
+            self.rows[mix] = V
+            prev = self.h[mix]
+        self.inp["out"] = prev
+        self.rows["out"] = V
+        self.pred = torch.empty(V, OUT_PAD, dtype=f32, device=d)
+        self.nvox = V
+        # backward
+        self.dpred = torch.empty(V, OUT_PAD, dtype=b16, device=d)
+        self.dpredf = torch.empty(V, OUT_PAD, dtype=f32, device=d)
+        big = V * CH
+        self.dA = torch.empty(big, dtype=f32, device=d)
+        self.dB = torch.empty(big, dtype=f32, device=d)
+        self.dzb = torch.empty(big, dtype=b16, device=d)
+        self.tA = torch.empty(max(big, ENC[-1] * _r16(B)), dtype=b16, device=d)
+        self.tB = torch.empty(max(big, ENC[-1] * _r16(B)), dtype=b16, device=d)
+        self.loss = torch.zeros(1, dtype=f32, device=d)
+
+    # -- forward ------------------------------------------------------------------
+    def forward(self, x):
+        """x: [B, IN_PAD] float32 (normalised parameters) -> self.pred
+        [B * 65536, OUT_PAD] in octree order."""
+        nn = self.nn
+        B = x.shape[0]
+        self._alloc(B)
+        nn.to_bf16(x.contiguous(), self.x0)
+        a = self.x0
+        for l in self.L[:4]:
+            nn.gemm(a, self.W(l), bias=self.bias(l), act=l.act, zf=self.z[l.name], yb=self.h[l.name])
+            a = self.h[l.name]
+        for l in self.L[4:-1]:
+            nn.gemm(self.inp[l.name], self.W(l), bias=self.bias(l), act=l.act, zf=self.z[l.name],
+                    yb=self.h[l.name])
+        lo = self.L[-1]
+        nn.gemm(self.inp["out"], self.W(lo), bias=self.bias(lo), act=0, zf=self.pred)
+        return self.pred
+
+    # -- backward + update ----------------------------------------------------------
+    def _wgrad(self, l, dzb, x, rows):
+        """gW(l) += dz^T x over `rows` rows: both operands transposed so that
+        the reduction (the rows) is the GEMM's contiguous K, split over CTAs."""
+        nn = self.nn
+        rp = _r16(rows)
+        a = self.tA[:l.n * rp].view(l.n, rp)
+        b = self.tB[:l.k * rp].view(l.k, rp)
+        nn.transpose(dzb, a, rows_pad=rp)
+        nn.transpose(x, b, rows_pad=rp)
+        tiles = ((l.n + 127) // 128) * ((l.k + 255) // 256)
+        splits = max(1, min(rp // 64, 296 // tiles))
+        ks = max(64, (rp + splits - 1) // splits + 63) // 64 * 64
+        nn.gemm(a, b, zf=self.gW(l), atomic=True, ksplit=ks)
+
+    def backward(self, tgt):
+        """Gradients of the mean-squared error of self.pred against tgt
+        [B * 65536, NVAR] (normalised targets, octree order) into self.g."""
+        nn, torch = self.nn, self.torch
+        self.g.zero_()
+        self.loss.zero_()
+        V = self.nvox
+        nn.mse(self.pred, tgt, self.dpred, self.loss, gradf=self.dpredf)
+        bufA, bufB = self.dA, self.dB
+        dy = None
+        for l in reversed(self.L):
+            rows = self.rows.get(l.name, self.B)
+            x = self.inp[l.name] if l.name in self.inp else self.h[f"enc{int(l.name[3:]) - 1}"]
+            if l.name == "out":
+                dzb, dzf = self.dpred, self.dpredf
+            else:
+                dy = dy.reshape(rows, l.n)   # the layer above returned it with its own row shape
+                dzb = self.dzb[:rows * l.n].view(rows, l.n)
+                dzf = bufB[:rows * l.n].view(rows, l.n)
+                if l.act:
+                    nn.silu_bwd(dy, self.z[l.name], dzb=dzb, dzf=dzf)
+                else:
+                    nn.to_bf16(dy, dzb)
+                    dzf = dy
+            self._wgrad(l, dzb, x, rows)
+            nn.colsum(dzf, self.gb(l))
+            if l.name == "enc1":
+                break
+            dx = bufA[:rows * l.k].view(rows, l.k)
+            nn.gemm(dzb, self.WT(l), zf=dx)
+            dy = dx
+        return self.loss
+
+    def adam(self, lr, wd=0.0):
+        nn = self.nn
+        self.step_n += 1
+        for l in self.L:
+            sl = slice(l.off, l.off + l.n * l.k)
+            nn.adam(self.w[sl], self.g[sl], self.m[sl], self.v[sl], self.step_n, lr, wd=wd, w16=self.w16[sl],
+                    w16t=self.w16t[sl], rows=l.n)
+        b0 = self.L[0].boff
+        sl = slice(b0, self.nparam)
+        nn.adam(self.w[sl], self.g[sl], self.m[sl], self.v[sl], self.step_n, lr)
+
+    def train(self, X, T, steps=2000, batch=16, lr=2e-3, seed=0, log_every=100):
+        """X: [n, IN_PAD] float32, T: [n, 65536, NVAR] float32 (device).
+        Adam with a cosine learning-rate decay; returns [(step, loss)]."""
+        torch = self.torch
+        gen = torch.Generator().manual_seed(seed)
+        n = X.shape[0]
+        batch = min(batch, n)
+        hist = []
+        for s in range(steps):
+            idx = torch.randperm(n, generator=gen)[:batch].to(self.dev)
+            self.forward(X[idx])
+            self.backward(T[idx].reshape(-1, NVAR))
+            lr_s = lr * (0.05 + 0.95 * 0.5 * (1.0 + math.cos(math.pi * s / steps)))
+            self.adam(lr_s)
+            if (s + 1) % log_every == 0 or s == steps - 1:
+                hist.append((s + 1, float(self.loss.item())))
+        self.nn.error()
+        return hist
+
+    def predict(self, X):
+        """[n, 65536, NVAR] float32 (normalised, octree order)."""
+        self.forward(X)
+        self.nn.error()
+        return self.pred[:, :NVAR].reshape(X.shape[0], -1, NVAR)
+
+    def state_dict(self):
+        return {"w": self.w.detach().cpu().numpy()}
+
+    def load_state_dict(self, d):
+        self.w.copy_(self.torch.as_tensor(d["w"], device=self.dev))
+        self._sync_bf16()
+
+
+# ---- solver side: training data, prediction as a start, time to tolerance ----
+
+CASE = dict(nodes=(65, 33, 33), reynolds=1e4, h1=1e-3, noise=1e-3)
+
+
+def sample_params(n, seed, mach_range=(0.3, 0.8), amp_range=(0.05, 0.15)):
+    rng = np.random.default_rng(seed)
+    return rng.uniform(*mach_range, size=n), rng.uniform(*amp_range, size=n)
+
+
+def make_case(mach, amp, seed=0, lusgs_fp32=False, **kw):
+    from . import case
+    c = dict(CASE, **kw)
+    levels, prms, fs = case.bump_case_mg(*c["nodes"], nlev=1, mach=float(mach), amp=float(amp),
+                                         reynolds=c["reynolds"], h1=c["h1"], noise=c["noise"], seed=seed,
+                                         lusgs_fp32=lusgs_fp32)
+    return levels[0], prms[0], fs
+
+
+@dataclass
+class Run:
+    cycles: int
+    seconds: float
+    hist: np.ndarray            # per-cycle sum of squares of the density residual
+    q: np.ndarray = field(default=None, repr=False)   # final conservative interior [cells, 5]
+
+
+def solve(mach, amp, cycles, init=None, tol=None, chunk=None, seed=0, keep_q=True, lusgs_fp32=False):
+    """Run the solver on one case for `cycles` cycles, or until the density
+    residual's sum of squares is <= tol; init = solver state (TEMP, U, V,
+    W, PDIFF) of the interior cells to start from instead of the free
+    stream; lusgs_fp32 runs the implicit stage in FP32.  Wall time covers
+    the cycles only (device synchronised)."""
+    from .gpu import GpuSolver
+    blk, prm, fs = make_case(mach, amp, seed=seed, lusgs_fp32=lusgs_fp32)
+    if init is not None:
+        for n, v in init.items():
+            blk.interior(n)[:] = v.reshape(blk.kmax, blk.jmax, blk.imax)
+    chunk = chunk or (10 if tol is not None else 200)   # cycles per graph replay between residual checks
+    g = GpuSolver(0)
+    try:
+        bid = g.add_block(blk, prm)
+        g.upload(bid)
+        g.start(bid)
+        g.sync()
+        hs = []
+        n = 0
+        t0 = time.perf_counter()
+        while n < cycles:
+            m = min(chunk, cycles - n)
+            h = g.cycles(m, bid, icycle0=n + 1)
+            hs.append(h[:, 0])
+            n += m
+            if tol is not None and np.nanmin(h[:, 0]) <= tol:
+                k = int(np.argmax(h[:, 0] <= tol))
+                n = n - m + k + 1
+                hs[-1] = h[:k + 1, 0]
+                break
+            if not np.isfinite(h[-1, 0]):
+                break
+        g.sync()
+        sec = time.perf_counter() - t0
+        q = None
+        if keep_q:
+            d = g.download(bid, ["RO", "RM", "RN", "RW", "E"])
+            q = np.stack([d[k].reshape(blk.kmax + 4, blk.jmax + 4, blk.imax + 4)[2:-2, 2:-2, 2:-2].ravel()
+                          for k in ("RO", "RM", "RN", "RW", "E")], axis=1)
+        return Run(n, sec, np.concatenate(hs), q)
+    finally:
+        g.close()
+
+
+class Dataset:
+    """Normalised training targets in octree order and the statistics that
+    undo the normalisation."""
+
+    def __init__(self, mach, amp, qs):
+        from .case import FlowConditions
+        self.perm = octree_order()
+        self.mach, self.amp = np.asarray(mach), np.asarray(amp)
+        sc = []
+        for m in self.mach:
+            fc = FlowConditions(mach=float(m), reynolds=CASE["reynolds"])
+            sc.append(freestream_scales(fc.freestream(), fc.gamma, fc.rgas))
+        self.scales = np.array(sc)
+        y = np.stack([q[self.perm] / s for q, s in zip(qs, self.scales)])    # [n, 65536, 5]
+        self.mean = y.mean(axis=0)
+        sd = (y - self.mean).reshape(-1, NVAR).std(axis=0)
+        sd[3] = sd[2]                       # RW on the scale of RN
+        self.std = np.maximum(sd, 1e-6)[None, :] * np.ones_like(self.mean)
+        self.y = ((y - self.mean) / self.std).astype(np.float32)
+        self.x = normalise_params(self.mach, self.amp)
+
+    def to_state(self, pred, mach, amp):
+        """Solver state of one prediction ([65536, 5] normalised, octree
+        order) for the case (mach, amp)."""
+        from .case import FlowConditions
+        fc = FlowConditions(mach=float(mach), reynolds=CASE["reynolds"])
+        fs = fc.freestream()
+        q = np.empty((len(self.perm), NVAR))
+        q[self.perm] = (pred * self.std + self.mean) * freestream_scales(fs, fc.gamma, fc.rgas)
+        return state_from_conservative(q, fs, fc.gamma, fc.rgas)
+
+
+def evaluate(net, data, mach, amp, tol_decades=2.0, max_cycles=3000, lusgs_fp32=True):
+    """For each case: cycles and wall time to a residual tolerance from the
+    free stream with the plain FP64 solver, and from the network's
+    prediction with the chosen implicit precision.  The tolerance is
+    tol_decades below the free-stream start's first-cycle density residual
+    (L2 norm), the same absolute level for both starts.  A prediction that
+    does not reach it within max_cycles is reported as such: the plain
+    solver stays the fallback."""
+    import torch
+    out = []
+    for m, a in zip(mach, amp):
+        first = solve(m, a, 1, keep_q=False)
+        tol = first.hist[0] * 10.0 ** (-2.0 * tol_decades)
+        base = solve(m, a, max_cycles, tol=tol, keep_q=False)
+        t0 = time.perf_counter()
+        pred = net.predict(torch.as_tensor(normalise_params([m], [a])).to(net.dev))[0].cpu().numpy()
+        st = data.to_state(pred, m, a)
+        t_inf = time.perf_counter() - t0
+        warm = solve(m, a, max_cycles, init=st, tol=tol, keep_q=False, lusgs_fp32=lusgs_fp32)
+        out.append(dict(mach=float(m), amp=float(a), tol=float(tol),
+                        base_cycles=base.cycles, base_s=base.seconds, base_reached=bool(base.hist.min() <= tol),
+                        warm_cycles=warm.cycles, warm_s=warm.seconds + t_inf, warm_reached=bool(warm.hist.min() <= tol),
+                        warm_start_decades=float(0.5 * np.log10(first.hist[0] / warm.hist[0]))))
+    return out
+
+
+def run_config(ntrain=64, ntest=16, cycles=2000, steps=6000, batch=16, lr=1e-3, tol_decades=2.0, seed_train=3,
+               seed_test=4, log=print):
+    """The learned-warm-start workload: solve ntrain seeded (Mach, amplitude)
+    points for `cycles` cycles as training data, train the network, then
+    evaluate the ntest held-out points.  Returns a summary dict."""
+    import torch
+    t0 = time.perf_counter()
+    mtr, atr = sample_params(ntrain, seed=seed_train)
+    mte, ate = sample_params(ntest, seed=seed_test)
+    runs = [solve(m, a, cycles) for m, a in zip(mtr, atr)]
+    t_data = time.perf_counter() - t0
+    log(f"training data: {ntrain} solves x {cycles} cycles in {t_data:.1f} s")
+    data = Dataset(mtr, atr, [r.q for r in runs])
+    net = WarmStartNet(seed=0)
+    X, T = torch.as_tensor(data.x).to(net.dev), torch.as_tensor(data.y).to(net.dev)
+    t1 = time.perf_counter()
+    hist = net.train(X, T, steps=steps, batch=batch, lr=lr, log_every=max(1, steps // 10))
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t1
+    log(f"training: {steps} steps in {t_train:.1f} s, loss {hist}")
+    ev = evaluate(net, data, mte, ate, tol_decades=tol_decades, max_cycles=max(3000, cycles))
+    base_s = sum(e["base_s"] for e in ev)
+    warm_s = sum(e["warm_s"] for e in ev)
+    return dict(cases=ev, base_s=base_s, warm_s=warm_s, speedup=base_s / warm_s,
+                base_cycles=sum(e["base_cycles"] for e in ev), warm_cycles=sum(e["warm_cycles"] for e in ev),
+                loss=hist, t_data=t_data, t_train=t_train, steps=steps, ntrain=ntrain, ntest=ntest, cycles=cycles)

@@ -49,11 +49,12 @@ int ffnn_to_bf16(const float *in, long n, void *out, void *stream);
 
 /* Mean-squared error of pred[rows, ld] (first cols columns) against
  * tgt[rows, cols]: *loss += mean((pred - tgt)^2), grad (BF16 [rows, ld]) =
- * d loss / d pred, zero in the padding columns. */
-int ffnn_mse(const float *pred, int ld, const float *tgt, int rows, int cols, void *grad, float *loss,
-             void *stream);
+ * d loss / d pred, zero in the padding columns; gradf (FP32, may be NULL)
+ * the same gradient in FP32. */
+int ffnn_mse(const float *pred, int ld, const float *tgt, int rows, int cols, void *grad, float *gradf,
+             float *loss, void *stream);
 
-/* One Adam step (bias-corrected, decoupled weight decay wd) on FP32 master
+/* One Adam step (bias-corrected; wd * w added to the gradient) on FP32 master
  * weights w[n] with moments m, v; writes the BF16 copy w16 and, when
  * rows > 0, the BF16 transpose w16t of w viewed as [rows, n/rows]. */
 int ffnn_adam(float *w, const float *g, float *m, float *v, long n, float lr, float b1, float b2, float eps,
