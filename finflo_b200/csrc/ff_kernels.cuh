@@ -20,6 +20,9 @@
 namespace ff {
 
 constexpr int TI = 32, TJ = 4, TK = 4;   // residual tile
+#ifndef RES_MIN_CTAS
+#define RES_MIN_CTAS 4                    // residual CTAs per SM the register budget aims at
+#endif
 constexpr int NCOEF = 13;                 // LU-SGS coefficients per cell
 
 // ---------------------------------------------------------------------------
@@ -502,8 +505,8 @@ FF_DI void face_flux(const DevBlock& b, const ff_params& p, int dir, size_t L, i
 }
 
 // RESIDU: fused k, i, j face fluxes and SWEEP res3c.f:992 for a 32x4x4 tile.
-__global__ void __launch_bounds__(128) k_residual(DevBlock b, ff_params p, int level) {
-  __shared__ double sF[5][TI * (TJ + 1) * TK];   // 640 faces x 5
+__global__ void __launch_bounds__(128, RES_MIN_CTAS) k_residual(DevBlock b, ff_params p, int level) {
+  __shared__ double sF[5][TI * (TJ + 1) * TK];   // one direction's faces (at most 640) x 5
   const int tid = threadIdx.x;
   const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ, k0 = blockIdx.z * TK;
   const int ci = tid % TI, cj = tid / TI;
@@ -512,64 +515,41 @@ __global__ void __launch_bounds__(128) k_residual(DevBlock b, ff_params p, int l
   for (int c = 0; c < TK; c++)
 #pragma unroll
     for (int v = 0; v < 5; v++) acc[c][v] = 0.;
-  // ---- k faces (SWEEP with KSTRID = IL, res3c.f:355) ----
-  for (int f = tid; f < TI * TJ * (TK + 1); f += blockDim.x) {
-    int fi = f % TI, fj = (f / TI) % TJ, fk = f / (TI * TJ);
-    int I = i0 + fi + 1, J = j0 + fj + 1, m = k0 + fk + 1;
-    if (I > b.imax || J > b.jmax || m > b.kmax + 1) continue;
-    double fl[5];
-    face_flux(b, p, 3, ix(b, I, J, m), m, I, J, level, fl);
+  // the directions in SWEEP order (k, i, j; res3c.f:355); one call site of the
+  // face flux keeps a single copy of its code in the instruction stream
+#pragma unroll 1
+  for (int pass = 0; pass < 3; pass++) {
+    const int dir = pass == 0 ? 3 : pass;   // k, i, j
+    const int ni = TI + (dir == 1), nj = TJ + (dir == 2), nk = TK + (dir == 3);
+    for (int f = tid; f < ni * nj * nk; f += blockDim.x) {
+      const int fi = f % ni, fj = (f / ni) % nj, fk = f / (ni * nj);
+      const int I = i0 + fi + 1, J = j0 + fj + 1, K = k0 + fk + 1;
+      if (I > b.imax + (dir == 1) || J > b.jmax + (dir == 2) || K > b.kmax + (dir == 3)) continue;
+      const int m = dir == 1 ? I : (dir == 2 ? J : K);
+      const int t1 = dir == 1 ? J : I, t2 = dir == 3 ? J : K;
+      double fl[5];
+      face_flux(b, p, dir, ix(b, I, J, K), m, t1, t2, level, fl);
 #pragma unroll
-    for (int v = 0; v < 5; v++) sF[v][f] = fl[v];
-  }
-  __syncthreads();
+      for (int v = 0; v < 5; v++) sF[v][f] = fl[v];
+    }
+    __syncthreads();
+    const int fs = dir == 1 ? 1 : (dir == 2 ? ni : ni * nj);   // low face -> high face of a cell
 #pragma unroll
-  for (int c = 0; c < TK; c++) {
-    int f0 = ci + TI * (cj + TJ * c), f1 = ci + TI * (cj + TJ * (c + 1));
-    if (i0 + ci < b.imax && j0 + cj < b.jmax && k0 + c < b.kmax)
+    for (int c = 0; c < TK; c++) {
+      const int f0 = ci + ni * (cj + nj * c);
+      const int I = i0 + ci + 1, J = j0 + cj + 1, K = k0 + c + 1;
+      if (I > b.imax || J > b.jmax || K > b.kmax) continue;
+      if (pass < 2) {
 #pragma unroll
-      for (int v = 0; v < 5; v++) acc[c][v] = acc[c][v] - (sF[v][f1] - sF[v][f0]);
-  }
-  __syncthreads();
-  // ---- i faces ----
-  for (int f = tid; f < (TI + 1) * TJ * TK; f += blockDim.x) {
-    int fi = f % (TI + 1), fj = (f / (TI + 1)) % TJ, fk = f / ((TI + 1) * TJ);
-    int m = i0 + fi + 1, J = j0 + fj + 1, K = k0 + fk + 1;
-    if (m > b.imax + 1 || J > b.jmax || K > b.kmax) continue;
-    double fl[5];
-    face_flux(b, p, 1, ix(b, m, J, K), m, J, K, level, fl);
+        for (int v = 0; v < 5; v++) acc[c][v] = acc[c][v] - (sF[v][f0 + fs] - sF[v][f0]);
+      } else {   // last direction, then 1/VOL (SWEEP IDO = 1)
+        const size_t n = ix(b, I, J, K);
+        const double rv = 1. / __ldg(b.a[FF_VOL] + n);
 #pragma unroll
-    for (int v = 0; v < 5; v++) sF[v][f] = fl[v];
-  }
-  __syncthreads();
-#pragma unroll
-  for (int c = 0; c < TK; c++) {
-    int f0 = ci + (TI + 1) * (cj + TJ * c);
-    if (i0 + ci < b.imax && j0 + cj < b.jmax && k0 + c < b.kmax)
-#pragma unroll
-      for (int v = 0; v < 5; v++) acc[c][v] = acc[c][v] - (sF[v][f0 + 1] - sF[v][f0]);
-  }
-  __syncthreads();
-  // ---- j faces, then 1/VOL (SWEEP IDO = 1) ----
-  for (int f = tid; f < TI * (TJ + 1) * TK; f += blockDim.x) {
-    int fi = f % TI, fj = (f / TI) % (TJ + 1), fk = f / (TI * (TJ + 1));
-    int I = i0 + fi + 1, m = j0 + fj + 1, K = k0 + fk + 1;
-    if (I > b.imax || m > b.jmax + 1 || K > b.kmax) continue;
-    double fl[5];
-    face_flux(b, p, 2, ix(b, I, m, K), m, I, K, level, fl);
-#pragma unroll
-    for (int v = 0; v < 5; v++) sF[v][f] = fl[v];
-  }
-  __syncthreads();
-#pragma unroll
-  for (int c = 0; c < TK; c++) {
-    int I = i0 + ci + 1, J = j0 + cj + 1, K = k0 + c + 1;
-    if (I > b.imax || J > b.jmax || K > b.kmax) continue;
-    int f0 = ci + TI * (cj + (TJ + 1) * c), f1 = ci + TI * (cj + 1 + (TJ + 1) * c);
-    size_t n = ix(b, I, J, K);
-    double rv = 1. / __ldg(b.a[FF_VOL] + n);
-#pragma unroll
-    for (int v = 0; v < 5; v++) b.a[FF_DRO + v][n] = (acc[c][v] - (sF[v][f1] - sF[v][f0])) * rv;
+        for (int v = 0; v < 5; v++) b.a[FF_DRO + v][n] = (acc[c][v] - (sF[v][f0 + fs] - sF[v][f0])) * rv;
+      }
+    }
+    __syncthreads();
   }
 }
 
