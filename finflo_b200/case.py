@@ -457,3 +457,113 @@ def periodic_box_case(nb=(4, 3, 2), sizes=None, *, seed=2, mach=0.3, target=None
         blocks.append(blk)
         prms.append(prm)
     return blocks, prms, fs
+
+
+# ---- multi-block bump with multigrid levels (the large combined case) -------
+
+def bump_block_cuts(cells, nb, seed, quantum=4, spread=0.1):
+    """Uneven cut positions of each direction: nb[d] blocks whose sizes are
+    multiples of `quantum` cells (so every block has its multigrid levels),
+    each within +-spread of the even split, drawn with the seed."""
+    rng = np.random.default_rng(seed)
+    cuts = []
+    for n, m in zip(cells, nb):
+        base = n / m
+        pos = [0]
+        for q in range(1, m):
+            jit = int(round(rng.uniform(-spread, spread) * base / quantum)) * quantum
+            pos.append(int(round(q * base / quantum)) * quantum + jit)
+        pos.append(n)
+        cuts.append(pos)
+    return cuts
+
+
+class _WallSurface:
+    """The solid walls of the whole channel (lower and upper node planes) in
+    the form wall_distance reads."""
+
+    def __init__(self, X, Y, Z):
+        sl = (slice(None), [0, -1], slice(None))
+        self.nodes = (X[sl], Y[sl], Z[sl])
+        kmax, imax = X.shape[0] - 1, X.shape[2] - 1
+        self.patches = [_patch(grid.BC_SOL, 2, (1, imax), (1, kmax)), _patch(grid.BC_SOL, 5, (1, imax), (1, kmax))]
+
+
+def bump_multiblock_blocks(cells=(512, 256, 128), nb=(2, 2, 2), nlev=3, *, seed=5, h1=2e-6, amp=0.1,
+                           span_amp=0.5, zlen=1.0, mach=0.7, reynolds=5e6, noise=1e-3, cfl=1.0, cfll=1.0,
+                           inter=3, turbulence="sst", tu=1.0e-3, mut_ratio=0.1, lusgs_fp32=True,
+                           coarse_fp32=True):
+    """The bump channel split into nb[0] x nb[1] x nb[2] blocks of uneven
+    sizes (cut positions from the seed), 1:1 patched on every interior cut,
+    periodic in z through 1:1 patches (the spanwise amplitude
+    a(z) = amp (1 + span_amp sin 2 pi z) is periodic on [0, zlen = 1]),
+    INL / OUT / SOL on the outer i and j faces.  Yields, block by block
+    (i fastest), (levels, prms) with nlev multigrid levels each; a 1:1
+    patch's IBTYPE is the source block's index.  Block metrics take mirror
+    ghost nodes at the cuts as well (the interface faces themselves are
+    exact); the wall distance is to the walls of the whole channel.  Also
+    yields the free stream first: the first item is ("fs", fs)."""
+    fc = FlowConditions(mach=mach, reynolds=reynolds)
+    fs = fc.freestream()
+    yield "fs", fs
+    NI, NJ, NK = cells
+    X, Y, Z = grid.bump_nodes(NI + 1, NJ + 1, NK + 1, h1=h1, amp=amp, zlen=zlen, span_amp=span_amp)
+    wall = _WallSurface(X, Y, Z)
+    cut = bump_block_cuts(cells, nb, seed)
+    ids = {}
+    for c in range(nb[2]):
+        for b in range(nb[1]):
+            for a in range(nb[0]):
+                ids[a, b, c] = len(ids)
+    inl = dict(bounr=fs["rho"], bounu=fs["u"], bounv=0.0, bounw=0.0, bount=fs["t"], bounp=fs["p"], bounpd=0.0)
+    for (a, b, c), bid in ids.items():
+        i0, i1 = cut[0][a], cut[0][a + 1]
+        j0, j1 = cut[1][b], cut[1][b + 1]
+        k0, k1 = cut[2][c], cut[2][c + 1]
+        Xb, Yb, Zb = (np.ascontiguousarray(A[k0:k1 + 1, j0:j1 + 1, i0:i1 + 1]) for A in (X, Y, Z))
+        levels = []
+        for lev, m in enumerate(grid.mg_metrics(Xb, Yb, Zb, nlev)):
+            pats = []
+            for iface in range(1, 7):
+                d = (iface - 1) % 3
+                r1, r2 = _face_ranges(iface, m.imax, m.jmax, m.kmax)
+                pos = (a, b, c)[d]
+                last = pos == nb[d] - 1
+                outer = (iface <= 3 and pos == 0) or (iface > 3 and last)
+                if outer and d == 0:
+                    pats.append(_patch(grid.BC_INL if iface == 1 else grid.BC_OUT, iface, r1, r2,
+                                       ibtype=4 if iface == 1 else 3, **inl))
+                elif outer and d == 1:
+                    pats.append(_patch(grid.BC_SOL, iface, r1, r2))
+                else:   # interior cut, or the periodic z faces
+                    nbr = [a, b, c]
+                    nbr[d] = (nbr[d] + (-1 if iface <= 3 else 1)) % nb[d]
+                    pa = _patch(grid.BC_CON, iface, r1, r2, ibtype=ids[tuple(nbr)])
+                    pa.nface = _OPP[iface]
+                    pa.n1a = pa.n2a = 1
+                    pats.append(pa)
+            blk = block_from_metrics(m, pats)
+            init_freestream(blk, fs, noise=noise if lev == 0 else 0.0, seed=seed + 100 * bid)
+            levels.append(blk)
+        prm = make_params(fc, levels[0].dims, cfl=cfl, cfll=cfll, inter=inter)
+        if turbulence == "sst":
+            for lev, blk in enumerate(levels):
+                setup_sst(blk, prm if lev == 0 else FFParams.from_buffer_copy(prm), fs, tu=tu,
+                          mut_ratio=mut_ratio, wall_block=wall)
+        prms = [level_params(prm, lev + 1) for lev in range(nlev)]
+        prms[0].lusgs_fp32 = int(lusgs_fp32)
+        for q in prms[1:]:
+            q.lusgs_fp32 = int(coarse_fp32)
+        yield levels, prms
+
+
+def bump_multiblock_case(*args, **kw):
+    """All blocks of bump_multiblock_blocks at once: (block_levels,
+    block_prms, fs)."""
+    it = bump_multiblock_blocks(*args, **kw)
+    _, fs = next(it)
+    bl, bp = [], []
+    for levels, prms in it:
+        bl.append(levels)
+        bp.append(prms)
+    return bl, bp, fs

@@ -69,6 +69,7 @@ struct Ctx {
   std::vector<cudaStream_t> side;
   std::vector<cudaEvent_t> side_ev;
   cudaEvent_t fork_ev = nullptr;
+  std::vector<BlockCtx*> tops;          // level-1 blocks (a multigrid block's coarse levels hang off them)
   DevBlock* d_blocks = nullptr;
   ConnItem* d_conn = nullptr;
   int nconn = 0, maxconn = 1, conn_blocks = -1;
@@ -514,14 +515,18 @@ int one_cycle(Ctx* c, BlockCtx* b, int icycle) {
   return 0;
 }
 
-// One multigrid cycle of CYCLES (ns3c.f:1400-2170): fine-level update, then
-// for each coarser level STATIM/RESIDI of the finer level, TRANSF, STATIM,
-// RESIDI, FORCFU, ADDRES, IMPSDI, FIN; then INTERP back up, REFLEC, BOUNDI.
-int mg_cycle(Ctx* c, BlockCtx* b, int icycle) {
+// The per-block part of a multigrid cycle of CYCLES (ns3c.f:1400-2130):
+// fine-level update, then for each coarser level STATIM/RESIDI of the finer
+// level, TRANSF, STATIM, RESIDI, FORCFU, ADDRES, IMPSDI, FIN; then INTERP
+// back up and REFLEC.  RESL2 of the level-1 residual after the fine update
+// is added to the context's sums; `own` (a single block) resets them here.
+int mg_body(Ctx* c, BlockCtx* b, int icycle, bool own) {
   int rc;
   const int sst = b->prm.iturb >= 3;
-  k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi, c->d_dromax);
-  c->nlaunch++;
+  if (own) {
+    k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi, c->d_dromax);
+    c->nlaunch++;
+  }
   if (sst && (rc = st_statim(c, b, 1))) return rc;
   if ((rc = st_residu(c, b, 1, icycle))) return rc;
   if ((rc = st_imps(c, b, 1, false))) return rc;
@@ -533,8 +538,10 @@ int mg_cycle(Ctx* c, BlockCtx* b, int icycle) {
     st_statim(c, f, 1);
     if ((rc = st_residu(c, f, (int)m, icycle, (int)m + 1))) return rc;
     if (m == 1) {   // RESL2 of the level-1 residual after the fine update
-      k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi, c->d_dromax);
-      c->nlaunch++;
+      if (own) {
+        k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi, c->d_dromax);
+        c->nlaunch++;
+      }
       int ncell = f->imax * f->jmax * f->kmax;
       k_resl2<<<min(nblk(ncell, 256), 4 * c->sm_count), 256, 0, c->stream>>>(f->db, c->d_resi);
       c->nlaunch++;
@@ -570,6 +577,14 @@ int mg_cycle(Ctx* c, BlockCtx* b, int icycle) {
     c->nlaunch++;
   }
   launch_patch(c, b, k_reflec, 0);
+  return 0;
+}
+
+// One multigrid cycle of one block: mg_body, BOUNDI, SUBIN.
+int mg_cycle(Ctx* c, BlockCtx* b, int icycle) {
+  int rc;
+  const int sst = b->prm.iturb >= 3;
+  if ((rc = mg_body(c, b, icycle, true))) return rc;
   if ((rc = st_boundi(c, b))) return rc;
   // SUBIN's *OLD copies (INTERP changed the level-1 state after FIN)
   k_subin_copy<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db);
@@ -599,11 +614,18 @@ int ensure_conn(Ctx* c) {
   std::vector<DevBlock> tab(nb);
   std::vector<ConnItem> items;
   int maxn = 1;
+  c->tops.clear();
   for (int n = 0; n < nb; n++) {
     tab[n] = c->blocks[n]->db;
+    // 1:1 ghosts are exchanged on level 1 only (BOUNDI(M) of the coarse
+    // levels is commented out in the reference, ns3c.f:1618 / 1843): coarse
+    // ghosts come from TRANSF
+    if (c->blocks[n]->level != 1) continue;
+    c->tops.push_back(c->blocks[n]);
     for (auto& pa : c->blocks[n]->h_patch) {
       if (pa.ityp != FF_BC_CON || pa.ibtype < 0) continue;   // negative: remote source
-      if (pa.ibtype >= nb) return fail(c, FF_ERR_ARG, "connection to an unknown block");
+      if (pa.ibtype >= nb || c->blocks[pa.ibtype]->level != 1)
+        return fail(c, FF_ERR_ARG, "connection to an unknown block (the source must be a level-1 block id)");
       ConnItem it;
       it.dst = n; it.src = pa.ibtype; it.pa = pa;
       items.push_back(it);
@@ -621,7 +643,7 @@ int ensure_conn(Ctx* c) {
     CK(cudaMalloc(&c->d_conn, sizeof(ConnItem) * c->nconn));
     CK(cudaMemcpy(c->d_conn, items.data(), sizeof(ConnItem) * c->nconn, cudaMemcpyHostToDevice));
   }
-  while ((int)c->side.size() < nb) {
+  while (c->side.size() < c->tops.size()) {
     cudaStream_t s; cudaEvent_t e;
     CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -639,14 +661,16 @@ int st_connec(Ctx* c) {
   return 0;
 }
 
-// Run fn(block) for every block on its own stream, forked from and joined
-// back into the context stream (captured as parallel graph branches).
+// Run fn(n) for every level-1 block c->tops[n] on its own stream, forked
+// from and joined back into the context stream (captured as parallel graph
+// branches).
 // Blocks whose sweep is the cooperative hyperplane kernel share the context's
 // grid barrier and need the whole GPU, so their chains run one after another.
 template <typename F>
 int fork_join(Ctx* c, int nb, F fn) {
   bool concurrent = nb > 1;
-  for (int n = 0; n < nb; n++) concurrent = concurrent && c->blocks[n]->use_lines;
+  for (int n = 0; n < nb; n++)
+    for (BlockCtx* x = c->tops[n]; x; x = x->coarse) concurrent = concurrent && x->use_lines;
   if (!concurrent) {
     for (int n = 0; n < nb; n++) {
       int rc = fn(n);
@@ -674,9 +698,9 @@ int fork_join(Ctx* c, int nb, F fn) {
 // BOUNDI ns3c.f:10608 over all blocks: REFCOR, MIR and STATIM per block,
 // CONNEC of every 1:1 patch in one launch, STATIM again.
 int mb_boundi(Ctx* c) {
-  int nb = (int)c->blocks.size(), rc;
+  int nb = (int)c->tops.size(), rc;
   rc = fork_join(c, nb, [&](int n) {
-    BlockCtx* b = c->blocks[n];
+    BlockCtx* b = c->tops[n];
     k_refcor<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db);
     c->nlaunch++;
     if (b->npatch) {
@@ -689,17 +713,21 @@ int mb_boundi(Ctx* c) {
   });
   if (rc) return rc;
   if ((rc = st_connec(c))) return rc;
-  return fork_join(c, nb, [&](int n) { return st_statim(c, c->blocks[n], 1); });
+  return fork_join(c, nb, [&](int n) { return st_statim(c, c->tops[n], 1); });
 }
 
 // One NS3D cycle over all single-grid blocks: CYCLES per block (concurrent
 // branches), then the all-block BOUNDI and SUBIN.
+int mb_mg_cycle(Ctx* c, int icycle);
+
 int mb_cycle(Ctx* c, int icycle) {
-  int nb = (int)c->blocks.size(), rc;
+  int nb = (int)c->tops.size(), rc;
+  for (auto* b : c->tops)
+    if (b->coarse) return mb_mg_cycle(c, icycle);
   k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi, c->d_dromax);
   c->nlaunch++;
   rc = fork_join(c, nb, [&](int n) {
-    BlockCtx* b = c->blocks[n];
+    BlockCtx* b = c->tops[n];
     int r;
     if (b->prm.iturb >= 3 && (r = st_statim(c, b, 1))) return r;
     if ((r = st_residu(c, b, 1, icycle))) return r;
@@ -711,11 +739,47 @@ int mb_cycle(Ctx* c, int icycle) {
   });
   if (rc) return rc;
   if ((rc = mb_boundi(c))) return rc;
-  for (auto* b : c->blocks)
+  for (auto* b : c->tops)
     if (b->prm.iturb >= 3) {
       k_subin_sst<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db, b->prm);
       c->nlaunch++;
     }
+  k_record<<<1, 1, 0, c->stream>>>(c->d_resi, c->d_dromax, c->d_hist, c->d_hist_pos, c->hist_cap);
+  c->nlaunch++;
+  return 0;
+}
+
+// One multigrid cycle of all blocks: every block's mg_body (concurrent
+// branches), BOUNDI over the level-1 blocks (1:1 ghosts on level 1 only),
+// SUBIN per block, then the monitor (RESL2 sums of all blocks, max|DE|).
+int mb_mg_cycle(Ctx* c, int icycle) {
+  int nb = (int)c->tops.size(), rc;
+  k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi, c->d_dromax);
+  c->nlaunch++;
+  rc = fork_join(c, nb, [&](int n) { return mg_body(c, c->tops[n], icycle, false); });
+  if (rc) return rc;
+  if ((rc = mb_boundi(c))) return rc;
+  rc = fork_join(c, nb, [&](int n) {
+    BlockCtx* b = c->tops[n];
+    k_subin_copy<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db);
+    c->nlaunch++;
+    if (b->prm.iturb >= 3) {
+      k_subin_sst<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db, b->prm);
+      c->nlaunch++;
+    }
+    return 0;
+  });
+  if (rc) return rc;
+  k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi + 6, c->d_dromax);
+  c->nlaunch++;
+  rc = fork_join(c, nb, [&](int n) {
+    BlockCtx* b = c->tops[n];
+    int ncell = b->imax * b->jmax * b->kmax;
+    k_maxabs_de<<<min(nblk(ncell, 256), 4 * c->sm_count), 256, 0, c->stream>>>(b->db, c->d_dromax);
+    c->nlaunch++;
+    return 0;
+  });
+  if (rc) return rc;
   k_record<<<1, 1, 0, c->stream>>>(c->d_resi, c->d_dromax, c->d_hist, c->d_hist_pos, c->hist_cap);
   c->nlaunch++;
   return 0;
@@ -731,12 +795,12 @@ int st_halo(Ctx* c, int mode) {
 
 // Multi-GPU phases (see ff_mb_phase in the header).
 int mb_phase(Ctx* c, int phase, int icycle) {
-  int nb = (int)c->blocks.size(), rc;
+  int nb = (int)c->tops.size(), rc;
   if (phase == FF_PHASE_CYCLE_A) {
     k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi, c->d_dromax);
     c->nlaunch++;
     rc = fork_join(c, nb, [&](int n) {
-      BlockCtx* b = c->blocks[n];
+      BlockCtx* b = c->tops[n];
       int r;
       if ((r = st_residu(c, b, 1, icycle))) return r;
       int ncell = b->imax * b->jmax * b->kmax;
@@ -749,7 +813,7 @@ int mb_phase(Ctx* c, int phase, int icycle) {
   }
   if (phase == FF_PHASE_CYCLE_A || phase == FF_PHASE_BOUNDI_A) {
     rc = fork_join(c, nb, [&](int n) {
-      BlockCtx* b = c->blocks[n];
+      BlockCtx* b = c->tops[n];
       k_refcor<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db);
       c->nlaunch++;
       if (b->npatch) {
@@ -766,7 +830,7 @@ int mb_phase(Ctx* c, int phase, int icycle) {
   }
   if (phase == FF_PHASE_B) {
     if ((rc = st_halo(c, 1))) return rc;
-    return fork_join(c, nb, [&](int n) { return st_statim(c, c->blocks[n], 1); });
+    return fork_join(c, nb, [&](int n) { return st_statim(c, c->tops[n], 1); });
   }
   if (phase == FF_PHASE_RECORD) {
     k_record<<<1, 1, 0, c->stream>>>(c->d_resi, c->d_dromax, c->d_hist, c->d_hist_pos, c->hist_cap);
@@ -911,6 +975,7 @@ int ff_mg_link(void* ctx, int fine, int coarse) {
     return fail(c, FF_ERR_ARG, "ff_mg_link: the coarse block must halve every dimension");
   f->coarse = cc;
   cc->level = f->level + 1;
+  c->conn_blocks = -1;   // the level-1 block list changes
   if (f->graph) { cudaGraphExecDestroy(f->graph); f->graph = nullptr; }
   return 0;
 }
@@ -1193,10 +1258,8 @@ int ff_history(void* ctx, int n, double* hist, int reset) {
 int ff_boundi_all(void* ctx) {
   Ctx* c = (Ctx*)ctx;
   if (!c || c->blocks.empty()) return fail(c, FF_ERR_ARG, "ff_boundi_all");
-  for (auto* b : c->blocks)
-    if (b->level != 1) return fail(c, FF_ERR_ARG, "ff_boundi_all: finest-level blocks only");
   int rc;
-  if ((rc = ensure_conn(c))) return rc;
+  if ((rc = ensure_conn(c))) return rc;   // BOUNDI over the level-1 blocks
   if ((rc = mb_boundi(c))) return rc;
   CK(cudaGetLastError());
   return 0;
@@ -1205,8 +1268,6 @@ int ff_boundi_all(void* ctx) {
 int ff_cycles_all(void* ctx, int ncycles, int icycle0, double* hist, int use_graph) {
   Ctx* c = (Ctx*)ctx;
   if (!c || ncycles < 0 || c->blocks.empty()) return fail(c, FF_ERR_ARG, "ff_cycles_all");
-  for (auto* b : c->blocks)
-    if (b->coarse || b->level != 1) return fail(c, FF_ERR_ARG, "ff_cycles_all: single-grid blocks only");
   int rc;
   if ((rc = ensure_conn(c))) return rc;
   if ((rc = ensure_hist(c, max(ncycles, 1)))) return rc;
@@ -1217,7 +1278,7 @@ int ff_cycles_all(void* ctx, int ncycles, int icycle0, double* hist, int use_gra
     it++;
   }
   if (it < ncycles) {
-    int nb = (int)c->blocks.size();
+    int nb = (int)c->tops.size();
     if (!c->mb_graph || c->mb_graph_n != nb) {
       if (c->mb_graph) { cudaGraphExecDestroy(c->mb_graph); c->mb_graph = nullptr; }
       cudaGraph_t g;

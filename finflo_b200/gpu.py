@@ -140,6 +140,7 @@ class GpuSolver:
         ids = [self.add_block(b, p) for b, p in zip(levels, prms)]
         for f, c in zip(ids[:-1], ids[1:]):
             self._check(self.L.ff_mg_link(self.ctx, f, c))
+        self._coarse = list(getattr(self, "_coarse", [])) + ids[1:]
         return ids[0]
 
     def set_params(self, bid: int, prm: FFParams):
@@ -219,13 +220,46 @@ class GpuSolver:
     def boundi_all(self):
         self._check(self.L.ff_boundi_all(self.ctx))
 
+    def add_multiblock(self, block_levels, block_prms):
+        """Blocks joined by 1:1 patches, each with its multigrid levels
+        (finest first; a patch's IBTYPE is the source block's index in
+        block_levels).  The context sees the 1:1 patches of the level-1
+        blocks renumbered to its own block ids; the Block objects keep
+        theirs.  Returns the ids of the level-1 blocks."""
+        from . import grid
+        from .case import FFPatch
+        base = len(self.blocks)
+        fine_ids, n = [], base
+        for levels in block_levels:
+            fine_ids.append(n)
+            n += len(levels)
+        ids = []
+        for levels, prms in zip(block_levels, block_prms):
+            fine = levels[0]
+            orig = fine.patches
+            pats = []
+            for pa in orig:
+                q = FFPatch.from_buffer_copy(pa)
+                if q.ityp == grid.BC_CON and q.ibtype >= 0:
+                    q.ibtype = fine_ids[q.ibtype]
+                pats.append(q)
+            fine.patches = pats
+            try:
+                ids.append(self.add_levels(levels, prms) if len(levels) > 1 else self.add_block(fine, prms[0]))
+            finally:
+                fine.patches = orig
+        assert ids == fine_ids
+        return ids
+
     def start_all(self):
         """NS3D start-up over every block: BOUNDI(1) with the 1:1
-        connections, then the *OLD copies of each block."""
+        connections, then the *OLD copies of each level-1 block."""
         self.boundi_all()
         self.sync()
+        coarse = set(getattr(self, "_coarse", ()))
         for bid in range(len(self.blocks)):
-            self._old_copies(bid)
+            if bid not in coarse:
+                self._old_copies(bid)
 
     def cycles_all(self, n, icycle0=1, use_graph=True) -> np.ndarray:
         """n cycles over every block (multi-block NS3D with 1:1 CONNEC)."""

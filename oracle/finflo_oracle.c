@@ -1524,7 +1524,10 @@ void orc_interp_limits(orc_block *c, orc_block *f, const ff_params *pf) {
 
 /* One multigrid cycle of CYCLES (ns3c.f:1400-2170) with BOUNDI and SUBIN.
  * lv[0] is the fine level; prm[m] are the level's parameters (IDM1..3). */
-void orc_mg_cycle(orc_block **lv, int nlev, const ff_params *prm, int icycle, double *resi5, double *dromax) {
+/* The per-block part of a multigrid cycle (CYCLES ns3c.f:1400-2130): fine
+ * update, the coarse levels down, INTERP back up, REFLEC.  resi5 gets the
+ * RESL2 sums of the level-1 residual after the fine update. */
+void orc_mg_body(orc_block **lv, int nlev, const ff_params *prm, int icycle, double *resi5) {
   orc_block *b = lv[0];
   orc_statim(b, &prm[0]);
   orc_adjuin_laminar(b);
@@ -1548,8 +1551,12 @@ void orc_mg_cycle(orc_block **lv, int nlev, const ff_params *prm, int icycle, do
   }
   for (int m = nlev - 1; m >= 1; m--) orc_interp_limits(lv[m], lv[m - 1], &prm[m - 1]);
   reflec(b, &prm[0]);
-  orc_boundi(b, &prm[0]);
-  orc_subin(b, dromax);
+}
+
+void orc_mg_cycle(orc_block **lv, int nlev, const ff_params *prm, int icycle, double *resi5, double *dromax) {
+  orc_mg_body(lv, nlev, prm, icycle, resi5);
+  orc_boundi(lv[0], &prm[0]);
+  orc_subin(lv[0], dromax);
 }
 
 /* ---------------------------------------------------------------------- */
@@ -1614,6 +1621,40 @@ void orc_mb_cycle(orc_block **blk, int nblk, const ff_params *prm, int icycle, d
   for (int n = 0; n < nblk; n++) {
     double d;
     orc_subin(blk[n], &d);
+    if (d > dm) dm = d;
+  }
+  *dromax = dm;
+}
+
+void orc_mg_body_sst(orc_block **lv, int nlev, const ff_params *prm, int icycle, double *resi5);
+
+/* Several blocks with nlev multigrid levels each (lv and prm hold block n's
+ * levels at [n * nlev .. n * nlev + nlev - 1]): the multigrid part of CYCLES
+ * per block, then BOUNDI over the level-1 blocks and SUBIN.  The reference
+ * exchanges 1:1 ghosts on level 1 only (BOUNDI(M) on the coarse levels is
+ * commented out, ns3c.f:1618 and 1843); coarse ghosts come from TRANSF.
+ * Patch IBTYPE of a 1:1 patch is the source block's index n. */
+void orc_mb_mg_cycle(orc_block **lv, int nblk, int nlev, const ff_params *prm, int icycle, double *resi5,
+                     double *dromax) {
+  for (int v = 0; v < 5; v++) resi5[v] = 0.;
+  orc_block *fine[256];
+  ff_params fprm[256] = {{0}};
+  if (nblk > 256) return;
+  const int sst = prm[0].iturb >= 3;
+  for (int n = 0; n < nblk; n++) {
+    double r[5];
+    if (sst) orc_mg_body_sst(lv + n * nlev, nlev, prm + n * nlev, icycle, r);
+    else orc_mg_body(lv + n * nlev, nlev, prm + n * nlev, icycle, r);
+    for (int v = 0; v < 5; v++) resi5[v] += r[v];
+    fine[n] = lv[n * nlev];
+    fprm[n] = prm[n * nlev];
+  }
+  orc_mb_boundi(fine, nblk, fprm);
+  double dm = 0.;
+  for (int n = 0; n < nblk; n++) {
+    double d;
+    if (sst) orc_subin_sst(fine[n], &fprm[n], &d);
+    else orc_subin(fine[n], &d);
     if (d > dm) dm = d;
   }
   *dromax = dm;

@@ -1240,7 +1240,8 @@ void orc_fin_coarse_sst(orc_block *b, const ff_params *p) {
 }
 
 /* One multigrid SST cycle of CYCLES (same order as orc_mg_cycle). */
-void orc_mg_cycle_sst(orc_block **lv, int nlev, const ff_params *prm, int icycle, double *resi5, double *dromax) {
+/* The per-block part of the k-omega multigrid cycle (see orc_mg_body). */
+void orc_mg_body_sst(orc_block **lv, int nlev, const ff_params *prm, int icycle, double *resi5) {
   orc_block *b = lv[0];
   orc_statim(b, &prm[0]);
   orc_turbeq_sst(b, &prm[0]);
@@ -1265,6 +1266,10 @@ void orc_mg_cycle_sst(orc_block **lv, int nlev, const ff_params *prm, int icycle
   }
   for (int m = nlev - 1; m >= 1; m--) orc_interp_limits(lv[m], lv[m - 1], &prm[m - 1]);
   reflec(b, &prm[0]);
-  orc_boundi(b, &prm[0]);
-  orc_subin_sst(b, &prm[0], dromax);
+}
+
+void orc_mg_cycle_sst(orc_block **lv, int nlev, const ff_params *prm, int icycle, double *resi5, double *dromax) {
+  orc_mg_body_sst(lv, nlev, prm, icycle, resi5);
+  orc_boundi(lv[0], &prm[0]);
+  orc_subin_sst(lv[0], &prm[0], dromax);
 }

@@ -199,3 +199,35 @@ class OracleMB:
         d = ctypes.c_double()
         self.L.orc_mb_cycle(self._ptrs, len(self.blocks), self._prms, icycle, r, ctypes.byref(d))
         return np.array(r[:]), d.value
+
+
+class OracleMBMG:
+    """Blocks joined by 1:1 patches, each with its multigrid levels (finest
+    first), for orc_mb_mg_cycle.  A 1:1 patch's IBTYPE is the source block's
+    index in block_levels."""
+
+    def __init__(self, block_levels, block_prms):
+        self.nblk, self.nlev = len(block_levels), len(block_levels[0])
+        self.objs = [[Oracle(b, p) for b, p in zip(lv, pr)] for lv, pr in zip(block_levels, block_prms)]
+        flat = [o for lv in self.objs for o in lv]
+        self._ptrs = (ctypes.POINTER(OrcBlock) * len(flat))(*[ctypes.pointer(o.ob) for o in flat])
+        self._prms = (FFParams * len(flat))(*[p for pr in block_prms for p in pr])
+        self.fine = OracleMB([lv[0] for lv in block_levels], [pr[0] for pr in block_prms])
+        self.L = lib()
+
+    def start(self):
+        """NS3D start-up over the level-1 blocks: SUBIN, BOUNDI(1), SUBIN (and
+        the k-omega *OLD copies)."""
+        self.fine.start()
+        for lv in self.objs:
+            o = lv[0]
+            if o.prm.iturb >= 3:
+                a = o.blk.arrays
+                a["RKOLD"][:] = a["RK"]
+                a["EPSOLD"][:] = a["REPS"]
+
+    def cycle(self, icycle):
+        r = (ctypes.c_double * 5)()
+        d = ctypes.c_double()
+        self.L.orc_mb_mg_cycle(self._ptrs, self.nblk, self.nlev, self._prms, icycle, r, ctypes.byref(d))
+        return np.array(r[:]), d.value
