@@ -307,6 +307,8 @@ class GpuSolver:
         if self.blocks[bid][1].iturb >= 3:
             pairs += [("RKOLD", "RK"), ("EPSOLD", "REPS")]
             st.update(self.download(bid, ["RK", "REPS"]))
-        for a, b2 in pairs:
-            blk.arrays[a][:] = st[b2]
-        self.upload(bid, [a for a, _ in pairs])
+        for a, b2 in pairs:   # device copies; the host block keeps a copy when it still has arrays
+            self._check(self.L.ff_upload(self.ctx, bid, SLOT[a], _dptr(st[b2])))
+            if a in blk.arrays:
+                blk.arrays[a][:] = st[b2]
+        self.sync()
