@@ -287,12 +287,22 @@ def wall_distance(blk: Block, wall_block: Block = None, nnear: int = 8):
     tree = cKDTree(cen)
     q = np.stack([blk.arrays["XC"], blk.arrays["YC"], blk.arrays["ZC"]], axis=1)
     k = min(nnear, len(cen))
-    _, idx = tree.query(q, k=k)
+    _, idx = tree.query(q, k=k, workers=-1)
     idx = idx.reshape(len(q), k)
     best = np.full(len(q), np.inf)
-    for j in range(k):
-        t = idx[:, j]
-        best = np.minimum(best, _closest_on_triangles(q, A[t], B[t], C[t]))
+
+    def chunk(lo, hi):   # NumPy releases the GIL on these array operations
+        qq, b = q[lo:hi], best[lo:hi]
+        for j in range(k):
+            t = idx[lo:hi, j]
+            np.minimum(b, _closest_on_triangles(qq, A[t], B[t], C[t]), out=b)
+
+    import os
+    from concurrent.futures import ThreadPoolExecutor
+    nth = max(1, min(os.cpu_count() or 1, len(q) // 65536))
+    bounds = np.linspace(0, len(q), nth + 1).astype(int)
+    with ThreadPoolExecutor(nth) as ex:
+        list(ex.map(lambda b: chunk(*b), zip(bounds[:-1], bounds[1:])))
     return best
 
 
