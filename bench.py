@@ -179,6 +179,8 @@ def run_reference(args):
     ws, rank, local = _dist()
     if rank != 0:
         return 0
+    if args.workload == "sst-precision":
+        args.workload = "sst-mg"   # the same workload; the reference has only its FP64 path
     if args.workload == "large":
         print(json.dumps({"impl": "reference", "unavailable": "the 16.8M-cell multi-block case holds ~13 GB of "
                           "host arrays per oracle copy and runs minutes per cycle on the host cores; the CPU "
@@ -477,6 +479,56 @@ def run_large(args):
     return 0
 
 
+def run_precision(args):
+    """The SST V-cycle workload run twice for the same number of cycles,
+    plain FP64 and with the FP32 implicit stage on every level: throughput
+    of each, the density-residual decades reached, and the L2 difference of
+    the FP32 run's fields from the FP64 run's."""
+    ws_, rank, local = _dist()
+    from finflo_b200 import case
+    from finflo_b200.gpu import GpuSolver
+    wl = WORKLOADS["sst-mg"]
+    out = {}
+    fields = {}
+    for tag, fp32 in (("fp64", False), ("fp32", True)):
+        levels, prms, fs = case.bump_case_mg(*wl["nodes"], nlev=wl["nlev"], lusgs_fp32=fp32, coarse_fp32=fp32,
+                                             cfl=args.prec_cfl, cfll=args.prec_cfl, **wl["kw"])
+        g = GpuSolver(local)
+        bid = g.add_levels(levels, prms)
+        for q in range(len(levels)):
+            g.upload(bid + q)
+        g.start(bid)
+        h0 = g.cycles(1, bid, icycle0=1)
+        ms = g.time_cycles(args.prec_cycles - 1, bid)
+        h = g.cycles(1, bid, icycle0=args.prec_cycles + 1)
+        fields[tag] = g.download(bid, wl["state"])
+        blk = levels[0]
+        out[tag] = {"cell_iters_per_s": blk.interior_cells * (args.prec_cycles - 1) / (ms * 1e-3),
+                    "ms_per_cycle": ms / (args.prec_cycles - 1),
+                    "decades": float(0.5 * np.log10(h0[0, 0] / h[0, 0])) if np.isfinite(h[0, 0]) else None}
+        g.close()
+    err = {}
+    ni, nj, nk = (n - 1 for n in wl["nodes"])
+    for n in wl["state"]:
+        a = fields["fp32"][n].reshape(nk + 4, nj + 4, ni + 4)[2:-2, 2:-2, 2:-2]
+        b = fields["fp64"][n].reshape(nk + 4, nj + 4, ni + 4)[2:-2, 2:-2, 2:-2]
+        ref = np.linalg.norm(b) if n != "PDIFF" else np.linalg.norm(b) + 1e-300
+        err[n] = float(np.linalg.norm(a - b) / ref)
+    line = {
+        "metric": "cell-iters/s", "value": out["fp32"]["cell_iters_per_s"], "unit": "cell-iters/s", "n_gpus": ws_,
+        "steps": args.prec_cycles, "warmup": 1, "ms_per_step": out["fp32"]["ms_per_cycle"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 residual / f32 LU-SGS",
+        "data": "synthetic (seeded bump-channel grid and noisy free stream)",
+        "config": {"workload": wl["name"].replace(", FP64", "") + f", CFL {args.prec_cfl:g}, "
+                   f"FP64 vs FP32 implicit stage on every level, {args.prec_cycles} cycles each"},
+        "fp64": out["fp64"], "fp32": out["fp32"], "fp32_l2_error_vs_fp64": err,
+        "e2e": None,
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
 WARM_NAME = ("learned warm start: bump channel 64x32x32 cells, laminar Re=1e4, Mach U[0.3,0.8] x bump "
              "amplitude U[0.05,0.15]; 64 solver solutions (seed 3) train a 4-layer MLP encoder + 3-D "
              "transposed-conv decoder (32 channels, BF16 weights, tcgen05 GEMMs); 16 held-out points (seed 4)")
@@ -525,7 +577,10 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--grid", default="", help="node counts ni,nj,nk (profiling runs)")
-    ap.add_argument("--workload", default="sst-mg", choices=["sst-mg", "bump", "box", "warmstart", "large"])
+    ap.add_argument("--workload", default="sst-mg",
+                    choices=["sst-mg", "bump", "box", "warmstart", "large", "sst-precision"])
+    ap.add_argument("--prec-cycles", type=int, default=2000)
+    ap.add_argument("--prec-cfl", type=float, default=1.0)
     ap.add_argument("--large-cells", default="512,256,128")
     ap.add_argument("--large-fp64", action="store_true", help="FP64 implicit stage in the large case")
     ap.add_argument("--ws-train", type=int, default=64)
@@ -545,6 +600,8 @@ def main():
         return run_warmstart(args)
     if args.workload == "large":
         return run_large(args)
+    if args.workload == "sst-precision":
+        return run_precision(args)
     return run_ours(args)
 
 
