@@ -47,6 +47,12 @@ WORKLOADS = {
 }
 
 
+# DRAM bytes (read + write) of one launch of the dominant kernel, from one
+# ncu capture of the same workload (profiles/k_residual_sst_sstmg128x64x64_full.md:
+# 578.0 MB read + 97.5 MB written, spill traffic included).
+TRAFFIC = {"sst-mg": 675.4e6}
+
+
 def build_case(wl, nodes=None):
     """Blocks (finest first) and parameters of a single-block workload."""
     from finflo_b200 import case
@@ -293,8 +299,9 @@ def run_ours(args):
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "kernel": "k_residual_sst" if prms[0].iturb >= 3 else "k_residual",
                      "achieved": achieved, "peak": peak, "peak_kind": pkind, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None, "ms_per_launch": ms_res,
-                     "bytes_per_cell": bytes_per_cell},
+                     "frac": achieved / peak,
+                     "traffic": TRAFFIC.get(args.workload) if not args.grid else None,
+                     "ms_per_launch": ms_res, "bytes_per_cell": bytes_per_cell},
         "e2e": {"value": e2e, "unit": "cell-iters/s", "h2d_bytes_per_step": h2d // max(1, args.steps),
                 "d2h_bytes_per_step": d2h // max(1, args.steps)},
         "clocks": clocks,
