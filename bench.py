@@ -269,6 +269,7 @@ def run_ours(args):
     launches = g.cycle_launches(bid) * args.steps
     lk = g.lusgs_kind(bid)
     chosen = (f"cluster lines, {lk // 100} CTAs" if lk % 100 == 1
+              else f"pipelined tile wavefront, {lk // 100} tiles" if lk % 100 == 3
               else f"cooperative hyperplane, {lk // 100} threads/CTA")
     sweep = dict(g.sweep_tuning(bid), chosen=chosen, ms_per_sweep=ms_sweep)
     # ---- end to end through the C-ABI with host buffers ----------------

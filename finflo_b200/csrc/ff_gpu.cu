@@ -34,6 +34,12 @@ struct BlockCtx {
   unsigned long long* d_red = nullptr;   // per-block reduction word (FUN1KO CDMAX)
   int coop_threads = 128;       // threads per CTA of the hyperplane sweep (tune_sweep)
   int use_lines = 0;            // 1: cluster line-wavefront LU-SGS
+  int can_lines = 0;            // the line sweep fits one cluster
+  int can_pipe = 0, use_pipe = 0;   // pipelined tile wavefront possible / chosen
+  int pipe_tk = 0;              // its tile height along k (8, 16 or 32 lines)
+  bool pipe_stage = false;
+  PipeGeom pg{};
+  float pipe_ms = 0.f;          // measured upper sweep of the pipelined kernel
   int tuned = 0;                // sweep kind chosen by tune_sweep
   float sweep_ms[2] = {0.f, 0.f};   // measured upper sweep: lines, best hyperplane
   LineGeom lg{};
@@ -389,11 +395,146 @@ int setup_lines(Ctx* c, BlockCtx* b) {
     b->lg = lg;
     b->lines_stage = stage;
     b->use_lines = 1;
+    b->can_lines = 1;
     return 0;
   }
   b->use_lines = 0;
+  b->can_lines = 0;
   return 0;
 }
+// ---- pipelined tile wavefront (k_lusgs_pipe) ------------------------------
+template <typename CT, int NV, int TK, bool ST>
+cudaError_t pipe_launch(cudaLaunchConfig_t* cfg, BlockCtx* b, const CT* sw, CT* dwp, int upper, int* err) {
+  return cudaLaunchKernelEx(cfg, k_lusgs_pipe<CT, NV, TK, ST>, b->db, sw, dwp, upper, b->pg, err);
+}
+
+template <typename CT, int NV, int TK>
+cudaError_t pipe_launch_st(cudaLaunchConfig_t* cfg, BlockCtx* b, const CT* sw, CT* dwp, int upper, int* err,
+                           bool st) {
+  return st ? pipe_launch<CT, NV, TK, true>(cfg, b, sw, dwp, upper, err)
+            : pipe_launch<CT, NV, TK, false>(cfg, b, sw, dwp, upper, err);
+}
+
+template <typename CT, int NV>
+cudaError_t pipe_launch_tk(cudaLaunchConfig_t* cfg, BlockCtx* b, const CT* sw, CT* dwp, int upper, int* err) {
+  switch (b->pipe_tk) {
+    case 8: return pipe_launch_st<CT, NV, 8>(cfg, b, sw, dwp, upper, err, b->pipe_stage);
+    case 16: return pipe_launch_st<CT, NV, 16>(cfg, b, sw, dwp, upper, err, b->pipe_stage);
+    default: return pipe_launch_st<CT, NV, 32>(cfg, b, sw, dwp, upper, err, b->pipe_stage);
+  }
+}
+
+int pipe_sweep(Ctx* c, BlockCtx* b, int upper, bool fp32) {
+  const int nv = b->prm.iturb >= 3 ? 7 : 5;
+  const int ntiles = b->pg.ntj * b->pg.ntk;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(ntiles);
+  cfg.blockDim = dim3(PTJ * b->pipe_tk);
+  cfg.dynamicSmemBytes = pipe_smem_bytes(nv, b->pipe_tk, fp32 ? sizeof(float) : sizeof(double), b->pipe_stage);
+  cfg.stream = c->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = ntiles;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaError_t e;
+  if (nv == 7)
+    e = fp32 ? pipe_launch_tk<float, 7>(&cfg, b, b->sw32, b->dwp32, upper, c->d_err)
+             : pipe_launch_tk<double, 7>(&cfg, b, b->sw, b->dwp, upper, c->d_err);
+  else
+    e = fp32 ? pipe_launch_tk<float, 5>(&cfg, b, b->sw32, b->dwp32, upper, c->d_err)
+             : pipe_launch_tk<double, 5>(&cfg, b, b->sw, b->dwp, upper, c->d_err);
+  if (e != cudaSuccess) return fail(c, FF_ERR_CUDA, "pipelined sweep launch", e);
+  c->nlaunch++;
+  return 0;
+}
+
+int g_pipe_smem[kMaxDev][2][2][3][2];   // granted dynamic shared memory per device and instantiation
+
+template <typename CT, int NV, int TK, bool ST>
+int pipe_attr(Ctx* c, size_t smem) {
+  int& g = g_pipe_smem[c->device][sizeof(CT) == 4][NV == 7][TK == 8 ? 0 : (TK == 16 ? 1 : 2)][ST];
+  if ((int)smem <= g) return 0;
+  CK(cudaFuncSetAttribute(k_lusgs_pipe<CT, NV, TK, ST>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  CK(cudaFuncSetAttribute(k_lusgs_pipe<CT, NV, TK, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  g = (int)smem;
+  return 0;
+}
+
+template <typename CT, int NV, int TK, bool ST>
+int pipe_fits(Ctx* c, int ntiles, size_t smem, bool* ok) {
+  *ok = false;
+  int rc = pipe_attr<CT, NV, TK, ST>(c, smem);
+  if (rc) return rc;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(ntiles);
+  cfg.blockDim = dim3(PTJ * TK);
+  cfg.dynamicSmemBytes = smem;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = ntiles; attr[0].val.clusterDim.y = 1; attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  cudaError_t e = cudaOccupancyMaxActiveClusters(&n, k_lusgs_pipe<CT, NV, TK, ST>, &cfg);
+  if (e != cudaSuccess) { cudaGetLastError(); return 0; }
+  *ok = n >= 1;
+  return 0;
+}
+
+template <typename CT, int NV, int TK>
+int pipe_try(Ctx* c, BlockCtx* b, int ntiles, bool* found) {
+  const size_t st_b = pipe_smem_bytes(NV, TK, sizeof(CT), true), un_b = pipe_smem_bytes(NV, TK, sizeof(CT), false);
+  bool ok = false;
+  int rc;
+  *found = false;
+  if (st_b <= (size_t)c->smem_optin) {
+    if ((rc = pipe_fits<CT, NV, TK, true>(c, ntiles, st_b, &ok))) return rc;
+    if (ok) { b->pipe_stage = true; *found = true; return 0; }
+  }
+  if (un_b <= (size_t)c->smem_optin) {
+    if ((rc = pipe_fits<CT, NV, TK, false>(c, ntiles, un_b, &ok))) return rc;
+    if (ok) { b->pipe_stage = false; *found = true; }
+  }
+  return 0;
+}
+
+template <int TK>
+int pipe_try_tk(Ctx* c, BlockCtx* b, int ntiles, bool* found) {
+  const bool fp32 = b->prm.lusgs_fp32 != 0, ke = b->prm.iturb >= 3;
+  if (fp32) return ke ? pipe_try<float, 7, TK>(c, b, ntiles, found) : pipe_try<float, 5, TK>(c, b, ntiles, found);
+  return ke ? pipe_try<double, 7, TK>(c, b, ntiles, found) : pipe_try<double, 5, TK>(c, b, ntiles, found);
+}
+
+// The pipelined tile wavefront fits when the (j,k) lines make at most 16
+// tiles of 16 x TK (the smallest TK of 8, 16, 32 that does; more tiles, more
+// SMs) and one cluster of them can be resident.
+int setup_pipe(Ctx* c, BlockCtx* b) {
+  b->can_pipe = 0;
+  const int tks[3] = {8, 16, 32};
+  for (int q = 0; q < 3; q++) {
+    const int tk = tks[q];
+    PipeGeom pg;
+    pg.ntj = (b->jmax + PTJ - 1) / PTJ;
+    pg.ntk = (b->kmax + tk - 1) / tk;
+    if (pg.ntj * pg.ntk > 16) continue;
+    bool found = false;
+    const int nt = pg.ntj * pg.ntk;
+    int rc = tk == 8 ? pipe_try_tk<8>(c, b, nt, &found)
+                     : (tk == 16 ? pipe_try_tk<16>(c, b, nt, &found) : pipe_try_tk<32>(c, b, nt, &found));
+    if (rc) return rc;
+    if (found) {
+      b->pg = pg;
+      b->pipe_tk = tk;
+      b->can_pipe = 1;
+      return 0;
+    }
+  }
+  return 0;
+}
+
 // Sweep data of one sweep in the sweep layout (and, for upper = 1, the
 // right-hand side copied into it).
 void sweep_coef(Ctx* c, BlockCtx* b, int upper, bool fp32) {
@@ -405,32 +546,40 @@ void sweep_coef(Ctx* c, BlockCtx* b, int upper, bool fp32) {
   c->nlaunch++;
 }
 
-// Sweep autotuner: a cluster line sweep uses at most 16 SMs per block, the
-// cooperative hyperplane sweep the whole GPU with a barrier per plane; which
-// is faster, and the hyperplane kernel's CTA size, depend on the block's
-// shape.  Time each candidate (upper sweep in the block's precision, on its
-// current state, in the block's own sweep buffers, which hold nothing
-// between implicit stages) and keep the fastest.  Blocks that run side by
-// side in a multi-block cycle keep the line sweep (see fork_join).
+// Sweep autotuner.  Candidates: the pipelined tile wavefront and the cluster
+// line sweep (each in one cluster of at most 16 CTAs), and the cooperative
+// hyperplane sweep over the whole GPU at 64/128/256 threads per CTA.  Which
+// is fastest depends on the block's shape.  Each candidate is timed (upper
+// sweep in the block's precision, on its current state, in the block's own
+// sweep buffers, which hold nothing between implicit stages) and the
+// fastest is kept.  FINFLO_LUSGS=pipe|lines|hyperplane restricts the choice.
+// Blocks that run side by side in a multi-block cycle use cluster sweeps
+// (see fork_join).
 int tune_sweep(Ctx* c, BlockCtx* b) {
   if (b->tuned) return 0;
   b->tuned = 1;
   const char* env = getenv("FINFLO_LUSGS");
   const bool fp32 = b->prm.lusgs_fp32 != 0;
   const int threads[3] = {64, 128, 256};
+  const bool only = env && (!strcmp(env, "pipe") || !strcmp(env, "lines") || !strcmp(env, "hyperplane"));
+  const bool try_pipe = b->can_pipe && (!only || !strcmp(env, "pipe"));
+  const bool try_lines = b->can_lines && (!only || !strcmp(env, "lines"));
+  bool try_hyp = !only || !strcmp(env, "hyperplane");
+  if (!try_pipe && !try_lines) try_hyp = true;   // nothing else fits
   sweep_coef(c, b, 1, fp32);
-  float best_lines = 0.f, best_hyp = 0.f;
+  float best_k[3] = {0.f, 0.f, 0.f};   // pipe, lines, hyperplane
   int best_t = b->coop_threads;
-  const bool try_lines = b->use_lines && !(env && !strcmp(env, "hyperplane"));
-  const bool try_hyp = !(env && !strcmp(env, "lines") && b->use_lines);
   int rc = 0;
-  for (int kind = 0; kind < 4 && !rc; kind++) {
-    if (kind == 0 && !try_lines) continue;
-    if (kind > 0 && !try_hyp) continue;
+  b->use_pipe = 0;
+  for (int kind = 0; kind < 5 && !rc; kind++) {
+    if (kind == 0 && !try_pipe) continue;
+    if (kind == 1 && !try_lines) continue;
+    if (kind > 1 && !try_hyp) continue;
     float best = 0.f;
     for (int rep = 0; rep < 4 && !rc; rep++) {   // rep 0 warms up
       cudaEventRecord(c->ev0, c->stream);
-      rc = kind == 0 ? lines_sweep(c, b, 1, fp32) : coop_sweep_n(c, b, 1, fp32, threads[kind - 1]);
+      rc = kind == 0 ? pipe_sweep(c, b, 1, fp32)
+                     : (kind == 1 ? lines_sweep(c, b, 1, fp32) : coop_sweep_n(c, b, 1, fp32, threads[kind - 2]));
       if (rc) break;
       cudaEventRecord(c->ev1, c->stream);
       cudaError_t s2 = cudaEventSynchronize(c->ev1);
@@ -439,18 +588,30 @@ int tune_sweep(Ctx* c, BlockCtx* b) {
       cudaEventElapsedTime(&ms, c->ev0, c->ev1);
       if (rep > 0) best = rep == 1 ? ms : fminf(best, ms);
     }
-    if (kind == 0) best_lines = best;
-    else if (best_hyp == 0.f || best < best_hyp) { best_hyp = best; best_t = threads[kind - 1]; }
+    if (kind < 2) best_k[kind] = best;
+    else if (best_k[2] == 0.f || best < best_k[2]) { best_k[2] = best; best_t = threads[kind - 2]; }
   }
   if (rc) return rc;
-  b->sweep_ms[0] = best_lines;
-  b->sweep_ms[1] = best_hyp;
+  int herr = 0;
+  CK(cudaMemcpy(&herr, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (herr) return fail(c, FF_ERR_TIMEOUT, "sweep autotune: a bounded wait gave up");
+  b->pipe_ms = best_k[0];
+  b->sweep_ms[0] = best_k[1];
+  b->sweep_ms[1] = best_k[2];
   b->coop_threads = best_t;
-  if (try_lines && try_hyp && best_hyp < best_lines) b->use_lines = 0;
+  // the fastest measured candidate
+  int pick = -1;
+  float bt = 0.f;
+  for (int k = 0; k < 3; k++)
+    if (best_k[k] > 0.f && (pick < 0 || best_k[k] < bt)) { pick = k; bt = best_k[k]; }
+  b->use_pipe = pick == 0;
+  b->use_lines = pick == 1 ? 1 : 0;
+  if (pick == 0) b->use_lines = 0;
   return 0;
 }
 
 int sweep(Ctx* c, BlockCtx* b, int upper, bool fp32) {
+  if (b->use_pipe) return pipe_sweep(c, b, upper, fp32);
   return b->use_lines ? lines_sweep(c, b, upper, fp32) : coop_sweep(c, b, upper, fp32);
 }
 
@@ -670,7 +831,7 @@ template <typename F>
 int fork_join(Ctx* c, int nb, F fn) {
   bool concurrent = nb > 1;
   for (int n = 0; n < nb; n++)
-    for (BlockCtx* x = c->tops[n]; x; x = x->coarse) concurrent = concurrent && x->use_lines;
+    for (BlockCtx* x = c->tops[n]; x; x = x->coarse) concurrent = concurrent && (x->use_lines || x->use_pipe);
   if (!concurrent) {
     for (int n = 0; n < nb; n++) {
       int rc = fn(n);
@@ -960,8 +1121,10 @@ int ff_block_add(void* ctx, int imax, int jmax, int kmax, int npatch, const ff_p
   {
     int rc = setup_lines(c, b);
     if (rc) return rc;
+    if ((rc = setup_pipe(c, b))) return rc;
     const char* env = getenv("FINFLO_LUSGS");
     if (env && strcmp(env, "hyperplane") == 0) b->use_lines = 0;
+    if (env && strcmp(env, "pipe") == 0 && b->can_pipe) { b->use_pipe = 1; b->use_lines = 0; }
   }
   b->tuned = 0;
   c->blocks.push_back(b);
@@ -994,6 +1157,11 @@ int ff_block_params(void* ctx, int blk, const ff_params* prm) {
   if (fp_changed) {
     int rc = alloc_sweep(c, b);
     if (rc) return rc;
+  }
+  if (nv_changed || fp_changed) {   // the pipelined sweep's instantiation and shared memory
+    int rc = setup_pipe(c, b);
+    if (rc) return rc;
+    if (!b->can_pipe) b->use_pipe = 0;
   }
   if (nv_changed || fp_changed) b->tuned = 0;
   // captured cycles of any block may include this one (multigrid levels)
@@ -1163,9 +1331,21 @@ int ff_sweep_tuning(void* ctx, int blk, float* ms2) {
   return 0;
 }
 
+int ff_sweep_times(void* ctx, int blk, float* ms3) {
+  Ctx* c = (Ctx*)ctx;
+  BlockCtx* b = getb(c, blk);
+  if (!b || !ms3) return fail(c, FF_ERR_ARG, "ff_sweep_times");
+  ms3[0] = b->pipe_ms;
+  ms3[1] = b->sweep_ms[0];
+  ms3[2] = b->sweep_ms[1];
+  return 0;
+}
+
 int ff_lusgs_kind(void* ctx, int blk) {
   BlockCtx* b = getb((Ctx*)ctx, blk);
-  return b ? (b->use_lines ? 1 + b->lg.cs * 100 : 2 + b->coop_threads * 100) : -FF_ERR_ARG;
+  if (!b) return -FF_ERR_ARG;
+  if (b->use_pipe) return 3 + 100 * b->pg.ntj * b->pg.ntk;
+  return b->use_lines ? 1 + b->lg.cs * 100 : 2 + b->coop_threads * 100;
 }
 
 int ff_cycle_launches(void* ctx, int blk) {

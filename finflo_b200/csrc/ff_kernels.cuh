@@ -1447,3 +1447,5 @@ __global__ void __launch_bounds__(LTHREADS * (STAGE ? LMAX_TPC_STAGE : LMAX_TPC)
     cluster_wait_acquire();
   }
 }
+
+#include "ff_pipe.cuh"

@@ -88,6 +88,7 @@ def lib():
         L.ff_cycle_launches.argtypes = [vp, ci]
         L.ff_lusgs_kind.argtypes = [vp, ci]
         L.ff_sweep_tuning.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_float)]
+        L.ff_sweep_times.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_float)]
         L.ff_imps_noalloc.argtypes = [ci, ci, ci, ctypes.POINTER(FFParams), ctypes.POINTER(vp), ci, vp]
         _LIB = L
     return _LIB
@@ -282,9 +283,9 @@ class GpuSolver:
         return self.L.ff_lusgs_kind(self.ctx, bid)
 
     def sweep_tuning(self, bid=0):
-        ms = (ctypes.c_float * 2)()
-        self._check(self.L.ff_sweep_tuning(self.ctx, bid, ms))
-        return {"lines_ms": ms[0], "hyperplane_ms": ms[1]}
+        ms = (ctypes.c_float * 3)()
+        self._check(self.L.ff_sweep_times(self.ctx, bid, ms))
+        return {"pipe_ms": ms[0], "lines_ms": ms[1], "hyperplane_ms": ms[2]}
 
     def cycle_launches(self, bid=0) -> int:
         return self.L.ff_cycle_launches(self.ctx, bid)

@@ -148,6 +148,10 @@ int ff_cycle_launches(void *ctx, int blk);
  * cooperative hyperplane} of a block (zeros until its first ff_cycles call
  * or sweep stage timing; lines 0 where the lines do not fit a cluster). */
 int ff_sweep_tuning(void *ctx, int blk, float *ms2);
+/* The autotuner's measured upper-sweep times in ms {pipelined tile
+ * wavefront, cluster lines, fastest cooperative hyperplane} (zero where not
+ * tried).  LU-SGS kind 3 + 100*tiles = the pipelined tile wavefront. */
+int ff_sweep_times(void *ctx, int blk, float *ms3);
 int ff_lusgs_kind(void *ctx, int blk);
 int ff_time_cycles(void *ctx, int blk, int ncycles, float *ms);
 int ff_time_stage(void *ctx, int blk, int stage, int reps, float *ms);

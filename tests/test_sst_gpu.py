@@ -116,6 +116,37 @@ def test_sst_line_and_hyperplane_sweeps_agree(gpu_lib, monkeypatch):
     g1.close(); g2.close()
 
 
+@pytest.mark.parametrize("fp32", [False, True])
+def test_sst_pipe_and_hyperplane_sweeps_agree(gpu_lib, monkeypatch, fp32):
+    """Seven-equation pipelined tile-wavefront sweeps against the cooperative
+    hyperplane kernel, FP64 and FP32."""
+    monkeypatch.setenv("FINFLO_LUSGS", "pipe")
+    bg1, bc, prm, fs = make_pair(33, 33, 17, **SST)
+    prm.lusgs_fp32 = int(fp32)
+    g1 = GpuSolver(0)
+    b1 = g1.add_block(bg1, prm)
+    assert g1.lusgs_kind(b1) % 100 == 3
+    g1.upload(b1)
+    g1.start(b1)
+    monkeypatch.setenv("FINFLO_LUSGS", "hyperplane")
+    g2 = GpuSolver(0)
+    bg2 = make_pair(33, 33, 17, **SST)[0]
+    b2 = g2.add_block(bg2, prm)
+    assert g2.lusgs_kind(b2) % 100 == 2
+    g2.upload(b2)
+    g2.start(b2)
+    for g, b in ((g1, b1), (g2, b2)):
+        g.residu(b, 1, 1)
+        g.imps(b, 1)
+    d1 = g1.download(b1, list(RES7))
+    d2 = g2.download(b2, list(RES7))
+    for n in RES7:
+        a, c = interior(bg1, d1[n]), interior(bg2, d2[n])
+        err = np.abs(a - c).max() / (np.abs(c).max() + 1e-300)
+        assert err <= (1e-5 if fp32 else 1e-12), (n, err)
+    g1.close(); g2.close()
+
+
 def test_sst_fp32_lusgs_tracks_fp64(gpu_lib):
     """FP32 seven-equation implicit operator: same fixed point, bounded
     difference from the FP64 run after the same cycles."""
