@@ -275,6 +275,7 @@ def run_ours(args):
     # ---- end to end through the C-ABI with host buffers ----------------
     names_in = wl["state"]
     host = {n: blk.arrays[n] for n in names_in}
+    g.pin(list(host.values()))   # page-locked host buffers, as a host that streams its arrays would use
     h2d = d2h = 0
     t0 = time.perf_counter()
     for s in range(0 if args.no_e2e else args.steps):
@@ -285,6 +286,7 @@ def run_ours(args):
         d2h += 8 * blk.ntot * len(names_in) + hist.nbytes
     g.sync()
     e2e_s = time.perf_counter() - t0
+    g.unpin(list(host.values()))
     e2e_s = _allreduce_max(e2e_s, ws)
     e2e = ncell * args.steps * ws / e2e_s if not args.no_e2e else None
     line = {

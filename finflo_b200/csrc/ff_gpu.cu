@@ -1179,6 +1179,20 @@ int ff_upload(void* ctx, int blk, int slot, const double* host) {
   return 0;
 }
 
+int ff_host_register(void* ctx, void* host, size_t bytes) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !host || !bytes) return fail(c, FF_ERR_ARG, "ff_host_register");
+  CK(cudaHostRegister(host, bytes, cudaHostRegisterDefault));
+  return 0;
+}
+
+int ff_host_unregister(void* ctx, void* host) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !host) return fail(c, FF_ERR_ARG, "ff_host_unregister");
+  CK(cudaHostUnregister(host));
+  return 0;
+}
+
 int ff_download(void* ctx, int blk, int slot, double* host) {
   Ctx* c = (Ctx*)ctx;
   BlockCtx* b = getb(c, blk);

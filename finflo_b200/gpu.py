@@ -89,6 +89,8 @@ def lib():
         L.ff_lusgs_kind.argtypes = [vp, ci]
         L.ff_sweep_tuning.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_float)]
         L.ff_sweep_times.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_float)]
+        L.ff_host_register.argtypes = [vp, vp, ctypes.c_size_t]
+        L.ff_host_unregister.argtypes = [vp, vp]
         L.ff_imps_noalloc.argtypes = [ci, ci, ci, ctypes.POINTER(FFParams), ctypes.POINTER(vp), ci, vp]
         _LIB = L
     return _LIB
@@ -152,6 +154,17 @@ class GpuSolver:
         for n in names or SLOTS:
             self._check(self.L.ff_upload(self.ctx, bid, SLOT[n], _dptr(blk.arrays[n])))
         self.sync()
+
+    def pin(self, arrays):
+        """Page-lock host arrays used for every-cycle uploads/downloads;
+        returns them (call unpin before they are freed)."""
+        for a in arrays:
+            self._check(self.L.ff_host_register(self.ctx, a.ctypes.data, a.nbytes))
+        return arrays
+
+    def unpin(self, arrays):
+        for a in arrays:
+            self._check(self.L.ff_host_unregister(self.ctx, a.ctypes.data))
 
     def download(self, bid: int, names=None, into=None) -> dict:
         blk = self.blocks[bid][0]

@@ -49,6 +49,13 @@ int ff_mg_link(void *ctx, int fine, int coarse);
 /* Host <-> device copy of one per-cell array slot (enum ff_slot), NTOT doubles. */
 int ff_upload(void *ctx, int blk, int slot, const double *host);
 int ff_download(void *ctx, int blk, int slot, double *host);
+/* Page-lock (and release) a host array that ff_upload / ff_download use
+ * every cycle, so the copies run as direct DMA at full PCIe/NVLink-C2C rate
+ * instead of through a staging buffer.  Nothing is allocated on the device;
+ * the host memory stays the caller's.  No reference counterpart (the
+ * reference's arrays never leave the host). */
+int ff_host_register(void *ctx, void *host, size_t bytes);
+int ff_host_unregister(void *ctx, void *host);
 void *ff_device_ptr(void *ctx, int blk, int slot);
 void *ff_stream(void *ctx);
 int ff_synchronize(void *ctx);
