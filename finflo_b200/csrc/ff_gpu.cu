@@ -9,6 +9,9 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 #include "ff_kernels.cuh"
 #include "../../include/finflo_gpu.h"
@@ -555,10 +558,37 @@ void sweep_coef(Ctx* c, BlockCtx* b, int upper, bool fp32) {
 // fastest is kept.  FINFLO_LUSGS=pipe|lines|hyperplane restricts the choice.
 // Blocks that run side by side in a multi-block cycle use cluster sweeps
 // (see fork_join).
+// The autotuner's choice per device, block shape, equation count and
+// precision, kept for the life of the process: a later context with a block
+// of the same shape takes it without timing again.
+struct TuneKey {
+  int dev, imax, jmax, kmax, nv, fp32;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(dev, imax, jmax, kmax, nv, fp32) < std::tie(o.dev, o.imax, o.jmax, o.kmax, o.nv, o.fp32);
+  }
+};
+struct TuneVal {
+  int use_pipe, use_lines, coop_threads;
+  float pipe_ms, lines_ms, hyp_ms;
+};
+std::map<TuneKey, TuneVal> g_tune_cache;
+std::mutex g_tune_mu;
+
 int tune_sweep(Ctx* c, BlockCtx* b) {
   if (b->tuned) return 0;
   b->tuned = 1;
   const char* env = getenv("FINFLO_LUSGS");
+  const TuneKey key{c->device, b->imax, b->jmax, b->kmax, b->prm.iturb >= 3 ? 7 : 5, b->prm.lusgs_fp32 != 0};
+  if (!env) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end() && (!it->second.use_pipe || b->can_pipe) && (!it->second.use_lines || b->can_lines)) {
+      const TuneVal& v = it->second;
+      b->use_pipe = v.use_pipe; b->use_lines = v.use_lines; b->coop_threads = v.coop_threads;
+      b->pipe_ms = v.pipe_ms; b->sweep_ms[0] = v.lines_ms; b->sweep_ms[1] = v.hyp_ms;
+      return 0;
+    }
+  }
   const bool fp32 = b->prm.lusgs_fp32 != 0;
   const int threads[3] = {64, 128, 256};
   const bool only = env && (!strcmp(env, "pipe") || !strcmp(env, "lines") || !strcmp(env, "hyperplane"));
@@ -607,6 +637,10 @@ int tune_sweep(Ctx* c, BlockCtx* b) {
   b->use_pipe = pick == 0;
   b->use_lines = pick == 1 ? 1 : 0;
   if (pick == 0) b->use_lines = 0;
+  if (!env) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = TuneVal{b->use_pipe, b->use_lines, b->coop_threads, b->pipe_ms, b->sweep_ms[0], b->sweep_ms[1]};
+  }
   return 0;
 }
 
