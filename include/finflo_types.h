@@ -64,7 +64,8 @@ typedef struct ff_params {
   int idi1, idi2, idi3;                 /* viscous extents IDI1..3 (nodes)    */
   int coarse_inter;                     /* INTEM on coarse levels (55)        */
   int lusgs_fp32;                       /* 1: implicit operator in FP32       */
-  int pad0;
+  int ddadi;                            /* 1: DDADI (LUSGS=0, imps3.f:320),    */
+                                        /* 0: LU-SGS (LUSGS=1, imps3.f:378)    */
 } ff_params;
 
 /* Per-cell array slots of one block (names are the reference's MAIN_ARRAYS,

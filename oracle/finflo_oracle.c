@@ -1214,15 +1214,22 @@ void orc_corrgs(orc_block *b, const ff_params *p) {
   free(cd); free(xi); free(xj); free(xk); free(dt); free(scinv); free(scinp); free(yd); free(bd);
 }
 
-/* IMPS imps3.f:6 (LUSGS=1, laminar): TIME3, LOCDT, COPR, PREDGS, DIAGGS,
- * CORRGS, then DRO/CP (dh -> dT, imps3.f:483). */
+static void ddadi_sweeps(orc_block *b, const ff_params *p, int nv);
+
+/* IMPS imps3.f:6 (laminar): TIME3, LOCDT, COPR, then PREDGS, DIAGGS, CORRGS
+ * (LUSGS=1) or the DDADI line sweeps (LUSGS=0, imps3.f:320), then DRO/CP
+ * (dh -> dT, imps3.f:483). */
 void orc_imps(orc_block *b, const ff_params *p, int level) {
   dims_t d = dims_of(b);
   orc_time3(b, p, level == 1 ? p->cfl : p->cfll);
   orc_locdt_copr(b);
-  orc_predgs(b, p);
-  orc_diaggs(b, p);
-  orc_corrgs(b, p);
+  if (p->ddadi) {
+    ddadi_sweeps(b, p, 5);
+  } else {
+    orc_predgs(b, p);
+    orc_diaggs(b, p);
+    orc_corrgs(b, p);
+  }
   for (int K = 1; K <= d.kmax; K++)
     for (int J = 1; J <= d.jmax; J++)
       for (int I = 1; I <= d.imax; I++) {
@@ -1695,3 +1702,4 @@ void orc_halo_unpack(orc_block *dst, const ff_patch *pa, const double *in) {
 }
 
 #include "finflo_oracle_sst.c"
+#include "finflo_oracle_ddadi.c"

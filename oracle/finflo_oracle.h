@@ -39,6 +39,7 @@ void orc_predgs(orc_block *b, const ff_params *p);
 void orc_diaggs(orc_block *b, const ff_params *p);
 void orc_corrgs(orc_block *b, const ff_params *p);
 void orc_imps(orc_block *b, const ff_params *p, int level);
+void orc_ddadi(orc_block *b, const ff_params *p);
 void orc_fin_limits(orc_block *b, const ff_params *p);
 void orc_refcor(orc_block *b);
 void orc_mir(orc_block *b);

@@ -1041,15 +1041,20 @@ static void cokegs(orc_block *b, const ff_params *p) {
   free(cd); free(xi); free(xj); free(xk); free(dt); free(scinv); free(scinp); free(yd); free(bd);
 }
 
-/* IMPS imps3.f:6 for SST (LUSGS=1, JRIMP=0): TIME3, LOCDTK, IMSOKO, COPRKE,
- * PRKEGS, DIKEGS, COKEGS, DRO/CP, DRK and DEPS times RO. */
+/* IMPS imps3.f:6 for SST (JRIMP=0): TIME3, LOCDTK, IMSOKO, COPRKE, then
+ * PRKEGS, DIKEGS, COKEGS (LUSGS=1) or the DDADI line sweeps (LUSGS=0), then
+ * DRO/CP, DRK and DEPS times RO. */
 void orc_imps_sst_lev(orc_block *b, const ff_params *p, int lev) {
   dims_t d = dims_of(b);
   orc_time3(b, p, lev == 1 ? p->cfl : p->cfll);
   locdtk_imsoko_coprke(b, p);
-  prkegs(b, p);
-  dikegs(b, p);
-  cokegs(b, p);
+  if (p->ddadi) {   /* LUSGS=0: PREDKE, DIAGKE, CORRKE per direction */
+    ddadi_sweeps(b, p, 7);
+  } else {
+    prkegs(b, p);
+    dikegs(b, p);
+    cokegs(b, p);
+  }
   for (int K = 1; K <= d.kmax; K++)
     for (int J = 1; J <= d.jmax; J++)
       for (int I = 1; I <= d.imax; I++) {

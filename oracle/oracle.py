@@ -109,6 +109,9 @@ class Oracle:
     def corrgs(self):
         self.L.orc_corrgs(self._b(), self._p())
 
+    def ddadi(self):
+        self.L.orc_ddadi(self._b(), self._p())
+
     def fin_limits(self):
         self.L.orc_fin_limits(self._b(), self._p())
 
