@@ -242,6 +242,9 @@ def run_ours(args):
     wl = WORKLOADS[args.workload]
     nodes = tuple(int(x) for x in args.grid.split(",")) if args.grid else None
     levels, prms = build_case(wl, nodes)
+    if args.ddadi:   # LUSGS=0: the reference's default implicit stage
+        for q in prms:
+            q.ddadi = 1
     blk = levels[0]
     g = GpuSolver(local)
     bid = g.add_levels(levels, prms) if len(levels) > 1 else g.add_block(blk, prms[0])
@@ -268,7 +271,8 @@ def run_ours(args):
     peak, pkind = _peaks()
     launches = g.cycle_launches(bid) * args.steps
     lk = g.lusgs_kind(bid)
-    chosen = (f"cluster lines, {lk // 100} CTAs" if lk % 100 == 1
+    chosen = ("DDADI k, i, j line sweeps, one thread per line" if args.ddadi
+              else f"cluster lines, {lk // 100} CTAs" if lk % 100 == 1
               else f"pipelined tile wavefront, {lk // 100} tiles" if lk % 100 == 3
               else f"cooperative hyperplane, {lk // 100} threads/CTA")
     sweep = dict(g.sweep_tuning(bid), chosen=chosen, ms_per_sweep=ms_sweep)
@@ -294,7 +298,8 @@ def run_ours(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": wl["dtype"],
         "data": "synthetic (seeded bump-channel grid and noisy free stream)",
-        "config": {"workload": wl["name"] if not args.grid else
+        "config": {"workload": (wl["name"] + (", DDADI implicit stage (LUSGS=0)" if args.ddadi else ""))
+                   if not args.grid else
                    f"{args.workload} at {blk.imax}x{blk.jmax}x{blk.kmax} cells (profiling size)",
                    "cells_per_gpu": ncell, "levels": len(levels), "parallelism": f"replicas x{ws}",
                    "l2": "state resident in HBM; per-cycle working set above L2 at the default size",
@@ -593,6 +598,7 @@ def main():
     ap.add_argument("--prec-cfl", type=float, default=1.0)
     ap.add_argument("--large-cells", default="512,256,128")
     ap.add_argument("--large-fp64", action="store_true", help="FP64 implicit stage in the large case")
+    ap.add_argument("--ddadi", action="store_true", help="DDADI implicit stage (LUSGS=0) instead of LU-SGS")
     ap.add_argument("--ws-train", type=int, default=64)
     ap.add_argument("--ws-test", type=int, default=16)
     ap.add_argument("--ws-cycles", type=int, default=2000)

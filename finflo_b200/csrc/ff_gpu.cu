@@ -577,6 +577,7 @@ std::mutex g_tune_mu;
 int tune_sweep(Ctx* c, BlockCtx* b) {
   if (b->tuned) return 0;
   b->tuned = 1;
+  if (b->prm.ddadi) return 0;   // the DDADI line sweeps have one form
   const char* env = getenv("FINFLO_LUSGS");
   const TuneKey key{c->device, b->imax, b->jmax, b->kmax, b->prm.iturb >= 3 ? 7 : 5, b->prm.lusgs_fp32 != 0};
   if (!env) {
@@ -649,6 +650,35 @@ int sweep(Ctx* c, BlockCtx* b, int upper, bool fp32) {
   return b->use_lines ? lines_sweep(c, b, upper, fp32) : coop_sweep(c, b, upper, fp32);
 }
 
+// DDADI (LUSGS=0): the k, i and j lines in turn (imps3.f:320-356), each a
+// PRED+DIAG launch and a CORR launch with one thread per line.
+constexpr int DD_PD = 4, DD_TPB = 32;
+
+template <typename CT, int NV>
+void ddadi_launch(Ctx* c, BlockCtx* b, int dir, int lines) {
+  const size_t sm = ddadi_smem_bytes(NV, DD_PD, DD_TPB);
+  k_ddadi_pred<CT, NV, DD_PD, DD_TPB><<<nblk(lines, DD_TPB), DD_TPB, sm, c->stream>>>(b->db, b->prm, dir);
+  k_ddadi_corr<CT, NV, DD_PD, DD_TPB><<<nblk(lines, DD_TPB), DD_TPB, sm, c->stream>>>(b->db, b->prm, dir);
+  c->nlaunch += 2;
+}
+
+int ddadi_sweeps(Ctx* c, BlockCtx* b) {
+  const bool fp32 = b->prm.lusgs_fp32 != 0, ke = b->prm.iturb >= 3;
+  const int dirs[3] = {3, 1, 2};
+  for (int d : dirs) {
+    const int n = d == 1 ? b->imax : (d == 2 ? b->jmax : b->kmax);
+    if (n <= 1) continue;   // IMPSWE skips a direction one cell deep (imps3.f:601)
+    const int lines = b->imax * b->jmax * b->kmax / n;
+    if (fp32) {
+      if (ke) ddadi_launch<float, 7>(c, b, d, lines); else ddadi_launch<float, 5>(c, b, d, lines);
+    } else {
+      if (ke) ddadi_launch<double, 7>(c, b, d, lines); else ddadi_launch<double, 5>(c, b, d, lines);
+    }
+  }
+  CK(cudaGetLastError());
+  return 0;
+}
+
 int st_imps(Ctx* c, BlockCtx* b, int level, bool divide_cp) {
   int ncell = b->imax * b->jmax * b->kmax;
   double cfl = level == 1 ? b->prm.cfl : b->prm.cfll;
@@ -662,15 +692,19 @@ int st_imps(Ctx* c, BlockCtx* b, int level, bool divide_cp) {
   }
   bool fp32 = b->prm.lusgs_fp32 != 0;
   int rc;
-  sweep_coef(c, b, 1, fp32);
-  if ((rc = sweep(c, b, 1, fp32))) return rc;
-  sweep_coef(c, b, 0, fp32);
-  if ((rc = sweep(c, b, 0, fp32))) return rc;
-  if (fp32)
-    k_sweep_out<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->dwp32, b->prm.iturb >= 3 ? 7 : 5);
-  else
-    k_sweep_out<double><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->dwp, b->prm.iturb >= 3 ? 7 : 5);
-  c->nlaunch++;
+  if (b->prm.ddadi) {
+    if ((rc = ddadi_sweeps(c, b))) return rc;
+  } else {
+    sweep_coef(c, b, 1, fp32);
+    if ((rc = sweep(c, b, 1, fp32))) return rc;
+    sweep_coef(c, b, 0, fp32);
+    if ((rc = sweep(c, b, 0, fp32))) return rc;
+    if (fp32)
+      k_sweep_out<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->dwp32, b->prm.iturb >= 3 ? 7 : 5);
+    else
+      k_sweep_out<double><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->dwp, b->prm.iturb >= 3 ? 7 : 5);
+    c->nlaunch++;
+  }
   if (divide_cp) {
     // standalone IMPS: finish with DRO/CP (imps3.f:483); the fused cycle
     // folds this division into the FIN kernel instead
@@ -1183,6 +1217,7 @@ int ff_block_params(void* ctx, int blk, const ff_params* prm) {
   if (!b || !prm) return fail(c, FF_ERR_ARG, "ff_block_params");
   bool nv_changed = (b->prm.iturb >= 3) != (prm->iturb >= 3);
   bool fp_changed = (b->prm.lusgs_fp32 != 0) != (prm->lusgs_fp32 != 0);
+  if ((b->prm.ddadi != 0) != (prm->ddadi != 0)) b->tuned = 0;
   b->prm = *prm;
   if (nv_changed) {   // the line sweep's shared memory depends on the equation count
     int rc = setup_lines(c, b);
@@ -1562,7 +1597,7 @@ int ff_time_stage(void* ctx, int blk, int stage, int reps, float* ms) {
   Ctx* c = (Ctx*)ctx;
   BlockCtx* b = getb(c, blk);
   if (!b || !ms || reps < 1) return fail(c, FF_ERR_ARG, "ff_time_stage");
-  if (stage == FF_STAGE_SWEEP) {   // the sweep's kernel choice and its data in the sweep layout
+  if (stage == FF_STAGE_SWEEP && !b->prm.ddadi) {   // the sweep's kernel choice and its data in the sweep layout
     int rc = tune_sweep(c, b);
     if (rc) return rc;
     sweep_coef(c, b, 1, b->prm.lusgs_fp32 != 0);
@@ -1576,8 +1611,8 @@ int ff_time_stage(void* ctx, int blk, int stage, int reps, float* ms) {
       else
         k_residual<<<g, 128, 0, c->stream>>>(b->db, b->prm, 1);
       c->nlaunch++;
-    } else if (stage == FF_STAGE_SWEEP) {
-      int rc = sweep(c, b, 1, b->prm.lusgs_fp32 != 0);
+    } else if (stage == FF_STAGE_SWEEP) {   // LU-SGS: the lower sweep; DDADI: all three directions
+      int rc = b->prm.ddadi ? ddadi_sweeps(c, b) : sweep(c, b, 1, b->prm.lusgs_fp32 != 0);
       if (rc) return rc;
     } else if (stage == FF_STAGE_GRAD) {
       long ng = (long)(b->imax + 2) * (b->jmax + 2) * (b->kmax + 2);

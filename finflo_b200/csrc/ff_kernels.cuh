@@ -1449,3 +1449,4 @@ __global__ void __launch_bounds__(LTHREADS * (STAGE ? LMAX_TPC_STAGE : LMAX_TPC)
 }
 
 #include "ff_pipe.cuh"
+#include "ff_ddadi.cuh"
