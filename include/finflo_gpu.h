@@ -13,7 +13,9 @@
  *   ff_statim    STATIM  ns3c.f:10318  (PDTOP, STATE/PERFGA, CONSVA, REFLEC)
  *   ff_residu    RESIDI  ns3c.f:2355 -> RESIDU res3c.f:6 (level 1, laminar)
  *   ff_resl2     RESL2   res3c.f:8920
- *   ff_imps      IMPSDI  ns3c.f:2683 -> IMPS imps3.f:6 (LUSGS = 1)
+ *   ff_imps      IMPSDI  ns3c.f:2683 -> IMPS imps3.f:6 (LUSGS = 1: PREDGS,
+ *                DIAGGS, CORRGS; prm->ddadi = 1 selects LUSGS = 0: IMPSWE
+ *                imps3.f:578 per direction, PRED/DIAG/CORR imps4.f:671-971)
  *   ff_fin       FIN     res3c.f:1077 + the limits of CYCLES ns3c.f:1553-1596
  *   ff_boundi    BOUNDI  ns3c.f:10608 (REFCOR, MIR, STATIM; single block)
  *   ff_cycles    CYCLES  ns3c.f:1354 + BOUNDI + SUBIN per cycle, graph-replayed
@@ -92,7 +94,8 @@ int ff_cycles(void *ctx, int blk, int ncycles, int icycle0, double *hist, int us
  * FF_ERR_SIZE with nothing queued.  The first call on a device resolves the
  * array's device address; make that first call before any stream capture.
  * Calls share the array, so calls that overlap on the GPU race: serialise
- * them (one stream, or events).  Laminar (five-equation) blocks only:
+ * them (one stream, or events).  With prm->ddadi = 1 it runs the DDADI line
+ * sweeps instead, which use no scratch.  Laminar (five-equation) blocks only:
  * prm->iturb >= 3 gives FF_ERR_ARG.  Asynchronous on `stream` (a cudaStream_t). */
 #define FF_NOALLOC_MAX_NTOT 98304
 int ff_imps_noalloc(int imax, int jmax, int kmax, const ff_params *prm,

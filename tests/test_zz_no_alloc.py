@@ -34,8 +34,11 @@ def _slots(g, bid):
     return arr
 
 
-def test_imps_noalloc_matches_imps_twice(gpu_lib):
+@pytest.mark.parametrize("ddadi", [0, 1])
+def test_imps_noalloc_matches_imps_twice(gpu_lib, ddadi):
+    """LU-SGS, and the DDADI line sweeps (LUSGS=0), which need no scratch."""
     blk, prm, fs = case.bump_case(33, 17, 17)          # 32x16x16 cells, NTOT = 29,160
+    prm.ddadi = ddadi
     g = GpuSolver(0)
     bid = g.add_block(blk, prm)
     g.upload(bid)
