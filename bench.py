@@ -271,11 +271,23 @@ def run_ours(args):
     peak, pkind = _peaks()
     launches = g.cycle_launches(bid) * args.steps
     lk = g.lusgs_kind(bid)
-    chosen = ("DDADI k, i, j line sweeps, one thread per line" if args.ddadi
-              else f"cluster lines, {lk // 100} CTAs" if lk % 100 == 1
-              else f"pipelined tile wavefront, {lk // 100} tiles" if lk % 100 == 3
-              else f"cooperative hyperplane, {lk // 100} threads/CTA")
+    forms = ["32x4", "16x4", "16x8", "8x8"]
+    if args.ddadi and lk >= 100:
+        chosen = ("DDADI k, i, j line sweeps, lines x cells per CTA chunk: k " + forms[(lk // 10000) % 10]
+                  + ", i " + forms[(lk // 1000) % 10] + ", j " + forms[(lk // 100) % 10])
+    elif args.ddadi:
+        chosen = "DDADI k, i, j line sweeps, one thread per line"
+    elif lk % 100 == 1:
+        chosen = f"cluster lines, {lk // 100} CTAs"
+    elif lk % 100 == 3:
+        chosen = f"pipelined tile wavefront, {lk // 100} tiles"
+    else:
+        chosen = f"cooperative hyperplane, {lk // 100} threads/CTA"
     sweep = dict(g.sweep_tuning(bid), chosen=chosen, ms_per_sweep=ms_sweep)
+    if args.ddadi:   # the tuner's PRED+CORR time per direction
+        t = g.sweep_tuning(bid)
+        sweep = dict(chosen=chosen, ms_per_stage=ms_sweep, ms_k=t["pipe_ms"], ms_i=t["lines_ms"],
+                     ms_j=t["hyperplane_ms"])
     # ---- end to end through the C-ABI with host buffers ----------------
     names_in = wl["state"]
     host = {n: blk.arrays[n] for n in names_in}

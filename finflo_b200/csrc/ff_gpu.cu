@@ -31,6 +31,11 @@ struct BlockCtx {
   // (7 x ns), FP64 or FP32 as the block's lusgs_fp32 asks
   double* sw = nullptr;
   double* dwp = nullptr;
+  // DDADI kernel form per direction (index 1..3 = i, j, k): index into
+  // DD_CFG, or -1 for one thread per line; the tuner's time of the chosen
+  // form per direction
+  int dd_cfg[4] = {0, 0, 0, 0};
+  float dd_ms[4] = {0.f, 0.f, 0.f, 0.f};
   float* sw32 = nullptr;
   float* dwp32 = nullptr;
   size_t ns = 0;
@@ -558,28 +563,89 @@ void sweep_coef(Ctx* c, BlockCtx* b, int upper, bool fp32) {
 // fastest is kept.  FINFLO_LUSGS=pipe|lines|hyperplane restricts the choice.
 // Blocks that run side by side in a multi-block cycle use cluster sweeps
 // (see fork_join).
+// DDADI kernel shapes: the prefetch depth and CTA size of the one thread
+// per line kernels, and the (lines per CTA, cells per chunk) of the
+// producer/consumer kernels the autotuner chooses from.
+constexpr int DD_PD = 4, DD_TPB = 32;
+// (lines per CTA, cells per chunk) of the producer/consumer kernels the
+// autotuner chooses from
+constexpr int DD_NCFG = 4;
+constexpr int DD_CFG[DD_NCFG][2] = {{32, 4}, {16, 4}, {16, 8}, {8, 8}};
+
 // The autotuner's choice per device, block shape, equation count and
 // precision, kept for the life of the process: a later context with a block
 // of the same shape takes it without timing again.
 struct TuneKey {
-  int dev, imax, jmax, kmax, nv, fp32;
+  int dev, imax, jmax, kmax, nv, fp32, ddadi;
   bool operator<(const TuneKey& o) const {
-    return std::tie(dev, imax, jmax, kmax, nv, fp32) < std::tie(o.dev, o.imax, o.jmax, o.kmax, o.nv, o.fp32);
+    return std::tie(dev, imax, jmax, kmax, nv, fp32, ddadi) <
+           std::tie(o.dev, o.imax, o.jmax, o.kmax, o.nv, o.fp32, o.ddadi);
   }
 };
 struct TuneVal {
-  int use_pipe, use_lines, coop_threads;
+  int use_pipe, use_lines, coop_threads, dd_cfg;
   float pipe_ms, lines_ms, hyp_ms;
 };
 std::map<TuneKey, TuneVal> g_tune_cache;
 std::mutex g_tune_mu;
 
+int ddadi_sweeps(Ctx* c, BlockCtx* b, int only_dir = 0);
+
+// DDADI: time the producer/consumer forms (lines per CTA, cells per chunk)
+// per direction -- the i lines are fewer and longer than the j and k lines
+// -- and keep the fastest.  FINFLO_DDADI=simple selects the one thread per
+// line kernels, FINFLO_DDADI=<index> one form everywhere without timing.
+int tune_ddadi(Ctx* c, BlockCtx* b, const TuneKey& key) {
+  const char* env = getenv("FINFLO_DDADI");
+  if (env) {
+    const int k = !strcmp(env, "simple") ? -1 : max(0, min(DD_NCFG - 1, atoi(env)));
+    for (int d = 1; d <= 3; d++) b->dd_cfg[d] = k;
+    return 0;
+  }
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      const int packed = it->second.dd_cfg;
+      b->dd_cfg[1] = packed / 100; b->dd_cfg[2] = (packed / 10) % 10; b->dd_cfg[3] = packed % 10;
+      b->dd_ms[1] = it->second.pipe_ms; b->dd_ms[2] = it->second.lines_ms; b->dd_ms[3] = it->second.hyp_ms;
+      return 0;
+    }
+  }
+  for (int d = 1; d <= 3; d++) {
+    int best = 0;
+    float best_ms = 0.f;
+    for (int k = 0; k < DD_NCFG; k++) {
+      b->dd_cfg[d] = k;
+      float bt = 0.f;
+      for (int rep = 0; rep < 3; rep++) {   // rep 0 warms up
+        CK(cudaEventRecord(c->ev0, c->stream));
+        int rc = ddadi_sweeps(c, b, d);
+        if (rc) return rc;
+        CK(cudaEventRecord(c->ev1, c->stream));
+        CK(cudaEventSynchronize(c->ev1));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        if (rep > 0) bt = rep == 1 ? ms : fminf(bt, ms);
+      }
+      if (k == 0 || bt < best_ms) { best = k; best_ms = bt; }
+    }
+    b->dd_cfg[d] = best;
+    b->dd_ms[d] = best_ms;
+  }
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_cache[key] = TuneVal{0, 0, 0, b->dd_cfg[1] * 100 + b->dd_cfg[2] * 10 + b->dd_cfg[3],
+                              b->dd_ms[1], b->dd_ms[2], b->dd_ms[3]};
+  return 0;
+}
+
 int tune_sweep(Ctx* c, BlockCtx* b) {
   if (b->tuned) return 0;
   b->tuned = 1;
-  if (b->prm.ddadi) return 0;   // the DDADI line sweeps have one form
+  const TuneKey key{c->device, b->imax, b->jmax, b->kmax, b->prm.iturb >= 3 ? 7 : 5, b->prm.lusgs_fp32 != 0,
+                    b->prm.ddadi != 0};
+  if (b->prm.ddadi) return tune_ddadi(c, b, key);
   const char* env = getenv("FINFLO_LUSGS");
-  const TuneKey key{c->device, b->imax, b->jmax, b->kmax, b->prm.iturb >= 3 ? 7 : 5, b->prm.lusgs_fp32 != 0};
   if (!env) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_cache.find(key);
@@ -640,7 +706,7 @@ int tune_sweep(Ctx* c, BlockCtx* b) {
   if (pick == 0) b->use_lines = 0;
   if (!env) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tune_cache[key] = TuneVal{b->use_pipe, b->use_lines, b->coop_threads, b->pipe_ms, b->sweep_ms[0], b->sweep_ms[1]};
+    g_tune_cache[key] = TuneVal{b->use_pipe, b->use_lines, b->coop_threads, 0, b->pipe_ms, b->sweep_ms[0], b->sweep_ms[1]};
   }
   return 0;
 }
@@ -651,21 +717,48 @@ int sweep(Ctx* c, BlockCtx* b, int upper, bool fp32) {
 }
 
 // DDADI (LUSGS=0): the k, i and j lines in turn (imps3.f:320-356), each a
-// PRED+DIAG launch and a CORR launch with one thread per line.
-constexpr int DD_PD = 4, DD_TPB = 32;
+// PRED+DIAG launch and a CORR launch.  Default: 32 lines per CTA with
+// producer warps (k_ddadi_pc); FINFLO_DDADI=simple selects one thread per
+// line with a cp.async prefetch ring (k_ddadi_pred/k_ddadi_corr).
+
+template <typename CT, int NV, int LPC, int CH>
+void ddadi_pc_launch_t(cudaStream_t st, const DevBlock& db, const ff_params& prm, int dir, int lines) {
+  auto kp = k_ddadi_pc<CT, NV, LPC, CH, false>;
+  auto kc = k_ddadi_pc<CT, NV, LPC, CH, true>;
+  const size_t sp = ddadi_pc_smem_bytes<CT>(NV, LPC, CH, false), sc = ddadi_pc_smem_bytes<CT>(NV, LPC, CH, true);
+  cudaFuncSetAttribute(kp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp);
+  cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sc);
+  kp<<<nblk(lines, LPC), 32 + LPC * CH, sp, st>>>(db, prm, dir);
+  kc<<<nblk(lines, LPC), 32 + LPC * CH, sc, st>>>(db, prm, dir);
+}
+
+template <typename CT, int NV>
+void ddadi_pc_launch(cudaStream_t st, const DevBlock& db, const ff_params& prm, int dir, int lines, int cfg) {
+  switch (cfg) {
+    case 1: ddadi_pc_launch_t<CT, NV, 16, 4>(st, db, prm, dir, lines); break;
+    case 2: ddadi_pc_launch_t<CT, NV, 16, 8>(st, db, prm, dir, lines); break;
+    case 3: ddadi_pc_launch_t<CT, NV, 8, 8>(st, db, prm, dir, lines); break;
+    default: ddadi_pc_launch_t<CT, NV, 32, 4>(st, db, prm, dir, lines); break;
+  }
+}
 
 template <typename CT, int NV>
 void ddadi_launch(Ctx* c, BlockCtx* b, int dir, int lines) {
-  const size_t sm = ddadi_smem_bytes(NV, DD_PD, DD_TPB);
-  k_ddadi_pred<CT, NV, DD_PD, DD_TPB><<<nblk(lines, DD_TPB), DD_TPB, sm, c->stream>>>(b->db, b->prm, dir);
-  k_ddadi_corr<CT, NV, DD_PD, DD_TPB><<<nblk(lines, DD_TPB), DD_TPB, sm, c->stream>>>(b->db, b->prm, dir);
+  if (b->dd_cfg[dir] < 0) {   // FINFLO_DDADI=simple
+    const size_t sm = ddadi_smem_bytes(NV, DD_PD, DD_TPB);
+    k_ddadi_pred<CT, NV, DD_PD, DD_TPB><<<nblk(lines, DD_TPB), DD_TPB, sm, c->stream>>>(b->db, b->prm, dir);
+    k_ddadi_corr<CT, NV, DD_PD, DD_TPB><<<nblk(lines, DD_TPB), DD_TPB, sm, c->stream>>>(b->db, b->prm, dir);
+  } else {
+    ddadi_pc_launch<CT, NV>(c->stream, b->db, b->prm, dir, lines, b->dd_cfg[dir]);
+  }
   c->nlaunch += 2;
 }
 
-int ddadi_sweeps(Ctx* c, BlockCtx* b) {
+int ddadi_sweeps(Ctx* c, BlockCtx* b, int only_dir) {
   const bool fp32 = b->prm.lusgs_fp32 != 0, ke = b->prm.iturb >= 3;
   const int dirs[3] = {3, 1, 2};
   for (int d : dirs) {
+    if (only_dir && d != only_dir) continue;
     const int n = d == 1 ? b->imax : (d == 2 ? b->jmax : b->kmax);
     if (n <= 1) continue;   // IMPSWE skips a direction one cell deep (imps3.f:601)
     const int lines = b->imax * b->jmax * b->kmax / n;
@@ -1418,6 +1511,10 @@ int ff_sweep_times(void* ctx, int blk, float* ms3) {
   Ctx* c = (Ctx*)ctx;
   BlockCtx* b = getb(c, blk);
   if (!b || !ms3) return fail(c, FF_ERR_ARG, "ff_sweep_times");
+  if (b->prm.ddadi) {   // DDADI: the chosen form's time per direction {k, i, j}
+    ms3[0] = b->dd_ms[3]; ms3[1] = b->dd_ms[1]; ms3[2] = b->dd_ms[2];
+    return 0;
+  }
   ms3[0] = b->pipe_ms;
   ms3[1] = b->sweep_ms[0];
   ms3[2] = b->sweep_ms[1];
@@ -1427,6 +1524,8 @@ int ff_sweep_times(void* ctx, int blk, float* ms3) {
 int ff_lusgs_kind(void* ctx, int blk) {
   BlockCtx* b = getb((Ctx*)ctx, blk);
   if (!b) return -FF_ERR_ARG;
+  if (b->prm.ddadi)
+    return b->dd_cfg[1] < 0 ? 4 : 4 + 100 * (1000 + 100 * b->dd_cfg[3] + 10 * b->dd_cfg[1] + b->dd_cfg[2]);
   if (b->use_pipe) return 3 + 100 * b->pg.ntj * b->pg.ntk;
   return b->use_lines ? 1 + b->lg.cs * 100 : 2 + b->coop_threads * 100;
 }
@@ -1597,10 +1696,10 @@ int ff_time_stage(void* ctx, int blk, int stage, int reps, float* ms) {
   Ctx* c = (Ctx*)ctx;
   BlockCtx* b = getb(c, blk);
   if (!b || !ms || reps < 1) return fail(c, FF_ERR_ARG, "ff_time_stage");
-  if (stage == FF_STAGE_SWEEP && !b->prm.ddadi) {   // the sweep's kernel choice and its data in the sweep layout
+  if (stage == FF_STAGE_SWEEP) {   // the sweep's kernel choice and (LU-SGS) its data in the sweep layout
     int rc = tune_sweep(c, b);
     if (rc) return rc;
-    sweep_coef(c, b, 1, b->prm.lusgs_fp32 != 0);
+    if (!b->prm.ddadi) sweep_coef(c, b, 1, b->prm.lusgs_fp32 != 0);
   }
   CK(cudaEventRecord(c->ev0, c->stream));
   for (int r = 0; r < reps; r++) {

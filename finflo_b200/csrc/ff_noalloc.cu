@@ -103,18 +103,11 @@ extern "C" int ff_imps_noalloc(int imax, int jmax, int kmax, const ff_params* pr
   k_time3_copr<<<(ncell + 127) / 128, 128, 0, st>>>(db, p, cfl);
   if (p.ddadi) {   // DDADI (LUSGS=0): k, i, j line sweeps, no scratch
     const int dirs[3] = {3, 1, 2};
-    const size_t sm = ddadi_smem_bytes(5, DD_PD, DD_TPB);
     for (int d : dirs) {
       const int n = d == 1 ? imax : (d == 2 ? jmax : kmax);
       if (n <= 1) continue;
-      const int nbl = (ncell / n + DD_TPB - 1) / DD_TPB;
-      if (p.lusgs_fp32) {
-        k_ddadi_pred<float, 5, DD_PD, DD_TPB><<<nbl, DD_TPB, sm, st>>>(db, p, d);
-        k_ddadi_corr<float, 5, DD_PD, DD_TPB><<<nbl, DD_TPB, sm, st>>>(db, p, d);
-      } else {
-        k_ddadi_pred<double, 5, DD_PD, DD_TPB><<<nbl, DD_TPB, sm, st>>>(db, p, d);
-        k_ddadi_corr<double, 5, DD_PD, DD_TPB><<<nbl, DD_TPB, sm, st>>>(db, p, d);
-      }
+      if (p.lusgs_fp32) ddadi_pc_launch<float, 5>(st, db, p, d, ncell / n, 1);
+      else ddadi_pc_launch<double, 5>(st, db, p, d, ncell / n, 1);
     }
     k_fin_divide<<<(int)((ntot + 255) / 256), 256, 0, st>>>(db, 0);
     if (cudaGetLastError() != cudaSuccess) return FF_ERR_CUDA;

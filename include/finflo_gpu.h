@@ -160,7 +160,12 @@ int ff_cycle_launches(void *ctx, int blk);
 int ff_sweep_tuning(void *ctx, int blk, float *ms2);
 /* The autotuner's measured upper-sweep times in ms {pipelined tile
  * wavefront, cluster lines, fastest cooperative hyperplane} (zero where not
- * tried).  LU-SGS kind 3 + 100*tiles = the pipelined tile wavefront. */
+ * tried).  LU-SGS kind 3 + 100*tiles = the pipelined tile wavefront.
+ * DDADI blocks (prm->ddadi = 1): the tuned PRED+CORR time per direction
+ * {k, i, j}, and kind 4 + 100*(1000 + 100*fk + 10*fi + fj) with f the
+ * chosen producer/consumer form per direction (0: 32 lines x 4 cells per
+ * CTA chunk, 1: 16 x 4, 2: 16 x 8, 3: 8 x 8), or 4 alone for one thread per
+ * line. */
 int ff_sweep_times(void *ctx, int blk, float *ms3);
 int ff_lusgs_kind(void *ctx, int blk);
 int ff_time_cycles(void *ctx, int blk, int ncycles, float *ms);
