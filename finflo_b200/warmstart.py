@@ -336,12 +336,13 @@ def sample_params(n, seed, mach_range=(0.3, 0.8), amp_range=(0.05, 0.15)):
     return rng.uniform(*mach_range, size=n), rng.uniform(*amp_range, size=n)
 
 
-def make_case(mach, amp, seed=0, lusgs_fp32=False, **kw):
+def make_case(mach, amp, seed=0, lusgs_fp32=False, ddadi=False, **kw):
     from . import case
     c = dict(CASE, **kw)
     levels, prms, fs = case.bump_case_mg(*c["nodes"], nlev=1, mach=float(mach), amp=float(amp),
                                          reynolds=c["reynolds"], h1=c["h1"], noise=c["noise"], seed=seed,
                                          lusgs_fp32=lusgs_fp32)
+    prms[0].ddadi = int(ddadi)
     return levels[0], prms[0], fs
 
 
@@ -353,14 +354,15 @@ class Run:
     q: np.ndarray = field(default=None, repr=False)   # final conservative interior [cells, 5]
 
 
-def solve(mach, amp, cycles, init=None, tol=None, chunk=None, seed=0, keep_q=True, lusgs_fp32=False):
+def solve(mach, amp, cycles, init=None, tol=None, chunk=None, seed=0, keep_q=True, lusgs_fp32=False, ddadi=False):
     """Run the solver on one case for `cycles` cycles, or until the density
     residual's sum of squares is <= tol; init = solver state (TEMP, U, V,
     W, PDIFF) of the interior cells to start from instead of the free
-    stream; lusgs_fp32 runs the implicit stage in FP32.  Wall time covers
+    stream; lusgs_fp32 runs the implicit stage in FP32, ddadi selects the
+    DDADI implicit stage (LUSGS=0) instead of LU-SGS.  Wall time covers
     the cycles only (device synchronised)."""
     from .gpu import GpuSolver
-    blk, prm, fs = make_case(mach, amp, seed=seed, lusgs_fp32=lusgs_fp32)
+    blk, prm, fs = make_case(mach, amp, seed=seed, lusgs_fp32=lusgs_fp32, ddadi=ddadi)
     if init is not None:
         for n, v in init.items():
             blk.interior(n)[:] = v.reshape(blk.kmax, blk.jmax, blk.imax)
@@ -430,14 +432,16 @@ class Dataset:
         return state_from_conservative(q, fs, fc.gamma, fc.rgas)
 
 
-def evaluate(net, data, mach, amp, tol_decades=2.0, max_cycles=3000, lusgs_fp32=True):
+def evaluate(net, data, mach, amp, tol_decades=2.0, max_cycles=3000, lusgs_fp32=True, ddadi_arms=False):
     """For each case: cycles and wall time to a residual tolerance from the
     free stream with the plain FP64 solver, and from the network's
     prediction with the chosen implicit precision.  The tolerance is
     tol_decades below the free-stream start's first-cycle density residual
     (L2 norm), the same absolute level for both starts.  A prediction that
     does not reach it within max_cycles is reported as such: the plain
-    solver stays the fallback."""
+    solver stays the fallback.  ddadi_arms adds the same two runs with the
+    DDADI implicit stage (LUSGS=0): FP64 from the free stream and FP32 from
+    the prediction."""
     import torch
     out = []
     for m, a in zip(mach, amp):
@@ -449,15 +453,23 @@ def evaluate(net, data, mach, amp, tol_decades=2.0, max_cycles=3000, lusgs_fp32=
         st = data.to_state(pred, m, a)
         t_inf = time.perf_counter() - t0
         warm = solve(m, a, max_cycles, init=st, tol=tol, keep_q=False, lusgs_fp32=lusgs_fp32)
-        out.append(dict(mach=float(m), amp=float(a), tol=float(tol),
-                        base_cycles=base.cycles, base_s=base.seconds, base_reached=bool(base.hist.min() <= tol),
-                        warm_cycles=warm.cycles, warm_s=warm.seconds + t_inf, warm_reached=bool(warm.hist.min() <= tol),
-                        warm_start_decades=float(0.5 * np.log10(first.hist[0] / warm.hist[0]))))
+        e = dict(mach=float(m), amp=float(a), tol=float(tol),
+                 base_cycles=base.cycles, base_s=base.seconds, base_reached=bool(base.hist.min() <= tol),
+                 warm_cycles=warm.cycles, warm_s=warm.seconds + t_inf, warm_reached=bool(warm.hist.min() <= tol),
+                 warm_start_decades=float(0.5 * np.log10(first.hist[0] / warm.hist[0])))
+        if ddadi_arms:
+            dbase = solve(m, a, max_cycles, tol=tol, keep_q=False, ddadi=True)
+            dwarm = solve(m, a, max_cycles, init=st, tol=tol, keep_q=False, lusgs_fp32=True, ddadi=True)
+            e.update(ddadi_base_cycles=dbase.cycles, ddadi_base_s=dbase.seconds,
+                     ddadi_base_reached=bool(dbase.hist.min() <= tol),
+                     ddadi_warm_cycles=dwarm.cycles, ddadi_warm_s=dwarm.seconds + t_inf,
+                     ddadi_warm_reached=bool(dwarm.hist.min() <= tol))
+        out.append(e)
     return out
 
 
 def run_config(ntrain=64, ntest=16, cycles=2000, steps=6000, batch=16, lr=1e-3, tol_decades=2.0, seed_train=3,
-               seed_test=4, log=print):
+               seed_test=4, log=print, ddadi_arms=False):
     """The learned-warm-start workload: solve ntrain seeded (Mach, amplitude)
     points for `cycles` cycles as training data, train the network, then
     evaluate the ntest held-out points.  Returns a summary dict."""
@@ -476,9 +488,14 @@ def run_config(ntrain=64, ntest=16, cycles=2000, steps=6000, batch=16, lr=1e-3, 
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t1
     log(f"training: {steps} steps in {t_train:.1f} s, loss {hist}")
-    ev = evaluate(net, data, mte, ate, tol_decades=tol_decades, max_cycles=max(3000, cycles))
+    ev = evaluate(net, data, mte, ate, tol_decades=tol_decades, max_cycles=max(3000, cycles), ddadi_arms=ddadi_arms)
     base_s = sum(e["base_s"] for e in ev)
     warm_s = sum(e["warm_s"] for e in ev)
-    return dict(cases=ev, base_s=base_s, warm_s=warm_s, speedup=base_s / warm_s,
-                base_cycles=sum(e["base_cycles"] for e in ev), warm_cycles=sum(e["warm_cycles"] for e in ev),
-                loss=hist, t_data=t_data, t_train=t_train, steps=steps, ntrain=ntrain, ntest=ntest, cycles=cycles)
+    out = dict(cases=ev, base_s=base_s, warm_s=warm_s, speedup=base_s / warm_s,
+               base_cycles=sum(e["base_cycles"] for e in ev), warm_cycles=sum(e["warm_cycles"] for e in ev),
+               loss=hist, t_data=t_data, t_train=t_train, steps=steps, ntrain=ntrain, ntest=ntest, cycles=cycles)
+    if ddadi_arms:
+        for k in ("ddadi_base_s", "ddadi_warm_s", "ddadi_base_cycles", "ddadi_warm_cycles"):
+            out[k] = sum(e[k] for e in ev)
+        out["ddadi_reached"] = all(e["ddadi_base_reached"] and e["ddadi_warm_reached"] for e in ev)
+    return out
