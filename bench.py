@@ -359,6 +359,8 @@ def run_box(args):
     from finflo_b200.gpu import FF_STAGE_RESIDUAL
     nb = tuple(int(x) for x in args.blocks.split(","))
     blocks, prms, fs = case.periodic_box_case(nb=nb, lusgs_fp32=True)
+    for q in prms:
+        q.ddadi = int(args.ddadi)
     total = sum(b.interior_cells for b in blocks)
     backend = fd.GpuBackend(local)
     if ws > 1:
@@ -411,7 +413,7 @@ def run_box(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "strong" if ws > 1 else "weak", "vs_baseline": None,
         "dtype": "f64 residual / f32 LU-SGS", "data": "synthetic (seeded block split and entropy-wave phase)",
-        "config": {"workload": BOX_NAME, "blocks": len(blocks), "cells": total,
+        "config": {"workload": BOX_NAME + (", DDADI implicit stage (LUSGS=0)" if args.ddadi else ""), "blocks": len(blocks), "cells": total,
                    "parallelism": f"blocks over {ws} GPU(s)", "l2": "inputs larger than L2"},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "kernel": "k_residual (all blocks)", "achieved": achieved, "peak": peak,
@@ -464,6 +466,8 @@ def run_large(args):
                 q.ibtype = q.ibtype * nlev
             pats.append(q)
         fine.patches = pats
+        for q in prms:
+            q.ddadi = int(args.ddadi)
         bid = g.add_levels(levels, prms)
         assert bid == n * nlev
         for q in range(nlev):
@@ -489,7 +493,8 @@ def run_large(args):
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64 residual / " + ("f32" if fp32 else "f64") + " LU-SGS",
         "data": "synthetic (seeded block cuts and free-stream noise)",
-        "config": {"workload": LARGE_NAME.format(cells="x".join(map(str, cells)), prec="FP32" if fp32 else "FP64"),
+        "config": {"workload": LARGE_NAME.format(cells="x".join(map(str, cells)), prec="FP32" if fp32 else "FP64")
+                   + (", DDADI implicit stage (LUSGS=0)" if args.ddadi else ""),
                    "cells": total, "blocks": len(fine_cells), "levels": nlev, "setup_s": setup_s,
                    "parallelism": "blocks on 1 GPU", "l2": "inputs larger than L2"},
         "gpu_launches": per_cycle * args.steps,

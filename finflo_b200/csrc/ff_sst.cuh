@@ -455,14 +455,19 @@ FF_DI void face_flux_ke(const DevBlock& b, const ff_params& p, int dir, size_t L
 }
 
 // RESIKE face cycles + SWEEPK for a 32x4x4 tile (k, i, j, then 1/VOL).
-__global__ void __launch_bounds__(128, RES_MIN_CTAS) k_residual_sst(DevBlock b, ff_params p, int level) {
+// NT threads per CTA (128, 256 or 512): each thread sums the faces of
+// CPT = 512 / NT cells of the 32x4x4 tile (a k column of CPT cells); the
+// register budget gives RES_MIN_CTAS * 128 threads per SM at every NT.
+template <int NT>
+__global__ void __launch_bounds__(NT, RES_MIN_CTAS * 128 / NT) k_residual_sst(DevBlock b, ff_params p, int level) {
+  constexpr int CPT = TI * TJ * TK / NT;
   __shared__ double sF[7][TI * (TJ + 1) * TK];   // one direction's faces (at most 640) x 7
   const int tid = threadIdx.x;
   const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ, k0 = blockIdx.z * TK;
-  const int ci = tid % TI, cj = tid / TI;
-  double acc[TK][7];
+  const int ci = tid % TI, cj = (tid / TI) % TJ, ck0 = (tid / (TI * TJ)) * CPT;
+  double acc[CPT][7];
 #pragma unroll
-  for (int c = 0; c < TK; c++)
+  for (int c = 0; c < CPT; c++)
 #pragma unroll
     for (int v = 0; v < 7; v++) acc[c][v] = 0.;
   // the directions in SWEEP order (k, i, j; RESIKE res3c.f:3423); one call site of the
@@ -485,9 +490,9 @@ __global__ void __launch_bounds__(128, RES_MIN_CTAS) k_residual_sst(DevBlock b, 
     __syncthreads();
     const int fs = dir == 1 ? 1 : (dir == 2 ? ni : ni * nj);   // low face -> high face of a cell
 #pragma unroll
-    for (int c = 0; c < TK; c++) {
-      const int f0 = ci + ni * (cj + nj * c);
-      const int I = i0 + ci + 1, J = j0 + cj + 1, K = k0 + c + 1;
+    for (int c = 0; c < CPT; c++) {
+      const int f0 = ci + ni * (cj + nj * (ck0 + c));
+      const int I = i0 + ci + 1, J = j0 + cj + 1, K = k0 + ck0 + c + 1;
       if (I > b.imax || J > b.jmax || K > b.kmax) continue;
       if (pass < 2) {
 #pragma unroll
