@@ -180,21 +180,26 @@ int res_threads(bool sst) {
   return env ? env : (sst ? 256 : 512);
 }
 
+template <int NT>
+void launch_residual_t(cudaStream_t st, dim3 g, const BlockCtx* b, int level, bool sst) {
+  // face buffer + running sums of the 32x4x4 tile, NV values each
+  const size_t sm = (size_t)(sst ? 7 : 5) * (TI * (TJ + 1) * TK + TI * TJ * TK) * sizeof(double);
+  if (sst) {
+    cudaFuncSetAttribute(k_residual_sst<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_residual_sst<NT><<<g, NT, sm, st>>>(b->db, b->prm, level);
+  } else {
+    cudaFuncSetAttribute(k_residual<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_residual<NT><<<g, NT, sm, st>>>(b->db, b->prm, level);
+  }
+}
+
 void launch_residual(cudaStream_t st, const BlockCtx* b, int level) {
   dim3 g(nblk(b->imax, TI), nblk(b->jmax, TJ), nblk(b->kmax, TK));
   const bool sst = b->prm.iturb >= 3;
   switch (res_threads(sst)) {
-    case 128:
-      if (sst) k_residual_sst<128><<<g, 128, 0, st>>>(b->db, b->prm, level);
-      else k_residual<128><<<g, 128, 0, st>>>(b->db, b->prm, level);
-      break;
-    case 512:
-      if (sst) k_residual_sst<512><<<g, 512, 0, st>>>(b->db, b->prm, level);
-      else k_residual<512><<<g, 512, 0, st>>>(b->db, b->prm, level);
-      break;
-    default:
-      if (sst) k_residual_sst<256><<<g, 256, 0, st>>>(b->db, b->prm, level);
-      else k_residual<256><<<g, 256, 0, st>>>(b->db, b->prm, level);
+    case 128: launch_residual_t<128>(st, g, b, level, sst); break;
+    case 512: launch_residual_t<512>(st, g, b, level, sst); break;
+    default: launch_residual_t<256>(st, g, b, level, sst);
   }
 }
 

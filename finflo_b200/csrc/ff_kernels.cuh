@@ -511,15 +511,19 @@ FF_DI void face_flux(const DevBlock& b, const ff_params& p, int dir, size_t L, i
 template <int NT>
 __global__ void __launch_bounds__(NT, RES_MIN_CTAS * 128 / NT) k_residual(DevBlock b, ff_params p, int level) {
   constexpr int CPT = TI * TJ * TK / NT;
-  __shared__ double sF[5][TI * (TJ + 1) * TK];   // one direction's faces (at most 640) x 5
+  constexpr int NF = TI * (TJ + 1) * TK, NC = TI * TJ * TK;
+  // one direction's faces (at most 640) x 5, then the cells' running sums
+  // (in shared memory, not registers: the face flux needs the registers)
+  extern __shared__ double res_smem[];
+  double(*sF)[NF] = reinterpret_cast<double(*)[NF]>(res_smem);
+  double(*sAcc)[NC] = reinterpret_cast<double(*)[NC]>(res_smem + 5 * NF);
   const int tid = threadIdx.x;
   const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ, k0 = blockIdx.z * TK;
   const int ci = tid % TI, cj = (tid / TI) % TJ, ck0 = (tid / (TI * TJ)) * CPT;
-  double acc[CPT][5];
 #pragma unroll
   for (int c = 0; c < CPT; c++)
 #pragma unroll
-    for (int v = 0; v < 5; v++) acc[c][v] = 0.;
+    for (int v = 0; v < 5; v++) sAcc[v][ci + TI * (cj + TJ * (ck0 + c))] = 0.;
   // the directions in SWEEP order (k, i, j; res3c.f:355); one call site of the
   // face flux keeps a single copy of its code in the instruction stream
 #pragma unroll 1
@@ -544,14 +548,15 @@ __global__ void __launch_bounds__(NT, RES_MIN_CTAS * 128 / NT) k_residual(DevBlo
       const int f0 = ci + ni * (cj + nj * (ck0 + c));
       const int I = i0 + ci + 1, J = j0 + cj + 1, K = k0 + ck0 + c + 1;
       if (I > b.imax || J > b.jmax || K > b.kmax) continue;
+      const int ca = ci + TI * (cj + TJ * (ck0 + c));
       if (pass < 2) {
 #pragma unroll
-        for (int v = 0; v < 5; v++) acc[c][v] = acc[c][v] - (sF[v][f0 + fs] - sF[v][f0]);
+        for (int v = 0; v < 5; v++) sAcc[v][ca] = sAcc[v][ca] - (sF[v][f0 + fs] - sF[v][f0]);
       } else {   // last direction, then 1/VOL (SWEEP IDO = 1)
         const size_t n = ix(b, I, J, K);
         const double rv = 1. / __ldg(b.a[FF_VOL] + n);
 #pragma unroll
-        for (int v = 0; v < 5; v++) b.a[FF_DRO + v][n] = (acc[c][v] - (sF[v][f0 + fs] - sF[v][f0])) * rv;
+        for (int v = 0; v < 5; v++) b.a[FF_DRO + v][n] = (sAcc[v][ca] - (sF[v][f0 + fs] - sF[v][f0])) * rv;
       }
     }
     __syncthreads();

@@ -423,35 +423,42 @@ FF_DI void face_flux_ke(const DevBlock& b, const ff_params& p, int dir, size_t L
     }
   }
   const int idi = dir == 1 ? p.idi1 : (dir == 2 ? p.idi2 : p.idi3);
+  // The inviscid flux first, into f from zero; the viscous flux after it,
+  // when the MUSCL stencil is no longer live.  The reference adds the
+  // inviscid flux to the viscous one (F = Fv + Fi per component), and one
+  // addition is the same either way round.
 #pragma unroll
   for (int v = 0; v < 7; v++) f[v] = 0.;
+  {
+    double q[7][4];
+    const int sl[7] = {FF_RO, FF_U, FF_V, FF_W, FF_P, FF_RK, FF_REPS};
+#pragma unroll
+    for (int v = 0; v < 7; v++) {
+      const double* a = b.a[sl[v]];
+      q[v][0] = __ldg(a + L - 2 * S); q[v][1] = __ldg(a + L - S); q[v][2] = __ldg(a + L); q[v][3] = __ldg(a + L + S);
+    }
+    size_t L2 = dir == 3 ? L : L - S;
+    double cr[4] = {__ldg(b.a[FF_DRDP] + L), __ldg(b.a[FF_DRDH] + L), q[0][2], q[4][2]};
+    double cl[4] = {__ldg(b.a[FF_DRDP] + L2), __ldg(b.a[FF_DRDH] + L2), __ldg(b.a[FF_RO] + L2), __ldg(b.a[FF_P] + L2)};
+    const int ao = 4 * (dir - 1);
+    roe_flux_ke(q, __ldg(b.a[FF_A1XA + ao] + L), __ldg(b.a[FF_A1YA + ao] + L), __ldg(b.a[FF_A1ZA + ao] + L),
+                __ldg(b.a[FF_A1 + ao] + L), intem, intet, p, __ldg(b.a[FF_C] + L), __ldg(b.a[FF_C] + L - S), cr, cl,
+                f);
+  }
   if (m <= min(idi, nmax + 1)) {
-    double frk, feps, fv[5];
+    double frk, feps, fv[5], f4;
     if (level == 1 && p.fullns) {   // FLKEBL, SETV12, FLUXBL
       flkebl_face(b, L, S, dir, frk, feps);
       visc_flux(b, p, L, S, dir, fv);
-      f[4] = frk + fv[4];
+      f4 = frk + fv[4];
     } else {                        // FLUDKE, FLUXDO
       fludke_face(b, L, S, dir, frk, feps);
       visc_flux_thin(b, p, L, S, dir, fv, frk);
-      f[4] = fv[4];
+      f4 = fv[4];
     }
-    f[1] = fv[1]; f[2] = fv[2]; f[3] = fv[3];
-    f[5] = frk; f[6] = feps;
+    f[1] = fv[1] + f[1]; f[2] = fv[2] + f[2]; f[3] = fv[3] + f[3];
+    f[4] = f4 + f[4]; f[5] = frk + f[5]; f[6] = feps + f[6];
   }
-  double q[7][4];
-  const int sl[7] = {FF_RO, FF_U, FF_V, FF_W, FF_P, FF_RK, FF_REPS};
-#pragma unroll
-  for (int v = 0; v < 7; v++) {
-    const double* a = b.a[sl[v]];
-    q[v][0] = __ldg(a + L - 2 * S); q[v][1] = __ldg(a + L - S); q[v][2] = __ldg(a + L); q[v][3] = __ldg(a + L + S);
-  }
-  size_t L2 = dir == 3 ? L : L - S;
-  double cr[4] = {__ldg(b.a[FF_DRDP] + L), __ldg(b.a[FF_DRDH] + L), q[0][2], q[4][2]};
-  double cl[4] = {__ldg(b.a[FF_DRDP] + L2), __ldg(b.a[FF_DRDH] + L2), __ldg(b.a[FF_RO] + L2), __ldg(b.a[FF_P] + L2)};
-  const int ao = 4 * (dir - 1);
-  roe_flux_ke(q, __ldg(b.a[FF_A1XA + ao] + L), __ldg(b.a[FF_A1YA + ao] + L), __ldg(b.a[FF_A1ZA + ao] + L),
-              __ldg(b.a[FF_A1 + ao] + L), intem, intet, p, __ldg(b.a[FF_C] + L), __ldg(b.a[FF_C] + L - S), cr, cl, f);
 }
 
 // RESIKE face cycles + SWEEPK for a 32x4x4 tile (k, i, j, then 1/VOL).
@@ -461,15 +468,19 @@ FF_DI void face_flux_ke(const DevBlock& b, const ff_params& p, int dir, size_t L
 template <int NT>
 __global__ void __launch_bounds__(NT, RES_MIN_CTAS * 128 / NT) k_residual_sst(DevBlock b, ff_params p, int level) {
   constexpr int CPT = TI * TJ * TK / NT;
-  __shared__ double sF[7][TI * (TJ + 1) * TK];   // one direction's faces (at most 640) x 7
+  constexpr int NF = TI * (TJ + 1) * TK, NC = TI * TJ * TK;
+  // one direction's faces (at most 640) x 7, then the cells' running sums
+  // (in shared memory, not registers: the face flux needs the registers)
+  extern __shared__ double res_smem[];
+  double(*sF)[NF] = reinterpret_cast<double(*)[NF]>(res_smem);
+  double(*sAcc)[NC] = reinterpret_cast<double(*)[NC]>(res_smem + 7 * NF);
   const int tid = threadIdx.x;
   const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ, k0 = blockIdx.z * TK;
   const int ci = tid % TI, cj = (tid / TI) % TJ, ck0 = (tid / (TI * TJ)) * CPT;
-  double acc[CPT][7];
 #pragma unroll
   for (int c = 0; c < CPT; c++)
 #pragma unroll
-    for (int v = 0; v < 7; v++) acc[c][v] = 0.;
+    for (int v = 0; v < 7; v++) sAcc[v][ci + TI * (cj + TJ * (ck0 + c))] = 0.;
   // the directions in SWEEP order (k, i, j; RESIKE res3c.f:3423); one call site of the
   // face flux keeps a single copy of its code in the instruction stream
 #pragma unroll 1
@@ -494,14 +505,15 @@ __global__ void __launch_bounds__(NT, RES_MIN_CTAS * 128 / NT) k_residual_sst(De
       const int f0 = ci + ni * (cj + nj * (ck0 + c));
       const int I = i0 + ci + 1, J = j0 + cj + 1, K = k0 + ck0 + c + 1;
       if (I > b.imax || J > b.jmax || K > b.kmax) continue;
+      const int ca = ci + TI * (cj + TJ * (ck0 + c));
       if (pass < 2) {
 #pragma unroll
-        for (int v = 0; v < 7; v++) acc[c][v] = acc[c][v] - (sF[v][f0 + fs] - sF[v][f0]);
+        for (int v = 0; v < 7; v++) sAcc[v][ca] = sAcc[v][ca] - (sF[v][f0 + fs] - sF[v][f0]);
       } else {   // last direction, then 1/VOL (SWEEP IDO = 1)
         const size_t n = ix(b, I, J, K);
         const double rv = 1. / __ldg(b.a[FF_VOL] + n);
 #pragma unroll
-        for (int v = 0; v < 7; v++) b.a[FF_DRO + v][n] = (acc[c][v] - (sF[v][f0 + fs] - sF[v][f0])) * rv;
+        for (int v = 0; v < 7; v++) b.a[FF_DRO + v][n] = (sAcc[v][ca] - (sF[v][f0 + fs] - sF[v][f0])) * rv;
       }
     }
     __syncthreads();
