@@ -49,8 +49,8 @@ WORKLOADS = {
 
 # DRAM bytes (read + write) of one launch of the dominant kernel, from one
 # ncu capture of the same workload (profiles/k_residual_sst_sstmg128x64x64_full.md:
-# 578.0 MB read + 97.5 MB written, spill traffic included).
-TRAFFIC = {"sst-mg": 675.4e6}
+# 264.9 MB read + 22.9 MB written).
+TRAFFIC = {"sst-mg": 287.9e6}
 
 
 def build_case(wl, nodes=None):
