@@ -167,17 +167,19 @@ int st_boundi(Ctx* c, BlockCtx* b) {
 // RESIKE res3c.f:3423 (k-omega SST) on a level; for m2 >= 2 RESIKE
 // recomputes the velocity gradients of the level itself.
 // Threads per CTA of the residual kernels: the same 32x4x4 tile and
-// arithmetic, with fewer cells per thread as the threads grow, so fewer
-// accumulator registers per thread.  Measured on B200 (128 / 256 / 512
-// threads): SST 0.571 / 0.498 / 0.504 ms on 128x64x64 cells, laminar
-// 0.132 / 0.079 / 0.056 ms on 64x32x32.  FINFLO_RES_THREADS overrides.
+// arithmetic.  Measured on B200 with one face work list per tile (128 /
+// 256 / 512 threads): SST 0.798 / 0.514 / 0.403 ms on 128x64x64 cells,
+// laminar 0.136 / 0.073 / 0.047 ms on 64x32x32; with one barrier per
+// direction (FINFLO_RES_FUSED=0) SST 0.571 / 0.457 / 0.500 ms.
+// FINFLO_RES_THREADS overrides.
 int res_threads(bool sst) {
   static const int env = [] {
     const char* e = getenv("FINFLO_RES_THREADS");
     const int v = e ? atoi(e) : 0;
     return (v == 128 || v == 256 || v == 512) ? v : 0;
   }();
-  return env ? env : (sst ? 256 : 512);
+  (void)sst;
+  return env ? env : 512;
 }
 
 template <int NT>
@@ -193,9 +195,30 @@ void launch_residual_t(cudaStream_t st, dim3 g, const BlockCtx* b, int level, bo
   }
 }
 
+// One face work list per tile (k_residual_fused) unless FINFLO_RES_FUSED=0.
+bool res_fused() {
+  static const bool f = [] { const char* e = getenv("FINFLO_RES_FUSED"); return !(e && !strcmp(e, "0")); }();
+  return f;
+}
+
+template <int NV, int NT>
+void launch_residual_fused_t(cudaStream_t st, dim3 g, const BlockCtx* b, int level) {
+  const size_t sm = residual_fused_smem(NV);
+  cudaFuncSetAttribute(k_residual_fused<NV, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k_residual_fused<NV, NT><<<g, NT, sm, st>>>(b->db, b->prm, level);
+}
+
 void launch_residual(cudaStream_t st, const BlockCtx* b, int level) {
   dim3 g(nblk(b->imax, TI), nblk(b->jmax, TJ), nblk(b->kmax, TK));
   const bool sst = b->prm.iturb >= 3;
+  if (res_fused()) {
+    switch (res_threads(sst)) {
+      case 128: sst ? launch_residual_fused_t<7, 128>(st, g, b, level) : launch_residual_fused_t<5, 128>(st, g, b, level); break;
+      case 512: sst ? launch_residual_fused_t<7, 512>(st, g, b, level) : launch_residual_fused_t<5, 512>(st, g, b, level); break;
+      default: sst ? launch_residual_fused_t<7, 256>(st, g, b, level) : launch_residual_fused_t<5, 256>(st, g, b, level);
+    }
+    return;
+  }
   switch (res_threads(sst)) {
     case 128: launch_residual_t<128>(st, g, b, level, sst); break;
     case 512: launch_residual_t<512>(st, g, b, level, sst); break;

@@ -520,6 +520,60 @@ __global__ void __launch_bounds__(NT, RES_MIN_CTAS * 128 / NT) k_residual_sst(De
   }
 }
 
+// RESIDU/RESIKE for a 32x4x4 tile with all three directions' faces in one
+// work list: the k, i and j faces (640 + 528 + 640) are computed by NT
+// threads into one shared-memory face buffer with a single barrier, then
+// each cell sums its six faces in the reference order (k, i, j, then
+// 1/VOL, SWEEP res3c.f:992 / SWEEPK res3c.f:1342).  Against one barrier per
+// direction this balances the face work over the threads (8 rounds for the
+// 1808 faces at 256 threads, against 3 + 3 + 3) and drops two barriers.
+template <int NV, int NT>
+__global__ void __launch_bounds__(NT, RES_MIN_CTAS * 128 / NT) k_residual_fused(DevBlock b, ff_params p, int level) {
+  constexpr int NFK = TI * TJ * (TK + 1), NFI = (TI + 1) * TJ * TK, NFJ = TI * (TJ + 1) * TK;
+  constexpr int NFT = NFK + NFI + NFJ, NC = TI * TJ * TK;
+  extern __shared__ double res_smem[];
+  double(*sF)[NFT] = reinterpret_cast<double(*)[NFT]>(res_smem);
+  const int tid = threadIdx.x;
+  const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ, k0 = blockIdx.z * TK;
+  for (int f = tid; f < NFT; f += NT) {
+    int dir, l, ni, nj;
+    if (f < NFK) { dir = 3; l = f; ni = TI; nj = TJ; }
+    else if (f < NFK + NFI) { dir = 1; l = f - NFK; ni = TI + 1; nj = TJ; }
+    else { dir = 2; l = f - NFK - NFI; ni = TI; nj = TJ + 1; }
+    const int fi = l % ni, fj = (l / ni) % nj, fk = l / (ni * nj);
+    const int I = i0 + fi + 1, J = j0 + fj + 1, K = k0 + fk + 1;
+    if (I > b.imax + (dir == 1) || J > b.jmax + (dir == 2) || K > b.kmax + (dir == 3)) continue;
+    const int m = dir == 1 ? I : (dir == 2 ? J : K);
+    const int t1 = dir == 1 ? J : I, t2 = dir == 3 ? J : K;
+    double fl[NV];
+    if constexpr (NV == 7) face_flux_ke(b, p, dir, ix(b, I, J, K), m, t1, t2, level, fl);
+    else face_flux(b, p, dir, ix(b, I, J, K), m, t1, t2, level, fl);
+#pragma unroll
+    for (int v = 0; v < NV; v++) sF[v][f] = fl[v];
+  }
+  __syncthreads();
+  for (int c = tid; c < NC; c += NT) {
+    const int ci = c % TI, cj = (c / TI) % TJ, ck = c / (TI * TJ);
+    const int I = i0 + ci + 1, J = j0 + cj + 1, K = k0 + ck + 1;
+    if (I > b.imax || J > b.jmax || K > b.kmax) continue;
+    const int fk0 = ci + TI * (cj + TJ * ck);                       // face K-1/2; K+1/2 at + TI*TJ
+    const int fi0 = NFK + ci + (TI + 1) * (cj + TJ * ck);          // face I-1/2; I+1/2 at + 1
+    const int fj0 = NFK + NFI + ci + TI * (cj + (TJ + 1) * ck);    // face J-1/2; J+1/2 at + TI
+    const size_t n = ix(b, I, J, K);
+    const double rv = 1. / __ldg(b.a[FF_VOL] + n);
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+      double acc = 0. - (sF[v][fk0 + TI * TJ] - sF[v][fk0]);
+      acc = acc - (sF[v][fi0 + 1] - sF[v][fi0]);
+      b.a[FF_DRO + v][n] = (acc - (sF[v][fj0 + TI] - sF[v][fj0])) * rv;
+    }
+  }
+}
+
+inline size_t residual_fused_smem(int nv) {
+  return (size_t)nv * (TI * TJ * (TK + 1) + (TI + 1) * TJ * TK + TI * (TJ + 1) * TK) * sizeof(double);
+}
+
 // SOURKO (KOVER=0, RANS, no rotation correction) + ADDSKE, interior cells.
 __global__ void k_sourko_addske(DevBlock b) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
