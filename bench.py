@@ -49,8 +49,8 @@ WORKLOADS = {
 
 # DRAM bytes (read + write) of one launch of the dominant kernel, from one
 # ncu capture of the same workload (profiles/k_residual_sst_sstmg128x64x64_full.md:
-# 264.9 MB read + 22.9 MB written).
-TRAFFIC = {"sst-mg": 287.9e6}
+# 244.2 MB read + 24.3 MB written).
+TRAFFIC = {"sst-mg": 268.5e6}
 
 
 def build_case(wl, nodes=None):
@@ -317,7 +317,7 @@ def run_ours(args):
                    "l2": "state resident in HBM; per-cycle working set above L2 at the default size",
                    "lusgs_sweep": sweep},
         "gpu_launches": launches,
-        "roofline": {"bound": "hbm", "kernel": "k_residual_sst" if prms[0].iturb >= 3 else "k_residual",
+        "roofline": {"bound": "hbm", "kernel": "k_residual_fused<7,512>" if prms[0].iturb >= 3 else "k_residual_fused<5,512>",
                      "achieved": achieved, "peak": peak, "peak_kind": pkind, "unit": "GB/s",
                      "frac": achieved / peak,
                      "traffic": TRAFFIC.get(args.workload) if not args.grid else None,
