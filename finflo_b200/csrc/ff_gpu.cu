@@ -604,11 +604,10 @@ int setup_pipe(Ctx* c, BlockCtx* b) {
 // Sweep data of one sweep in the sweep layout (and, for upper = 1, the
 // right-hand side copied into it).
 void sweep_coef(Ctx* c, BlockCtx* b, int upper, bool fp32) {
-  int ncell = b->imax * b->jmax * b->kmax;
   if (fp32)
-    k_sweep_coef<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, b->sw32, b->dwp32, upper);
+    k_sweep_coef<float><<<nblk((long)b->ns, 128), 128, 0, c->stream>>>(b->db, b->prm, b->sw32, b->dwp32, upper);
   else
-    k_sweep_coef<double><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, b->sw, b->dwp, upper);
+    k_sweep_coef<double><<<nblk((long)b->ns, 128), 128, 0, c->stream>>>(b->db, b->prm, b->sw, b->dwp, upper);
   c->nlaunch++;
 }
 

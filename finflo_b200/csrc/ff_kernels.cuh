@@ -725,9 +725,15 @@ __global__ void k_lusgs_coef(DevBlock b, ff_params p, CT* coef, int upper) {
 // dwp in the same layout and type.
 template <typename CT>
 __global__ void k_sweep_coef(DevBlock b, ff_params p, CT* sw, CT* dwp, int upper) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= b.imax * b.jmax * b.kmax) return;
-  int I = t % b.imax + 1, J = (t / b.imax) % b.jmax + 1, K = t / (b.imax * b.jmax) + 1;
+  // one thread per slot of the sweep layout, in slot order, so that the
+  // ~50 stores of a warp are contiguous; slots outside the block (I < 1 or
+  // I > IMAX on a diagonal) have no cell
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t row = (size_t)(b.imax + b.jmax - 1) * b.jmax;
+  if (t >= row * b.kmax) return;
+  const int K = (int)(t / row) + 1;
+  const int r = (int)(t % row), J = r % b.jmax + 1, I = r / b.jmax + 2 - J;
+  if (I < 1 || I > b.imax) return;
   CellCoef cc;
   lusgs_cell_coef(b, p, I, J, K, upper, cc);
   const size_t ns = sw_size(b.imax, b.jmax, b.kmax), S = sw_index(b, I, J, K);
