@@ -41,7 +41,8 @@ class FFParams(ctypes.Structure):
         "rklim", "epslim", "turlim", "csimps", "re")] + [
         (n, ctypes.c_int) for n in (
             "interi", "interj", "interk", "entropy_fix", "iturb", "fullns",
-            "idi1", "idi2", "idi3", "coarse_inter", "lusgs_fp32", "ddadi")]
+            "idi1", "idi2", "idi3", "coarse_inter", "lusgs_fp32", "ddadi", "timel", "pad1")] + [
+        ("dt", ctypes.c_double)]
 
 
 class FFHaloItem(ctypes.Structure):
@@ -63,7 +64,9 @@ SLOTS = ["RO", "RM", "RN", "RW", "E", "P", "PDIFF", "U", "V", "W", "C",
          "ROP2H", "RMP2H", "RNP2H", "RWP2H", "EP2H",
          "RK", "REPS", "DISTW", "FUN1", "SRK", "SEPS", "PTUR",
          "DKDX", "DKDY", "DKDZ", "DEDX", "DEDY", "DEDZ",
-         "RKOLD", "EPSOLD", "F1RK", "F1EPS", "RKP2H", "EPP2H"]
+         "RKOLD", "EPSOLD", "F1RK", "F1EPS", "RKP2H", "EPP2H",
+         "ROLE2", "RMLE2", "RNLE2", "RWLE2", "ELE2", "RKLE2", "EPSLE2",
+         "ROLE3", "RMLE3", "RNLE3", "RWLE3", "ELE3", "RKLE3", "EPSLE3"]
 SLOT = {n: i for i, n in enumerate(SLOTS)}
 STATE_SLOTS = SLOTS[:19]
 METRIC_SLOTS = list(grid.METRIC_NAMES)

@@ -261,6 +261,10 @@ int st_residu_sst(Ctx* c, BlockCtx* b, int level, int m2, int icycle) {
   launch_residual(c->stream, b, level);
   k_sourko_addske<<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db);
   c->nlaunch += 2;
+  if (b->prm.timel && level == 1) {   // TIMDER + TIMDKE after ADDSKE (res3c.f:5097)
+    k_timder<7><<<nblk(ncell, 256), 256, 0, c->stream>>>(b->db, b->prm);
+    c->nlaunch++;
+  }
   return 0;
 }
 
@@ -282,6 +286,10 @@ int st_residu(Ctx* c, BlockCtx* b, int level, int icycle, int m2 = 1) {
   if (level == 1) launch_patch(c, b, k_inlet_outlet, icycle);
   launch_residual(c->stream, b, level);
   c->nlaunch++;
+  if (b->prm.timel && level == 1) {   // TIMDER after SWEEP (res3c.f:705)
+    k_timder<5><<<nblk((long)b->imax * b->jmax * b->kmax, 256), 256, 0, c->stream>>>(b->db, b->prm);
+    c->nlaunch++;
+  }
   return 0;
 }
 
@@ -1480,6 +1488,17 @@ int ff_resl2(void* ctx, int blk, double* out5) {
   c->nlaunch++;
   CK(cudaMemcpyAsync(out5, c->d_resi, 5 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int ff_time_levels(void* ctx, int blk, int mode) {
+  Ctx* c = (Ctx*)ctx;
+  BlockCtx* b = getb(c, blk);
+  if (!b || (mode != 0 && mode != 1)) return fail(c, FF_ERR_ARG, "ff_time_levels");
+  const long n = mode == 0 ? (long)b->ntot : (long)b->imax * b->jmax * b->kmax;
+  k_time_levels<<<nblk(n, 256), 256, 0, c->stream>>>(b->db, b->prm.iturb >= 3 ? 7 : 5, mode);
+  c->nlaunch++;
+  CK(cudaGetLastError());
   return 0;
 }
 

@@ -624,6 +624,7 @@ __global__ void k_time3_copr(DevBlock b, ff_params p, double cfl, int mode = 0) 
   double denlow = 1. + dmax(0., (p.frspre - 2. * P) / P);
   double denmax = 1. + dmax(0., (ro - 2. * p.frsden) * ypro) * 5.;
   double dtl = 1. / (b11 * dmax(denlow, denmax));
+  if (p.timel) dtl = dtl * p.dt / (1.5 * dtl + p.dt);   // TIMEL dual time step, base3c.f:206-215
   b.a[FF_DTL][kk] = dtl;
   if (mode == 1) return;
   // LOCDT + COPR
@@ -1240,6 +1241,49 @@ __global__ void k_maxabs_de(DevBlock b, unsigned long long* dm_bits) {
   }
   for (int o = 16; o > 0; o >>= 1) amax = dmax(amax, __shfl_down_sync(0xffffffffu, amax, o));
   if ((threadIdx.x & 31) == 0 && amax > 0.) atomicMax(dm_bits, (unsigned long long)__double_as_longlong(amax));
+}
+
+// TIMDER res3c.f:3014 / TIMDKE res3c.f:3062 on the interior cells: the
+// second-order physical-time derivative of TIMEL added to the residual,
+// PDT * (-1.5 VOL (Q - Q2) + 0.5 VOL (Q2 - Q3)) with PDT = 1 / (VOL DT).
+template <int NV>
+__global__ void k_timder(DevBlock b, ff_params p) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= b.imax * b.jmax * b.kmax) return;
+  int I = t % b.imax + 1, J = (t / b.imax) % b.jmax + 1, K = t / (b.imax * b.jmax) + 1;
+  const size_t n = ix(b, I, J, K);
+  const int sq[7] = {FF_RO, FF_RM, FF_RN, FF_RW, FF_E, FF_RK, FF_REPS};
+  const double vol = b.a[FF_VOL][n], pdt = 1. / (vol * p.dt);
+#pragma unroll
+  for (int v = 0; v < NV; v++) {
+    const double q = b.a[sq[v]][n], q2 = b.a[FF_ROLE2 + v][n], q3 = b.a[FF_ROLE3 + v][n];
+    b.a[FF_DRO + v][n] = b.a[FF_DRO + v][n] + pdt * (-1.5 * vol * (q - q2) + 0.5 * vol * (q2 - q3));
+  }
+}
+
+// STARTI res3c.f:3175 (mode 0: both old time levels = the state, every
+// cell) and NEWTIM ns3c.f:9420 with R1 = 1 (mode 1: level n-1 <- level n,
+// level n <- the state, interior cells).
+__global__ void k_time_levels(DevBlock b, int nv, int mode) {
+  const int sq[7] = {FF_RO, FF_RM, FF_RN, FF_RW, FF_E, FF_RK, FF_REPS};
+  if (mode == 0) {
+    size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= (size_t)b.ntot) return;
+    for (int v = 0; v < nv; v++) {
+      const double q = b.a[sq[v]][n];
+      b.a[FF_ROLE3 + v][n] = q;
+      b.a[FF_ROLE2 + v][n] = q;
+    }
+    return;
+  }
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= b.imax * b.jmax * b.kmax) return;
+  int I = t % b.imax + 1, J = (t / b.imax) % b.jmax + 1, K = t / (b.imax * b.jmax) + 1;
+  const size_t n = ix(b, I, J, K);
+  for (int v = 0; v < nv; v++) {
+    b.a[FF_ROLE3 + v][n] = b.a[FF_ROLE2 + v][n];
+    b.a[FF_ROLE2 + v][n] = b.a[sq[v]][n];
+  }
 }
 
 #include "ff_sst.cuh"

@@ -82,6 +82,7 @@ def lib():
         L.ff_residu.argtypes = [vp, ci, ci, ci]
         L.ff_resl2.argtypes = [vp, ci, ctypes.POINTER(cd)]
         L.ff_imps.argtypes = [vp, ci, ci]
+        L.ff_time_levels.argtypes = [vp, ci, ci]
         L.ff_fin.argtypes = [vp, ci, ctypes.POINTER(cd)]
         L.ff_cycles.argtypes = [vp, ci, ci, ci, ctypes.POINTER(cd), ci]
         L.ff_time_cycles.argtypes = [vp, ci, ci, ctypes.POINTER(ctypes.c_float)]
@@ -200,6 +201,10 @@ class GpuSolver:
 
     def imps(self, bid=0, level=1):
         self._check(self.L.ff_imps(self.ctx, bid, level))
+
+    def time_levels(self, bid=0, mode=1):
+        """TIMEL: mode 0 = STARTI (both old levels = the state), 1 = NEWTIM."""
+        self._check(self.L.ff_time_levels(self.ctx, bid, mode))
 
     def fin(self, bid=0) -> float:
         d = ctypes.c_double()

@@ -70,6 +70,15 @@ int ff_resl2(void *ctx, int blk, double *out5);
 int ff_imps(void *ctx, int blk, int level);
 int ff_fin(void *ctx, int blk, double *dromax);
 
+/* Time-accurate runs (ff_params.timel = 1, physical step ff_params.dt):
+ * ff_residu adds TIMDER res3c.f:3014 (and TIMDKE res3c.f:3062) on level 1
+ * and TIME3 takes the dual time step (base3c.f:206-215).  The old time
+ * levels live in slots FF_ROLE2..FF_EPSLE3.  mode 0 = STARTI res3c.f:3175
+ * (both old levels = the current state, once before the first physical
+ * step), mode 1 = NEWTIM ns3c.f:9420 (shift the levels at the start of
+ * every later physical step), asynchronous. */
+int ff_time_levels(void *ctx, int blk, int mode);
+
 /* With ff_params.iturb = 6 (k-omega SST) ff_residu is
  * TURBEQ res3c.f:5845 + RESIKE res3c.f:3423, ff_imps the seven-equation
  * IMPS (LOCDTK, IMSOKO, COPRKE, PRKEGS/DIKEGS/COKEGS) and ff_fin also

@@ -66,6 +66,10 @@ typedef struct ff_params {
   int lusgs_fp32;                       /* 1: implicit operator in FP32       */
   int ddadi;                            /* 1: DDADI (LUSGS=0, imps3.f:320),    */
                                         /* 0: LU-SGS (LUSGS=1, imps3.f:378)    */
+  int timel;                            /* 1: time-accurate dual time stepping */
+                                        /* (TIMEL, level 1 of the block only)  */
+  int pad1;
+  double dt;                            /* physical time step DT (TIMEL)       */
 } ff_params;
 
 /* Per-cell array slots of one block (names are the reference's MAIN_ARRAYS,
@@ -97,6 +101,11 @@ enum ff_slot {
   FF_RK, FF_REPS, FF_DISTW, FF_FUN1, FF_SRK, FF_SEPS, FF_PTUR,
   FF_DKDX, FF_DKDY, FF_DKDZ, FF_DEDX, FF_DEDY, FF_DEDZ,
   FF_RKOLD, FF_EPSOLD, FF_F1RK, FF_F1EPS, FF_RKP2H, FF_EPP2H,
+  /* the two previous physical time levels of the conservative variables
+   * (TIMEL: ROLE2..EPSLE2 = level n, ROLE3..EPSLE3 = level n-1; STARTI
+   * res3c.f:3175, NEWTIM ns3c.f:9420) */
+  FF_ROLE2, FF_RMLE2, FF_RNLE2, FF_RWLE2, FF_ELE2, FF_RKLE2, FF_EPSLE2,
+  FF_ROLE3, FF_RMLE3, FF_RNLE3, FF_RWLE3, FF_ELE3, FF_RKLE3, FF_EPSLE3,
   FF_NSLOTS
 };
 

@@ -819,6 +819,51 @@ void orc_sweep(orc_block *b, int dir, int ido) {
 }
 
 /* RESIDU res3c.f:6 (laminar): zero D, REFCEN, gradients, k, i, j fluxes. */
+/* TIMDER res3c.f:3014 (and TIMDKE res3c.f:3062 for nv = 7): the second
+ * order physical-time derivative added to the residual of the interior
+ * cells, PDT * (-1.5 VOL (Q - Q2) + 0.5 VOL (Q2 - Q3)), PDT = 1/(VOL DT). */
+void orc_timder(orc_block *b, const ff_params *p, int nv) {
+  dims_t d = dims_of(b);
+  const int sq[7] = {FF_RO, FF_RM, FF_RN, FF_RW, FF_E, FF_RK, FF_REPS};
+  const int s2[7] = {FF_ROLE2, FF_RMLE2, FF_RNLE2, FF_RWLE2, FF_ELE2, FF_RKLE2, FF_EPSLE2};
+  const int s3[7] = {FF_ROLE3, FF_RMLE3, FF_RNLE3, FF_RWLE3, FF_ELE3, FF_RKLE3, FF_EPSLE3};
+  const double *VOL = b->a[FF_VOL];
+  for (int K = 1; K <= d.kmax; K++)
+    for (int J = 1; J <= d.jmax; J++)
+      for (int I = 1; I <= d.imax; I++) {
+        size_t n = IX(d, I, J, K);
+        double pdt = 1. / (VOL[n] * p->dt);
+        for (int v = 0; v < nv; v++) {
+          const double q = b->a[sq[v]][n], q2 = b->a[s2[v]][n], q3 = b->a[s3[v]][n];
+          b->a[FF_DRO + v][n] = b->a[FF_DRO + v][n] + pdt * (-1.5 * VOL[n] * (q - q2) + 0.5 * VOL[n] * (q2 - q3));
+        }
+      }
+}
+
+/* STARTI res3c.f:3175 (mode 0: both old levels = the current state, every
+ * cell) and NEWTIM ns3c.f:9420 with R1 = 1, R2 = R3 = 0 (mode 1: level n-1
+ * <- level n, level n <- the current state, interior cells). */
+void orc_time_levels(orc_block *b, int nv, int mode) {
+  dims_t d = dims_of(b);
+  const int sq[7] = {FF_RO, FF_RM, FF_RN, FF_RW, FF_E, FF_RK, FF_REPS};
+  const int s2[7] = {FF_ROLE2, FF_RMLE2, FF_RNLE2, FF_RWLE2, FF_ELE2, FF_RKLE2, FF_EPSLE2};
+  const int s3[7] = {FF_ROLE3, FF_RMLE3, FF_RNLE3, FF_RWLE3, FF_ELE3, FF_RKLE3, FF_EPSLE3};
+  for (int v = 0; v < nv; v++) {
+    double *Q = b->a[sq[v]], *Q2 = b->a[s2[v]], *Q3 = b->a[s3[v]];
+    if (mode == 0) {
+      for (int n = 0; n < d.ntot; n++) { Q3[n] = Q[n]; Q2[n] = Q[n]; }
+    } else {
+      for (int K = 1; K <= d.kmax; K++)
+        for (int J = 1; J <= d.jmax; J++)
+          for (int I = 1; I <= d.imax; I++) {
+            size_t n = IX(d, I, J, K);
+            Q3[n] = Q2[n];
+            Q2[n] = Q[n];
+          }
+    }
+  }
+}
+
 void orc_residu(orc_block *b, const ff_params *p, int level, int icycle) {
   dims_t d = dims_of(b);
   for (int s = FF_DRO; s <= FF_DE; s++) memset(b->a[s], 0, sizeof(double) * d.ntot);
@@ -833,6 +878,7 @@ void orc_residu(orc_block *b, const ff_params *p, int level, int icycle) {
     orc_flux_dir(b, p, dir, level);
     orc_sweep(b, dir, dir == 2);
   }
+  if (p->timel && level == 1) orc_timder(b, p, 5);   /* res3c.f:705 */
 }
 
 /* RESL2 res3c.f:8920: sums of squares of the explicit residuals. */
@@ -897,6 +943,8 @@ void orc_time3(orc_block *b, const ff_params *p, double cfl) {
         double denmax = (1. + MAXD(0., (RO[kk] - 2. * p->frsden) * ypro) * 5.);
         denlow = MAXD(denlow, denmax);
         DTL[kk] = 1. / (b11 * denlow);
+        /* TIMEL: the dual time step, base3c.f:206-215 */
+        if (p->timel) DTL[kk] = DTL[kk] * p->dt / (1.5 * DTL[kk] + p->dt);
       }
 }
 

@@ -40,6 +40,8 @@ void orc_diaggs(orc_block *b, const ff_params *p);
 void orc_corrgs(orc_block *b, const ff_params *p);
 void orc_imps(orc_block *b, const ff_params *p, int level);
 void orc_ddadi(orc_block *b, const ff_params *p);
+void orc_timder(orc_block *b, const ff_params *p, int nv);
+void orc_time_levels(orc_block *b, int nv, int mode);
 void orc_fin_limits(orc_block *b, const ff_params *p);
 void orc_refcor(orc_block *b);
 void orc_mir(orc_block *b);

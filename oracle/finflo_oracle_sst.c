@@ -691,6 +691,7 @@ void orc_residu_sst_lev(orc_block *b, const ff_params *p, int lev, int m2, int i
     sweepk(b, dir, dir == 2);
   }
   sourko_addske(b);
+  if (p->timel && lev == 1) orc_timder(b, p, 7);   /* TIMDER + TIMDKE, res3c.f:5097 */
 }
 
 void orc_residu_sst(orc_block *b, const ff_params *p, int icycle) {

@@ -112,6 +112,10 @@ class Oracle:
     def ddadi(self):
         self.L.orc_ddadi(self._b(), self._p())
 
+    def time_levels(self, mode):
+        """TIMEL: mode 0 = STARTI (both old levels = the state), 1 = NEWTIM."""
+        self.L.orc_time_levels(self._b(), 7 if self.prm.iturb >= 3 else 5, mode)
+
     def fin_limits(self):
         self.L.orc_fin_limits(self._b(), self._p())
 
