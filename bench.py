@@ -245,12 +245,17 @@ def run_ours(args):
     if args.ddadi:   # LUSGS=0: the reference's default implicit stage
         for q in prms:
             q.ddadi = 1
+    if args.timel:   # time-accurate: the timed cycles are inner cycles of one physical step
+        for q in prms:
+            q.timel, q.dt = 1, args.timel
     blk = levels[0]
     g = GpuSolver(local)
     bid = g.add_levels(levels, prms) if len(levels) > 1 else g.add_block(blk, prms[0])
     for q in range(len(levels)):
         g.upload(bid + q)
     g.start(bid)
+    if args.timel:
+        g.time_levels(bid, 0)   # STARTI
     g.cycles(1 + args.warmup, bid, icycle0=1)   # warm-up incl. the sweep autotuner and graph capture
     g.sync()
     ncell = blk.interior_cells
@@ -310,7 +315,9 @@ def run_ours(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": wl["dtype"],
         "data": "synthetic (seeded bump-channel grid and noisy free stream)",
-        "config": {"workload": (wl["name"] + (", DDADI implicit stage (LUSGS=0)" if args.ddadi else ""))
+        "config": {"workload": (wl["name"] + (", DDADI implicit stage (LUSGS=0)" if args.ddadi else "")
+                                + (f", time-accurate dual time stepping (TIMEL, DT={args.timel:g})"
+                                   if args.timel else ""))
                    if not args.grid else
                    f"{args.workload} at {blk.imax}x{blk.jmax}x{blk.kmax} cells (profiling size)",
                    "cells_per_gpu": ncell, "levels": len(levels), "parallelism": f"replicas x{ws}",
@@ -624,6 +631,8 @@ def main():
     ap.add_argument("--large-cells", default="512,256,128")
     ap.add_argument("--large-fp64", action="store_true", help="FP64 implicit stage in the large case")
     ap.add_argument("--ddadi", action="store_true", help="DDADI implicit stage (LUSGS=0) instead of LU-SGS")
+    ap.add_argument("--timel", type=float, default=0.0,
+                    help="physical time step DT of a time-accurate (TIMEL) run; 0 = steady")
     ap.add_argument("--ws-train", type=int, default=64)
     ap.add_argument("--ws-test", type=int, default=16)
     ap.add_argument("--ws-cycles", type=int, default=2000)

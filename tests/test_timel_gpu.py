@@ -54,8 +54,8 @@ def test_timel_residual_matches_oracle(gpu_lib):
     """One residual evaluation with old time levels that differ from the
     state: per cell within 1e-12 of the largest residual."""
     g, bid, bg, o, bc = _setup(False, 1e-5)
-    for _ in range(3):
-        o.cycle(1)
+    for i in range(3):
+        o.cycle(i + 1)
     g.cycles(3, bid, icycle0=1)
     o.time_levels(1)
     g.time_levels(bid, 1)
