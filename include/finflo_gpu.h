@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define FF_ABI_VERSION 2
+#define FF_ABI_VERSION 3   /* 3: ff_params gains ddadi, timel, dt; slots FF_ROLE2..FF_EPSLE3 */
 
 enum { FF_OK = 0, FF_ERR_CUDA = 1, FF_ERR_ARG = 2, FF_ERR_TIMEOUT = 3, FF_ERR_SIZE = 4 };
 enum { FF_STAGE_RESIDUAL = 1, FF_STAGE_GRAD = 2, FF_STAGE_STATE = 3, FF_STAGE_SWEEP = 4 };

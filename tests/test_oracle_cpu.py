@@ -185,7 +185,7 @@ def test_abi_exports_every_declared_symbol():
     assert len(names) >= 15
     for n in names:
         assert hasattr(L, n), n
-    assert L.ff_abi_version() == 2
+    assert L.ff_abi_version() == 3
 
 
 def test_nn_abi_exports_every_declared_symbol():
