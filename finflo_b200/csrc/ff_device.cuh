@@ -25,6 +25,9 @@ FF_DI size_t ix(const DevBlock& b, int I, int J, int K) {
 }
 
 template <typename T> FF_DI T dmax(T a, T b) { return a > b ? a : b; }
+// 1/x correctly rounded (the same value as 1. / x), through the reciprocal
+// intrinsic rather than the general division
+FF_DI double rcp(double x) { return __drcp_rn(x); }
 template <typename T> FF_DI T dmin(T a, T b) { return a < b ? a : b; }
 
 // SURFVECTS base3c.f:12245: two tangent unit vectors completing the normal.
@@ -94,9 +97,9 @@ FF_DI void roe_flux(const double q[5][4], double nx, double ny, double nz, doubl
   double elr = ppi / (gm1 * roim) - p.e0ref;
   double erl = pmi / (gm1 * roip) - p.e0ref;
   // DERIV base3c.f:707 (Glaister hat derivatives)
-  double ypro1 = 1. / cr[2], ypro2 = 1. / cl2[2];
+  double ypro1 = rcp(cr[2]), ypro2 = rcp(cl2[2]);
   double dedph = 0.5 * ((-cr[0] / cr[1] - ypro1) + (-cl2[0] / cl2[1] - ypro2));
-  double dedrh = 0.5 * ((1. / cr[1] + cr[3] * (ypro1 * ypro1)) + (1. / cl2[1] + cl2[3] * (ypro2 * ypro2)));
+  double dedrh = 0.5 * ((rcp(cr[1]) + cr[3] * (ypro1 * ypro1)) + (rcp(cl2[1]) + cl2[3] * (ypro2 * ypro2)));
   {
     double dpp = 2. * (ppi - pmi), drr = 2. * (roip - roim);
     if (fabs(dpp) >= 1.e-2 * (ppi + pmi)) dedph = (eip + elr - eim - erl) / dpp;
@@ -110,21 +113,21 @@ FF_DI void roe_flux(const double q[5][4], double nx, double ny, double nz, doubl
   double ul = nx * rmim + ny * rnim + nz * rwim;
   double vl = a21 * rmim + a22 * rnim + a23 * rwim;
   double wl = a31 * rmim + a32 * rnim + a33 * rwim;
-  double ypror = 1. / roip, yprol = 1. / roim;
+  double ypror = rcp(roip), yprol = rcp(roim);
   double eir = eip + .5 * (ur * ur + vr * vr + wr * wr);
   double eil = eim + .5 * (ul * ul + vl * vl + wl * wl);
   double pr = ppi, pl = pmi;
   double hr = eir + pr * ypror, hl = eil + yprol * pl;
-  double rohat = sqrt(roip * roim), yproh = 1. / rohat;
-  double sqrl = 1. / (roim + rohat), cql = roim * sqrl, cqr = 1. - cql;
+  double rohat = sqrt(roip * roim), yproh = rcp(rohat);
+  double sqrl = rcp(roim + rohat), cql = roim * sqrl, cqr = 1. - cql;
   double uhat = cqr * ur + cql * ul, vhat = cqr * vr + cql * vl, what = cqr * wr + cql * wl;
   double hhat = cqr * hr + cql * hl, ehat = cqr * eip + cql * eim;
   double phat = rohat * (hhat - ehat - .5 * (uhat * uhat + vhat * vhat + what * what));
   phat = dmin(dmax(pr, pl), phat);
   phat = dmax(dmin(pr, pl), phat);
-  double drdhh = 1. / (dedrh - phat * (yproh * yproh));
+  double drdhh = rcp(dedrh - phat * (yproh * yproh));
   double drdph = -drdhh * (dedph + yproh);
-  double chat2 = 1. / (drdhh * yproh + drdph);
+  double chat2 = rcp(drdhh * yproh + drdph);
   double cmin = dmin(c_r, c_l), cmax = dmax(c_r, c_l);
   chat2 = dmin(cmax * cmax, chat2);
   chat2 = dmax(cmin * cmin, chat2);
@@ -132,7 +135,7 @@ FF_DI void roe_flux(const double q[5][4], double nx, double ny, double nz, doubl
   double pdpde = dedph;
   double dro = roip - roim, du = ur - ul;
   double dp = pr - pl;
-  double pchat2 = 1. / (chat * chat);
+  double pchat2 = rcp(chat * chat);
   double alfa1 = .5 * (dp + rohat * chat * du) * pchat2;
   double alfa2 = .5 * (dp - rohat * chat * du) * pchat2;
   double alfa3 = dro - dp * pchat2;

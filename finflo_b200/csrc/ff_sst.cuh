@@ -209,9 +209,9 @@ FF_DI void roe_flux_ke(const double q[7][4], double nx, double ny, double nz, do
   double eim = pmi / (gm1 * roim) - p.e0ref;
   double elr = ppi / (gm1 * roim) - p.e0ref;
   double erl = pmi / (gm1 * roip) - p.e0ref;
-  double ypro1 = 1. / cr[2], ypro2 = 1. / cl2[2];
+  double ypro1 = rcp(cr[2]), ypro2 = rcp(cl2[2]);
   double dedph = 0.5 * ((-cr[0] / cr[1] - ypro1) + (-cl2[0] / cl2[1] - ypro2));
-  double dedrh = 0.5 * ((1. / cr[1] + cr[3] * (ypro1 * ypro1)) + (1. / cl2[1] + cl2[3] * (ypro2 * ypro2)));
+  double dedrh = 0.5 * ((rcp(cr[1]) + cr[3] * (ypro1 * ypro1)) + (rcp(cl2[1]) + cl2[3] * (ypro2 * ypro2)));
   {
     double dpp = 2. * (ppi - pmi), drr = 2. * (roip - roim);
     if (fabs(dpp) >= 1.e-2 * (ppi + pmi)) dedph = (eip + elr - eim - erl) / dpp;
@@ -227,22 +227,22 @@ FF_DI void roe_flux_ke(const double q[7][4], double nx, double ny, double nz, do
   double wl = a31 * rmim + a32 * rnim + a33 * rwim;
   double rkipi = dmax(0.001 * p.rklim, rkip), reipi = dmax(0.001 * p.epslim, reip);
   double rkimi = dmax(0.001 * p.rklim, rkim), reimi = dmax(0.001 * p.epslim, reim);
-  double ypror = 1. / roip, yprol = 1. / roim;
+  double ypror = rcp(roip), yprol = rcp(roim);
   double rkr = rkipi * ypror, rkl = rkimi * yprol;
   double eir = eip + .5 * (ur * ur + vr * vr + wr * wr) + rkr;
   double eil = eim + .5 * (ul * ul + vl * vl + wl * wl) + rkl;
   double pr = ppi, pl = pmi, pkr = .6667 * rkipi, pkl = .6667 * rkimi;
   double epsr = reipi * ypror, epsl = reimi * yprol;
   double hr = eir + pr * ypror, hl = eil + yprol * pl;
-  double rohat = sqrt(roip * roim), yproh = 1. / rohat;
-  double sqrl = 1. / (roim + rohat), cql = roim * sqrl, cqr = 1. - cql;
+  double rohat = sqrt(roip * roim), yproh = rcp(rohat);
+  double sqrl = rcp(roim + rohat), cql = roim * sqrl, cqr = 1. - cql;
   double uhat = cqr * ur + cql * ul, vhat = cqr * vr + cql * vl, what = cqr * wr + cql * wl;
   double hhat = cqr * hr + cql * hl, ehat = cqr * eip + cql * eim;
   double rkhat = cqr * rkr + cql * rkl, epshat = cqr * epsr + cql * epsl;
   double phat = rohat * (hhat - ehat - .5 * (uhat * uhat + vhat * vhat + what * what) - rkhat);
   phat = dmin(dmax(pr, pl), phat);
   phat = dmax(dmin(pr, pl), phat);
-  double drdhh = 1. / (dedrh - phat * (yproh * yproh));
+  double drdhh = rcp(dedrh - phat * (yproh * yproh));
   double drdph = -drdhh * (dedph + yproh);
   double xturb = 1. + .6667 * rkhat * yproh * drdph;
   double chat2 = xturb / (drdhh * yproh + drdph);
@@ -253,7 +253,7 @@ FF_DI void roe_flux_ke(const double q[7][4], double nx, double ny, double nz, do
   double pdpde = dedph;
   double dro = roip - roim, du = ur - ul, dk = rkr - rkl;
   double dp = pr - pl + .6667 * (rkhat * dro + rohat * dk);
-  double pchat2 = 1. / (chat * chat);
+  double pchat2 = rcp(chat * chat);
   double alfa1 = .5 * (dp + rohat * chat * du) * pchat2;
   double alfa2 = .5 * (dp - rohat * chat * du) * pchat2;
   double alfa3 = dro - dp * pchat2;
@@ -316,7 +316,7 @@ FF_DI void flkebl_face(const DevBlock& b, size_t I, int S, int dir, double& frk,
   double vv = LD(FF_VIS, I) + LD(FF_VIS, M), area = LD(FF_A1 + ao, I);
   double surfk = 0.5 * area * (vv + rmut2 * psigk);
   double surfep = 0.5 * area * (vv + rmut2 * psige);
-  double ypro1 = 1. / LD(FF_RO, I), ypro2 = 1. / LD(FF_RO, M);
+  double ypro1 = rcp(LD(FF_RO, I)), ypro2 = rcp(LD(FF_RO, M));
   frk = -surfk * (alfa * (LD(FF_RK, I) * ypro1 - LD(FF_RK, M) * ypro2) / slen + dkdxi * (nx - alfa * sxi) +
                   dkdyi * (ny - alfa * syi) + dkdzi * (nz - alfa * szi));
   feps = -surfep * (alfa * (LD(FF_REPS, I) * ypro1 - LD(FF_REPS, M) * ypro2) / slen + dedxi * (nx - alfa * sxi) +
@@ -336,7 +336,7 @@ FF_DI void fludke_face(const DevBlock& b, size_t I, int S, int dir, double& frk,
   double surg = -area * ypd2;
   double rmut2 = (LD(FF_EPS2, I) - 1.) * LD(FF_VIS, I) + (LD(FF_EPS2, M) - 1.) * LD(FF_VIS, M);
   double vv = LD(FF_VIS, I) + LD(FF_VIS, M);
-  double ypro1 = 1. / LD(FF_RO, I), ypro2 = 1. / LD(FF_RO, M);
+  double ypro1 = rcp(LD(FF_RO, I)), ypro2 = rcp(LD(FF_RO, M));
   frk = surg * (vv + rmut2 * psigk) * (LD(FF_RK, I) * ypro1 - LD(FF_RK, M) * ypro2);
   feps = surg * (vv + rmut2 * psige) * (LD(FF_REPS, I) * ypro1 - LD(FF_REPS, M) * ypro2);
 #undef LD
@@ -366,7 +366,7 @@ FF_DI void wall_flux_ke(const DevBlock& b, const ff_params& p, size_t II, int S,
   double rapub = 1.0E-20;
   double surfrk = surg * (1.0 + SST_SIGRK1 * rapub) * visb;
   double surfep = surg * (1.0 + SST_SIGOM1 * rapub) * visb;
-  double ypro1 = 1. / LD(FF_RO, II), ypro2 = 1. / LD(FF_RO, II2);
+  double ypro1 = rcp(LD(FF_RO, II)), ypro2 = rcp(LD(FF_RO, II2));
   double rnub = visb / rob;
   double plusfc = sqrt(rnub * straib) / rnub;
   double yplus1 = 2.0 * plusfc / dist;
