@@ -261,6 +261,26 @@ def _closest_on_triangles(p, a, b, c):
     return dist
 
 
+def wall_triangles(wb: Block) -> np.ndarray:
+    """The solid-wall faces (patch types 7-10) of wb's nodes, each split in
+    two triangles: [ntri, 9] = corners a, b, c."""
+    X, Y, Z = wb.nodes
+    P = np.stack([X, Y, Z], axis=-1)
+    tris = []
+    for pa in wb.patches:
+        if not (7 <= pa.ityp <= 10):
+            continue
+        d = (pa.iface - 1) % 3
+        idx = 0 if pa.iface <= 3 else (P.shape[2 - d] - 1)
+        sl = [slice(None)] * 3
+        sl[2 - d] = idx
+        F = P[tuple(sl)]
+        n00, n10, n01, n11 = F[:-1, :-1], F[1:, :-1], F[:-1, 1:], F[1:, 1:]
+        for a, b, c in ((n00, n10, n11), (n00, n11, n01)):
+            tris.append(np.concatenate([a.reshape(-1, 3), b.reshape(-1, 3), c.reshape(-1, 3)], axis=1))
+    return np.concatenate(tris) if tris else np.zeros((0, 9))
+
+
 def wall_distance(blk: Block, wall_block: Block = None, nnear: int = 8):
     """DISTW: distance of every cell centre (ghosts included) to the nearest
     point of the solid-wall surface of wall_block (default: blk itself;
@@ -269,23 +289,10 @@ def wall_distance(blk: Block, wall_block: Block = None, nnear: int = 8):
     reference's DISTANCES pass before the iteration loop."""
     from scipy.spatial import cKDTree
     wb = wall_block if wall_block is not None else blk
-    X, Y, Z = wb.nodes
-    P = np.stack([X, Y, Z], axis=-1)
-    tri_a, tri_b, tri_c = [], [], []
-    for pa in wb.patches:
-        if not (7 <= pa.ityp <= 10):
-            continue
-        d = (pa.iface - 1) % 3
-        idx = 0 if pa.iface <= 3 else (P.shape[2 - d] - 1)
-        sl = [slice(None)] * 3
-        sl[2 - d] = idx
-        F = P[tuple(sl)]                                    # 2-D node array of the face
-        n00, n10, n01, n11 = F[:-1, :-1], F[1:, :-1], F[:-1, 1:], F[1:, 1:]
-        for a, b, c in ((n00, n10, n11), (n00, n11, n01)):
-            tri_a.append(a.reshape(-1, 3)); tri_b.append(b.reshape(-1, 3)); tri_c.append(c.reshape(-1, 3))
-    if not tri_a:
+    T = wall_triangles(wb)
+    if not len(T):
         return np.full(blk.ntot, 1.0e3)
-    A, B, C = (np.concatenate(t) for t in (tri_a, tri_b, tri_c))
+    A, B, C = T[:, 0:3], T[:, 3:6], T[:, 6:9]
     cen = (A + B + C) / 3.0
     tree = cKDTree(cen)
     q = np.stack([blk.arrays["XC"], blk.arrays["YC"], blk.arrays["ZC"]], axis=1)

@@ -14,6 +14,7 @@
 #include <tuple>
 #include <vector>
 #include "ff_kernels.cuh"
+#include "ff_grid.cuh"
 #include "../../include/finflo_gpu.h"
 
 using namespace ff;
@@ -1488,6 +1489,79 @@ int ff_resl2(void* ctx, int blk, double* out5) {
   c->nlaunch++;
   CK(cudaMemcpyAsync(out5, c->d_resi, 5 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int ff_block_metrics(void* ctx, int blk, const double* xyz) {
+  Ctx* c = (Ctx*)ctx;
+  BlockCtx* b = getb(c, blk);
+  if (!b || !xyz) return fail(c, FF_ERR_ARG, "ff_block_metrics");
+  const GridDims g{b->imax + 1, b->jmax + 1, b->kmax + 1};
+  const size_t nn = (size_t)g.ni * g.nj * g.nk, ne = (size_t)(g.ni + 4) * (g.nj + 4) * (g.nk + 4);
+  double *dn = nullptr, *de = nullptr;
+  CK(cudaMalloc(&dn, 3 * nn * sizeof(double)));
+  if (cudaMalloc(&de, 3 * ne * sizeof(double)) != cudaSuccess) { cudaFree(dn); return fail(c, FF_ERR_CUDA, "ff_block_metrics"); }
+  cudaError_t e = cudaMemcpyAsync(dn, xyz, 3 * nn * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) {
+    k_extend_nodes<<<nblk((long)ne, 256), 256, 0, c->stream>>>(dn, de, g);
+    k_cell_metrics<<<nblk((long)b->ntot, 256), 256, 0, c->stream>>>(b->db, de);
+    c->nlaunch += 2;
+    e = cudaStreamSynchronize(c->stream);
+  }
+  cudaFree(dn);
+  cudaFree(de);
+  if (e != cudaSuccess) return fail(c, FF_ERR_CUDA, "ff_block_metrics", e);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int ff_wall_distance(void* ctx, int blk, const double* tri, int ntri) {
+  Ctx* c = (Ctx*)ctx;
+  BlockCtx* b = getb(c, blk);
+  if (!b || ntri < 0 || (ntri > 0 && !tri)) return fail(c, FF_ERR_ARG, "ff_wall_distance");
+  // tiles of WD_TT triangles with their bounding boxes (pruned search), or
+  // the plain search over all triangles for very long lists
+  const int ntile = (ntri + WD_TT - 1) / WD_TT;
+  const bool pruned = ntile > 0 && wd_pruned_smem(ntile) <= (size_t)c->smem_optin;
+  std::vector<double> box(pruned ? (size_t)ntile * 6 : 0);
+  for (int q = 0; q < (pruned ? ntile : 0); q++) {
+    double* bx = &box[(size_t)q * 6];
+    for (int cc = 0; cc < 3; cc++) { bx[cc] = 1e300; bx[3 + cc] = -1e300; }
+    for (int u = q * WD_TT; u < std::min(ntri, (q + 1) * WD_TT); u++)
+      for (int v = 0; v < 3; v++)
+        for (int cc = 0; cc < 3; cc++) {
+          const double x = tri[(size_t)u * 9 + 3 * v + cc];
+          bx[cc] = std::min(bx[cc], x);
+          bx[3 + cc] = std::max(bx[3 + cc], x);
+        }
+  }
+  double *dt = nullptr, *dbox = nullptr;
+  if (ntri > 0) CK(cudaMalloc(&dt, (size_t)ntri * 9 * sizeof(double)));
+  if (pruned && cudaMalloc(&dbox, box.size() * sizeof(double)) != cudaSuccess) {
+    cudaFree(dt);
+    return fail(c, FF_ERR_CUDA, "ff_wall_distance");
+  }
+  cudaError_t e = ntri > 0 ? cudaMemcpyAsync(dt, tri, (size_t)ntri * 9 * sizeof(double), cudaMemcpyHostToDevice, c->stream)
+                           : cudaSuccess;
+  if (e == cudaSuccess && pruned)
+    e = cudaMemcpyAsync(dbox, box.data(), box.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) {
+    if (pruned) {
+      const size_t sm = wd_pruned_smem(ntile);
+      cudaFuncSetAttribute(k_wall_distance_pruned, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      const int is = b->imax + 4, js = b->jmax + 4, ks = b->kmax + 4;
+      const int nb = nblk(is, WD_BI) * nblk(js, WD_BJ) * nblk(ks, WD_BK);
+      k_wall_distance_pruned<<<nb, WD_THREADS, sm, c->stream>>>(b->db, dt, ntri, dbox, ntile);
+    } else {
+      k_wall_distance<<<nblk((long)b->ntot, WD_THREADS), WD_THREADS, 0, c->stream>>>(b->db, dt, ntri);
+    }
+    c->nlaunch++;
+    e = cudaStreamSynchronize(c->stream);
+  }
+  if (dt) cudaFree(dt);
+  if (dbox) cudaFree(dbox);
+  if (e != cudaSuccess) return fail(c, FF_ERR_CUDA, "ff_wall_distance", e);
+  CK(cudaGetLastError());
   return 0;
 }
 

@@ -22,7 +22,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libfinflo_gpu.so")
 _SRC = [os.path.join(_HERE, "csrc", f) for f in ("ff_gpu.cu", "ff_kernels.cuh", "ff_device.cuh",
                                                  "ff_noalloc.cu", "ff_sst.cuh", "ff_pipe.cuh",
-                                                 "ff_ddadi.cuh")]
+                                                 "ff_ddadi.cuh", "ff_grid.cuh")]
 NVCC_FLAGS = ["-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC", "-shared", "-std=c++17"]
 
@@ -83,6 +83,8 @@ def lib():
         L.ff_resl2.argtypes = [vp, ci, ctypes.POINTER(cd)]
         L.ff_imps.argtypes = [vp, ci, ci]
         L.ff_time_levels.argtypes = [vp, ci, ci]
+        L.ff_block_metrics.argtypes = [vp, ci, vp]
+        L.ff_wall_distance.argtypes = [vp, ci, vp, ci]
         L.ff_fin.argtypes = [vp, ci, ctypes.POINTER(cd)]
         L.ff_cycles.argtypes = [vp, ci, ci, ci, ctypes.POINTER(cd), ci]
         L.ff_time_cycles.argtypes = [vp, ci, ci, ctypes.POINTER(ctypes.c_float)]
@@ -201,6 +203,16 @@ class GpuSolver:
 
     def imps(self, bid=0, level=1):
         self._check(self.L.ff_imps(self.ctx, bid, level))
+
+    def block_metrics(self, bid, X, Y, Z):
+        """Metrics of the block from its nodes (arrays [nk, nj, ni]) on the device."""
+        xyz = np.ascontiguousarray(np.concatenate([np.ravel(X), np.ravel(Y), np.ravel(Z)]), dtype=np.float64)
+        self._check(self.L.ff_block_metrics(self.ctx, bid, xyz.ctypes.data))
+
+    def wall_distance(self, bid, tri):
+        """DISTW on the device from wall triangles tri [ntri, 9] (corners a, b, c)."""
+        t = np.ascontiguousarray(tri, dtype=np.float64).reshape(-1, 9)
+        self._check(self.L.ff_wall_distance(self.ctx, bid, t.ctypes.data if len(t) else None, len(t)))
 
     def time_levels(self, bid=0, mode=1):
         """TIMEL: mode 0 = STARTI (both old levels = the state), 1 = NEWTIM."""

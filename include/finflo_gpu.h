@@ -79,6 +79,19 @@ int ff_fin(void *ctx, int blk, double *dromax);
  * every later physical step), asynchronous. */
 int ff_time_levels(void *ctx, int blk, int mode);
 
+/* Block set-up on the device (no counterpart call in the reference, which
+ * computes its metrics in GRIVAL/GRID1B ns3c.f:5636, gluebm.f:1265 and its
+ * wall distance in DISTANCES gluebm.f:9136 on the host).
+ * ff_block_metrics: xyz = the block's nodes, X then Y then Z, each
+ * (KMAX+1)(JMAX+1)(IMAX+1) values with i fastest; fills A1..A3ZA, VOL,
+ * XC..ZC and D1..D3 of every cell, ghosts included (ghost nodes by mirror
+ * extrapolation).  ff_wall_distance: tri = ntri wall triangles of 9 values
+ * (three corners); fills DISTW of every cell with the exact distance of its
+ * centre (XC, YC, ZC as on the device) to the nearest triangle, 1e3 when
+ * ntri = 0.  Both synchronous. */
+int ff_block_metrics(void *ctx, int blk, const double *xyz);
+int ff_wall_distance(void *ctx, int blk, const double *tri, int ntri);
+
 /* With ff_params.iturb = 6 (k-omega SST) ff_residu is
  * TURBEQ res3c.f:5845 + RESIKE res3c.f:3423, ff_imps the seven-equation
  * IMPS (LOCDTK, IMSOKO, COPRKE, PRKEGS/DIKEGS/COKEGS) and ff_fin also
