@@ -1515,6 +1515,61 @@ int ff_block_metrics(void* ctx, int blk, const double* xyz) {
   return 0;
 }
 
+int ff_block_metrics_levels(void* ctx, int blk, int nlev, const double* xyz) {
+  Ctx* c = (Ctx*)ctx;
+  BlockCtx* b = getb(c, blk);
+  if (!b || !xyz || nlev < 1) return fail(c, FF_ERR_ARG, "ff_block_metrics_levels");
+  std::vector<BlockCtx*> lv;
+  for (BlockCtx* x = b; x && (int)lv.size() < nlev; x = x->coarse) lv.push_back(x);
+  if ((int)lv.size() != nlev) return fail(c, FF_ERR_ARG, "ff_block_metrics_levels: fewer linked levels than nlev");
+  const int ng = 2 << (nlev - 1);
+  const GridDims g{b->imax + 1, b->jmax + 1, b->kmax + 1};
+  const size_t nn = (size_t)g.ni * g.nj * g.nk;
+  RawDims r{b->imax + 2 * ng, b->jmax + 2 * ng, b->kmax + 2 * ng};
+  const size_t ne = (size_t)(r.ci + 1) * (r.cj + 1) * (r.ck + 1);
+  double *dn = nullptr, *de = nullptr, *raw = nullptr, *raw2 = nullptr;
+  auto cleanup = [&]() { cudaFree(dn); cudaFree(de); cudaFree(raw); cudaFree(raw2); };
+  if (cudaMalloc(&dn, 3 * nn * sizeof(double)) != cudaSuccess || cudaMalloc(&de, 3 * ne * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&raw, RW_N * r.n() * sizeof(double)) != cudaSuccess) {
+    cleanup();
+    return fail(c, FF_ERR_CUDA, "ff_block_metrics_levels: device memory");
+  }
+  cudaError_t e = cudaMemcpyAsync(dn, xyz, 3 * nn * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) {
+    k_extend_nodes<<<nblk((long)ne, 256), 256, 0, c->stream>>>(dn, de, g, ng);
+    k_raw_metrics<<<nblk((long)r.n(), 256), 256, 0, c->stream>>>(de, raw, r);
+    c->nlaunch += 2;
+    int lng = ng;
+    for (int l = 0; l < nlev && e == cudaSuccess; l++) {
+      BlockCtx* x = lv[l];
+      k_finish_metrics<<<nblk((long)x->ntot, 256), 256, 0, c->stream>>>(x->db, raw, r, lng);
+      c->nlaunch++;
+      if (l + 1 < nlev) {
+        RawDims rc{r.ci / 2, r.cj / 2, r.ck / 2};
+        if (lv[l + 1]->imax + 2 * (lng / 2) != rc.ci || lv[l + 1]->jmax + 2 * (lng / 2) != rc.cj ||
+            lv[l + 1]->kmax + 2 * (lng / 2) != rc.ck) {
+          cleanup();
+          return fail(c, FF_ERR_ARG, "ff_block_metrics_levels: a coarse level does not halve the finer one");
+        }
+        if (cudaMalloc(&raw2, RW_N * rc.n() * sizeof(double)) != cudaSuccess) { e = cudaErrorMemoryAllocation; break; }
+        k_lump<<<nblk((long)rc.n(), 256), 256, 0, c->stream>>>(raw, r, raw2, rc);
+        c->nlaunch++;
+        e = cudaStreamSynchronize(c->stream);
+        cudaFree(raw);
+        raw = raw2;
+        raw2 = nullptr;
+        r = rc;
+        lng /= 2;
+      }
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  }
+  cleanup();
+  if (e != cudaSuccess) return fail(c, FF_ERR_CUDA, "ff_block_metrics_levels", e);
+  CK(cudaGetLastError());
+  return 0;
+}
+
 int ff_wall_distance(void* ctx, int blk, const double* tri, int ntri) {
   Ctx* c = (Ctx*)ctx;
   BlockCtx* b = getb(c, blk);

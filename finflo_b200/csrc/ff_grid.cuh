@@ -40,12 +40,13 @@ FF_DI double node_ijk(const double* X, const GridDims& g, int i, int j, int k) {
   return node_jk(X, g, i, j, k);
 }
 
-// The extended nodes, (ni+4)(nj+4)(nk+4) per coordinate, i fastest.
-__global__ void k_extend_nodes(const double* __restrict__ xyz, double* __restrict__ ext, GridDims g) {
-  const int ei = g.ni + 4, ej = g.nj + 4, ek = g.nk + 4;
+// The extended nodes with ng ghost layers, (ni+2ng)(nj+2ng)(nk+2ng) per
+// coordinate, i fastest.
+__global__ void k_extend_nodes(const double* __restrict__ xyz, double* __restrict__ ext, GridDims g, int ng = 2) {
+  const int ei = g.ni + 2 * ng, ej = g.nj + 2 * ng, ek = g.nk + 2 * ng;
   const size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x, ne = (size_t)ei * ej * ek;
   if (n >= ne) return;
-  const int i = (int)(n % ei) - 2, j = (int)((n / ei) % ej) - 2, k = (int)(n / ((size_t)ei * ej)) - 2;
+  const int i = (int)(n % ei) - ng, j = (int)((n / ei) % ej) - ng, k = (int)(n / ((size_t)ei * ej)) - ng;
   const size_t ni = (size_t)g.ni * g.nj * g.nk;
   for (int c = 0; c < 3; c++) ext[c * ne + n] = node_ijk(xyz + c * ni, g, i, j, k);
 }
@@ -100,6 +101,104 @@ __global__ void k_cell_metrics(DevBlock b, const double* __restrict__ ext) {
     b.a[FF_A1YA + 4 * d][n] = lo[d].y / safe;
     b.a[FF_A1ZA + 4 * d][n] = lo[d].z / safe;
     const double ah = sqrt(vdot(hi[d], hi[d]));
+    b.a[FF_D1 + d][n] = dmin(1e4, (vol + eps) / (mag + ah + eps) * 2.0);
+  }
+}
+
+// Multigrid levels (the host's mg_metrics): the fine level's face vectors,
+// volumes and volume-weighted centres with NG = 2 * 2^(nlev-1) ghost
+// layers ("raw" arrays, 22 values per cell: S1, S2, S3 low / high, VOL, C),
+// lumped level by level (coarse volume = sum of the 8 children, coarse face
+// vector = sum of the 4 child faces, centre volume-weighted, ghost layers
+// halved), each level then cropped to 2 ghost layers and finished (areas,
+// unit normals, D1..D3) into its block.
+struct RawDims {
+  int ci, cj, ck;   // cells per direction including the ng ghost layers
+  __host__ __device__ size_t n() const { return (size_t)ci * cj * ck; }
+};
+enum : int { RW_S1 = 0, RW_S2 = 3, RW_S3 = 6, RW_S1H = 9, RW_S2H = 12, RW_S3H = 15, RW_VOL = 18, RW_C = 19, RW_N = 22 };
+
+__global__ void k_raw_metrics(const double* __restrict__ ext, double* __restrict__ raw, RawDims r) {
+  const size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x, nr = r.n();
+  if (n >= nr) return;
+  const int i = (int)(n % r.ci), j = (int)((n / r.ci) % r.cj), k = (int)(n / ((size_t)r.ci * r.cj));
+  const int ei = r.ci + 1, ej = r.cj + 1;
+  const size_t ne = (size_t)ei * ej * (r.ck + 1);
+  auto P = [&](int dk, int dj, int di) { return v3(ext, ne, ((size_t)(k + dk) * ej + (j + dj)) * ei + (i + di)); };
+  const V3 p000 = P(0, 0, 0), p001 = P(0, 0, 1), p010 = P(0, 1, 0), p011 = P(0, 1, 1);
+  const V3 p100 = P(1, 0, 0), p101 = P(1, 0, 1), p110 = P(1, 1, 0), p111 = P(1, 1, 1);
+  const V3 f[6] = {face_vec(p000, p110, p100, p010), face_vec(p000, p101, p001, p100), face_vec(p000, p011, p010, p001),
+                   face_vec(p001, p111, p101, p011), face_vec(p010, p111, p011, p110), face_vec(p100, p111, p110, p101)};
+  const V3 ci = centroid4(p000, p100, p010, p110), cih = centroid4(p001, p101, p011, p111);
+  const V3 cj = centroid4(p000, p100, p001, p101), cjh = centroid4(p010, p110, p011, p111);
+  const V3 ck = centroid4(p000, p010, p001, p011), ckh = centroid4(p100, p110, p101, p111);
+  const double vol = (vdot(cih, f[3]) - vdot(ci, f[0]) + vdot(cjh, f[4]) - vdot(cj, f[1]) + vdot(ckh, f[5]) - vdot(ck, f[2])) / 3.0;
+  for (int q = 0; q < 6; q++) {
+    raw[(size_t)(3 * q + 0) * nr + n] = f[q].x;
+    raw[(size_t)(3 * q + 1) * nr + n] = f[q].y;
+    raw[(size_t)(3 * q + 2) * nr + n] = f[q].z;
+  }
+  const V3 c8[8] = {p000, p001, p010, p011, p100, p101, p110, p111};
+  double cx = 0., cy = 0., cz = 0.;
+  for (int q = 0; q < 8; q++) { cx = cx + c8[q].x; cy = cy + c8[q].y; cz = cz + c8[q].z; }
+  raw[(size_t)RW_VOL * nr + n] = vol;
+  raw[(size_t)(RW_C + 0) * nr + n] = 0.125 * cx;
+  raw[(size_t)(RW_C + 1) * nr + n] = 0.125 * cy;
+  raw[(size_t)(RW_C + 2) * nr + n] = 0.125 * cz;
+}
+
+// One coarsening step: coarse cell (i, j, k) from the fine children
+// (2i+a, 2j+b, 2k+c), in the host's summation order.
+__global__ void k_lump(const double* __restrict__ fr, RawDims f, double* __restrict__ cr, RawDims c) {
+  const size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x, nc = c.n(), nf = f.n();
+  if (n >= nc) return;
+  const int i = (int)(n % c.ci), j = (int)((n / c.ci) % c.cj), k = (int)(n / ((size_t)c.ci * c.cj));
+  auto F = [&](int comp, int dk, int dj, int di) {
+    return fr[(size_t)comp * nf + ((size_t)(2 * k + dk) * f.cj + (2 * j + dj)) * f.ci + (2 * i + di)];
+  };
+  // the eight children in the order (k, j, i) = 000, 001, 010, 011, 100, ...
+  auto csum = [&](auto val) {
+    return val(0, 0, 0) + val(0, 0, 1) + val(0, 1, 0) + val(0, 1, 1) + val(1, 0, 0) + val(1, 0, 1) + val(1, 1, 0) +
+           val(1, 1, 1);
+  };
+  const double vc = csum([&](int a, int bq, int cq) { return F(RW_VOL, a, bq, cq); });
+  cr[(size_t)RW_VOL * nc + n] = vc;
+  for (int d = 0; d < 3; d++)
+    cr[(size_t)(RW_C + d) * nc + n] =
+        csum([&](int a, int bq, int cq) { return F(RW_C + d, a, bq, cq) * F(RW_VOL, a, bq, cq); }) / vc;
+  for (int d = 0; d < 3; d++) {
+    // low faces: the four children on the low side of the direction
+    cr[(size_t)(RW_S1 + d) * nc + n] = F(RW_S1 + d, 0, 0, 0) + F(RW_S1 + d, 0, 1, 0) + F(RW_S1 + d, 1, 0, 0) + F(RW_S1 + d, 1, 1, 0);
+    cr[(size_t)(RW_S2 + d) * nc + n] = F(RW_S2 + d, 0, 0, 0) + F(RW_S2 + d, 0, 0, 1) + F(RW_S2 + d, 1, 0, 0) + F(RW_S2 + d, 1, 0, 1);
+    cr[(size_t)(RW_S3 + d) * nc + n] = F(RW_S3 + d, 0, 0, 0) + F(RW_S3 + d, 0, 0, 1) + F(RW_S3 + d, 0, 1, 0) + F(RW_S3 + d, 0, 1, 1);
+    cr[(size_t)(RW_S1H + d) * nc + n] = F(RW_S1H + d, 0, 0, 1) + F(RW_S1H + d, 0, 1, 1) + F(RW_S1H + d, 1, 0, 1) + F(RW_S1H + d, 1, 1, 1);
+    cr[(size_t)(RW_S2H + d) * nc + n] = F(RW_S2H + d, 0, 1, 0) + F(RW_S2H + d, 0, 1, 1) + F(RW_S2H + d, 1, 1, 0) + F(RW_S2H + d, 1, 1, 1);
+    cr[(size_t)(RW_S3H + d) * nc + n] = F(RW_S3H + d, 1, 0, 0) + F(RW_S3H + d, 1, 0, 1) + F(RW_S3H + d, 1, 1, 0) + F(RW_S3H + d, 1, 1, 1);
+  }
+}
+
+// A level's metric slots from its raw arrays (ng ghost layers, cropped to 2).
+__global__ void k_finish_metrics(DevBlock b, const double* __restrict__ raw, RawDims r, int ng) {
+  const int is = b.imax + 4, js = b.jmax + 4;
+  const size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x, nr = r.n();
+  if (n >= (size_t)b.ntot) return;
+  const int i = (int)(n % is), j = (int)((n / is) % js), k = (int)(n / ((size_t)is * js));
+  const int o = ng - 2;
+  const size_t m = ((size_t)(k + o) * r.cj + (j + o)) * r.ci + (i + o);
+  auto R = [&](int comp) { return raw[(size_t)comp * nr + m]; };
+  const double vol = R(RW_VOL), eps = 1e-20;
+  b.a[FF_VOL][n] = vol;
+  b.a[FF_XC][n] = R(RW_C);
+  b.a[FF_YC][n] = R(RW_C + 1);
+  b.a[FF_ZC][n] = R(RW_C + 2);
+  for (int d = 0; d < 3; d++) {
+    const V3 lo{R(3 * d), R(3 * d + 1), R(3 * d + 2)}, hi{R(9 + 3 * d), R(10 + 3 * d), R(11 + 3 * d)};
+    const double mag = sqrt(vdot(lo, lo)), safe = mag > 0. ? mag : 1.;
+    b.a[FF_A1 + 4 * d][n] = mag;
+    b.a[FF_A1XA + 4 * d][n] = lo.x / safe;
+    b.a[FF_A1YA + 4 * d][n] = lo.y / safe;
+    b.a[FF_A1ZA + 4 * d][n] = lo.z / safe;
+    const double ah = sqrt(vdot(hi, hi));
     b.a[FF_D1 + d][n] = dmin(1e4, (vol + eps) / (mag + ah + eps) * 2.0);
   }
 }

@@ -84,6 +84,7 @@ def lib():
         L.ff_imps.argtypes = [vp, ci, ci]
         L.ff_time_levels.argtypes = [vp, ci, ci]
         L.ff_block_metrics.argtypes = [vp, ci, vp]
+        L.ff_block_metrics_levels.argtypes = [vp, ci, ci, vp]
         L.ff_wall_distance.argtypes = [vp, ci, vp, ci]
         L.ff_fin.argtypes = [vp, ci, ctypes.POINTER(cd)]
         L.ff_cycles.argtypes = [vp, ci, ci, ci, ctypes.POINTER(cd), ci]
@@ -208,6 +209,11 @@ class GpuSolver:
         """Metrics of the block from its nodes (arrays [nk, nj, ni]) on the device."""
         xyz = np.ascontiguousarray(np.concatenate([np.ravel(X), np.ravel(Y), np.ravel(Z)]), dtype=np.float64)
         self._check(self.L.ff_block_metrics(self.ctx, bid, xyz.ctypes.data))
+
+    def block_metrics_levels(self, bid, nlev, X, Y, Z):
+        """Metrics of the block and its nlev - 1 linked coarse levels on the device."""
+        xyz = np.ascontiguousarray(np.concatenate([np.ravel(X), np.ravel(Y), np.ravel(Z)]), dtype=np.float64)
+        self._check(self.L.ff_block_metrics_levels(self.ctx, bid, nlev, xyz.ctypes.data))
 
     def wall_distance(self, bid, tri):
         """DISTW on the device from wall triangles tri [ntri, 9] (corners a, b, c)."""

@@ -90,6 +90,11 @@ int ff_time_levels(void *ctx, int blk, int mode);
  * centre (XC, YC, ZC as on the device) to the nearest triangle, 1e3 when
  * ntri = 0.  Both synchronous. */
 int ff_block_metrics(void *ctx, int blk, const double *xyz);
+/* The same for a block and its nlev - 1 linked coarse levels (ff_mg_link):
+ * the fine cells with 2 * 2^(nlev-1) ghost layers, each coarse level lumped
+ * from the finer one (volumes and face vectors summed over the children,
+ * centres volume-weighted). */
+int ff_block_metrics_levels(void *ctx, int blk, int nlev, const double *xyz);
 int ff_wall_distance(void *ctx, int blk, const double *tri, int ntri);
 
 /* With ff_params.iturb = 6 (k-omega SST) ff_residu is

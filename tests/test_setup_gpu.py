@@ -42,6 +42,27 @@ def test_device_metrics_match_host(gpu_lib, kind):
     g.close()
 
 
+def test_device_multigrid_metrics_match_host(gpu_lib):
+    """Three levels: the fine cells with 8 ghost layers, lumped twice."""
+    levels, prms, fs = case.bump_case_mg(33, 17, 17, nlev=3)
+    ref = [{n: lv.arrays[n].copy() for n in grid.METRIC_NAMES} for lv in levels]
+    for lv in levels:
+        for n in grid.METRIC_NAMES:
+            lv.arrays[n][:] = 0.0
+    g = GpuSolver(0)
+    bid = g.add_levels(levels, prms)
+    for q in range(len(levels)):
+        g.upload(bid + q)
+    g.block_metrics_levels(bid, 3, *levels[0].nodes)
+    for q in range(len(levels)):
+        d = g.download(bid + q, list(grid.METRIC_NAMES))
+        for n in grid.METRIC_NAMES:
+            scale = 1.0 if n.endswith(("XA", "YA", "ZA")) else np.abs(ref[q][n]).max()
+            err = np.abs(d[n] - ref[q][n]).max() / scale
+            assert err <= 1e-12, (q, n, err)
+    g.close()
+
+
 def _brute_force_distance(q, T):
     best = np.full(len(q), np.inf)
     for t in T:
