@@ -459,9 +459,11 @@ def run_large(args):
     nlev = 3
     t0 = time.perf_counter()
     g = GpuSolver(local)
+    dev = not args.host_setup   # metrics and wall distance on the device (ff_block_metrics_levels)
     it = case.bump_multiblock_blocks(cells=cells, nb=(2, 2, 2), nlev=nlev, seed=5, lusgs_fp32=fp32,
-                                     coarse_fp32=fp32)
+                                     coarse_fp32=fp32, device_setup=dev)
     _, fs = next(it)
+    tri = next(it)[1] if dev else None
     fine_cells = []
     for n, (levels, prms) in enumerate(it):
         fine = levels[0]
@@ -479,6 +481,11 @@ def run_large(args):
         assert bid == n * nlev
         for q in range(nlev):
             g.upload(bid + q)
+        if dev:
+            g.block_metrics_levels(bid, nlev, *fine.nodes)
+            for q in range(nlev):
+                g.wall_distance(bid + q, tri)
+        for q in range(nlev):
             levels[q].arrays = {}
         fine_cells.append(fine.imax * fine.jmax * fine.kmax)
     setup_s = time.perf_counter() - t0
@@ -503,6 +510,8 @@ def run_large(args):
         "config": {"workload": LARGE_NAME.format(cells="x".join(map(str, cells)), prec="FP32" if fp32 else "FP64")
                    + (", DDADI implicit stage (LUSGS=0)" if args.ddadi else ""),
                    "cells": total, "blocks": len(fine_cells), "levels": nlev, "setup_s": setup_s,
+                   "setup": "metrics and wall distance on the host" if args.host_setup else
+                            "metrics and wall distance on the device",
                    "parallelism": "blocks on 1 GPU", "l2": "inputs larger than L2"},
         "gpu_launches": per_cycle * args.steps,
         "roofline": {"bound": "hbm", "kernel": "k_residual_sst (block 0)", "achieved": achieved, "peak": peak,
@@ -630,6 +639,7 @@ def main():
     ap.add_argument("--prec-cfl", type=float, default=1.0)
     ap.add_argument("--large-cells", default="512,256,128")
     ap.add_argument("--large-fp64", action="store_true", help="FP64 implicit stage in the large case")
+    ap.add_argument("--host-setup", action="store_true", help="large case: metrics and wall distance on the host")
     ap.add_argument("--ddadi", action="store_true", help="DDADI implicit stage (LUSGS=0) instead of LU-SGS")
     ap.add_argument("--timel", type=float, default=0.0,
                     help="physical time step DT of a time-accurate (TIMEL) run; 0 = steady")

@@ -342,16 +342,18 @@ def bump_case(ni=65, nj=33, nk=33, *, h1=1e-3, amp=0.1, mach=0.5, reynolds=1e4,
     return blk, prm, fs
 
 
-def setup_sst(blk: Block, prm: FFParams, fs, tu=1.0e-3, mut_ratio=0.1, wall_block: Block = None):
+def setup_sst(blk: Block, prm: FFParams, fs, tu=1.0e-3, mut_ratio=0.1, wall_block: Block = None, distw=True):
     """Switch a case to k-omega SST: ITURB=6, the free-stream limits RKLIM /
-    EPSLIM, inlet BOUNRK/BOUNEP, DISTW, and rho*k, rho*omega, mu_t of the
-    free stream in every cell."""
+    EPSLIM, inlet BOUNRK/BOUNEP, DISTW (distw=False leaves it to the device,
+    ff_wall_distance), and rho*k, rho*omega, mu_t of the free stream in
+    every cell."""
     rk, re = sst_freestream(fs, tu, mut_ratio)
     prm.iturb = 6
     prm.rklim, prm.epslim = rk, re
     for pa in blk.patches:
         pa.bounrk, pa.bounep = rk, re
-    blk.arrays["DISTW"][:] = wall_distance(blk, wall_block)
+    if distw:
+        blk.arrays["DISTW"][:] = wall_distance(blk, wall_block)
     blk.arrays["RK"][:] = rk
     blk.arrays["REPS"][:] = re
     blk.arrays["EPS2"][:] = 1.0 + mut_ratio
@@ -512,7 +514,7 @@ class _WallSurface:
 def bump_multiblock_blocks(cells=(512, 256, 128), nb=(2, 2, 2), nlev=3, *, seed=5, h1=2e-6, amp=0.1,
                            span_amp=0.5, zlen=1.0, mach=0.7, reynolds=5e6, noise=1e-3, cfl=1.0, cfll=1.0,
                            inter=3, turbulence="sst", tu=1.0e-3, mut_ratio=0.1, lusgs_fp32=True,
-                           coarse_fp32=True):
+                           coarse_fp32=True, device_setup=False):
     """The bump channel split into nb[0] x nb[1] x nb[2] blocks of uneven
     sizes (cut positions from the seed), 1:1 patched on every interior cut,
     periodic in z through 1:1 patches (the spanwise amplitude
@@ -522,13 +524,18 @@ def bump_multiblock_blocks(cells=(512, 256, 128), nb=(2, 2, 2), nlev=3, *, seed=
     patch's IBTYPE is the source block's index.  Block metrics take mirror
     ghost nodes at the cuts as well (the interface faces themselves are
     exact); the wall distance is to the walls of the whole channel.  Also
-    yields the free stream first: the first item is ("fs", fs)."""
+    yields the free stream first: the first item is ("fs", fs).  With
+    device_setup the metric arrays and DISTW are left at zero for
+    ff_block_metrics_levels / ff_wall_distance: the second item is then
+    ("wall", triangles), and each level-1 block carries its nodes."""
     fc = FlowConditions(mach=mach, reynolds=reynolds)
     fs = fc.freestream()
     yield "fs", fs
     NI, NJ, NK = cells
     X, Y, Z = grid.bump_nodes(NI + 1, NJ + 1, NK + 1, h1=h1, amp=amp, zlen=zlen, span_amp=span_amp)
     wall = _WallSurface(X, Y, Z)
+    if device_setup:
+        yield "wall", wall_triangles(wall)
     cut = bump_block_cuts(cells, nb, seed)
     ids = {}
     for c in range(nb[2]):
@@ -542,7 +549,13 @@ def bump_multiblock_blocks(cells=(512, 256, 128), nb=(2, 2, 2), nlev=3, *, seed=
         k0, k1 = cut[2][c], cut[2][c + 1]
         Xb, Yb, Zb = (np.ascontiguousarray(A[k0:k1 + 1, j0:j1 + 1, i0:i1 + 1]) for A in (X, Y, Z))
         levels = []
-        for lev, m in enumerate(grid.mg_metrics(Xb, Yb, Zb, nlev)):
+        if device_setup:   # dimensions only; the device fills the metrics
+            mets = [grid.Metrics((i1 - i0) >> lev, (j1 - j0) >> lev, (k1 - k0) >> lev) for lev in range(nlev)]
+            for m in mets:
+                m.arrays = {n: np.zeros(m.ntot) for n in grid.METRIC_NAMES}
+        else:
+            mets = grid.mg_metrics(Xb, Yb, Zb, nlev)
+        for lev, m in enumerate(mets):
             pats = []
             for iface in range(1, 7):
                 d = (iface - 1) % 3
@@ -562,14 +575,14 @@ def bump_multiblock_blocks(cells=(512, 256, 128), nb=(2, 2, 2), nlev=3, *, seed=
                     pa.nface = _OPP[iface]
                     pa.n1a = pa.n2a = 1
                     pats.append(pa)
-            blk = block_from_metrics(m, pats)
+            blk = block_from_metrics(m, pats, nodes=(Xb, Yb, Zb) if device_setup and lev == 0 else None)
             init_freestream(blk, fs, noise=noise if lev == 0 else 0.0, seed=seed + 100 * bid)
             levels.append(blk)
         prm = make_params(fc, levels[0].dims, cfl=cfl, cfll=cfll, inter=inter)
         if turbulence == "sst":
             for lev, blk in enumerate(levels):
                 setup_sst(blk, prm if lev == 0 else FFParams.from_buffer_copy(prm), fs, tu=tu,
-                          mut_ratio=mut_ratio, wall_block=wall)
+                          mut_ratio=mut_ratio, wall_block=wall, distw=not device_setup)
         prms = [level_params(prm, lev + 1) for lev in range(nlev)]
         prms[0].lusgs_fp32 = int(lusgs_fp32)
         for q in prms[1:]:
@@ -579,11 +592,12 @@ def bump_multiblock_blocks(cells=(512, 256, 128), nb=(2, 2, 2), nlev=3, *, seed=
 
 def bump_multiblock_case(*args, **kw):
     """All blocks of bump_multiblock_blocks at once: (block_levels,
-    block_prms, fs)."""
+    block_prms, fs), and the wall triangles last with device_setup."""
     it = bump_multiblock_blocks(*args, **kw)
     _, fs = next(it)
+    tri = next(it)[1] if kw.get("device_setup") else None
     bl, bp = [], []
     for levels, prms in it:
         bl.append(levels)
         bp.append(prms)
-    return bl, bp, fs
+    return (bl, bp, fs, tri) if tri is not None else (bl, bp, fs)

@@ -63,6 +63,32 @@ def test_device_multigrid_metrics_match_host(gpu_lib):
     g.close()
 
 
+def test_device_setup_runs_like_host_setup(gpu_lib):
+    """The eight-block SST bump with two levels per block, set up on the
+    host and on the device: the same residual history over 10 multi-block
+    V-cycles (the two set-ups differ at rounding level in the metrics and by
+    the host search's 1e-11 in DISTW)."""
+    kw = dict(cells=(40, 16, 16), nb=(2, 2, 2), nlev=2, reynolds=1e6, mach=0.6, h1=1e-4, cfl=1.0, cfll=1.0,
+              lusgs_fp32=False, coarse_fp32=False, turbulence="sst")
+    hists = []
+    for dev in (False, True):
+        out = case.bump_multiblock_case(**kw, device_setup=dev)
+        bl, bp = out[0], out[1]
+        g = GpuSolver(0)
+        ids = g.add_multiblock(bl, bp)
+        for bid in range(len(g.blocks)):
+            g.upload(bid)
+        if dev:
+            for k, bid in enumerate(ids):
+                g.block_metrics_levels(bid, 2, *bl[k][0].nodes)
+                for q in range(2):
+                    g.wall_distance(bid + q, out[3])
+        g.start_all()
+        hists.append(g.cycles_all(10, icycle0=1, use_graph=True)[:, :5])
+        g.close()
+    np.testing.assert_allclose(hists[1], hists[0], rtol=1e-6)
+
+
 def _brute_force_distance(q, T):
     best = np.full(len(q), np.inf)
     for t in T:
