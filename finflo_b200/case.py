@@ -41,7 +41,7 @@ class FFParams(ctypes.Structure):
         "rklim", "epslim", "turlim", "csimps", "re")] + [
         (n, ctypes.c_int) for n in (
             "interi", "interj", "interk", "entropy_fix", "iturb", "fullns",
-            "idi1", "idi2", "idi3", "coarse_inter", "lusgs_fp32", "ddadi", "timel", "pad1")] + [
+            "idi1", "idi2", "idi3", "coarse_inter", "lusgs_fp32", "ddadi", "timel", "vanleer")] + [
         ("dt", ctypes.c_double)]
 
 

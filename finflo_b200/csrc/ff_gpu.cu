@@ -1319,6 +1319,8 @@ int ff_block_add(void* ctx, int imax, int jmax, int kmax, int npatch, const ff_p
                  const ff_params* prm) {
   Ctx* c = (Ctx*)ctx;
   if (!c || imax < 2 || jmax < 2 || kmax < 1 || npatch < 0 || !prm) return fail(c, FF_ERR_ARG, "ff_block_add: bad dims");
+  if (prm->vanleer && prm->iturb >= 3)   // FLUXVL has no k-omega form (res3c.f:7041)
+    return fail(c, FF_ERR_ARG, "ff_block_add: van Leer flux (IFLUX=0) is laminar only");
   BlockCtx* b = new BlockCtx();
   b->imax = imax; b->jmax = jmax; b->kmax = kmax;
   b->ntot = (imax + 4) * (jmax + 4) * (kmax + 4);
@@ -1374,6 +1376,8 @@ int ff_block_params(void* ctx, int blk, const ff_params* prm) {
   Ctx* c = (Ctx*)ctx;
   BlockCtx* b = getb(c, blk);
   if (!b || !prm) return fail(c, FF_ERR_ARG, "ff_block_params");
+  if (prm->vanleer && prm->iturb >= 3)   // FLUXVL has no k-omega form (res3c.f:7041)
+    return fail(c, FF_ERR_ARG, "ff_block_params: van Leer flux (IFLUX=0) is laminar only");
   bool nv_changed = (b->prm.iturb >= 3) != (prm->iturb >= 3);
   bool fp_changed = (b->prm.lusgs_fp32 != 0) != (prm->lusgs_fp32 != 0);
   if ((b->prm.ddadi != 0) != (prm->ddadi != 0)) b->tuned = 0;

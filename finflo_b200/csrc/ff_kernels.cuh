@@ -463,6 +463,64 @@ FF_DI void wall_flux(const DevBlock& b, const ff_params& p, size_t II, int S, in
 }
 
 // Flux of one face (dir, cell L on the high side, normal index m).
+// FLUXVL base3c.f:1733-1961 (IFLUX=0) at one face: van Leer flux-vector
+// splitting of the MUSCL-extrapolated conservative variables qc[v][m]
+// (v = RO, RM, RN, RW, E; cells I-2S..I+S), perfect gas, added to f.
+FF_DI void vl_flux(const double qc[5][4], double nx, double ny, double nz, double area, int intem,
+                   const ff_params& p, double f[5]) {
+  const double gamma = p.gamma, gm1 = gamma - 1., ygm = 1. / gamma;
+  double ip[5], im[5];
+#pragma unroll
+  for (int v = 0; v < 5; v++) xxtrap(qc[v][0], qc[v][1], qc[v][2], qc[v][3], intem, ip[v], im[v]);
+  double ppi = (gamma - 1.) * (ip[4] - .5 / ip[0] * (ip[1] * ip[1] + ip[2] * ip[2] + ip[3] * ip[3]));
+  double pmi = (gamma - 1.) * (im[4] - .5 / im[0] * (im[1] * im[1] + im[2] * im[2] + im[3] * im[3]));
+  ip[0] = dmax(0.001 * p.frsden, ip[0]);
+  ppi = dmax(0.001 * p.frspre, ppi);
+  im[0] = dmax(0.001 * p.frsden, im[0]);
+  pmi = dmax(0.001 * p.frspre, pmi);
+  double a21, a22, a23, a31, a32, a33;
+  surfvects(nx, ny, nz, a21, a22, a23, a31, a32, a33);
+  const double rip0 = nx * ip[1] + ny * ip[2] + nz * ip[3], rip1 = a21 * ip[1] + a22 * ip[2] + a23 * ip[3],
+               rip2 = a31 * ip[1] + a32 * ip[2] + a33 * ip[3];
+  const double rim0 = nx * im[1] + ny * im[2] + nz * im[3], rim1 = a21 * im[1] + a22 * im[2] + a23 * im[3],
+               rim2 = a31 * im[1] + a32 * im[2] + a33 * im[3];
+  double fm[5], fp[5];
+  {  // F- from the right state
+    const double ypro = 1. / ip[0], u = ypro * rip0, v = ypro * rip1, w = ypro * rip2;
+    const double pp = dmax(0.01, ppi), c = sqrt(gamma * pp * ypro), rma = u / c;
+    if (rma < -1.) {
+      fm[0] = area * rip0; fm[1] = area * (rip0 * u + pp); fm[2] = area * rip0 * v;
+      fm[3] = area * rip0 * w; fm[4] = area * u * (ip[4] + pp);
+    } else if (rma < 1.) {
+      const double h = .5 * (rma - 1.), f1 = -area * ip[0] * c * (h * h);
+      fm[0] = f1; fm[1] = f1 * (gm1 * u - 2. * c) * ygm; fm[2] = f1 * v; fm[3] = f1 * w;
+      fm[4] = f1 * (ip[4] + pp) * ypro;
+    } else {
+      fm[0] = fm[1] = fm[2] = fm[3] = fm[4] = 0.;
+    }
+  }
+  {  // F+ from the left state
+    const double ypro = 1. / im[0], u = ypro * rim0, v = ypro * rim1, w = ypro * rim2;
+    const double pm = dmax(0.01, pmi), c = sqrt(gamma * pm * ypro), rma = u / c;
+    if (rma > 1.) {
+      fp[0] = area * rim0; fp[1] = area * (rim0 * u + pm); fp[2] = area * rim0 * v;
+      fp[3] = area * rim0 * w; fp[4] = area * u * (im[4] + pm);
+    } else if (rma > -1.) {
+      const double h = .5 * (rma + 1.), f1 = +area * im[0] * c * (h * h);
+      fp[0] = f1; fp[1] = f1 * (gm1 * u + 2. * c) * ygm; fp[2] = f1 * v; fp[3] = f1 * w;
+      fp[4] = f1 * (im[4] + pm) * ypro;
+    } else {
+      fp[0] = fp[1] = fp[2] = fp[3] = fp[4] = 0.;
+    }
+  }
+  const double f2 = fp[1] + fm[1], f3 = fp[2] + fm[2], f4 = fp[3] + fm[3];
+  f[0] = fm[0] + fp[0] + f[0];
+  f[1] = nx * f2 + a21 * f3 + a31 * f4 + f[1];
+  f[2] = ny * f2 + a22 * f3 + a32 * f4 + f[2];
+  f[3] = nz * f2 + a23 * f3 + a33 * f4 + f[3];
+  f[4] = fm[4] + fp[4] + f[4];
+}
+
 FF_DI void face_flux(const DevBlock& b, const ff_params& p, int dir, size_t L, int m, int t1, int t2,
                      int level, double f[5]) {
   const int S = dir == 1 ? 1 : (dir == 2 ? b.is : b.il);
@@ -489,6 +547,19 @@ FF_DI void face_flux(const DevBlock& b, const ff_params& p, int dir, size_t L, i
   } else {
     f[0] = f[1] = f[2] = f[3] = f[4] = 0.;
   }
+  const int ao = 4 * (dir - 1);
+  if (p.vanleer) {   // IFLUX=0: FLUXVL on the conservative variables
+    double qc[5][4];
+    const int sc[5] = {FF_RO, FF_RM, FF_RN, FF_RW, FF_E};
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+      const double* a = b.a[sc[v]];
+      qc[v][0] = __ldg(a + L - 2 * S); qc[v][1] = __ldg(a + L - S); qc[v][2] = __ldg(a + L); qc[v][3] = __ldg(a + L + S);
+    }
+    vl_flux(qc, __ldg(b.a[FF_A1XA + ao] + L), __ldg(b.a[FF_A1YA + ao] + L), __ldg(b.a[FF_A1ZA + ao] + L),
+            __ldg(b.a[FF_A1 + ao] + L), intem, p, f);
+    return;
+  }
   double q[5][4];
   const int sl[5] = {FF_RO, FF_U, FF_V, FF_W, FF_P};
 #pragma unroll
@@ -499,7 +570,6 @@ FF_DI void face_flux(const DevBlock& b, const ff_params& p, int dir, size_t L, i
   size_t L2 = dir == 3 ? L : L - S;
   double cr[4] = {__ldg(b.a[FF_DRDP] + L), __ldg(b.a[FF_DRDH] + L), q[0][2], q[4][2]};
   double cl[4] = {__ldg(b.a[FF_DRDP] + L2), __ldg(b.a[FF_DRDH] + L2), __ldg(b.a[FF_RO] + L2), __ldg(b.a[FF_P] + L2)};
-  const int ao = 4 * (dir - 1);
   roe_flux(q, __ldg(b.a[FF_A1XA + ao] + L), __ldg(b.a[FF_A1YA + ao] + L), __ldg(b.a[FF_A1ZA + ao] + L),
            __ldg(b.a[FF_A1 + ao] + L), intem, p, __ldg(b.a[FF_C] + L), __ldg(b.a[FF_C] + L - S), cr, cl, f);
 }

@@ -68,7 +68,8 @@ typedef struct ff_params {
                                         /* 0: LU-SGS (LUSGS=1, imps3.f:378)    */
   int timel;                            /* 1: time-accurate dual time stepping */
                                         /* (TIMEL, level 1 of the block only)  */
-  int pad1;
+  int vanleer;                          /* 1: van Leer FVS (IFLUX=0, laminar), */
+                                        /* 0: Roe (IFLUX=1)                    */
   double dt;                            /* physical time step DT (TIMEL)       */
 } ff_params;
 

@@ -741,6 +741,66 @@ static void botske_face(const orc_block *b, const ff_params *p, size_t II, int S
 
 /* FLUCYC res3c.f:7572 for one direction: zero the face fluxes, inlet/outlet
  * ghosts (done by the caller), viscous flux, Roe flux, wall faces. */
+/* FLUXVL base3c.f:1733-1961 (IFLUX=0) for one face: van Leer flux-vector
+ * splitting of the MUSCL-extrapolated conservative variables (cells
+ * I-2S..I+S in qc[v][m], v = RO, RM, RN, RW, E), added to f (perfect gas). */
+static void vl_face(const double qc[5][4], const double *nrm, double area, int intem, const ff_params *p,
+                    double *f) {
+  const double gamma = p->gamma, gm1 = gamma - 1., ygm = 1. / gamma;
+  double ip[5], im[5];
+  for (int v = 0; v < 5; v++) xxtrap(qc[v][0], qc[v][1], qc[v][2], qc[v][3], intem, &ip[v], &im[v]);
+  double ppi = (gamma - 1.) * (ip[4] - .5 / ip[0] * (ip[1] * ip[1] + ip[2] * ip[2] + ip[3] * ip[3]));
+  double pmi = (gamma - 1.) * (im[4] - .5 / im[0] * (im[1] * im[1] + im[2] * im[2] + im[3] * im[3]));
+  ip[0] = MAXD(0.001 * p->frsden, ip[0]);
+  ppi = MAXD(0.001 * p->frspre, ppi);
+  im[0] = MAXD(0.001 * p->frsden, im[0]);
+  pmi = MAXD(0.001 * p->frspre, pmi);
+  const double a11 = nrm[0], a12 = nrm[1], a13 = nrm[2];
+  double a21, a22, a23, a31, a32, a33;
+  surfvects(a11, a12, a13, &a21, &a22, &a23, &a31, &a32, &a33);
+  double rip[3] = {a11 * ip[1] + a12 * ip[2] + a13 * ip[3], a21 * ip[1] + a22 * ip[2] + a23 * ip[3],
+                   a31 * ip[1] + a32 * ip[2] + a33 * ip[3]};
+  double rim[3] = {a11 * im[1] + a12 * im[2] + a13 * im[3], a21 * im[1] + a22 * im[2] + a23 * im[3],
+                   a31 * im[1] + a32 * im[2] + a33 * im[3]};
+  double fm[5], fp[5];
+  { /* F- from the right state (IP) */
+    double ypro = 1. / ip[0], u = ypro * rip[0], v = ypro * rip[1], w = ypro * rip[2];
+    double pp = MAXD(0.01, ppi), c = sqrt(gamma * pp * ypro), rma = u / c;
+    if (rma < -1.) {
+      fm[0] = area * rip[0]; fm[1] = area * (rip[0] * u + pp); fm[2] = area * rip[0] * v;
+      fm[3] = area * rip[0] * w; fm[4] = area * u * (ip[4] + pp);
+    } else if (rma < 1.) {
+      double h = .5 * (rma - 1.);
+      double f1 = -area * ip[0] * c * (h * h);
+      fm[0] = f1; fm[1] = f1 * (gm1 * u - 2. * c) * ygm; fm[2] = f1 * v; fm[3] = f1 * w;
+      fm[4] = f1 * (ip[4] + pp) * ypro;
+    } else {
+      fm[0] = fm[1] = fm[2] = fm[3] = fm[4] = 0.;
+    }
+  }
+  { /* F+ from the left state (IM) */
+    double ypro = 1. / im[0], u = ypro * rim[0], v = ypro * rim[1], w = ypro * rim[2];
+    double pm = MAXD(0.01, pmi), c = sqrt(gamma * pm * ypro), rma = u / c;
+    if (rma > 1.) {
+      fp[0] = area * rim[0]; fp[1] = area * (rim[0] * u + pm); fp[2] = area * rim[0] * v;
+      fp[3] = area * rim[0] * w; fp[4] = area * u * (im[4] + pm);
+    } else if (rma > -1.) {
+      double h = .5 * (rma + 1.);
+      double f1 = +area * im[0] * c * (h * h);
+      fp[0] = f1; fp[1] = f1 * (gm1 * u + 2. * c) * ygm; fp[2] = f1 * v; fp[3] = f1 * w;
+      fp[4] = f1 * (im[4] + pm) * ypro;
+    } else {
+      fp[0] = fp[1] = fp[2] = fp[3] = fp[4] = 0.;
+    }
+  }
+  double f2 = fp[1] + fm[1], f3 = fp[2] + fm[2], f4 = fp[3] + fm[3];
+  f[0] = fm[0] + fp[0] + f[0];
+  f[1] = a11 * f2 + a21 * f3 + a31 * f4 + f[1];
+  f[2] = a12 * f2 + a22 * f3 + a32 * f4 + f[2];
+  f[3] = a13 * f2 + a23 * f3 + a33 * f4 + f[3];
+  f[4] = fm[4] + fp[4] + f[4];
+}
+
 void orc_flux_dir(orc_block *b, const ff_params *p, int dir, int level) {
   dims_t d = dims_of(b);
   int S = dir == 1 ? 1 : (dir == 2 ? d.is : d.il);
@@ -775,7 +835,17 @@ void orc_flux_dir(orc_block *b, const ff_params *p, int dir, int level) {
         double cr[5] = {C[L], DRDP[L], DRDH[L], RO[L], P[L]};
         size_t L2 = dir == 3 ? L : L - S;      /* DERIV I2 = I-IL, or I itself */
         double cl[5] = {C[L2], DRDP[L2], DRDH[L2], RO[L2], P[L2]};
-        roe_face_core(q, nrm, A[L], intem, p, C[L], C[L - S], cr, cl, f);
+        if (p->vanleer) {   /* IFLUX=0: FLUXVL on the conservative variables */
+          const double *cons[5] = {RO, b->a[FF_RM], b->a[FF_RN], b->a[FF_RW], b->a[FF_E]};
+          double qc[5][4];
+          for (int v = 0; v < 5; v++) {
+            qc[v][0] = cons[v][L - 2 * S]; qc[v][1] = cons[v][L - S];
+            qc[v][2] = cons[v][L]; qc[v][3] = cons[v][L + S];
+          }
+          vl_face(qc, nrm, A[L], intem, p, f);
+        } else {
+          roe_face_core(q, nrm, A[L], intem, p, C[L], C[L - S], cr, cl, f);
+        }
         for (int v = 0; v < 5; v++) F[v][L] = f[v];
       }
   /* wall faces: BOTSKE overwrites (res3c.f:8092, only where IDIM > KBOT) */
