@@ -10,6 +10,17 @@ length as a 4-byte integer before and after it.
 Reading a coarser multigrid level takes every 2^(LEVEL-1)-th node per
 direction, except in a direction three nodes long (k: three or fewer),
 which keeps every node (GRIMP messp.f:1091-1096).
+
+The restart file RSTART (WRITRS outp3.f:2042, READRS outp3.f:1119) is
+unformatted sequential too: a record with the flags TIMEL, COORL, CHIMEL
+(4-byte Fortran logicals), then per block one record per variable over all
+NNMAX = (IMAX+4)(JMAX+4)(KMAX+4) cells, ghost cells included.  The state is
+stored as U, V, W, temperature and PDIFF = P - FRSPRE (no conservative
+variables); the start-up after READRS rebuilds P (ns3c.f:341) and STATIM
+the rest.  This module writes and reads the records of the variants this
+path runs: no scalars (NSCAL=0), no transition or multiphase variables, no
+Reynolds stresses, IPRESC=0 without FRESUL, and neither deforming nor
+chimera grids.
 """
 from __future__ import annotations
 
@@ -75,3 +86,80 @@ def read_grid(path, level=1):
             XYZ = [a[c * ngrid:(c + 1) * ngrid].reshape(iz, iy, ix)[::sk, ::sj, ::si].copy() for c in range(3)]
             blocks.append(tuple(XYZ))
         return blocks
+
+
+# WRITRS outp3.f:2095-2115: the per-block records, in file order.  With
+# IPRESC=0 and no FRESUL the three PRC records repeat DDEPS, PDIFF and TEMP.
+RESTART_FIELDS = ("U", "V", "W", "EPS2", "VIST", "OHMI", "RK", "REPS", "PTUR",
+                  "DDEPS", "PDIFF", "TEMP", "DDEPS", "PDIFF", "TEMP")
+# WRITRS outp3.f:2299-2341 (TIMEL): the previous time level, then the running
+# time averages (first and second moments).
+RESTART_TIME_FIELDS = ("ROLE2", "RMLE2", "RNLE2", "RWLE2", "RKLE2", "EPSLE2", "ELE2",
+                       "ROAV1", "RMAV1", "RNAV1", "RWAV1", "RKAV1", "EPSAV1", "EAV1",
+                       "ROAV2", "RMAV2", "RNAV2", "RWAV2", "PAV1", "TAV1", "EAV2",
+                       "RUVAV", "RUWAV", "RVWAV")
+
+
+def write_restart(path, blocks, *, timel=False):
+    """Write RSTART.  blocks: list of dicts, variable name -> the block's
+    NNMAX values; a variable the dict lacks (DDEPS, the time averages) is
+    written as zeros, as a block that never accumulated it holds."""
+    with open(path, "wb") as f:
+        _write_record(f, struct.pack("<3i", int(bool(timel)), 0, 0))
+        sizes = [_block_size(d) for d in blocks]
+        for names in (RESTART_FIELDS,) + ((RESTART_TIME_FIELDS,) if timel else ()):
+            for d, n in zip(blocks, sizes):
+                for name in names:
+                    a = d.get(name)
+                    a = np.zeros(n) if a is None else np.asarray(a, dtype="<f8").ravel()
+                    if a.size != n:
+                        raise ValueError(f"restart: {name} has {a.size} values, expected {n}")
+                    _write_record(f, a.tobytes())
+
+
+def _block_size(d):
+    for a in d.values():
+        return np.asarray(a).size
+    raise ValueError("restart: a block without variables")
+
+
+def read_restart(path, sizes, *, timel=False):
+    """Read RSTART.  sizes: NNMAX of each block (the file holds no
+    dimensions; READRS takes them from the grid).  Returns (time_level,
+    blocks): the file's TIMEL flag and per block a dict of its variables.
+    The time-level records are read only when both the file and `timel`
+    have them (READRS outp3.f:1483, IF(TIMEL .AND. TIME2))."""
+    with open(path, "rb") as f:
+        flags = _read_record(f)
+        if len(flags) != 12:
+            raise ValueError("restart: the first record is not TIMEL, COORL, CHIMEL")
+        time2, coor2, chime2 = struct.unpack("<3i", flags)
+        if coor2 or chime2:
+            raise ValueError("restart: deforming-grid and chimera restarts are not read")
+        out = [dict() for _ in sizes]
+        groups = (RESTART_FIELDS,) + ((RESTART_TIME_FIELDS,) if (timel and time2) else ())
+        for names in groups:
+            for d, n in zip(out, sizes):
+                for name in names:
+                    a = np.frombuffer(_read_record(f), dtype="<f8")
+                    if a.size != n:
+                        raise ValueError(f"restart: {name} has {a.size} values, expected {n}")
+                    d[name] = a.copy()
+        return bool(time2), out
+
+
+def block_restart_vars(blk, *, timel=False):
+    """The restart variables a block holds (views of its arrays)."""
+    names = RESTART_FIELDS + (RESTART_TIME_FIELDS if timel else ())
+    return {n: blk.arrays[n] for n in dict.fromkeys(names) if n in blk.arrays}
+
+
+def load_restart_vars(blk, d):
+    """Copy a block's restart variables into its arrays.  The conservative
+    state follows from them at start-up: BOUNDI's STATIM rebuilds RO, RM,
+    RN, RW and E from U, V, W, TEMP and PDIFF."""
+    for n, a in d.items():
+        if n in blk.arrays:
+            if a.size != blk.arrays[n].size:
+                raise ValueError(f"restart: {n} has {a.size} values, the block {blk.arrays[n].size}")
+            blk.arrays[n][:] = a.reshape(blk.arrays[n].shape)

@@ -1,9 +1,12 @@
-"""FINFLO's unformatted multi-block grid file (finflo_b200/fileio.py)."""
+"""FINFLO's unformatted multi-block grid file and restart file RSTART
+(finflo_b200/fileio.py)."""
 import struct
 
 import numpy as np
+import pytest
 
 from finflo_b200 import case, fileio, grid
+from oracle.oracle import Oracle
 
 
 def _blocks():
@@ -52,3 +55,73 @@ def test_block_from_a_grid_file_has_the_same_metrics(tmp_path):
     b = case.new_block(Xr, Yr, Zr, case.channel_patches(16, 8, 8, fs))
     for n in grid.METRIC_NAMES:
         np.testing.assert_array_equal(a.arrays[n], b.arrays[n])
+
+
+def test_restart_record_layout(tmp_path):
+    """RSTART: the flags record (three 4-byte logicals), then per block the
+    fifteen NNMAX records of WRITRS in order, DDEPS written as zeros."""
+    blk, prm, fs = case.bump_case(9, 7, 5)
+    path = tmp_path / "RSTART"
+    fileio.write_restart(path, [fileio.block_restart_vars(blk)])
+    raw = path.read_bytes()
+    assert struct.unpack("<5i", raw[:20]) == (12, 0, 0, 0, 12)
+    n = blk.ntot
+    rec = 8 * n + 8
+    assert len(raw) == 20 + 15 * rec
+    for k, name in enumerate(fileio.RESTART_FIELDS):
+        off = 20 + k * rec
+        assert struct.unpack("<i", raw[off:off + 4]) == (8 * n,)
+        a = np.frombuffer(raw[off + 4:off + 4 + 8 * n], dtype="<f8")
+        want = blk.arrays[name].ravel() if name in blk.arrays else np.zeros(n)
+        np.testing.assert_array_equal(a, want)
+
+
+def test_restart_round_trip_timel(tmp_path):
+    """Two blocks with the time-level records; a reader without TIMEL stops
+    after the main records, as READRS does."""
+    blocks = []
+    for dims in ((9, 7, 5), (5, 5, 3)):
+        blk, prm, fs = case.bump_case(*dims, turbulence="sst", reynolds=1e6)
+        rng = np.random.default_rng(dims[0])
+        for n in ("ROLE2", "RMLE2", "ELE2"):
+            blk.arrays[n][:] = rng.standard_normal(blk.ntot)
+        blocks.append(blk)
+    path = tmp_path / "RSTART"
+    fileio.write_restart(path, [fileio.block_restart_vars(b, timel=True) for b in blocks], timel=True)
+    time2, got = fileio.read_restart(path, [b.ntot for b in blocks], timel=True)
+    assert time2
+    for b, d in zip(blocks, got):
+        for n in ("U", "TEMP", "PDIFF", "RK", "REPS", "VIST", "ROLE2", "RMLE2", "ELE2"):
+            np.testing.assert_array_equal(d[n], b.arrays[n].ravel())
+        assert not d["DDEPS"].any() and not d["RVWAV"].any()
+    time2, got = fileio.read_restart(path, [b.ntot for b in blocks])
+    assert time2 and "ROLE2" not in got[0]
+    with pytest.raises(ValueError):
+        fileio.read_restart(path, [blocks[0].ntot + 1, blocks[1].ntot])
+
+
+@pytest.mark.parametrize("sst", [False, True])
+def test_restart_continues_the_run(tmp_path, sst):
+    """Ten cycles, RSTART, a fresh case read from it and started as usual,
+    five more cycles: the residual history equals fifteen cycles in one run
+    (every cycle starts with STATIM, which rebuilds the conservative state
+    from the primitive variables the file holds)."""
+    kw = dict(turbulence="sst", reynolds=1e6, mach=0.6, h1=1e-4) if sst else {}
+    blk, prm, fs = case.bump_case(17, 9, 9, **kw)
+    o = Oracle(blk, prm)
+    o.start()
+    full = [o.cycle(i + 1)[0] for i in range(15)]
+    blk, prm, fs = case.bump_case(17, 9, 9, **kw)
+    o = Oracle(blk, prm)
+    o.start()
+    for i in range(10):
+        o.cycle(i + 1)
+    path = tmp_path / "RSTART"
+    fileio.write_restart(path, [fileio.block_restart_vars(blk)])
+    blk2, prm2, fs2 = case.bump_case(17, 9, 9, **kw)
+    _, got = fileio.read_restart(path, [blk2.ntot])
+    fileio.load_restart_vars(blk2, got[0])
+    o2 = Oracle(blk2, prm2)
+    o2.start()
+    rest = [o2.cycle(i + 11)[0] for i in range(5)]
+    np.testing.assert_allclose(np.array(rest), np.array(full[10:]), rtol=1e-9)
