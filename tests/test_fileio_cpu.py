@@ -125,3 +125,14 @@ def test_restart_continues_the_run(tmp_path, sst):
     o2.start()
     rest = [o2.cycle(i + 11)[0] for i in range(5)]
     np.testing.assert_allclose(np.array(rest), np.array(full[10:]), rtol=1e-9)
+
+
+@pytest.mark.parametrize("flags", [(0, 1, 0), (0, 0, 1)])
+def test_restart_rejects_deforming_and_chimera_files(tmp_path, flags):
+    """A file whose COORL or CHIMEL flag is set holds records this path does
+    not read; the reader refuses it instead of misreading what follows."""
+    path = tmp_path / "RSTART"
+    with open(path, "wb") as f:
+        fileio._write_record(f, struct.pack("<3i", *flags))
+    with pytest.raises(ValueError, match="chimera"):
+        fileio.read_restart(path, [10])
