@@ -42,7 +42,7 @@ class FFParams(ctypes.Structure):
         (n, ctypes.c_int) for n in (
             "interi", "interj", "interk", "entropy_fix", "iturb", "fullns",
             "idi1", "idi2", "idi3", "coarse_inter", "lusgs_fp32", "ddadi", "timel", "vanleer")] + [
-        ("dt", ctypes.c_double)]
+        ("dt", ctypes.c_double), ("predgs_full", ctypes.c_int), ("pad_", ctypes.c_int)]
 
 
 class FFHaloItem(ctypes.Structure):
@@ -287,9 +287,15 @@ def wall_distance(blk: Block, wall_block: Block = None, nnear: int = 8):
     coarse multigrid levels pass the finest level, whose nodes they lack),
     each wall face split into two triangles -- set-up data, like the
     reference's DISTANCES pass before the iteration loop."""
-    from scipy.spatial import cKDTree
     wb = wall_block if wall_block is not None else blk
-    T = wall_triangles(wb)
+    return wall_distance_tri(blk, wall_triangles(wb), nnear)
+
+
+def wall_distance_tri(blk: Block, T: np.ndarray, nnear: int = 8):
+    """DISTW of every cell centre of blk to the nearest of the wall triangles
+    T ([ntri, 9]: three corners each), searching the nnear triangles with
+    the nearest centroids (1e3 without triangles)."""
+    from scipy.spatial import cKDTree
     if not len(T):
         return np.full(blk.ntot, 1.0e3)
     A, B, C = T[:, 0:3], T[:, 3:6], T[:, 6:9]

@@ -778,6 +778,8 @@ int tune_sweep(Ctx* c, BlockCtx* b) {
 }
 
 int sweep(Ctx* c, BlockCtx* b, int upper, bool fp32) {
+  // bit 2 of the lower (PREDGS) sweep's flag keeps the row-JMAX i+1 coupling
+  if (upper && b->prm.predgs_full) upper |= 2;
   if (b->use_pipe) return pipe_sweep(c, b, upper, fp32);
   return b->use_lines ? lines_sweep(c, b, upper, fp32) : coop_sweep(c, b, upper, fp32);
 }
@@ -1476,8 +1478,67 @@ int ff_boundi(void* ctx, int blk) {
 int ff_residu(void* ctx, int blk, int level, int icycle) {
   Ctx* c = (Ctx*)ctx;
   BlockCtx* b = getb(c, blk);
-  if (!b || level != 1) return fail(c, FF_ERR_ARG, "ff_residu (level 1 only)");
-  st_residu(c, b, level, icycle);
+  if (!b || level != b->level) return fail(c, FF_ERR_ARG, "ff_residu: level is not the block's multigrid level");
+  st_residu(c, b, level, icycle, level);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int ff_residi(void* ctx, int blk, int m2, int icycle) {
+  Ctx* c = (Ctx*)ctx;
+  BlockCtx* b = getb(c, blk);
+  if (!b || m2 < b->level || m2 > b->level + 1) return fail(c, FF_ERR_ARG, "ff_residi: M2 must be M or M+1");
+  st_residu(c, b, b->level, icycle, m2);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int ff_transf(void* ctx, int fine, int coarse) {
+  Ctx* c = (Ctx*)ctx;
+  BlockCtx *f = getb(c, fine), *cc = getb(c, coarse);
+  if (!f || !cc || f->coarse != cc) return fail(c, FF_ERR_ARG, "ff_transf: blocks are not linked levels");
+  const int sst = f->prm.iturb >= 3;
+  long nc = (long)(cc->imax + 2) * (cc->jmax + 2) * (cc->kmax + 2);
+  k_transf<<<nblk(nc, 128), 128, 0, c->stream>>>(f->db, cc->db, sst);
+  k_transf_ring<<<nblk(cc->ntot, 256), 256, 0, c->stream>>>(cc->db, sst);
+  c->nlaunch += 2;
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int ff_forcfu(void* ctx, int blk) {
+  Ctx* c = (Ctx*)ctx;
+  BlockCtx* b = getb(c, blk);
+  if (!b) return fail(c, FF_ERR_ARG, "ff_forcfu");
+  k_forcing<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db, 0, b->prm.iturb >= 3);
+  c->nlaunch++;
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int ff_addres(void* ctx, int blk) {
+  Ctx* c = (Ctx*)ctx;
+  BlockCtx* b = getb(c, blk);
+  if (!b) return fail(c, FF_ERR_ARG, "ff_addres");
+  k_forcing<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db, 1, b->prm.iturb >= 3);
+  c->nlaunch++;
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int ff_interp(void* ctx, int coarse, int fine) {
+  Ctx* c = (Ctx*)ctx;
+  BlockCtx *f = getb(c, fine), *cc = getb(c, coarse);
+  if (!f || !cc || f->coarse != cc) return fail(c, FF_ERR_ARG, "ff_interp: blocks are not linked levels");
+  int nf = f->imax * f->jmax * f->kmax;
+  k_interp<<<nblk(nf, 256), 256, 0, c->stream>>>(cc->db, f->db);
+  c->nlaunch++;
+  if (f->prm.iturb >= 3) {
+    k_intert<<<nblk(nf, 256), 256, 0, c->stream>>>(cc->db, f->db, f->prm);
+    c->nlaunch++;
+  }
+  k_fin_coarse<<<nblk(f->ntot, 256), 256, 0, c->stream>>>(f->db, f->prm, 0);
+  c->nlaunch++;
   CK(cudaGetLastError());
   return 0;
 }
@@ -1638,7 +1699,7 @@ int ff_time_levels(void* ctx, int blk, int mode) {
 int ff_imps(void* ctx, int blk, int level) {
   Ctx* c = (Ctx*)ctx;
   BlockCtx* b = getb(c, blk);
-  if (!b || level != 1) return fail(c, FF_ERR_ARG, "ff_imps (level 1 only)");
+  if (!b || level != b->level) return fail(c, FF_ERR_ARG, "ff_imps: level is not the block's multigrid level");
   int rc = st_imps(c, b, level, true);
   if (rc) return rc;
   CK(cudaGetLastError());
@@ -1651,6 +1712,13 @@ int ff_fin(void* ctx, int blk, double* dromax) {
   if (!b) return fail(c, FF_ERR_ARG, "ff_fin");
   k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi, c->d_dromax);
   c->nlaunch++;
+  if (b->level > 1) {   // coarse level: FIN with the coarse limits (ns3c.f:1935-1990)
+    k_fin_coarse<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db, b->prm, 1);
+    c->nlaunch++;
+    if (dromax) *dromax = 0.0;
+    CK(cudaGetLastError());
+    return 0;
+  }
   st_fin(c, b, 0);
   if (dromax) {
     unsigned long long bits;
@@ -1940,3 +2008,5 @@ int ff_time_stage(void* ctx, int blk, int stage, int reps, float* ms) {
 
 // The allocation-free implicit stage shares this translation unit's kernels.
 #include "ff_noalloc.cu"
+// The Fortran call-site wrappers (statim_, residi_, impsdi_, fin_, boundi_).
+#include "ff_fortran.cu"

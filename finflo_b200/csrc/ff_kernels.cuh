@@ -891,8 +891,9 @@ __global__ void k_lusgs_sweep_basic(DevBlock b, const CT* __restrict__ coef, CT*
 #pragma unroll
       for (int v = 0; v < NV; v++) { ck[v] = 0; yd[v] = 0; bd[v] = 0; }
       const int st[3] = {1, IS, IL};
-      // PREDGS drops the i+1 coupling of row J = JMAX; PRKEGS does not
-      const bool has[3] = {upper ? (I < IMAX && (NV == 7 || J < JMAX)) : (I > 1), upper ? (J < JMAX) : (J > 1),
+      // PREDGS drops the i+1 coupling of row J = JMAX unless bit 2 of upper
+      // (predgs_full) asks for it; PRKEGS does not drop it
+      const bool has[3] = {upper ? (I < IMAX && (NV == 7 || J < JMAX || (upper & 2))) : (I > 1), upper ? (J < JMAX) : (J > 1),
                            upper ? (K < KMAX) : (K > 1)};
 #pragma unroll
       for (int d = 2; d >= 0; d--) {
@@ -952,8 +953,9 @@ __global__ void k_lusgs_sweep(DevBlock b, const CT* __restrict__ sw, CT* dwp, in
       const int K = klo + q / JMAX, J = q % JMAX + 1, I = m - J - K;
       if (I < 1 || I > IMAX) continue;
       const size_t S = ((size_t)(K - 1) * W + (m - K - 2)) * JMAX + (J - 1);
-      // PREDGS drops the i+1 coupling of row J = JMAX; PRKEGS does not
-      const bool has[3] = {upper ? (I < IMAX && (NV == 7 || J < JMAX)) : (I > 1), upper ? (J < JMAX) : (J > 1),
+      // PREDGS drops the i+1 coupling of row J = JMAX unless bit 2 of upper
+      // (predgs_full) asks for it; PRKEGS does not drop it
+      const bool has[3] = {upper ? (I < IMAX && (NV == 7 || J < JMAX || (upper & 2))) : (I > 1), upper ? (J < JMAX) : (J > 1),
                            upper ? (K < KMAX) : (K > 1)};
       CT ck[NV], yd[NV], bd[NV];
 #pragma unroll
@@ -1520,8 +1522,9 @@ __global__ void __launch_bounds__(LTHREADS * (STAGE ? LMAX_TPC_STAGE : LMAX_TPC)
         if (STAGE) return my[c * nthr];
         return c < SW_N ? __ldg(sw + c * ns + S) : dwp[(c - SW_N) * ns + S];
       };
-      // PREDGS drops the i+1 coupling of row J = JMAX; PRKEGS does not
-      const bool hy = upper ? (I < IMAX && (NV == 7 || J < JMAX)) : (I > 1);
+      // PREDGS drops the i+1 coupling of row J = JMAX unless bit 2 of upper
+      // (predgs_full) asks for it; PRKEGS does not drop it
+      const bool hy = upper ? (I < IMAX && (NV == 7 || J < JMAX || (upper & 2))) : (I > 1);
       // ---- consume: neighbour contributions of the previous plane ----
       CT yd[NV], bd[NV], ck[NV];
 #pragma unroll

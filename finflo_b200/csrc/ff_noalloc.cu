@@ -24,7 +24,9 @@
 #define FF_NOALLOC_BAR_WORDS 64   // doubles reserved for the barrier words
 
 // Scratch: NCOEF coefficient arrays of FF_NOALLOC_MAX_NTOT doubles, then the
-// barrier words {count, generation, error}.  In host code the name below is
+// barrier words {count, generation, error, sticky error}.  The sticky word
+// collects the time-outs of every call since the caller last asked for the
+// status (level = 0).  In host code the name below is
 // only a host-side stand-in for the array; its device address comes from
 // cudaGetSymbolAddress in noalloc_setup().
 static __device__ __align__(256) double ff_noalloc_scratch[ff::NCOEF * (size_t)FF_NOALLOC_MAX_NTOT + FF_NOALLOC_BAR_WORDS];
@@ -59,13 +61,45 @@ int noalloc_setup(int dev) {
   return 0;
 }
 
+// Start of a call, in stream order: fold the previous call's time-out flag
+// into the sticky word, then clear the barrier words for this call's sweeps.
+__global__ void k_noalloc_begin(unsigned* bar) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    bar[3] |= bar[2];
+    bar[0] = 0u;
+    bar[1] = 0u;
+    bar[2] = 0u;
+  }
+}
+
+// level = 0: wait for `stream`, then report and clear the time-out flags of
+// the calls queued on it so far.
+int noalloc_status(cudaStream_t st) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return FF_ERR_CUDA;
+  int rc = noalloc_setup(dev);
+  if (rc) return rc;
+  unsigned* bar = (unsigned*)(g_noalloc[dev].scratch + ff::NCOEF * (size_t)FF_NOALLOC_MAX_NTOT);
+  unsigned w[2] = {0u, 0u};
+  if (cudaMemcpyAsync(w, bar + 2, sizeof(w), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return FF_ERR_CUDA;
+  if (!(w[0] | w[1])) return 0;
+  if (cudaMemsetAsync(bar + 2, 0, sizeof(w), st) != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess)
+    return FF_ERR_CUDA;
+  return FF_ERR_TIMEOUT;
+}
+
 }  // namespace
 
 extern "C" int ff_imps_noalloc(int imax, int jmax, int kmax, const ff_params* prm,
                                double* const* slots, int level, void* stream) {
+  if (level == 0) return noalloc_status((cudaStream_t)stream);
   if (imax < 2 || jmax < 2 || kmax < 1 || !prm || !slots || (level != 1 && level != 2 && level != 3))
     return FF_ERR_ARG;
   if (prm->iturb >= 3) return FF_ERR_ARG;   // five-equation (laminar) implicit stage only
+  // the LU-SGS sweeps here run in FP64 only; the DDADI branch honours FP32
+  if (prm->lusgs_fp32 && !prm->ddadi) return FF_ERR_ARG;
   long ntot = (long)(imax + 4) * (jmax + 4) * (kmax + 4);
   if (ntot > FF_NOALLOC_MAX_NTOT) return FF_ERR_SIZE;
   static const int needed[] = {FF_RO, FF_E, FF_P, FF_U, FF_V, FF_W, FF_C, FF_VIS, FF_CP, FF_DRDP, FF_DRDH,
@@ -94,8 +128,9 @@ extern "C" int ff_imps_noalloc(int imax, int jmax, int kmax, const ff_params* pr
   double* coef = nd.scratch;
   unsigned* bar = (unsigned*)(nd.scratch + ff::NCOEF * (size_t)FF_NOALLOC_MAX_NTOT);
   int* err = (int*)(bar + 2);
-  // every call shares the array: the barrier words must start at zero
-  if (cudaMemsetAsync(bar, 0, 4 * sizeof(unsigned), st) != cudaSuccess) return FF_ERR_CUDA;
+  // every call shares the array: the barrier words must start at zero, and
+  // an earlier call's time-out moves to the sticky word
+  k_noalloc_begin<<<1, 32, 0, st>>>(bar);
 
   int ncell = imax * jmax * kmax;
   ff_params p = *prm;
@@ -127,7 +162,8 @@ extern "C" int ff_imps_noalloc(int imax, int jmax, int kmax, const ff_params* pr
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (cudaLaunchKernelEx(&cfg, k_lusgs_sweep_basic<double, 5>, db, (const double*)coef, dw, upper, bar, err) != cudaSuccess)
+    const int uflag = upper && p.predgs_full ? (upper | 2) : upper;
+    if (cudaLaunchKernelEx(&cfg, k_lusgs_sweep_basic<double, 5>, db, (const double*)coef, dw, uflag, bar, err) != cudaSuccess)
       return FF_ERR_CUDA;
   }
   k_fin_divide<<<(int)((ntot + 255) / 256), 256, 0, st>>>(db, 0);

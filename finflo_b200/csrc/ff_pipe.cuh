@@ -158,8 +158,9 @@ __global__ void __launch_bounds__(PTJ* TK) k_lusgs_pipe(DevBlock b, const CT* __
         if (STAGE) return my[c * NT];
         return c < SW_N ? __ldg(sw + c * ns + S) : dwp[(c - SW_N) * ns + S];
       };
-      // PREDGS drops the i+1 coupling of row J = JMAX; PRKEGS does not
-      const bool hy = upper ? (I < IMAX && (NV == 7 || J < JMAX)) : (I > 1);
+      // PREDGS drops the i+1 coupling of row J = JMAX unless bit 2 of upper
+      // (predgs_full) asks for it; PRKEGS does not drop it
+      const bool hy = upper ? (I < IMAX && (NV == 7 || J < JMAX || (upper & 2))) : (I > 1);
       CT bd[NV], ck[NV];
 #pragma unroll
       for (int v = 0; v < NV; v++) {

@@ -36,17 +36,22 @@ def _write_record(f, payload: bytes):
     f.write(n)
 
 
-def _read_record(f) -> bytes:
+def _read_record(f, label="grid file") -> bytes:
+    """One unformatted sequential record; `label` names the file kind in the
+    error messages (grid file, RSTART)."""
     head = f.read(4)
     if len(head) < 4:
-        raise EOFError("grid file: unexpected end")
+        raise EOFError(f"{label}: unexpected end")
     (n,) = struct.unpack("<i", head)
     if n < 0:
-        raise ValueError("grid file: record of more than 2 GiB (subrecords are not read)")
+        raise ValueError(f"{label}: record of more than 2 GiB (subrecords are not read)")
     payload = f.read(n)
-    (m,) = struct.unpack("<i", f.read(4))
-    if m != n or len(payload) != n:
-        raise ValueError("grid file: record markers do not match")
+    tail = f.read(4)
+    if len(payload) != n or len(tail) < 4:
+        raise EOFError(f"{label}: unexpected end inside a record")
+    (m,) = struct.unpack("<i", tail)
+    if m != n:
+        raise ValueError(f"{label}: record markers do not match")
     return payload
 
 
@@ -130,7 +135,7 @@ def read_restart(path, sizes, *, timel=False):
     The time-level records are read only when both the file and `timel`
     have them (READRS outp3.f:1483, IF(TIMEL .AND. TIME2))."""
     with open(path, "rb") as f:
-        flags = _read_record(f)
+        flags = _read_record(f, "restart")
         if len(flags) != 12:
             raise ValueError("restart: the first record is not TIMEL, COORL, CHIMEL")
         time2, coor2, chime2 = struct.unpack("<3i", flags)
@@ -141,7 +146,7 @@ def read_restart(path, sizes, *, timel=False):
         for names in groups:
             for d, n in zip(out, sizes):
                 for name in names:
-                    a = np.frombuffer(_read_record(f), dtype="<f8")
+                    a = np.frombuffer(_read_record(f, "restart"), dtype="<f8")
                     if a.size != n:
                         raise ValueError(f"restart: {name} has {a.size} values, expected {n}")
                     d[name] = a.copy()

@@ -22,7 +22,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libfinflo_gpu.so")
 _SRC = [os.path.join(_HERE, "csrc", f) for f in ("ff_gpu.cu", "ff_kernels.cuh", "ff_device.cuh",
                                                  "ff_noalloc.cu", "ff_sst.cuh", "ff_pipe.cuh",
-                                                 "ff_ddadi.cuh", "ff_grid.cuh")]
+                                                 "ff_ddadi.cuh", "ff_grid.cuh", "ff_fortran.cu")]
 NVCC_FLAGS = ["-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC", "-shared", "-std=c++17"]
 
@@ -97,6 +97,15 @@ def lib():
         L.ff_host_register.argtypes = [vp, vp, ctypes.c_size_t]
         L.ff_host_unregister.argtypes = [vp, vp]
         L.ff_imps_noalloc.argtypes = [ci, ci, ci, ctypes.POINTER(FFParams), ctypes.POINTER(vp), ci, vp]
+        L.ff_residi.argtypes = [vp, ci, ci, ci]
+        L.ff_transf.argtypes = [vp, ci, ci]
+        L.ff_forcfu.argtypes = [vp, ci]
+        L.ff_addres.argtypes = [vp, ci]
+        L.ff_interp.argtypes = [vp, ci, ci]
+        L.ff_fortran_bind.argtypes = [vp]
+        L.ff_fortran_block.argtypes = [ci, ci, ci, ci]
+        L.ff_fortran_cycle.argtypes = [ci]
+        L.ff_fortran_ierr.argtypes = []
         _LIB = L
     return _LIB
 
@@ -154,10 +163,13 @@ class GpuSolver:
     def set_params(self, bid: int, prm: FFParams):
         self._check(self.L.ff_block_params(self.ctx, bid, ctypes.byref(prm)))
 
-    def upload(self, bid: int, names=None):
+    def upload(self, bid: int, names=None, src=None):
+        """Host -> device copies of the named slots, from the block's own
+        arrays or from the dict `src`."""
         blk = self.blocks[bid][0]
         for n in names or SLOTS:
-            self._check(self.L.ff_upload(self.ctx, bid, SLOT[n], _dptr(blk.arrays[n])))
+            a = src[n] if src is not None else blk.arrays[n]
+            self._check(self.L.ff_upload(self.ctx, bid, SLOT[n], _dptr(a)))
         self.sync()
 
     def pin(self, arrays):
@@ -201,6 +213,22 @@ class GpuSolver:
         r = (ctypes.c_double * 5)()
         self._check(self.L.ff_resl2(self.ctx, bid, r))
         return np.array(r[:])
+
+    def residi(self, bid, m2, icycle=1):
+        """RESIDI(M, N, M2) on the block's own multigrid level."""
+        self._check(self.L.ff_residi(self.ctx, bid, m2, icycle))
+
+    def transf(self, fine, coarse):
+        self._check(self.L.ff_transf(self.ctx, fine, coarse))
+
+    def forcfu(self, bid):
+        self._check(self.L.ff_forcfu(self.ctx, bid))
+
+    def addres(self, bid):
+        self._check(self.L.ff_addres(self.ctx, bid))
+
+    def interp(self, coarse, fine):
+        self._check(self.L.ff_interp(self.ctx, coarse, fine))
 
     def imps(self, bid=0, level=1):
         self._check(self.L.ff_imps(self.ctx, bid, level))

@@ -19,6 +19,13 @@
  *   ff_fin       FIN     res3c.f:1077 + the limits of CYCLES ns3c.f:1553-1596
  *   ff_boundi    BOUNDI  ns3c.f:10608 (REFCOR, MIR, STATIM; single block)
  *   ff_cycles    CYCLES  ns3c.f:1354 + BOUNDI + SUBIN per cycle, graph-replayed
+ *   ff_residi    RESIDI  ns3c.f:2355 on any multigrid level (M2 as passed)
+ *   ff_transf    TRANSF  multi.f:156 (+ TRANKE multi.f:434 for k-omega)
+ *   ff_forcfu    FORCFU  multi.f:1609    ff_addres  ADDRES multi.f:1686
+ *   ff_interp    INTERP  multi.f:1763 (+ INTERT multi.f:2051) and the limits
+ *                after it (ns3c.f:2059-2125)
+ * and, for a Fortran host, the call-site wrappers statim_, residi_, impsdi_,
+ * fin_ and boundi_ (gfortran names; declared at the end of this header).
  */
 #ifndef FINFLO_GPU_H
 #define FINFLO_GPU_H
@@ -28,7 +35,7 @@
 extern "C" {
 #endif
 
-#define FF_ABI_VERSION 3   /* 3: ff_params gains ddadi, timel, dt; slots FF_ROLE2..FF_EPSLE3 */
+#define FF_ABI_VERSION 4   /* 4: ff_params gains predgs_full (3: ddadi, timel, dt; slots FF_ROLE2..FF_EPSLE3) */
 
 enum { FF_OK = 0, FF_ERR_CUDA = 1, FF_ERR_ARG = 2, FF_ERR_TIMEOUT = 3, FF_ERR_SIZE = 4 };
 enum { FF_STAGE_RESIDUAL = 1, FF_STAGE_GRAD = 2, FF_STAGE_STATE = 3, FF_STAGE_SWEEP = 4 };
@@ -69,6 +76,32 @@ int ff_residu(void *ctx, int blk, int level, int icycle);
 int ff_resl2(void *ctx, int blk, double *out5);
 int ff_imps(void *ctx, int blk, int level);
 int ff_fin(void *ctx, int blk, double *dromax);
+/* ff_residu, ff_imps and ff_fin also run on a coarse multigrid level: level
+ * must be the block's own level (1 + its depth in the ff_mg_link chain); on
+ * a coarse level ff_residu is RESIDI(M, N, M) (first-order Roe, FLUXDO),
+ * ff_fin applies the coarse-level limits (ns3c.f:1935-1990) and returns
+ * dromax = 0. */
+
+/* RESIDI(M, N, M2) ns3c.f:2355 on the block's own level M: M2 = M, or
+ * M2 = M + 1 for the finer level's residual that TRANSF restricts next (the
+ * k-omega gradients are then recomputed, ns3c.f:1626).  ICYCLE as passed. */
+int ff_residi(void *ctx, int blk, int m2, int icycle);
+
+/* Multigrid stages of CYCLES (ns3c.f:1607-2170) for a host that drives the
+ * V-cycle itself; `fine` and `coarse` must be linked by ff_mg_link.
+ * ff_transf  TRANSF multi.f:156 (TRANKE multi.f:434 with k-omega): volume-
+ *            weighted restriction of TEMP, U, V, W, PDIFF, EPS2, VIST (RK,
+ *            REPS) and of the fine residual into the coarse P2H, the coarse
+ *            *OLD copies and ghost rings (ns3c.f:1687);
+ * ff_forcfu  FORCFU multi.f:1609: P2H = P2H - R(coarse) (ns3c.f:1859);
+ * ff_addres  ADDRES multi.f:1686: R = P2H + R (ns3c.f:1677, 1877);
+ * ff_interp  INTERP multi.f:1763 (INTERT multi.f:2051 with k-omega): the
+ *            coarse correction injected into the fine level, then the limits
+ *            CYCLES applies after it (ns3c.f:2017-2125). */
+int ff_transf(void *ctx, int fine, int coarse);
+int ff_forcfu(void *ctx, int blk);
+int ff_addres(void *ctx, int blk);
+int ff_interp(void *ctx, int coarse, int fine);
 
 /* Time-accurate runs (ff_params.timel = 1, physical step ff_params.dt):
  * ff_residu adds TIMDER res3c.f:3014 (and TIMDKE res3c.f:3062) on level 1
@@ -123,7 +156,13 @@ int ff_cycles(void *ctx, int blk, int ncycles, int icycle0, double *hist, int us
  * Calls share the array, so calls that overlap on the GPU race: serialise
  * them (one stream, or events).  With prm->ddadi = 1 it runs the DDADI line
  * sweeps instead, which use no scratch.  Laminar (five-equation) blocks only:
- * prm->iturb >= 3 gives FF_ERR_ARG.  Asynchronous on `stream` (a cudaStream_t). */
+ * prm->iturb >= 3 gives FF_ERR_ARG.  The LU-SGS sweeps here are FP64 only:
+ * prm->lusgs_fp32 = 1 without ddadi gives FF_ERR_ARG.  Asynchronous on
+ * `stream` (a cudaStream_t), so a sweep whose bounded grid barrier timed out
+ * cannot report it from the call that queued it: the flag stays set on the
+ * device until the caller asks.  level = 0 is that status query (the other
+ * arguments are ignored): it waits for `stream` and returns FF_ERR_TIMEOUT if
+ * any call since the last query timed out (and clears the flag), else 0. */
 #define FF_NOALLOC_MAX_NTOT 98304
 int ff_imps_noalloc(int imax, int jmax, int kmax, const ff_params *prm,
                     double *const *slots, int level, void *stream);
@@ -197,6 +236,39 @@ int ff_sweep_times(void *ctx, int blk, float *ms3);
 int ff_lusgs_kind(void *ctx, int blk);
 int ff_time_cycles(void *ctx, int blk, int ncycles, float *ms);
 int ff_time_stage(void *ctx, int blk, int stage, int reps, float *ms);
+
+/* ---- Fortran call sites ------------------------------------------------
+ * External subroutines with the reference's names and argument lists, for a
+ * FINFLO host built with gfortran (lower case, trailing underscore, every
+ * argument by reference), linked in place of the CPU routines CYCLES calls:
+ *   statim_  STATIM(M, N, INN, REFLEL)  ns3c.f:10318 (call ns3c.f:1450)
+ *   residi_  RESIDI(M, N, M2, IPR)      ns3c.f:2355  (call ns3c.f:1484)
+ *   impsdi_  IMPSDI(M, N, M2, AMGDIVL)  ns3c.f:2683  (call ns3c.f:1497)
+ *   fin_     FIN(TEMP, ..., NGL, ICYCLE) res3c.f:1077 (call ns3c.f:1517)
+ *   boundi_  BOUNDI(M)                  ns3c.f:10608 (call ns3c.f:556)
+ * They act on one module-level context: ff_fortran_bind names it,
+ * ff_fortran_block maps the host's level M, block N and global block number
+ * NGL to a block id, ff_fortran_cycle sets the cycle number RESIDI passes
+ * on.  A subroutine returns no status: ff_fortran_ierr returns (and clears)
+ * the first failing stage's FF_ERR_* code since it was last called.  FIN's
+ * host arrays are not read (the state is on the device), and fin_ includes
+ * the limits CYCLES applies right after FIN (ns3c.f:1553-1596), which the
+ * host then skips. */
+int ff_fortran_bind(void *ctx);
+int ff_fortran_block(int m, int n, int ngl, int blk);
+int ff_fortran_cycle(int icycle);
+int ff_fortran_ierr(void);
+void statim_(const int *m, const int *n, const int *inn, const int *reflel);
+void residi_(const int *m, const int *n, const int *m2, const int *ipr);
+void impsdi_(const int *m, const int *n, const int *m2, const double *amgdivl);
+void fin_(void *temp, void *u, void *v, void *w, void *pdiff, void *dtemp, void *du, void *dv, void *dw,
+          void *dp, void *told, void *uold, void *vold, void *wold, void *pold, void *rk, void *reps,
+          void *drk, void *deps, void *rkold, void *epsold, const double *rklim, const double *epslim,
+          void *pro, void *var, void *fi, void *dfi, void *fiold, void *rlolim, void *upplim,
+          const int *imax, const int *jmax, const int *kmax, const int *maxsb, const int *nscal,
+          const int *nsca2, const int *iturb, const int *ipresc, const double *turlim, void *vis,
+          const int *transl, void *trm, void *blks, const int *ngl, const int *icycle);
+void boundi_(const int *m);
 
 #ifdef __cplusplus
 }

@@ -71,6 +71,12 @@ typedef struct ff_params {
   int vanleer;                          /* 1: van Leer FVS (IFLUX=0, laminar), */
                                         /* 0: Roe (IFLUX=1)                    */
   double dt;                            /* physical time step DT (TIMEL)       */
+  int predgs_full;                      /* 1: the LU-SGS lower sweep (PREDGS)  */
+                                        /* keeps the i+1 coupling in row JMAX  */
+                                        /* that imps4.f:1460-1466 drops (its   */
+                                        /* shift loop starts one index late);  */
+                                        /* 0: the reference's sweep            */
+  int pad_;                             /* keeps the struct a multiple of 8   */
 } ff_params;
 
 /* Per-cell array slots of one block (names are the reference's MAIN_ARRAYS,

@@ -1181,7 +1181,10 @@ void orc_predgs(orc_block *b, const ff_params *p) {
         jac_product(out, dw, C[N], RO[N], A2X[N], A2Y[N], A2Z[N], xj[3 * L], xj[3 * L + 1], xj[3 * L + 2]);
         for (int v = 0; v < 5; v++) bd[5 * I + v] = out[v];
       }
-      for (int I = ialku; I <= iloppu - 1; I++)
+      /* imps4.f:1460 starts the shift at IALKU, so cell (IALKU-1, JMAX) of the
+       * next hyperplane never receives the i+1 product of (IALKU, JMAX);
+       * predgs_full starts it one index earlier */
+      for (int I = (p->predgs_full && ialku > 1) ? ialku - 1 : ialku; I <= iloppu - 1; I++)
         for (int v = 0; v < 5; v++) yd[5 * I + v] = yd[5 * (I + 1) + v];
       for (int v = 0; v < 5; v++) yd[5 * iloppu + v] = 0.;
     }

@@ -136,3 +136,59 @@ def test_restart_rejects_deforming_and_chimera_files(tmp_path, flags):
         fileio._write_record(f, struct.pack("<3i", *flags))
     with pytest.raises(ValueError, match="chimera"):
         fileio.read_restart(path, [10])
+
+
+def test_restart_truncated_file_names_the_restart(tmp_path):
+    """A truncated RSTART is reported as a restart error, not a grid error."""
+    blk, prm, fs = case.bump_case(9, 7, 5)
+    path = tmp_path / "RSTART"
+    fileio.write_restart(path, [fileio.block_restart_vars(blk)])
+    data = path.read_bytes()
+    path.write_bytes(data[:len(data) - 100])
+    with pytest.raises((EOFError, ValueError), match="restart"):
+        fileio.read_restart(path, [blk.ntot])
+
+
+def _timel_steps(o, steps, inner, first_step=0, hist=None):
+    for s in range(first_step, first_step + steps):
+        if s:
+            o.time_levels(1)   # NEWTIM at the start of every later physical step
+        for i in range(inner):
+            r = o.cycle(i + 1)[0]
+            if hist is not None:
+                hist.append(r)
+
+
+def test_restart_continues_a_timel_run(tmp_path):
+    """Time-accurate run: two physical steps, RSTART with the time-level
+    records (written at the end of a step, as WRITRS is), a fresh case read
+    from it whose next step begins with NEWTIM; its third step equals the
+    third step of the uninterrupted run."""
+    inner, dt = 8, 2e-5
+    blk, prm, fs = case.bump_case(17, 9, 9)
+    prm.timel, prm.dt = 1, dt
+    o = Oracle(blk, prm)
+    o.start()
+    o.time_levels(0)   # STARTI
+    full = []
+    _timel_steps(o, 3, inner, hist=full)
+
+    blk, prm, fs = case.bump_case(17, 9, 9)
+    prm.timel, prm.dt = 1, dt
+    o = Oracle(blk, prm)
+    o.start()
+    o.time_levels(0)
+    _timel_steps(o, 2, inner)
+    path = tmp_path / "RSTART"
+    fileio.write_restart(path, [fileio.block_restart_vars(blk, timel=True)], timel=True)
+
+    blk2, prm2, fs2 = case.bump_case(17, 9, 9)
+    prm2.timel, prm2.dt = 1, dt
+    time2, got = fileio.read_restart(path, [blk2.ntot], timel=True)
+    assert time2
+    fileio.load_restart_vars(blk2, got[0])
+    o2 = Oracle(blk2, prm2)
+    o2.start()
+    rest = []
+    _timel_steps(o2, 1, inner, first_step=2, hist=rest)
+    np.testing.assert_allclose(np.array(rest), np.array(full[2 * inner:]), rtol=1e-9)

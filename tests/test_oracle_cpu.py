@@ -187,9 +187,12 @@ def test_abi_exports_every_declared_symbol():
     hdr = open(os.path.join(ROOT, "include", "finflo_gpu.h")).read()
     names = re.findall(r"^\s*(?:int|void \*|const char \*)\s*\**\s*(ff_\w+)\s*\(", hdr, re.M)
     assert len(names) >= 15
-    for n in names:
+    # the Fortran call-site wrappers: gfortran names (lower case, trailing _)
+    fnames = re.findall(r"^\s*void\s+([a-z]+_)\s*\(", hdr, re.M)
+    assert sorted(fnames) == ["boundi_", "fin_", "impsdi_", "residi_", "statim_"]
+    for n in names + fnames:
         assert hasattr(L, n), n
-    assert L.ff_abi_version() == 3
+    assert L.ff_abi_version() == 4
 
 
 def test_nn_abi_exports_every_declared_symbol():

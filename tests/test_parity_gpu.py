@@ -16,8 +16,9 @@ pytestmark = pytest.mark.gpu
 RES = ("DRO", "DM", "DN", "DW", "DE")
 
 
-def _setup(ni=17, nj=9, nk=9, **kw):
+def _setup(ni=17, nj=9, nk=9, predgs_full=0, **kw):
     bg, bc, prm, fs = make_pair(ni, nj, nk, **kw)
+    prm.predgs_full = predgs_full
     o = Oracle(bc, prm)
     o.start()
     g = GpuSolver(0)
@@ -97,6 +98,42 @@ def test_imps_lusgs(gpu_lib, dims):
         ref = interior(bc, bc.arrays[n]); got = interior(bg, d[n])
         err = np.abs(got - ref).max() / (np.abs(ref).max() + 1e-300)
         assert err <= 1e-11, (n, err)
+    g.close()
+
+
+@pytest.mark.parametrize("kind", ["lines", "hyperplane", "pipe"])
+def test_imps_lusgs_predgs_full(gpu_lib, kind, monkeypatch):
+    """predgs_full: the lower sweep keeps the row-JMAX i+1 coupling that the
+    reference's PREDGS drops (imps4.f:1460); every sweep kernel against the
+    oracle."""
+    monkeypatch.setenv("FINFLO_LUSGS", kind)
+    g, bid, bg, o, bc, prm = _setup(33, 17, 17, predgs_full=1)
+    want = {"pipe": 3, "lines": 1, "hyperplane": 2}[kind]
+    assert g.lusgs_kind(bid) % 100 == want
+    o.statim(); o.adjuin(); o.residu(1, 1)
+    g.residu(bid, 1, 1)
+    g.sync()
+    bg_res = g.download(bid, list(RES))
+    for n in RES:
+        bc.arrays[n][:] = bg_res[n]
+    o.imps(1)
+    g.imps(bid, 1)
+    g.sync()
+    d = g.download(bid, list(RES))
+    for n in RES:
+        ref = interior(bc, bc.arrays[n]); got = interior(bg, d[n])
+        err = np.abs(got - ref).max() / (np.abs(ref).max() + 1e-300)
+        assert err <= 1e-11, (n, err)
+    g.close()
+
+
+def test_cycles_predgs_full_match_oracle(gpu_lib):
+    """30 graph-captured cycles with predgs_full against the oracle."""
+    g, bid, bg, o, bc, prm = _setup(17, 9, 9, predgs_full=1)
+    n = 30
+    hist = g.cycles(n, bid, icycle0=1, use_graph=True)
+    ref = np.array([o.cycle(i + 1)[0] for i in range(n)])
+    np.testing.assert_allclose(hist[:, :5], ref, rtol=1e-8)
     g.close()
 
 

@@ -23,6 +23,7 @@ from tests.util import interior
 pytestmark = pytest.mark.gpu
 
 RES = ["DRO", "DM", "DN", "DW", "DE"]
+FF_ERR_ARG = 2
 FF_ERR_SIZE = 4
 FF_NOALLOC_MAX_NTOT = 98304
 
@@ -70,7 +71,21 @@ def test_imps_noalloc_matches_imps_twice(gpu_lib, ddadi):
             a, b = interior(blk, got[n]), interior(blk, ref[n])
             err = np.abs(a - b).max() / (np.abs(b).max() + 1e-300)
             assert err <= 1e-12, (call, n, err)
+    # the status query (level 0): no sweep of these calls timed out
+    assert L.ff_imps_noalloc(0, 0, 0, None, None, 0, stream) == 0
     g.close()
+
+
+def test_imps_noalloc_refuses_fp32_lusgs(gpu_lib):
+    """Its LU-SGS sweeps are FP64 only: an FP32 request is refused, not
+    silently run in FP64."""
+    L = gpu_lib
+    blk, prm, fs = case.bump_case(17, 9, 9)
+    prm.lusgs_fp32 = 1
+    slots = (ctypes.c_void_p * len(SLOTS))(*([1] * len(SLOTS)))
+    rc = L.ff_imps_noalloc(blk.imax, blk.jmax, blk.kmax, ctypes.byref(prm),
+                           ctypes.cast(slots, ctypes.POINTER(ctypes.c_void_p)), 1, None)
+    assert rc == FF_ERR_ARG
 
 
 def test_imps_noalloc_rejects_oversized_block(gpu_lib):
