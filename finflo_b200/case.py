@@ -607,3 +607,65 @@ def bump_multiblock_case(*args, **kw):
         bl.append(levels)
         bp.append(prms)
     return (bl, bp, fs, tri) if tri is not None else (bl, bp, fs)
+
+
+# ---- patches from / to FINFLO's BC file (READBC gluebm.f:2553) -------------
+
+def patches_from_bc(bc_patches, nblocks, fs, rk=0.0, reps=0.0):
+    """The library's patch tables (one FFPatch list per block, file order)
+    from the patches fileio.read_bc returns.  Inlet/outlet boundary values
+    are the free stream's, uniform over the patch (the boundary-value files
+    are not read); a connection's IBTYPE is its source block's 0-based index,
+    NFACE its face and N1A/N2A the start of the matching range."""
+    out = [[] for _ in range(nblocks)]
+    inl = dict(bounr=fs["rho"], bounu=fs["u"], bounv=0.0, bounw=0.0, bount=fs["t"], bounp=fs["p"], bounpd=0.0,
+               bounrk=rk, bounep=reps)
+    for p in bc_patches:
+        if p.ityp == grid.BC_CON:
+            pa = _patch(grid.BC_CON, p.iface, (p.r1a, p.r1b), (p.r2a, p.r2b), ibtype=p.nblock - 1)
+            pa.nface, pa.n1a, pa.n2a = p.nface, p.n1a, p.n2a
+        elif p.ityp in (grid.BC_INL, grid.BC_OUT):
+            pa = _patch(p.ityp, p.iface, (p.r1a, p.r1b), (p.r2a, p.r2b), ibtype=p.itype, **inl)
+        elif p.ityp in (grid.BC_SOL, grid.BC_MIR):
+            pa = _patch(p.ityp, p.iface, (p.r1a, p.r1b), (p.r2a, p.r2b), iheat=p.iheat if p.ityp == grid.BC_SOL else 0)
+        else:
+            raise ValueError(f"BC type {p.kind} is not on this path")
+        out[p.block - 1].append(pa)
+    return out
+
+
+def bc_from_patches(block_patches, periodic_faces=()):
+    """The BC-file patches (fileio.BcPatch) of the library's patch tables:
+    the inverse of patches_from_bc.  A connection through a face listed in
+    periodic_faces is written as PER."""
+    from . import fileio
+    names = {grid.BC_INL: "INL", grid.BC_OUT: "OUT", grid.BC_SOL: "SOL", grid.BC_MIR: "MIR", grid.BC_CON: "CON"}
+    out = []
+    for ib, pats in enumerate(block_patches, start=1):
+        seen = {}
+        for pa in pats:
+            seen[pa.iface] = seen.get(pa.iface, 0) + 1
+            kind = names[pa.ityp]
+            if kind == "CON" and pa.iface in periodic_faces:
+                kind = "PER"
+            p = fileio.BcPatch(kind, ib, pa.iface, seen[pa.iface])
+            p.r1a, p.r1b, p.r2a, p.r2b = pa.r1a, pa.r1b, pa.r2a, pa.r2b
+            if pa.ityp == grid.BC_CON:
+                p.nblock, p.nface = pa.ibtype + 1, pa.nface
+            elif pa.ityp in (grid.BC_INL, grid.BC_OUT):
+                p.itype = pa.ibtype
+                p.bfile = "INLET.DAT" if pa.ityp == grid.BC_INL else "OUTLET.DAT"
+            elif pa.ityp == grid.BC_SOL:
+                p.iheat = pa.iheat
+                p.rcon = [0.0] * 13 + [1.0]
+            out.append(p)
+    # a connection names its partner by the partner's position on its face
+    for p in out:
+        if p.kind in ("CON", "PER"):
+            pa = block_patches[p.block - 1][[q for q in out if q.block == p.block].index(p)]
+            cands = [q for q in out if q.block == p.nblock and q.iface == p.nface and q.kind in ("CON", "PER")]
+            match = [q for q in cands if q.r1a <= pa.n1a <= q.r1b and q.r2a <= pa.n2a <= q.r2b]
+            if not match:
+                raise ValueError(f"block {p.block} face {p.iface}: no partner patch")
+            p.npatch = match[0].local
+    return out
