@@ -188,9 +188,24 @@ def run_reference(args):
     if args.workload == "sst-precision":
         args.workload = "sst-mg"   # the same workload; the reference has only its FP64 path
     if args.workload == "large":
-        print(json.dumps({"impl": "reference", "unavailable": "the 16.8M-cell multi-block case holds ~13 GB of "
-                          "host arrays per oracle copy and runs minutes per cycle on the host cores; the CPU "
-                          "baseline is measured on the single-block workloads"}))
+        cells = tuple(int(x) for x in args.large_cells.split(","))
+        seconds = max(10.0, min(30.0, 1.5 * args.steps))
+        rate, nproc, ncyc, bc = large_oracle_rate(cells, seconds, os.cpu_count() or 1)
+        name = LARGE_NAME.format(cells="x".join(map(str, cells)), prec="FP64")
+        line = {
+            "metric": "cell-iters/s", "value": rate, "unit": "cell-iters/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 residual / f64 LU-SGS",
+            "data": "synthetic (seeded block cuts and free-stream noise)",
+            "config": {"workload": name, "parallelism": f"{nproc} host processes, one block each"},
+            "impl": "reference",
+            "cpu_baseline": {"value": rate, "unit": "cell-iters/s", "cores": nproc, "kind": "port",
+                             "sample": f"{ncyc} V-cycles in total, one process per block (blocks 0-{nproc - 1}, "
+                                       f"{sum(bc)} cells), each timing its own block's V-cycles for ~{seconds:.0f} s "
+                                       "after a warm-up cycle; the sum of the per-block rates"},
+            "e2e": {"value": rate, "unit": "cell-iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line))
         return 0
     if args.workload == "warmstart":
         print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned warm start; its "
@@ -440,31 +455,96 @@ def run_box(args):
 
 LARGE_NAME = ("3-D bump channel, spanwise amplitude 0.1(1+0.5 sin 2 pi z) on z in [0,1] (periodic), {cells} cells "
               "in 8 uneven blocks (2x2x2 cuts, seed 5, 1:1 patches), k-omega SST Re=5e6 M=0.7, first cell 2e-6, "
-              "3-level V-cycle per block, FP64 residual + {prec} LU-SGS and coarse levels, graph-captured "
-              "multi-block cycle")
+              "Roe+MUSCL(INTER=1), 3-level V-cycle per block, FP64 residual + {prec} LU-SGS and coarse levels, "
+              "graph-captured multi-block cycle")
+LARGE_STATE = ["TEMP", "U", "V", "W", "PDIFF", "RK", "REPS"]
+
+
+def _large_blocks(cells, nlev=3, fp32=False, ddadi=False, device_setup=True):
+    """The large case's block generator (fs, wall triangles, then (levels,
+    prms) per block) with the settings every arm uses: INTER=1 and the full
+    lower sweep (the converging choices), FP64 or FP32 implicit stage."""
+    from finflo_b200 import case
+    it = case.bump_multiblock_blocks(cells=cells, nb=(2, 2, 2), nlev=nlev, seed=5, inter=1, lusgs_fp32=fp32,
+                                     coarse_fp32=fp32, device_setup=device_setup)
+    for item in it:
+        if isinstance(item, tuple) and len(item) == 2 and isinstance(item[0], list):
+            for q in item[1]:
+                q.predgs_full = 1
+                q.ddadi = int(ddadi)
+        yield item
+
+
+def _large_block_worker(args):
+    """The oracle on block k of the large case (its three levels, host
+    metrics and wall distance): V-cycles of that block alone until `seconds`
+    have passed (at least one after a warm-up cycle).  Returns (cells,
+    cycles, seconds)."""
+    k, cells, seconds = args
+    sys.path.insert(0, ROOT)
+    from finflo_b200 import case, grid
+    from oracle.oracle import OracleMG
+    it = _large_blocks(cells, fp32=False)
+    next(it)
+    tri = next(it)[1]
+    for n, (levels, prms) in enumerate(it):
+        if n == k:
+            break
+    for lev, m in zip(levels, grid.mg_metrics(*levels[0].nodes, len(levels))):
+        for name in grid.METRIC_NAMES:
+            lev.arrays[name][:] = m.arrays[name]
+        lev.arrays["DISTW"][:] = case.wall_distance_tri(lev, tri)
+    om = OracleMG(levels, prms)
+    om.start()
+    om.cycle(1)
+    n, t0 = 0, time.perf_counter()
+    while n < 1 or time.perf_counter() - t0 < seconds:
+        om.cycle(n + 2)
+        n += 1
+    return levels[0].interior_cells, n, time.perf_counter() - t0
+
+
+def large_oracle_rate(cells, seconds, nproc):
+    """Cell-iters/s of the oracle on the large case: one process per block
+    (blocks 0..nproc-1, spawned), each timing V-cycles of its block; the
+    rate is the sum over processes.  Returns (rate, processes, cycles)."""
+    import multiprocessing as mp
+    nproc = max(1, min(8, nproc))
+    try:
+        import psutil
+        nproc = max(1, min(nproc, int(psutil.virtual_memory().available * 0.6 // 4.0e9)))
+    except Exception:
+        pass
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(nproc) as pool:
+        res = pool.map(_large_block_worker, [(k, cells, seconds) for k in range(nproc)])
+    return sum(c * n / t for c, n, t in res), nproc, sum(n for _, n, _ in res), [c for c, _, _ in res]
 
 
 def run_large(args):
-    """The large combined case: every block's V-cycle as a branch of one
-    captured multi-block cycle, BOUNDI/CONNEC on device.  Blocks are built,
-    uploaded and dropped from host memory one at a time."""
-    ws_, rank, local = _dist()
+    """The large combined case (the default workload): every block's V-cycle
+    as a branch of one captured multi-block cycle, BOUNDI/CONNEC on device.
+    Blocks are built, uploaded and dropped from host memory one at a time.
+    N > 1 runs N replicas of the whole case (weak scaling)."""
+    ws, rank, local = _dist()
     import torch
     torch.cuda.set_device(local)
-    from finflo_b200 import case, grid
+    if ws > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    from finflo_b200 import grid
     from finflo_b200.case import FFPatch
-    from finflo_b200.gpu import GpuSolver, FF_STAGE_RESIDUAL
+    from finflo_b200.gpu import GpuSolver, FF_STAGE_RESIDUAL, FF_STAGE_SWEEP
     cells = tuple(int(x) for x in args.large_cells.split(","))
-    fp32 = not args.large_fp64
+    fp32 = args.large_fp32
     nlev = 3
     t0 = time.perf_counter()
     g = GpuSolver(local)
     dev = not args.host_setup   # metrics and wall distance on the device (ff_block_metrics_levels)
-    it = case.bump_multiblock_blocks(cells=cells, nb=(2, 2, 2), nlev=nlev, seed=5, lusgs_fp32=fp32,
-                                     coarse_fp32=fp32, device_setup=dev)
+    it = _large_blocks(cells, nlev, fp32=fp32, ddadi=args.ddadi, device_setup=dev)
     _, fs = next(it)
     tri = next(it)[1] if dev else None
-    fine_cells = []
+    fine_cells, fine_ntot = [], []
     for n, (levels, prms) in enumerate(it):
         fine = levels[0]
         orig = fine.patches
@@ -475,8 +555,6 @@ def run_large(args):
                 q.ibtype = q.ibtype * nlev
             pats.append(q)
         fine.patches = pats
-        for q in prms:
-            q.ddadi = int(args.ddadi)
         bid = g.add_levels(levels, prms)
         assert bid == n * nlev
         for q in range(nlev):
@@ -488,42 +566,91 @@ def run_large(args):
         for q in range(nlev):
             levels[q].arrays = {}
         fine_cells.append(fine.imax * fine.jmax * fine.kmax)
+        fine_ntot.append(fine.ntot)
     setup_s = time.perf_counter() - t0
     total = sum(fine_cells)
+    nblk = len(fine_cells)
     g.start_all()
-    g.cycles_all(1 + args.warmup, icycle0=1)
+    g.cycles_all(1 + args.warmup, icycle0=1)   # warm-up incl. the sweep autotuner and graph capture
     g.sync()
+    # ---- device-timed cycles -------------------------------------------
     clk = ClockSampler(local)
+    _barrier(ws)
     clk.start()
     ms, per_cycle = g.time_cycles_all(args.steps)
     clocks = clk.stop()
-    value = total * args.steps / (ms * 1e-3)
-    ms_res = g.time_stage(FF_STAGE_RESIDUAL, reps=5, bid=0)
-    achieved = 328.0 * fine_cells[0] / (ms_res * 1e-3) / 1e9
+    _barrier(ws)
+    ms = _allreduce_max(ms, ws)
+    value = total * args.steps * ws / (ms * 1e-3)
+    # ---- dominant kernels: the fused residual and one LU-SGS sweep of the
+    # largest block, each timed alone
+    big = int(np.argmax(fine_cells))
+    ms_res = g.time_stage(FF_STAGE_RESIDUAL, reps=10, bid=big * nlev)
+    ms_sweep = g.time_stage(FF_STAGE_SWEEP, reps=5, bid=big * nlev)
+    achieved = 328.0 * fine_cells[big] / (ms_res * 1e-3) / 1e9
+    sweep_bpc = 132.0 if fp32 else 264.0
+    achieved_sweep = sweep_bpc * fine_cells[big] / (ms_sweep * 1e-3) / 1e9
     peak, pkind = _peaks()
+    # ---- end to end through the C-ABI with host buffers: every step uploads
+    # the fine blocks' state from page-locked host arrays, runs the cycle and
+    # downloads the state and the residual history
+    host = [{n: np.zeros(nt) for n in LARGE_STATE} for nt in fine_ntot]
+    for k in range(nblk):
+        g.download(k * nlev, LARGE_STATE, into=host[k])
+    flat = [a for h in host for a in h.values()]
+    g.pin(flat)
+    h2d = d2h = 0
+    _barrier(ws)
+    t1 = time.perf_counter()
+    nsteps_e2e = 0 if args.no_e2e else args.steps
+    for s_ in range(nsteps_e2e):
+        for k in range(nblk):
+            g.upload(k * nlev, LARGE_STATE, src=host[k])
+        hist = g.cycles_all(1, icycle0=2 + args.warmup + s_)
+        for k in range(nblk):
+            g.download(k * nlev, LARGE_STATE, into=host[k])
+        h2d += 8 * sum(fine_ntot) * len(LARGE_STATE)
+        d2h += 8 * sum(fine_ntot) * len(LARGE_STATE) + hist.nbytes
+    g.sync()
+    e2e_s = _allreduce_max(time.perf_counter() - t1, ws)
+    g.unpin(flat)
+    e2e = total * nsteps_e2e * ws / e2e_s if nsteps_e2e else None
     hist = g.cycles_all(2, icycle0=2 + args.warmup + args.steps)
     line = {
-        "metric": "cell-iters/s", "value": value, "unit": "cell-iters/s", "n_gpus": ws_, "steps": args.steps,
+        "metric": "cell-iters/s", "value": value, "unit": "cell-iters/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64 residual / " + ("f32" if fp32 else "f64") + " LU-SGS",
         "data": "synthetic (seeded block cuts and free-stream noise)",
         "config": {"workload": LARGE_NAME.format(cells="x".join(map(str, cells)), prec="FP32" if fp32 else "FP64")
                    + (", DDADI implicit stage (LUSGS=0)" if args.ddadi else ""),
-                   "cells": total, "blocks": len(fine_cells), "levels": nlev, "setup_s": setup_s,
+                   "cells": total, "blocks": nblk, "levels": nlev, "setup_s": setup_s,
                    "setup": "metrics and wall distance on the host" if args.host_setup else
                             "metrics and wall distance on the device",
-                   "parallelism": "blocks on 1 GPU", "l2": "inputs larger than L2"},
+                   "parallelism": f"8 blocks per GPU, replicas x{ws}",
+                   "l2": "state resident in HBM (~30 GB), per-cycle working set far above L2"},
         "gpu_launches": per_cycle * args.steps,
-        "roofline": {"bound": "hbm", "kernel": "k_residual_sst (block 0)", "achieved": achieved, "peak": peak,
-                     "peak_kind": pkind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
-                     "ms_per_launch": ms_res, "bytes_per_cell": 328.0},
-        "e2e": None,
+        "roofline": {"bound": "hbm", "kernel": "k_residual_fused<7,512> (largest block)", "achieved": achieved,
+                     "peak": peak, "peak_kind": pkind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "ms_per_launch": ms_res, "bytes_per_cell": 328.0},
+        "lusgs_sweep": {"kernel": "one lower LU-SGS sweep (largest block, alone)", "ms_per_sweep": ms_sweep,
+                        "bytes_per_cell": sweep_bpc, "achieved_gbs": achieved_sweep,
+                        "frac": achieved_sweep / peak},
+        "e2e": {"value": e2e, "unit": "cell-iters/s", "h2d_bytes_per_step": h2d // max(1, nsteps_e2e),
+                "d2h_bytes_per_step": d2h // max(1, nsteps_e2e)} if e2e else None,
         "clocks": clocks,
         "residual_finite": bool(np.isfinite(hist).all()),
     }
+    g.close()
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        rate, nproc, ncyc, bc = large_oracle_rate(cells, max(3.0, args.cpu_seconds), 1)
+        line["cpu_baseline"] = {"value": rate, "unit": "cell-iters/s", "cores": 1, "kind": "port",
+                                "sample": f"{ncyc} oracle V-cycles of block 0 ({bc[0]} cells, its 3 levels, "
+                                          "host metrics) on one core after one warm-up cycle"}
     if rank == 0:
         print(json.dumps(line))
-    g.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
     return 0
 
 
@@ -580,6 +707,10 @@ def run_precision(args):
 WARM_NAME = ("learned warm start: bump channel 64x32x32 cells, laminar Re=1e4, Mach U[0.3,0.8] x bump "
              "amplitude U[0.05,0.15]; 64 solver solutions (seed 3) train a 4-layer MLP encoder + 3-D "
              "transposed-conv decoder (32 channels, BF16 weights, tcgen05 GEMMs); 16 held-out points (seed 4)")
+WARM_SST_NAME = ("learned warm start: k-omega SST bump channel 128x64x64 cells (first cell 2e-6, Re=1e6), 3-level "
+                 "V-cycle, INTER=1, CFL 1, Mach U[0.5,0.7]; solver solutions (seed 3) train the network (5 "
+                 "refinement levels, k and omega as logs); held-out Mach points (seed 4); FP64 LU-SGS from the "
+                 "free stream vs FP32 LU-SGS (every level) from the free stream and from the prediction")
 
 
 def run_warmstart(args):
@@ -591,9 +722,11 @@ def run_warmstart(args):
     import torch
     torch.cuda.set_device(local)
     from finflo_b200 import warmstart as wsm
+    spec = wsm.SST if args.ws_family == "sst" else wsm.BUMP
     logs = []
     r = wsm.run_config(ntrain=args.ws_train, ntest=args.ws_test, cycles=args.ws_cycles, steps=args.ws_steps,
-                       tol_decades=args.ws_decades, log=logs.append, ddadi_arms=True)
+                       tol_decades=args.ws_decades, log=logs.append, ddadi_arms=args.ws_family != "sst",
+                       spec=spec, batch=min(16, args.ws_train), max_cycles=args.ws_max_cycles or None)
     if rank != 0:
         return 0
     line = {
@@ -602,20 +735,23 @@ def run_warmstart(args):
         "ms_per_step": 1e3 * r["t_train"] / args.ws_steps, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "bf16 network / f32 LU-SGS / f64 residual",
         "data": "synthetic (seeded parameter points; training fields generated by the solver)",
-        "config": {"workload": WARM_NAME, "ntrain": args.ws_train, "ntest": args.ws_test,
+        "config": {"workload": WARM_NAME if args.ws_family != "sst" else WARM_SST_NAME,
+                   "ntrain": args.ws_train, "ntest": args.ws_test,
                    "training_cycles": args.ws_cycles, "training_steps": args.ws_steps,
                    "parallelism": f"replicas x{ws_}"},
-        "plain_fp64_free_stream_s": r["base_s"], "speedup": r["speedup"],
-        "cycles": {"plain_fp64_free_stream": r["base_cycles"], "fp32_lusgs_warm_start": r["warm_cycles"]},
-        # the same two runs with the reference's default implicit stage (DDADI, LUSGS=0)
-        "ddadi": {"fp64_free_stream_s": r["ddadi_base_s"], "fp32_warm_start_s": r["ddadi_warm_s"],
-                  "fp64_free_stream_cycles": r["ddadi_base_cycles"], "fp32_warm_start_cycles": r["ddadi_warm_cycles"],
-                  "all_reached": r["ddadi_reached"],
-                  "speedup_vs_plain_fp64_lusgs": r["base_s"] / r["ddadi_warm_s"]},
+        "plain_fp64_free_stream_s": r["base_s"], "fp32_free_stream_s": r["free32_s"], "speedup": r["speedup"],
+        "network_gain": r["network_gain"], "all_reached": r["all_reached"],
+        "cycles": {"plain_fp64_free_stream": r["base_cycles"], "fp32_lusgs_free_stream": r["free32_cycles"],
+                   "fp32_lusgs_warm_start": r["warm_cycles"]},
         "training": {"data_s": r["t_data"], "train_s": r["t_train"], "loss": r["loss"]},
         "cases": r["cases"],
         "e2e": {"value": r["warm_s"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if "ddadi_base_s" in r:   # the same runs with the reference's default implicit stage (DDADI, LUSGS=0)
+        line["ddadi"] = {"fp64_free_stream_s": r["ddadi_base_s"], "fp32_warm_start_s": r["ddadi_warm_s"],
+                         "fp64_free_stream_cycles": r["ddadi_base_cycles"],
+                         "fp32_warm_start_cycles": r["ddadi_warm_cycles"], "all_reached": r["ddadi_reached"],
+                         "speedup_vs_plain_fp64_lusgs": r["base_s"] / r["ddadi_warm_s"]}
     print(json.dumps(line))
     return 0
 
@@ -630,7 +766,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--grid", default="", help="node counts ni,nj,nk (profiling runs)")
-    ap.add_argument("--workload", default="sst-mg",
+    ap.add_argument("--workload", default="large",
                     choices=["sst-mg", "bump", "box", "warmstart", "large", "sst-precision"])
     # 1200 cycles: both runs stay ahead of the transient near cycle 1400 (the
     # density residual jumps three decades in the FP64 run, and the FP32
@@ -638,7 +774,8 @@ def main():
     ap.add_argument("--prec-cycles", type=int, default=1200)
     ap.add_argument("--prec-cfl", type=float, default=1.0)
     ap.add_argument("--large-cells", default="512,256,128")
-    ap.add_argument("--large-fp64", action="store_true", help="FP64 implicit stage in the large case")
+    ap.add_argument("--large-fp32", action="store_true",
+                    help="large case: FP32 implicit stage on every level (default: plain FP64)")
     ap.add_argument("--host-setup", action="store_true", help="large case: metrics and wall distance on the host")
     ap.add_argument("--ddadi", action="store_true", help="DDADI implicit stage (LUSGS=0) instead of LU-SGS")
     ap.add_argument("--timel", type=float, default=0.0,
@@ -648,6 +785,9 @@ def main():
     ap.add_argument("--ws-cycles", type=int, default=2000)
     ap.add_argument("--ws-steps", type=int, default=6000)
     ap.add_argument("--ws-decades", type=float, default=2.0)
+    ap.add_argument("--ws-family", default="bump", choices=["bump", "sst"],
+                    help="warm start: the laminar bump family (Mach, amplitude) or the SST V-cycle case (Mach)")
+    ap.add_argument("--ws-max-cycles", type=int, default=0)
     ap.add_argument("--blocks", default="4,3,2", help="block arrangement of the box workload")
     args = ap.parse_args()
     if args.warmup < 3:
