@@ -629,12 +629,15 @@ def run_large(args):
                    "parallelism": f"8 blocks per GPU, replicas x{ws}",
                    "l2": "state resident in HBM (~30 GB), per-cycle working set far above L2"},
         "gpu_launches": per_cycle * args.steps,
-        "roofline": {"bound": "hbm", "kernel": "k_residual_fused<7,512> (largest block)", "achieved": achieved,
-                     "peak": peak, "peak_kind": pkind, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "ms_per_launch": ms_res, "bytes_per_cell": 328.0},
-        "lusgs_sweep": {"kernel": "one lower LU-SGS sweep (largest block, alone)", "ms_per_sweep": ms_sweep,
-                        "bytes_per_cell": sweep_bpc, "achieved_gbs": achieved_sweep,
-                        "frac": achieved_sweep / peak},
+        # the dominant kernel of the cycle (profiles/launches_large8blk_512x256x128.md):
+        # the LU-SGS line-wavefront sweep; one lower sweep of the largest block, timed alone
+        "roofline": {"bound": "hbm", "kernel": "k_lusgs_lines<double,7> (lower sweep, largest block)",
+                     "achieved": achieved_sweep, "peak": peak, "peak_kind": pkind, "unit": "GB/s",
+                     "frac": achieved_sweep / peak, "traffic": None, "ms_per_launch": ms_sweep,
+                     "bytes_per_cell": sweep_bpc, "cells": fine_cells[big]},
+        "residual": {"kernel": "k_residual_fused<7,512> (largest block, alone)", "ms_per_launch": ms_res,
+                     "tile": g.residual_shape(big * nlev),
+                     "bytes_per_cell": 328.0, "achieved_gbs": achieved, "frac": achieved / peak},
         "e2e": {"value": e2e, "unit": "cell-iters/s", "h2d_bytes_per_step": h2d // max(1, nsteps_e2e),
                 "d2h_bytes_per_step": d2h // max(1, nsteps_e2e)} if e2e else None,
         "clocks": clocks,

@@ -61,9 +61,13 @@ FF_DI void xxtrap(double r0, double r1, double r2, double r3, int intem, double&
     rip = r2 - (diff1 * R1 + diff2 * R2);
     rim = r1 + (diff1 * R1 + diff0 * R2);
   } else if (inter <= 4) {
+    // the two van Albada ratios through one reciprocal of the product of
+    // their denominators (each at least 1e-10, far from over- or underflow)
     double diff12 = diff1 * diff1 + 1.e-10;
-    double phibi = (diff12 + diff1 * diff0) / (diff12 + diff0 * diff0);
-    double phifi = (diff12 + diff1 * diff2) / (diff12 + diff2 * diff2);
+    double db = diff12 + diff0 * diff0, df = diff12 + diff2 * diff2;
+    double r = rcp(db * df);
+    double phibi = (diff12 + diff1 * diff0) * (df * r);
+    double phifi = (diff12 + diff1 * diff2) * (db * r);
     rip = r2 - phifi * (diff1 * R1 + diff2 * R2);
     rim = r1 + phibi * (diff1 * R1 + diff0 * R2);
   } else {
@@ -90,16 +94,18 @@ FF_DI void roe_flux(const double q[5][4], double nx, double ny, double nz, doubl
   ppi = dmax(0.001 * p.frspre, ppi);
   roim = dmax(0.001 * p.frsden, roim);
   pmi = dmax(0.001 * p.frspre, pmi);
-  const double gm1 = p.gamma - 1.;
-  // EFPRO state.f:620 (perfect gas)
-  double eip = ppi / (gm1 * roip) - p.e0ref;
-  double eim = pmi / (gm1 * roim) - p.e0ref;
-  double elr = ppi / (gm1 * roim) - p.e0ref;
-  double erl = pmi / (gm1 * roip) - p.e0ref;
+  const double rgm1 = rcp(p.gamma - 1.);
+  const double ypror = rcp(roip), yprol = rcp(roim);
+  // EFPRO state.f:620 (perfect gas): p / ((gamma - 1) rho)
+  double eip = ppi * rgm1 * ypror - p.e0ref;
+  double eim = pmi * rgm1 * yprol - p.e0ref;
+  double elr = ppi * rgm1 * yprol - p.e0ref;
+  double erl = pmi * rgm1 * ypror - p.e0ref;
   // DERIV base3c.f:707 (Glaister hat derivatives)
   double ypro1 = rcp(cr[2]), ypro2 = rcp(cl2[2]);
-  double dedph = 0.5 * ((-cr[0] / cr[1] - ypro1) + (-cl2[0] / cl2[1] - ypro2));
-  double dedrh = 0.5 * ((rcp(cr[1]) + cr[3] * (ypro1 * ypro1)) + (rcp(cl2[1]) + cl2[3] * (ypro2 * ypro2)));
+  double rdh1 = rcp(cr[1]), rdh2 = rcp(cl2[1]);
+  double dedph = 0.5 * ((-cr[0] * rdh1 - ypro1) + (-cl2[0] * rdh2 - ypro2));
+  double dedrh = 0.5 * ((rdh1 + cr[3] * (ypro1 * ypro1)) + (rdh2 + cl2[3] * (ypro2 * ypro2)));
   {
     double dpp = 2. * (ppi - pmi), drr = 2. * (roip - roim);
     if (fabs(dpp) >= 1.e-2 * (ppi + pmi)) dedph = (eip + elr - eim - erl) / dpp;
@@ -113,7 +119,6 @@ FF_DI void roe_flux(const double q[5][4], double nx, double ny, double nz, doubl
   double ul = nx * rmim + ny * rnim + nz * rwim;
   double vl = a21 * rmim + a22 * rnim + a23 * rwim;
   double wl = a31 * rmim + a32 * rnim + a33 * rwim;
-  double ypror = rcp(roip), yprol = rcp(roim);
   double eir = eip + .5 * (ur * ur + vr * vr + wr * wr);
   double eil = eim + .5 * (ul * ul + vl * vl + wl * wl);
   double pr = ppi, pl = pmi;

@@ -50,6 +50,8 @@ struct BlockCtx {
   PipeGeom pg{};
   float pipe_ms = 0.f;          // measured upper sweep of the pipelined kernel
   int tuned = 0;                // sweep kind chosen by tune_sweep
+  int res_shape = 0;            // residual tile shape (RES_SHAPES), chosen by tune_residual
+  int res_tuned = 0;
   float sweep_ms[2] = {0.f, 0.f};   // measured upper sweep: lines, best hyperplane
   LineGeom lg{};
   bool lines_stage = false;     // the staged line sweep fits (one tile per thread group)
@@ -202,11 +204,22 @@ bool res_fused() {
   return f;
 }
 
+template <int NV, int NT, int I_, int J_, int K_>
+void launch_residual_fused_s(cudaStream_t st, const BlockCtx* b, int level) {
+  dim3 g(nblk(b->imax, I_), nblk(b->jmax, J_), nblk(b->kmax, K_));
+  const size_t sm = residual_fused_smem(NV, I_, J_, K_);
+  cudaFuncSetAttribute(k_residual_fused<NV, NT, I_, J_, K_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k_residual_fused<NV, NT, I_, J_, K_><<<g, NT, sm, st>>>(b->db, b->prm, level);
+}
+
 template <int NV, int NT>
 void launch_residual_fused_t(cudaStream_t st, dim3 g, const BlockCtx* b, int level) {
-  const size_t sm = residual_fused_smem(NV);
-  cudaFuncSetAttribute(k_residual_fused<NV, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k_residual_fused<NV, NT><<<g, NT, sm, st>>>(b->db, b->prm, level);
+  (void)g;
+  // the tile shape the autotuner chose for this block (512 threads only)
+  const int sh = NT == 512 ? b->res_shape : 0;
+  if (sh == 1) return launch_residual_fused_s<NV, NT, 16, 8, 4>(st, b, level);
+  if (sh == 2) return launch_residual_fused_s<NV, NT, 8, 8, 8>(st, b, level);
+  launch_residual_fused_s<NV, NT, 32, 4, 4>(st, b, level);
 }
 
 void launch_residual(cudaStream_t st, const BlockCtx* b, int level) {
@@ -227,8 +240,13 @@ void launch_residual(cudaStream_t st, const BlockCtx* b, int level) {
   }
 }
 
-int st_residu_sst(Ctx* c, BlockCtx* b, int level, int m2, int icycle) {
-  int ncell = b->imax * b->jmax * b->kmax;
+// part: 0 the whole stage, 1 the kernels before the residual's face pass
+// (gradients, sources, ghost updates), 2 the kernels after it -- so that a
+// multi-block cycle can run the face pass of all blocks in one launch.
+int st_residu_sst(Ctx* c, BlockCtx* b, int level, int m2, int icycle, int part = 0) {
+  if (part == 2) goto post;
+  {
+  const int ncell = b->imax * b->jmax * b->kmax;
   int gg = level == 1 ? 2 : 0;
   long ng = (long)(b->imax + gg) * (b->jmax + gg) * (b->kmax + gg);
   if (m2 >= 2 || level == 1) {   // DERFUN (+ TEMDER of T) of this level
@@ -259,9 +277,16 @@ int st_residu_sst(Ctx* c, BlockCtx* b, int level, int m2, int icycle) {
     c->nlaunch++;
   }
   if (level == 1) launch_patch(c, b, k_inlet_outlet, icycle);
-  launch_residual(c->stream, b, level);
+  }
+  if (part == 1) return 0;
+  if (part == 0) {
+    launch_residual(c->stream, b, level);
+    c->nlaunch++;
+  }
+post:
+  const int ncell = b->imax * b->jmax * b->kmax;
   k_sourko_addske<<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db);
-  c->nlaunch += 2;
+  c->nlaunch++;
   if (b->prm.timel && level == 1) {   // TIMDER + TIMDKE after ADDSKE (res3c.f:5097)
     k_timder<7><<<nblk(ncell, 256), 256, 0, c->stream>>>(b->db, b->prm);
     c->nlaunch++;
@@ -269,29 +294,84 @@ int st_residu_sst(Ctx* c, BlockCtx* b, int level, int m2, int icycle) {
   return 0;
 }
 
-int st_residu(Ctx* c, BlockCtx* b, int level, int icycle, int m2 = 1) {
-  if (b->prm.iturb >= 3) return st_residu_sst(c, b, level, m2, icycle);
-  if (level == 1) {
-    if (b->npatch) {
-      int maxn = 1;
-      for (auto& p : b->h_patch) maxn = max(maxn, (p.r1b - p.r1a + 1) * (p.r2b - p.r2a + 1));
-      k_refcen<<<dim3(nblk(maxn, 128), b->npatch), 128, 0, c->stream>>>(b->db, b->prm);
+int st_residu(Ctx* c, BlockCtx* b, int level, int icycle, int m2 = 1, int part = 0) {
+  if (b->prm.iturb >= 3) return st_residu_sst(c, b, level, m2, icycle, part);
+  if (part != 2) {
+    if (level == 1) {
+      if (b->npatch) {
+        int maxn = 1;
+        for (auto& p : b->h_patch) maxn = max(maxn, (p.r1b - p.r1a + 1) * (p.r2b - p.r2a + 1));
+        k_refcen<<<dim3(nblk(maxn, 128), b->npatch), 128, 0, c->stream>>>(b->db, b->prm);
+        c->nlaunch++;
+      }
+    }
+    if (b->prm.fullns && level == 1) {
+      long ng = (long)(b->imax + 2) * (b->jmax + 2) * (b->kmax + 2);
+      k_grad<<<nblk(ng, 128), 128, 0, c->stream>>>(b->db, level);
       c->nlaunch++;
     }
-  }
-  if (b->prm.fullns && level == 1) {
-    long ng = (long)(b->imax + 2) * (b->jmax + 2) * (b->kmax + 2);
-    k_grad<<<nblk(ng, 128), 128, 0, c->stream>>>(b->db, level);
+    if (level == 1) launch_patch(c, b, k_inlet_outlet, icycle);
+    if (part == 1) return 0;
+    launch_residual(c->stream, b, level);
     c->nlaunch++;
   }
-  if (level == 1) launch_patch(c, b, k_inlet_outlet, icycle);
-  launch_residual(c->stream, b, level);
-  c->nlaunch++;
   if (b->prm.timel && level == 1) {   // TIMDER after SWEEP (res3c.f:705)
     k_timder<5><<<nblk((long)b->imax * b->jmax * b->kmax, 256), 256, 0, c->stream>>>(b->db, b->prm);
     c->nlaunch++;
   }
   return 0;
+}
+
+// The residual face pass of several level-1 blocks in one launch over their
+// tiles (k_residual_batch, RB_MAX blocks per launch); every block must have
+// the same equation count.  The tile shape is the first block's.
+template <int NV, int I_, int J_, int K_>
+void launch_residual_batch_t(cudaStream_t st, const ResBatch& rb, int level) {
+  const size_t sm = residual_fused_smem(NV, I_, J_, K_);
+  cudaFuncSetAttribute(k_residual_batch<NV, 512, I_, J_, K_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k_residual_batch<NV, 512, I_, J_, K_><<<rb.tile0[rb.nblk], 512, sm, st>>>(rb, level);
+}
+
+int launch_residual_batch(Ctx* c, const std::vector<BlockCtx*>& blks, int level) {
+  const int shape = blks[0]->res_shape;
+  const bool sst = blks[0]->prm.iturb >= 3;
+  const int ti = RES_SHAPES[shape][0], tj = RES_SHAPES[shape][1], tk = RES_SHAPES[shape][2];
+  for (size_t s0 = 0; s0 < blks.size(); s0 += RB_MAX) {
+    static ResBatch rb;   // ~19 KB: kept off the host stack
+    rb = ResBatch{};
+    rb.nblk = (int)min(blks.size() - s0, (size_t)RB_MAX);
+    rb.tile0[0] = 0;
+    for (int n = 0; n < rb.nblk; n++) {
+      const BlockCtx* b = blks[s0 + n];
+      if ((b->prm.iturb >= 3) != sst) return fail(c, FF_ERR_ARG, "batched residual: mixed equation counts");
+      rb.ntx[n] = nblk(b->imax, ti);
+      rb.nty[n] = nblk(b->jmax, tj);
+      rb.tile0[n + 1] = rb.tile0[n] + rb.ntx[n] * rb.nty[n] * nblk(b->kmax, tk);
+      rb.b[n] = b->db;
+      rb.p[n] = b->prm;
+    }
+    if (shape == 1) sst ? launch_residual_batch_t<7, 16, 8, 4>(c->stream, rb, level)
+                        : launch_residual_batch_t<5, 16, 8, 4>(c->stream, rb, level);
+    else if (shape == 2) sst ? launch_residual_batch_t<7, 8, 8, 8>(c->stream, rb, level)
+                             : launch_residual_batch_t<5, 8, 8, 8>(c->stream, rb, level);
+    else sst ? launch_residual_batch_t<7, 32, 4, 4>(c->stream, rb, level)
+             : launch_residual_batch_t<5, 32, 4, 4>(c->stream, rb, level);
+    c->nlaunch++;
+  }
+  CK(cudaGetLastError());
+  return 0;
+}
+
+// Batched face pass in the multi-block cycles unless FINFLO_RES_BATCH=0;
+// only with the fused 512-thread residual and one equation count.
+bool res_batch_ok(Ctx* c) {
+  static const bool env = [] { const char* e = getenv("FINFLO_RES_BATCH"); return !(e && !strcmp(e, "0")); }();
+  if (!env || !res_fused() || c->tops.size() < 2) return false;
+  const bool sst = c->tops[0]->prm.iturb >= 3;
+  if (res_threads(sst) != 512) return false;
+  for (auto* b : c->tops)
+    if ((b->prm.iturb >= 3) != sst) return false;
+  return true;
 }
 
 // Sweep-layout buffers in the block's LU-SGS precision (the other
@@ -705,7 +785,51 @@ int tune_ddadi(Ctx* c, BlockCtx* b, const TuneKey& key) {
   return 0;
 }
 
+// Residual tile shape of a block: each of RES_SHAPES timed on the block's
+// own level (CUDA events, after one untimed launch), the fastest kept;
+// cached per device, block shape and equation count.  FINFLO_RES_SHAPE
+// (0, 1, 2) fixes it.
+std::map<TuneKey, int> g_res_cache;
+
+int tune_residual(Ctx* c, BlockCtx* b) {
+  if (b->res_tuned) return 0;
+  b->res_tuned = 1;
+  static const int env = [] {
+    const char* e = getenv("FINFLO_RES_SHAPE");
+    return e ? atoi(e) : -1;
+  }();
+  if (env >= 0 && env < RES_NSHAPE) { b->res_shape = env; return 0; }
+  if (!res_fused() || res_threads(b->prm.iturb >= 3) != 512) return 0;
+  const TuneKey key{c->device, b->imax, b->jmax, b->kmax, (b->prm.iturb >= 3 ? 7 : 5) + 10 * b->level, 0, 0};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_res_cache.find(key);
+    if (it != g_res_cache.end()) { b->res_shape = it->second; return 0; }
+  }
+  float best = 1e30f;
+  int pick = 0;
+  for (int s = 0; s < RES_NSHAPE; s++) {
+    b->res_shape = s;
+    launch_residual(c->stream, b, b->level);
+    CK(cudaEventRecord(c->ev0, c->stream));
+    for (int r = 0; r < 3; r++) launch_residual(c->stream, b, b->level);
+    CK(cudaEventRecord(c->ev1, c->stream));
+    CK(cudaEventSynchronize(c->ev1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    if (ms < best) { best = ms; pick = s; }
+  }
+  b->res_shape = pick;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_res_cache[key] = pick;
+  return 0;
+}
+
 int tune_sweep(Ctx* c, BlockCtx* b) {
+  {
+    int rc = tune_residual(c, b);
+    if (rc) return rc;
+  }
   if (b->tuned) return 0;
   b->tuned = 1;
   const TuneKey key{c->device, b->imax, b->jmax, b->kmax, b->prm.iturb >= 3 ? 7 : 5, b->prm.lusgs_fp32 != 0,
@@ -910,15 +1034,21 @@ int one_cycle(Ctx* c, BlockCtx* b, int icycle) {
 // level, TRANSF, STATIM, RESIDI, FORCFU, ADDRES, IMPSDI, FIN; then INTERP
 // back up and REFLEC.  RESL2 of the level-1 residual after the fine update
 // is added to the context's sums; `own` (a single block) resets them here.
-int mg_body(Ctx* c, BlockCtx* b, int icycle, bool own) {
+// part: 0 all of it; 1 up to the level-1 residual's face pass (not
+// included); 2 from after that face pass on (launch_residual_batch runs the
+// face pass of all blocks in between).
+int mg_body(Ctx* c, BlockCtx* b, int icycle, bool own, int part = 0) {
   int rc;
   const int sst = b->prm.iturb >= 3;
-  if (own) {
-    k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi, c->d_dromax);
-    c->nlaunch++;
+  if (part != 2) {
+    if (own) {
+      k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi, c->d_dromax);
+      c->nlaunch++;
+    }
+    if (sst && (rc = st_statim(c, b, 1))) return rc;
   }
-  if (sst && (rc = st_statim(c, b, 1))) return rc;
-  if ((rc = st_residu(c, b, 1, icycle))) return rc;
+  if ((rc = st_residu(c, b, 1, icycle, 1, part))) return rc;
+  if (part == 1) return 0;
   if ((rc = st_imps(c, b, 1, false))) return rc;
   if ((rc = st_fin(c, b, 1))) return rc;
   std::vector<BlockCtx*> lv;
@@ -1116,11 +1246,22 @@ int mb_cycle(Ctx* c, int icycle) {
     if (b->coarse) return mb_mg_cycle(c, icycle);
   k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi, c->d_dromax);
   c->nlaunch++;
+  const bool batch = res_batch_ok(c);
+  if (batch) {   // the face pass of all blocks in one launch
+    rc = fork_join(c, nb, [&](int n) {
+      BlockCtx* b = c->tops[n];
+      int r;
+      if (b->prm.iturb >= 3 && (r = st_statim(c, b, 1))) return r;
+      return st_residu(c, b, 1, icycle, 1, 1);
+    });
+    if (rc) return rc;
+    if ((rc = launch_residual_batch(c, c->tops, 1))) return rc;
+  }
   rc = fork_join(c, nb, [&](int n) {
     BlockCtx* b = c->tops[n];
     int r;
-    if (b->prm.iturb >= 3 && (r = st_statim(c, b, 1))) return r;
-    if ((r = st_residu(c, b, 1, icycle))) return r;
+    if (!batch && b->prm.iturb >= 3 && (r = st_statim(c, b, 1))) return r;
+    if ((r = st_residu(c, b, 1, icycle, 1, batch ? 2 : 0))) return r;
     int ncell = b->imax * b->jmax * b->kmax;
     k_resl2<<<min(nblk(ncell, 256), 4 * c->sm_count), 256, 0, c->stream>>>(b->db, c->d_resi);
     c->nlaunch++;
@@ -1146,7 +1287,14 @@ int mb_mg_cycle(Ctx* c, int icycle) {
   int nb = (int)c->tops.size(), rc;
   k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi, c->d_dromax);
   c->nlaunch++;
-  rc = fork_join(c, nb, [&](int n) { return mg_body(c, c->tops[n], icycle, false); });
+  if (res_batch_ok(c)) {   // the level-1 face pass of all blocks in one launch
+    rc = fork_join(c, nb, [&](int n) { return mg_body(c, c->tops[n], icycle, false, 1); });
+    if (rc) return rc;
+    if ((rc = launch_residual_batch(c, c->tops, 1))) return rc;
+    rc = fork_join(c, nb, [&](int n) { return mg_body(c, c->tops[n], icycle, false, 2); });
+  } else {
+    rc = fork_join(c, nb, [&](int n) { return mg_body(c, c->tops[n], icycle, false); });
+  }
   if (rc) return rc;
   if ((rc = mb_boundi(c))) return rc;
   rc = fork_join(c, nb, [&](int n) {
@@ -1805,6 +1953,12 @@ int ff_lusgs_kind(void* ctx, int blk) {
     return b->dd_cfg[1] < 0 ? 4 : 4 + 100 * (1000 + 100 * b->dd_cfg[3] + 10 * b->dd_cfg[1] + b->dd_cfg[2]);
   if (b->use_pipe) return 3 + 100 * b->pg.ntj * b->pg.ntk;
   return b->use_lines ? 1 + b->lg.cs * 100 : 2 + b->coop_threads * 100;
+}
+
+int ff_residual_shape(void* ctx, int blk) {
+  BlockCtx* b = getb((Ctx*)ctx, blk);
+  if (!b) return -FF_ERR_ARG;
+  return b->res_shape;
 }
 
 int ff_cycle_launches(void* ctx, int blk) {

@@ -341,10 +341,36 @@ __global__ void k_grad(DevBlock b, int level) {
 
 // FLUXBL base3c.f:4085 (IDIFF = 1) for the face between M = L-S and L; the
 // result is the viscous part of the face flux (FRO untouched).
-FF_DI void visc_flux(const DevBlock& b, const ff_params& p, size_t L, int S, int dir, double f[5]) {
-  size_t M = L - S;
+// Face geometry both viscous face fluxes (FLUXBL, FLKEBL) read: the
+// interpolation weights from the cell thicknesses D1..D3, the unit vector s
+// between the two cell centres with its length and reciprocal, and the face's
+// unit normal and area.  Computed once per face.
+struct FaceGeom {
+  double w1, w2, sx, sy, sz, slen, rslen, nx, ny, nz, area;
+};
+
+FF_DI FaceGeom face_geom(const DevBlock& b, size_t L, int S, int dir) {
+#define LD(s, n) __ldg(b.a[s] + (n))
+  FaceGeom g;
+  const size_t M = L - S;
   const double* D = b.a[FF_D1 + dir - 1];
-  double w1 = 2.0 * (__ldg(D + L) / (__ldg(D + L) + __ldg(D + M))), w2 = 2.0 - w1;
+  g.w1 = 2.0 * (__ldg(D + L) / (__ldg(D + L) + __ldg(D + M)));
+  g.w2 = 2.0 - g.w1;
+  double sx = LD(FF_XC, L) - LD(FF_XC, M), sy = LD(FF_YC, L) - LD(FF_YC, M), sz = LD(FF_ZC, L) - LD(FF_ZC, M);
+  g.slen = sqrt(sx * sx + sy * sy + sz * sz) + 1.e-21;
+  g.rslen = rcp(g.slen);
+  g.sx = sx * g.rslen; g.sy = sy * g.rslen; g.sz = sz * g.rslen;
+  const int ao = 4 * (dir - 1);
+  g.nx = LD(FF_A1XA + ao, L); g.ny = LD(FF_A1YA + ao, L); g.nz = LD(FF_A1ZA + ao, L);
+  g.area = LD(FF_A1 + ao, L);
+#undef LD
+  return g;
+}
+
+FF_DI void visc_flux(const DevBlock& b, const ff_params& p, size_t L, int S, int dir, const FaceGeom& g,
+                     double f[5]) {
+  size_t M = L - S;
+  const double w1 = g.w1, w2 = g.w2;
   double w1p = .5 * w1, w2p = .5 * w2;
 #define LD(s, n) __ldg(b.a[s] + (n))
   double s11l = LD(FF_S11, L), s11m = LD(FF_S11, M), s22l = LD(FF_S22, L), s22m = LD(FF_S22, M);
@@ -364,15 +390,13 @@ FF_DI void visc_flux(const DevBlock& b, const ff_params& p, size_t L, int S, int
   double dtdxi = w2p * LD(FF_DTDX, L) + w1p * LD(FF_DTDX, M);
   double dtdyi = w2p * LD(FF_DTDY, L) + w1p * LD(FF_DTDY, M);
   double dtdzi = w2p * LD(FF_DTDZ, L) + w1p * LD(FF_DTDZ, M);
-  double sxi = LD(FF_XC, L) - LD(FF_XC, M), syi = LD(FF_YC, L) - LD(FF_YC, M), szi = LD(FF_ZC, L) - LD(FF_ZC, M);
-  double slen = sqrt(sxi * sxi + syi * syi + szi * szi) + 1.e-21;
-  sxi = sxi / slen; syi = syi / slen; szi = szi / slen;
-  double nx = LD(FF_A1XA + 4 * (dir - 1), L), ny = LD(FF_A1YA + 4 * (dir - 1), L), nz = LD(FF_A1ZA + 4 * (dir - 1), L);
-  double area = LD(FF_A1 + 4 * (dir - 1), L);
+  const double sxi = g.sx, syi = g.sy, szi = g.sz, rslen = g.rslen;
+  const double nx = g.nx, ny = g.ny, nz = g.nz, area = g.area;
   double alfa = sxi * nx + syi * ny + szi * nz;
   double surf = 0.5 * area * (LD(FF_EPS2, L) * LD(FF_VIS, L) + LD(FF_EPS2, M) * LD(FF_VIS, M));
-  double surfe = 0.5 * area * (LD(FF_CP, L) * LD(FF_VIST, L) / p.prt + LD(FF_CH, L)
-                               + LD(FF_CP, M) * LD(FF_VIST, M) / p.prt + LD(FF_CH, M));
+  const double rprt = rcp(p.prt);
+  double surfe = 0.5 * area * (LD(FF_CP, L) * LD(FF_VIST, L) * rprt + LD(FF_CH, L)
+                               + LD(FF_CP, M) * LD(FF_VIST, M) * rprt + LD(FF_CH, M));
   double ul = LD(FF_U, L), um = LD(FF_U, M), vl = LD(FF_V, L), vm = LD(FF_V, M), wl = LD(FF_W, L), wm = LD(FF_W, M);
   double duvwsj = nx * (dudx * sxi + dudy * syi + dudz * szi) + ny * (dvdx * sxi + dvdy * syi + dvdz * szi)
                 + nz * (dwdx * sxi + dwdy * syi + dwdz * szi);
@@ -381,10 +405,10 @@ FF_DI void visc_flux(const DevBlock& b, const ff_params& p, size_t L, int S, int
   double f4 = nx * s13i + ny * s23i + nz * s33i;
   if (alfa > 0.) {
     double adotu = nx * (ul - um) + ny * (vl - vm) + nz * (wl - wm);
-    double cc = adotu / slen - duvwsj;
-    f2 = alfa * ((ul - um) / slen - (sxi * dudx + syi * dudy + szi * dudz)) + sxi * cc + f2;
-    f3 = alfa * ((vl - vm) / slen - (sxi * dvdx + syi * dvdy + szi * dvdz)) + syi * cc + f3;
-    f4 = alfa * ((wl - wm) / slen - (sxi * dwdx + syi * dwdy + szi * dwdz)) + szi * cc + f4;
+    double cc = adotu * rslen - duvwsj;
+    f2 = alfa * ((ul - um) * rslen - (sxi * dudx + syi * dudy + szi * dudz)) + sxi * cc + f2;
+    f3 = alfa * ((vl - vm) * rslen - (sxi * dvdx + syi * dvdy + szi * dvdz)) + syi * cc + f3;
+    f4 = alfa * ((wl - wm) * rslen - (sxi * dwdx + syi * dwdy + szi * dwdz)) + szi * cc + f4;
   }
   const double R23 = .6666667;
   double dv = dudx + dvdy + dwdz;
@@ -393,9 +417,13 @@ FF_DI void visc_flux(const DevBlock& b, const ff_params& p, size_t L, int S, int
   f4 = surf * (f4 - R23 * nz * dv);
   double f5 = .5 * ((ul + um) * f2 + (vl + vm) * f3 + (wl + wm) * f4) + surfe * (dtdxi * nx + dtdyi * ny + dtdzi * nz);
   if (alfa > 0.)
-    f5 = surfe * alfa * ((LD(FF_TEMP, L) - LD(FF_TEMP, M)) / slen - sxi * dtdxi - syi * dtdyi - szi * dtdzi) + f5;
+    f5 = surfe * alfa * ((LD(FF_TEMP, L) - LD(FF_TEMP, M)) * rslen - sxi * dtdxi - syi * dtdyi - szi * dtdzi) + f5;
 #undef LD
   f[0] = 0.; f[1] = -f2; f[2] = -f3; f[3] = -f4; f[4] = -f5;
+}
+
+FF_DI void visc_flux(const DevBlock& b, const ff_params& p, size_t L, int S, int dir, double f[5]) {
+  visc_flux(b, p, L, S, dir, face_geom(b, L, S, dir), f);
 }
 
 // FLUXDO base3c.f:3677 (thin layer, IDIFF = 1): the viscous flux on coarse
@@ -1434,6 +1462,22 @@ FF_DI void lines_stage(CT* stg, int stride, const CT* __restrict__ sw, const CT*
   for (int v = 0; v < NV; v++) cp_async_ca(stg + (SW_N + v) * stride, dwp + v * ns + S);
 }
 
+FF_DI void prefetch_l2(const void* g) { asm volatile("prefetch.global.L2 [%0];\n" ::"l"(g)); }
+
+// The sweep data and right-hand side of one cell into L2 (the values
+// lines_stage copies, without a destination).
+template <typename CT, int NV>
+FF_DI void lines_prefetch_l2(const CT* __restrict__ sw, const CT* dwp, size_t ns, size_t S, int upper) {
+#pragma unroll
+  for (int c = 0; c < SW_N; c++) {
+    if (c == SW_FD && upper) continue;
+    if (NV == 5 && (c == SW_RO || c == SW_SC + 3 || c == SW_SC + 4)) continue;
+    prefetch_l2(sw + c * ns + S);
+  }
+#pragma unroll
+  for (int v = 0; v < NV; v++) prefetch_l2(dwp + v * ns + S);
+}
+
 // A lane's line in one tile slot of its CTA, with the DSMEM sources of its
 // j and k neighbours' products (offsets within one pub buffer).
 template <typename CT>
@@ -1576,6 +1620,19 @@ __global__ void __launch_bounds__(LTHREADS * (STAGE ? LMAX_TPC_STAGE : LMAX_TPC)
       int I;
       size_t S;
       if (plane_cell(s + 1, d0.J, d0.K, I, S)) lines_stage<CT, NV>(my, nthr, sw, dwp, ns, S, upper);
+    }
+    if (!STAGE && s + 1 < nplanes) {
+      // unstaged: pull the next plane's cells of every tile of the thread
+      // group into L2 (a hint: no registers or shared memory held)
+      for (int q = g0; q < tpc; q += ng) {
+        const int t = q * lg.cs + rank;
+        if (t >= lg.ntiles) break;
+        const int J = (t % lg.ntj) * LTJ + lj + 1, K = (t / lg.ntj) * LTK + lk + 1;
+        int I;
+        size_t S;
+        if (J > JMAX || K > KMAX || !plane_cell(s + 1, J, K, I, S)) continue;
+        lines_prefetch_l2<CT, NV>(sw, dwp, ns, S, upper);
+      }
     }
     cluster_wait_acquire();
   }

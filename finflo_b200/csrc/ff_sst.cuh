@@ -204,14 +204,16 @@ FF_DI void roe_flux_ke(const double q[7][4], double nx, double ny, double nz, do
   ppi = dmax(0.001 * p.frspre, ppi);
   roim = dmax(0.001 * p.frsden, roim);
   pmi = dmax(0.001 * p.frspre, pmi);
-  const double gm1 = p.gamma - 1.;
-  double eip = ppi / (gm1 * roip) - p.e0ref;
-  double eim = pmi / (gm1 * roim) - p.e0ref;
-  double elr = ppi / (gm1 * roim) - p.e0ref;
-  double erl = pmi / (gm1 * roip) - p.e0ref;
+  const double rgm1 = rcp(p.gamma - 1.);
+  const double ypror = rcp(roip), yprol = rcp(roim);
+  double eip = ppi * rgm1 * ypror - p.e0ref;
+  double eim = pmi * rgm1 * yprol - p.e0ref;
+  double elr = ppi * rgm1 * yprol - p.e0ref;
+  double erl = pmi * rgm1 * ypror - p.e0ref;
   double ypro1 = rcp(cr[2]), ypro2 = rcp(cl2[2]);
-  double dedph = 0.5 * ((-cr[0] / cr[1] - ypro1) + (-cl2[0] / cl2[1] - ypro2));
-  double dedrh = 0.5 * ((rcp(cr[1]) + cr[3] * (ypro1 * ypro1)) + (rcp(cl2[1]) + cl2[3] * (ypro2 * ypro2)));
+  double rdh1 = rcp(cr[1]), rdh2 = rcp(cl2[1]);
+  double dedph = 0.5 * ((-cr[0] * rdh1 - ypro1) + (-cl2[0] * rdh2 - ypro2));
+  double dedrh = 0.5 * ((rdh1 + cr[3] * (ypro1 * ypro1)) + (rdh2 + cl2[3] * (ypro2 * ypro2)));
   {
     double dpp = 2. * (ppi - pmi), drr = 2. * (roip - roim);
     if (fabs(dpp) >= 1.e-2 * (ppi + pmi)) dedph = (eip + elr - eim - erl) / dpp;
@@ -227,7 +229,6 @@ FF_DI void roe_flux_ke(const double q[7][4], double nx, double ny, double nz, do
   double wl = a31 * rmim + a32 * rnim + a33 * rwim;
   double rkipi = dmax(0.001 * p.rklim, rkip), reipi = dmax(0.001 * p.epslim, reip);
   double rkimi = dmax(0.001 * p.rklim, rkim), reimi = dmax(0.001 * p.epslim, reim);
-  double ypror = rcp(roip), yprol = rcp(roim);
   double rkr = rkipi * ypror, rkl = rkimi * yprol;
   double eir = eip + .5 * (ur * ur + vr * vr + wr * wr) + rkr;
   double eil = eim + .5 * (ul * ul + vl * vl + wl * wl) + rkl;
@@ -292,34 +293,30 @@ FF_DI void roe_flux_ke(const double q[7][4], double nx, double ny, double nz, do
 }
 
 // FLKEBL: k and omega diffusion of one face (I = high-side cell).
-FF_DI void flkebl_face(const DevBlock& b, size_t I, int S, int dir, double& frk, double& feps) {
+FF_DI void flkebl_face(const DevBlock& b, size_t I, int S, int dir, const FaceGeom& g, double& frk, double& feps) {
 #define LD(s, n) __ldg(b.a[s] + (n))
   size_t M = I - S;
-  const int ao = 4 * (dir - 1);
   double f1 = LD(FF_FUN1, I), onemf1 = dmax(0.0, 1.0 - f1);
   double psigk = f1 * SST_SIGRK1 + onemf1 * SST_SIGRK2;
   double psige = f1 * SST_SIGOM1 + onemf1 * SST_SIGOM2;
-  const double* D = b.a[FF_D1 + dir - 1];
-  double w1 = 2.0 * (__ldg(D + I) / (__ldg(D + I) + __ldg(D + M))), w2 = 2.0 - w1;
+  const double w1 = g.w1, w2 = g.w2;
   double dkdxi = 0.5 * (w2 * LD(FF_DKDX, I) + w1 * LD(FF_DKDX, M));
   double dkdyi = 0.5 * (w2 * LD(FF_DKDY, I) + w1 * LD(FF_DKDY, M));
   double dkdzi = 0.5 * (w2 * LD(FF_DKDZ, I) + w1 * LD(FF_DKDZ, M));
   double dedxi = 0.5 * (w2 * LD(FF_DEDX, I) + w1 * LD(FF_DEDX, M));
   double dedyi = 0.5 * (w2 * LD(FF_DEDY, I) + w1 * LD(FF_DEDY, M));
   double dedzi = 0.5 * (w2 * LD(FF_DEDZ, I) + w1 * LD(FF_DEDZ, M));
-  double sxi = LD(FF_XC, I) - LD(FF_XC, M), syi = LD(FF_YC, I) - LD(FF_YC, M), szi = LD(FF_ZC, I) - LD(FF_ZC, M);
-  double slen = sqrt(sxi * sxi + syi * syi + szi * szi) + 1.E-21;
-  sxi = sxi / slen; syi = syi / slen; szi = szi / slen;
-  double nx = LD(FF_A1XA + ao, I), ny = LD(FF_A1YA + ao, I), nz = LD(FF_A1ZA + ao, I);
+  const double sxi = g.sx, syi = g.sy, szi = g.sz, rslen = g.rslen;
+  const double nx = g.nx, ny = g.ny, nz = g.nz;
   double alfa = dmax(sxi * nx + syi * ny + szi * nz, 0.);
   double rmut2 = LD(FF_VIST, I) + LD(FF_VIST, M);
-  double vv = LD(FF_VIS, I) + LD(FF_VIS, M), area = LD(FF_A1 + ao, I);
+  double vv = LD(FF_VIS, I) + LD(FF_VIS, M), area = g.area;
   double surfk = 0.5 * area * (vv + rmut2 * psigk);
   double surfep = 0.5 * area * (vv + rmut2 * psige);
   double ypro1 = rcp(LD(FF_RO, I)), ypro2 = rcp(LD(FF_RO, M));
-  frk = -surfk * (alfa * (LD(FF_RK, I) * ypro1 - LD(FF_RK, M) * ypro2) / slen + dkdxi * (nx - alfa * sxi) +
+  frk = -surfk * (alfa * (LD(FF_RK, I) * ypro1 - LD(FF_RK, M) * ypro2) * rslen + dkdxi * (nx - alfa * sxi) +
                   dkdyi * (ny - alfa * syi) + dkdzi * (nz - alfa * szi));
-  feps = -surfep * (alfa * (LD(FF_REPS, I) * ypro1 - LD(FF_REPS, M) * ypro2) / slen + dedxi * (nx - alfa * sxi) +
+  feps = -surfep * (alfa * (LD(FF_REPS, I) * ypro1 - LD(FF_REPS, M) * ypro2) * rslen + dedxi * (nx - alfa * sxi) +
                     dedyi * (ny - alfa * syi) + dedzi * (nz - alfa * szi));
 #undef LD
 }
@@ -448,8 +445,9 @@ FF_DI void face_flux_ke(const DevBlock& b, const ff_params& p, int dir, size_t L
   if (m <= min(idi, nmax + 1)) {
     double frk, feps, fv[5], f4;
     if (level == 1 && p.fullns) {   // FLKEBL, SETV12, FLUXBL
-      flkebl_face(b, L, S, dir, frk, feps);
-      visc_flux(b, p, L, S, dir, fv);
+      const FaceGeom g = face_geom(b, L, S, dir);
+      flkebl_face(b, L, S, dir, g, frk, feps);
+      visc_flux(b, p, L, S, dir, g, fv);
       f4 = frk + fv[4];
     } else {                        // FLUDKE, FLUXDO
       fludke_face(b, L, S, dir, frk, feps);
@@ -527,14 +525,19 @@ __global__ void __launch_bounds__(NT, RES_MIN_CTAS * 128 / NT) k_residual_sst(De
 // 1/VOL, SWEEP res3c.f:992 / SWEEPK res3c.f:1342).  Against one barrier per
 // direction this balances the face work over the threads (8 rounds for the
 // 1808 faces at 256 threads, against 3 + 3 + 3) and drops two barriers.
-template <int NV, int NT>
-__global__ void __launch_bounds__(NT, RES_MIN_CTAS * 128 / NT) k_residual_fused(DevBlock b, ff_params p, int level) {
+//
+// The tile shape (TI_ x TJ_ x TK_ cells, 512 of them) is a template
+// parameter: 32x4x4, 16x8x4 and 8x8x8 trade i-direction coalescing against
+// the faces computed per cell (3.53, 3.44, 3.38); the autotuner picks one
+// per block shape.
+template <int NV, int NT, int TI_, int TJ_, int TK_>
+FF_DI void residual_tile(const DevBlock& b, const ff_params& p, int level, int i0, int j0, int k0,
+                         double* res_smem) {
+  constexpr int TI = TI_, TJ = TJ_, TK = TK_;
   constexpr int NFK = TI * TJ * (TK + 1), NFI = (TI + 1) * TJ * TK, NFJ = TI * (TJ + 1) * TK;
   constexpr int NFT = NFK + NFI + NFJ, NC = TI * TJ * TK;
-  extern __shared__ double res_smem[];
   double(*sF)[NFT] = reinterpret_cast<double(*)[NFT]>(res_smem);
   const int tid = threadIdx.x;
-  const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ, k0 = blockIdx.z * TK;
   for (int f = tid; f < NFT; f += NT) {
     int dir, l, ni, nj;
     if (f < NFK) { dir = 3; l = f; ni = TI; nj = TJ; }
@@ -570,9 +573,44 @@ __global__ void __launch_bounds__(NT, RES_MIN_CTAS * 128 / NT) k_residual_fused(
   }
 }
 
-inline size_t residual_fused_smem(int nv) {
-  return (size_t)nv * (TI * TJ * (TK + 1) + (TI + 1) * TJ * TK + TI * (TJ + 1) * TK) * sizeof(double);
+template <int NV, int NT, int TI_ = TI, int TJ_ = TJ, int TK_ = TK>
+__global__ void __launch_bounds__(NT, RES_MIN_CTAS * 128 / NT) k_residual_fused(DevBlock b, ff_params p, int level) {
+  extern __shared__ double res_smem[];
+  residual_tile<NV, NT, TI_, TJ_, TK_>(b, p, level, blockIdx.x * TI_, blockIdx.y * TJ_, blockIdx.z * TK_, res_smem);
 }
+
+// The same residual for several blocks in one launch: a block work-list of
+// tiles (north-star batching: one launch per stage over all blocks of
+// uneven size).  CTA t takes tile t of the concatenated lists; blocks and
+// their parameters travel in the kernel's parameter space.
+constexpr int RB_MAX = 16;
+struct ResBatch {
+  int nblk;
+  int tile0[RB_MAX + 1];   // first tile of each block, and the total
+  int ntx[RB_MAX], nty[RB_MAX];
+  DevBlock b[RB_MAX];
+  ff_params p[RB_MAX];
+};
+
+template <int NV, int NT, int TI_, int TJ_, int TK_>
+__global__ void __launch_bounds__(NT, RES_MIN_CTAS * 128 / NT)
+    k_residual_batch(const __grid_constant__ ResBatch rb, int level) {
+  extern __shared__ double res_smem[];
+  const int t = blockIdx.x;
+  int bi = 0;
+  while (bi + 1 < rb.nblk && t >= rb.tile0[bi + 1]) bi++;
+  const int l = t - rb.tile0[bi], nx = rb.ntx[bi], ny = rb.nty[bi];
+  const int ti = l % nx, tj = (l / nx) % ny, tk = l / (nx * ny);
+  residual_tile<NV, NT, TI_, TJ_, TK_>(rb.b[bi], rb.p[bi], level, ti * TI_, tj * TJ_, tk * TK_, res_smem);
+}
+
+inline size_t residual_fused_smem(int nv, int ti = TI, int tj = TJ, int tk = TK) {
+  return (size_t)nv * (ti * tj * (tk + 1) + (ti + 1) * tj * tk + ti * (tj + 1) * tk) * sizeof(double);
+}
+
+// The residual tile shapes the autotuner chooses from (cells in i, j, k).
+constexpr int RES_NSHAPE = 3;
+constexpr int RES_SHAPES[RES_NSHAPE][3] = {{32, 4, 4}, {16, 8, 4}, {8, 8, 8}};
 
 // SOURKO (KOVER=0, RANS, no rotation correction) + ADDSKE, interior cells.
 __global__ void k_sourko_addske(DevBlock b) {

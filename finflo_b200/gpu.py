@@ -92,6 +92,7 @@ def lib():
         L.ff_time_stage.argtypes = [vp, ci, ci, ci, ctypes.POINTER(ctypes.c_float)]
         L.ff_cycle_launches.argtypes = [vp, ci]
         L.ff_lusgs_kind.argtypes = [vp, ci]
+        L.ff_residual_shape.argtypes = [vp, ci]
         L.ff_sweep_tuning.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_float)]
         L.ff_sweep_times.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_float)]
         L.ff_host_register.argtypes = [vp, vp, ctypes.c_size_t]
@@ -343,6 +344,9 @@ class GpuSolver:
         ms = ctypes.c_float()
         self._check(self.L.ff_time_cycles(self.ctx, bid, n, ctypes.byref(ms)))
         return ms.value
+
+    def residual_shape(self, bid=0) -> str:
+        return ("32x4x4", "16x8x4", "8x8x8")[self.L.ff_residual_shape(self.ctx, bid)]
 
     def lusgs_kind(self, bid=0) -> int:
         return self.L.ff_lusgs_kind(self.ctx, bid)

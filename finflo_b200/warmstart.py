@@ -32,13 +32,57 @@ from dataclasses import dataclass, field
 import numpy as np
 
 CH = 32                # decoder channels
-ROOT = (4, 2, 2)       # root voxels in i, j, k
-LEVELS = 4             # 2x refinements: 4x2x2 -> 64x32x32
-NVAR = 5               # RO, RM, RN, RW, E
 OUT_PAD = 16           # output channels padded to the GEMM's N step
 IN_PAD = 16            # parameters padded to the GEMM's K step
-ENC = [IN_PAD, 64, 128, 256, CH * ROOT[0] * ROOT[1] * ROOT[2]]
-GRID = tuple(r << LEVELS for r in ROOT)   # cells: 64, 32, 32
+
+
+@dataclass(frozen=True)
+class Spec:
+    """A family of cases the network learns: the solver case built from the
+    parameters, the decoder's grid (root voxels refined `levels` times) and
+    the predicted variables (5 conservative, or 7 with k and omega)."""
+    name: str
+    root: tuple = (4, 2, 2)
+    levels: int = 4
+    nvar: int = 5
+    params: tuple = ("mach", "amp")
+    ranges: tuple = ((0.3, 0.8), (0.05, 0.15))
+    nodes: tuple = (65, 33, 33)
+    nlev: int = 1                       # solver multigrid levels
+    reynolds: float = 1e4
+    h1: float = 1e-3
+    noise: float = 1e-3
+    amp: float = 0.1                    # bump amplitude when it is not a parameter
+    inter: int = 3
+    cfl: float = 2.0
+    turbulence: str = None
+
+    @property
+    def grid(self):
+        return tuple(r << self.levels for r in self.root)
+
+    @property
+    def ncell(self):
+        g = self.grid
+        return g[0] * g[1] * g[2]
+
+    @property
+    def enc(self):
+        return [IN_PAD, 64, 128, 256, CH * self.root[0] * self.root[1] * self.root[2]]
+
+
+# the config-4 family: laminar bump channel 64x32x32, Mach and bump amplitude
+BUMP = Spec("laminar bump channel 64x32x32 cells, Re 1e4, Mach U[0.3,0.8], amplitude U[0.05,0.15]")
+# the SST bump channel of the V-cycle workload (128x64x64, first cell 2e-6,
+# Re 1e6, 3 levels, INTER=1, CFL 1) over a Mach sweep; predicts k and omega too
+SST = Spec("k-omega SST bump channel 128x64x64 cells, Re 1e6, first cell 2e-6, 3-level V-cycle, Mach U[0.5,0.7]",
+           root=(4, 2, 2), levels=5, nvar=7, params=("mach",), ranges=((0.5, 0.7),), nodes=(129, 65, 65), nlev=3,
+           reynolds=1e6, h1=2e-6, noise=1e-3, inter=1, cfl=1.0, turbulence="sst")
+
+# the config-4 family's sizes, kept as module constants
+ROOT, LEVELS, NVAR = BUMP.root, BUMP.levels, BUMP.nvar
+ENC = BUMP.enc
+GRID = BUMP.grid   # cells: 64, 32, 32
 
 
 def octree_order(root=ROOT, levels=LEVELS):
@@ -59,9 +103,13 @@ def octree_order(root=ROOT, levels=LEVELS):
     return (K * nj + J) * ni + I
 
 
-def conservative(blk):
-    """Interior (RO, RM, RN, RW, E) of a block as [cells, 5], i fastest."""
-    return np.stack([blk.interior(n).ravel() for n in ("RO", "RM", "RN", "RW", "E")], axis=1)
+QVARS = ("RO", "RM", "RN", "RW", "E", "RK", "REPS")
+
+
+def conservative(blk, nvar=5):
+    """Interior (RO, RM, RN, RW, E[, RK, REPS]) of a block as [cells, nvar],
+    i fastest."""
+    return np.stack([blk.interior(n).ravel() for n in QVARS[:nvar]], axis=1)
 
 
 def freestream_scales(fs, gamma=1.4, rgas=287.05287):
@@ -76,19 +124,29 @@ def state_from_conservative(q, fs, gamma=1.4, rgas=287.05287):
     """Solver state (TEMP, U, V, W, PDIFF) of conservative values q [cells, 5]
     for a perfect gas (PERFGA: e = R T / (gamma - 1), p = rho R T), with the
     density and temperature kept above a fraction of the free stream's;
-    PDIFF is the pressure minus the free stream's (FRSPRE)."""
+    PDIFF is the pressure minus the free stream's (FRSPRE).  With q
+    [cells, 7] (k and omega in columns 5, 6: rho k, rho omega) the internal
+    energy excludes k, as CONSVA's E includes it, and RK, REPS are added."""
     ro = np.maximum(q[:, 0], 0.2 * fs["rho"])
     u, v, w = q[:, 1] / ro, q[:, 2] / ro, q[:, 3] / ro
     e = q[:, 4] / ro - 0.5 * (u * u + v * v + w * w)
+    if q.shape[1] >= 7:
+        e = e - q[:, 5] / ro
     T = np.maximum(e * (gamma - 1.0) / rgas, 0.2 * fs["t"])
     p = ro * rgas * T
-    return {"TEMP": T, "U": u, "V": v, "W": w, "PDIFF": p - fs["p"]}
+    st = {"TEMP": T, "U": u, "V": v, "W": w, "PDIFF": p - fs["p"]}
+    if q.shape[1] >= 7:
+        st["RK"], st["REPS"] = q[:, 5], q[:, 6]
+    return st
 
 
-def normalise_params(mach, amp, mach_range=(0.3, 0.8), amp_range=(0.05, 0.15)):
-    x = np.zeros((len(mach), IN_PAD), dtype=np.float32)
-    x[:, 0] = 2.0 * (np.asarray(mach) - mach_range[0]) / (mach_range[1] - mach_range[0]) - 1.0
-    x[:, 1] = 2.0 * (np.asarray(amp) - amp_range[0]) / (amp_range[1] - amp_range[0]) - 1.0
+def normalise_params(*cols, spec=BUMP):
+    """[n, IN_PAD] float32: each parameter column mapped from its range to
+    [-1, 1] (normalise_params(mach, amp) for the config-4 family)."""
+    n = len(cols[0])
+    x = np.zeros((n, IN_PAD), dtype=np.float32)
+    for c, (col, (lo, hi)) in enumerate(zip(cols, spec.ranges)):
+        x[:, c] = 2.0 * (np.asarray(col) - lo) / (hi - lo) - 1.0
     return x
 
 
@@ -106,9 +164,10 @@ class Layer:
     boff: int = 0     # bias offset
 
 
-def layers():
-    L = [Layer(f"enc{i + 1}", ENC[i + 1], ENC[i], 1 if i < 3 else 0) for i in range(4)]
-    for lv in range(LEVELS):
+def layers(spec=BUMP):
+    enc = spec.enc
+    L = [Layer(f"enc{i + 1}", enc[i + 1], enc[i], 1 if i < 3 else 0) for i in range(4)]
+    for lv in range(spec.levels):
         L.append(Layer(f"up{lv + 1}", 8 * CH, CH, 1))
         L.append(Layer(f"mix{lv + 1}", CH, CH, 1))
     L.append(Layer("out", OUT_PAD, CH, 0))
@@ -127,18 +186,19 @@ class WarmStartNet:
     holds the memory; every GEMM, activation gradient, reduction and the
     Adam update run in libfinflo_nn.so."""
 
-    def __init__(self, device="cuda", seed=0):
+    def __init__(self, device="cuda", seed=0, spec=BUMP):
         import torch
         from . import nn
         self.torch, self.nn = torch, nn
+        self.spec = spec
         self.dev = torch.device(device)
-        self.L, self.nparam = layers()
+        self.L, self.nparam = layers(spec)
         g = torch.Generator().manual_seed(seed)
         w = torch.zeros(self.nparam)
         for l in self.L:   # Kaiming-uniform weights for SiLU layers, zero biases
             bound = math.sqrt(6.0 / l.k) if l.act else math.sqrt(3.0 / l.k)
             if l.name == "enc1":
-                bound = math.sqrt(6.0 / 2)   # two real inputs, the rest is padding
+                bound = math.sqrt(6.0 / len(spec.params))   # the real inputs; the rest is padding
             w[l.off:l.off + l.n * l.k] = (torch.rand(l.n * l.k, generator=g) * 2 - 1) * bound
         self.w = w.to(self.dev)
         self.g = torch.zeros_like(self.w)
@@ -184,11 +244,12 @@ class WarmStartNet:
         for l in self.L[:4]:
             self.z[l.name] = torch.empty(B, l.n, dtype=f32, device=d)
             self.h[l.name] = torch.empty(B, l.n, dtype=b16, device=d)
-        V = B * ROOT[0] * ROOT[1] * ROOT[2]
+        root = self.spec.root
+        V = B * root[0] * root[1] * root[2]
         self.rows = {}
         prev = self.h["enc4"].view(V, CH)
         self.inp = {}
-        for lv in range(LEVELS):
+        for lv in range(self.spec.levels):
             up, mix = f"up{lv + 1}", f"mix{lv + 1}"
             self.inp[up] = prev
             self.z[up] = torch.empty(V, 8 * CH, dtype=f32, device=d)
@@ -211,14 +272,14 @@ class WarmStartNet:
         self.dA = torch.empty(big, dtype=f32, device=d)
         self.dB = torch.empty(big, dtype=f32, device=d)
         self.dzb = torch.empty(big, dtype=b16, device=d)
-        self.tA = torch.empty(max(big, ENC[-1] * _r16(B)), dtype=b16, device=d)
-        self.tB = torch.empty(max(big, ENC[-1] * _r16(B)), dtype=b16, device=d)
+        self.tA = torch.empty(max(big, self.spec.enc[-1] * _r16(B)), dtype=b16, device=d)
+        self.tB = torch.empty(max(big, self.spec.enc[-1] * _r16(B)), dtype=b16, device=d)
         self.loss = torch.zeros(1, dtype=f32, device=d)
 
     # -- forward ------------------------------------------------------------------
     def forward(self, x):
         """x: [B, IN_PAD] float32 (normalised parameters) -> self.pred
-        [B * 65536, OUT_PAD] in octree order."""
+        [B * ncell, OUT_PAD] in octree order."""
         nn = self.nn
         B = x.shape[0]
         self._alloc(B)
@@ -249,9 +310,13 @@ class WarmStartNet:
         ks = max(64, (rp + splits - 1) // splits + 63) // 64 * 64
         nn.gemm(a, b, zf=self.gW(l), atomic=True, ksplit=ks)
 
-    def backward(self, tgt):
+    def backward(self, tgt, capture=None):
         """Gradients of the mean-squared error of self.pred against tgt
-        [B * 65536, NVAR] (normalised targets, octree order) into self.g."""
+        [B * ncell, nvar] (normalised targets, octree order) into self.g.
+        capture (a dict): receives per layer copies of the tensors its
+        backward step consumed -- the BF16 pre-activation gradient (dzb),
+        the FP32 one (dzf) and the BF16 layer input (x) -- and the input
+        gradient it produced (dx, FP32), for layer-by-layer checks."""
         nn, torch = self.nn, self.torch
         self.g.zero_()
         self.loss.zero_()
@@ -275,10 +340,14 @@ class WarmStartNet:
                     dzf = dy
             self._wgrad(l, dzb, x, rows)
             nn.colsum(dzf, self.gb(l))
+            if capture is not None:
+                capture[l.name] = {"dzb": dzb.clone(), "dzf": dzf.clone(), "x": x.reshape(rows, l.k).clone()}
             if l.name == "enc1":
                 break
             dx = bufA[:rows * l.k].view(rows, l.k)
             nn.gemm(dzb, self.WT(l), zf=dx)
+            if capture is not None:
+                capture[l.name]["dx"] = dx.clone()
             dy = dx
         return self.loss
 
@@ -294,7 +363,7 @@ class WarmStartNet:
         nn.adam(self.w[sl], self.g[sl], self.m[sl], self.v[sl], self.step_n, lr)
 
     def train(self, X, T, steps=2000, batch=16, lr=2e-3, seed=0, log_every=100):
-        """X: [n, IN_PAD] float32, T: [n, 65536, NVAR] float32 (device).
+        """X: [n, IN_PAD] float32, T: [n, ncell, nvar] float32 (device).
         Adam with a cosine learning-rate decay; returns [(step, loss)]."""
         torch = self.torch
         gen = torch.Generator().manual_seed(seed)
@@ -304,7 +373,7 @@ class WarmStartNet:
         for s in range(steps):
             idx = torch.randperm(n, generator=gen)[:batch].to(self.dev)
             self.forward(X[idx])
-            self.backward(T[idx].reshape(-1, NVAR))
+            self.backward(T[idx].reshape(-1, self.spec.nvar))
             lr_s = lr * (0.05 + 0.95 * 0.5 * (1.0 + math.cos(math.pi * s / steps)))
             self.adam(lr_s)
             if (s + 1) % log_every == 0 or s == steps - 1:
@@ -313,10 +382,11 @@ class WarmStartNet:
         return hist
 
     def predict(self, X):
-        """[n, 65536, NVAR] float32 (normalised, octree order)."""
+        """[n, ncell, nvar] float32 (normalised, octree order)."""
         self.forward(X)
         self.nn.error()
-        return self.pred[:, :NVAR].reshape(X.shape[0], -1, NVAR)
+        nv = self.spec.nvar
+        return self.pred[:, :nv].reshape(X.shape[0], -1, nv)
 
     def state_dict(self):
         return {"w": self.w.detach().cpu().numpy()}
@@ -328,22 +398,27 @@ class WarmStartNet:
 
 # ---- solver side: training data, prediction as a start, time to tolerance ----
 
-CASE = dict(nodes=(65, 33, 33), reynolds=1e4, h1=1e-3, noise=1e-3)
 
-
-def sample_params(n, seed, mach_range=(0.3, 0.8), amp_range=(0.05, 0.15)):
+def sample_params(n, seed, spec=BUMP):
+    """[n, nparams] seeded uniform draws over the family's ranges (for the
+    config-4 family: columns Mach, amplitude)."""
     rng = np.random.default_rng(seed)
-    return rng.uniform(*mach_range, size=n), rng.uniform(*amp_range, size=n)
+    return np.stack([rng.uniform(lo, hi, size=n) for lo, hi in spec.ranges], axis=1)
 
 
-def make_case(mach, amp, seed=0, lusgs_fp32=False, ddadi=False, **kw):
+def make_case(pv, seed=0, lusgs_fp32=False, ddadi=False, spec=BUMP):
+    """The family's case at parameter values pv: (levels, prms, fs)."""
     from . import case
-    c = dict(CASE, **kw)
-    levels, prms, fs = case.bump_case_mg(*c["nodes"], nlev=1, mach=float(mach), amp=float(amp),
-                                         reynolds=c["reynolds"], h1=c["h1"], noise=c["noise"], seed=seed,
-                                         lusgs_fp32=lusgs_fp32)
-    prms[0].ddadi = int(ddadi)
-    return levels[0], prms[0], fs
+    kw = dict(zip(spec.params, [float(x) for x in pv]))
+    levels, prms, fs = case.bump_case_mg(*spec.nodes, nlev=spec.nlev, mach=kw.get("mach", 0.5),
+                                         amp=kw.get("amp", spec.amp), reynolds=spec.reynolds, h1=spec.h1,
+                                         noise=spec.noise, seed=seed, inter=spec.inter, cfl=spec.cfl,
+                                         cfll=spec.cfl, lusgs_fp32=lusgs_fp32, coarse_fp32=lusgs_fp32,
+                                         turbulence=spec.turbulence)
+    for q in prms:
+        q.ddadi = int(ddadi)
+        q.predgs_full = 1
+    return levels, prms, fs
 
 
 @dataclass
@@ -351,26 +426,33 @@ class Run:
     cycles: int
     seconds: float
     hist: np.ndarray            # per-cycle sum of squares of the density residual
-    q: np.ndarray = field(default=None, repr=False)   # final conservative interior [cells, 5]
+    q: np.ndarray = field(default=None, repr=False)   # final interior targets [cells, nvar]
 
 
-def solve(mach, amp, cycles, init=None, tol=None, chunk=None, seed=0, keep_q=True, lusgs_fp32=False, ddadi=False):
-    """Run the solver on one case for `cycles` cycles, or until the density
-    residual's sum of squares is <= tol; init = solver state (TEMP, U, V,
-    W, PDIFF) of the interior cells to start from instead of the free
-    stream; lusgs_fp32 runs the implicit stage in FP32, ddadi selects the
-    DDADI implicit stage (LUSGS=0) instead of LU-SGS.  Wall time covers
-    the cycles only (device synchronised)."""
+def solve(pv, cycles, init=None, tol=None, chunk=None, seed=0, keep_q=True, lusgs_fp32=False, ddadi=False,
+          spec=BUMP):
+    """Run the solver on the family's case at parameters pv for `cycles`
+    cycles, or until the density residual's sum of squares is <= tol; init =
+    solver state (TEMP, U, V, W, PDIFF[, RK, REPS]) of the fine interior
+    cells to start from instead of the free stream; lusgs_fp32 runs every
+    level's implicit stage in FP32, ddadi selects the DDADI implicit stage
+    (LUSGS=0) instead of LU-SGS.  Wall time covers the cycles only (device
+    synchronised)."""
     from .gpu import GpuSolver
-    blk, prm, fs = make_case(mach, amp, seed=seed, lusgs_fp32=lusgs_fp32, ddadi=ddadi)
+    levels, prms, fs = make_case(pv, seed=seed, lusgs_fp32=lusgs_fp32, ddadi=ddadi, spec=spec)
+    blk = levels[0]
     if init is not None:
         for n, v in init.items():
             blk.interior(n)[:] = v.reshape(blk.kmax, blk.jmax, blk.imax)
+        if "RK" in init:   # the start-up's *OLD copies of k and omega
+            blk.arrays["RKOLD"][:] = blk.arrays["RK"]
+            blk.arrays["EPSOLD"][:] = blk.arrays["REPS"]
     chunk = chunk or (10 if tol is not None else 200)   # cycles per graph replay between residual checks
     g = GpuSolver(0)
     try:
-        bid = g.add_block(blk, prm)
-        g.upload(bid)
+        bid = g.add_levels(levels, prms) if len(levels) > 1 else g.add_block(blk, prms[0])
+        for q in range(len(levels)):
+            g.upload(bid + q)
         g.start(bid)
         g.sync()
         hs = []
@@ -392,9 +474,9 @@ def solve(mach, amp, cycles, init=None, tol=None, chunk=None, seed=0, keep_q=Tru
         sec = time.perf_counter() - t0
         q = None
         if keep_q:
-            d = g.download(bid, ["RO", "RM", "RN", "RW", "E"])
+            d = g.download(bid, list(QVARS[:spec.nvar]))
             q = np.stack([d[k].reshape(blk.kmax + 4, blk.jmax + 4, blk.imax + 4)[2:-2, 2:-2, 2:-2].ravel()
-                          for k in ("RO", "RM", "RN", "RW", "E")], axis=1)
+                          for k in QVARS[:spec.nvar]], axis=1)
         return Run(n, sec, np.concatenate(hs), q)
     finally:
         g.close()
@@ -402,64 +484,114 @@ def solve(mach, amp, cycles, init=None, tol=None, chunk=None, seed=0, keep_q=Tru
 
 class Dataset:
     """Normalised training targets in octree order and the statistics that
-    undo the normalisation."""
+    undo the normalisation.  The conservative variables are scaled by each
+    case's free-stream values; k and omega (7-variable families) enter as
+    log(rho k / rho k_inf) and log(rho omega / rho omega_inf), which span
+    the many decades between the wall and the free stream."""
 
-    def __init__(self, mach, amp, qs):
-        from .case import FlowConditions
-        self.perm = octree_order()
-        self.mach, self.amp = np.asarray(mach), np.asarray(amp)
+    def __init__(self, P, qs, spec=BUMP):
+        from .case import FlowConditions, sst_freestream
+        self.spec = spec
+        self.perm = octree_order(spec.root, spec.levels)
+        self.P = np.asarray(P, dtype=float).reshape(len(qs), -1)
         sc = []
-        for m in self.mach:
-            fc = FlowConditions(mach=float(m), reynolds=CASE["reynolds"])
-            sc.append(freestream_scales(fc.freestream(), fc.gamma, fc.rgas))
+        for pv in self.P:
+            fc, fs = self._fc(pv)
+            s5 = freestream_scales(fs, fc.gamma, fc.rgas)
+            if spec.nvar >= 7:
+                rk, re = sst_freestream(fs)
+                s5 = np.concatenate([s5, [rk, re]])
+            sc.append(s5)
         self.scales = np.array(sc)
-        y = np.stack([q[self.perm] / s for q, s in zip(qs, self.scales)])    # [n, 65536, 5]
+        y = np.stack([self._fwd(q[self.perm], s) for q, s in zip(qs, self.scales)])    # [n, ncell, nvar]
         self.mean = y.mean(axis=0)
-        sd = (y - self.mean).reshape(-1, NVAR).std(axis=0)
+        sd = (y - self.mean).reshape(-1, spec.nvar).std(axis=0)
         sd[3] = sd[2]                       # RW on the scale of RN
         self.std = np.maximum(sd, 1e-6)[None, :] * np.ones_like(self.mean)
         self.y = ((y - self.mean) / self.std).astype(np.float32)
-        self.x = normalise_params(self.mach, self.amp)
+        self.x = normalise_params(*self.P.T, spec=spec)
 
-    def to_state(self, pred, mach, amp):
-        """Solver state of one prediction ([65536, 5] normalised, octree
-        order) for the case (mach, amp)."""
+    def _fc(self, pv):
         from .case import FlowConditions
-        fc = FlowConditions(mach=float(mach), reynolds=CASE["reynolds"])
-        fs = fc.freestream()
-        q = np.empty((len(self.perm), NVAR))
-        q[self.perm] = (pred * self.std + self.mean) * freestream_scales(fs, fc.gamma, fc.rgas)
-        return state_from_conservative(q, fs, fc.gamma, fc.rgas)
+        kw = dict(zip(self.spec.params, pv))
+        fc = FlowConditions(mach=float(kw.get("mach", 0.5)), reynolds=self.spec.reynolds)
+        return fc, fc.freestream()
+
+    def _fwd(self, q, s):
+        y = q / s
+        if self.spec.nvar >= 7:
+            y[:, 5:7] = np.log(np.maximum(y[:, 5:7], 1e-30))
+        return y
+
+    def to_state(self, pred, pv):
+        """Solver state of one prediction ([ncell, nvar] normalised, octree
+        order) for the case at parameters pv."""
+        fc, fs = self._fc(pv)
+        s = freestream_scales(fs, fc.gamma, fc.rgas)
+        y = pred * self.std + self.mean
+        q = np.empty((len(self.perm), self.spec.nvar))
+        if self.spec.nvar >= 7:
+            from .case import sst_freestream
+            rk, re = sst_freestream(fs)
+            q[self.perm, :5] = y[:, :5] * s
+            # k and omega kept inside the limits the solver itself applies:
+            # LOLIM's free-stream floor (RKLIM, EPSLIM) and SUBIN's cap
+            # RKMAX = FRSDEN FRSVEL^2 on rho k (ns3c.f:9742)
+            q[self.perm, 5] = np.clip(np.exp(np.minimum(y[:, 5], 50.0)) * rk, rk, fs["rho"] * fs["u"] ** 2)
+            q[self.perm, 6] = np.maximum(np.exp(np.minimum(y[:, 6], 60.0)) * re, re)
+        else:
+            q[self.perm] = y * s
+        st = state_from_conservative(q, fs, fc.gamma, fc.rgas)
+        # temperature and velocity inside the bounds the update limits keep
+        # (TLOLIM / TUPLIM = 0.05 / 6 x FRSTEM) and twice the free-stream speed
+        st["TEMP"] = np.minimum(st["TEMP"], 6.0 * fs["t"])
+        vmax = 2.0 * fs["u"]
+        for n in ("U", "V", "W"):
+            st[n] = np.clip(st[n], -vmax, vmax)
+        return st
 
 
-def evaluate(net, data, mach, amp, tol_decades=2.0, max_cycles=3000, lusgs_fp32=True, ddadi_arms=False):
-    """For each case: cycles and wall time to a residual tolerance from the
-    free stream with the plain FP64 solver, and from the network's
-    prediction with the chosen implicit precision.  The tolerance is
-    tol_decades below the free-stream start's first-cycle density residual
-    (L2 norm), the same absolute level for both starts.  A prediction that
-    does not reach it within max_cycles is reported as such: the plain
-    solver stays the fallback.  ddadi_arms adds the same two runs with the
-    DDADI implicit stage (LUSGS=0): FP64 from the free stream and FP32 from
-    the prediction."""
+def evaluate(net, data, P, tol_decades=2.0, max_cycles=3000, lusgs_fp32=True, ddadi_arms=False, spec=BUMP):
+    """For each held-out case (rows of P): cycles and wall time to a residual
+    tolerance
+    * from the free stream with the plain FP64 solver (base),
+    * from the free stream with the FP32 implicit stage (free32: what the
+      precision form alone gains),
+    * from the network's prediction with the FP32 implicit stage (warm).
+    The tolerance is tol_decades below the free-stream start's first-cycle
+    density residual (L2 norm), the same absolute level for every arm.  A
+    run that does not reach it within max_cycles is reported as such: the
+    plain solver stays the fallback.  ddadi_arms adds FP64 from the free
+    stream and FP32 from the prediction with the DDADI implicit stage
+    (LUSGS=0)."""
     import torch
     out = []
-    for m, a in zip(mach, amp):
-        first = solve(m, a, 1, keep_q=False)
+    for pv in np.asarray(P).reshape(len(P), -1):
+        first = solve(pv, 1, keep_q=False, spec=spec)
         tol = first.hist[0] * 10.0 ** (-2.0 * tol_decades)
-        base = solve(m, a, max_cycles, tol=tol, keep_q=False)
+        base = solve(pv, max_cycles, tol=tol, keep_q=False, spec=spec)
+        free32 = solve(pv, max_cycles, tol=tol, keep_q=False, lusgs_fp32=lusgs_fp32, spec=spec)
         t0 = time.perf_counter()
-        pred = net.predict(torch.as_tensor(normalise_params([m], [a])).to(net.dev))[0].cpu().numpy()
-        st = data.to_state(pred, m, a)
+        pred = net.predict(torch.as_tensor(normalise_params(*[[x] for x in pv], spec=spec)).to(net.dev))
+        st = data.to_state(pred[0].cpu().numpy(), pv)
         t_inf = time.perf_counter() - t0
-        warm = solve(m, a, max_cycles, init=st, tol=tol, keep_q=False, lusgs_fp32=lusgs_fp32)
-        e = dict(mach=float(m), amp=float(a), tol=float(tol),
+        warm = solve(pv, max_cycles, init=st, tol=tol, keep_q=False, lusgs_fp32=lusgs_fp32, spec=spec)
+        warm_reached = bool(np.isfinite(warm.hist).all() and warm.hist.min() <= tol)
+        warm_cycles, warm_s = warm.cycles, warm.seconds + t_inf
+        if not warm_reached:
+            # the plain solver is the fallback: a start that fails costs its
+            # own cycles plus the free-stream run (FP32 implicit stage)
+            warm_cycles += free32.cycles
+            warm_s += free32.seconds
+        e = dict(params=[float(x) for x in pv], tol=float(tol),
                  base_cycles=base.cycles, base_s=base.seconds, base_reached=bool(base.hist.min() <= tol),
-                 warm_cycles=warm.cycles, warm_s=warm.seconds + t_inf, warm_reached=bool(warm.hist.min() <= tol),
-                 warm_start_decades=float(0.5 * np.log10(first.hist[0] / warm.hist[0])))
+                 free32_cycles=free32.cycles, free32_s=free32.seconds,
+                 free32_reached=bool(free32.hist.min() <= tol),
+                 warm_cycles=warm_cycles, warm_s=warm_s, warm_reached=warm_reached, fallback=not warm_reached,
+                 warm_start_decades=float(0.5 * np.log10(first.hist[0] / warm.hist[0])), infer_s=t_inf)
         if ddadi_arms:
-            dbase = solve(m, a, max_cycles, tol=tol, keep_q=False, ddadi=True)
-            dwarm = solve(m, a, max_cycles, init=st, tol=tol, keep_q=False, lusgs_fp32=True, ddadi=True)
+            dbase = solve(pv, max_cycles, tol=tol, keep_q=False, ddadi=True, spec=spec)
+            dwarm = solve(pv, max_cycles, init=st, tol=tol, keep_q=False, lusgs_fp32=True, ddadi=True, spec=spec)
             e.update(ddadi_base_cycles=dbase.cycles, ddadi_base_s=dbase.seconds,
                      ddadi_base_reached=bool(dbase.hist.min() <= tol),
                      ddadi_warm_cycles=dwarm.cycles, ddadi_warm_s=dwarm.seconds + t_inf,
@@ -469,31 +601,38 @@ def evaluate(net, data, mach, amp, tol_decades=2.0, max_cycles=3000, lusgs_fp32=
 
 
 def run_config(ntrain=64, ntest=16, cycles=2000, steps=6000, batch=16, lr=1e-3, tol_decades=2.0, seed_train=3,
-               seed_test=4, log=print, ddadi_arms=False):
-    """The learned-warm-start workload: solve ntrain seeded (Mach, amplitude)
-    points for `cycles` cycles as training data, train the network, then
-    evaluate the ntest held-out points.  Returns a summary dict."""
+               seed_test=4, log=print, ddadi_arms=False, spec=BUMP, max_cycles=None):
+    """The learned-warm-start workload: solve ntrain seeded parameter points
+    for `cycles` cycles as training data, train the network, then evaluate
+    the ntest held-out points.  Returns a summary dict."""
     import torch
     t0 = time.perf_counter()
-    mtr, atr = sample_params(ntrain, seed=seed_train)
-    mte, ate = sample_params(ntest, seed=seed_test)
-    runs = [solve(m, a, cycles) for m, a in zip(mtr, atr)]
+    Ptr = sample_params(ntrain, seed=seed_train, spec=spec)
+    Pte = sample_params(ntest, seed=seed_test, spec=spec)
+    runs = [solve(pv, cycles, spec=spec) for pv in Ptr]
     t_data = time.perf_counter() - t0
     log(f"training data: {ntrain} solves x {cycles} cycles in {t_data:.1f} s")
-    data = Dataset(mtr, atr, [r.q for r in runs])
-    net = WarmStartNet(seed=0)
+    data = Dataset(Ptr, [r.q for r in runs], spec=spec)
+    net = WarmStartNet(seed=0, spec=spec)
     X, T = torch.as_tensor(data.x).to(net.dev), torch.as_tensor(data.y).to(net.dev)
     t1 = time.perf_counter()
     hist = net.train(X, T, steps=steps, batch=batch, lr=lr, log_every=max(1, steps // 10))
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t1
     log(f"training: {steps} steps in {t_train:.1f} s, loss {hist}")
-    ev = evaluate(net, data, mte, ate, tol_decades=tol_decades, max_cycles=max(3000, cycles), ddadi_arms=ddadi_arms)
+    ev = evaluate(net, data, Pte, tol_decades=tol_decades, max_cycles=max_cycles or max(3000, cycles),
+                  ddadi_arms=ddadi_arms, spec=spec)
     base_s = sum(e["base_s"] for e in ev)
     warm_s = sum(e["warm_s"] for e in ev)
-    out = dict(cases=ev, base_s=base_s, warm_s=warm_s, speedup=base_s / warm_s,
+    free32_s = sum(e["free32_s"] for e in ev)
+    out = dict(cases=ev, base_s=base_s, warm_s=warm_s, free32_s=free32_s, speedup=base_s / warm_s,
+               network_gain=free32_s / warm_s,
                base_cycles=sum(e["base_cycles"] for e in ev), warm_cycles=sum(e["warm_cycles"] for e in ev),
-               loss=hist, t_data=t_data, t_train=t_train, steps=steps, ntrain=ntrain, ntest=ntest, cycles=cycles)
+               free32_cycles=sum(e["free32_cycles"] for e in ev),
+               all_reached=all(e["base_reached"] and e["warm_reached"] and e["free32_reached"] for e in ev),
+               fallbacks=sum(e["fallback"] for e in ev),
+               loss=hist, t_data=t_data, t_train=t_train, steps=steps, ntrain=ntrain, ntest=ntest, cycles=cycles,
+               family=spec.name, tol_decades=tol_decades)
     if ddadi_arms:
         for k in ("ddadi_base_s", "ddadi_warm_s", "ddadi_base_cycles", "ddadi_warm_cycles"):
             out[k] = sum(e[k] for e in ev)

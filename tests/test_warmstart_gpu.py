@@ -1,6 +1,7 @@
-"""The warm-start network on the GPU: its forward pass and gradients against
-torch autograd on the same BF16 weights, and what the trained network gains
-over the free-stream start (solver cycles to the same residual tolerance)."""
+"""The warm-start network on the GPU: its loss and gradients against an FP64
+CPU restatement with the same BF16 rounding points, and what the trained
+network gains over the free-stream start (solver cycles to the same residual
+tolerance, with the same FP32 implicit stage, so the gain is the network's)."""
 import numpy as np
 import pytest
 
@@ -16,61 +17,126 @@ def ws():
     return m
 
 
-def _torch_reference(net, x, tgt):
-    """The same network in torch FP32 autograd, rounding to BF16 where the
-    kernels store BF16 (GEMM operands); returns the loss and the flat
-    gradient in the layout of net.g."""
-    import torch.nn.functional as F
-    w = net.w.detach().clone().requires_grad_(True)
-    bf = lambda t: t.to(torch.bfloat16).float()
-
-    def b(l):
-        return w[l.boff:l.boff + l.n]
-
-    # straight-through BF16 rounding of the weights: the gradient w.r.t. the
-    # rounded weight is the gradient w.r.t. the master weight
-    def Wst(l):
-        m = w[l.off:l.off + l.n * l.k].view(l.n, l.k)
-        return m + (bf(m) - m).detach()
-
-    def rnd(t):
-        return t + (bf(t) - t).detach()
-
-    h = rnd(x.float())
-    for l in net.L[:4]:
-        z = h @ Wst(l).T + b(l)
-        h = rnd(F.silu(z) if l.act else z)
-    a = h.reshape(-1, net.L[4].k)
-    for l in net.L[4:-1]:
-        z = a @ Wst(l).T + b(l)
-        a = rnd(F.silu(z)).reshape(-1, net.L[4].k if l.name.startswith("up") else l.n)
-    lo = net.L[-1]
-    pred = a @ Wst(lo).T + b(lo)
-    loss = ((pred[:, :tgt.shape[1]] - tgt) ** 2).mean()
-    loss.backward()
-    return loss.item(), w.grad
+def _bf16(a):
+    """Round to BF16 (nearest even) through FP32, as the kernels store it."""
+    f = np.asarray(a, dtype=np.float32)
+    u = f.view(np.uint32).astype(np.uint64)
+    u = ((u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000).astype(np.uint32)
+    return u.view(np.float32).astype(np.float64)
 
 
-def test_forward_and_gradients_match_torch(ws):
+def _cpu_reference(net, x, tgt):
+    """The network's loss and flat gradient in FP64 on the CPU, rounding to
+    BF16 exactly where the kernels store BF16: the input, every activation
+    that feeds a GEMM, the weights, and the pre-activation gradients that
+    feed the weight and input-gradient GEMMs (the bias gradients sum the
+    unrounded copy).  Straight-through: the gradient of a rounded weight is
+    the master weight's."""
+    w = net.w.detach().cpu().numpy().astype(np.float64)
+    L = net.L
+    W = {l.name: _bf16(w[l.off:l.off + l.n * l.k].reshape(l.n, l.k)) for l in L}
+    b = {l.name: w[l.boff:l.boff + l.n] for l in L}
+    sig = lambda z: 1.0 / (1.0 + np.exp(-z))
+    f32 = lambda a: np.asarray(a, dtype=np.float32).astype(np.float64)   # FP32 storage points
+    ins, zs = {}, {}
+    h = _bf16(x.cpu().numpy())
+    for l in L:
+        if not l.name.startswith("enc"):
+            h = h.reshape(-1, l.k)   # octree order: a voxel's 8 children are the next 8 rows
+        ins[l.name] = h
+        z = f32(h @ W[l.name].T + b[l.name])
+        zs[l.name] = z
+        if l.name != "out":
+            h = _bf16(z * sig(z) if l.act else z)
+    pred = zs["out"]
+    t = tgt.cpu().numpy().astype(np.float64)
+    nv = t.shape[1]
+    diff = pred[:, :nv] - t
+    loss = (diff ** 2).mean()
+    g = np.zeros_like(w)
+    dpred = np.zeros_like(pred)
+    dpred[:, :nv] = 2.0 * diff / diff.size
+    dy = None
+    for l in reversed(L):
+        if l.name == "out":
+            dzf = dpred
+        else:
+            dy = dy.reshape(-1, l.n)
+            z = zs[l.name]
+            if l.act:
+                s_ = sig(z)
+                dzf = dy * s_ * (1.0 + z * (1.0 - s_))
+            else:
+                dzf = dy
+        dzb = _bf16(dzf)
+        g[l.off:l.off + l.n * l.k] = (dzb.T @ ins[l.name]).ravel()
+        g[l.boff:l.boff + l.n] = dzf.sum(axis=0)
+        if l.name == "enc1":
+            break
+        dy = f32(dzb @ W[l.name])
+    return loss, g
+
+
+def test_each_layer_backward_matches_fp64_on_its_own_inputs(ws):
+    """Every layer's backward kernels on the GPU's own inputs to that layer
+    (its BF16 input activations and pre-activation gradients, captured in
+    the backward pass) against FP64 products on the CPU: the weight
+    gradient dz^T x, the bias gradient sum(dz) and the input gradient
+    dz W, each within 1e-5 (relative norm) -- FP32 accumulation only."""
     net = ws.WarmStartNet(seed=1)
     g = torch.Generator().manual_seed(2)
-    x = torch.zeros(2, ws.IN_PAD)
-    x[:, :2] = torch.rand(2, 2, generator=g) * 2 - 1
+    x = torch.zeros(4, ws.IN_PAD)
+    x[:, :2] = torch.rand(4, 2, generator=g) * 2 - 1
     x = x.cuda()
-    tgt = torch.randn(2 * 65536, ws.NVAR, generator=g).cuda()
+    tgt = torch.randn(4 * 65536, ws.NVAR, generator=g).cuda()
+    net.forward(x)
+    cap = {}
+    net.backward(tgt, capture=cap)
+    torch.cuda.synchronize()
+    net.nn.error()
+    f64 = lambda t: t.float().cpu().numpy().astype(np.float64)
+    w = net.w.detach().cpu().numpy().astype(np.float64)
+    gg = net.g.detach().cpu().numpy().astype(np.float64)
+    rel = lambda a, r: np.linalg.norm(a - r) / (np.linalg.norm(r) + 1e-300)
+    for l in net.L:
+        c = cap[l.name]
+        dzb, dzf, xin = f64(c["dzb"]), f64(c["dzf"]), f64(c["x"])
+        gw = gg[l.off:l.off + l.n * l.k].reshape(l.n, l.k)
+        assert rel(gw, dzb.T @ xin) <= 1e-5, (l.name, "weights")
+        assert rel(gg[l.boff:l.boff + l.n], dzf.sum(axis=0)) <= 1e-5, (l.name, "bias")
+        if "dx" in c:
+            wb = _bf16(w[l.off:l.off + l.n * l.k].reshape(l.n, l.k))
+            assert rel(f64(c["dx"]), dzb @ wb) <= 1e-5, (l.name, "input gradient")
+
+
+def test_forward_and_gradients_match_the_cpu_fp64_reference(ws):
+    """Loss and every layer's weight and bias gradient end to end against an
+    FP64 CPU restatement with the same BF16 rounding points: within 1e-3
+    (relative norm per layer) for the layers whose weight gradients sum over
+    4,096 or more rows.  The encoder and the first decoder levels sum over
+    8 to 512 rows, so the few BF16 roundings that the FP32 and FP64 upstream
+    values send to different sides show: 1e-2 there (the layer-by-layer test
+    above checks those kernels to 1e-5 on their own inputs)."""
+    net = ws.WarmStartNet(seed=1)
+    g = torch.Generator().manual_seed(2)
+    B = 8   # the encoder layers' weight gradients sum over the batch rows
+    x = torch.zeros(B, ws.IN_PAD)
+    x[:, :2] = torch.rand(B, 2, generator=g) * 2 - 1
+    x = x.cuda()
+    tgt = torch.randn(B * 65536, ws.NVAR, generator=g).cuda()
     net.forward(x)
     loss = net.backward(tgt).item()
     torch.cuda.synchronize()
     net.nn.error()
-    ref_loss, ref_g = _torch_reference(net, x, tgt)
-    assert abs(loss - ref_loss) <= 2e-3 * ref_loss
-    # per layer: BF16 gradients of the activations -> a few per cent
+    ref_loss, ref_g = _cpu_reference(net, x, tgt)
+    assert abs(loss - ref_loss) <= 1e-4 * ref_loss
+    got = net.g.detach().cpu().numpy().astype(np.float64)
+    rows = {"enc1": 8, "enc2": 8, "enc3": 8, "enc4": 8, "up1": 8 * 16, "mix1": 8 * 128, "up2": 8 * 128}
     for l in net.L:
-        a = net.g[l.off:l.off + l.n * l.k]
-        r = ref_g[l.off:l.off + l.n * l.k]
-        assert (a - r).norm().item() <= 5e-2 * r.norm().item() + 1e-12, l.name
-        a, r = net.g[l.boff:l.boff + l.n], ref_g[l.boff:l.boff + l.n]
-        assert (a - r).norm().item() <= 5e-2 * r.norm().item() + 1e-12, l.name + " bias"
+        for sl, what in ((slice(l.off, l.off + l.n * l.k), "weights"), (slice(l.boff, l.boff + l.n), "bias")):
+            a, r = got[sl], ref_g[sl]
+            rel = np.linalg.norm(a - r) / (np.linalg.norm(r) + 1e-300)
+            assert rel <= (1e-2 if rows.get(l.name, 4096) < 4096 else 1e-3), (l.name, what, rel)
 
 
 def test_warm_start_beats_the_free_stream(ws):
@@ -86,3 +152,5 @@ def test_warm_start_beats_the_free_stream(ws):
     assert all(c["base_reached"] for c in r["cases"])
     assert all(c["warm_start_decades"] > 0.3 for c in r["cases"])   # the prediction starts closer
     assert r["warm_cycles"] < r["base_cycles"]
+    # the network's own gain: the same FP32 implicit stage from the free stream
+    assert r["warm_cycles"] < r["free32_cycles"]
