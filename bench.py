@@ -711,7 +711,7 @@ WARM_NAME = ("learned warm start: bump channel 64x32x32 cells, laminar Re=1e4, M
              "amplitude U[0.05,0.15]; 64 solver solutions (seed 3) train a 4-layer MLP encoder + 3-D "
              "transposed-conv decoder (32 channels, BF16 weights, tcgen05 GEMMs); 16 held-out points (seed 4)")
 WARM_SST_NAME = ("learned warm start: k-omega SST bump channel 128x64x64 cells (first cell 2e-6, Re=1e6), 3-level "
-                 "V-cycle, INTER=1, CFL 1, Mach U[0.5,0.7]; solver solutions (seed 3) train the network (5 "
+                 "V-cycle, INTER=1, CFL 1, Mach U[0.5,0.65]; solver solutions (seed 3) train the network (5 "
                  "refinement levels, k and omega as logs); held-out Mach points (seed 4); FP64 LU-SGS from the "
                  "free stream vs FP32 LU-SGS (every level) from the free stream and from the prediction")
 

@@ -1418,9 +1418,13 @@ __global__ void k_time_levels(DevBlock b, int nv, int mode) {
 // footprint keeps more CTAs resident.  The published values are
 // double-buffered, so a plane reads only the previous plane's outputs.
 // ---------------------------------------------------------------------------
-constexpr int LTJ = 16, LTK = 8, LTHREADS = LTJ * LTK;
-constexpr int LMAX_TPC = 4;          // tile groups per CTA (threads per CTA <= 512)
-constexpr int LMAX_TPC_STAGE = 2;    // staged: <= 256 threads, so up to 255 registers a thread
+// 16x4-line tiles (two warps, each 16 consecutive J of two K rows, so a
+// warp's sweep-layout loads are two 128-byte runs): a 16-CTA cluster then
+// holds up to 160 tiles in one pass (10 per CTA, 640 threads), enough for
+// the ~9,000 i-lines of a 2.4M-cell block.
+constexpr int LTJ = 16, LTK = 4, LTHREADS = LTJ * LTK;
+constexpr int LMAX_TPC = 10;         // tile groups per CTA (threads per CTA <= 640)
+constexpr int LMAX_TPC_STAGE = 4;    // staged: <= 256 threads, so up to 255 registers a thread
 constexpr int LSTAGE = SW_N + 7;     // staged values per thread: sweep data + right-hand side
 
 struct LineGeom {

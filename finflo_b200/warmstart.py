@@ -74,9 +74,12 @@ class Spec:
 # the config-4 family: laminar bump channel 64x32x32, Mach and bump amplitude
 BUMP = Spec("laminar bump channel 64x32x32 cells, Re 1e4, Mach U[0.3,0.8], amplitude U[0.05,0.15]")
 # the SST bump channel of the V-cycle workload (128x64x64, first cell 2e-6,
-# Re 1e6, 3 levels, INTER=1, CFL 1) over a Mach sweep; predicts k and omega too
-SST = Spec("k-omega SST bump channel 128x64x64 cells, Re 1e6, first cell 2e-6, 3-level V-cycle, Mach U[0.5,0.7]",
-           root=(4, 2, 2), levels=5, nvar=7, params=("mach",), ranges=((0.5, 0.7),), nodes=(129, 65, 65), nlev=3,
+# Re 1e6, 3 levels, INTER=1, CFL 1) over a subsonic Mach sweep around its
+# M = 0.6; predicts k and omega too.  (From M ~ 0.69 on, a supersonic pocket
+# forms over the bump; predicted starts there diverged and the plain solver
+# took over, so the family stops at 0.65.)
+SST = Spec("k-omega SST bump channel 128x64x64 cells, Re 1e6, first cell 2e-6, 3-level V-cycle, Mach U[0.5,0.65]",
+           root=(4, 2, 2), levels=5, nvar=7, params=("mach",), ranges=((0.5, 0.65),), nodes=(129, 65, 65), nlev=3,
            reynolds=1e6, h1=2e-6, noise=1e-3, inter=1, cfl=1.0, turbulence="sst")
 
 # the config-4 family's sizes, kept as module constants
