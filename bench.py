@@ -746,7 +746,8 @@ def run_warmstart(args):
         "network_gain": r["network_gain"], "all_reached": r["all_reached"],
         "cycles": {"plain_fp64_free_stream": r["base_cycles"], "fp32_lusgs_free_stream": r["free32_cycles"],
                    "fp32_lusgs_warm_start": r["warm_cycles"]},
-        "training": {"data_s": r["t_data"], "train_s": r["t_train"], "loss": r["loss"]},
+        "training": {"data_s": r["t_data"], "train_s": r["t_train"], "loss": r["loss"], "solves_kept": r["ntrain"],
+                     "solves_not_converged": r["dropped"]},
         "cases": r["cases"],
         "e2e": {"value": r["warm_s"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }

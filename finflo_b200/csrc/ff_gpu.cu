@@ -452,13 +452,24 @@ int lines_sweep(Ctx* c, BlockCtx* b, int upper, bool fp32) {
   cfg.blockDim = dim3(LTHREADS * b->lg.ng);
   cfg.dynamicSmemBytes = lines_smem_bytes(nv, b->lg.tpc, fp32 ? sizeof(float) : sizeof(double), stage);
   cfg.stream = c->stream;
-  cudaLaunchAttribute attr[1];
+  cudaLaunchAttribute attr[2];
   attr[0].id = cudaLaunchAttributeClusterDimension;
   attr[0].val.clusterDim.x = b->lg.cs;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
+  static const int prio = [] {
+    const char* e = getenv("FINFLO_SWEEP_PRIO");
+    int lo = 0, hi = 0;
+    if (!e || !strcmp(e, "0") || cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess) return 1;
+    return hi;
+  }();
+  if (c->side_by_side && prio <= 0) {   // side by side: the sweeps' CTAs first
+    attr[1].id = cudaLaunchAttributePriority;
+    attr[1].val.priority = prio;
+    cfg.numAttrs = 2;
+  }
   cudaError_t e;
   if (nv == 7)
     e = fp32 ? launch_lines<float, 7>(&cfg, b, b->sw32, b->dwp32, upper, stage)
@@ -557,6 +568,107 @@ int setup_lines(Ctx* c, BlockCtx* b) {
   b->can_lines = 0;
   return 0;
 }
+// ---- all blocks' line sweeps in one launch ----------------------------------
+// The blocks of one multigrid level, swept together by k_lusgs_lines_batch:
+// one cluster per block, every cluster of the launch the same size (the
+// smallest of the blocks' own), so a block with a larger own cluster gets
+// more tiles per CTA.  Returns false when a block cannot be swept this way.
+struct LinesBatchShape {
+  int cs = 0, threads = 0;
+  size_t smem = 0;
+};
+
+bool lines_batch_shape(Ctx* c, const std::vector<BlockCtx*>& v, size_t elem, LinesBatchShape& sh,
+                       std::vector<LineGeom>* geoms = nullptr) {
+  sh = LinesBatchShape{};
+  int cs = 16;
+  for (auto* b : v) {
+    if (!b->can_lines || b->prm.ddadi) return false;
+    cs = min(cs, b->lg.cs);
+  }
+  if (geoms) geoms->clear();
+  int ng_max = 1;
+  for (auto* b : v) {
+    LineGeom g = b->lg;
+    if (g.cs != cs) {
+      g.cs = cs;
+      g.tpc = (g.ntiles + cs - 1) / cs;
+      g.ng = min(g.tpc, LMAX_TPC);
+    }
+    const int nv = b->prm.iturb >= 3 ? 7 : 5;
+    sh.smem = max(sh.smem, lines_smem_bytes(nv, g.tpc, elem, false));
+    ng_max = max(ng_max, g.ng);
+    if (geoms) geoms->push_back(g);
+  }
+  sh.cs = cs;
+  sh.threads = LTHREADS * ng_max;
+  return sh.smem <= (size_t)c->smem_optin;
+}
+
+int g_lb_smem[kMaxDev][4];   // dynamic shared memory granted to k_lusgs_lines_batch<f64|f32, 5|7>
+
+template <typename CT, int NV>
+int lines_batch_launch(Ctx* c, const std::vector<BlockCtx*>& v, int upper) {
+  const bool fp32 = sizeof(CT) == 4;
+  for (size_t s0 = 0; s0 < v.size(); s0 += LB_MAX) {
+    std::vector<BlockCtx*> part(v.begin() + s0, v.begin() + min(v.size(), s0 + LB_MAX));
+    LinesBatchShape sh;
+    std::vector<LineGeom> geoms;
+    if (!lines_batch_shape(c, part, sizeof(CT), sh, &geoms))
+      return fail(c, FF_ERR_ARG, "batched line sweep: a block does not fit");
+    int& granted = g_lb_smem[c->device][(fp32 ? 1 : 0) + (NV == 7 ? 2 : 0)];
+    if ((int)sh.smem > granted) {
+      CK(cudaFuncSetAttribute(k_lusgs_lines_batch<CT, NV>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+      CK(cudaFuncSetAttribute(k_lusgs_lines_batch<CT, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)sh.smem));
+      granted = (int)sh.smem;
+    }
+    static LinesBatch lb;   // ~15 KB: kept off the host stack
+    lb = LinesBatch{};
+    lb.n = (int)part.size();
+    for (int n = 0; n < lb.n; n++) {
+      BlockCtx* b = part[n];
+      lb.upper[n] = upper ? (b->prm.predgs_full ? 3 : 1) : 0;
+      lb.lg[n] = geoms[n];
+      lb.sw[n] = fp32 ? (const void*)b->sw32 : (const void*)b->sw;
+      lb.dwp[n] = fp32 ? (void*)b->dwp32 : (void*)b->dwp;
+      lb.b[n] = b->db;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(lb.n * sh.cs);
+    cfg.blockDim = dim3(sh.threads);
+    cfg.dynamicSmemBytes = sh.smem;
+    cfg.stream = c->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = sh.cs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, k_lusgs_lines_batch<CT, NV>, lb);
+    if (e != cudaSuccess) return fail(c, FF_ERR_CUDA, "batched line sweep launch", e);
+    c->nlaunch++;
+  }
+  return 0;
+}
+
+// One sweep (upper = 1: PREDGS order, 0: CORRGS) of every block of v, one
+// launch per equation count and precision.
+int lines_batch(Ctx* c, const std::vector<BlockCtx*>& v, int upper) {
+  for (int nv : {5, 7})
+    for (int fp32 : {0, 1}) {
+      std::vector<BlockCtx*> g;
+      for (auto* b : v)
+        if ((b->prm.iturb >= 3 ? 7 : 5) == nv && (b->prm.lusgs_fp32 != 0) == (fp32 != 0)) g.push_back(b);
+      if (g.empty()) continue;
+      int rc = nv == 7 ? (fp32 ? lines_batch_launch<float, 7>(c, g, upper) : lines_batch_launch<double, 7>(c, g, upper))
+                       : (fp32 ? lines_batch_launch<float, 5>(c, g, upper) : lines_batch_launch<double, 5>(c, g, upper));
+      if (rc) return rc;
+    }
+  return 0;
+}
+
 // ---- pipelined tile wavefront (k_lusgs_pipe) ------------------------------
 template <typename CT, int NV, int TK, bool ST>
 cudaError_t pipe_launch(cudaLaunchConfig_t* cfg, BlockCtx* b, const CT* sw, CT* dwp, int upper, int* err) {
@@ -964,7 +1076,10 @@ int ddadi_sweeps(Ctx* c, BlockCtx* b, int only_dir) {
   return 0;
 }
 
-int st_imps(Ctx* c, BlockCtx* b, int level, bool divide_cp) {
+// IMPS (imps3.f:6) in three parts: the time step and COPR before the
+// sweeps, the sweeps, and the increments out of the sweep layout (plus
+// DRO/CP for a standalone IMPS) after them.
+void st_imps_pre(Ctx* c, BlockCtx* b, int level) {
   int ncell = b->imax * b->jmax * b->kmax;
   double cfl = level == 1 ? b->prm.cfl : b->prm.cfll;
   if (b->prm.iturb >= 3) {   // TIME3, then LOCDTK + IMSOKO + COPRKE
@@ -975,6 +1090,28 @@ int st_imps(Ctx* c, BlockCtx* b, int level, bool divide_cp) {
     k_time3_copr<<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->prm, cfl);
     c->nlaunch++;
   }
+}
+
+void st_sweep_out(Ctx* c, BlockCtx* b) {
+  int ncell = b->imax * b->jmax * b->kmax;
+  if (b->prm.lusgs_fp32)
+    k_sweep_out<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->dwp32, b->prm.iturb >= 3 ? 7 : 5);
+  else
+    k_sweep_out<double><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->dwp, b->prm.iturb >= 3 ? 7 : 5);
+  c->nlaunch++;
+}
+
+void st_imps_post(Ctx* c, BlockCtx* b, bool divide_cp) {
+  if (divide_cp) {
+    // standalone IMPS: finish with DRO/CP (imps3.f:483); the fused cycle
+    // folds this division into the FIN kernel instead
+    k_fin_divide<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db, b->prm.iturb >= 3);
+    c->nlaunch++;
+  }
+}
+
+int st_imps(Ctx* c, BlockCtx* b, int level, bool divide_cp) {
+  st_imps_pre(c, b, level);
   bool fp32 = b->prm.lusgs_fp32 != 0;
   int rc;
   if (b->prm.ddadi) {
@@ -984,18 +1121,9 @@ int st_imps(Ctx* c, BlockCtx* b, int level, bool divide_cp) {
     if ((rc = sweep(c, b, 1, fp32))) return rc;
     sweep_coef(c, b, 0, fp32);
     if ((rc = sweep(c, b, 0, fp32))) return rc;
-    if (fp32)
-      k_sweep_out<float><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->dwp32, b->prm.iturb >= 3 ? 7 : 5);
-    else
-      k_sweep_out<double><<<nblk(ncell, 128), 128, 0, c->stream>>>(b->db, b->dwp, b->prm.iturb >= 3 ? 7 : 5);
-    c->nlaunch++;
+    st_sweep_out(c, b);
   }
-  if (divide_cp) {
-    // standalone IMPS: finish with DRO/CP (imps3.f:483); the fused cycle
-    // folds this division into the FIN kernel instead
-    k_fin_divide<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(b->db, b->prm.iturb >= 3);
-    c->nlaunch++;
-  }
+  st_imps_post(c, b, divide_cp);
   return 0;
 }
 
@@ -1215,6 +1343,158 @@ int fork_join(Ctx* c, int nb, F fn) {
   return rc;
 }
 
+// fn(n) for n < cnt on side streams, forked from and joined back into the
+// context stream, with no sweep inside (the lockstep cycle's per-block
+// stages between its batched sweeps).
+template <typename F>
+int fork_n(Ctx* c, int cnt, F fn) {
+  if (cnt <= 1) return cnt == 1 ? fn(0) : 0;
+  cudaStream_t main = c->stream;
+  CK(cudaEventRecord(c->fork_ev, main));
+  int rc = 0;
+  c->side_by_side = true;
+  for (int n = 0; n < cnt && !rc; n++) {
+    CK(cudaStreamWaitEvent(c->side[n], c->fork_ev, 0));
+    c->stream = c->side[n];
+    rc = fn(n);
+    c->stream = main;
+    CK(cudaEventRecord(c->side_ev[n], c->side[n]));
+  }
+  c->side_by_side = false;
+  c->stream = main;
+  for (int n = 0; n < cnt; n++) CK(cudaStreamWaitEvent(main, c->side_ev[n], 0));
+  return rc;
+}
+
+// Multi-block cycles in lockstep (the reference's order: each stage of
+// CYCLES over all blocks, ns3c.f:1400-2130) with every level's LU-SGS sweeps
+// as one batched launch, with FINFLO_MB_LOCKSTEP=1.  Needs the cluster line
+// sweep on every block and level.  Not the default: the per-block branches
+// overlap one block's latency-bound sweeps (16 SMs each) with the other
+// blocks' residual work, which lockstep cannot (8-block SST case,
+// 512x256x128 cells: 64.2 ms per V-cycle as branches, 71.8 ms in lockstep).
+bool ls_ok(Ctx* c) {
+  const char* env = getenv("FINFLO_MB_LOCKSTEP");
+  const char* kind = getenv("FINFLO_LUSGS");
+  if (!env || strcmp(env, "1") || (kind && strcmp(kind, "lines")) || c->tops.size() < 2) return false;
+  std::vector<std::vector<BlockCtx*>> lv;
+  for (auto* t : c->tops) {
+    size_t m = 0;
+    for (BlockCtx* x = t; x; x = x->coarse, m++) {
+      if (lv.size() <= m) lv.resize(m + 1);
+      lv[m].push_back(x);
+    }
+  }
+  for (auto& v : lv) {
+    LinesBatchShape sh;
+    for (size_t s0 = 0; s0 < v.size(); s0 += LB_MAX) {
+      std::vector<BlockCtx*> part(v.begin() + s0, v.begin() + min(v.size(), s0 + LB_MAX));
+      if (!lines_batch_shape(c, part, sizeof(double), sh)) return false;
+    }
+  }
+  return true;
+}
+
+// IMPS of the blocks v (one level) in lockstep: both sweeps batched.
+int ls_imps(Ctx* c, const std::vector<BlockCtx*>& v, int level, bool divide_cp) {
+  const int n = (int)v.size();
+  int rc = fork_n(c, n, [&](int i) {
+    st_imps_pre(c, v[i], level);
+    sweep_coef(c, v[i], 1, v[i]->prm.lusgs_fp32 != 0);
+    return 0;
+  });
+  if (rc || (rc = lines_batch(c, v, 1))) return rc;
+  rc = fork_n(c, n, [&](int i) {
+    sweep_coef(c, v[i], 0, v[i]->prm.lusgs_fp32 != 0);
+    return 0;
+  });
+  if (rc || (rc = lines_batch(c, v, 0))) return rc;
+  return fork_n(c, n, [&](int i) {
+    st_sweep_out(c, v[i]);
+    st_imps_post(c, v[i], divide_cp);
+    return 0;
+  });
+}
+
+// mg_body of every level-1 block in lockstep, stage by stage in mg_body's
+// order within each block.
+int mb_mg_body_ls(Ctx* c, int icycle) {
+  std::vector<BlockCtx*>& tops = c->tops;
+  const int nb = (int)tops.size();
+  const bool rbatch = res_batch_ok(c);
+  int rc = fork_n(c, nb, [&](int n) {
+    BlockCtx* b = tops[n];
+    int r;
+    if (b->prm.iturb >= 3 && (r = st_statim(c, b, 1))) return r;
+    return st_residu(c, b, 1, icycle, 1, rbatch ? 1 : 0);
+  });
+  if (rc) return rc;
+  if (rbatch && (rc = launch_residual_batch(c, tops, 1))) return rc;
+  if (rbatch && (rc = fork_n(c, nb, [&](int n) { return st_residu(c, tops[n], 1, icycle, 1, 2); }))) return rc;
+  if ((rc = ls_imps(c, tops, 1, false))) return rc;
+  if ((rc = fork_n(c, nb, [&](int n) { return st_fin(c, tops[n], 1); }))) return rc;
+  std::vector<std::vector<BlockCtx*>> chain(nb);
+  size_t nlev = 0;
+  for (int n = 0; n < nb; n++) {
+    for (BlockCtx* x = tops[n]; x; x = x->coarse) chain[n].push_back(x);
+    nlev = max(nlev, chain[n].size());
+  }
+  for (size_t m = 1; m < nlev; m++) {
+    std::vector<BlockCtx*> fs, cs;
+    for (int n = 0; n < nb; n++)
+      if (chain[n].size() > m) { fs.push_back(chain[n][m - 1]); cs.push_back(chain[n][m]); }
+    rc = fork_n(c, (int)fs.size(), [&](int n) {
+      BlockCtx *f = fs[n], *cc = cs[n];
+      const int sst = f->prm.iturb >= 3;
+      int r;
+      st_statim(c, f, 1);
+      if ((r = st_residu(c, f, (int)m, icycle, (int)m + 1))) return r;
+      if (m == 1) {   // RESL2 of the level-1 residual after the fine update
+        int ncell = f->imax * f->jmax * f->kmax;
+        k_resl2<<<min(nblk(ncell, 256), 4 * c->sm_count), 256, 0, c->stream>>>(f->db, c->d_resi);
+        c->nlaunch++;
+      } else {
+        k_forcing<<<nblk(f->ntot, 256), 256, 0, c->stream>>>(f->db, 1, sst);
+        c->nlaunch++;
+      }
+      long nc = (long)(cc->imax + 2) * (cc->jmax + 2) * (cc->kmax + 2);
+      k_transf<<<nblk(nc, 128), 128, 0, c->stream>>>(f->db, cc->db, sst);
+      k_transf_ring<<<nblk(cc->ntot, 256), 256, 0, c->stream>>>(cc->db, sst);
+      c->nlaunch += 2;
+      st_statim(c, cc, 1);
+      if ((r = st_residu(c, cc, (int)m + 1, icycle, (int)m + 1))) return r;
+      k_forcing<<<nblk(cc->ntot, 256), 256, 0, c->stream>>>(cc->db, 0, sst);
+      k_forcing<<<nblk(cc->ntot, 256), 256, 0, c->stream>>>(cc->db, 1, sst);
+      c->nlaunch += 2;
+      return 0;
+    });
+    if (rc || (rc = ls_imps(c, cs, (int)m + 1, true))) return rc;
+    rc = fork_n(c, (int)cs.size(), [&](int n) {
+      k_fin_coarse<<<nblk(cs[n]->ntot, 256), 256, 0, c->stream>>>(cs[n]->db, cs[n]->prm, 1);
+      c->nlaunch++;
+      return 0;
+    });
+    if (rc) return rc;
+  }
+  return fork_n(c, nb, [&](int n) {
+    auto& lv = chain[n];
+    for (size_t m = lv.size() - 1; m >= 1; m--) {
+      BlockCtx *f = lv[m - 1], *cc = lv[m];
+      int nf = f->imax * f->jmax * f->kmax;
+      k_interp<<<nblk(nf, 256), 256, 0, c->stream>>>(cc->db, f->db);
+      c->nlaunch++;
+      if (f->prm.iturb >= 3) {
+        k_intert<<<nblk(nf, 256), 256, 0, c->stream>>>(cc->db, f->db, f->prm);
+        c->nlaunch++;
+      }
+      k_fin_coarse<<<nblk(f->ntot, 256), 256, 0, c->stream>>>(f->db, f->prm, 0);
+      c->nlaunch++;
+    }
+    launch_patch(c, tops[n], k_reflec, 0);
+    return 0;
+  });
+}
+
 // BOUNDI ns3c.f:10608 over all blocks: REFCOR, MIR and STATIM per block,
 // CONNEC of every 1:1 patch in one launch, STATIM again.
 int mb_boundi(Ctx* c) {
@@ -1246,8 +1526,28 @@ int mb_cycle(Ctx* c, int icycle) {
     if (b->coarse) return mb_mg_cycle(c, icycle);
   k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi, c->d_dromax);
   c->nlaunch++;
-  const bool batch = res_batch_ok(c);
-  if (batch) {   // the face pass of all blocks in one launch
+  const bool batch = res_batch_ok(c), lockstep = ls_ok(c);
+  if (lockstep) {   // lockstep: RESIDI, RESL2, IMPSDI (batched sweeps), FIN
+    rc = fork_n(c, nb, [&](int n) {
+      BlockCtx* b = c->tops[n];
+      int r;
+      if (b->prm.iturb >= 3 && (r = st_statim(c, b, 1))) return r;
+      return st_residu(c, b, 1, icycle, 1, batch ? 1 : 0);
+    });
+    if (rc) return rc;
+    if (batch && (rc = launch_residual_batch(c, c->tops, 1))) return rc;
+    rc = fork_n(c, nb, [&](int n) {
+      BlockCtx* b = c->tops[n];
+      int r;
+      if (batch && (r = st_residu(c, b, 1, icycle, 1, 2))) return r;
+      int ncell = b->imax * b->jmax * b->kmax;
+      k_resl2<<<min(nblk(ncell, 256), 4 * c->sm_count), 256, 0, c->stream>>>(b->db, c->d_resi);
+      c->nlaunch++;
+      return 0;
+    });
+    if (rc || (rc = ls_imps(c, c->tops, 1, false))) return rc;
+    if ((rc = fork_n(c, nb, [&](int n) { return st_fin(c, c->tops[n], 1); }))) return rc;
+  } else if (batch) {   // the face pass of all blocks in one launch
     rc = fork_join(c, nb, [&](int n) {
       BlockCtx* b = c->tops[n];
       int r;
@@ -1257,18 +1557,20 @@ int mb_cycle(Ctx* c, int icycle) {
     if (rc) return rc;
     if ((rc = launch_residual_batch(c, c->tops, 1))) return rc;
   }
-  rc = fork_join(c, nb, [&](int n) {
-    BlockCtx* b = c->tops[n];
-    int r;
-    if (!batch && b->prm.iturb >= 3 && (r = st_statim(c, b, 1))) return r;
-    if ((r = st_residu(c, b, 1, icycle, 1, batch ? 2 : 0))) return r;
-    int ncell = b->imax * b->jmax * b->kmax;
-    k_resl2<<<min(nblk(ncell, 256), 4 * c->sm_count), 256, 0, c->stream>>>(b->db, c->d_resi);
-    c->nlaunch++;
-    if ((r = st_imps(c, b, 1, false))) return r;
-    return st_fin(c, b, 1);
-  });
-  if (rc) return rc;
+  if (!lockstep) {
+    rc = fork_join(c, nb, [&](int n) {
+      BlockCtx* b = c->tops[n];
+      int r;
+      if (!batch && b->prm.iturb >= 3 && (r = st_statim(c, b, 1))) return r;
+      if ((r = st_residu(c, b, 1, icycle, 1, batch ? 2 : 0))) return r;
+      int ncell = b->imax * b->jmax * b->kmax;
+      k_resl2<<<min(nblk(ncell, 256), 4 * c->sm_count), 256, 0, c->stream>>>(b->db, c->d_resi);
+      c->nlaunch++;
+      if ((r = st_imps(c, b, 1, false))) return r;
+      return st_fin(c, b, 1);
+    });
+    if (rc) return rc;
+  }
   if ((rc = mb_boundi(c))) return rc;
   for (auto* b : c->tops)
     if (b->prm.iturb >= 3) {
@@ -1287,7 +1589,9 @@ int mb_mg_cycle(Ctx* c, int icycle) {
   int nb = (int)c->tops.size(), rc;
   k_reset_acc<<<1, 32, 0, c->stream>>>(c->d_resi, c->d_dromax);
   c->nlaunch++;
-  if (res_batch_ok(c)) {   // the level-1 face pass of all blocks in one launch
+  if (ls_ok(c)) {
+    rc = mb_mg_body_ls(c, icycle);
+  } else if (res_batch_ok(c)) {   // the level-1 face pass of all blocks in one launch
     rc = fork_join(c, nb, [&](int n) { return mg_body(c, c->tops[n], icycle, false, 1); });
     if (rc) return rc;
     if ((rc = launch_residual_batch(c, c->tops, 1))) return rc;

@@ -1521,9 +1521,11 @@ FF_DI LineDesc<CT> line_desc(const cooperative_groups::cluster_group& cluster, C
   return d;
 }
 
+// The sweep of one block by one cluster.  The CTA may hold more thread
+// groups than lg.ng (a batched launch sized for its largest block): the
+// extra groups own no tile and only take part in the cluster barriers.
 template <typename CT, int NV, bool STAGE>
-__global__ void __launch_bounds__(LTHREADS * (STAGE ? LMAX_TPC_STAGE : LMAX_TPC))
-    k_lusgs_lines(DevBlock b, const CT* __restrict__ sw, CT* dwp, int upper, LineGeom lg) {
+FF_DI void lines_body(const DevBlock& b, const CT* __restrict__ sw, CT* dwp, int upper, const LineGeom& lg) {
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1640,6 +1642,34 @@ __global__ void __launch_bounds__(LTHREADS * (STAGE ? LMAX_TPC_STAGE : LMAX_TPC)
     }
     cluster_wait_acquire();
   }
+}
+
+template <typename CT, int NV, bool STAGE>
+__global__ void __launch_bounds__(LTHREADS * (STAGE ? LMAX_TPC_STAGE : LMAX_TPC))
+    k_lusgs_lines(DevBlock b, const CT* __restrict__ sw, CT* dwp, int upper, LineGeom lg) {
+  lines_body<CT, NV, STAGE>(b, sw, dwp, upper, lg);
+}
+
+// Several blocks' sweeps in one launch (a block work-list): cluster e of
+// the grid sweeps entry e.  All entries share the cluster size; each has its
+// own tile geometry and sweep flags.
+constexpr int LB_MAX = 16;
+struct LinesBatch {
+  int n;
+  int upper[LB_MAX];
+  LineGeom lg[LB_MAX];
+  const void* sw[LB_MAX];
+  void* dwp[LB_MAX];
+  DevBlock b[LB_MAX];
+};
+
+template <typename CT, int NV>
+__global__ void __launch_bounds__(LTHREADS * LMAX_TPC)
+    k_lusgs_lines_batch(const __grid_constant__ LinesBatch lb) {
+  const int e = blockIdx.x / lb.lg[0].cs;
+  if (e >= lb.n) return;   // whole clusters only: the launch has n * cs CTAs
+  lines_body<CT, NV, false>(lb.b[e], static_cast<const CT*>(lb.sw[e]), static_cast<CT*>(lb.dwp[e]), lb.upper[e],
+                            lb.lg[e]);
 }
 
 #include "ff_pipe.cuh"

@@ -615,6 +615,18 @@ def run_config(ntrain=64, ntest=16, cycles=2000, steps=6000, batch=16, lr=1e-3, 
     runs = [solve(pv, cycles, spec=spec) for pv in Ptr]
     t_data = time.perf_counter() - t0
     log(f"training data: {ntrain} solves x {cycles} cycles in {t_data:.1f} s")
+    # a training field is a solution only where its solve converged: keep
+    # the runs whose density residual fell by 4 decades (sum of squares) and
+    # whose fields are finite, drop (and report) the others
+    keep = [bool(np.isfinite(r.q).all() and np.isfinite(r.hist[-1]) and r.hist[-1] <= 1e-4 * r.hist[0])
+            for r in runs]
+    dropped = [[float(x) for x in pv] for pv, k in zip(Ptr, keep) if not k]
+    if dropped:
+        log(f"training data: {len(dropped)} solves did not converge and are left out: {dropped}")
+    if sum(keep) < 2:
+        raise RuntimeError("warm start: fewer than two converged training solves")
+    Ptr = Ptr[np.array(keep)]
+    runs = [r for r, k in zip(runs, keep) if k]
     data = Dataset(Ptr, [r.q for r in runs], spec=spec)
     net = WarmStartNet(seed=0, spec=spec)
     X, T = torch.as_tensor(data.x).to(net.dev), torch.as_tensor(data.y).to(net.dev)
@@ -634,7 +646,8 @@ def run_config(ntrain=64, ntest=16, cycles=2000, steps=6000, batch=16, lr=1e-3, 
                free32_cycles=sum(e["free32_cycles"] for e in ev),
                all_reached=all(e["base_reached"] and e["warm_reached"] and e["free32_reached"] for e in ev),
                fallbacks=sum(e["fallback"] for e in ev),
-               loss=hist, t_data=t_data, t_train=t_train, steps=steps, ntrain=ntrain, ntest=ntest, cycles=cycles,
+               loss=hist, t_data=t_data, t_train=t_train, steps=steps, ntrain=len(runs), ntest=ntest, cycles=cycles,
+               dropped=dropped,
                family=spec.name, tol_decades=tol_decades)
     if ddadi_arms:
         for k in ("ddadi_base_s", "ddadi_warm_s", "ddadi_base_cycles", "ddadi_warm_cycles"):

@@ -286,13 +286,17 @@ def test_multigrid_cycles_match_oracle(gpu_lib, nlev, dims):
     g.close()
 
 
-@pytest.mark.parametrize("kind", ["lines", "hyperplane"])
+@pytest.mark.parametrize("kind", ["lockstep", "lines", "hyperplane"])
 def test_multiblock_cycles_match_oracle(gpu_lib, kind, monkeypatch):
     """Periodic box of 2x2x2 uneven blocks: all-block BOUNDI with device
-    CONNEC, concurrent per-block chains in one captured graph, against the
-    oracle's multi-block cycle."""
+    CONNEC, against the oracle's multi-block cycle.  lockstep: each stage
+    over all blocks with both LU-SGS sweeps of all blocks in one batched
+    launch; lines / hyperplane: concurrent per-block chains in one captured
+    graph, with that sweep kernel."""
     from finflo_b200 import case
     from oracle.oracle import OracleMB
+    if kind == "lockstep":
+        monkeypatch.setenv("FINFLO_MB_LOCKSTEP", "1")
     if kind == "hyperplane":
         monkeypatch.setenv("FINFLO_LUSGS", "hyperplane")
     sizes = ([9, 13], [7, 11], [9, 6])
@@ -321,13 +325,17 @@ def test_multiblock_cycles_match_oracle(gpu_lib, kind, monkeypatch):
 
 
 @pytest.mark.parametrize("turb", [None, "sst"])
-def test_multiblock_multigrid_matches_oracle(gpu_lib, turb):
+@pytest.mark.parametrize("mode", ["lockstep", "branches"])
+def test_multiblock_multigrid_matches_oracle(gpu_lib, turb, mode, monkeypatch):
     """Eight uneven blocks of the spanwise-varying bump (1:1 cuts, periodic
-    z), two multigrid levels each: per-block V-cycles as concurrent graph
-    branches, BOUNDI/CONNEC over the level-1 blocks, against the oracle's
-    multi-block multigrid cycle."""
+    z), two multigrid levels each, BOUNDI/CONNEC over the level-1 blocks,
+    against the oracle's multi-block multigrid cycle: stage by stage over
+    all blocks with each level's sweeps batched (lockstep), or per-block
+    V-cycles as concurrent graph branches."""
     from finflo_b200 import case
     from oracle.oracle import OracleMBMG
+    if mode == "lockstep":
+        monkeypatch.setenv("FINFLO_MB_LOCKSTEP", "1")
     kw = dict(cells=(40, 16, 16), nb=(2, 2, 2), nlev=2, h1=1e-3, reynolds=1e4, mach=0.5, cfl=2.0, cfll=2.0,
               lusgs_fp32=False, coarse_fp32=False, turbulence=turb)
     if turb == "sst":
