@@ -209,6 +209,76 @@ def block_from_metrics(m, patches, nodes=None) -> Block:
     return Block(m.imax, m.jmax, m.kmax, arrays, patches, nodes=nodes)
 
 
+# ---- orientation of 1:1 patches (ICON(14)) ----------------------------------
+
+# CORNER gluebm.f:2480: the four corner nodes of a patch, as (first, second)
+# in-face node offsets from (lo, lo); odd faces go round the second index
+# first, even faces the first.
+_CORNER_ORDER = {1: ((0, 0), (0, 1), (1, 1), (1, 0)), 2: ((0, 0), (1, 0), (1, 1), (0, 1)),
+                 3: ((0, 0), (0, 1), (1, 1), (1, 0)), 4: ((0, 0), (1, 0), (1, 1), (0, 1)),
+                 5: ((0, 0), (0, 1), (1, 1), (1, 0)), 6: ((0, 0), (1, 0), (1, 1), (0, 1))}
+
+
+def patch_corners(nodes, iface, r1, r2):
+    """CORNER gluebm.f:2480: [4, 3] corner coordinates of the patch with cell
+    ranges r1 = (r1a, r1b), r2 = (r2a, r2b) on face iface of the block with
+    nodes (X, Y, Z), each [k, j, i]."""
+    X, Y, Z = nodes
+    kmax, jmax, imax = (n - 1 for n in X.shape)
+    lo = (r1[0] - 1, r2[0] - 1)
+    hi = (r1[1], r2[1])          # IXUQ + 1, IYUQ + 1 as 0-based node indices
+    out = np.empty((4, 3))
+    for q, (u, v) in enumerate(_CORNER_ORDER[iface]):
+        t1 = hi[0] if u else lo[0]
+        t2 = hi[1] if v else lo[1]
+        d = (iface - 1) % 3
+        layer = 0 if iface <= 3 else (imax, jmax, kmax)[d]
+        i, j, k = (layer, t1, t2) if d == 0 else ((t1, layer, t2) if d == 1 else (t1, t2, layer))
+        out[q] = X[k, j, i], Y[k, j, i], Z[k, j, i]
+    return out
+
+
+def orient(xcol, xcog, chlref=1.0):
+    """ORIENT gluebm.f:8506: ICON(14) of a 1:1 patch from the diagonals of
+    its corners xcol and its partner's xcog ([4, 3] each): the turn 0..3 of
+    the partner whose diagonals match; -1 when none is within 1e-3 chlref."""
+    a13, a24 = xcol[2] - xcol[0], xcol[3] - xcol[1]
+    b13, b24 = xcog[2] - xcog[0], xcog[3] - xcog[1]
+    b31, b42 = -b13, -b24
+    nrm = np.linalg.norm
+    s = [nrm(a13 - b13) + nrm(a24 - b42), nrm(a13 - b24) + nrm(a24 - b13),
+         nrm(a13 - b31) + nrm(a24 - b24), nrm(a13 - b42) + nrm(a24 - b31)]
+    iori, ss = -1, 1.0e-3 * chlref
+    for q in range(4):
+        if s[q] < ss:
+            iori, ss = q, s[q]
+    return iori
+
+
+def orient_connections(blocks, chlref=1.0):
+    """The orientation (ICON(14), ORIENT's turn, gluebm.f:8188) of every 1:1
+    patch of the blocks (each with its nodes), from its corners and its
+    partner's: the patch on block IBTYPE, face NFACE starting at (N1A,
+    N2A).  Raises where no orientation matches."""
+    for b in blocks:
+        for pa in b.patches:
+            if pa.ityp != grid.BC_CON:
+                continue
+            nb = blocks[pa.ibtype]
+            part = [q for q in nb.patches if q.ityp == grid.BC_CON and q.iface == pa.nface
+                    and q.r1a == pa.n1a and q.r2a == pa.n2a]
+            if not part:
+                raise ValueError(f"1:1 patch on face {pa.iface}: no partner on block {pa.ibtype} face {pa.nface}")
+            q = part[0]
+            xcol = patch_corners(b.nodes, pa.iface, (pa.r1a, pa.r1b), (pa.r2a, pa.r2b))
+            xcog = patch_corners(nb.nodes, q.iface, (q.r1a, q.r1b), (q.r2a, q.r2b))
+            iori = orient(xcol, xcog, chlref)
+            if iori < 0:
+                raise ValueError(f"1:1 patch on face {pa.iface}: the patch orientation cannot be solved")
+            pa.iori = iori
+    return blocks
+
+
 def init_freestream(b: Block, fs, *, noise=1e-3, seed=0):
     """Uniform free stream plus seeded Gaussian noise on the density of the
     interior cells, held at constant pressure (T = p/(R rho))."""
@@ -484,6 +554,7 @@ def periodic_box_case(nb=(4, 3, 2), sizes=None, *, seed=2, mach=0.3, target=None
         prm.idi1 = prm.idi2 = prm.idi3 = 0
         blocks.append(blk)
         prms.append(prm)
+    orient_connections(blocks)
     return blocks, prms, fs
 
 
@@ -581,7 +652,7 @@ def bump_multiblock_blocks(cells=(512, 256, 128), nb=(2, 2, 2), nlev=3, *, seed=
                     pa.nface = _OPP[iface]
                     pa.n1a = pa.n2a = 1
                     pats.append(pa)
-            blk = block_from_metrics(m, pats, nodes=(Xb, Yb, Zb) if device_setup and lev == 0 else None)
+            blk = block_from_metrics(m, pats, nodes=(Xb, Yb, Zb) if lev == 0 else None)
             init_freestream(blk, fs, noise=noise if lev == 0 else 0.0, seed=seed + 100 * bid)
             levels.append(blk)
         prm = make_params(fc, levels[0].dims, cfl=cfl, cfll=cfll, inter=inter)
@@ -606,6 +677,7 @@ def bump_multiblock_case(*args, **kw):
     for levels, prms in it:
         bl.append(levels)
         bp.append(prms)
+    orient_connections([lv[0] for lv in bl])
     return (bl, bp, fs, tri) if tri is not None else (bl, bp, fs)
 
 
@@ -616,7 +688,9 @@ def patches_from_bc(bc_patches, nblocks, fs, rk=0.0, reps=0.0):
     from the patches fileio.read_bc returns.  Inlet/outlet boundary values
     are the free stream's, uniform over the patch (the boundary-value files
     are not read); a connection's IBTYPE is its source block's 0-based index,
-    NFACE its face and N1A/N2A the start of the matching range."""
+    NFACE its face and N1A/N2A the start of the matching range.  A
+    connection's orientation ICON(14) comes from the grid: orient_connections
+    on the blocks built with these tables."""
     out = [[] for _ in range(nblocks)]
     inl = dict(bounr=fs["rho"], bounu=fs["u"], bounv=0.0, bounw=0.0, bount=fs["t"], bounp=fs["p"], bounpd=0.0,
                bounrk=rk, bounep=reps)

@@ -1260,6 +1260,29 @@ __global__ void k_fin_coarse(DevBlock b, ff_params p, int update) {
 // destination patch (TEMP,U,V,W,E,EPS2,VIST,CH,P,PDIFF,RK,REPS, as BOUNDI passes).
 struct ConnItem { int dst, src; ff_patch pa; };
 
+// The donor face cell (ad, cd) of receiver patch point (a, c) of a 1:1
+// connection in orientation ICON(14) = pa.iori: the donor's export order
+// (second in-face index fastest on odd faces, first on even faces; EXPVOL
+// gluebm.f:6115-6136), the receiver's import order (first index fastest on
+// odd faces, second on even; IMPVO2 7040-7080) and PERMUT's turn of the
+// receiver sequence (gluebm.f:4868).
+FF_DI void conn_donor(const ff_patch& pa, int a, int c, int& ad, int& cd) {
+  const int n1 = pa.r1b - pa.r1a + 1, n2 = pa.r2b - pa.r2a + 1;
+  const bool rodd = pa.iface & 1, dodd = pa.nface & 1;
+  const int P = rodd ? n1 : n2, Q = rodd ? n2 : n1;
+  const int x = rodd ? a - pa.r1a + 1 : c - pa.r2a + 1;
+  const int y = rodd ? c - pa.r2a + 1 : a - pa.r1a + 1;
+  int u, v;
+  switch (pa.iori & 3) {
+    case 1: u = Q + 1 - y; v = x; break;
+    case 2: u = P + 1 - x; v = Q + 1 - y; break;
+    case 3: u = y; v = P + 1 - x; break;
+    default: u = x; v = y;
+  }
+  if (dodd) { cd = pa.n2a + u - 1; ad = pa.n1a + v - 1; }
+  else { ad = pa.n1a + u - 1; cd = pa.n2a + v - 1; }
+}
+
 __global__ void k_connec(const DevBlock* __restrict__ blocks, const ConnItem* __restrict__ items) {
   const ConnItem& it = items[blockIdx.y];
   const ff_patch& pa = it.pa;
@@ -1270,8 +1293,10 @@ __global__ void k_connec(const DevBlock* __restrict__ blocks, const ConnItem* __
   const DevBlock& d = blocks[it.dst];
   const DevBlock& s = blocks[it.src];
   FaceG fd = face_g(d, pa.iface), fs = face_g(s, pa.nface);
+  int ad, cd;
+  conn_donor(pa, a, c, ad, cd);
   size_t L = face_cell(d, fd, a, c);
-  size_t S = face_cell(s, fs, a - pa.r1a + pa.n1a, c - pa.r2a + pa.n2a);
+  size_t S = face_cell(s, fs, ad, cd);
   const int vs[12] = {FF_TEMP, FF_U, FF_V, FF_W, FF_E, FF_EPS2, FF_VIST, FF_CH, FF_P, FF_PDIFF, FF_RK, FF_REPS};
   int lsd = fd.idir * fd.s, lss = fs.idir * fs.s;
 #pragma unroll
@@ -1299,7 +1324,9 @@ __global__ void k_halo(const DevBlock* __restrict__ blocks, const HaloItem* __re
   const int vs[12] = {FF_TEMP, FF_U, FF_V, FF_W, FF_E, FF_EPS2, FF_VIST, FF_CH, FF_P, FF_PDIFF, FF_RK, FF_REPS};
   if (mode == 0) {
     FaceG fs = face_g(b, pa.nface);
-    size_t S = face_cell(b, fs, a + pa.n1a, c + pa.n2a);
+    int ad, cd;
+    conn_donor(pa, a + pa.r1a, c + pa.r2a, ad, cd);
+    size_t S = face_cell(b, fs, ad, cd);
     int lss = fs.idir * fs.s;
     double* o = sbuf + it.offset;
 #pragma unroll

@@ -1689,8 +1689,32 @@ void orc_mg_cycle(orc_block **lv, int nlev, const ff_params *prm, int icycle, do
 
 /* ---------------------------------------------------------------------- */
 /* Multi-block: 1:1 connections (CONNEC ns3c.f:8605 -> EXPTOT gluebm.f:6819 */
-/* / IMPVO2 gluebm.f:6964) for aligned patches (ICON(14) = 0).             */
+/* / IMPVO2 gluebm.f:6964) in the four orientations ICON(14) = 0..3.       */
 /* ---------------------------------------------------------------------- */
+
+/* The donor face cell (*ad, *cd) of receiver patch point (a, c).  The donor
+ * exports its patch with the second in-face index running fastest on odd
+ * faces and the first on even faces (EXPVOL gluebm.f:6115-6136, EXPORT
+ * 5096); the receiver reads that sequence with its first index fastest on
+ * odd faces and its second on even faces (IMPVO2 7040-7080, IMPORT 5174),
+ * after PERMUT (4868: PERM1/2/3, a quarter, half or three-quarter turn of
+ * the P x Q receiver sequence) by ICON(14). */
+void orc_conn_donor(const ff_patch *pa, int a, int c, int *ad, int *cd) {
+  const int n1 = pa->r1b - pa->r1a + 1, n2 = pa->r2b - pa->r2a + 1;
+  const int rodd = pa->iface & 1, dodd = pa->nface & 1;
+  const int P = rodd ? n1 : n2, Q = rodd ? n2 : n1;
+  const int x = rodd ? a - pa->r1a + 1 : c - pa->r2a + 1;
+  const int y = rodd ? c - pa->r2a + 1 : a - pa->r1a + 1;
+  int u, v;
+  switch (pa->iori & 3) {
+    case 1: u = Q + 1 - y; v = x; break;     /* PERM1: I' = J, J' = ISTR - I + 1 */
+    case 2: u = P + 1 - x; v = Q + 1 - y; break;
+    case 3: u = y; v = P + 1 - x; break;     /* PERM3: I' = JSTR - J + 1, J' = I */
+    default: u = x; v = y;
+  }
+  if (dodd) { *cd = pa->n2a + u - 1; *ad = pa->n1a + v - 1; }
+  else { *ad = pa->n1a + u - 1; *cd = pa->n2a + v - 1; }
+}
 
 /* Copy the two interior layers next to the source face of block `src` into
  * the two ghost layers of patch `pa` of block `dst`.  BOUNDI passes TEMP in
@@ -1704,8 +1728,10 @@ void orc_connec_patch(orc_block *dst, const ff_patch *pa, const orc_block *src) 
   int lsd = fd.idir * fd.s, lss = fs.idir * fs.s;
   for (int bb = pa->r2a; bb <= pa->r2b; bb++)
     for (int a = pa->r1a; a <= pa->r1b; a++) {
+      int ad, cd;
+      orc_conn_donor(pa, a, bb, &ad, &cd);
       size_t L = face_cell(&dd, &fd, a, bb);
-      size_t S = face_cell(&ds, &fs, a - pa->r1a + pa->n1a, bb - pa->r2a + pa->n2a);
+      size_t S = face_cell(&ds, &fs, ad, cd);
       for (int g = 1; g <= 2; g++) {
         size_t G = L - g * lsd, Q = S + (g - 1) * lss;
         for (int v = 0; v < 12; v++) dst->a[vs[v]][G] = src->a[vs[v]][Q];
@@ -1801,7 +1827,9 @@ void orc_halo_pack(const orc_block *src, const ff_patch *pa, double *out) {
   int n1 = pa->r1b - pa->r1a + 1, n2 = pa->r2b - pa->r2a + 1, n = n1 * n2;
   for (int c = 0; c < n2; c++)
     for (int a = 0; a < n1; a++) {
-      size_t S = face_cell(&ds, &fs, a + pa->n1a, c + pa->n2a);
+      int ad, cd;
+      orc_conn_donor(pa, a + pa->r1a, c + pa->r2a, &ad, &cd);
+      size_t S = face_cell(&ds, &fs, ad, cd);
       for (int g = 0; g < 2; g++)
         for (int v = 0; v < 12; v++) out[(size_t)(g * 12 + v) * n + c * n1 + a] = src->a[vs[v]][S + g * lss];
     }
