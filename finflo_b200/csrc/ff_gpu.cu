@@ -204,19 +204,26 @@ bool res_fused() {
   return f;
 }
 
-template <int NV, int NT, int I_, int J_, int K_>
+template <int NV, int NT, int I_, int J_, int K_, bool ST = false>
 void launch_residual_fused_s(cudaStream_t st, const BlockCtx* b, int level) {
   dim3 g(nblk(b->imax, I_), nblk(b->jmax, J_), nblk(b->kmax, K_));
-  const size_t sm = residual_fused_smem(NV, I_, J_, K_);
-  cudaFuncSetAttribute(k_residual_fused<NV, NT, I_, J_, K_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k_residual_fused<NV, NT, I_, J_, K_><<<g, NT, sm, st>>>(b->db, b->prm, level);
+  const size_t sm = residual_fused_smem(NV, I_, J_, K_, ST);
+  cudaFuncSetAttribute(k_residual_fused<NV, NT, I_, J_, K_, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sm);
+  k_residual_fused<NV, NT, I_, J_, K_, ST><<<g, NT, sm, st>>>(b->db, b->prm, level);
 }
 
 template <int NV, int NT>
 void launch_residual_fused_t(cudaStream_t st, dim3 g, const BlockCtx* b, int level) {
   (void)g;
-  // the tile shape the autotuner chose for this block (512 threads only)
+  // the form the autotuner chose for this block (512 threads only): tile
+  // shape, and the stencil staged in shared memory or not
   const int sh = NT == 512 ? b->res_shape : 0;
+  if constexpr (NT == 512) {
+    if (sh == 3) return launch_residual_fused_s<NV, NT, 32, 4, 4, true>(st, b, level);
+    if (sh == 4) return launch_residual_fused_s<NV, NT, 16, 8, 4, true>(st, b, level);
+    if (sh == 5) return launch_residual_fused_s<NV, NT, 8, 8, 8, true>(st, b, level);
+  }
   if (sh == 1) return launch_residual_fused_s<NV, NT, 16, 8, 4>(st, b, level);
   if (sh == 2) return launch_residual_fused_s<NV, NT, 8, 8, 8>(st, b, level);
   launch_residual_fused_s<NV, NT, 32, 4, 4>(st, b, level);
@@ -325,17 +332,19 @@ int st_residu(Ctx* c, BlockCtx* b, int level, int icycle, int m2 = 1, int part =
 // The residual face pass of several level-1 blocks in one launch over their
 // tiles (k_residual_batch, RB_MAX blocks per launch); every block must have
 // the same equation count.  The tile shape is the first block's.
-template <int NV, int I_, int J_, int K_>
+template <int NV, int I_, int J_, int K_, bool ST = false>
 void launch_residual_batch_t(cudaStream_t st, const ResBatch& rb, int level) {
-  const size_t sm = residual_fused_smem(NV, I_, J_, K_);
-  cudaFuncSetAttribute(k_residual_batch<NV, 512, I_, J_, K_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k_residual_batch<NV, 512, I_, J_, K_><<<rb.tile0[rb.nblk], 512, sm, st>>>(rb, level);
+  const size_t sm = residual_fused_smem(NV, I_, J_, K_, ST);
+  cudaFuncSetAttribute(k_residual_batch<NV, 512, I_, J_, K_, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sm);
+  k_residual_batch<NV, 512, I_, J_, K_, ST><<<rb.tile0[rb.nblk], 512, sm, st>>>(rb, level);
 }
 
 int launch_residual_batch(Ctx* c, const std::vector<BlockCtx*>& blks, int level) {
   const int shape = blks[0]->res_shape;
   const bool sst = blks[0]->prm.iturb >= 3;
-  const int ti = RES_SHAPES[shape][0], tj = RES_SHAPES[shape][1], tk = RES_SHAPES[shape][2];
+  const int ti = RES_SHAPES[shape % RES_NSHAPE][0], tj = RES_SHAPES[shape % RES_NSHAPE][1],
+            tk = RES_SHAPES[shape % RES_NSHAPE][2];
   for (size_t s0 = 0; s0 < blks.size(); s0 += RB_MAX) {
     static ResBatch rb;   // ~19 KB: kept off the host stack
     rb = ResBatch{};
@@ -350,12 +359,20 @@ int launch_residual_batch(Ctx* c, const std::vector<BlockCtx*>& blks, int level)
       rb.b[n] = b->db;
       rb.p[n] = b->prm;
     }
-    if (shape == 1) sst ? launch_residual_batch_t<7, 16, 8, 4>(c->stream, rb, level)
-                        : launch_residual_batch_t<5, 16, 8, 4>(c->stream, rb, level);
-    else if (shape == 2) sst ? launch_residual_batch_t<7, 8, 8, 8>(c->stream, rb, level)
-                             : launch_residual_batch_t<5, 8, 8, 8>(c->stream, rb, level);
-    else sst ? launch_residual_batch_t<7, 32, 4, 4>(c->stream, rb, level)
-             : launch_residual_batch_t<5, 32, 4, 4>(c->stream, rb, level);
+    switch (shape) {
+      case 1: sst ? launch_residual_batch_t<7, 16, 8, 4>(c->stream, rb, level)
+                  : launch_residual_batch_t<5, 16, 8, 4>(c->stream, rb, level); break;
+      case 2: sst ? launch_residual_batch_t<7, 8, 8, 8>(c->stream, rb, level)
+                  : launch_residual_batch_t<5, 8, 8, 8>(c->stream, rb, level); break;
+      case 3: sst ? launch_residual_batch_t<7, 32, 4, 4, true>(c->stream, rb, level)
+                  : launch_residual_batch_t<5, 32, 4, 4, true>(c->stream, rb, level); break;
+      case 4: sst ? launch_residual_batch_t<7, 16, 8, 4, true>(c->stream, rb, level)
+                  : launch_residual_batch_t<5, 16, 8, 4, true>(c->stream, rb, level); break;
+      case 5: sst ? launch_residual_batch_t<7, 8, 8, 8, true>(c->stream, rb, level)
+                  : launch_residual_batch_t<5, 8, 8, 8, true>(c->stream, rb, level); break;
+      default: sst ? launch_residual_batch_t<7, 32, 4, 4>(c->stream, rb, level)
+                   : launch_residual_batch_t<5, 32, 4, 4>(c->stream, rb, level);
+    }
     c->nlaunch++;
   }
   CK(cudaGetLastError());
@@ -897,20 +914,18 @@ int tune_ddadi(Ctx* c, BlockCtx* b, const TuneKey& key) {
   return 0;
 }
 
-// Residual tile shape of a block: each of RES_SHAPES timed on the block's
-// own level (CUDA events, after one untimed launch), the fastest kept;
-// cached per device, block shape and equation count.  FINFLO_RES_SHAPE
-// (0, 1, 2) fixes it.
+// Residual form of a block: each tile shape of RES_SHAPES, with and without
+// the staged stencil, timed on the block's own level (CUDA events, after
+// one untimed launch), the fastest kept; cached per device, block shape and
+// equation count.  FINFLO_RES_SHAPE (0..5) fixes it.
 std::map<TuneKey, int> g_res_cache;
 
 int tune_residual(Ctx* c, BlockCtx* b) {
   if (b->res_tuned) return 0;
   b->res_tuned = 1;
-  static const int env = [] {
-    const char* e = getenv("FINFLO_RES_SHAPE");
-    return e ? atoi(e) : -1;
-  }();
-  if (env >= 0 && env < RES_NSHAPE) { b->res_shape = env; return 0; }
+  const char* e = getenv("FINFLO_RES_SHAPE");
+  const int env = e ? atoi(e) : -1;
+  if (env >= 0 && env < RES_NFORM) { b->res_shape = env; return 0; }
   if (!res_fused() || res_threads(b->prm.iturb >= 3) != 512) return 0;
   const TuneKey key{c->device, b->imax, b->jmax, b->kmax, (b->prm.iturb >= 3 ? 7 : 5) + 10 * b->level, 0, 0};
   {
@@ -920,7 +935,7 @@ int tune_residual(Ctx* c, BlockCtx* b) {
   }
   float best = 1e30f;
   int pick = 0;
-  for (int s = 0; s < RES_NSHAPE; s++) {
+  for (int s = 0; s < RES_NFORM; s++) {
     b->res_shape = s;
     launch_residual(c->stream, b, b->level);
     CK(cudaEventRecord(c->ev0, c->stream));

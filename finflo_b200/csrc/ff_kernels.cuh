@@ -549,8 +549,10 @@ FF_DI void vl_flux(const double qc[5][4], double nx, double ny, double nz, doubl
   f[4] = fm[4] + fp[4] + f[4];
 }
 
+// sq (optional): RO, U, V, W, P of cell L in a staged stencil, variable v
+// at sq[v * vs], the cells along the face normal es apart.
 FF_DI void face_flux(const DevBlock& b, const ff_params& p, int dir, size_t L, int m, int t1, int t2,
-                     int level, double f[5]) {
+                     int level, double f[5], const double* sq = nullptr, int es = 0, int vs = 0) {
   const int S = dir == 1 ? 1 : (dir == 2 ? b.is : b.il);
   const int nmax = dir == 1 ? b.imax : (dir == 2 ? b.jmax : b.kmax);
   int intem = dir == 1 ? p.interi : (dir == 2 ? p.interj : p.interk);
@@ -590,14 +592,24 @@ FF_DI void face_flux(const DevBlock& b, const ff_params& p, int dir, size_t L, i
   }
   double q[5][4];
   const int sl[5] = {FF_RO, FF_U, FF_V, FF_W, FF_P};
+  if (sq) {
 #pragma unroll
-  for (int v = 0; v < 5; v++) {
-    const double* a = b.a[sl[v]];
-    q[v][0] = __ldg(a + L - 2 * S); q[v][1] = __ldg(a + L - S); q[v][2] = __ldg(a + L); q[v][3] = __ldg(a + L + S);
+    for (int v = 0; v < 5; v++) {
+      const double* a = sq + v * vs;
+      q[v][0] = a[-2 * es]; q[v][1] = a[-es]; q[v][2] = a[0]; q[v][3] = a[es];
+    }
+  } else {
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+      const double* a = b.a[sl[v]];
+      q[v][0] = __ldg(a + L - 2 * S); q[v][1] = __ldg(a + L - S); q[v][2] = __ldg(a + L); q[v][3] = __ldg(a + L + S);
+    }
   }
   size_t L2 = dir == 3 ? L : L - S;
   double cr[4] = {__ldg(b.a[FF_DRDP] + L), __ldg(b.a[FF_DRDH] + L), q[0][2], q[4][2]};
-  double cl[4] = {__ldg(b.a[FF_DRDP] + L2), __ldg(b.a[FF_DRDH] + L2), __ldg(b.a[FF_RO] + L2), __ldg(b.a[FF_P] + L2)};
+  // RO and P of cell L2 (L itself for k faces) are in the stencil
+  double cl[4] = {__ldg(b.a[FF_DRDP] + L2), __ldg(b.a[FF_DRDH] + L2), dir == 3 ? q[0][2] : q[0][1],
+                  dir == 3 ? q[4][2] : q[4][1]};
   roe_flux(q, __ldg(b.a[FF_A1XA + ao] + L), __ldg(b.a[FF_A1YA + ao] + L), __ldg(b.a[FF_A1ZA + ao] + L),
            __ldg(b.a[FF_A1 + ao] + L), intem, p, __ldg(b.a[FF_C] + L), __ldg(b.a[FF_C] + L - S), cr, cl, f);
 }

@@ -400,8 +400,10 @@ FF_DI void wall_flux_ke(const DevBlock& b, const ff_params& p, size_t II, int S,
 
 // Flux of one face with k and omega (FLXCYC order: FLKEBL, SETV12, FLUXBL,
 // FLUXKE; BOTSKE on walls).
+// sq (optional): the seven MUSCL variables of cell L in a staged stencil,
+// variable v at sq[v * vs], the cells along the face normal es apart.
 FF_DI void face_flux_ke(const DevBlock& b, const ff_params& p, int dir, size_t L, int m, int t1, int t2,
-                        int level, double f[7]) {
+                        int level, double f[7], const double* sq = nullptr, int es = 0, int vs = 0) {
   const int S = dir == 1 ? 1 : (dir == 2 ? b.is : b.il);
   const int nmax = dir == 1 ? b.imax : (dir == 2 ? b.jmax : b.kmax);
   int intem = dir == 1 ? p.interi : (dir == 2 ? p.interj : p.interk);
@@ -429,14 +431,24 @@ FF_DI void face_flux_ke(const DevBlock& b, const ff_params& p, int dir, size_t L
   {
     double q[7][4];
     const int sl[7] = {FF_RO, FF_U, FF_V, FF_W, FF_P, FF_RK, FF_REPS};
+    if (sq) {
 #pragma unroll
-    for (int v = 0; v < 7; v++) {
-      const double* a = b.a[sl[v]];
-      q[v][0] = __ldg(a + L - 2 * S); q[v][1] = __ldg(a + L - S); q[v][2] = __ldg(a + L); q[v][3] = __ldg(a + L + S);
+      for (int v = 0; v < 7; v++) {
+        const double* a = sq + v * vs;
+        q[v][0] = a[-2 * es]; q[v][1] = a[-es]; q[v][2] = a[0]; q[v][3] = a[es];
+      }
+    } else {
+#pragma unroll
+      for (int v = 0; v < 7; v++) {
+        const double* a = b.a[sl[v]];
+        q[v][0] = __ldg(a + L - 2 * S); q[v][1] = __ldg(a + L - S); q[v][2] = __ldg(a + L); q[v][3] = __ldg(a + L + S);
+      }
     }
     size_t L2 = dir == 3 ? L : L - S;
     double cr[4] = {__ldg(b.a[FF_DRDP] + L), __ldg(b.a[FF_DRDH] + L), q[0][2], q[4][2]};
-    double cl[4] = {__ldg(b.a[FF_DRDP] + L2), __ldg(b.a[FF_DRDH] + L2), __ldg(b.a[FF_RO] + L2), __ldg(b.a[FF_P] + L2)};
+    // RO and P of cell L2 (L itself for k faces) are in the stencil
+    double cl[4] = {__ldg(b.a[FF_DRDP] + L2), __ldg(b.a[FF_DRDH] + L2), dir == 3 ? q[0][2] : q[0][1],
+                    dir == 3 ? q[4][2] : q[4][1]};
     const int ao = 4 * (dir - 1);
     roe_flux_ke(q, __ldg(b.a[FF_A1XA + ao] + L), __ldg(b.a[FF_A1YA + ao] + L), __ldg(b.a[FF_A1ZA + ao] + L),
                 __ldg(b.a[FF_A1 + ao] + L), intem, intet, p, __ldg(b.a[FF_C] + L), __ldg(b.a[FF_C] + L - S), cr, cl,
@@ -530,14 +542,35 @@ __global__ void __launch_bounds__(NT, RES_MIN_CTAS * 128 / NT) k_residual_sst(De
 // parameter: 32x4x4, 16x8x4 and 8x8x8 trade i-direction coalescing against
 // the faces computed per cell (3.53, 3.44, 3.38); the autotuner picks one
 // per block shape.
-template <int NV, int NT, int TI_, int TJ_, int TK_>
+//
+// STAGE: the MUSCL variables (RO, U, V, W, P(, RK, REPS)) of the tile's
+// cells and of the two cells beyond each of its six faces are first copied
+// into shared memory (a box of (TI+4)(TJ+4)(TK+4) cells of which the
+// tile's three cross arms are filled), and every face reads its four-cell
+// stencil from there instead of global memory.
+template <int NV, int NT, int TI_, int TJ_, int TK_, bool STAGE = false>
 FF_DI void residual_tile(const DevBlock& b, const ff_params& p, int level, int i0, int j0, int k0,
                          double* res_smem) {
   constexpr int TI = TI_, TJ = TJ_, TK = TK_;
   constexpr int NFK = TI * TJ * (TK + 1), NFI = (TI + 1) * TJ * TK, NFJ = TI * (TJ + 1) * TK;
   constexpr int NFT = NFK + NFI + NFJ, NC = TI * TJ * TK;
+  constexpr int BI = TI + 4, BJ = TJ + 4, BOX = BI * BJ * (TK + 4);
   double(*sF)[NFT] = reinterpret_cast<double(*)[NFT]>(res_smem);
+  double* sQ = res_smem + NV * NFT;
   const int tid = threadIdx.x;
+  if constexpr (STAGE) {
+    const int sl[7] = {FF_RO, FF_U, FF_V, FF_W, FF_P, FF_RK, FF_REPS};
+    for (int e = tid; e < BOX; e += NT) {
+      const int ci = e % BI - 2, cj = (e / BI) % BJ - 2, ck = e / (BI * BJ) - 2;
+      const int out = (ci < 0 || ci >= TI) + (cj < 0 || cj >= TJ) + (ck < 0 || ck >= TK);
+      const int I = i0 + ci + 1, J = j0 + cj + 1, K = k0 + ck + 1;
+      if (out > 1 || I < -1 || I > b.imax + 2 || J < -1 || J > b.jmax + 2 || K < -1 || K > b.kmax + 2) continue;
+      const size_t n = ix(b, I, J, K);
+#pragma unroll
+      for (int v = 0; v < NV; v++) sQ[v * BOX + e] = __ldg(b.a[sl[v]] + n);
+    }
+    __syncthreads();
+  }
   for (int f = tid; f < NFT; f += NT) {
     int dir, l, ni, nj;
     if (f < NFK) { dir = 3; l = f; ni = TI; nj = TJ; }
@@ -549,8 +582,14 @@ FF_DI void residual_tile(const DevBlock& b, const ff_params& p, int level, int i
     const int m = dir == 1 ? I : (dir == 2 ? J : K);
     const int t1 = dir == 1 ? J : I, t2 = dir == 3 ? J : K;
     double fl[NV];
-    if constexpr (NV == 7) face_flux_ke(b, p, dir, ix(b, I, J, K), m, t1, t2, level, fl);
-    else face_flux(b, p, dir, ix(b, I, J, K), m, t1, t2, level, fl);
+    const double* sq = nullptr;
+    int es = 0;
+    if constexpr (STAGE) {   // the face's high cell in the staged box
+      sq = sQ + ((fk + 2) * BJ + (fj + 2)) * BI + (fi + 2);
+      es = dir == 1 ? 1 : (dir == 2 ? BI : BI * BJ);
+    }
+    if constexpr (NV == 7) face_flux_ke(b, p, dir, ix(b, I, J, K), m, t1, t2, level, fl, sq, es, BOX);
+    else face_flux(b, p, dir, ix(b, I, J, K), m, t1, t2, level, fl, sq, es, BOX);
 #pragma unroll
     for (int v = 0; v < NV; v++) sF[v][f] = fl[v];
   }
@@ -573,10 +612,11 @@ FF_DI void residual_tile(const DevBlock& b, const ff_params& p, int level, int i
   }
 }
 
-template <int NV, int NT, int TI_ = TI, int TJ_ = TJ, int TK_ = TK>
+template <int NV, int NT, int TI_ = TI, int TJ_ = TJ, int TK_ = TK, bool STAGE = false>
 __global__ void __launch_bounds__(NT, RES_MIN_CTAS * 128 / NT) k_residual_fused(DevBlock b, ff_params p, int level) {
   extern __shared__ double res_smem[];
-  residual_tile<NV, NT, TI_, TJ_, TK_>(b, p, level, blockIdx.x * TI_, blockIdx.y * TJ_, blockIdx.z * TK_, res_smem);
+  residual_tile<NV, NT, TI_, TJ_, TK_, STAGE>(b, p, level, blockIdx.x * TI_, blockIdx.y * TJ_, blockIdx.z * TK_,
+                                              res_smem);
 }
 
 // The same residual for several blocks in one launch: a block work-list of
@@ -592,7 +632,7 @@ struct ResBatch {
   ff_params p[RB_MAX];
 };
 
-template <int NV, int NT, int TI_, int TJ_, int TK_>
+template <int NV, int NT, int TI_, int TJ_, int TK_, bool STAGE = false>
 __global__ void __launch_bounds__(NT, RES_MIN_CTAS * 128 / NT)
     k_residual_batch(const __grid_constant__ ResBatch rb, int level) {
   extern __shared__ double res_smem[];
@@ -601,15 +641,18 @@ __global__ void __launch_bounds__(NT, RES_MIN_CTAS * 128 / NT)
   while (bi + 1 < rb.nblk && t >= rb.tile0[bi + 1]) bi++;
   const int l = t - rb.tile0[bi], nx = rb.ntx[bi], ny = rb.nty[bi];
   const int ti = l % nx, tj = (l / nx) % ny, tk = l / (nx * ny);
-  residual_tile<NV, NT, TI_, TJ_, TK_>(rb.b[bi], rb.p[bi], level, ti * TI_, tj * TJ_, tk * TK_, res_smem);
+  residual_tile<NV, NT, TI_, TJ_, TK_, STAGE>(rb.b[bi], rb.p[bi], level, ti * TI_, tj * TJ_, tk * TK_, res_smem);
 }
 
-inline size_t residual_fused_smem(int nv, int ti = TI, int tj = TJ, int tk = TK) {
-  return (size_t)nv * (ti * tj * (tk + 1) + (ti + 1) * tj * tk + ti * (tj + 1) * tk) * sizeof(double);
+inline size_t residual_fused_smem(int nv, int ti = TI, int tj = TJ, int tk = TK, bool stage = false) {
+  const size_t faces = (size_t)nv * (ti * tj * (tk + 1) + (ti + 1) * tj * tk + ti * (tj + 1) * tk);
+  const size_t box = stage ? (size_t)nv * (ti + 4) * (tj + 4) * (tk + 4) : 0;
+  return (faces + box) * sizeof(double);
 }
 
-// The residual tile shapes the autotuner chooses from (cells in i, j, k).
-constexpr int RES_NSHAPE = 3;
+// The residual forms the autotuner chooses from: tile shape (cells in i,
+// j, k) and staged stencil or not (form s: shape s % 3, staged for s >= 3).
+constexpr int RES_NSHAPE = 3, RES_NFORM = 6;
 constexpr int RES_SHAPES[RES_NSHAPE][3] = {{32, 4, 4}, {16, 8, 4}, {8, 8, 8}};
 
 // SOURKO (KOVER=0, RANS, no rotation correction) + ADDSKE, interior cells.

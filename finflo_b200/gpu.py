@@ -346,7 +346,8 @@ class GpuSolver:
         return ms.value
 
     def residual_shape(self, bid=0) -> str:
-        return ("32x4x4", "16x8x4", "8x8x8")[self.L.ff_residual_shape(self.ctx, bid)]
+        return ("32x4x4", "16x8x4", "8x8x8", "32x4x4 staged", "16x8x4 staged",
+                "8x8x8 staged")[self.L.ff_residual_shape(self.ctx, bid)]
 
     def lusgs_kind(self, bid=0) -> int:
         return self.L.ff_lusgs_kind(self.ctx, bid)

@@ -233,9 +233,10 @@ int ff_sweep_tuning(void *ctx, int blk, float *ms2);
  * CTA chunk, 1: 16 x 4, 2: 16 x 8, 3: 8 x 8), or 4 alone for one thread per
  * line. */
 int ff_sweep_times(void *ctx, int blk, float *ms3);
-/* The residual tile shape the autotuner chose for a block (its first
+/* The residual form the autotuner chose for a block (its first
  * ff_cycles / ff_cycles_all call times each): 0 = 32x4x4, 1 = 16x8x4,
- * 2 = 8x8x8 cells per CTA (i, j, k). */
+ * 2 = 8x8x8 cells per CTA (i, j, k); 3, 4, 5 the same tiles with the face
+ * stencils staged in shared memory. */
 int ff_residual_shape(void *ctx, int blk);
 int ff_lusgs_kind(void *ctx, int blk);
 int ff_time_cycles(void *ctx, int blk, int ncycles, float *ms);
