@@ -486,14 +486,16 @@ def _large_block_worker(args):
     from oracle.oracle import OracleMG
     it = _large_blocks(cells, fp32=False)
     next(it)
-    tri = next(it)[1]
+    walls = next(it)[1]
     for n, (levels, prms) in enumerate(it):
         if n == k:
             break
-    for lev, m in zip(levels, grid.mg_metrics(*levels[0].nodes, len(levels))):
+    for q, (lev, m) in enumerate(zip(levels, grid.mg_metrics(*levels[0].nodes, len(levels)))):
         for name in grid.METRIC_NAMES:
             lev.arrays[name][:] = m.arrays[name]
-        lev.arrays["DISTW"][:] = case.wall_distance_tri(lev, tri)
+        lev.arrays["DISTW"][:] = case.wall_distance_points(lev, walls)
+        if q:
+            case.lump_wall_distance(levels[q - 1], lev)
     om = OracleMG(levels, prms)
     om.start()
     om.cycle(1)
@@ -543,7 +545,7 @@ def run_large(args):
     dev = not args.host_setup   # metrics and wall distance on the device (ff_block_metrics_levels)
     it = _large_blocks(cells, nlev, fp32=fp32, ddadi=args.ddadi, device_setup=dev)
     _, fs = next(it)
-    tri = next(it)[1] if dev else None
+    walls = next(it)[1] if dev else None
     fine_cells, fine_ntot = [], []
     for n, (levels, prms) in enumerate(it):
         fine = levels[0]
@@ -561,8 +563,7 @@ def run_large(args):
             g.upload(bid + q)
         if dev:
             g.block_metrics_levels(bid, nlev, *fine.nodes)
-            for q in range(nlev):
-                g.wall_distance(bid + q, tri)
+            g.wall_distance(bid, walls)
         for q in range(nlev):
             levels[q].arrays = {}
         fine_cells.append(fine.imax * fine.jmax * fine.kmax)

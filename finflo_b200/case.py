@@ -298,98 +298,89 @@ def init_freestream(b: Block, fs, *, noise=1e-3, seed=0):
     return b
 
 
-def _closest_on_triangles(p, a, b, c):
-    """Distance from points p (n,3) to triangles (a,b,c) (n,3 each): the
-    closest-point regions of a triangle (vertex, edge, face), vectorised."""
-    ab, ac, ap = b - a, c - a, p - a
-    d1, d2 = np.einsum("ij,ij->i", ab, ap), np.einsum("ij,ij->i", ac, ap)
-    bp = p - b
-    d3, d4 = np.einsum("ij,ij->i", ab, bp), np.einsum("ij,ij->i", ac, bp)
-    cp = p - c
-    d5, d6 = np.einsum("ij,ij->i", ab, cp), np.einsum("ij,ij->i", ac, cp)
-    va = d3 * d6 - d5 * d4
-    vb = d5 * d2 - d1 * d6
-    vc = d1 * d4 - d3 * d2
-    den = np.where(va + vb + vc == 0, 1.0, va + vb + vc)
-    v, w = vb / den, vc / den
-    q = a + ab * v[:, None] + ac * w[:, None]                      # inside the face
-    with np.errstate(divide="ignore", invalid="ignore"):
-        t_ab = np.clip(np.where(d1 - d3 != 0, d1 / (d1 - d3), 0), 0, 1)
-        t_ac = np.clip(np.where(d2 - d6 != 0, d2 / (d2 - d6), 0), 0, 1)
-        t_bc = np.clip(np.where((d4 - d3) + (d5 - d6) != 0, (d4 - d3) / ((d4 - d3) + (d5 - d6)), 0), 0, 1)
-    e_ab = a + ab * t_ab[:, None]
-    e_ac = a + ac * t_ac[:, None]
-    e_bc = b + (c - b) * t_bc[:, None]
-    cand = [q, a, b, c, e_ab, e_ac, e_bc]
-    inside = (va >= 0) & (vb >= 0) & (vc >= 0)
-    dist = np.full(len(p), np.inf)
-    for k, x in enumerate(cand):
-        dk = np.linalg.norm(p - x, axis=1)
-        if k == 0:
-            dk = np.where(inside, dk, np.inf)
-        dist = np.minimum(dist, dk)
-    return dist
+# ---- wall distance (DISTANCES gluebm.f:9136) ---------------------------------
+
+def _kpass_centres(P):
+    """AREVC1's cell centres (its last, k-direction pass: corners at the
+    offsets 0, j, i+j, i, k, k+j, k+i+j, k+i, summed in that order) of the
+    cells spanned by the node array P [k, j, i, 3]."""
+    nk, nj, ni = P.shape[0] - 1, P.shape[1] - 1, P.shape[2] - 1
+
+    def c(di, dj, dk):
+        return P[dk:dk + nk, dj:dj + nj, di:di + ni]
+
+    return 0.125 * (c(0, 0, 0) + c(0, 1, 0) + c(1, 1, 0) + c(1, 0, 0) + c(0, 0, 1) + c(0, 1, 1) + c(1, 1, 1)
+                    + c(1, 0, 1))
 
 
-def wall_triangles(wb: Block) -> np.ndarray:
-    """The solid-wall faces (patch types 7-10) of wb's nodes, each split in
-    two triangles: [ntri, 9] = corners a, b, c."""
-    X, Y, Z = wb.nodes
+def wall_points(nodes, patches):
+    """PICK_XYZ gluebm.f:9452 for one block: the points halfway between the
+    centre of the first interior cell and of the first ghost cell at every
+    cell of its solid patches (ICON(1) 8..10), [n, 3], in patch order and,
+    within a patch, the second in-face index outermost.  The centres are
+    AREVC1's (the ghost cell's nodes reflected through the face, GRIDEX)."""
+    X, Y, Z = nodes
     P = np.stack([X, Y, Z], axis=-1)
-    tris = []
-    for pa in wb.patches:
-        if not (7 <= pa.ityp <= 10):
+    out = []
+    for pa in patches:
+        if not 8 <= pa.ityp <= 10:
             continue
-        d = (pa.iface - 1) % 3
-        idx = 0 if pa.iface <= 3 else (P.shape[2 - d] - 1)
-        sl = [slice(None)] * 3
-        sl[2 - d] = idx
-        F = P[tuple(sl)]
-        n00, n10, n01, n11 = F[:-1, :-1], F[1:, :-1], F[:-1, 1:], F[1:, 1:]
-        for a, b, c in ((n00, n10, n11), (n00, n11, n01)):
-            tris.append(np.concatenate([a.reshape(-1, 3), b.reshape(-1, 3), c.reshape(-1, 3)], axis=1))
-    return np.concatenate(tris) if tris else np.zeros((0, 9))
+        d = (pa.iface - 1) % 3          # 0 = i, 1 = j, 2 = k
+        ax = 2 - d                      # its axis of P
+        n = P.shape[ax]
+        if pa.iface <= 3:               # the reflected node plane, then planes 0 and 1
+            pl = [2 * np.take(P, 0, axis=ax) - np.take(P, 1, axis=ax), np.take(P, 0, axis=ax),
+                  np.take(P, 1, axis=ax)]
+        else:
+            pl = [np.take(P, n - 2, axis=ax), np.take(P, n - 1, axis=ax),
+                  2 * np.take(P, n - 1, axis=ax) - np.take(P, n - 2, axis=ax)]
+        slab = np.stack(pl, axis=ax)
+        cen = _kpass_centres(slab)                   # two cells along the normal
+        lo, hi = np.take(cen, 0, axis=ax), np.take(cen, 1, axis=ax)
+        pt = 0.5 * (lo + hi)                         # XC(KMI) + XC(KMA): the lower cell first
+        # pt is [second, first] in-face index for every face direction
+        sub = pt[pa.r2a - 1:pa.r2b, pa.r1a - 1:pa.r1b]
+        out.append(sub.reshape(-1, 3))
+    return np.concatenate(out) if out else np.zeros((0, 3))
 
 
-def wall_distance(blk: Block, wall_block: Block = None, nnear: int = 8):
-    """DISTW: distance of every cell centre (ghosts included) to the nearest
-    point of the solid-wall surface of wall_block (default: blk itself;
-    coarse multigrid levels pass the finest level, whose nodes they lack),
-    each wall face split into two triangles -- set-up data, like the
-    reference's DISTANCES pass before the iteration loop."""
-    wb = wall_block if wall_block is not None else blk
-    return wall_distance_tri(blk, wall_triangles(wb), nnear)
-
-
-def wall_distance_tri(blk: Block, T: np.ndarray, nnear: int = 8):
-    """DISTW of every cell centre of blk to the nearest of the wall triangles
-    T ([ntri, 9]: three corners each), searching the nnear triangles with
-    the nearest centroids (1e3 without triangles)."""
+def wall_distance_points(blk: Block, pts, ncand: int = 8):
+    """WALL_DIST gluebm.f:9533: DISTW of every storage cell of blk, the
+    distance of its centre to the nearest wall point (squared distances
+    (dx^2 + dy^2) + dz^2 compared, the root of the least; 1e4 without
+    points, the root of DISTANCES' initial 1e8).  The ncand points nearest
+    by a k-d tree are the candidates."""
+    if not len(pts):
+        return np.full(blk.ntot, 1.0e4)
     from scipy.spatial import cKDTree
-    if not len(T):
-        return np.full(blk.ntot, 1.0e3)
-    A, B, C = T[:, 0:3], T[:, 3:6], T[:, 6:9]
-    cen = (A + B + C) / 3.0
-    tree = cKDTree(cen)
     q = np.stack([blk.arrays["XC"], blk.arrays["YC"], blk.arrays["ZC"]], axis=1)
-    k = min(nnear, len(cen))
-    _, idx = tree.query(q, k=k, workers=-1)
+    k = min(ncand, len(pts))
+    _, idx = cKDTree(pts).query(q, k=k, workers=-1)
     idx = idx.reshape(len(q), k)
-    best = np.full(len(q), np.inf)
+    best = np.full(len(q), 1.0e8)
+    for j in range(k):
+        p = pts[idx[:, j]]
+        dx, dy, dz = q[:, 0] - p[:, 0], q[:, 1] - p[:, 1], q[:, 2] - p[:, 2]
+        r = dx * dx + dy * dy + dz * dz
+        best = np.where(r < best, r, best)
+    return np.sqrt(best)
 
-    def chunk(lo, hi):   # NumPy releases the GIL on these array operations
-        qq, b = q[lo:hi], best[lo:hi]
-        for j in range(k):
-            t = idx[lo:hi, j]
-            np.minimum(b, _closest_on_triangles(qq, A[t], B[t], C[t]), out=b)
 
-    import os
-    from concurrent.futures import ThreadPoolExecutor
-    nth = max(1, min(os.cpu_count() or 1, len(q) // 65536))
-    bounds = np.linspace(0, len(q), nth + 1).astype(int)
-    with ThreadPoolExecutor(nth) as ex:
-        list(ex.map(lambda b: chunk(*b), zip(bounds[:-1], bounds[1:])))
-    return best
+def lump_wall_distance(fine: Block, coarse: Block):
+    """LUMP_DIST gluebm.f:9562: the coarse interior cells' DISTW, the mean
+    of their eight children in LUMPVS's order (in place; the coarse ghost
+    cells keep theirs)."""
+    f = fine.arrays["DISTW"].reshape(fine.kmax + 4, fine.jmax + 4, fine.imax + 4)
+    c = coarse.arrays["DISTW"].reshape(coarse.kmax + 4, coarse.jmax + 4, coarse.imax + 4)
+    ci, cj, ck = coarse.imax, coarse.jmax, coarse.kmax
+
+    def child(di, dj, dk):
+        return f[2 + dk:2 + dk + 2 * ck:2, 2 + dj:2 + dj + 2 * cj:2, 2 + di:2 + di + 2 * ci:2]
+
+    ra = child(0, 0, 0)
+    for o in ((0, 1, 0), (0, 0, 1), (0, 1, 1), (1, 0, 0), (1, 1, 0), (1, 0, 1), (1, 1, 1)):
+        ra = ra + child(*o)
+    c[2:-2, 2:-2, 2:-2] = 0.125 * ra
 
 
 def sst_freestream(fs, tu=1.0e-3, mut_ratio=0.1):
@@ -418,18 +409,26 @@ def bump_case(ni=65, nj=33, nk=33, *, h1=1e-3, amp=0.1, mach=0.5, reynolds=1e4,
     return blk, prm, fs
 
 
-def setup_sst(blk: Block, prm: FFParams, fs, tu=1.0e-3, mut_ratio=0.1, wall_block: Block = None, distw=True):
+def setup_sst(blk: Block, prm: FFParams, fs, tu=1.0e-3, mut_ratio=0.1, walls=None, fine: Block = None,
+              distw=True):
     """Switch a case to k-omega SST: ITURB=6, the free-stream limits RKLIM /
-    EPSLIM, inlet BOUNRK/BOUNEP, DISTW (distw=False leaves it to the device,
-    ff_wall_distance), and rho*k, rho*omega, mu_t of the free stream in
-    every cell."""
+    EPSLIM, inlet BOUNRK/BOUNEP, DISTW, and rho*k, rho*omega, mu_t of the
+    free stream in every cell.  DISTW: the distance to the wall points
+    `walls` (default: blk's own solid patches, from its nodes); a coarse
+    level passes its finer level as `fine`, whose DISTW its interior cells
+    average (LUMP_DIST).  distw=False leaves it to the device
+    (ff_wall_distance)."""
     rk, re = sst_freestream(fs, tu, mut_ratio)
     prm.iturb = 6
     prm.rklim, prm.epslim = rk, re
     for pa in blk.patches:
         pa.bounrk, pa.bounep = rk, re
     if distw:
-        blk.arrays["DISTW"][:] = wall_distance(blk, wall_block)
+        if walls is None:
+            walls = wall_points(blk.nodes, blk.patches)
+        blk.arrays["DISTW"][:] = wall_distance_points(blk, walls)
+        if fine is not None:
+            lump_wall_distance(fine, blk)
     blk.arrays["RK"][:] = rk
     blk.arrays["REPS"][:] = re
     blk.arrays["EPS2"][:] = 1.0 + mut_ratio
@@ -457,9 +456,10 @@ def bump_case_mg(ni=65, nj=33, nk=33, nlev=3, *, h1=1e-3, amp=0.1, mach=0.5, rey
         levels.append(blk)
     prm = make_params(fc, levels[0].dims, cfl=cfl, cfll=cfll, inter=inter)
     if turbulence == "sst":
+        walls = wall_points(levels[0].nodes, levels[0].patches)
         for lev, blk in enumerate(levels):
             setup_sst(blk, prm if lev == 0 else FFParams.from_buffer_copy(prm), fs, tu=tu,
-                      mut_ratio=mut_ratio, wall_block=levels[0])
+                      mut_ratio=mut_ratio, walls=walls, fine=levels[lev - 1] if lev else None)
     prms = [level_params(prm, lev + 1) for lev in range(nlev)]
     prms[0].lusgs_fp32 = int(lusgs_fp32)
     for q in prms[1:]:
@@ -577,15 +577,13 @@ def bump_block_cuts(cells, nb, seed, quantum=4, spread=0.1):
     return cuts
 
 
-class _WallSurface:
-    """The solid walls of the whole channel (lower and upper node planes) in
-    the form wall_distance reads."""
-
-    def __init__(self, X, Y, Z):
-        sl = (slice(None), [0, -1], slice(None))
-        self.nodes = (X[sl], Y[sl], Z[sl])
-        kmax, imax = X.shape[0] - 1, X.shape[2] - 1
-        self.patches = [_patch(grid.BC_SOL, 2, (1, imax), (1, kmax)), _patch(grid.BC_SOL, 5, (1, imax), (1, kmax))]
+def channel_wall_points(X, Y, Z):
+    """The wall points of the whole channel's lower and upper walls: those
+    of the solid j faces of all its blocks (the nearest point does not
+    depend on their order)."""
+    kmax, imax = X.shape[0] - 1, X.shape[2] - 1
+    pats = [_patch(grid.BC_SOL, 2, (1, imax), (1, kmax)), _patch(grid.BC_SOL, 5, (1, imax), (1, kmax))]
+    return wall_points((X, Y, Z), pats)
 
 
 def bump_multiblock_blocks(cells=(512, 256, 128), nb=(2, 2, 2), nlev=3, *, seed=5, h1=2e-6, amp=0.1,
@@ -604,15 +602,16 @@ def bump_multiblock_blocks(cells=(512, 256, 128), nb=(2, 2, 2), nlev=3, *, seed=
     yields the free stream first: the first item is ("fs", fs).  With
     device_setup the metric arrays and DISTW are left at zero for
     ff_block_metrics_levels / ff_wall_distance: the second item is then
-    ("wall", triangles), and each level-1 block carries its nodes."""
+    ("wall", points) (the channel's wall points, [n, 3]), and each level-1
+    block carries its nodes."""
     fc = FlowConditions(mach=mach, reynolds=reynolds)
     fs = fc.freestream()
     yield "fs", fs
     NI, NJ, NK = cells
     X, Y, Z = grid.bump_nodes(NI + 1, NJ + 1, NK + 1, h1=h1, amp=amp, zlen=zlen, span_amp=span_amp)
-    wall = _WallSurface(X, Y, Z)
+    wall = channel_wall_points(X, Y, Z)
     if device_setup:
-        yield "wall", wall_triangles(wall)
+        yield "wall", wall
     cut = bump_block_cuts(cells, nb, seed)
     ids = {}
     for c in range(nb[2]):
@@ -659,7 +658,8 @@ def bump_multiblock_blocks(cells=(512, 256, 128), nb=(2, 2, 2), nlev=3, *, seed=
         if turbulence == "sst":
             for lev, blk in enumerate(levels):
                 setup_sst(blk, prm if lev == 0 else FFParams.from_buffer_copy(prm), fs, tu=tu,
-                          mut_ratio=mut_ratio, wall_block=wall, distw=not device_setup)
+                          mut_ratio=mut_ratio, walls=wall, fine=levels[lev - 1] if lev else None,
+                          distw=not device_setup)
         prms = [level_params(prm, lev + 1) for lev in range(nlev)]
         prms[0].lusgs_fp32 = int(lusgs_fp32)
         for q in prms[1:]:
@@ -669,7 +669,7 @@ def bump_multiblock_blocks(cells=(512, 256, 128), nb=(2, 2, 2), nlev=3, *, seed=
 
 def bump_multiblock_case(*args, **kw):
     """All blocks of bump_multiblock_blocks at once: (block_levels,
-    block_prms, fs), and the wall triangles last with device_setup."""
+    block_prms, fs), and the wall points last with device_setup."""
     it = bump_multiblock_blocks(*args, **kw)
     _, fs = next(it)
     tri = next(it)[1] if kw.get("device_setup") else None

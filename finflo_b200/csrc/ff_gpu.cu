@@ -2102,53 +2102,29 @@ int ff_block_metrics_levels(void* ctx, int blk, int nlev, const double* xyz) {
   return 0;
 }
 
-int ff_wall_distance(void* ctx, int blk, const double* tri, int ntri) {
+int ff_wall_distance(void* ctx, int blk, const double* pts, int npts) {
   Ctx* c = (Ctx*)ctx;
   BlockCtx* b = getb(c, blk);
-  if (!b || ntri < 0 || (ntri > 0 && !tri)) return fail(c, FF_ERR_ARG, "ff_wall_distance");
-  // tiles of WD_TT triangles with their bounding boxes (pruned search), or
-  // the plain search over all triangles for very long lists
-  const int ntile = (ntri + WD_TT - 1) / WD_TT;
-  const bool pruned = ntile > 0 && wd_pruned_smem(ntile) <= (size_t)c->smem_optin;
-  std::vector<double> box(pruned ? (size_t)ntile * 6 : 0);
-  for (int q = 0; q < (pruned ? ntile : 0); q++) {
-    double* bx = &box[(size_t)q * 6];
-    for (int cc = 0; cc < 3; cc++) { bx[cc] = 1e300; bx[3 + cc] = -1e300; }
-    for (int u = q * WD_TT; u < std::min(ntri, (q + 1) * WD_TT); u++)
-      for (int v = 0; v < 3; v++)
-        for (int cc = 0; cc < 3; cc++) {
-          const double x = tri[(size_t)u * 9 + 3 * v + cc];
-          bx[cc] = std::min(bx[cc], x);
-          bx[3 + cc] = std::max(bx[3 + cc], x);
-        }
-  }
-  double *dt = nullptr, *dbox = nullptr;
-  if (ntri > 0) CK(cudaMalloc(&dt, (size_t)ntri * 9 * sizeof(double)));
-  if (pruned && cudaMalloc(&dbox, box.size() * sizeof(double)) != cudaSuccess) {
-    cudaFree(dt);
-    return fail(c, FF_ERR_CUDA, "ff_wall_distance");
-  }
-  cudaError_t e = ntri > 0 ? cudaMemcpyAsync(dt, tri, (size_t)ntri * 9 * sizeof(double), cudaMemcpyHostToDevice, c->stream)
+  if (!b || npts < 0 || (npts > 0 && !pts)) return fail(c, FF_ERR_ARG, "ff_wall_distance");
+  double* dp = nullptr;
+  if (npts > 0) CK(cudaMalloc(&dp, (size_t)npts * 3 * sizeof(double)));
+  cudaError_t e = npts > 0 ? cudaMemcpyAsync(dp, pts, (size_t)npts * 3 * sizeof(double), cudaMemcpyHostToDevice, c->stream)
                            : cudaSuccess;
-  if (e == cudaSuccess && pruned)
-    e = cudaMemcpyAsync(dbox, box.data(), box.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
-  if (e == cudaSuccess) {
-    if (pruned) {
-      const size_t sm = wd_pruned_smem(ntile);
-      cudaFuncSetAttribute(k_wall_distance_pruned, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      const int is = b->imax + 4, js = b->jmax + 4, ks = b->kmax + 4;
-      const int nb = nblk(is, WD_BI) * nblk(js, WD_BJ) * nblk(ks, WD_BK);
-      k_wall_distance_pruned<<<nb, WD_THREADS, sm, c->stream>>>(b->db, dt, ntri, dbox, ntile);
-    } else {
-      k_wall_distance<<<nblk((long)b->ntot, WD_THREADS), WD_THREADS, 0, c->stream>>>(b->db, dt, ntri);
-    }
+  // the block, then each coarser level: every cell's nearest point, and
+  // the interior cells again as the mean of their children (LUMP_DIST)
+  BlockCtx* fine = nullptr;
+  for (BlockCtx* x = b; x && e == cudaSuccess; fine = x, x = x->coarse) {
+    k_wall_distance<<<nblk((long)x->ntot, WD_THREADS), WD_THREADS, 0, c->stream>>>(x->db, dp, npts);
     c->nlaunch++;
-    e = cudaStreamSynchronize(c->stream);
+    if (fine) {
+      k_lump_distw<<<nblk((long)x->imax * x->jmax * x->kmax, 256), 256, 0, c->stream>>>(fine->db, x->db);
+      c->nlaunch++;
+    }
+    e = cudaGetLastError();
   }
-  if (dt) cudaFree(dt);
-  if (dbox) cudaFree(dbox);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (dp) cudaFree(dp);
   if (e != cudaSuccess) return fail(c, FF_ERR_CUDA, "ff_wall_distance", e);
-  CK(cudaGetLastError());
   return 0;
 }
 

@@ -244,9 +244,10 @@ class GpuSolver:
         xyz = np.ascontiguousarray(np.concatenate([np.ravel(X), np.ravel(Y), np.ravel(Z)]), dtype=np.float64)
         self._check(self.L.ff_block_metrics_levels(self.ctx, bid, nlev, xyz.ctypes.data))
 
-    def wall_distance(self, bid, tri):
-        """DISTW on the device from wall triangles tri [ntri, 9] (corners a, b, c)."""
-        t = np.ascontiguousarray(tri, dtype=np.float64).reshape(-1, 9)
+    def wall_distance(self, bid, pts):
+        """DISTW on the device of the block and its linked coarse levels from
+        the wall points pts [n, 3] (case.wall_points, PICK_XYZ)."""
+        t = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
         self._check(self.L.ff_wall_distance(self.ctx, bid, t.ctypes.data if len(t) else None, len(t)))
 
     def time_levels(self, bid=0, mode=1):

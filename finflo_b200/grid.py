@@ -12,12 +12,15 @@ N-1 and N), pointing towards +i; likewise A2 (j) and A3 (k).  ``D1..D3`` are
 the cell thicknesses of D1D2D3 (gluebm.f:2326-2372):
 ``min(1e4, (V+eps)/(A_low+A_high+eps)*2)``.
 
-The grid metrics themselves (GRIVAL/AREVC1, ns3c.f:5636, gluebm.f:1586) are not
-restated: this module computes them from node coordinates with the
-diagonal-cross-product face vectors, so every cell is exactly closed
-(sum of outward face vectors = 0) and ghost cells get the geometry of
-mirror-extrapolated ghost nodes.  The oracle and the CUDA path both take the
-metrics as inputs, so parity does not depend on how they were produced.
+The metrics follow the reference's set-up (GRIVAL ns3c.f:5636 -> GRID1B
+gluebm.f:1265): ghost nodes as GRIDEX (1029), face areas, unit normals,
+volumes (three passes) and centres as AREVC1 (1586), thicknesses as D1D2D3
+(2326), coarse levels as LUMPA1 / LUMPVS (2194, 2256), in the reference's
+order of operations, so that the interior cells, their faces and the first
+ghost layer equal the reference's to the bit.  The further ghost layers (the
+reference fills them in BOUNDX / BOUNDV / MIRC / CONEC after GRID1B) come
+from continued mirror reflection of the nodes and, on coarse levels, from
+lumping the fine ghost cells.
 """
 from __future__ import annotations
 
@@ -102,14 +105,44 @@ def box_nodes(x, y, z):
 
 
 def _extend(a: np.ndarray, ng: int = NG) -> np.ndarray:
-    """Add ng ghost node layers per side by mirror extrapolation x[-m] = 2x[0]-x[m]."""
+    """Add ng ghost node layers per side.  The first layer is GRIDEX's
+    (gluebm.f:1029, REFXYZ 1175): faces reflected, x[-1] = 2 x[0] - x[1],
+    and the edges and corners reflected diagonally through the first
+    interior node, x[-1, -1] = 2 x[0, 0] - x[1, 1].  Further layers (the
+    reference keeps one) continue the mirror reflection along each axis in
+    turn, x[-m] = 2 x[0] - x[m]."""
     for ax in range(3):
         n = a.shape[ax]
         lo = [2 * np.take(a, 0, axis=ax) - np.take(a, m, axis=ax) for m in range(ng, 0, -1)]
         hi = [2 * np.take(a, n - 1, axis=ax) - np.take(a, n - 1 - m, axis=ax) for m in range(1, ng + 1)]
         a = np.concatenate([np.expand_dims(t, ax) for t in lo] + [a]
                            + [np.expand_dims(t, ax) for t in hi], axis=ax)
+    if ng >= 1:
+        _gridex_edges(a, ng)
     return a
+
+
+def _gridex_edges(e: np.ndarray, ng: int):
+    """GRIDEX's diagonal reflection of the first-layer edge and corner nodes
+    of the extended array e (ng layers), in place."""
+    n = [e.shape[ax] - 2 * ng for ax in range(3)]
+
+    def pos(ax, side):   # (ghost, first interior, second interior) indices
+        return (ng - 1, ng, ng + 1) if side == 0 else (ng + n[ax], ng + n[ax] - 1, ng + n[ax] - 2)
+
+    for u, v in ((0, 1), (0, 2), (1, 2)):        # edges: two ghost axes, the third interior
+        w = 3 - u - v
+        for su in (0, 1):
+            for sv in (0, 1):
+                pu, pv = pos(u, su), pos(v, sv)
+                idx, src1, src2 = [None] * 3, [None] * 3, [None] * 3
+                idx[u], idx[v], idx[w] = pu[0], pv[0], slice(ng, ng + n[w])
+                src1[u], src1[v], src1[w] = pu[1], pv[1], slice(ng, ng + n[w])
+                src2[u], src2[v], src2[w] = pu[2], pv[2], slice(ng, ng + n[w])
+                e[tuple(idx)] = 2. * e[tuple(src1)] - e[tuple(src2)]
+    for c in range(8):                           # corners
+        p = [pos(ax, (c >> ax) & 1) for ax in range(3)]
+        e[p[0][0], p[1][0], p[2][0]] = 2. * e[p[0][1], p[1][1], p[2][1]] - e[p[0][2], p[1][2], p[2][2]]
 
 
 @dataclass
@@ -129,96 +162,121 @@ METRIC_NAMES = ("A1", "A1XA", "A1YA", "A1ZA", "A2", "A2XA", "A2YA", "A2ZA",
                 "D1", "D2", "D3")
 
 
+# AREVC1's corner nodes of a cell in its pass for direction d (0 = i, 1 = j,
+# 2 = k): the pass's (ISTR, JSTR, KSTR) are the axes (d, d+1, d+2) cyclic,
+# and the corners IT1..IT8 step by 0, KSTR, JSTR+KSTR, JSTR, ISTR,
+# ISTR+KSTR, ISTR+JSTR+KSTR, ISTR+JSTR (gluebm.f:1640-1660).
+def _corner_offsets(d):
+    a, b, c = d, (d + 1) % 3, (d + 2) % 3
+    steps = ((), (c,), (b, c), (b,), (a,), (a, c), (a, b, c), (a, b))
+    out = []
+    for st in steps:
+        o = [0, 0, 0]
+        for ax in st:
+            o[ax] = 1
+        out.append(tuple(o))   # (di, dj, dk)
+    return out
+
+
+def _arevc1(P, ncell):
+    """AREVC1 gluebm.f:1586 on the extended nodes P [k, j, i, 3] for every
+    cell of the ncell = (ci, cj, ck) storage range: per direction the face
+    vectors (AXX, AYY, AZZ) of the ncell[d] + 1 face planes, and the cell
+    volumes accumulated over the three passes (VSUM, VDIV) and the centres
+    of the last pass."""
+    ci, cj, ck = ncell
+    faces, vol, cen = [], None, None
+    for d in range(3):
+        nf = [ci, cj, ck]
+        nf[d] += 1
+        offs = _corner_offsets(d)
+
+        def corner(q, nrange):
+            di, dj, dk = offs[q]
+            return P[dk:dk + nrange[2], dj:dj + nrange[1], di:di + nrange[0]]
+
+        # face vectors of the face planes 0..ncell[d] (IT0 form, corners 1-4)
+        p1, p2, p3, p4 = (corner(q, nf) for q in range(4))
+        x1, y1, z1 = p1[..., 0], p1[..., 1], p1[..., 2]
+        x2, y2, z2 = p2[..., 0], p2[..., 1], p2[..., 2]
+        x3, y3, z3 = p3[..., 0], p3[..., 1], p3[..., 2]
+        x4, y4, z4 = p4[..., 0], p4[..., 1], p4[..., 2]
+        axx = 0.5 * ((z3 - z1) * (y4 - y2) - (y3 - y1) * (z4 - z2))
+        ayy = 0.5 * ((x3 - x1) * (z4 - z2) - (z3 - z1) * (x4 - x2))
+        azz = 0.5 * ((y3 - y1) * (x4 - x2) - (x3 - x1) * (y4 - y2))
+        faces.append(np.stack([axx, ayy, azz], axis=-1))
+        # the cell terms of the pass: centre, diagonals, low and high face
+        c = [corner(q, ncell) for q in range(8)]
+        xce = 0.125 * (c[0] + c[1] + c[2] + c[3] + c[4] + c[5] + c[6] + c[7])
+        rd = xce - 0.5 * (c[0] + c[1])
+        rd2 = xce - 0.5 * (c[6] + c[7])
+        sl_lo = [slice(0, ck), slice(0, cj), slice(0, ci)]
+        sl_hi = list(sl_lo)
+        sl_hi[2 - d] = slice(1, ncell[d] + 1)
+        lo = faces[d][tuple(sl_lo)]
+        hi = -faces[d][tuple(sl_hi)]                 # AXX2 = -(next cell's AXX)
+        # (VSUM V + RDIAG.A + RD2AG.A2) / VDIV, summed left to right
+        v = np.zeros(lo.shape[:-1]) if d == 0 else vol
+        for t in (rd[..., 0] * lo[..., 0], rd[..., 1] * lo[..., 1], rd[..., 2] * lo[..., 2],
+                  rd2[..., 0] * hi[..., 0], rd2[..., 1] * hi[..., 1], rd2[..., 2] * hi[..., 2]):
+            v = v + t
+        vol = v / 3.0 if d == 2 else v
+        cen = xce
+    return faces, vol, cen
+
+
+def _area_normal(S):
+    """AREVC1's area A = sqrt(AXX**2 + AYY**2 + AZZ**2) and unit normal
+    A*/(A + 1e-20); a zero-area face keeps the normal (1, 0, 0)."""
+    a = np.sqrt(S[..., 0] * S[..., 0] + S[..., 1] * S[..., 1] + S[..., 2] * S[..., 2])
+    n = S / (a + 1.0e-20)[..., None]
+    z = a < 1.0e-20
+    n[z] = (1.0, 0.0, 0.0)
+    return a, n
+
+
 def compute_metrics(X, Y, Z, ng: int = NG, raw: bool = False):
-    """Metrics of all cells (ng ghost layers) from interior node arrays (nk,nj,ni)."""
+    """Metrics of all cells (ng ghost layers) from interior node arrays
+    (nk, nj, ni), by AREVC1 on the GRIDEX-extended nodes; D1..D3 as
+    D1D2D3 (gluebm.f:2326)."""
     nk, nj, ni = X.shape
     imax, jmax, kmax = ni - 1, nj - 1, nk - 1
     P = np.stack([_extend(X, ng), _extend(Y, ng), _extend(Z, ng)], axis=-1)
-    ks, js, is_ = kmax + 2 * ng, jmax + 2 * ng, imax + 2 * ng
-
-    def face_vec(c00, c11, c01, c10):
-        return 0.5 * np.cross(c11 - c00, c01 - c10)
-
-    # i-faces on the low side of storage (s,t,u): node plane s
-    p = P
-    Si = face_vec(p[:ks, :js, :is_], p[1:ks + 1, 1:js + 1, :is_],
-                  p[1:ks + 1, :js, :is_], p[:ks, 1:js + 1, :is_])
-    Sj = face_vec(p[:ks, :js, :is_], p[1:ks + 1, :js, 1:is_ + 1],
-                  p[:ks, :js, 1:is_ + 1], p[1:ks + 1, :js, :is_])
-    Sk = face_vec(p[:ks, :js, :is_], p[:ks, 1:js + 1, 1:is_ + 1],
-                  p[:ks, 1:js + 1, :is_], p[:ks, :js, 1:is_ + 1])
-    # high-side faces needed for the volume / D arrays
-    Si_hi = face_vec(p[:ks, :js, 1:is_ + 1], p[1:ks + 1, 1:js + 1, 1:is_ + 1],
-                     p[1:ks + 1, :js, 1:is_ + 1], p[:ks, 1:js + 1, 1:is_ + 1])
-    Sj_hi = face_vec(p[:ks, 1:js + 1, :is_], p[1:ks + 1, 1:js + 1, 1:is_ + 1],
-                     p[:ks, 1:js + 1, 1:is_ + 1], p[1:ks + 1, 1:js + 1, :is_])
-    Sk_hi = face_vec(p[1:ks + 1, :js, :is_], p[1:ks + 1, 1:js + 1, 1:is_ + 1],
-                     p[1:ks + 1, 1:js + 1, :is_], p[1:ks + 1, :js, 1:is_ + 1])
-
-    def centroid(a, b, c, d):
-        return 0.25 * (a + b + c + d)
-
-    ci_lo = centroid(p[:ks, :js, :is_], p[1:ks + 1, :js, :is_], p[:ks, 1:js + 1, :is_], p[1:ks + 1, 1:js + 1, :is_])
-    ci_hi = centroid(p[:ks, :js, 1:is_ + 1], p[1:ks + 1, :js, 1:is_ + 1], p[:ks, 1:js + 1, 1:is_ + 1], p[1:ks + 1, 1:js + 1, 1:is_ + 1])
-    cj_lo = centroid(p[:ks, :js, :is_], p[1:ks + 1, :js, :is_], p[:ks, :js, 1:is_ + 1], p[1:ks + 1, :js, 1:is_ + 1])
-    cj_hi = centroid(p[:ks, 1:js + 1, :is_], p[1:ks + 1, 1:js + 1, :is_], p[:ks, 1:js + 1, 1:is_ + 1], p[1:ks + 1, 1:js + 1, 1:is_ + 1])
-    ck_lo = centroid(p[:ks, :js, :is_], p[:ks, 1:js + 1, :is_], p[:ks, :js, 1:is_ + 1], p[:ks, 1:js + 1, 1:is_ + 1])
-    ck_hi = centroid(p[1:ks + 1, :js, :is_], p[1:ks + 1, 1:js + 1, :is_], p[1:ks + 1, :js, 1:is_ + 1], p[1:ks + 1, 1:js + 1, 1:is_ + 1])
-
-    vol = (np.sum(ci_hi * Si_hi, -1) - np.sum(ci_lo * Si, -1)
-           + np.sum(cj_hi * Sj_hi, -1) - np.sum(cj_lo * Sj, -1)
-           + np.sum(ck_hi * Sk_hi, -1) - np.sum(ck_lo * Sk, -1)) / 3.0
-    cen = 0.125 * sum(p[a:a + ks, b:b + js, c:c + is_] for a in (0, 1) for b in (0, 1) for c in (0, 1))
-
-    out = {}
-    for name, S in (("A1", Si), ("A2", Sj), ("A3", Sk)):
-        mag = np.sqrt(np.sum(S * S, -1))
-        safe = np.where(mag > 0, mag, 1.0)
-        out[name] = mag
-        out[name + "XA"] = S[..., 0] / safe
-        out[name + "YA"] = S[..., 1] / safe
-        out[name + "ZA"] = S[..., 2] / safe
-    out["VOL"] = vol
-    out["XC"], out["YC"], out["ZC"] = cen[..., 0], cen[..., 1], cen[..., 2]
-    eps = 1e-20
-    a1h = np.sqrt(np.sum(Si_hi * Si_hi, -1))
-    a2h = np.sqrt(np.sum(Sj_hi * Sj_hi, -1))
-    a3h = np.sqrt(np.sum(Sk_hi * Sk_hi, -1))
-    out["D1"] = np.minimum(1e4, (vol + eps) / (out["A1"] + a1h + eps) * 2.0)
-    out["D2"] = np.minimum(1e4, (vol + eps) / (out["A2"] + a2h + eps) * 2.0)
-    out["D3"] = np.minimum(1e4, (vol + eps) / (out["A3"] + a3h + eps) * 2.0)
+    ncell = (imax + 2 * ng, jmax + 2 * ng, kmax + 2 * ng)
+    faces, vol, cen = _arevc1(P, ncell)
+    r = dict(dims=(imax, jmax, kmax), ng=ng, VOL=vol, C=cen)
+    for d in range(3):
+        r[f"A{d + 1}"], r[f"N{d + 1}"] = _area_normal(faces[d])
     if raw:
-        return dict(S1=Si, S2=Sj, S3=Sk, S1h=Si_hi, S2h=Sj_hi, S3h=Sk_hi, VOL=vol, C=cen,
-                    dims=(imax, jmax, kmax), ng=ng)
-    m = Metrics(imax, jmax, kmax)
-    for k2 in METRIC_NAMES:
-        m.arrays[k2] = np.ascontiguousarray(out[k2], dtype=np.float64).reshape(-1)
-    return m
+        return r
+    return _finish(r)
 
 
-def _finish(S1, S2, S3, S1h, S2h, S3h, vol, cen, dims, ng):
-    """Metrics arrays (2 ghost layers) from face vectors, volumes and centres
-    given with ng >= 2 ghost layers."""
-    imax, jmax, kmax = dims
+def _finish(r):
+    """Metrics arrays (2 ghost layers) from per-face areas and normals
+    (one more face plane than cells in each face's direction), volumes and
+    centres given with ng >= 2 ghost layers."""
+    imax, jmax, kmax = r["dims"]
+    ng = r["ng"]
     c = ng - NG
-    sl = (slice(c, c + kmax + 2 * NG), slice(c, c + jmax + 2 * NG), slice(c, c + imax + 2 * NG))
+    ks, js, is_ = kmax + 2 * NG, jmax + 2 * NG, imax + 2 * NG
+    sl = (slice(c, c + ks), slice(c, c + js), slice(c, c + is_))
     out = {}
-    for name, S in (("A1", S1), ("A2", S2), ("A3", S3)):
-        S = S[sl]
-        mag = np.sqrt(np.sum(S * S, -1))
-        safe = np.where(mag > 0, mag, 1.0)
-        out[name] = mag
-        out[name + "XA"] = S[..., 0] / safe
-        out[name + "YA"] = S[..., 1] / safe
-        out[name + "ZA"] = S[..., 2] / safe
-    v = vol[sl]
+    v = r["VOL"][sl]
     out["VOL"] = v
-    cc = cen[sl]
+    cc = r["C"][sl]
     out["XC"], out["YC"], out["ZC"] = cc[..., 0], cc[..., 1], cc[..., 2]
     eps = 1e-20
-    for d, Sh in (("1", S1h), ("2", S2h), ("3", S3h)):
-        ah = np.sqrt(np.sum(Sh[sl] ** 2, -1))
-        out["D" + d] = np.minimum(1e4, (v + eps) / (out["A" + d] + ah + eps) * 2.0)
+    for d in range(3):
+        A, N = r[f"A{d + 1}"], r[f"N{d + 1}"]
+        name = f"A{d + 1}"
+        out[name] = A[sl]
+        out[name + "XA"] = N[sl][..., 0]
+        out[name + "YA"] = N[sl][..., 1]
+        out[name + "ZA"] = N[sl][..., 2]
+        hs = list(sl)
+        hs[2 - d] = slice(sl[2 - d].start + 1, sl[2 - d].stop + 1)
+        out[f"D{d + 1}"] = np.minimum(1e4, (v + eps) / (A[sl] + A[tuple(hs)] + eps) * 2.0)
     m = Metrics(imax, jmax, kmax)
     for k2 in METRIC_NAMES:
         m.arrays[k2] = np.ascontiguousarray(out[k2], dtype=np.float64).reshape(-1)
@@ -226,39 +284,67 @@ def _finish(S1, S2, S3, S1h, S2h, S3h, vol, cen, dims, ng):
 
 
 def _lump(r):
-    """One coarsening step (GRID1B/LUMPA1 gluebm.f:1492-1496): coarse volumes
-    are sums of the 8 children, coarse face vectors sums of the 4 child
-    faces, centres volume-weighted; ng halves."""
+    """One coarsening step: LUMPA1 gluebm.f:2194 for the faces (area = sum
+    of the four child areas + 1e-20, normal = the area-weighted sum of the
+    child normals, normalised; (1, ., .) where that sum vanishes) and LUMPVS
+    gluebm.f:2256 for volumes and volume-weighted centres, children in the
+    reference's order (i, j, k), (i, j+1, k), (i, j, k+1), (i, j+1, k+1),
+    then the same at i+1; ghost layers halve."""
     ng = r["ng"]
     imax, jmax, kmax = r["dims"]
     assert ng % 2 == 0 and imax % 2 == 0 and jmax % 2 == 0 and kmax % 2 == 0
     vol, cen = r["VOL"], r["C"]
+    ck, cj, ci = (n // 2 for n in vol.shape)
 
-    def csum(a):  # sum over 2x2x2 children (k, j, i axes)
-        return (a[0::2, 0::2, 0::2] + a[0::2, 0::2, 1::2] + a[0::2, 1::2, 0::2] + a[0::2, 1::2, 1::2]
-                + a[1::2, 0::2, 0::2] + a[1::2, 0::2, 1::2] + a[1::2, 1::2, 0::2] + a[1::2, 1::2, 1::2])
-    vc = csum(vol)
-    cc = csum(cen * vol[..., None]) / vc[..., None]
-    S1 = r["S1"][0::2, 0::2, 0::2] + r["S1"][0::2, 1::2, 0::2] + r["S1"][1::2, 0::2, 0::2] + r["S1"][1::2, 1::2, 0::2]
-    S2 = r["S2"][0::2, 0::2, 0::2] + r["S2"][0::2, 0::2, 1::2] + r["S2"][1::2, 0::2, 0::2] + r["S2"][1::2, 0::2, 1::2]
-    S3 = r["S3"][0::2, 0::2, 0::2] + r["S3"][0::2, 0::2, 1::2] + r["S3"][0::2, 1::2, 0::2] + r["S3"][0::2, 1::2, 1::2]
-    S1h = r["S1h"][0::2, 0::2, 1::2] + r["S1h"][0::2, 1::2, 1::2] + r["S1h"][1::2, 0::2, 1::2] + r["S1h"][1::2, 1::2, 1::2]
-    S2h = r["S2h"][0::2, 1::2, 0::2] + r["S2h"][0::2, 1::2, 1::2] + r["S2h"][1::2, 1::2, 0::2] + r["S2h"][1::2, 1::2, 1::2]
-    S3h = r["S3h"][1::2, 0::2, 0::2] + r["S3h"][1::2, 0::2, 1::2] + r["S3h"][1::2, 1::2, 0::2] + r["S3h"][1::2, 1::2, 1::2]
-    return dict(S1=S1, S2=S2, S3=S3, S1h=S1h, S2h=S2h, S3h=S3h, VOL=vc, C=cc,
-                dims=(imax // 2, jmax // 2, kmax // 2), ng=ng // 2)
+    def child(a, di, dj, dk):
+        return a[dk::2, dj::2, di::2][:ck, :cj, :ci]
+
+    order = [(0, 0, 0), (0, 1, 0), (0, 0, 1), (0, 1, 1), (1, 0, 0), (1, 1, 0), (1, 0, 1), (1, 1, 1)]
+    vs = [child(vol, *o) for o in order]
+    vl = vs[0]
+    for q in range(1, 8):
+        vl = vl + vs[q]
+    cs = [child(cen, *o) for o in order]
+    s = vs[0][..., None] * cs[0]
+    for q in range(1, 8):
+        s = s + vs[q][..., None] * cs[q]
+    out = dict(dims=(imax // 2, jmax // 2, kmax // 2), ng=ng // 2, VOL=vl, C=s / vl[..., None])
+    for d in range(3):
+        A, N = r[f"A{d + 1}"], r[f"N{d + 1}"]
+        nf = [ci, cj, ck]
+        nf[d] += 1
+        bd, cd = (d + 1) % 3, (d + 2) % 3           # LUMPA1's J and K directions of the pass
+        kids = []
+        for q in range(4):
+            o = [0, 0, 0]
+            if q & 1:
+                o[bd] = 1
+            if q & 2:
+                o[cd] = 1
+            sl = tuple(slice(o[ax], o[ax] + 2 * nf[ax], 2) for ax in (2, 1, 0))
+            kids.append((A[sl], N[sl]))
+        vec = kids[0][0][..., None] * kids[0][1]
+        for q in range(1, 4):
+            vec = vec + kids[q][0][..., None] * kids[q][1]
+        al = kids[0][0] + kids[1][0] + kids[2][0] + kids[3][0] + 1.0e-20
+        axyzl = np.sqrt(vec[..., 0] * vec[..., 0] + vec[..., 1] * vec[..., 1] + vec[..., 2] * vec[..., 2])
+        n = vec / (axyzl + 1.0e-20)[..., None]
+        z = axyzl < 1.0e-20
+        n[..., 0] = np.where(z, 1.0, n[..., 0])
+        out[f"A{d + 1}"], out[f"N{d + 1}"] = al, n
+    return out
 
 
 def mg_metrics(X, Y, Z, nlev: int):
     """Metrics of every multigrid level (level 1 first), coarse levels
-    lumped from the fine cells so that the 8 children of a coarse cell fill
-    it exactly (volumes and face vectors add up)."""
+    lumped from the fine cells (LUMPA1 / LUMPVS); the ghost layers of a
+    coarse level are lumped from the fine level's, which carries
+    2 * 2^(nlev-1) of them."""
     ng = NG * 2 ** (nlev - 1)
     r = compute_metrics(X, Y, Z, ng=ng, raw=True)
     levels = []
     for lev in range(nlev):
-        levels.append(_finish(r["S1"], r["S2"], r["S3"], r["S1h"], r["S2h"], r["S3h"], r["VOL"], r["C"],
-                              r["dims"], r["ng"]))
+        levels.append(_finish(r))
         if lev + 1 < nlev:
             r = _lump(r)
     return levels

@@ -615,10 +615,11 @@ def run_config(ntrain=64, ntest=16, cycles=2000, steps=6000, batch=16, lr=1e-3, 
     runs = [solve(pv, cycles, spec=spec) for pv in Ptr]
     t_data = time.perf_counter() - t0
     log(f"training data: {ntrain} solves x {cycles} cycles in {t_data:.1f} s")
-    # a training field is a solution only where its solve converged: keep
-    # the runs whose density residual fell by 4 decades (sum of squares) and
-    # whose fields are finite, drop (and report) the others
-    keep = [bool(np.isfinite(r.q).all() and np.isfinite(r.hist[-1]) and r.hist[-1] <= 1e-4 * r.hist[0])
+    # a diverged solve is no training field: keep the runs whose fields are
+    # finite and whose density residual ends within 100x of its least value
+    # (a solve that blew up after converging part-way ends far above it),
+    # drop (and report) the others
+    keep = [bool(np.isfinite(r.q).all() and np.isfinite(r.hist).all() and r.hist[-1] <= 100.0 * np.min(r.hist))
             for r in runs]
     dropped = [[float(x) for x in pv] for pv, k in zip(Ptr, keep) if not k]
     if dropped:

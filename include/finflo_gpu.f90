@@ -22,7 +22,7 @@ module finflo_gpu
   use, intrinsic :: iso_c_binding
   implicit none
 
-  integer(c_int), parameter :: FF_ABI_VERSION = 4
+  integer(c_int), parameter :: FF_ABI_VERSION = 5
   integer(c_int), parameter :: FF_OK = 0, FF_ERR_CUDA = 1, FF_ERR_ARG = 2, &
                                FF_ERR_TIMEOUT = 3, FF_ERR_SIZE = 4
   integer(c_int), parameter :: FF_BC_CON = 1, FF_BC_INL = 3, FF_BC_MIR = 4, &

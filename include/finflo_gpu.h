@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define FF_ABI_VERSION 4   /* 4: ff_params gains predgs_full (3: ddadi, timel, dt; slots FF_ROLE2..FF_EPSLE3) */
+#define FF_ABI_VERSION 5   /* 5: ff_wall_distance takes wall points (4: ff_params gains predgs_full) */
 
 enum { FF_OK = 0, FF_ERR_CUDA = 1, FF_ERR_ARG = 2, FF_ERR_TIMEOUT = 3, FF_ERR_SIZE = 4 };
 enum { FF_STAGE_RESIDUAL = 1, FF_STAGE_GRAD = 2, FF_STAGE_STATE = 3, FF_STAGE_SWEEP = 4 };
@@ -117,18 +117,23 @@ int ff_time_levels(void *ctx, int blk, int mode);
  * wall distance in DISTANCES gluebm.f:9136 on the host).
  * ff_block_metrics: xyz = the block's nodes, X then Y then Z, each
  * (KMAX+1)(JMAX+1)(IMAX+1) values with i fastest; fills A1..A3ZA, VOL,
- * XC..ZC and D1..D3 of every cell, ghosts included (ghost nodes by mirror
- * extrapolation).  ff_wall_distance: tri = ntri wall triangles of 9 values
- * (three corners); fills DISTW of every cell with the exact distance of its
- * centre (XC, YC, ZC as on the device) to the nearest triangle, 1e3 when
- * ntri = 0.  Both synchronous. */
+ * XC..ZC and D1..D3 of every cell, ghosts included: GRID1B's construction
+ * (gluebm.f:1265; GRIDEX ghost nodes 1029, AREVC1 1586, D1D2D3 2326), the
+ * further ghost layers from continued mirror reflection of the nodes.
+ * ff_wall_distance: pts = npts wall points of 3 values (PICK_XYZ
+ * gluebm.f:9452: halfway between the first interior and ghost cell centres
+ * of the solid patches, of every block); fills DISTW of every cell of the
+ * block with the distance of its centre to the nearest point (WALL_DIST
+ * 9533; 1e4 when npts = 0), and of its linked coarse levels the same, their
+ * interior cells then the mean of their eight children (LUMP_DIST 9562).
+ * Both synchronous. */
 int ff_block_metrics(void *ctx, int blk, const double *xyz);
 /* The same for a block and its nlev - 1 linked coarse levels (ff_mg_link):
  * the fine cells with 2 * 2^(nlev-1) ghost layers, each coarse level lumped
- * from the finer one (volumes and face vectors summed over the children,
- * centres volume-weighted). */
+ * from the finer one (LUMPA1 gluebm.f:2194 for the faces, LUMPVS 2256 for
+ * volumes and centres). */
 int ff_block_metrics_levels(void *ctx, int blk, int nlev, const double *xyz);
-int ff_wall_distance(void *ctx, int blk, const double *tri, int ntri);
+int ff_wall_distance(void *ctx, int blk, const double *pts, int npts);
 
 /* With ff_params.iturb = 6 (k-omega SST) ff_residu is
  * TURBEQ res3c.f:5845 + RESIKE res3c.f:3423, ff_imps the seven-equation

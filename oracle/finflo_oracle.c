@@ -1852,3 +1852,4 @@ void orc_halo_unpack(orc_block *dst, const ff_patch *pa, const double *in) {
 
 #include "finflo_oracle_sst.c"
 #include "finflo_oracle_ddadi.c"
+#include "finflo_oracle_grid.c"

@@ -83,6 +83,12 @@ void orc_roe_face(const double *qr, const double *ql, const double *qrr, const d
                   const double *nrm, double area, int intem, const ff_params *p,
                   const double *cell_r, const double *cell_l, int kquirk, double *f5);
 
+/* the reference's block set-up (finflo_oracle_grid.c) */
+void orc_grid_metrics(orc_block *b, const double *X, const double *Y, const double *Z);
+void orc_grid_lump(const orc_block *f, orc_block *c);
+int orc_wall_points(orc_block **blk, int nblk, double *xyz);
+void orc_wall_distance(orc_block *b, const double *xyz, int np);
+
 #ifdef __cplusplus
 }
 #endif

@@ -109,23 +109,3 @@ def test_multiblock_multigrid_converges():
     h = [om.cycle(i + 1)[0][0] for i in range(30)]
     assert np.all(np.isfinite(h))
     assert min(h[-5:]) < 0.3 * h[0]
-
-
-def test_wall_triangles_and_host_wall_distance():
-    """The walls of the SST bump channel (lower and upper) as triangles (two
-    per wall face), and the
-    host DISTW (nearest-candidate search) against the exact distance to
-    every triangle: never below it, and equal to 1e-9 of the cell size."""
-    import numpy as np
-    from finflo_b200 import case
-    blk, prm, fs = case.bump_case(9, 7, 5, turbulence="sst", reynolds=1e6, mach=0.6, h1=1e-3)
-    T = case.wall_triangles(blk)
-    assert T.shape == (2 * 2 * 8 * 4, 9)
-    q = np.stack([blk.arrays["XC"], blk.arrays["YC"], blk.arrays["ZC"]], axis=1)
-    exact = np.full(len(q), np.inf)
-    for t in T:
-        a, b, c = (np.broadcast_to(t[3 * m:3 * m + 3], q.shape) for m in range(3))
-        np.minimum(exact, case._closest_on_triangles(q, a, b, c), out=exact)
-    host = blk.arrays["DISTW"]
-    assert (host >= exact * (1 - 1e-12)).all()
-    assert np.abs(host - exact).max() <= 1e-9 * max(1.0, np.abs(exact).max())

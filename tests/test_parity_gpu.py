@@ -9,7 +9,7 @@ import pytest
 
 from finflo_b200.gpu import GpuSolver
 from oracle.oracle import Oracle
-from tests.util import flux_scale, interior, make_pair
+from tests.util import hist_close, flux_scale, interior, make_pair
 
 pytestmark = pytest.mark.gpu
 
@@ -133,7 +133,7 @@ def test_cycles_predgs_full_match_oracle(gpu_lib):
     n = 30
     hist = g.cycles(n, bid, icycle0=1, use_graph=True)
     ref = np.array([o.cycle(i + 1)[0] for i in range(n)])
-    np.testing.assert_allclose(hist[:, :5], ref, rtol=1e-8)
+    hist_close(hist[:, :5], ref, 1e-8)
     g.close()
 
 
@@ -160,7 +160,7 @@ def test_cycles_match_oracle(gpu_lib, use_graph):
     n = 30
     hist = g.cycles(n, bid, icycle0=1, use_graph=use_graph)
     ref = np.array([o.cycle(i + 1)[0] for i in range(n)])
-    np.testing.assert_allclose(hist[:, :5], ref, rtol=1e-8)
+    hist_close(hist[:, :5], ref, 1e-8)
     d = g.download(bid, ["TEMP", "U", "V", "W", "PDIFF"])
     for nme in d:
         a = interior(bg, d[nme]); b = interior(bc, bc.arrays[nme])
@@ -255,7 +255,7 @@ def test_pipe_cycles_match_oracle(gpu_lib, monkeypatch):
     n = 20
     hist = g.cycles(n, bid, icycle0=1, use_graph=True)
     ref = np.array([o.cycle(i + 1)[0] for i in range(n)])
-    np.testing.assert_allclose(hist[:, :5], ref, rtol=1e-9)
+    hist_close(hist[:, :5], ref, 1e-9)
     g.close()
 
 
@@ -277,7 +277,7 @@ def test_multigrid_cycles_match_oracle(gpu_lib, nlev, dims):
     n = 12
     hist = g.cycles(n, bid, icycle0=1, use_graph=True)
     ref = np.array([om.cycle(i + 1)[0] for i in range(n)])
-    np.testing.assert_allclose(hist[:, :5], ref, rtol=1e-7)
+    hist_close(hist[:, :5], ref, 1e-7)
     d = g.download(bid, ["TEMP", "U", "V", "PDIFF"])
     for nme in d:
         a = interior(lv_g[0], d[nme]); b = interior(lv_c[0], lv_c[0].arrays[nme])
@@ -312,7 +312,7 @@ def test_multiblock_cycles_match_oracle(gpu_lib, kind, monkeypatch):
     n = 15
     hist = g.cycles_all(n, icycle0=1, use_graph=True)
     ref = np.array([om.cycle(i + 1)[0] for i in range(n)])
-    np.testing.assert_allclose(hist[:, :5], ref, rtol=1e-9)
+    hist_close(hist[:, :5], ref, 1e-9)
     for bid in range(len(bg)):
         d = g.download(bid, ["TEMP", "U", "V", "W", "PDIFF"])
         for nme in d:
@@ -352,7 +352,7 @@ def test_multiblock_multigrid_matches_oracle(gpu_lib, turb, mode, monkeypatch):
     n = 10
     hist = g.cycles_all(n, icycle0=1, use_graph=True)
     ref = np.array([om.cycle(i + 1)[0] for i in range(n)])
-    np.testing.assert_allclose(hist[:, :5], ref, rtol=1e-8 if turb else 1e-9)
+    hist_close(hist[:, :5], ref, 1e-8 if turb else 1e-9)
     names = ["TEMP", "U", "V", "W", "PDIFF"] + (["RK", "REPS"] if turb else [])
     for k, bid in enumerate(ids):
         d = g.download(bid, names)
@@ -406,7 +406,7 @@ def test_halo_loopback_matches_oracle(gpu_lib):
         g.mb_phase(fd.PHASE_RECORD, i + 1, True)
     hist = g.history(n)
     ref = np.array([om.cycle(i + 1)[0] for i in range(n)])
-    np.testing.assert_allclose(hist[:, :5], ref, rtol=1e-9)
+    hist_close(hist[:, :5], ref, 1e-9)
     for bid in range(len(bg)):
         d = g.download(bid, ["TEMP", "U", "V", "W", "PDIFF"])
         for nme in d:

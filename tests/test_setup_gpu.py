@@ -1,5 +1,9 @@
-"""Block set-up on the device (ff_block_metrics, ff_wall_distance) against
-the host construction in finflo_b200/grid.py and case.py."""
+"""Block set-up on the device (ff_block_metrics, ff_block_metrics_levels,
+ff_wall_distance): the reference's construction (GRIDEX, AREVC1, D1D2D3,
+LUMPA1, LUMPVS, PICK_XYZ, WALL_DIST, LUMP_DIST), written with
+non-contracted arithmetic, equals the host set-up (finflo_b200/grid.py,
+case.py) to the bit -- and through it the oracle's restatement
+(tests/test_grid_setup_cpu.py)."""
 import numpy as np
 import pytest
 
@@ -20,8 +24,8 @@ def _warped_block():
 
 
 @pytest.mark.parametrize("kind", ["bump", "warped"])
-def test_device_metrics_match_host(gpu_lib, kind):
-    blk = case.bump_case(33, 17, 17)[0] if kind == "bump" else _warped_block()
+def test_device_metrics_equal_host(gpu_lib, kind):
+    blk = case.bump_case(33, 17, 17, span_amp=0.5, zlen=1.0)[0] if kind == "bump" else _warped_block()
     prm = case.make_params(case.FlowConditions(), blk.dims)
     ref = {n: blk.arrays[n].copy() for n in grid.METRIC_NAMES}
     for n in grid.METRIC_NAMES:
@@ -32,19 +36,13 @@ def test_device_metrics_match_host(gpu_lib, kind):
     g.block_metrics(bid, *blk.nodes)
     d = g.download(bid, list(grid.METRIC_NAMES))
     for n in grid.METRIC_NAMES:
-        # unit-normal components on the scale of 1 (a component that is zero
-        # on the host, e.g. the z part of a j face of an extruded grid, comes
-        # out at rounding level with fused multiply-adds); the rest relative
-        # to the array's largest magnitude
-        scale = 1.0 if n.endswith(("XA", "YA", "ZA")) else np.abs(ref[n]).max()
-        err = np.abs(d[n] - ref[n]).max() / scale
-        assert err <= 1e-12, (n, err)
+        np.testing.assert_array_equal(d[n], ref[n], err_msg=n)
     g.close()
 
 
-def test_device_multigrid_metrics_match_host(gpu_lib):
+def test_device_multigrid_metrics_equal_host(gpu_lib):
     """Three levels: the fine cells with 8 ghost layers, lumped twice."""
-    levels, prms, fs = case.bump_case_mg(33, 17, 17, nlev=3)
+    levels, prms, fs = case.bump_case_mg(33, 17, 17, nlev=3, span_amp=0.5, zlen=1.0)
     ref = [{n: lv.arrays[n].copy() for n in grid.METRIC_NAMES} for lv in levels]
     for lv in levels:
         for n in grid.METRIC_NAMES:
@@ -57,17 +55,33 @@ def test_device_multigrid_metrics_match_host(gpu_lib):
     for q in range(len(levels)):
         d = g.download(bid + q, list(grid.METRIC_NAMES))
         for n in grid.METRIC_NAMES:
-            scale = 1.0 if n.endswith(("XA", "YA", "ZA")) else np.abs(ref[q][n]).max()
-            err = np.abs(d[n] - ref[q][n]).max() / scale
-            assert err <= 1e-12, (q, n, err)
+            np.testing.assert_array_equal(d[n], ref[q][n], err_msg=f"level {q + 1} {n}")
+    g.close()
+
+
+def test_device_wall_distance_equals_host(gpu_lib):
+    """DISTW of all three levels (every cell of each, the coarse interior
+    cells lumped) from the block's own wall points."""
+    levels, prms, fs = case.bump_case_mg(33, 17, 17, nlev=3, turbulence="sst", reynolds=1e6, mach=0.6, h1=1e-4)
+    ref = [lv.arrays["DISTW"].copy() for lv in levels]
+    pts = case.wall_points(levels[0].nodes, levels[0].patches)
+    assert len(pts) > 0
+    g = GpuSolver(0)
+    bid = g.add_levels(levels, prms)
+    for q, lv in enumerate(levels):
+        lv.arrays["DISTW"][:] = 0.0
+        g.upload(bid + q)
+    g.wall_distance(bid, pts)
+    for q in range(len(levels)):
+        d = g.download(bid + q, ["DISTW"])["DISTW"]
+        np.testing.assert_array_equal(d, ref[q], err_msg=f"level {q + 1}")
     g.close()
 
 
 def test_device_setup_runs_like_host_setup(gpu_lib):
     """The eight-block SST bump with two levels per block, set up on the
-    host and on the device: the same residual history over 10 multi-block
-    V-cycles (the two set-ups differ at rounding level in the metrics and by
-    the host search's 1e-11 in DISTW)."""
+    host and on the device: identical set-up, identical residual history
+    over 10 multi-block V-cycles."""
     kw = dict(cells=(40, 16, 16), nb=(2, 2, 2), nlev=2, reynolds=1e6, mach=0.6, h1=1e-4, cfl=1.0, cfll=1.0,
               lusgs_fp32=False, coarse_fp32=False, turbulence="sst")
     hists = []
@@ -81,36 +95,8 @@ def test_device_setup_runs_like_host_setup(gpu_lib):
         if dev:
             for k, bid in enumerate(ids):
                 g.block_metrics_levels(bid, 2, *bl[k][0].nodes)
-                for q in range(2):
-                    g.wall_distance(bid + q, out[3])
+                g.wall_distance(bid, out[3])
         g.start_all()
         hists.append(g.cycles_all(10, icycle0=1, use_graph=True)[:, :5])
         g.close()
-    np.testing.assert_allclose(hists[1], hists[0], rtol=1e-6)
-
-
-def _brute_force_distance(q, T):
-    best = np.full(len(q), np.inf)
-    for t in T:
-        a, b, c = (np.broadcast_to(t[3 * m:3 * m + 3], q.shape) for m in range(3))
-        np.minimum(best, case._closest_on_triangles(q, a, b, c), out=best)
-    return best
-
-
-def test_device_wall_distance(gpu_lib):
-    """Exact distance to every wall triangle: against a host brute force, and
-    never above the host's nearest-candidate search."""
-    blk, prm, fs = case.bump_case(17, 9, 9, turbulence="sst", reynolds=1e6, mach=0.6, h1=1e-4)
-    T = case.wall_triangles(blk)
-    assert len(T) > 0
-    q = np.stack([blk.arrays["XC"], blk.arrays["YC"], blk.arrays["ZC"]], axis=1)
-    exact = _brute_force_distance(q, T)
-    host = blk.arrays["DISTW"].copy()
-    g = GpuSolver(0)
-    bid = g.add_block(blk, prm)
-    g.upload(bid)
-    g.wall_distance(bid, T)
-    d = g.download(bid, ["DISTW"])["DISTW"]
-    np.testing.assert_allclose(d, exact, rtol=1e-12, atol=1e-15)
-    assert (d <= host * (1 + 1e-12) + 1e-15).all()
-    g.close()
+    np.testing.assert_allclose(hists[1], hists[0], rtol=1e-12)

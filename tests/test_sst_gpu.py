@@ -4,7 +4,7 @@ import pytest
 
 from finflo_b200.gpu import GpuSolver
 from oracle.oracle import Oracle
-from tests.util import flux_scale_sst, interior, make_pair
+from tests.util import hist_close, flux_scale_sst, interior, make_pair
 
 pytestmark = pytest.mark.gpu
 
@@ -85,7 +85,7 @@ def test_sst_cycles_match_oracle(gpu_lib, use_graph):
     n = 40
     hist = g.cycles(n, bid, icycle0=1, use_graph=use_graph)
     ref = _run_oracle_cycles(o, n)
-    np.testing.assert_allclose(hist[:, :5], ref, rtol=1e-8)
+    hist_close(hist[:, :5], ref, 1e-8)
     d = g.download(bid, ["TEMP", "U", "V", "W", "RK", "REPS", "VIST"])
     for nme in d:
         a = interior(bg, d[nme]); b = interior(bc, bc.arrays[nme])
@@ -187,7 +187,7 @@ def test_sst_multigrid_cycles_match_oracle(gpu_lib, nlev, dims):
     n = 12
     hist = g.cycles(n, bid, icycle0=1, use_graph=True)
     ref = np.array([om.cycle(i + 1)[0] for i in range(n)])
-    np.testing.assert_allclose(hist[:, :5], ref, rtol=1e-7)
+    hist_close(hist[:, :5], ref, 1e-7)
     d = g.download(bid, ["TEMP", "U", "V", "RK", "REPS"])
     for nme in d:
         a = interior(lv_g[0], d[nme]); b = interior(lv_c[0], lv_c[0].arrays[nme])
