@@ -460,13 +460,15 @@ LARGE_NAME = ("3-D bump channel, spanwise amplitude 0.1(1+0.5 sin 2 pi z) on z i
 LARGE_STATE = ["TEMP", "U", "V", "W", "PDIFF", "RK", "REPS"]
 
 
-def _large_blocks(cells, nlev=3, fp32=False, ddadi=False, device_setup=True):
-    """The large case's block generator (fs, wall triangles, then (levels,
+def _large_blocks(cells, nlev=3, fp32=False, ddadi=False, device_setup=True, coarse_res_fp32=False):
+    """The large case's block generator (fs, wall points, then (levels,
     prms) per block) with the settings every arm uses: INTER=1 and the full
-    lower sweep (the converging choices), FP64 or FP32 implicit stage."""
+    lower sweep (the converging choices), FP64 or FP32 implicit stage, and
+    optionally the coarse levels' face fluxes in FP32."""
     from finflo_b200 import case
     it = case.bump_multiblock_blocks(cells=cells, nb=(2, 2, 2), nlev=nlev, seed=5, inter=1, lusgs_fp32=fp32,
-                                     coarse_fp32=fp32, device_setup=device_setup)
+                                     coarse_fp32=fp32 or coarse_res_fp32, coarse_res_fp32=coarse_res_fp32,
+                                     device_setup=device_setup)
     for item in it:
         if isinstance(item, tuple) and len(item) == 2 and isinstance(item[0], list):
             for q in item[1]:
@@ -543,7 +545,8 @@ def run_large(args):
     t0 = time.perf_counter()
     g = GpuSolver(local)
     dev = not args.host_setup   # metrics and wall distance on the device (ff_block_metrics_levels)
-    it = _large_blocks(cells, nlev, fp32=fp32, ddadi=args.ddadi, device_setup=dev)
+    it = _large_blocks(cells, nlev, fp32=fp32, ddadi=args.ddadi, device_setup=dev,
+                       coarse_res_fp32=args.coarse_fp32)
     _, fs = next(it)
     walls = next(it)[1] if dev else None
     fine_cells, fine_ntot = [], []
@@ -620,10 +623,12 @@ def run_large(args):
     line = {
         "metric": "cell-iters/s", "value": value, "unit": "cell-iters/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64 residual / " + ("f32" if fp32 else "f64") + " LU-SGS",
+        "vs_baseline": None, "dtype": "f64 residual / " + ("f32" if fp32 else "f64") + " LU-SGS"
+        + (" (coarse levels: f32 face fluxes and LU-SGS)" if args.coarse_fp32 and not fp32 else ""),
         "data": "synthetic (seeded block cuts and free-stream noise)",
         "config": {"workload": LARGE_NAME.format(cells="x".join(map(str, cells)), prec="FP32" if fp32 else "FP64")
-                   + (", DDADI implicit stage (LUSGS=0)" if args.ddadi else ""),
+                   + (", DDADI implicit stage (LUSGS=0)" if args.ddadi else "")
+                   + (", coarse levels' face fluxes and LU-SGS in FP32" if args.coarse_fp32 and not fp32 else ""),
                    "cells": total, "blocks": nblk, "levels": nlev, "setup_s": setup_s,
                    "setup": "metrics and wall distance on the host" if args.host_setup else
                             "metrics and wall distance on the device",
@@ -782,6 +787,8 @@ def main():
     ap.add_argument("--large-fp32", action="store_true",
                     help="large case: FP32 implicit stage on every level (default: plain FP64)")
     ap.add_argument("--host-setup", action="store_true", help="large case: metrics and wall distance on the host")
+    ap.add_argument("--coarse-fp32", action="store_true",
+                    help="large case: the coarse levels' face fluxes and implicit stage in FP32 (fine level FP64)")
     ap.add_argument("--ddadi", action="store_true", help="DDADI implicit stage (LUSGS=0) instead of LU-SGS")
     ap.add_argument("--timel", type=float, default=0.0,
                     help="physical time step DT of a time-accurate (TIMEL) run; 0 = steady")

@@ -42,7 +42,7 @@ class FFParams(ctypes.Structure):
         (n, ctypes.c_int) for n in (
             "interi", "interj", "interk", "entropy_fix", "iturb", "fullns",
             "idi1", "idi2", "idi3", "coarse_inter", "lusgs_fp32", "ddadi", "timel", "vanleer")] + [
-        ("dt", ctypes.c_double), ("predgs_full", ctypes.c_int), ("pad_", ctypes.c_int)]
+        ("dt", ctypes.c_double), ("predgs_full", ctypes.c_int), ("res_fp32", ctypes.c_int)]
 
 
 class FFHaloItem(ctypes.Structure):
@@ -440,12 +440,14 @@ def setup_sst(blk: Block, prm: FFParams, fs, tu=1.0e-3, mut_ratio=0.1, walls=Non
 
 def bump_case_mg(ni=65, nj=33, nk=33, nlev=3, *, h1=1e-3, amp=0.1, mach=0.5, reynolds=1e4,
                  zlen=0.5, noise=1e-3, seed=0, cfl=2.0, cfll=2.0, inter=3, span_amp=0.0,
-                 lusgs_fp32=False, coarse_fp32=False, turbulence=None, tu=1.0e-3, mut_ratio=0.1):
+                 lusgs_fp32=False, coarse_fp32=False, coarse_res_fp32=False, turbulence=None, tu=1.0e-3,
+                 mut_ratio=0.1):
     """The bump channel with nlev multigrid levels (finest first); coarse
     metrics are lumped from the fine cells, patch ranges follow each level.
     lusgs_fp32 runs the fine level's implicit operator in FP32, coarse_fp32
     the coarse levels' (their correction reaches the fine level through
-    INTERP; residuals and updates stay FP64)."""
+    INTERP), coarse_res_fp32 the coarse levels' face fluxes; the fine
+    level's residual, every update and the norms stay FP64."""
     fc = FlowConditions(mach=mach, reynolds=reynolds)
     fs = fc.freestream()
     X, Y, Z = grid.bump_nodes(ni, nj, nk, h1=h1, amp=amp, zlen=zlen, span_amp=span_amp)
@@ -464,6 +466,7 @@ def bump_case_mg(ni=65, nj=33, nk=33, nlev=3, *, h1=1e-3, amp=0.1, mach=0.5, rey
     prms[0].lusgs_fp32 = int(lusgs_fp32)
     for q in prms[1:]:
         q.lusgs_fp32 = int(coarse_fp32)
+        q.res_fp32 = int(coarse_res_fp32)
     return levels, prms, fs
 
 
@@ -589,7 +592,7 @@ def channel_wall_points(X, Y, Z):
 def bump_multiblock_blocks(cells=(512, 256, 128), nb=(2, 2, 2), nlev=3, *, seed=5, h1=2e-6, amp=0.1,
                            span_amp=0.5, zlen=1.0, mach=0.7, reynolds=5e6, noise=1e-3, cfl=1.0, cfll=1.0,
                            inter=3, turbulence="sst", tu=1.0e-3, mut_ratio=0.1, lusgs_fp32=True,
-                           coarse_fp32=True, device_setup=False):
+                           coarse_fp32=True, coarse_res_fp32=False, device_setup=False):
     """The bump channel split into nb[0] x nb[1] x nb[2] blocks of uneven
     sizes (cut positions from the seed), 1:1 patched on every interior cut,
     periodic in z through 1:1 patches (the spanwise amplitude
@@ -664,6 +667,7 @@ def bump_multiblock_blocks(cells=(512, 256, 128), nb=(2, 2, 2), nlev=3, *, seed=
         prms[0].lusgs_fp32 = int(lusgs_fp32)
         for q in prms[1:]:
             q.lusgs_fp32 = int(coarse_fp32)
+            q.res_fp32 = int(coarse_res_fp32)
         yield levels, prms
 
 

@@ -28,6 +28,7 @@ template <typename T> FF_DI T dmax(T a, T b) { return a > b ? a : b; }
 // 1/x correctly rounded (the same value as 1. / x), through the reciprocal
 // intrinsic rather than the general division
 FF_DI double rcp(double x) { return __drcp_rn(x); }
+FF_DI float rcp(float x) { return __frcp_rn(x); }
 template <typename T> FF_DI T dmin(T a, T b) { return a < b ? a : b; }
 
 // SURFVECTS base3c.f:12245: two tangent unit vectors completing the normal.
@@ -49,25 +50,27 @@ FF_DI void surfvects(T a11, T a12, T a13, T& a21, T& a22, T& a23, T& a31, T& a32
 }
 
 // XXTRAP base3c.f:750 (kappa scheme, van Albada limiter); r0..r3 are the
-// cells I-2S, I-S, I, I+S of the face between I-S and I.
-FF_DI void xxtrap(double r0, double r1, double r2, double r3, int intem, double& rip, double& rim) {
+// cells I-2S, I-S, I, I+S of the face between I-S and I.  T = double, or
+// float for a coarse level's face pass in FP32.
+template <typename T>
+FF_DI void xxtrap(T r0, T r1, T r2, T r3, int intem, T& rip, T& rim) {
   int inter = intem < 0 ? -intem : intem;
   int inte2 = inter < 1 ? 1 : (inter > 5 ? 5 : inter);
-  double rk1 = inte2 == 1 ? 0. : (inte2 == 2 ? 1. : (inte2 == 3 ? 1.3333333 : (inte2 == 4 ? 2. : 1.5)));
-  double rk2 = 2. - rk1;
-  double R1 = .25 * rk1, R2 = .25 * rk2;
-  double diff0 = r1 - r0, diff1 = r2 - r1, diff2 = r3 - r2;
+  T rk1 = inte2 == 1 ? T(0.) : (inte2 == 2 ? T(1.) : (inte2 == 3 ? T(1.3333333) : (inte2 == 4 ? T(2.) : T(1.5))));
+  T rk2 = T(2.) - rk1;
+  T R1 = T(.25) * rk1, R2 = T(.25) * rk2;
+  T diff0 = r1 - r0, diff1 = r2 - r1, diff2 = r3 - r2;
   if (intem <= 0 && intem >= -5) {
     rip = r2 - (diff1 * R1 + diff2 * R2);
     rim = r1 + (diff1 * R1 + diff0 * R2);
   } else if (inter <= 4) {
     // the two van Albada ratios through one reciprocal of the product of
     // their denominators (each at least 1e-10, far from over- or underflow)
-    double diff12 = diff1 * diff1 + 1.e-10;
-    double db = diff12 + diff0 * diff0, df = diff12 + diff2 * diff2;
-    double r = rcp(db * df);
-    double phibi = (diff12 + diff1 * diff0) * (df * r);
-    double phifi = (diff12 + diff1 * diff2) * (db * r);
+    T diff12 = diff1 * diff1 + T(1.e-10);
+    T db = diff12 + diff0 * diff0, df = diff12 + diff2 * diff2;
+    T r = rcp(db * df);
+    T phibi = (diff12 + diff1 * diff0) * (df * r);
+    T phifi = (diff12 + diff1 * diff2) * (db * r);
     rip = r2 - phifi * (diff1 * R1 + diff2 * R2);
     rim = r1 + phibi * (diff1 * R1 + diff0 * R2);
   } else {
@@ -80,92 +83,92 @@ FF_DI void xxtrap(double r0, double r1, double r2, double r3, int intem, double&
 // at one face; laminar (k = omega = 0), UROT = 0.  q[v][m]: v = ro,u,v,w,p,
 // m = cells I-2S, I-S, I, I+S.  cr / cl2 = {DRDP, DRDH, RO, P} of cell I and of
 // the cell DERIV pairs it with (I-S, or I itself for the k direction,
-// base3c.f:4892 with IL > NTOT).  Returns the 5 flux components.
-FF_DI void roe_flux(const double q[5][4], double nx, double ny, double nz, double area,
-                    int intem, const ff_params& p, double c_r, double c_l,
-                    const double cr[4], const double cl2[4], double f[5]) {
-  double roip, roim, rmip, rmim, rnip, rnim, rwip, rwim, ppi, pmi;
+// base3c.f:4892 with IL > NTOT).  Adds the 5 flux components to f.
+template <typename T>
+FF_DI void roe_flux(const T q[5][4], T nx, T ny, T nz, T area, int intem, const ff_params& p, T c_r, T c_l,
+                    const T cr[4], const T cl2[4], T f[5]) {
+  T roip, roim, rmip, rmim, rnip, rnim, rwip, rwim, ppi, pmi;
   xxtrap(q[0][0], q[0][1], q[0][2], q[0][3], intem, roip, roim);
   xxtrap(q[1][0], q[1][1], q[1][2], q[1][3], intem, rmip, rmim);
   xxtrap(q[2][0], q[2][1], q[2][2], q[2][3], intem, rnip, rnim);
   xxtrap(q[3][0], q[3][1], q[3][2], q[3][3], intem, rwip, rwim);
   xxtrap(q[4][0], q[4][1], q[4][2], q[4][3], intem, ppi, pmi);
-  roip = dmax(0.001 * p.frsden, roip);
-  ppi = dmax(0.001 * p.frspre, ppi);
-  roim = dmax(0.001 * p.frsden, roim);
-  pmi = dmax(0.001 * p.frspre, pmi);
-  const double rgm1 = rcp(p.gamma - 1.);
-  const double ypror = rcp(roip), yprol = rcp(roim);
+  roip = dmax(T(0.001) * T(p.frsden), roip);
+  ppi = dmax(T(0.001) * T(p.frspre), ppi);
+  roim = dmax(T(0.001) * T(p.frsden), roim);
+  pmi = dmax(T(0.001) * T(p.frspre), pmi);
+  const T rgm1 = rcp(T(p.gamma) - T(1.)), e0 = T(p.e0ref);
+  const T ypror = rcp(roip), yprol = rcp(roim);
   // EFPRO state.f:620 (perfect gas): p / ((gamma - 1) rho)
-  double eip = ppi * rgm1 * ypror - p.e0ref;
-  double eim = pmi * rgm1 * yprol - p.e0ref;
-  double elr = ppi * rgm1 * yprol - p.e0ref;
-  double erl = pmi * rgm1 * ypror - p.e0ref;
+  T eip = ppi * rgm1 * ypror - e0;
+  T eim = pmi * rgm1 * yprol - e0;
+  T elr = ppi * rgm1 * yprol - e0;
+  T erl = pmi * rgm1 * ypror - e0;
   // DERIV base3c.f:707 (Glaister hat derivatives)
-  double ypro1 = rcp(cr[2]), ypro2 = rcp(cl2[2]);
-  double rdh1 = rcp(cr[1]), rdh2 = rcp(cl2[1]);
-  double dedph = 0.5 * ((-cr[0] * rdh1 - ypro1) + (-cl2[0] * rdh2 - ypro2));
-  double dedrh = 0.5 * ((rdh1 + cr[3] * (ypro1 * ypro1)) + (rdh2 + cl2[3] * (ypro2 * ypro2)));
+  T ypro1 = rcp(cr[2]), ypro2 = rcp(cl2[2]);
+  T rdh1 = rcp(cr[1]), rdh2 = rcp(cl2[1]);
+  T dedph = T(0.5) * ((-cr[0] * rdh1 - ypro1) + (-cl2[0] * rdh2 - ypro2));
+  T dedrh = T(0.5) * ((rdh1 + cr[3] * (ypro1 * ypro1)) + (rdh2 + cl2[3] * (ypro2 * ypro2)));
   {
-    double dpp = 2. * (ppi - pmi), drr = 2. * (roip - roim);
-    if (fabs(dpp) >= 1.e-2 * (ppi + pmi)) dedph = (eip + elr - eim - erl) / dpp;
-    if (fabs(drr) >= 1.e-2 * (roip + roim)) dedrh = (eip + erl - eim - elr) / drr;
+    T dpp = T(2.) * (ppi - pmi), drr = T(2.) * (roip - roim);
+    if (fabs(dpp) >= T(1.e-2) * (ppi + pmi)) dedph = (eip + elr - eim - erl) / dpp;
+    if (fabs(drr) >= T(1.e-2) * (roip + roim)) dedrh = (eip + erl - eim - elr) / drr;
   }
-  double a21, a22, a23, a31, a32, a33;
+  T a21, a22, a23, a31, a32, a33;
   surfvects(nx, ny, nz, a21, a22, a23, a31, a32, a33);
-  double ur = nx * rmip + ny * rnip + nz * rwip;
-  double vr = a21 * rmip + a22 * rnip + a23 * rwip;
-  double wr = a31 * rmip + a32 * rnip + a33 * rwip;
-  double ul = nx * rmim + ny * rnim + nz * rwim;
-  double vl = a21 * rmim + a22 * rnim + a23 * rwim;
-  double wl = a31 * rmim + a32 * rnim + a33 * rwim;
-  double eir = eip + .5 * (ur * ur + vr * vr + wr * wr);
-  double eil = eim + .5 * (ul * ul + vl * vl + wl * wl);
-  double pr = ppi, pl = pmi;
-  double hr = eir + pr * ypror, hl = eil + yprol * pl;
-  double rohat = sqrt(roip * roim), yproh = rcp(rohat);
-  double sqrl = rcp(roim + rohat), cql = roim * sqrl, cqr = 1. - cql;
-  double uhat = cqr * ur + cql * ul, vhat = cqr * vr + cql * vl, what = cqr * wr + cql * wl;
-  double hhat = cqr * hr + cql * hl, ehat = cqr * eip + cql * eim;
-  double phat = rohat * (hhat - ehat - .5 * (uhat * uhat + vhat * vhat + what * what));
+  T ur = nx * rmip + ny * rnip + nz * rwip;
+  T vr = a21 * rmip + a22 * rnip + a23 * rwip;
+  T wr = a31 * rmip + a32 * rnip + a33 * rwip;
+  T ul = nx * rmim + ny * rnim + nz * rwim;
+  T vl = a21 * rmim + a22 * rnim + a23 * rwim;
+  T wl = a31 * rmim + a32 * rnim + a33 * rwim;
+  T eir = eip + T(.5) * (ur * ur + vr * vr + wr * wr);
+  T eil = eim + T(.5) * (ul * ul + vl * vl + wl * wl);
+  T pr = ppi, pl = pmi;
+  T hr = eir + pr * ypror, hl = eil + yprol * pl;
+  T rohat = sqrt(roip * roim), yproh = rcp(rohat);
+  T sqrl = rcp(roim + rohat), cql = roim * sqrl, cqr = T(1.) - cql;
+  T uhat = cqr * ur + cql * ul, vhat = cqr * vr + cql * vl, what = cqr * wr + cql * wl;
+  T hhat = cqr * hr + cql * hl, ehat = cqr * eip + cql * eim;
+  T phat = rohat * (hhat - ehat - T(.5) * (uhat * uhat + vhat * vhat + what * what));
   phat = dmin(dmax(pr, pl), phat);
   phat = dmax(dmin(pr, pl), phat);
-  double drdhh = rcp(dedrh - phat * (yproh * yproh));
-  double drdph = -drdhh * (dedph + yproh);
-  double chat2 = rcp(drdhh * yproh + drdph);
-  double cmin = dmin(c_r, c_l), cmax = dmax(c_r, c_l);
+  T drdhh = rcp(dedrh - phat * (yproh * yproh));
+  T drdph = -drdhh * (dedph + yproh);
+  T chat2 = rcp(drdhh * yproh + drdph);
+  T cmin = dmin(c_r, c_l), cmax = dmax(c_r, c_l);
   chat2 = dmin(cmax * cmax, chat2);
   chat2 = dmax(cmin * cmin, chat2);
-  double chat = sqrt(chat2);
-  double pdpde = dedph;
-  double dro = roip - roim, du = ur - ul;
-  double dp = pr - pl;
-  double pchat2 = rcp(chat * chat);
-  double alfa1 = .5 * (dp + rohat * chat * du) * pchat2;
-  double alfa2 = .5 * (dp - rohat * chat * du) * pchat2;
-  double alfa3 = dro - dp * pchat2;
-  double alfa4 = rohat * (vr - vl), alfa5 = rohat * (wr - wl);
-  double rl1h = uhat + chat, rl2h = uhat - chat, rl3h = uhat;
-  double rl1 = fabs(rl1h), rl2 = fabs(rl2h), rl3 = fabs(rl3h);
+  T chat = sqrt(chat2);
+  T pdpde = dedph;
+  T dro = roip - roim, du = ur - ul;
+  T dp = pr - pl;
+  T pchat2 = rcp(chat * chat);
+  T alfa1 = T(.5) * (dp + rohat * chat * du) * pchat2;
+  T alfa2 = T(.5) * (dp - rohat * chat * du) * pchat2;
+  T alfa3 = dro - dp * pchat2;
+  T alfa4 = rohat * (vr - vl), alfa5 = rohat * (wr - wl);
+  T rl1h = uhat + chat, rl2h = uhat - chat, rl3h = uhat;
+  T rl1 = fabs(rl1h), rl2 = fabs(rl2h), rl3 = fabs(rl3h);
   if (p.entropy_fix) {
-    double e22;
-    e22 = 4. * dmax(dmax(1.e-10, rl1h - (ul + c_l)), (ur + c_r) - rl1h);
-    if (rl1 <= e22) rl1 = .5 * (rl1h * rl1h + e22 * e22) / e22;
-    e22 = 4. * dmax(dmax(1.e-10, rl2h - (ul - c_l)), (ur - c_r) - rl2h);
-    if (rl2 <= e22) rl2 = .5 * (rl2h * rl2h + e22 * e22) / e22;
-    e22 = 4. * dmax(dmax(1.e-10, rl3h - ul), ur - rl3h);
-    if (rl3 <= e22) rl3 = .5 * (rl3h * rl3h + e22 * e22) / e22;
+    T e22;
+    e22 = T(4.) * dmax(dmax(T(1.e-10), rl1h - (ul + c_l)), (ur + c_r) - rl1h);
+    if (rl1 <= e22) rl1 = T(.5) * (rl1h * rl1h + e22 * e22) / e22;
+    e22 = T(4.) * dmax(dmax(T(1.e-10), rl2h - (ul - c_l)), (ur - c_r) - rl2h);
+    if (rl2 <= e22) rl2 = T(.5) * (rl2h * rl2h + e22 * e22) / e22;
+    e22 = T(4.) * dmax(dmax(T(1.e-10), rl3h - ul), ur - rl3h);
+    if (rl3 <= e22) rl3 = T(.5) * (rl3h * rl3h + e22 * e22) / e22;
   }
-  double roucr = roip * ur, roucl = roim * ul;
-  double damp = rl1 * alfa1 + rl2 * alfa2 + rl3 * alfa3;
-  double ha = .5 * area;
-  double f1 = ha * (roucr + roucl - damp);
-  double f2 = ha * (roucr * ur + pr + roucl * ul + pl - (damp * uhat + (rl1 * alfa1 - rl2 * alfa2) * chat));
-  double f3 = ha * (roucr * vr + roucl * vl - damp * vhat - rl3 * alfa4);
-  double f4 = ha * (roucr * wr + roucl * wl - damp * what - rl3 * alfa5);
-  double f5 = ha * (roucr * hr + roucl * hl - damp * hhat
-                    - ((rl1 * alfa1 - rl2 * alfa2) * uhat * chat - rl3 * alfa3 * rohat * (chat * chat) * pdpde
-                       + rl3 * alfa4 * vhat + rl3 * alfa5 * what));
+  T roucr = roip * ur, roucl = roim * ul;
+  T damp = rl1 * alfa1 + rl2 * alfa2 + rl3 * alfa3;
+  T ha = T(.5) * area;
+  T f1 = ha * (roucr + roucl - damp);
+  T f2 = ha * (roucr * ur + pr + roucl * ul + pl - (damp * uhat + (rl1 * alfa1 - rl2 * alfa2) * chat));
+  T f3 = ha * (roucr * vr + roucl * vl - damp * vhat - rl3 * alfa4);
+  T f4 = ha * (roucr * wr + roucl * wl - damp * what - rl3 * alfa5);
+  T f5 = ha * (roucr * hr + roucl * hl - damp * hhat
+               - ((rl1 * alfa1 - rl2 * alfa2) * uhat * chat - rl3 * alfa3 * rohat * (chat * chat) * pdpde
+                  + rl3 * alfa4 * vhat + rl3 * alfa5 * what));
   f[0] += f1;
   f[1] += nx * f2 + a21 * f3 + a31 * f4;
   f[2] += ny * f2 + a22 * f3 + a32 * f4;

@@ -204,13 +204,13 @@ bool res_fused() {
   return f;
 }
 
-template <int NV, int NT, int I_, int J_, int K_, bool ST = false>
+template <int NV, int NT, int I_, int J_, int K_, bool ST = false, typename FT = double>
 void launch_residual_fused_s(cudaStream_t st, const BlockCtx* b, int level) {
   dim3 g(nblk(b->imax, I_), nblk(b->jmax, J_), nblk(b->kmax, K_));
   const size_t sm = residual_fused_smem(NV, I_, J_, K_, ST);
-  cudaFuncSetAttribute(k_residual_fused<NV, NT, I_, J_, K_, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaFuncSetAttribute(k_residual_fused<NV, NT, I_, J_, K_, ST, FT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sm);
-  k_residual_fused<NV, NT, I_, J_, K_, ST><<<g, NT, sm, st>>>(b->db, b->prm, level);
+  k_residual_fused<NV, NT, I_, J_, K_, ST, FT><<<g, NT, sm, st>>>(b->db, b->prm, level);
 }
 
 template <int NV, int NT>
@@ -219,6 +219,12 @@ void launch_residual_fused_t(cudaStream_t st, dim3 g, const BlockCtx* b, int lev
   // the form the autotuner chose for this block (512 threads only): tile
   // shape, and the stencil staged in shared memory or not
   const int sh = NT == 512 ? b->res_shape : 0;
+  if (level > 1 && b->prm.res_fp32) {   // a coarse level's face fluxes in FP32 (unstaged tiles)
+    const int s3 = sh % RES_NSHAPE;
+    if (s3 == 1) return launch_residual_fused_s<NV, NT, 16, 8, 4, false, float>(st, b, level);
+    if (s3 == 2) return launch_residual_fused_s<NV, NT, 8, 8, 8, false, float>(st, b, level);
+    return launch_residual_fused_s<NV, NT, 32, 4, 4, false, float>(st, b, level);
+  }
   if constexpr (NT == 512) {
     if (sh == 3) return launch_residual_fused_s<NV, NT, 32, 4, 4, true>(st, b, level);
     if (sh == 4) return launch_residual_fused_s<NV, NT, 16, 8, 4, true>(st, b, level);

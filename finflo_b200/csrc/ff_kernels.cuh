@@ -427,62 +427,65 @@ FF_DI void visc_flux(const DevBlock& b, const ff_params& p, size_t L, int S, int
 }
 
 // FLUXDO base3c.f:3677 (thin layer, IDIFF = 1): the viscous flux on coarse
-// levels and whenever FULLNS is off.
-FF_DI void visc_flux_thin(const DevBlock& b, const ff_params& p, size_t L, int S, int dir, double f[5],
-                          double fe0 = 0.) {
-#define LD(s, n) __ldg(b.a[s] + (n))
+// levels and whenever FULLNS is off (T = float for a coarse face pass in
+// FP32).
+template <typename T>
+FF_DI void visc_flux_thin(const DevBlock& b, const ff_params& p, size_t L, int S, int dir, T f[5], T fe0 = T(0.)) {
+#define LD(s, n) T(__ldg(b.a[s] + (n)))
   size_t M = L - S;
   const int ao = 4 * (dir - 1);
-  double area = LD(FF_A1 + ao, L);
-  double nx = LD(FF_A1XA + ao, L), ny = LD(FF_A1YA + ao, L), nz = LD(FF_A1ZA + ao, L);
-  double surg = -area * (area / (LD(FF_VOL, L) + LD(FF_VOL, M)));
-  double surf = surg * (LD(FF_EPS2, L) * LD(FF_VIS, L) + LD(FF_EPS2, M) * LD(FF_VIS, M));
-  double surfe = surg * (LD(FF_CP, L) * LD(FF_VIST, L) / p.prt + LD(FF_CH, L)
-                         + LD(FF_CP, M) * LD(FF_VIST, M) / p.prt + LD(FF_CH, M));
-  double ul = LD(FF_U, L), um = LD(FF_U, M), vl = LD(FF_V, L), vm = LD(FF_V, M), wl = LD(FF_W, L), wm = LD(FF_W, M);
-  double duc = .333333 * (nx * (ul - um) + ny * (vl - vm) + nz * (wl - wm));
-  double f2 = surf * (ul - um + nx * duc);
-  double f3 = surf * (vl - vm + ny * duc);
-  double f4 = surf * (wl - wm + nz * duc);
-  double f5 = .5 * ((ul + um) * f2 + (vl + vm) * f3 + (wl + wm) * f4);
-  f[0] = 0.; f[1] = f2; f[2] = f3; f[3] = f4;
+  T area = LD(FF_A1 + ao, L);
+  T nx = LD(FF_A1XA + ao, L), ny = LD(FF_A1YA + ao, L), nz = LD(FF_A1ZA + ao, L);
+  T surg = -area * (area / (LD(FF_VOL, L) + LD(FF_VOL, M)));
+  T surf = surg * (LD(FF_EPS2, L) * LD(FF_VIS, L) + LD(FF_EPS2, M) * LD(FF_VIS, M));
+  const T prt = T(p.prt);
+  T surfe = surg * (LD(FF_CP, L) * LD(FF_VIST, L) / prt + LD(FF_CH, L)
+                    + LD(FF_CP, M) * LD(FF_VIST, M) / prt + LD(FF_CH, M));
+  T ul = LD(FF_U, L), um = LD(FF_U, M), vl = LD(FF_V, L), vm = LD(FF_V, M), wl = LD(FF_W, L), wm = LD(FF_W, M);
+  T duc = T(.333333) * (nx * (ul - um) + ny * (vl - vm) + nz * (wl - wm));
+  T f2 = surf * (ul - um + nx * duc);
+  T f3 = surf * (vl - vm + ny * duc);
+  T f4 = surf * (wl - wm + nz * duc);
+  T f5 = T(.5) * ((ul + um) * f2 + (vl + vm) * f3 + (wl + wm) * f4);
+  f[0] = T(0.); f[1] = f2; f[2] = f3; f[3] = f4;
   f[4] = fe0 + f5 + surfe * (LD(FF_TEMP, L) - LD(FF_TEMP, M));
 #undef LD
 }
 
 // BOTSKE base3c.f:6147 wall-face flux (laminar, TURCOR false as FLUCYC passes
 // it, wall at rest).  II = interior cell at the wall.
+template <typename T>
 FF_DI void wall_flux(const DevBlock& b, const ff_params& p, size_t II, int S, int idir, int dir,
-                     int iheat, int intem, double f[5]) {
-#define LD(s, n) __ldg(b.a[s] + (n))
-  double rc1 = intem == 6 ? 1. : 1.5, rc2 = rc1 - 1.;
-  const double prs = p.pr / p.prt, ymr = .166666667, eps = 1.e-3;
+                     int iheat, int intem, T f[5]) {
+#define LD(s, n) T(__ldg(b.a[s] + (n)))
+  T rc1 = intem == 6 ? T(1.) : T(1.5), rc2 = rc1 - T(1.);
+  const T prs = T(p.pr) / T(p.prt), ymr = T(.166666667), eps = T(1.e-3);
   int lstrid = S * idir;
   size_t II2 = II + lstrid, IF1 = idir == 1 ? II : II + S;
   int ihfl = (iheat == 2 || iheat >= 12) ? 1 : 0;
   int iht = (iheat == 0 || iheat == 15) ? 0 : 1;
   const int ao = 4 * (dir - 1);
-  double a_f = LD(FF_A1 + ao, IF1);
-  double dist = (a_f + LD(FF_A1 + ao, IF1 + lstrid)) / LD(FF_VOL, II);
-  double surg = -dist * ymr;
-  double visb = dmax(0.01 * p.frsvis, rc1 * LD(FF_VIS, II) - rc2 * LD(FF_VIS, II2));
-  double chsb = dmax(eps, rc1 * LD(FF_CH, II) - rc2 * LD(FF_CH, II2));
-  double pb1 = dmax(0.01 * p.frspre, rc1 * LD(FF_P, II) - rc2 * LD(FF_P, II2));
-  double surf = surg * visb;
-  double surfe = surg * (prs * 0. / visb + 1.) * chsb;
-  double tempb = dmax(0.01 * p.frstem, rc1 * LD(FF_TEMP, II) - rc2 * LD(FF_TEMP, II2));
-  double tsurf = iheat == 3 ? tempb : p.frstem;
-  double cvii = iht * idir * (9.000 * LD(FF_TEMP, II) - 1.000 * LD(FF_TEMP, II2) - 8. * tsurf);
-  double uvii = idir * (9.000 * LD(FF_U, II) - 1.000 * LD(FF_U, II2));
-  double vvii = idir * (9.000 * LD(FF_V, II) - 1.000 * LD(FF_V, II2));
-  double wvii = idir * (9.000 * LD(FF_W, II) - 1.000 * LD(FF_W, II2));
-  double ax = LD(FF_A1XA + ao, IF1), ay = LD(FF_A1YA + ao, IF1), az = LD(FF_A1ZA + ao, IF1);
-  double duc = .33333 * (ay * vvii + az * wvii + ax * uvii);
-  double f2v = surf * (uvii + ax * duc);
-  double f3v = surf * (vvii + ay * duc);
-  double f4v = surf * (wvii + az * duc);
-  double f5v = (1 - ihfl) * surfe * cvii;
-  f[0] = 0.;
+  T a_f = LD(FF_A1 + ao, IF1);
+  T dist = (a_f + LD(FF_A1 + ao, IF1 + lstrid)) / LD(FF_VOL, II);
+  T surg = -dist * ymr;
+  T visb = dmax(T(0.01) * T(p.frsvis), rc1 * LD(FF_VIS, II) - rc2 * LD(FF_VIS, II2));
+  T chsb = dmax(eps, rc1 * LD(FF_CH, II) - rc2 * LD(FF_CH, II2));
+  T pb1 = dmax(T(0.01) * T(p.frspre), rc1 * LD(FF_P, II) - rc2 * LD(FF_P, II2));
+  T surf = surg * visb;
+  T surfe = surg * (prs * T(0.) / visb + T(1.)) * chsb;
+  T tempb = dmax(T(0.01) * T(p.frstem), rc1 * LD(FF_TEMP, II) - rc2 * LD(FF_TEMP, II2));
+  T tsurf = iheat == 3 ? tempb : T(p.frstem);
+  T cvii = T(iht * idir) * (T(9.000) * LD(FF_TEMP, II) - T(1.000) * LD(FF_TEMP, II2) - T(8.) * tsurf);
+  T uvii = T(idir) * (T(9.000) * LD(FF_U, II) - T(1.000) * LD(FF_U, II2));
+  T vvii = T(idir) * (T(9.000) * LD(FF_V, II) - T(1.000) * LD(FF_V, II2));
+  T wvii = T(idir) * (T(9.000) * LD(FF_W, II) - T(1.000) * LD(FF_W, II2));
+  T ax = LD(FF_A1XA + ao, IF1), ay = LD(FF_A1YA + ao, IF1), az = LD(FF_A1ZA + ao, IF1);
+  T duc = T(.33333) * (ay * vvii + az * wvii + ax * uvii);
+  T f2v = surf * (uvii + ax * duc);
+  T f3v = surf * (vvii + ay * duc);
+  T f4v = surf * (wvii + az * duc);
+  T f5v = T(1 - ihfl) * surfe * cvii;
+  f[0] = T(0.);
   f[1] = a_f * (ax * pb1 + f2v);
   f[2] = a_f * (ay * pb1 + f3v);
   f[3] = a_f * (az * pb1 + f4v);
@@ -550,9 +553,11 @@ FF_DI void vl_flux(const double qc[5][4], double nx, double ny, double nz, doubl
 }
 
 // sq (optional): RO, U, V, W, P of cell L in a staged stencil, variable v
-// at sq[v * vs], the cells along the face normal es apart.
+// at sq[v * vs], the cells along the face normal es apart.  T = float: a
+// coarse level's face in FP32 (loads converted, fluxes in FP32).
+template <typename T>
 FF_DI void face_flux(const DevBlock& b, const ff_params& p, int dir, size_t L, int m, int t1, int t2,
-                     int level, double f[5], const double* sq = nullptr, int es = 0, int vs = 0) {
+                     int level, T f[5], const double* sq = nullptr, int es = 0, int vs = 0) {
   const int S = dir == 1 ? 1 : (dir == 2 ? b.is : b.il);
   const int nmax = dir == 1 ? b.imax : (dir == 2 ? b.jmax : b.kmax);
   int intem = dir == 1 ? p.interi : (dir == 2 ? p.interj : p.interk);
@@ -572,46 +577,52 @@ FF_DI void face_flux(const DevBlock& b, const ff_params& p, int dir, size_t L, i
   }
   const int idi = dir == 1 ? p.idi1 : (dir == 2 ? p.idi2 : p.idi3);
   if (m <= min(idi, nmax + 1)) {   // SINVIS base3c.f:3876: viscous faces
-    if (level == 1 && p.fullns) visc_flux(b, p, L, S, dir, f);
-    else visc_flux_thin(b, p, L, S, dir, f);
+    bool full = false;
+    if constexpr (sizeof(T) == sizeof(double)) {
+      if (level == 1 && p.fullns) { visc_flux(b, p, L, S, dir, f); full = true; }
+    }
+    if (!full) visc_flux_thin(b, p, L, S, dir, f);
   } else {
-    f[0] = f[1] = f[2] = f[3] = f[4] = 0.;
+    f[0] = f[1] = f[2] = f[3] = f[4] = T(0.);
   }
   const int ao = 4 * (dir - 1);
-  if (p.vanleer) {   // IFLUX=0: FLUXVL on the conservative variables
-    double qc[5][4];
-    const int sc[5] = {FF_RO, FF_RM, FF_RN, FF_RW, FF_E};
+  if constexpr (sizeof(T) == sizeof(double)) {
+    if (p.vanleer) {   // IFLUX=0: FLUXVL on the conservative variables
+      double qc[5][4];
+      const int sc[5] = {FF_RO, FF_RM, FF_RN, FF_RW, FF_E};
 #pragma unroll
-    for (int v = 0; v < 5; v++) {
-      const double* a = b.a[sc[v]];
-      qc[v][0] = __ldg(a + L - 2 * S); qc[v][1] = __ldg(a + L - S); qc[v][2] = __ldg(a + L); qc[v][3] = __ldg(a + L + S);
+      for (int v = 0; v < 5; v++) {
+        const double* a = b.a[sc[v]];
+        qc[v][0] = __ldg(a + L - 2 * S); qc[v][1] = __ldg(a + L - S); qc[v][2] = __ldg(a + L); qc[v][3] = __ldg(a + L + S);
+      }
+      vl_flux(qc, __ldg(b.a[FF_A1XA + ao] + L), __ldg(b.a[FF_A1YA + ao] + L), __ldg(b.a[FF_A1ZA + ao] + L),
+              __ldg(b.a[FF_A1 + ao] + L), intem, p, f);
+      return;
     }
-    vl_flux(qc, __ldg(b.a[FF_A1XA + ao] + L), __ldg(b.a[FF_A1YA + ao] + L), __ldg(b.a[FF_A1ZA + ao] + L),
-            __ldg(b.a[FF_A1 + ao] + L), intem, p, f);
-    return;
   }
-  double q[5][4];
+  T q[5][4];
   const int sl[5] = {FF_RO, FF_U, FF_V, FF_W, FF_P};
   if (sq) {
 #pragma unroll
     for (int v = 0; v < 5; v++) {
       const double* a = sq + v * vs;
-      q[v][0] = a[-2 * es]; q[v][1] = a[-es]; q[v][2] = a[0]; q[v][3] = a[es];
+      q[v][0] = T(a[-2 * es]); q[v][1] = T(a[-es]); q[v][2] = T(a[0]); q[v][3] = T(a[es]);
     }
   } else {
 #pragma unroll
     for (int v = 0; v < 5; v++) {
       const double* a = b.a[sl[v]];
-      q[v][0] = __ldg(a + L - 2 * S); q[v][1] = __ldg(a + L - S); q[v][2] = __ldg(a + L); q[v][3] = __ldg(a + L + S);
+      q[v][0] = T(__ldg(a + L - 2 * S)); q[v][1] = T(__ldg(a + L - S)); q[v][2] = T(__ldg(a + L));
+      q[v][3] = T(__ldg(a + L + S));
     }
   }
   size_t L2 = dir == 3 ? L : L - S;
-  double cr[4] = {__ldg(b.a[FF_DRDP] + L), __ldg(b.a[FF_DRDH] + L), q[0][2], q[4][2]};
+  T cr[4] = {T(__ldg(b.a[FF_DRDP] + L)), T(__ldg(b.a[FF_DRDH] + L)), q[0][2], q[4][2]};
   // RO and P of cell L2 (L itself for k faces) are in the stencil
-  double cl[4] = {__ldg(b.a[FF_DRDP] + L2), __ldg(b.a[FF_DRDH] + L2), dir == 3 ? q[0][2] : q[0][1],
-                  dir == 3 ? q[4][2] : q[4][1]};
-  roe_flux(q, __ldg(b.a[FF_A1XA + ao] + L), __ldg(b.a[FF_A1YA + ao] + L), __ldg(b.a[FF_A1ZA + ao] + L),
-           __ldg(b.a[FF_A1 + ao] + L), intem, p, __ldg(b.a[FF_C] + L), __ldg(b.a[FF_C] + L - S), cr, cl, f);
+  T cl[4] = {T(__ldg(b.a[FF_DRDP] + L2)), T(__ldg(b.a[FF_DRDH] + L2)), dir == 3 ? q[0][2] : q[0][1],
+             dir == 3 ? q[4][2] : q[4][1]};
+  roe_flux(q, T(__ldg(b.a[FF_A1XA + ao] + L)), T(__ldg(b.a[FF_A1YA + ao] + L)), T(__ldg(b.a[FF_A1ZA + ao] + L)),
+           T(__ldg(b.a[FF_A1 + ao] + L)), intem, p, T(__ldg(b.a[FF_C] + L)), T(__ldg(b.a[FF_C] + L - S)), cr, cl, f);
 }
 
 // RESIDU: fused k, i, j face fluxes and SWEEP res3c.f:992 for a 32x4x4 tile.

@@ -188,11 +188,12 @@ __global__ void k_temder_ke(DevBlock b, int level) {
 // ---- face fluxes of the seven equations ---------------------------------
 
 // FLUXKE base3c.f:4753-5120 with k and omega (UROT = 0); q[v][m], v = ro, u,
-// v, w, p, rk, reps; m = cells I-2S..I+S.  Adds to f[7].
-FF_DI void roe_flux_ke(const double q[7][4], double nx, double ny, double nz, double area, int intem,
-                       int intet, const ff_params& p, double c_r, double c_l, const double cr[4],
-                       const double cl2[4], double f[7]) {
-  double roip, roim, rmip, rmim, rnip, rnim, rwip, rwim, ppi, pmi, rkip, rkim, reip, reim;
+// v, w, p, rk, reps; m = cells I-2S..I+S.  Adds to f[7].  T = float for a
+// coarse face pass in FP32.
+template <typename T>
+FF_DI void roe_flux_ke(const T q[7][4], T nx, T ny, T nz, T area, int intem, int intet, const ff_params& p,
+                       T c_r, T c_l, const T cr[4], const T cl2[4], T f[7]) {
+  T roip, roim, rmip, rmim, rnip, rnim, rwip, rwim, ppi, pmi, rkip, rkim, reip, reim;
   xxtrap(q[0][0], q[0][1], q[0][2], q[0][3], intem, roip, roim);
   xxtrap(q[1][0], q[1][1], q[1][2], q[1][3], intem, rmip, rmim);
   xxtrap(q[2][0], q[2][1], q[2][2], q[2][3], intem, rnip, rnim);
@@ -200,89 +201,89 @@ FF_DI void roe_flux_ke(const double q[7][4], double nx, double ny, double nz, do
   xxtrap(q[4][0], q[4][1], q[4][2], q[4][3], intem, ppi, pmi);
   xxtrap(q[5][0], q[5][1], q[5][2], q[5][3], intet, rkip, rkim);
   xxtrap(q[6][0], q[6][1], q[6][2], q[6][3], intet, reip, reim);
-  roip = dmax(0.001 * p.frsden, roip);
-  ppi = dmax(0.001 * p.frspre, ppi);
-  roim = dmax(0.001 * p.frsden, roim);
-  pmi = dmax(0.001 * p.frspre, pmi);
-  const double rgm1 = rcp(p.gamma - 1.);
-  const double ypror = rcp(roip), yprol = rcp(roim);
-  double eip = ppi * rgm1 * ypror - p.e0ref;
-  double eim = pmi * rgm1 * yprol - p.e0ref;
-  double elr = ppi * rgm1 * yprol - p.e0ref;
-  double erl = pmi * rgm1 * ypror - p.e0ref;
-  double ypro1 = rcp(cr[2]), ypro2 = rcp(cl2[2]);
-  double rdh1 = rcp(cr[1]), rdh2 = rcp(cl2[1]);
-  double dedph = 0.5 * ((-cr[0] * rdh1 - ypro1) + (-cl2[0] * rdh2 - ypro2));
-  double dedrh = 0.5 * ((rdh1 + cr[3] * (ypro1 * ypro1)) + (rdh2 + cl2[3] * (ypro2 * ypro2)));
+  roip = dmax(T(0.001) * T(p.frsden), roip);
+  ppi = dmax(T(0.001) * T(p.frspre), ppi);
+  roim = dmax(T(0.001) * T(p.frsden), roim);
+  pmi = dmax(T(0.001) * T(p.frspre), pmi);
+  const T rgm1 = rcp(T(p.gamma) - T(1.)), e0 = T(p.e0ref);
+  const T ypror = rcp(roip), yprol = rcp(roim);
+  T eip = ppi * rgm1 * ypror - e0;
+  T eim = pmi * rgm1 * yprol - e0;
+  T elr = ppi * rgm1 * yprol - e0;
+  T erl = pmi * rgm1 * ypror - e0;
+  T ypro1 = rcp(cr[2]), ypro2 = rcp(cl2[2]);
+  T rdh1 = rcp(cr[1]), rdh2 = rcp(cl2[1]);
+  T dedph = T(0.5) * ((-cr[0] * rdh1 - ypro1) + (-cl2[0] * rdh2 - ypro2));
+  T dedrh = T(0.5) * ((rdh1 + cr[3] * (ypro1 * ypro1)) + (rdh2 + cl2[3] * (ypro2 * ypro2)));
   {
-    double dpp = 2. * (ppi - pmi), drr = 2. * (roip - roim);
-    if (fabs(dpp) >= 1.e-2 * (ppi + pmi)) dedph = (eip + elr - eim - erl) / dpp;
-    if (fabs(drr) >= 1.e-2 * (roip + roim)) dedrh = (eip + erl - eim - elr) / drr;
+    T dpp = T(2.) * (ppi - pmi), drr = T(2.) * (roip - roim);
+    if (fabs(dpp) >= T(1.e-2) * (ppi + pmi)) dedph = (eip + elr - eim - erl) / dpp;
+    if (fabs(drr) >= T(1.e-2) * (roip + roim)) dedrh = (eip + erl - eim - elr) / drr;
   }
-  double a21, a22, a23, a31, a32, a33;
+  T a21, a22, a23, a31, a32, a33;
   surfvects(nx, ny, nz, a21, a22, a23, a31, a32, a33);
-  double ur = nx * rmip + ny * rnip + nz * rwip;
-  double vr = a21 * rmip + a22 * rnip + a23 * rwip;
-  double wr = a31 * rmip + a32 * rnip + a33 * rwip;
-  double ul = nx * rmim + ny * rnim + nz * rwim;
-  double vl = a21 * rmim + a22 * rnim + a23 * rwim;
-  double wl = a31 * rmim + a32 * rnim + a33 * rwim;
-  double rkipi = dmax(0.001 * p.rklim, rkip), reipi = dmax(0.001 * p.epslim, reip);
-  double rkimi = dmax(0.001 * p.rklim, rkim), reimi = dmax(0.001 * p.epslim, reim);
-  double rkr = rkipi * ypror, rkl = rkimi * yprol;
-  double eir = eip + .5 * (ur * ur + vr * vr + wr * wr) + rkr;
-  double eil = eim + .5 * (ul * ul + vl * vl + wl * wl) + rkl;
-  double pr = ppi, pl = pmi, pkr = .6667 * rkipi, pkl = .6667 * rkimi;
-  double epsr = reipi * ypror, epsl = reimi * yprol;
-  double hr = eir + pr * ypror, hl = eil + yprol * pl;
-  double rohat = sqrt(roip * roim), yproh = rcp(rohat);
-  double sqrl = rcp(roim + rohat), cql = roim * sqrl, cqr = 1. - cql;
-  double uhat = cqr * ur + cql * ul, vhat = cqr * vr + cql * vl, what = cqr * wr + cql * wl;
-  double hhat = cqr * hr + cql * hl, ehat = cqr * eip + cql * eim;
-  double rkhat = cqr * rkr + cql * rkl, epshat = cqr * epsr + cql * epsl;
-  double phat = rohat * (hhat - ehat - .5 * (uhat * uhat + vhat * vhat + what * what) - rkhat);
+  T ur = nx * rmip + ny * rnip + nz * rwip;
+  T vr = a21 * rmip + a22 * rnip + a23 * rwip;
+  T wr = a31 * rmip + a32 * rnip + a33 * rwip;
+  T ul = nx * rmim + ny * rnim + nz * rwim;
+  T vl = a21 * rmim + a22 * rnim + a23 * rwim;
+  T wl = a31 * rmim + a32 * rnim + a33 * rwim;
+  T rkipi = dmax(T(0.001) * T(p.rklim), rkip), reipi = dmax(T(0.001) * T(p.epslim), reip);
+  T rkimi = dmax(T(0.001) * T(p.rklim), rkim), reimi = dmax(T(0.001) * T(p.epslim), reim);
+  T rkr = rkipi * ypror, rkl = rkimi * yprol;
+  T eir = eip + T(.5) * (ur * ur + vr * vr + wr * wr) + rkr;
+  T eil = eim + T(.5) * (ul * ul + vl * vl + wl * wl) + rkl;
+  T pr = ppi, pl = pmi, pkr = T(.6667) * rkipi, pkl = T(.6667) * rkimi;
+  T epsr = reipi * ypror, epsl = reimi * yprol;
+  T hr = eir + pr * ypror, hl = eil + yprol * pl;
+  T rohat = sqrt(roip * roim), yproh = rcp(rohat);
+  T sqrl = rcp(roim + rohat), cql = roim * sqrl, cqr = T(1.) - cql;
+  T uhat = cqr * ur + cql * ul, vhat = cqr * vr + cql * vl, what = cqr * wr + cql * wl;
+  T hhat = cqr * hr + cql * hl, ehat = cqr * eip + cql * eim;
+  T rkhat = cqr * rkr + cql * rkl, epshat = cqr * epsr + cql * epsl;
+  T phat = rohat * (hhat - ehat - T(.5) * (uhat * uhat + vhat * vhat + what * what) - rkhat);
   phat = dmin(dmax(pr, pl), phat);
   phat = dmax(dmin(pr, pl), phat);
-  double drdhh = rcp(dedrh - phat * (yproh * yproh));
-  double drdph = -drdhh * (dedph + yproh);
-  double xturb = 1. + .6667 * rkhat * yproh * drdph;
-  double chat2 = xturb / (drdhh * yproh + drdph);
-  double cmin = dmin(c_r, c_l), cmax = dmax(c_r, c_l);
+  T drdhh = rcp(dedrh - phat * (yproh * yproh));
+  T drdph = -drdhh * (dedph + yproh);
+  T xturb = T(1.) + T(.6667) * rkhat * yproh * drdph;
+  T chat2 = xturb / (drdhh * yproh + drdph);
+  T cmin = dmin(c_r, c_l), cmax = dmax(c_r, c_l);
   chat2 = dmin(cmax * cmax, chat2);
   chat2 = dmax(cmin * cmin, chat2);
-  double chat = sqrt(chat2);
-  double pdpde = dedph;
-  double dro = roip - roim, du = ur - ul, dk = rkr - rkl;
-  double dp = pr - pl + .6667 * (rkhat * dro + rohat * dk);
-  double pchat2 = rcp(chat * chat);
-  double alfa1 = .5 * (dp + rohat * chat * du) * pchat2;
-  double alfa2 = .5 * (dp - rohat * chat * du) * pchat2;
-  double alfa3 = dro - dp * pchat2;
-  double alfa4 = rohat * (vr - vl), alfa5 = rohat * (wr - wl), alfa6 = rohat * dk, alfa7 = rohat * (epsr - epsl);
-  double rl1h = uhat + chat, rl2h = uhat - chat, rl3h = uhat;
-  double rl1 = fabs(rl1h), rl2 = fabs(rl2h), rl3 = fabs(rl3h);
+  T chat = sqrt(chat2);
+  T pdpde = dedph;
+  T dro = roip - roim, du = ur - ul, dk = rkr - rkl;
+  T dp = pr - pl + T(.6667) * (rkhat * dro + rohat * dk);
+  T pchat2 = rcp(chat * chat);
+  T alfa1 = T(.5) * (dp + rohat * chat * du) * pchat2;
+  T alfa2 = T(.5) * (dp - rohat * chat * du) * pchat2;
+  T alfa3 = dro - dp * pchat2;
+  T alfa4 = rohat * (vr - vl), alfa5 = rohat * (wr - wl), alfa6 = rohat * dk, alfa7 = rohat * (epsr - epsl);
+  T rl1h = uhat + chat, rl2h = uhat - chat, rl3h = uhat;
+  T rl1 = fabs(rl1h), rl2 = fabs(rl2h), rl3 = fabs(rl3h);
   if (p.entropy_fix) {
-    double e22;
-    e22 = 4. * dmax(dmax(1.e-10, rl1h - (ul + c_l)), (ur + c_r) - rl1h);
-    if (rl1 <= e22) rl1 = .5 * (rl1h * rl1h + e22 * e22) / e22;
-    e22 = 4. * dmax(dmax(1.e-10, rl2h - (ul - c_l)), (ur - c_r) - rl2h);
-    if (rl2 <= e22) rl2 = .5 * (rl2h * rl2h + e22 * e22) / e22;
-    e22 = 4. * dmax(dmax(1.e-10, rl3h - ul), ur - rl3h);
-    if (rl3 <= e22) rl3 = .5 * (rl3h * rl3h + e22 * e22) / e22;
+    T e22;
+    e22 = T(4.) * dmax(dmax(T(1.e-10), rl1h - (ul + c_l)), (ur + c_r) - rl1h);
+    if (rl1 <= e22) rl1 = T(.5) * (rl1h * rl1h + e22 * e22) / e22;
+    e22 = T(4.) * dmax(dmax(T(1.e-10), rl2h - (ul - c_l)), (ur - c_r) - rl2h);
+    if (rl2 <= e22) rl2 = T(.5) * (rl2h * rl2h + e22 * e22) / e22;
+    e22 = T(4.) * dmax(dmax(T(1.e-10), rl3h - ul), ur - rl3h);
+    if (rl3 <= e22) rl3 = T(.5) * (rl3h * rl3h + e22 * e22) / e22;
   }
-  double roucr = roip * ur, roucl = roim * ul;
-  double damp = rl1 * alfa1 + rl2 * alfa2 + rl3 * alfa3;
-  double ha = .5 * area;
-  double f1 = ha * (roucr + roucl - damp);
-  double f2 = ha * (roucr * ur + pr + pkr + roucl * ul + pl + pkl - (damp * uhat + (rl1 * alfa1 - rl2 * alfa2) * chat));
-  double f3 = ha * (roucr * vr + roucl * vl - damp * vhat - rl3 * alfa4);
-  double f4 = ha * (roucr * wr + roucl * wl - damp * what - rl3 * alfa5);
-  double f5 = ha * (roucr * (hr + pkr * ypror) + roucl * (hl + pkl * yprol) - damp * hhat -
-                    ((rl1 * alfa1 - rl2 * alfa2) * uhat * chat - rl3 * alfa3 * rohat * (chat * chat) * pdpde +
-                     rl3 * alfa4 * vhat + rl3 * alfa5 * what) +
-                    rl3 * alfa6 * (1. - .6667 * rohat * pdpde));
-  double f6 = ha * (roucr * rkr + roucl * rkl - damp * rkhat - rl3 * alfa6);
-  double f7 = ha * (roucr * epsr + roucl * epsl - damp * epshat - rl3 * alfa7);
+  T roucr = roip * ur, roucl = roim * ul;
+  T damp = rl1 * alfa1 + rl2 * alfa2 + rl3 * alfa3;
+  T ha = T(.5) * area;
+  T f1 = ha * (roucr + roucl - damp);
+  T f2 = ha * (roucr * ur + pr + pkr + roucl * ul + pl + pkl - (damp * uhat + (rl1 * alfa1 - rl2 * alfa2) * chat));
+  T f3 = ha * (roucr * vr + roucl * vl - damp * vhat - rl3 * alfa4);
+  T f4 = ha * (roucr * wr + roucl * wl - damp * what - rl3 * alfa5);
+  T f5 = ha * (roucr * (hr + pkr * ypror) + roucl * (hl + pkl * yprol) - damp * hhat -
+               ((rl1 * alfa1 - rl2 * alfa2) * uhat * chat - rl3 * alfa3 * rohat * (chat * chat) * pdpde +
+                rl3 * alfa4 * vhat + rl3 * alfa5 * what) +
+               rl3 * alfa6 * (T(1.) - T(.6667) * rohat * pdpde));
+  T f6 = ha * (roucr * rkr + roucl * rkl - damp * rkhat - rl3 * alfa6);
+  T f7 = ha * (roucr * epsr + roucl * epsl - damp * epshat - rl3 * alfa7);
   f[0] += f1;
   f[1] += nx * f2 + a21 * f3 + a31 * f4;
   f[2] += ny * f2 + a22 * f3 + a32 * f4;
@@ -322,73 +323,76 @@ FF_DI void flkebl_face(const DevBlock& b, size_t I, int S, int dir, const FaceGe
 }
 
 // FLUDKE base3c.f:5547: thin-layer k and omega diffusion (coarse levels).
-FF_DI void fludke_face(const DevBlock& b, size_t I, int S, int dir, double& frk, double& feps) {
-#define LD(s, n) __ldg(b.a[s] + (n))
+template <typename T>
+FF_DI void fludke_face(const DevBlock& b, size_t I, int S, int dir, T& frk, T& feps) {
+#define LD(s, n) T(__ldg(b.a[s] + (n)))
   size_t M = I - S;
-  double f1 = LD(FF_FUN1, I), onemf1 = dmax(0.0, 1.0 - f1);
-  double psigk = f1 * SST_SIGRK1 + onemf1 * SST_SIGRK2;
-  double psige = f1 * SST_SIGOM1 + onemf1 * SST_SIGOM2;
-  double area = LD(FF_A1 + 4 * (dir - 1), I);
-  double ypd2 = area / (LD(FF_VOL, I) + LD(FF_VOL, M));
-  double surg = -area * ypd2;
-  double rmut2 = (LD(FF_EPS2, I) - 1.) * LD(FF_VIS, I) + (LD(FF_EPS2, M) - 1.) * LD(FF_VIS, M);
-  double vv = LD(FF_VIS, I) + LD(FF_VIS, M);
-  double ypro1 = rcp(LD(FF_RO, I)), ypro2 = rcp(LD(FF_RO, M));
+  T f1 = LD(FF_FUN1, I), onemf1 = dmax(T(0.0), T(1.0) - f1);
+  T psigk = f1 * T(SST_SIGRK1) + onemf1 * T(SST_SIGRK2);
+  T psige = f1 * T(SST_SIGOM1) + onemf1 * T(SST_SIGOM2);
+  T area = LD(FF_A1 + 4 * (dir - 1), I);
+  T ypd2 = area / (LD(FF_VOL, I) + LD(FF_VOL, M));
+  T surg = -area * ypd2;
+  T rmut2 = (LD(FF_EPS2, I) - T(1.)) * LD(FF_VIS, I) + (LD(FF_EPS2, M) - T(1.)) * LD(FF_VIS, M);
+  T vv = LD(FF_VIS, I) + LD(FF_VIS, M);
+  T ypro1 = rcp(LD(FF_RO, I)), ypro2 = rcp(LD(FF_RO, M));
   frk = surg * (vv + rmut2 * psigk) * (LD(FF_RK, I) * ypro1 - LD(FF_RK, M) * ypro2);
   feps = surg * (vv + rmut2 * psige) * (LD(FF_REPS, I) * ypro1 - LD(FF_REPS, M) * ypro2);
 #undef LD
 }
 
-// BOTSKE with k and omega (smooth wall, IDIS=2): seven wall fluxes.
+// BOTSKE with k and omega (smooth wall, IDIS=2): seven wall fluxes (T =
+// float for a coarse face pass in FP32).
+template <typename T>
 FF_DI void wall_flux_ke(const DevBlock& b, const ff_params& p, size_t II, int S, int idir, int dir, int iheat,
-                        int intem, double f[7]) {
-#define LD(s, n) __ldg(b.a[s] + (n))
-  double rc1 = intem == 6 ? 1. : 1.5, rc2 = rc1 - 1.;
-  const double prs = p.pr / p.prt, ymr = .166666667, eps = 1.e-3;
+                        int intem, T f[7]) {
+#define LD(s, n) T(__ldg(b.a[s] + (n)))
+  T rc1 = intem == 6 ? T(1.) : T(1.5), rc2 = rc1 - T(1.);
+  const T prs = T(p.pr) / T(p.prt), ymr = T(.166666667), eps = T(1.e-3);
   int lstrid = S * idir;
   size_t II2 = II + lstrid, IF1 = idir == 1 ? II : II + S;
   int ihfl = (iheat == 2 || iheat >= 12) ? 1 : 0;
   int iht = (iheat == 0 || iheat == 15) ? 0 : 1;
   const int ao = 4 * (dir - 1);
-  double a_f = LD(FF_A1 + ao, IF1);
-  double dist = (a_f + LD(FF_A1 + ao, IF1 + lstrid)) / LD(FF_VOL, II);
-  double surg = -dist * ymr;
-  double visb = dmax(0.01 * p.frsvis, rc1 * LD(FF_VIS, II) - rc2 * LD(FF_VIS, II2));
-  double chsb = dmax(eps, rc1 * LD(FF_CH, II) - rc2 * LD(FF_CH, II2));
-  double straib = dmax(eps, rc1 * LD(FF_STRAIN, II) - rc2 * LD(FF_STRAIN, II2));
-  double pb1 = dmax(0.01 * p.frspre, rc1 * LD(FF_P, II) - rc2 * LD(FF_P, II2));
-  double rob = dmax(0.001 * p.frsden, rc1 * LD(FF_RO, II) - rc2 * LD(FF_RO, II2));
-  double surf = surg * visb;
-  double surfe = surg * (prs * 0. / visb + 1.) * chsb;
-  double rapub = 1.0E-20;
-  double surfrk = surg * (1.0 + SST_SIGRK1 * rapub) * visb;
-  double surfep = surg * (1.0 + SST_SIGOM1 * rapub) * visb;
-  double ypro1 = rcp(LD(FF_RO, II)), ypro2 = rcp(LD(FF_RO, II2));
-  double rnub = visb / rob;
-  double plusfc = sqrt(rnub * straib) / rnub;
-  double yplus1 = 2.0 * plusfc / dist;
-  double skpmin = dmax(dmin(2.4 * pow(yplus1, 0.85), 8.0), 1.e-3);
-  double skplus = dmax(0.0 * plusfc, skpmin);
-  double pskp = 1.0 / skplus;
-  double omsurf = straib * dmax(2500.0 * pskp * pskp, 100.0 * pskp);
-  double tempb = dmax(0.01 * p.frstem, rc1 * LD(FF_TEMP, II) - rc2 * LD(FF_TEMP, II2));
-  double tsurf = iheat == 3 ? tempb : p.frstem;
-  double cvii = iht * idir * (9.000 * LD(FF_TEMP, II) - 1.000 * LD(FF_TEMP, II2) - 8. * tsurf);
-  double uvii = idir * (9.000 * LD(FF_U, II) - 1.000 * LD(FF_U, II2));
-  double vvii = idir * (9.000 * LD(FF_V, II) - 1.000 * LD(FF_V, II2));
-  double wvii = idir * (9.000 * LD(FF_W, II) - 1.000 * LD(FF_W, II2));
-  double ax = LD(FF_A1XA + ao, IF1), ay = LD(FF_A1YA + ao, IF1), az = LD(FF_A1ZA + ao, IF1);
-  double duc = .33333 * (ay * vvii + az * wvii + ax * uvii);
-  double f2v = surf * (uvii + ax * duc);
-  double f3v = surf * (vvii + ay * duc);
-  double f4v = surf * (wvii + az * duc);
-  double f5v = (1 - ihfl) * surfe * cvii;
-  double evii = idir * (9.0 * LD(FF_REPS, II) * ypro1 - 1.0 * LD(FF_REPS, II2) * ypro2 - 8. * omsurf);
-  double rkii = idir * (9.000 * LD(FF_RK, II) * ypro1 - 1.000 * LD(FF_RK, II2) * ypro2);
-  rkii = idir * dmax(idir * rkii, 0.0);
-  double f6v = surfrk * rkii;
-  double f7v = surfep * evii;
-  f[0] = 0.;
+  T a_f = LD(FF_A1 + ao, IF1);
+  T dist = (a_f + LD(FF_A1 + ao, IF1 + lstrid)) / LD(FF_VOL, II);
+  T surg = -dist * ymr;
+  T visb = dmax(T(0.01) * T(p.frsvis), rc1 * LD(FF_VIS, II) - rc2 * LD(FF_VIS, II2));
+  T chsb = dmax(eps, rc1 * LD(FF_CH, II) - rc2 * LD(FF_CH, II2));
+  T straib = dmax(eps, rc1 * LD(FF_STRAIN, II) - rc2 * LD(FF_STRAIN, II2));
+  T pb1 = dmax(T(0.01) * T(p.frspre), rc1 * LD(FF_P, II) - rc2 * LD(FF_P, II2));
+  T rob = dmax(T(0.001) * T(p.frsden), rc1 * LD(FF_RO, II) - rc2 * LD(FF_RO, II2));
+  T surf = surg * visb;
+  T surfe = surg * (prs * T(0.) / visb + T(1.)) * chsb;
+  T rapub = T(1.0E-20);
+  T surfrk = surg * (T(1.0) + T(SST_SIGRK1) * rapub) * visb;
+  T surfep = surg * (T(1.0) + T(SST_SIGOM1) * rapub) * visb;
+  T ypro1 = rcp(LD(FF_RO, II)), ypro2 = rcp(LD(FF_RO, II2));
+  T rnub = visb / rob;
+  T plusfc = sqrt(rnub * straib) / rnub;
+  T yplus1 = T(2.0) * plusfc / dist;
+  T skpmin = dmax(dmin(T(2.4) * pow(yplus1, T(0.85)), T(8.0)), T(1.e-3));
+  T skplus = dmax(T(0.0) * plusfc, skpmin);
+  T pskp = T(1.0) / skplus;
+  T omsurf = straib * dmax(T(2500.0) * pskp * pskp, T(100.0) * pskp);
+  T tempb = dmax(T(0.01) * T(p.frstem), rc1 * LD(FF_TEMP, II) - rc2 * LD(FF_TEMP, II2));
+  T tsurf = iheat == 3 ? tempb : T(p.frstem);
+  T cvii = T(iht * idir) * (T(9.000) * LD(FF_TEMP, II) - T(1.000) * LD(FF_TEMP, II2) - T(8.) * tsurf);
+  T uvii = T(idir) * (T(9.000) * LD(FF_U, II) - T(1.000) * LD(FF_U, II2));
+  T vvii = T(idir) * (T(9.000) * LD(FF_V, II) - T(1.000) * LD(FF_V, II2));
+  T wvii = T(idir) * (T(9.000) * LD(FF_W, II) - T(1.000) * LD(FF_W, II2));
+  T ax = LD(FF_A1XA + ao, IF1), ay = LD(FF_A1YA + ao, IF1), az = LD(FF_A1ZA + ao, IF1);
+  T duc = T(.33333) * (ay * vvii + az * wvii + ax * uvii);
+  T f2v = surf * (uvii + ax * duc);
+  T f3v = surf * (vvii + ay * duc);
+  T f4v = surf * (wvii + az * duc);
+  T f5v = T(1 - ihfl) * surfe * cvii;
+  T evii = T(idir) * (T(9.0) * LD(FF_REPS, II) * ypro1 - T(1.0) * LD(FF_REPS, II2) * ypro2 - T(8.) * omsurf);
+  T rkii = T(idir) * (T(9.000) * LD(FF_RK, II) * ypro1 - T(1.000) * LD(FF_RK, II2) * ypro2);
+  rkii = T(idir) * dmax(T(idir) * rkii, T(0.0));
+  T f6v = surfrk * rkii;
+  T f7v = surfep * evii;
+  f[0] = T(0.);
   f[1] = a_f * (ax * pb1 + f2v);
   f[2] = a_f * (ay * pb1 + f3v);
   f[3] = a_f * (az * pb1 + f4v);
@@ -402,8 +406,9 @@ FF_DI void wall_flux_ke(const DevBlock& b, const ff_params& p, size_t II, int S,
 // FLUXKE; BOTSKE on walls).
 // sq (optional): the seven MUSCL variables of cell L in a staged stencil,
 // variable v at sq[v * vs], the cells along the face normal es apart.
+template <typename T>
 FF_DI void face_flux_ke(const DevBlock& b, const ff_params& p, int dir, size_t L, int m, int t1, int t2,
-                        int level, double f[7], const double* sq = nullptr, int es = 0, int vs = 0) {
+                        int level, T f[7], const double* sq = nullptr, int es = 0, int vs = 0) {
   const int S = dir == 1 ? 1 : (dir == 2 ? b.is : b.il);
   const int nmax = dir == 1 ? b.imax : (dir == 2 ? b.jmax : b.kmax);
   int intem = dir == 1 ? p.interi : (dir == 2 ? p.interj : p.interk);
@@ -427,41 +432,47 @@ FF_DI void face_flux_ke(const DevBlock& b, const ff_params& p, int dir, size_t L
   // inviscid flux to the viscous one (F = Fv + Fi per component), and one
   // addition is the same either way round.
 #pragma unroll
-  for (int v = 0; v < 7; v++) f[v] = 0.;
+  for (int v = 0; v < 7; v++) f[v] = T(0.);
   {
-    double q[7][4];
+    T q[7][4];
     const int sl[7] = {FF_RO, FF_U, FF_V, FF_W, FF_P, FF_RK, FF_REPS};
     if (sq) {
 #pragma unroll
       for (int v = 0; v < 7; v++) {
         const double* a = sq + v * vs;
-        q[v][0] = a[-2 * es]; q[v][1] = a[-es]; q[v][2] = a[0]; q[v][3] = a[es];
+        q[v][0] = T(a[-2 * es]); q[v][1] = T(a[-es]); q[v][2] = T(a[0]); q[v][3] = T(a[es]);
       }
     } else {
 #pragma unroll
       for (int v = 0; v < 7; v++) {
         const double* a = b.a[sl[v]];
-        q[v][0] = __ldg(a + L - 2 * S); q[v][1] = __ldg(a + L - S); q[v][2] = __ldg(a + L); q[v][3] = __ldg(a + L + S);
+        q[v][0] = T(__ldg(a + L - 2 * S)); q[v][1] = T(__ldg(a + L - S)); q[v][2] = T(__ldg(a + L));
+        q[v][3] = T(__ldg(a + L + S));
       }
     }
     size_t L2 = dir == 3 ? L : L - S;
-    double cr[4] = {__ldg(b.a[FF_DRDP] + L), __ldg(b.a[FF_DRDH] + L), q[0][2], q[4][2]};
+    T cr[4] = {T(__ldg(b.a[FF_DRDP] + L)), T(__ldg(b.a[FF_DRDH] + L)), q[0][2], q[4][2]};
     // RO and P of cell L2 (L itself for k faces) are in the stencil
-    double cl[4] = {__ldg(b.a[FF_DRDP] + L2), __ldg(b.a[FF_DRDH] + L2), dir == 3 ? q[0][2] : q[0][1],
-                    dir == 3 ? q[4][2] : q[4][1]};
+    T cl[4] = {T(__ldg(b.a[FF_DRDP] + L2)), T(__ldg(b.a[FF_DRDH] + L2)), dir == 3 ? q[0][2] : q[0][1],
+               dir == 3 ? q[4][2] : q[4][1]};
     const int ao = 4 * (dir - 1);
-    roe_flux_ke(q, __ldg(b.a[FF_A1XA + ao] + L), __ldg(b.a[FF_A1YA + ao] + L), __ldg(b.a[FF_A1ZA + ao] + L),
-                __ldg(b.a[FF_A1 + ao] + L), intem, intet, p, __ldg(b.a[FF_C] + L), __ldg(b.a[FF_C] + L - S), cr, cl,
-                f);
+    roe_flux_ke(q, T(__ldg(b.a[FF_A1XA + ao] + L)), T(__ldg(b.a[FF_A1YA + ao] + L)),
+                T(__ldg(b.a[FF_A1ZA + ao] + L)), T(__ldg(b.a[FF_A1 + ao] + L)), intem, intet, p,
+                T(__ldg(b.a[FF_C] + L)), T(__ldg(b.a[FF_C] + L - S)), cr, cl, f);
   }
   if (m <= min(idi, nmax + 1)) {
-    double frk, feps, fv[5], f4;
-    if (level == 1 && p.fullns) {   // FLKEBL, SETV12, FLUXBL
-      const FaceGeom g = face_geom(b, L, S, dir);
-      flkebl_face(b, L, S, dir, g, frk, feps);
-      visc_flux(b, p, L, S, dir, g, fv);
-      f4 = frk + fv[4];
-    } else {                        // FLUDKE, FLUXDO
+    T frk, feps, fv[5], f4;
+    bool full = false;
+    if constexpr (sizeof(T) == sizeof(double)) {
+      if (level == 1 && p.fullns) {   // FLKEBL, SETV12, FLUXBL
+        const FaceGeom g = face_geom(b, L, S, dir);
+        flkebl_face(b, L, S, dir, g, frk, feps);
+        visc_flux(b, p, L, S, dir, g, fv);
+        f4 = frk + fv[4];
+        full = true;
+      }
+    }
+    if (!full) {                      // FLUDKE, FLUXDO
       fludke_face(b, L, S, dir, frk, feps);
       visc_flux_thin(b, p, L, S, dir, fv, frk);
       f4 = fv[4];
@@ -548,7 +559,10 @@ __global__ void __launch_bounds__(NT, RES_MIN_CTAS * 128 / NT) k_residual_sst(De
 // into shared memory (a box of (TI+4)(TJ+4)(TK+4) cells of which the
 // tile's three cross arms are filled), and every face reads its four-cell
 // stencil from there instead of global memory.
-template <int NV, int NT, int TI_, int TJ_, int TK_, bool STAGE = false>
+//
+// FT = float: the face fluxes of a coarse level in FP32 (the cells' sums
+// of their faces and the result stay FP64).
+template <int NV, int NT, int TI_, int TJ_, int TK_, bool STAGE = false, typename FT = double>
 FF_DI void residual_tile(const DevBlock& b, const ff_params& p, int level, int i0, int j0, int k0,
                          double* res_smem) {
   constexpr int TI = TI_, TJ = TJ_, TK = TK_;
@@ -581,7 +595,7 @@ FF_DI void residual_tile(const DevBlock& b, const ff_params& p, int level, int i
     if (I > b.imax + (dir == 1) || J > b.jmax + (dir == 2) || K > b.kmax + (dir == 3)) continue;
     const int m = dir == 1 ? I : (dir == 2 ? J : K);
     const int t1 = dir == 1 ? J : I, t2 = dir == 3 ? J : K;
-    double fl[NV];
+    FT fl[NV];
     const double* sq = nullptr;
     int es = 0;
     if constexpr (STAGE) {   // the face's high cell in the staged box
@@ -591,7 +605,7 @@ FF_DI void residual_tile(const DevBlock& b, const ff_params& p, int level, int i
     if constexpr (NV == 7) face_flux_ke(b, p, dir, ix(b, I, J, K), m, t1, t2, level, fl, sq, es, BOX);
     else face_flux(b, p, dir, ix(b, I, J, K), m, t1, t2, level, fl, sq, es, BOX);
 #pragma unroll
-    for (int v = 0; v < NV; v++) sF[v][f] = fl[v];
+    for (int v = 0; v < NV; v++) sF[v][f] = double(fl[v]);
   }
   __syncthreads();
   for (int c = tid; c < NC; c += NT) {
@@ -612,11 +626,11 @@ FF_DI void residual_tile(const DevBlock& b, const ff_params& p, int level, int i
   }
 }
 
-template <int NV, int NT, int TI_ = TI, int TJ_ = TJ, int TK_ = TK, bool STAGE = false>
+template <int NV, int NT, int TI_ = TI, int TJ_ = TJ, int TK_ = TK, bool STAGE = false, typename FT = double>
 __global__ void __launch_bounds__(NT, RES_MIN_CTAS * 128 / NT) k_residual_fused(DevBlock b, ff_params p, int level) {
   extern __shared__ double res_smem[];
-  residual_tile<NV, NT, TI_, TJ_, TK_, STAGE>(b, p, level, blockIdx.x * TI_, blockIdx.y * TJ_, blockIdx.z * TK_,
-                                              res_smem);
+  residual_tile<NV, NT, TI_, TJ_, TK_, STAGE, FT>(b, p, level, blockIdx.x * TI_, blockIdx.y * TJ_,
+                                                  blockIdx.z * TK_, res_smem);
 }
 
 // The same residual for several blocks in one launch: a block work-list of

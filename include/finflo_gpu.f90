@@ -67,7 +67,7 @@ module finflo_gpu
     integer(c_int) :: vanleer
     real(c_double) :: dt
     integer(c_int) :: predgs_full
-    integer(c_int) :: pad_
+    integer(c_int) :: res_fp32
   end type ff_params
 
   ! slot indices (enum ff_slot, include/finflo_types.h)

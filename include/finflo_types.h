@@ -76,7 +76,9 @@ typedef struct ff_params {
                                         /* that imps4.f:1460-1466 drops (its   */
                                         /* shift loop starts one index late);  */
                                         /* 0: the reference's sweep            */
-  int pad_;                             /* keeps the struct a multiple of 8   */
+  int res_fp32;                         /* 1 on a coarse level: its face      */
+                                        /* fluxes in FP32 (sums, update and   */
+                                        /* norms FP64); ignored on level 1    */
 } ff_params;
 
 /* Per-cell array slots of one block (names are the reference's MAIN_ARRAYS,
