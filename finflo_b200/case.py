@@ -41,8 +41,9 @@ class FFParams(ctypes.Structure):
         "rklim", "epslim", "turlim", "csimps", "re")] + [
         (n, ctypes.c_int) for n in (
             "interi", "interj", "interk", "entropy_fix", "iturb", "fullns",
-            "idi1", "idi2", "idi3", "coarse_inter", "lusgs_fp32", "ddadi", "timel", "vanleer")] + [
-        ("dt", ctypes.c_double), ("predgs_full", ctypes.c_int), ("res_fp32", ctypes.c_int)]
+            "idi1", "idi2", "idi3", "coarse_inter", "lusgs_fp32", "ddadi", "timel", "flux")] + [
+        ("dt", ctypes.c_double), ("predgs_full", ctypes.c_int), ("res_fp32", ctypes.c_int),
+        ("xxtral", ctypes.c_int)]
 
 
 class FFHaloItem(ctypes.Structure):
@@ -98,8 +99,14 @@ class FlowConditions:
         return dict(rho=rho, u=u, p=p, t=t, mu=mu, c=c)
 
 
+# enum ff_flux (include/finflo_types.h): the inviscid face flux by the
+# reference's FLUXTY names (FLUXME multi.f:3567)
+FLUX = {"roe": 0, "vanleer": 1, "wps": 2, "ausm": 3, "kt": 7, "hcusp": 8}
+FLUX_LAMINAR_ONLY = ("vanleer", "wps", "ausm")   # no RESIKE form (res3c.f:6946-7030)
+
+
 def make_params(fc: FlowConditions, dims, *, cfl=2.0, cfll=2.0, inter=3,
-                fullns=True, iturb=0, entropy_fix=False, lusgs_fp32=False) -> FFParams:
+                fullns=True, iturb=0, entropy_fix=False, lusgs_fp32=False, flux="roe") -> FFParams:
     fs = fc.freestream()
     p = FFParams()
     p.gamma, p.rgas, p.pr, p.prt = fc.gamma, fc.rgas, fc.pr, fc.prt
@@ -121,6 +128,7 @@ def make_params(fc: FlowConditions, dims, *, cfl=2.0, cfll=2.0, inter=3,
     p.idi1, p.idi2, p.idi3 = imax + 1, jmax + 1, kmax + 1
     p.coarse_inter = 55
     p.lusgs_fp32 = int(lusgs_fp32)
+    p.flux = FLUX[flux]
     return p
 
 

@@ -79,20 +79,60 @@ FF_DI void xxtrap(T r0, T r1, T r2, T r3, int intem, T& rip, T& rim) {
   }
 }
 
+// XXTRAA base3c.f:1444-1570: XXTRAP with the cells' extents d[0..3] along
+// the face normal (D1/D2/D3 of cells I-2S..I+S): differences become slopes
+// over the centre distances, the half extents scale the extrapolation.
+// FLUXKE, FLUXKT and FLUCUSP use it in place of XXTRAP when XXTRAL is set.
+template <typename T>
+FF_DI void xxtraa(T r0, T r1, T r2, T r3, const T d[4], int intem, T& rip, T& rim) {
+  int inter = intem < 0 ? -intem : intem;
+  int inte2 = inter < 1 ? 1 : (inter > 5 ? 5 : inter);
+  T rk1 = inte2 == 1 ? T(0.) : (inte2 == 2 ? T(1.) : (inte2 == 3 ? T(1.3333333) : (inte2 == 4 ? T(2.) : T(1.5))));
+  T rk2 = T(2.) - rk1;
+  if (inter > 4 && !(intem <= 0 && intem >= -5)) {
+    rip = r2;
+    rim = r1;
+    return;
+  }
+  const T eps = T(1.e-10);
+  const T dxl = T(.5) * d[1], dxr = T(.5) * d[2];
+  const T dx0 = T(1.) / (d[0] + d[1] + eps), dx1 = T(1.) / (d[1] + d[2] + eps), dx2 = T(1.) / (d[2] + d[3] + eps);
+  if (intem <= 0 && intem >= -5) {
+    rip = r2 - dxr * (dx1 * (r2 - r1) * rk1 + dx2 * (r3 - r2) * rk2);
+    rim = r1 + dxl * (dx1 * (r2 - r1) * rk1 + dx0 * (r1 - r0) * rk2);
+  } else {
+    const T diff0 = dx0 * (r1 - r0), diff1 = dx1 * (r2 - r1), diff2 = dx2 * (r3 - r2);
+    const T diff12 = diff1 * diff1 + eps;
+    const T phibi = (diff12 + diff1 * diff0) / (diff12 + diff0 * diff0);
+    const T phifi = (diff12 + diff1 * diff2) / (diff12 + diff2 * diff2);
+    rip = r2 - dxr * phifi * (diff1 * rk1 + diff2 * rk2);
+    rim = r1 + dxl * phibi * (diff1 * rk1 + diff0 * rk2);
+  }
+}
+
+// The MUSCL pair of one variable (q = cells I-2S..I+S): XXTRAP, or XXTRAA
+// over the extents d (DD, XXTRAL set).
+template <bool DD, typename T>
+FF_DI void muscl(const T q[4], const T* d, int intem, T& ip, T& im) {
+  if constexpr (DD) xxtraa(q[0], q[1], q[2], q[3], d, intem, ip, im);
+  else xxtrap(q[0], q[1], q[2], q[3], intem, ip, im);
+}
+
 // Roe flux-difference splitting for a general EOS (FLUXKE base3c.f:4753-5120)
 // at one face; laminar (k = omega = 0), UROT = 0.  q[v][m]: v = ro,u,v,w,p,
 // m = cells I-2S, I-S, I, I+S.  cr / cl2 = {DRDP, DRDH, RO, P} of cell I and of
 // the cell DERIV pairs it with (I-S, or I itself for the k direction,
-// base3c.f:4892 with IL > NTOT).  Adds the 5 flux components to f.
-template <typename T>
+// base3c.f:4892 with IL > NTOT).  DD: XXTRAA over the extents dd (XXTRAL).
+// Adds the 5 flux components to f.
+template <typename T, bool DD = false>
 FF_DI void roe_flux(const T q[5][4], T nx, T ny, T nz, T area, int intem, const ff_params& p, T c_r, T c_l,
-                    const T cr[4], const T cl2[4], T f[5]) {
+                    const T cr[4], const T cl2[4], T f[5], const T* dd = nullptr) {
   T roip, roim, rmip, rmim, rnip, rnim, rwip, rwim, ppi, pmi;
-  xxtrap(q[0][0], q[0][1], q[0][2], q[0][3], intem, roip, roim);
-  xxtrap(q[1][0], q[1][1], q[1][2], q[1][3], intem, rmip, rmim);
-  xxtrap(q[2][0], q[2][1], q[2][2], q[2][3], intem, rnip, rnim);
-  xxtrap(q[3][0], q[3][1], q[3][2], q[3][3], intem, rwip, rwim);
-  xxtrap(q[4][0], q[4][1], q[4][2], q[4][3], intem, ppi, pmi);
+  muscl<DD>(q[0], dd, intem, roip, roim);
+  muscl<DD>(q[1], dd, intem, rmip, rmim);
+  muscl<DD>(q[2], dd, intem, rnip, rnim);
+  muscl<DD>(q[3], dd, intem, rwip, rwim);
+  muscl<DD>(q[4], dd, intem, ppi, pmi);
   roip = dmax(T(0.001) * T(p.frsden), roip);
   ppi = dmax(T(0.001) * T(p.frspre), ppi);
   roim = dmax(T(0.001) * T(p.frsden), roim);

@@ -219,7 +219,9 @@ void launch_residual_fused_t(cudaStream_t st, dim3 g, const BlockCtx* b, int lev
   // the form the autotuner chose for this block (512 threads only): tile
   // shape, and the stencil staged in shared memory or not
   const int sh = NT == 512 ? b->res_shape : 0;
-  if (level > 1 && b->prm.res_fp32) {   // a coarse level's face fluxes in FP32 (unstaged tiles)
+  // a coarse level's face fluxes in FP32 (unstaged tiles; Roe with XXTRAP
+  // only: the other schemes and XXTRAA run their FP64 face code)
+  if (level > 1 && b->prm.res_fp32 && b->prm.flux == FF_FLUX_ROE && !b->prm.xxtral) {
     const int s3 = sh % RES_NSHAPE;
     if (s3 == 1) return launch_residual_fused_s<NV, NT, 16, 8, 4, false, float>(st, b, level);
     if (s3 == 2) return launch_residual_fused_s<NV, NT, 8, 8, 8, false, float>(st, b, level);
@@ -1790,12 +1792,23 @@ int ff_destroy(void* ctx) {
   return 0;
 }
 
-int ff_block_add(void* ctx, int imax, int jmax, int kmax, int npatch, const ff_patch* patches,
-                 const ff_params* prm) {
-  Ctx* c = (Ctx*)ctx;
+// ff_params.flux: a known scheme, and for a k-omega block one that RESIKE
+// offers (van Leer, WPS and AUSM are laminar only: res3c.f:6946-7041).
+static const char* flux_check(const ff_params* prm) {
+  const int f = prm->flux;
+  if (f != FF_FLUX_ROE && f != FF_FLUX_VANLEER && f != FF_FLUX_WPS && f != FF_FLUX_AUSM && f != FF_FLUX_KT &&
+      f != FF_FLUX_HCUSP)
+    return "ff_params.flux: unknown scheme";
+  if (prm->iturb >= 3 && (f == FF_FLUX_VANLEER || f == FF_FLUX_WPS || f == FF_FLUX_AUSM))
+    return "ff_params.flux: van Leer, WPS and AUSM (IFLUX=0, 2, 3) are laminar only";
+  return nullptr;
+}
+
+// The body of ff_block_add: 0 and the new block's id in *id, or an error code.
+static int block_add(Ctx* c, int imax, int jmax, int kmax, int npatch, const ff_patch* patches,
+                     const ff_params* prm, int* id) {
   if (!c || imax < 2 || jmax < 2 || kmax < 1 || npatch < 0 || !prm) return fail(c, FF_ERR_ARG, "ff_block_add: bad dims");
-  if (prm->vanleer && prm->iturb >= 3)   // FLUXVL has no k-omega form (res3c.f:7041)
-    return fail(c, FF_ERR_ARG, "ff_block_add: van Leer flux (IFLUX=0) is laminar only");
+  if (const char* why = flux_check(prm)) return fail(c, FF_ERR_ARG, why);
   BlockCtx* b = new BlockCtx();
   b->imax = imax; b->jmax = jmax; b->kmax = kmax;
   b->ntot = (imax + 4) * (jmax + 4) * (kmax + 4);
@@ -1832,7 +1845,15 @@ int ff_block_add(void* ctx, int imax, int jmax, int kmax, int npatch, const ff_p
   }
   b->tuned = 0;
   c->blocks.push_back(b);
-  return (int)c->blocks.size() - 1;
+  *id = (int)c->blocks.size() - 1;
+  return FF_OK;
+}
+
+int ff_block_add(void* ctx, int imax, int jmax, int kmax, int npatch, const ff_patch* patches,
+                 const ff_params* prm) {
+  int id = -1;
+  const int rc = block_add((Ctx*)ctx, imax, jmax, kmax, npatch, patches, prm, &id);
+  return rc ? -rc : id;
 }
 
 int ff_mg_link(void* ctx, int fine, int coarse) {
@@ -1851,8 +1872,7 @@ int ff_block_params(void* ctx, int blk, const ff_params* prm) {
   Ctx* c = (Ctx*)ctx;
   BlockCtx* b = getb(c, blk);
   if (!b || !prm) return fail(c, FF_ERR_ARG, "ff_block_params");
-  if (prm->vanleer && prm->iturb >= 3)   // FLUXVL has no k-omega form (res3c.f:7041)
-    return fail(c, FF_ERR_ARG, "ff_block_params: van Leer flux (IFLUX=0) is laminar only");
+  if (const char* why = flux_check(prm)) return fail(c, FF_ERR_ARG, why);
   bool nv_changed = (b->prm.iturb >= 3) != (prm->iturb >= 3);
   bool fp_changed = (b->prm.lusgs_fp32 != 0) != (prm->lusgs_fp32 != 0);
   if ((b->prm.ddadi != 0) != (prm->ddadi != 0)) b->tuned = 0;

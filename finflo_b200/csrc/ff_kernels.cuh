@@ -470,7 +470,11 @@ FF_DI void wall_flux(const DevBlock& b, const ff_params& p, size_t II, int S, in
   T surg = -dist * ymr;
   T visb = dmax(T(0.01) * T(p.frsvis), rc1 * LD(FF_VIS, II) - rc2 * LD(FF_VIS, II2));
   T chsb = dmax(eps, rc1 * LD(FF_CH, II) - rc2 * LD(FF_CH, II2));
-  T pb1 = dmax(T(0.01) * T(p.frspre), rc1 * LD(FF_P, II) - rc2 * LD(FF_P, II2));
+  // PB = YP1*PB1 + YP4*PB4 (base3c.f:6304-6315, 6487): the extrapolated
+  // pressure, or its difference from FRSPRE for KT (IFLUX=7)
+  T pb1 = p.flux == FF_FLUX_KT
+              ? dmax(T(-.99) * T(p.frspre), rc1 * LD(FF_PDIFF, II) - rc2 * LD(FF_PDIFF, II2))
+              : dmax(T(0.01) * T(p.frspre), rc1 * LD(FF_P, II) - rc2 * LD(FF_P, II2));
   T surf = surg * visb;
   T surfe = surg * (prs * T(0.) / visb + T(1.)) * chsb;
   T tempb = dmax(T(0.01) * T(p.frstem), rc1 * LD(FF_TEMP, II) - rc2 * LD(FF_TEMP, II2));
@@ -497,8 +501,10 @@ FF_DI void wall_flux(const DevBlock& b, const ff_params& p, size_t II, int S, in
 // FLUXVL base3c.f:1733-1961 (IFLUX=0) at one face: van Leer flux-vector
 // splitting of the MUSCL-extrapolated conservative variables qc[v][m]
 // (v = RO, RM, RN, RW, E; cells I-2S..I+S), perfect gas, added to f.
+// wps: FLUXWP base3c.f:1967-2195 (IFLUX=2), the wave/particle split of the
+// subsonic momentum and energy fluxes (base3c.f:2118-2125, 2156-2163).
 FF_DI void vl_flux(const double qc[5][4], double nx, double ny, double nz, double area, int intem,
-                   const ff_params& p, double f[5]) {
+                   const ff_params& p, bool wps, double f[5]) {
   const double gamma = p.gamma, gm1 = gamma - 1., ygm = 1. / gamma;
   double ip[5], im[5];
 #pragma unroll
@@ -524,8 +530,15 @@ FF_DI void vl_flux(const double qc[5][4], double nx, double ny, double nz, doubl
       fm[3] = area * rip0 * w; fm[4] = area * u * (ip[4] + pp);
     } else if (rma < 1.) {
       const double h = .5 * (rma - 1.), f1 = -area * ip[0] * c * (h * h);
-      fm[0] = f1; fm[1] = f1 * (gm1 * u - 2. * c) * ygm; fm[2] = f1 * v; fm[3] = f1 * w;
-      fm[4] = f1 * (ip[4] + pp) * ypro;
+      fm[0] = f1; fm[2] = f1 * v; fm[3] = f1 * w;
+      if (wps) {
+        const double rma2 = .25 * ((rma - 1.) * (rma - 1.)) * (2. + rma);
+        fm[1] = f1 * u + area * pp * rma2;
+        fm[4] = f1 * ip[4] * ypro + area * u * pp * rma2;
+      } else {
+        fm[1] = f1 * (gm1 * u - 2. * c) * ygm;
+        fm[4] = f1 * (ip[4] + pp) * ypro;
+      }
     } else {
       fm[0] = fm[1] = fm[2] = fm[3] = fm[4] = 0.;
     }
@@ -538,8 +551,15 @@ FF_DI void vl_flux(const double qc[5][4], double nx, double ny, double nz, doubl
       fp[3] = area * rim0 * w; fp[4] = area * u * (im[4] + pm);
     } else if (rma > -1.) {
       const double h = .5 * (rma + 1.), f1 = +area * im[0] * c * (h * h);
-      fp[0] = f1; fp[1] = f1 * (gm1 * u + 2. * c) * ygm; fp[2] = f1 * v; fp[3] = f1 * w;
-      fp[4] = f1 * (im[4] + pm) * ypro;
+      fp[0] = f1; fp[2] = f1 * v; fp[3] = f1 * w;
+      if (wps) {
+        const double rma2 = .25 * ((rma + 1.) * (rma + 1.)) * (2. - rma);
+        fp[1] = f1 * u + area * pm * rma2;
+        fp[4] = f1 * im[4] * ypro + area * u * pm * rma2;
+      } else {
+        fp[1] = f1 * (gm1 * u + 2. * c) * ygm;
+        fp[4] = f1 * (im[4] + pm) * ypro;
+      }
     } else {
       fp[0] = fp[1] = fp[2] = fp[3] = fp[4] = 0.;
     }
@@ -551,6 +571,8 @@ FF_DI void vl_flux(const double qc[5][4], double nx, double ny, double nz, doubl
   f[3] = nz * f2 + a23 * f3 + a33 * f4 + f[3];
   f[4] = fm[4] + fp[4] + f[4];
 }
+
+#include "ff_fluxes.cuh"
 
 // sq (optional): RO, U, V, W, P of cell L in a staged stencil, variable v
 // at sq[v * vs], the cells along the face normal es apart.  T = float: a
@@ -587,16 +609,8 @@ FF_DI void face_flux(const DevBlock& b, const ff_params& p, int dir, size_t L, i
   }
   const int ao = 4 * (dir - 1);
   if constexpr (sizeof(T) == sizeof(double)) {
-    if (p.vanleer) {   // IFLUX=0: FLUXVL on the conservative variables
-      double qc[5][4];
-      const int sc[5] = {FF_RO, FF_RM, FF_RN, FF_RW, FF_E};
-#pragma unroll
-      for (int v = 0; v < 5; v++) {
-        const double* a = b.a[sc[v]];
-        qc[v][0] = __ldg(a + L - 2 * S); qc[v][1] = __ldg(a + L - S); qc[v][2] = __ldg(a + L); qc[v][3] = __ldg(a + L + S);
-      }
-      vl_flux(qc, __ldg(b.a[FF_A1XA + ao] + L), __ldg(b.a[FF_A1YA + ao] + L), __ldg(b.a[FF_A1ZA + ao] + L),
-              __ldg(b.a[FF_A1 + ao] + L), intem, p, f);
+    if (p.flux != FF_FLUX_ROE) {   // the other IFLUX schemes (FLUCYC res3c.f:7890-7990)
+      alt_flux<5>(b, p, dir, L, S, intem, 1, f);
       return;
     }
   }
@@ -621,6 +635,16 @@ FF_DI void face_flux(const DevBlock& b, const ff_params& p, int dir, size_t L, i
   // RO and P of cell L2 (L itself for k faces) are in the stencil
   T cl[4] = {T(__ldg(b.a[FF_DRDP] + L2)), T(__ldg(b.a[FF_DRDH] + L2)), dir == 3 ? q[0][2] : q[0][1],
              dir == 3 ? q[4][2] : q[4][1]};
+  if constexpr (sizeof(T) == sizeof(double)) {
+    if (p.xxtral) {   // XXTRAA over the cells' extents along the normal
+      const double* D = b.a[FF_D1 + dir - 1];
+      const double dd[4] = {__ldg(D + L - 2 * S), __ldg(D + L - S), __ldg(D + L), __ldg(D + L + S)};
+      roe_flux<double, true>(q, __ldg(b.a[FF_A1XA + ao] + L), __ldg(b.a[FF_A1YA + ao] + L),
+                             __ldg(b.a[FF_A1ZA + ao] + L), __ldg(b.a[FF_A1 + ao] + L), intem, p, __ldg(b.a[FF_C] + L),
+                             __ldg(b.a[FF_C] + L - S), cr, cl, f, dd);
+      return;
+    }
+  }
   roe_flux(q, T(__ldg(b.a[FF_A1XA + ao] + L)), T(__ldg(b.a[FF_A1YA + ao] + L)), T(__ldg(b.a[FF_A1ZA + ao] + L)),
            T(__ldg(b.a[FF_A1 + ao] + L)), intem, p, T(__ldg(b.a[FF_C] + L)), T(__ldg(b.a[FF_C] + L - S)), cr, cl, f);
 }

@@ -190,17 +190,19 @@ __global__ void k_temder_ke(DevBlock b, int level) {
 // FLUXKE base3c.f:4753-5120 with k and omega (UROT = 0); q[v][m], v = ro, u,
 // v, w, p, rk, reps; m = cells I-2S..I+S.  Adds to f[7].  T = float for a
 // coarse face pass in FP32.
-template <typename T>
+// DD: XXTRAA over the extents dd (XXTRAL), with INTEM for k and omega too
+// (base3c.f:4861-4862).
+template <typename T, bool DD = false>
 FF_DI void roe_flux_ke(const T q[7][4], T nx, T ny, T nz, T area, int intem, int intet, const ff_params& p,
-                       T c_r, T c_l, const T cr[4], const T cl2[4], T f[7]) {
+                       T c_r, T c_l, const T cr[4], const T cl2[4], T f[7], const T* dd = nullptr) {
   T roip, roim, rmip, rmim, rnip, rnim, rwip, rwim, ppi, pmi, rkip, rkim, reip, reim;
-  xxtrap(q[0][0], q[0][1], q[0][2], q[0][3], intem, roip, roim);
-  xxtrap(q[1][0], q[1][1], q[1][2], q[1][3], intem, rmip, rmim);
-  xxtrap(q[2][0], q[2][1], q[2][2], q[2][3], intem, rnip, rnim);
-  xxtrap(q[3][0], q[3][1], q[3][2], q[3][3], intem, rwip, rwim);
-  xxtrap(q[4][0], q[4][1], q[4][2], q[4][3], intem, ppi, pmi);
-  xxtrap(q[5][0], q[5][1], q[5][2], q[5][3], intet, rkip, rkim);
-  xxtrap(q[6][0], q[6][1], q[6][2], q[6][3], intet, reip, reim);
+  muscl<DD>(q[0], dd, intem, roip, roim);
+  muscl<DD>(q[1], dd, intem, rmip, rmim);
+  muscl<DD>(q[2], dd, intem, rnip, rnim);
+  muscl<DD>(q[3], dd, intem, rwip, rwim);
+  muscl<DD>(q[4], dd, intem, ppi, pmi);
+  muscl<DD>(q[5], dd, DD ? intem : intet, rkip, rkim);
+  muscl<DD>(q[6], dd, DD ? intem : intet, reip, reim);
   roip = dmax(T(0.001) * T(p.frsden), roip);
   ppi = dmax(T(0.001) * T(p.frspre), ppi);
   roim = dmax(T(0.001) * T(p.frsden), roim);
@@ -360,7 +362,11 @@ FF_DI void wall_flux_ke(const DevBlock& b, const ff_params& p, size_t II, int S,
   T visb = dmax(T(0.01) * T(p.frsvis), rc1 * LD(FF_VIS, II) - rc2 * LD(FF_VIS, II2));
   T chsb = dmax(eps, rc1 * LD(FF_CH, II) - rc2 * LD(FF_CH, II2));
   T straib = dmax(eps, rc1 * LD(FF_STRAIN, II) - rc2 * LD(FF_STRAIN, II2));
-  T pb1 = dmax(T(0.01) * T(p.frspre), rc1 * LD(FF_P, II) - rc2 * LD(FF_P, II2));
+  // PB = YP1*PB1 + YP4*PB4 (base3c.f:6304-6315, 6487): the extrapolated
+  // pressure, or its difference from FRSPRE for KT (IFLUX=7)
+  T pb1 = p.flux == FF_FLUX_KT
+              ? dmax(T(-.99) * T(p.frspre), rc1 * LD(FF_PDIFF, II) - rc2 * LD(FF_PDIFF, II2))
+              : dmax(T(0.01) * T(p.frspre), rc1 * LD(FF_P, II) - rc2 * LD(FF_P, II2));
   T rob = dmax(T(0.001) * T(p.frsden), rc1 * LD(FF_RO, II) - rc2 * LD(FF_RO, II2));
   T surf = surg * visb;
   T surfe = surg * (prs * T(0.) / visb + T(1.)) * chsb;
@@ -433,7 +439,14 @@ FF_DI void face_flux_ke(const DevBlock& b, const ff_params& p, int dir, size_t L
   // addition is the same either way round.
 #pragma unroll
   for (int v = 0; v < 7; v++) f[v] = T(0.);
-  {
+  bool alt = false;
+  if constexpr (sizeof(T) == sizeof(double)) {
+    if (p.flux != FF_FLUX_ROE) {   // KT or H-CUSP (RESIKE res3c.f:7017-7036)
+      alt_flux<7>(b, p, dir, L, S, intem, intet, f);
+      alt = true;
+    }
+  }
+  if (!alt) {
     T q[7][4];
     const int sl[7] = {FF_RO, FF_U, FF_V, FF_W, FF_P, FF_RK, FF_REPS};
     if (sq) {
@@ -456,9 +469,21 @@ FF_DI void face_flux_ke(const DevBlock& b, const ff_params& p, int dir, size_t L
     T cl[4] = {T(__ldg(b.a[FF_DRDP] + L2)), T(__ldg(b.a[FF_DRDH] + L2)), dir == 3 ? q[0][2] : q[0][1],
                dir == 3 ? q[4][2] : q[4][1]};
     const int ao = 4 * (dir - 1);
-    roe_flux_ke(q, T(__ldg(b.a[FF_A1XA + ao] + L)), T(__ldg(b.a[FF_A1YA + ao] + L)),
-                T(__ldg(b.a[FF_A1ZA + ao] + L)), T(__ldg(b.a[FF_A1 + ao] + L)), intem, intet, p,
-                T(__ldg(b.a[FF_C] + L)), T(__ldg(b.a[FF_C] + L - S)), cr, cl, f);
+    bool done = false;
+    if constexpr (sizeof(T) == sizeof(double)) {
+      if (p.xxtral) {   // XXTRAA over the cells' extents along the normal
+        const double* D = b.a[FF_D1 + dir - 1];
+        const double dd[4] = {__ldg(D + L - 2 * S), __ldg(D + L - S), __ldg(D + L), __ldg(D + L + S)};
+        roe_flux_ke<double, true>(q, __ldg(b.a[FF_A1XA + ao] + L), __ldg(b.a[FF_A1YA + ao] + L),
+                                  __ldg(b.a[FF_A1ZA + ao] + L), __ldg(b.a[FF_A1 + ao] + L), intem, intet, p,
+                                  __ldg(b.a[FF_C] + L), __ldg(b.a[FF_C] + L - S), cr, cl, f, dd);
+        done = true;
+      }
+    }
+    if (!done)
+      roe_flux_ke(q, T(__ldg(b.a[FF_A1XA + ao] + L)), T(__ldg(b.a[FF_A1YA + ao] + L)),
+                  T(__ldg(b.a[FF_A1ZA + ao] + L)), T(__ldg(b.a[FF_A1 + ao] + L)), intem, intet, p,
+                  T(__ldg(b.a[FF_C] + L)), T(__ldg(b.a[FF_C] + L - S)), cr, cl, f);
   }
   if (m <= min(idi, nmax + 1)) {
     T frk, feps, fv[5], f4;

@@ -22,7 +22,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libfinflo_gpu.so")
 _SRC = [os.path.join(_HERE, "csrc", f) for f in ("ff_gpu.cu", "ff_kernels.cuh", "ff_device.cuh",
                                                  "ff_noalloc.cu", "ff_sst.cuh", "ff_pipe.cuh",
-                                                 "ff_ddadi.cuh", "ff_grid.cuh", "ff_fortran.cu")]
+                                                 "ff_ddadi.cuh", "ff_grid.cuh", "ff_fortran.cu", "ff_fluxes.cuh")]
 NVCC_FLAGS = ["-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC", "-shared", "-std=c++17"]
 

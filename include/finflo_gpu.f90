@@ -22,11 +22,15 @@ module finflo_gpu
   use, intrinsic :: iso_c_binding
   implicit none
 
-  integer(c_int), parameter :: FF_ABI_VERSION = 5
+  integer(c_int), parameter :: FF_ABI_VERSION = 6
   integer(c_int), parameter :: FF_OK = 0, FF_ERR_CUDA = 1, FF_ERR_ARG = 2, &
                                FF_ERR_TIMEOUT = 3, FF_ERR_SIZE = 4
   integer(c_int), parameter :: FF_BC_CON = 1, FF_BC_INL = 3, FF_BC_MIR = 4, &
                                FF_BC_OUT = 5, FF_BC_SOL = 8
+  ! ff_params%flux (enum ff_flux): a host with IFLUX sets
+  ! flux = merge(FF_FLUX_ROE, merge(FF_FLUX_VANLEER, IFLUX, IFLUX == 0), IFLUX == 1)
+  integer(c_int), parameter :: FF_FLUX_ROE = 0, FF_FLUX_VANLEER = 1, FF_FLUX_WPS = 2, &
+                               FF_FLUX_AUSM = 3, FF_FLUX_KT = 7, FF_FLUX_HCUSP = 8
 
   ! ICON(IC9,L) columns of one patch (charac.f:182) and its boundary values
   type, bind(C) :: ff_patch
@@ -64,10 +68,11 @@ module finflo_gpu
     integer(c_int) :: lusgs_fp32
     integer(c_int) :: ddadi
     integer(c_int) :: timel
-    integer(c_int) :: vanleer
+    integer(c_int) :: flux
     real(c_double) :: dt
     integer(c_int) :: predgs_full
     integer(c_int) :: res_fp32
+    integer(c_int) :: xxtral
   end type ff_params
 
   ! slot indices (enum ff_slot, include/finflo_types.h)

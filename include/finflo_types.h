@@ -40,6 +40,20 @@ typedef struct ff_patch {
   double bounrk, bounep;
 } ff_patch;
 
+/* ff_params.flux: the inviscid face flux (IFLUX, FLUXME multi.f:3567).
+ * Zero is the reference's default, Roe; the others carry IFLUX's own number,
+ * except van Leer (IFLUX = 0), which takes the 1 that Roe leaves free.
+ * Van Leer, WPS and AUSM have no two-equation form (FLUCYC res3c.f:7890-7960
+ * calls them, RESIKE res3c.f:6946-7030 does not). */
+enum ff_flux {
+  FF_FLUX_ROE = 0,       /* IFLUX = 1: FLUXKE base3c.f:4753           */
+  FF_FLUX_VANLEER = 1,   /* IFLUX = 0: FLUXVL base3c.f:1733, laminar  */
+  FF_FLUX_WPS = 2,       /* IFLUX = 2: FLUXWP base3c.f:1967, laminar  */
+  FF_FLUX_AUSM = 3,      /* IFLUX = 3: FLUXAU base3c.f:2201, laminar  */
+  FF_FLUX_KT = 7,        /* IFLUX = 7: FLUXKT base3c.f:4403           */
+  FF_FLUX_HCUSP = 8      /* IFLUX = 8: FLUCUSP base3c.f:5133          */
+};
+
 /* Flow, gas and solver constants (defaults: main.f:5234-5440, 3499, 3827). */
 typedef struct ff_params {
   double gamma, rgas, pr, prt;          /* 1.4, 287.05287, 0.72, 0.9          */
@@ -68,17 +82,20 @@ typedef struct ff_params {
                                         /* 0: LU-SGS (LUSGS=1, imps3.f:378)    */
   int timel;                            /* 1: time-accurate dual time stepping */
                                         /* (TIMEL, level 1 of the block only)  */
-  int vanleer;                          /* 1: van Leer FVS (IFLUX=0, laminar), */
-                                        /* 0: Roe (IFLUX=1)                    */
+  int flux;                             /* inviscid face flux, ff_flux below   */
+                                        /* (IFLUX of the reference)            */
   double dt;                            /* physical time step DT (TIMEL)       */
   int predgs_full;                      /* 1: the LU-SGS lower sweep (PREDGS)  */
                                         /* keeps the i+1 coupling in row JMAX  */
                                         /* that imps4.f:1460-1466 drops (its   */
                                         /* shift loop starts one index late);  */
                                         /* 0: the reference's sweep            */
-  int res_fp32;                         /* 1 on a coarse level: its face      */
+  int res_fp32;                         /* 1 on a coarse level: its Roe face  */
                                         /* fluxes in FP32 (sums, update and   */
                                         /* norms FP64); ignored on level 1    */
+  int xxtral;                           /* XXTRAL: MUSCL weighted by the cell */
+                                        /* extents D1..D3 (XXTRAA) for Roe,   */
+                                        /* KT and H-CUSP                      */
 } ff_params;
 
 /* Per-cell array slots of one block (names are the reference's MAIN_ARRAYS,

@@ -459,20 +459,60 @@ static void xxtrap(double r0, double r1, double r2, double r3, int intem, double
   }
 }
 
+/* XXTRAA base3c.f:1444-1570 (INCHIML false): XXTRAP with the cells' extents
+ * along the face normal, d0..d3 = D(I-KL), D(I-IL), D(I), D(I+IL) (D1/D2/D3
+ * of the direction): the differences become slopes over the centre
+ * distances and the half extents scale the extrapolation.  FLUXKE, FLUXKT
+ * and FLUCUSP call it in place of XXTRAP when XXTRAL is set. */
+static void xxtraa(double r0, double r1, double r2, double r3, double d0, double d1, double d2, double d3,
+                   int intem, double *rip, double *rim) {
+  static const double rkk1[5] = {0., 1., 1.3333333, 2., 1.5};
+  const double eps = 1.e-10;
+  int inter = abs(intem);
+  int inte2 = inter < 1 ? 1 : (inter > 5 ? 5 : inter);
+  double rk1 = rkk1[inte2 - 1], rk2 = 2. - rk1;
+  if (intem <= 0 && intem >= -5) {
+    double dxl = .5 * d1, dxr = .5 * d2;
+    double dx0 = 1. / (d0 + d1 + eps), dx1 = 1. / (d1 + d2 + eps), dx2 = 1. / (d2 + d3 + eps);
+    *rip = r2 - dxr * (dx1 * (r2 - r1) * rk1 + dx2 * (r3 - r2) * rk2);
+    *rim = r1 + dxl * (dx1 * (r2 - r1) * rk1 + dx0 * (r1 - r0) * rk2);
+  } else if (inter <= 4) {
+    double dxl = .5 * d1, dxr = .5 * d2;
+    double dx0 = 1. / (d0 + d1 + eps), dx1 = 1. / (d1 + d2 + eps), dx2 = 1. / (d2 + d3 + eps);
+    double diff0 = dx0 * (r1 - r0), diff1 = dx1 * (r2 - r1), diff2 = dx2 * (r3 - r2);
+    double diff12 = diff1 * diff1 + eps;
+    double phibi = (diff12 + diff1 * diff0) / (diff12 + diff0 * diff0);
+    double phifi = (diff12 + diff1 * diff2) / (diff12 + diff2 * diff2);
+    *rip = r2 - dxr * phifi * (diff1 * rk1 + diff2 * rk2);
+    *rim = r1 + dxl * phibi * (diff1 * rk1 + diff0 * rk2);
+  } else {
+    *rip = r2;
+    *rim = r1;
+  }
+}
+
+/* The MUSCL pair of one variable, q[0..3] = cells I-2S..I+S: XXTRAP, or
+ * XXTRAA with the cells' extents dd[0..3] when dd is given (XXTRAL). */
+static void xxm(const double *q, const double *dd, int intem, double *ip, double *im) {
+  if (dd) xxtraa(q[0], q[1], q[2], q[3], dd[0], dd[1], dd[2], dd[3], intem, ip, im);
+  else xxtrap(q[0], q[1], q[2], q[3], intem, ip, im);
+}
+
 /* One face of FLUXKE base3c.f:4753-5120 (laminar: k = eps = 0, UROT = 0),
  * with EFPRO state.f:620 (perfect gas) and DERIV base3c.f:707.
  * q[v][m]: v = ro,u,v,w,p ; m = 0..3 -> cells I-2S, I-S, I, I+S.
  * cr/cl = {C, DRDP, DRDH, RO, P} of cell I and of cell I2 (DERIV).
+ * dd: the cells' extents for XXTRAA (XXTRAL), or NULL for XXTRAP.
  * Adds the 5 flux components to f5[]. */
 static void roe_face_core(const double q[5][4], const double *nrm, double area, int intem,
                           const ff_params *p, double c_r, double c_l, const double *cr,
-                          const double *cl2, double *f5) {
+                          const double *cl2, const double *dd, double *f5) {
   double roip, roim, rmip, rmim, rnip, rnim, rwip, rwim, ppi, pmi;
-  xxtrap(q[0][0], q[0][1], q[0][2], q[0][3], intem, &roip, &roim);
-  xxtrap(q[1][0], q[1][1], q[1][2], q[1][3], intem, &rmip, &rmim);
-  xxtrap(q[2][0], q[2][1], q[2][2], q[2][3], intem, &rnip, &rnim);
-  xxtrap(q[3][0], q[3][1], q[3][2], q[3][3], intem, &rwip, &rwim);
-  xxtrap(q[4][0], q[4][1], q[4][2], q[4][3], intem, &ppi, &pmi);
+  xxm(q[0], dd, intem, &roip, &roim);
+  xxm(q[1], dd, intem, &rmip, &rmim);
+  xxm(q[2], dd, intem, &rnip, &rnim);
+  xxm(q[3], dd, intem, &rwip, &rwim);
+  xxm(q[4], dd, intem, &ppi, &pmi);
   roip = MAXD(0.001 * p->frsden, roip);
   ppi = MAXD(0.001 * p->frspre, ppi);
   roim = MAXD(0.001 * p->frsden, roim);
@@ -578,7 +618,7 @@ void orc_roe_face(const double *qr, const double *ql, const double *qrr, const d
                   const double *cell_r, const double *cell_l, int kquirk, double *f5) {
   double q[5][4];
   for (int v = 0; v < 5; v++) { q[v][0] = qll[v]; q[v][1] = ql[v]; q[v][2] = qr[v]; q[v][3] = qrr[v]; }
-  roe_face_core(q, nrm, area, intem, p, cell_r[0], cell_l[0], cell_r, kquirk ? cell_r : cell_l, f5);
+  roe_face_core(q, nrm, area, intem, p, cell_r[0], cell_l[0], cell_r, kquirk ? cell_r : cell_l, NULL, f5);
 }
 
 /* FLUXBL base3c.f:4085 (IDIFF=1) for the face between L-S and L. */
@@ -717,7 +757,9 @@ static void botske_face(const orc_block *b, const ff_params *p, size_t II, int S
   double vvi1 = idir * (V[II] - vsurf) * 6.;
   double wvi1 = idir * (W[II] - wsurf) * 6.;
   double pb4 = MAXD(-.99 * p->frspre, rc1 * b->a[FF_PDIFF][II] - rc2 * b->a[FF_PDIFF][II2]);
-  double pb = 1. * pb1 + 0. * pb4;                /* YP1=1, YP4=0 for IFLUX=1 */
+  /* YP1, YP4 (base3c.f:6304-6315): the pressure difference for KT (IFLUX=7) */
+  const double yp1 = p->flux == FF_FLUX_KT ? 0. : 1., yp4 = 1. - yp1;
+  double pb = yp1 * pb1 + yp4 * pb4;
   double alpha = 1.;
   double cvii = (1. - alpha) * cvi1 + alpha * cvi2;
   double uvii = (1. - alpha) * uvi1 + alpha * uvi2;
@@ -743,9 +785,12 @@ static void botske_face(const orc_block *b, const ff_params *p, size_t II, int S
  * ghosts (done by the caller), viscous flux, Roe flux, wall faces. */
 /* FLUXVL base3c.f:1733-1961 (IFLUX=0) for one face: van Leer flux-vector
  * splitting of the MUSCL-extrapolated conservative variables (cells
- * I-2S..I+S in qc[v][m], v = RO, RM, RN, RW, E), added to f (perfect gas). */
+ * I-2S..I+S in qc[v][m], v = RO, RM, RN, RW, E), added to f (perfect gas).
+ * wps = 1: FLUXWP base3c.f:1967-2195 (IFLUX=2), the same routine with the
+ * wave/particle split of the subsonic momentum and energy fluxes
+ * (base3c.f:2118-2125, 2156-2163). */
 static void vl_face(const double qc[5][4], const double *nrm, double area, int intem, const ff_params *p,
-                    double *f) {
+                    int wps, double *f) {
   const double gamma = p->gamma, gm1 = gamma - 1., ygm = 1. / gamma;
   double ip[5], im[5];
   for (int v = 0; v < 5; v++) xxtrap(qc[v][0], qc[v][1], qc[v][2], qc[v][3], intem, &ip[v], &im[v]);
@@ -772,8 +817,15 @@ static void vl_face(const double qc[5][4], const double *nrm, double area, int i
     } else if (rma < 1.) {
       double h = .5 * (rma - 1.);
       double f1 = -area * ip[0] * c * (h * h);
-      fm[0] = f1; fm[1] = f1 * (gm1 * u - 2. * c) * ygm; fm[2] = f1 * v; fm[3] = f1 * w;
-      fm[4] = f1 * (ip[4] + pp) * ypro;
+      fm[0] = f1; fm[2] = f1 * v; fm[3] = f1 * w;
+      if (wps) {
+        double rma2 = .25 * ((rma - 1.) * (rma - 1.)) * (2. + rma);
+        fm[1] = f1 * u + area * pp * rma2;
+        fm[4] = f1 * ip[4] * ypro + area * u * pp * rma2;
+      } else {
+        fm[1] = f1 * (gm1 * u - 2. * c) * ygm;
+        fm[4] = f1 * (ip[4] + pp) * ypro;
+      }
     } else {
       fm[0] = fm[1] = fm[2] = fm[3] = fm[4] = 0.;
     }
@@ -787,8 +839,15 @@ static void vl_face(const double qc[5][4], const double *nrm, double area, int i
     } else if (rma > -1.) {
       double h = .5 * (rma + 1.);
       double f1 = +area * im[0] * c * (h * h);
-      fp[0] = f1; fp[1] = f1 * (gm1 * u + 2. * c) * ygm; fp[2] = f1 * v; fp[3] = f1 * w;
-      fp[4] = f1 * (im[4] + pm) * ypro;
+      fp[0] = f1; fp[2] = f1 * v; fp[3] = f1 * w;
+      if (wps) {
+        double rma2 = .25 * ((rma + 1.) * (rma + 1.)) * (2. - rma);
+        fp[1] = f1 * u + area * pm * rma2;
+        fp[4] = f1 * im[4] * ypro + area * u * pm * rma2;
+      } else {
+        fp[1] = f1 * (gm1 * u + 2. * c) * ygm;
+        fp[4] = f1 * (im[4] + pm) * ypro;
+      }
     } else {
       fp[0] = fp[1] = fp[2] = fp[3] = fp[4] = 0.;
     }
@@ -800,6 +859,8 @@ static void vl_face(const double qc[5][4], const double *nrm, double area, int i
   f[3] = a13 * f2 + a23 * f3 + a33 * f4 + f[3];
   f[4] = fm[4] + fp[4] + f[4];
 }
+
+#include "finflo_oracle_flux.c"
 
 void orc_flux_dir(orc_block *b, const ff_params *p, int dir, int level) {
   dims_t d = dims_of(b);
@@ -835,16 +896,11 @@ void orc_flux_dir(orc_block *b, const ff_params *p, int dir, int level) {
         double cr[5] = {C[L], DRDP[L], DRDH[L], RO[L], P[L]};
         size_t L2 = dir == 3 ? L : L - S;      /* DERIV I2 = I-IL, or I itself */
         double cl[5] = {C[L2], DRDP[L2], DRDH[L2], RO[L2], P[L2]};
-        if (p->vanleer) {   /* IFLUX=0: FLUXVL on the conservative variables */
-          const double *cons[5] = {RO, b->a[FF_RM], b->a[FF_RN], b->a[FF_RW], b->a[FF_E]};
-          double qc[5][4];
-          for (int v = 0; v < 5; v++) {
-            qc[v][0] = cons[v][L - 2 * S]; qc[v][1] = cons[v][L - S];
-            qc[v][2] = cons[v][L]; qc[v][3] = cons[v][L + S];
-          }
-          vl_face(qc, nrm, A[L], intem, p, f);
+        if (p->flux != FF_FLUX_ROE) {   /* the other IFLUX schemes */
+          alt_face(b, p, dir, L, S, intem, 1, 5, f);
         } else {
-          roe_face_core(q, nrm, A[L], intem, p, C[L], C[L - S], cr, cl, f);
+          double dd[4];
+          roe_face_core(q, nrm, A[L], intem, p, C[L], C[L - S], cr, cl, stencil_d(b, p, dir, L, S, dd), f);
         }
         for (int v = 0; v < 5; v++) F[v][L] = f[v];
       }

@@ -248,15 +248,16 @@ static void flkebl_face(const orc_block *b, size_t I, int S, int dir, double *fr
  * q[v][m]: v = ro,u,v,w,p,rk,reps; m = cells I-2S..I+S.  Adds 7 fluxes. */
 static void roe_face_ke(const double q[7][4], const double *nrm, double area, int intem, int intet,
                         const ff_params *p, double c_r, double c_l, const double *cr,
-                        const double *cl2, double *f7) {
+                        const double *cl2, const double *dd, double *f7) {
   double roip, roim, rmip, rmim, rnip, rnim, rwip, rwim, ppi, pmi, rkip, rkim, reip, reim;
-  xxtrap(q[0][0], q[0][1], q[0][2], q[0][3], intem, &roip, &roim);
-  xxtrap(q[1][0], q[1][1], q[1][2], q[1][3], intem, &rmip, &rmim);
-  xxtrap(q[2][0], q[2][1], q[2][2], q[2][3], intem, &rnip, &rnim);
-  xxtrap(q[3][0], q[3][1], q[3][2], q[3][3], intem, &rwip, &rwim);
-  xxtrap(q[4][0], q[4][1], q[4][2], q[4][3], intem, &ppi, &pmi);
-  xxtrap(q[5][0], q[5][1], q[5][2], q[5][3], intet, &rkip, &rkim);
-  xxtrap(q[6][0], q[6][1], q[6][2], q[6][3], intet, &reip, &reim);
+  xxm(q[0], dd, intem, &roip, &roim);
+  xxm(q[1], dd, intem, &rmip, &rmim);
+  xxm(q[2], dd, intem, &rnip, &rnim);
+  xxm(q[3], dd, intem, &rwip, &rwim);
+  xxm(q[4], dd, intem, &ppi, &pmi);
+  /* XXTRAA takes INTEM for k and omega too (base3c.f:4861-4862) */
+  xxm(q[5], dd, dd ? intem : intet, &rkip, &rkim);
+  xxm(q[6], dd, dd ? intem : intet, &reip, &reim);
   roip = MAXD(0.001 * p->frsden, roip);
   ppi = MAXD(0.001 * p->frspre, ppi);
   roim = MAXD(0.001 * p->frsden, roim);
@@ -424,7 +425,9 @@ static void botske_face_ke(const orc_block *b, const ff_params *p, size_t II, in
   double vvi1 = idir * (V[II] - vsurf) * 6.;
   double wvi1 = idir * (W[II] - wsurf) * 6.;
   double pb4 = MAXD(-.99 * p->frspre, rc1 * b->a[FF_PDIFF][II] - rc2 * b->a[FF_PDIFF][II2]);
-  double pb = 1. * pb1 + 0. * pb4;
+  /* YP1, YP4 (base3c.f:6304-6315): the pressure difference for KT (IFLUX=7) */
+  const double yp1 = p->flux == FF_FLUX_KT ? 0. : 1., yp4 = 1. - yp1;
+  double pb = yp1 * pb1 + yp4 * pb4;
   double alpha = 1.;
   double cvii = (1. - alpha) * cvi1 + alpha * cvi2;
   double uvii = (1. - alpha) * uvi1 + alpha * uvi2;
@@ -494,7 +497,11 @@ void orc_flux_dir_sst(orc_block *b, const ff_params *p, int dir) {
         double cr[5] = {C[L], DRDP[L], DRDH[L], RO[L], P[L]};
         size_t L2 = dir == 3 ? L : L - S;
         double cl[5] = {C[L2], DRDP[L2], DRDH[L2], RO[L2], P[L2]};
-        roe_face_ke(q, nrm, A[L], intem, intet, p, C[L], C[L - S], cr, cl, f);
+        if (p->flux != FF_FLUX_ROE) alt_face(b, p, dir, L, S, intem, intet, 7, f);   /* IFLUX 7, 8 */
+        else {
+          double dd[4];
+          roe_face_ke(q, nrm, A[L], intem, intet, p, C[L], C[L - S], cr, cl, stencil_d(b, p, dir, L, S, dd), f);
+        }
         for (int v = 0; v < 7; v++) F[v][L] = f[v];
       }
   for (int ip = 0; ip < b->npatch; ip++) {
@@ -630,7 +637,11 @@ static void flux_dir_sst_coarse(orc_block *b, const ff_params *p, int dir) {
         double cr[5] = {C[L], DRDP[L], DRDH[L], RO[L], P[L]};
         size_t L2 = dir == 3 ? L : L - S;
         double cl[5] = {C[L2], DRDP[L2], DRDH[L2], RO[L2], P[L2]};
-        roe_face_ke(q, nrm, A[L], intem, intet, p, C[L], C[L - S], cr, cl, f);
+        if (p->flux != FF_FLUX_ROE) alt_face(b, p, dir, L, S, intem, intet, 7, f);   /* IFLUX 7, 8 */
+        else {
+          double dd[4];
+          roe_face_ke(q, nrm, A[L], intem, intet, p, C[L], C[L - S], cr, cl, stencil_d(b, p, dir, L, S, dd), f);
+        }
         for (int v = 0; v < 7; v++) F[v][L] = f[v];
       }
   for (int ip = 0; ip < b->npatch; ip++) {

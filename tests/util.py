@@ -47,6 +47,16 @@ def flux_scale_sst(o, blk):
     return out
 
 
+def momentum_floor(S):
+    """Schemes whose momentum fluxes carry PDIFF rather than P (AUSM, KT): in
+    a near-uniform field a cell's face fluxes of one momentum component can
+    all vanish, and its S with them.  The three momentum components then
+    share a floor of 1e-3 of the largest momentum scale in the block
+    (hist_close does the same for the residual norms)."""
+    fl = 1e-3 * max(S[m].max() for m in ("DM", "DN", "DW"))
+    return {n: (np.maximum(v, fl) if n in ("DM", "DN", "DW") else v) for n, v in S.items()}
+
+
 def make_pair(ni=17, nj=9, nk=9, **kw):
     bg, prm, fs = case.bump_case(ni, nj, nk, **kw)
     bc, _, _ = case.bump_case(ni, nj, nk, **kw)
