@@ -43,7 +43,7 @@ class FFParams(ctypes.Structure):
             "interi", "interj", "interk", "entropy_fix", "iturb", "fullns",
             "idi1", "idi2", "idi3", "coarse_inter", "lusgs_fp32", "ddadi", "timel", "flux")] + [
         ("dt", ctypes.c_double), ("predgs_full", ctypes.c_int), ("res_fp32", ctypes.c_int),
-        ("xxtral", ctypes.c_int)]
+        ("xxtral", ctypes.c_int), ("rjk2", ctypes.c_double), ("rjk4", ctypes.c_double)]
 
 
 class FFHaloItem(ctypes.Structure):
@@ -67,7 +67,8 @@ SLOTS = ["RO", "RM", "RN", "RW", "E", "P", "PDIFF", "U", "V", "W", "C",
          "DKDX", "DKDY", "DKDZ", "DEDX", "DEDY", "DEDZ",
          "RKOLD", "EPSOLD", "F1RK", "F1EPS", "RKP2H", "EPP2H",
          "ROLE2", "RMLE2", "RNLE2", "RWLE2", "ELE2", "RKLE2", "EPSLE2",
-         "ROLE3", "RMLE3", "RNLE3", "RWLE3", "ELE3", "RKLE3", "EPSLE3"]
+         "ROLE3", "RMLE3", "RNLE3", "RWLE3", "ELE3", "RKLE3", "EPSLE3",
+         "SCALEJ"]
 SLOT = {n: i for i, n in enumerate(SLOTS)}
 STATE_SLOTS = SLOTS[:19]
 METRIC_SLOTS = list(grid.METRIC_NAMES)

@@ -258,9 +258,19 @@ void launch_residual(cudaStream_t st, const BlockCtx* b, int level) {
 // part: 0 the whole stage, 1 the kernels before the residual's face pass
 // (gradients, sources, ghost updates), 2 the kernels after it -- so that a
 // multi-block cycle can run the face pass of all blocks in one launch.
+// SCALARD res3c.f:146, 3599: the JAMESON scale, first in the stage, before
+// the inlet/outlet ghost update (finest level, RJK2 or RJK4 > 0).
+static void launch_scalard(Ctx* c, BlockCtx* b, int level) {
+  if (level != 1 || !(b->prm.rjk2 > 0. || b->prm.rjk4 > 0.)) return;
+  const long n = (long)(b->imax + 2) * (b->jmax + 2) * (b->kmax + 2);
+  k_scalard<<<nblk(n, 256), 256, 0, c->stream>>>(b->db);
+  c->nlaunch++;
+}
+
 int st_residu_sst(Ctx* c, BlockCtx* b, int level, int m2, int icycle, int part = 0) {
   if (part == 2) goto post;
   {
+  launch_scalard(c, b, level);
   const int ncell = b->imax * b->jmax * b->kmax;
   int gg = level == 1 ? 2 : 0;
   long ng = (long)(b->imax + gg) * (b->jmax + gg) * (b->kmax + gg);
@@ -312,6 +322,7 @@ post:
 int st_residu(Ctx* c, BlockCtx* b, int level, int icycle, int m2 = 1, int part = 0) {
   if (b->prm.iturb >= 3) return st_residu_sst(c, b, level, m2, icycle, part);
   if (part != 2) {
+    launch_scalard(c, b, level);
     if (level == 1) {
       if (b->npatch) {
         int maxn = 1;

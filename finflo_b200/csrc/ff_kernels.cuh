@@ -574,6 +574,59 @@ FF_DI void vl_flux(const double qc[5][4], double nx, double ny, double nz, doubl
 
 #include "ff_fluxes.cuh"
 
+// JAMESON base3c.f:2827-3019 (IPRESC = 0) at face L (cells L-S | L): the
+// pressure sensors of the two cells (second differences of PDIFF), EPS2 =
+// RJK2 * their max, EPS4 = max(0, RJK4 - EPS2), SCALEJ averaged to the face;
+// the second- and fourth-difference dissipation of RO, RM, RN, RW, E taken
+// off f.  Added to Roe's flux on the finest level when RJK2 or RJK4 > 0
+// (FLUCYC res3c.f:7899-7906, RESIKE 6955-6962); k and omega keep theirs.
+FF_DI void jst_flux(const DevBlock& b, const ff_params& p, size_t L, int S, double* f) {
+  const double* PD = b.a[FF_PDIFF];
+  const double pd0 = __ldg(PD + L - 2 * S), pd1 = __ldg(PD + L - S), pd2 = __ldg(PD + L), pd3 = __ldg(PD + L + S);
+  const double fp4 = 4. * p.frspre;
+  const double pres1 = fabs(pd2 - 2. * pd1 + pd0) / (pd2 + 2. * pd1 + pd0 + fp4);
+  const double pres2 = fabs(pd3 - 2. * pd2 + pd1) / (pd3 + 2. * pd2 + pd1 + fp4);
+  const double eps2 = p.rjk2 * dmax(pres1, pres2), eps4 = dmax(0., p.rjk4 - eps2);
+  const double rlami = .5 * (__ldg(b.a[FF_SCALEJ] + L) + __ldg(b.a[FF_SCALEJ] + L - S));
+  const int sl[5] = {FF_RO, FF_RM, FF_RN, FF_RW, FF_E};
+#pragma unroll
+  for (int v = 0; v < 5; v++) {
+    const double* q = b.a[sl[v]];
+    const double q0 = __ldg(q + L - 2 * S), q1 = __ldg(q + L - S), q2 = __ldg(q + L), q3 = __ldg(q + L + S);
+    f[v] = -(rlami * (eps2 * (q2 - q1) - eps4 * (q3 - 3. * q2 + 3. * q1 - q0))) + f[v];
+  }
+}
+
+// SCALARD base3c.f:6-78 (IPRESC = 0, no grid rotation): SCALEJ of cells
+// 0..MAX+1 in each direction, |(U,V,W) . mean face vectors| + C * the mean
+// face areas; the JAMESON dissipation scale.
+__global__ void k_scalard(DevBlock b) {
+  const int ni = b.imax + 2, nj = b.jmax + 2;
+  const long n = (long)ni * nj * (b.kmax + 2);
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int I = t % ni, J = (t / ni) % nj, K = t / ((long)ni * nj);
+  const size_t kk = ix(b, I, J, K), is = b.is, il = b.il;
+#define LD(s, n) __ldg(b.a[s] + (n))
+  const double a1 = LD(FF_A1, kk), a1p = LD(FF_A1, kk + 1), a2 = LD(FF_A2, kk), a2p = LD(FF_A2, kk + is);
+  const double a3 = LD(FF_A3, kk), a3p = LD(FF_A3, kk + il);
+  const double a1k = .5 * (a1 + a1p), a2k = .5 * (a2 + a2p), a3k = .5 * (a3 + a3p);
+  const double a1xk = .5 * (LD(FF_A1XA, kk) * a1 + LD(FF_A1XA, kk + 1) * a1p);
+  const double a1yk = .5 * (LD(FF_A1YA, kk) * a1 + LD(FF_A1YA, kk + 1) * a1p);
+  const double a1zk = .5 * (LD(FF_A1ZA, kk) * a1 + LD(FF_A1ZA, kk + 1) * a1p);
+  const double a2xk = .5 * (LD(FF_A2XA, kk) * a2 + LD(FF_A2XA, kk + is) * a2p);
+  const double a2yk = .5 * (LD(FF_A2YA, kk) * a2 + LD(FF_A2YA, kk + is) * a2p);
+  const double a2zk = .5 * (LD(FF_A2ZA, kk) * a2 + LD(FF_A2ZA, kk + is) * a2p);
+  const double a3xk = .5 * (LD(FF_A3XA, kk) * a3 + LD(FF_A3XA, kk + il) * a3p);
+  const double a3yk = .5 * (LD(FF_A3YA, kk) * a3 + LD(FF_A3YA, kk + il) * a3p);
+  const double a3zk = .5 * (LD(FF_A3ZA, kk) * a3 + LD(FF_A3ZA, kk + il) * a3p);
+  const double u = LD(FF_U, kk), v = LD(FF_V, kk), w = LD(FF_W, kk);
+  const double ucii = a1xk * u + a1yk * v + a1zk * w, vcii = a2xk * u + a2yk * v + a2zk * w;
+  const double wcii = a3xk * u + a3yk * v + a3zk * w;
+  b.a[FF_SCALEJ][kk] = sqrt(ucii * ucii + vcii * vcii + wcii * wcii) + (a1k + a2k + a3k) * LD(FF_C, kk);
+#undef LD
+}
+
 // sq (optional): RO, U, V, W, P of cell L in a staged stencil, variable v
 // at sq[v * vs], the cells along the face normal es apart.  T = float: a
 // coarse level's face in FP32 (loads converted, fluxes in FP32).
@@ -642,8 +695,12 @@ FF_DI void face_flux(const DevBlock& b, const ff_params& p, int dir, size_t L, i
       roe_flux<double, true>(q, __ldg(b.a[FF_A1XA + ao] + L), __ldg(b.a[FF_A1YA + ao] + L),
                              __ldg(b.a[FF_A1ZA + ao] + L), __ldg(b.a[FF_A1 + ao] + L), intem, p, __ldg(b.a[FF_C] + L),
                              __ldg(b.a[FF_C] + L - S), cr, cl, f, dd);
-      return;
+    } else {
+      roe_flux(q, __ldg(b.a[FF_A1XA + ao] + L), __ldg(b.a[FF_A1YA + ao] + L), __ldg(b.a[FF_A1ZA + ao] + L),
+               __ldg(b.a[FF_A1 + ao] + L), intem, p, __ldg(b.a[FF_C] + L), __ldg(b.a[FF_C] + L - S), cr, cl, f);
     }
+    if (level == 1 && (p.rjk2 > 0. || p.rjk4 > 0.)) jst_flux(b, p, L, S, f);
+    return;
   }
   roe_flux(q, T(__ldg(b.a[FF_A1XA + ao] + L)), T(__ldg(b.a[FF_A1YA + ao] + L)), T(__ldg(b.a[FF_A1ZA + ao] + L)),
            T(__ldg(b.a[FF_A1 + ao] + L)), intem, p, T(__ldg(b.a[FF_C] + L)), T(__ldg(b.a[FF_C] + L - S)), cr, cl, f);

@@ -505,6 +505,9 @@ FF_DI void face_flux_ke(const DevBlock& b, const ff_params& p, int dir, size_t L
     f[1] = fv[1] + f[1]; f[2] = fv[2] + f[2]; f[3] = fv[3] + f[3];
     f[4] = f4 + f[4]; f[5] = frk + f[5]; f[6] = feps + f[6];
   }
+  if constexpr (sizeof(T) == sizeof(double)) {   // JAMESON after the viscous and Roe fluxes
+    if (!alt && level == 1 && (p.rjk2 > 0. || p.rjk4 > 0.)) jst_flux(b, p, L, S, f);
+  }
 }
 
 // RESIKE face cycles + SWEEPK for a 32x4x4 tile (k, i, j, then 1/VOL).

@@ -22,7 +22,7 @@ module finflo_gpu
   use, intrinsic :: iso_c_binding
   implicit none
 
-  integer(c_int), parameter :: FF_ABI_VERSION = 6
+  integer(c_int), parameter :: FF_ABI_VERSION = 7
   integer(c_int), parameter :: FF_OK = 0, FF_ERR_CUDA = 1, FF_ERR_ARG = 2, &
                                FF_ERR_TIMEOUT = 3, FF_ERR_SIZE = 4
   integer(c_int), parameter :: FF_BC_CON = 1, FF_BC_INL = 3, FF_BC_MIR = 4, &
@@ -73,6 +73,7 @@ module finflo_gpu
     integer(c_int) :: predgs_full
     integer(c_int) :: res_fp32
     integer(c_int) :: xxtral
+    real(c_double) :: rjk2, rjk4
   end type ff_params
 
   ! slot indices (enum ff_slot, include/finflo_types.h)
@@ -83,7 +84,7 @@ module finflo_gpu
     FF_DRK = 24, FF_DEPS = 25, FF_DTL = 26, FF_TOLD = 27, FF_UOLD = 28, FF_VOLD = 29, &
     FF_WOLD = 30, FF_POLD = 31, FF_A1 = 32, FF_VOL = 44, FF_XC = 45, FF_D1 = 48, &
     FF_RK = 75, FF_REPS = 76, FF_DISTW = 77, FF_RKOLD = 88, FF_EPSOLD = 89, &
-    FF_ROLE2 = 94, FF_ROLE3 = 101, FF_NSLOTS = 108
+    FF_ROLE2 = 94, FF_ROLE3 = 101, FF_SCALEJ = 108, FF_NSLOTS = 109
 
   interface
     integer(c_int) function ff_abi_version() bind(C, name="ff_abi_version")

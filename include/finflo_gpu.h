@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define FF_ABI_VERSION 6   /* 6: ff_params.flux (ff_flux) replaces vanleer; 5: ff_wall_distance takes wall points */
+#define FF_ABI_VERSION 7   /* 7: ff_params.xxtral, rjk2, rjk4 and the FF_SCALEJ slot; 6: ff_params.flux (ff_flux) replaces vanleer */
 
 enum { FF_OK = 0, FF_ERR_CUDA = 1, FF_ERR_ARG = 2, FF_ERR_TIMEOUT = 3, FF_ERR_SIZE = 4 };
 enum { FF_STAGE_RESIDUAL = 1, FF_STAGE_GRAD = 2, FF_STAGE_STATE = 3, FF_STAGE_SWEEP = 4 };

@@ -96,6 +96,10 @@ typedef struct ff_params {
   int xxtral;                           /* XXTRAL: MUSCL weighted by the cell */
                                         /* extents D1..D3 (XXTRAA) for Roe,   */
                                         /* KT and H-CUSP                      */
+  double rjk2, rjk4;                    /* RJK2, RJK4: JAMESON's second- and  */
+                                        /* fourth-difference dissipation with */
+                                        /* Roe on the finest level (0, 0 off; */
+                                        /* main.f:5289-5290)                  */
 } ff_params;
 
 /* Per-cell array slots of one block (names are the reference's MAIN_ARRAYS,
@@ -132,6 +136,9 @@ enum ff_slot {
    * res3c.f:3175, NEWTIM ns3c.f:9420) */
   FF_ROLE2, FF_RMLE2, FF_RNLE2, FF_RWLE2, FF_ELE2, FF_RKLE2, FF_EPSLE2,
   FF_ROLE3, FF_RMLE3, FF_RNLE3, FF_RWLE3, FF_ELE3, FF_RKLE3, FF_EPSLE3,
+  /* SCALEJ: the spectral-radius scale of JAMESON's dissipation (SCALARD
+   * base3c.f:6; the finest level, when RJK2 or RJK4 > 0) */
+  FF_SCALEJ,
   FF_NSLOTS
 };
 

@@ -901,6 +901,7 @@ void orc_flux_dir(orc_block *b, const ff_params *p, int dir, int level) {
         } else {
           double dd[4];
           roe_face_core(q, nrm, A[L], intem, p, C[L], C[L - S], cr, cl, stencil_d(b, p, dir, L, S, dd), f);
+          if (level == 1 && (p->rjk2 > 0. || p->rjk4 > 0.)) jst_face(b, p, L, S, f);
         }
         for (int v = 0; v < 5; v++) F[v][L] = f[v];
       }
@@ -995,6 +996,7 @@ void orc_residu(orc_block *b, const ff_params *p, int level, int icycle) {
   for (int s = FF_DRO; s <= FF_DE; s++) memset(b->a[s], 0, sizeof(double) * d.ntot);
   for (int s = FF_W12; s <= FF_W23; s++) memset(b->a[s], 0, sizeof(double) * d.ntot);
   for (int s = FF_DTDX; s <= FF_DTDZ; s++) memset(b->a[s], 0, sizeof(double) * d.ntot);
+  if (level == 1 && (p->rjk2 > 0. || p->rjk4 > 0.)) orc_scalard(b);   /* res3c.f:146 */
   if (level == 1) orc_refcen(b, p);
   if (p->fullns && level == 1) orc_gradients(b, level);
   const int order[3] = {3, 1, 2};

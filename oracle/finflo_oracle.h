@@ -83,6 +83,9 @@ void orc_roe_face(const double *qr, const double *ql, const double *qrr, const d
                   const double *nrm, double area, int intem, const ff_params *p,
                   const double *cell_r, const double *cell_l, int kquirk, double *f5);
 
+/* SCALARD base3c.f:6: the JAMESON dissipation scale SCALEJ of cells 0..MAX+1 */
+void orc_scalard(orc_block *b);
+
 /* the reference's block set-up (finflo_oracle_grid.c) */
 void orc_grid_metrics(orc_block *b, const double *X, const double *Y, const double *Z);
 void orc_grid_lump(const orc_block *f, orc_block *c);

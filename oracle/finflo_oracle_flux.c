@@ -376,3 +376,63 @@ static void alt_face(const orc_block *b, const ff_params *p, int dir, size_t L, 
       return;
   }
 }
+
+/* SCALARD base3c.f:6-78 (IPRESC = 0, UROT = VROT = WROT = 0): SCALEJ of the
+ * cells 0..MAX+1 in each direction, |contravariant velocity| summed over the
+ * cell's mean face vectors plus C times the mean face areas. */
+void orc_scalard(orc_block *b) {
+  dims_t d = dims_of(b);
+  double *SJ = b->a[FF_SCALEJ];
+  memset(SJ, 0, sizeof(double) * d.ntot);
+  const double *A1 = b->a[FF_A1], *A2 = b->a[FF_A2], *A3 = b->a[FF_A3];
+  const double *A1X = b->a[FF_A1XA], *A1Y = b->a[FF_A1YA], *A1Z = b->a[FF_A1ZA];
+  const double *A2X = b->a[FF_A2XA], *A2Y = b->a[FF_A2YA], *A2Z = b->a[FF_A2ZA];
+  const double *A3X = b->a[FF_A3XA], *A3Y = b->a[FF_A3YA], *A3Z = b->a[FF_A3ZA];
+  const double *U = b->a[FF_U], *V = b->a[FF_V], *W = b->a[FF_W], *C = b->a[FF_C];
+  const int is = d.is, il = d.il;
+  for (int K = 0; K <= d.kmax + 1; K++)
+    for (int J = 0; J <= d.jmax + 1; J++)
+      for (int I = 0; I <= d.imax + 1; I++) {
+        size_t kk = IX(d, I, J, K);
+        double chat = C[kk];
+        double a1k = .5 * (A1[kk] + A1[kk + 1]);
+        double a2k = .5 * (A2[kk] + A2[kk + is]);
+        double a3k = .5 * (A3[kk] + A3[kk + il]);
+        double a1xk = .5 * (A1X[kk] * A1[kk] + A1X[kk + 1] * A1[kk + 1]);
+        double a1yk = .5 * (A1Y[kk] * A1[kk] + A1Y[kk + 1] * A1[kk + 1]);
+        double a1zk = .5 * (A1Z[kk] * A1[kk] + A1Z[kk + 1] * A1[kk + 1]);
+        double a2xk = .5 * (A2X[kk] * A2[kk] + A2X[kk + is] * A2[kk + is]);
+        double a2yk = .5 * (A2Y[kk] * A2[kk] + A2Y[kk + is] * A2[kk + is]);
+        double a2zk = .5 * (A2Z[kk] * A2[kk] + A2Z[kk + is] * A2[kk + is]);
+        double a3xk = .5 * (A3X[kk] * A3[kk] + A3X[kk + il] * A3[kk + il]);
+        double a3yk = .5 * (A3Y[kk] * A3[kk] + A3Y[kk + il] * A3[kk + il]);
+        double a3zk = .5 * (A3Z[kk] * A3[kk] + A3Z[kk + il] * A3[kk + il]);
+        double ucii = a1xk * U[kk] + a1yk * V[kk] + a1zk * W[kk] - 0.;
+        double vcii = a2xk * U[kk] + a2yk * V[kk] + a2zk * W[kk] - 0.;
+        double wcii = a3xk * U[kk] + a3yk * V[kk] + a3zk * W[kk] - 0.;
+        double ccii = (a1k + a2k + a3k) * chat;
+        SJ[kk] = sqrt(ucii * ucii + vcii * vcii + wcii * wcii) + ccii;
+      }
+}
+
+/* JAMESON base3c.f:2827-3019 (IPRESC = 0) at face L (cells L-S | L): the
+ * pressure sensors of the two cells (PDIFF second differences), EPS2 =
+ * RJK2 * max, EPS4 = max(0, RJK4 - EPS2), SCALEJ averaged to the face; the
+ * second- and fourth-difference dissipation of RO, RM, RN, RW, E subtracted
+ * from f.  FLUCYC and RESIKE add it to Roe's flux on the finest level
+ * (res3c.f:7899-7906, 6955-6962); k and omega keep theirs. */
+static void jst_face(const orc_block *b, const ff_params *p, size_t L, int S, double *f) {
+  const double *PD = b->a[FF_PDIFF], *SJ = b->a[FF_SCALEJ];
+  const double fp4 = 4. * p->frspre;
+  double pres1 = fabs(PD[L] - 2. * PD[L - S] + PD[L - 2 * S]) / (PD[L] + 2. * PD[L - S] + PD[L - 2 * S] + fp4);
+  double pres2 = fabs(PD[L + S] - 2. * PD[L] + PD[L - S]) / (PD[L + S] + 2. * PD[L] + PD[L - S] + fp4);
+  double eps2i = p->rjk2 * MAXD(pres1, pres2);
+  double eps4i = MAXD(0., (p->rjk4 - eps2i));
+  double rlami = .5 * (SJ[L] + SJ[L - S]);
+  const int sl[5] = {FF_RO, FF_RM, FF_RN, FF_RW, FF_E};
+  for (int v = 0; v < 5; v++) {
+    const double *Q = b->a[sl[v]];
+    double fj = rlami * (eps2i * (Q[L] - Q[L - S]) - eps4i * (Q[L + S] - 3. * Q[L] + 3. * Q[L - S] - Q[L - 2 * S]));
+    f[v] = -fj + f[v];
+  }
+}

@@ -501,6 +501,7 @@ void orc_flux_dir_sst(orc_block *b, const ff_params *p, int dir) {
         else {
           double dd[4];
           roe_face_ke(q, nrm, A[L], intem, intet, p, C[L], C[L - S], cr, cl, stencil_d(b, p, dir, L, S, dd), f);
+          if (p->rjk2 > 0. || p->rjk4 > 0.) jst_face(b, p, L, S, f);   /* res3c.f:6955 */
         }
         for (int v = 0; v < 7; v++) F[v][L] = f[v];
       }
@@ -671,6 +672,7 @@ void orc_residu_sst_lev(orc_block *b, const ff_params *p, int lev, int m2, int i
   for (int s = FF_DRO; s <= FF_DEPS; s++) memset(b->a[s], 0, sizeof(double) * d.ntot);
   memset(b->a[FF_SRK], 0, sizeof(double) * d.ntot);
   memset(b->a[FF_FUN1], 0, sizeof(double) * d.ntot);
+  if (lev == 1 && (p->rjk2 > 0. || p->rjk4 > 0.)) orc_scalard(b);   /* res3c.f:3599 */
   if (m2 >= 2) {
     static const int z[] = {FF_OHMI, FF_W12, FF_W13, FF_W23, FF_DTDX, FF_DTDY, FF_DTDZ, FF_DKDX, FF_DKDY,
                             FF_DKDZ, FF_DEDX, FF_DEDY, FF_DEDZ, FF_S11, FF_S12, FF_S13, FF_S22, FF_S23, FF_S33};

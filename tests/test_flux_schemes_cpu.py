@@ -123,3 +123,47 @@ def test_xxtral_cycles_fall(flux):
     r = np.array([o.cycle(i + 1)[0][0] for i in range(60)])
     assert np.isfinite(r).all()
     assert r[-1] < 0.01 * r[0]
+
+
+@pytest.mark.parametrize("sst", [False, True])
+def test_jameson_dissipation_cycles(sst):
+    """JAMESON (base3c.f:2827; RJK2 = 1/2, RJK4 = 1/64) on Roe's flux of the
+    finest level: the residual of a uniform state stays Roe's (the
+    differences vanish), the cycles converge, and the dissipation changes
+    the residual of a disturbed state."""
+    kw = dict(turbulence="sst", reynolds=1e6, mach=0.5, h1=1e-4) if sst else {}
+    base, fs = None, None
+    out = []
+    for rj in ((0.0, 0.0), (0.5, 1.0 / 64)):
+        blk, prm, fs = case.bump_case(17, 9, 9, **kw)
+        prm.rjk2, prm.rjk4 = rj
+        o = Oracle(blk, prm)
+        o.start()
+        r = np.array([o.cycle(i + 1)[0][0] for i in range(60)])
+        assert np.isfinite(r).all()
+        assert r[-1] < 0.01 * r[0]
+        out.append(r)
+    assert abs(out[1][1] - out[0][1]) > 1e-6 * out[0][1]
+
+
+def test_jameson_keeps_the_free_stream():
+    """A uniform laminar state on the flat slip-wall channel: the residual
+    with JAMESON's dissipation is Roe's (every difference it takes is zero;
+    SCALEJ is not).  (In the k-omega form OUTLET's ghost E carries rho*k
+    once more than the interior's, so its last cells see a jump in E.)"""
+    out = []
+    for rj in ((0.0, 0.0), (0.5, 1.0 / 64)):
+        blk, prm, fs = case.bump_case(17, 9, 9, amp=0.0, noise=0.0)
+        for pa in blk.patches:
+            if pa.ityp == grid.BC_SOL:
+                pa.ityp = grid.BC_MIR
+        prm.idi1 = prm.idi2 = prm.idi3 = 0
+        prm.rjk2, prm.rjk4 = rj
+        r, S = _residual(blk, prm, scale=True)
+        out.append((r, S))
+        if rj[0] > 0:
+            assert np.abs(blk.arrays["SCALEJ"]).max() > 0
+    (r0, S), (r1, _) = out
+    S = momentum_floor(S)
+    for n in r0:
+        assert (np.abs(r1[n] - r0[n]) / (np.maximum(np.abs(r0[n]), S[n]) + 1e-300)).max() <= 1e-12, n

@@ -197,3 +197,47 @@ def test_xxtral_cycles_match_oracle(gpu_lib, sst):
     ref = np.array([o.cycle(i + 1)[0] for i in range(n)])
     hist_close(hist[:, :5], ref, 1e-8)
     g.close()
+
+
+@pytest.mark.parametrize("sst", [False, True])
+def test_jameson_residual(gpu_lib, sst):
+    """JAMESON's dissipation (RJK2 = 1/2, RJK4 = 1/64; SCALARD's SCALEJ) on
+    Roe's flux: the residual per cell after a few cycles, and SCALEJ."""
+    g, bid, bg, o, bc, prm = _setup("roe", **(SST if sst else {}))
+    prm.rjk2, prm.rjk4 = 0.5, 1.0 / 64
+    g.set_params(bid, prm)
+    for i in range(3):
+        o.cycle(i + 1)
+    g.cycles(3, bid, icycle0=1, use_graph=False)
+    d = g.download(bid)
+    for n, a in d.items():
+        bc.arrays[n][:] = a
+    if sst:
+        o.statim(); o.turbeq(); o.residu_sst(4)
+        g.statim(bid); g.residu(bid, 1, 4)
+    else:
+        o.statim(); o.adjuin(); o.residu(1, 4)
+        g.statim(bid); g.residu(bid, 1, 4)
+    g.sync()
+    names = RES7 if sst else RES
+    got_all = g.download(bid, list(names) + ["SCALEJ"])
+    a, b = interior(bg, got_all["SCALEJ"]), interior(bc, bc.arrays["SCALEJ"])
+    assert np.abs(a - b).max() <= 1e-13 * np.abs(b).max()
+    S = momentum_floor(flux_scale_sst(o, bc) if sst else flux_scale(o, bc))
+    for n in names:
+        ref = interior(bc, bc.arrays[n]); got = interior(bg, got_all[n])
+        err = (np.abs(got - ref) / (np.maximum(np.abs(ref), S[n]) + 1e-300)).max()
+        assert err <= 1e-12, (n, err)
+    g.close()
+
+
+@pytest.mark.parametrize("sst", [False, True])
+def test_jameson_cycles_match_oracle(gpu_lib, sst):
+    g, bid, bg, o, bc, prm = _setup("roe", **(SST if sst else {}))
+    prm.rjk2, prm.rjk4 = 0.5, 1.0 / 64
+    g.set_params(bid, prm)
+    n = 20
+    hist = g.cycles(n, bid, icycle0=1, use_graph=True)
+    ref = np.array([o.cycle(i + 1)[0] for i in range(n)])
+    hist_close(hist[:, :5], ref, 1e-8)
+    g.close()

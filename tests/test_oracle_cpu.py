@@ -192,7 +192,7 @@ def test_abi_exports_every_declared_symbol():
     assert sorted(fnames) == ["boundi_", "fin_", "impsdi_", "residi_", "statim_"]
     for n in names + fnames:
         assert hasattr(L, n), n
-    assert L.ff_abi_version() == 6
+    assert L.ff_abi_version() == 7
 
 
 def test_nn_abi_exports_every_declared_symbol():
