@@ -204,13 +204,13 @@ bool res_fused() {
   return f;
 }
 
-template <int NV, int NT, int I_, int J_, int K_, bool ST = false, typename FT = double>
+template <int NV, int NT, int I_, int J_, int K_, bool ST = false, typename FT = double, bool ALT = false>
 void launch_residual_fused_s(cudaStream_t st, const BlockCtx* b, int level) {
   dim3 g(nblk(b->imax, I_), nblk(b->jmax, J_), nblk(b->kmax, K_));
   const size_t sm = residual_fused_smem(NV, I_, J_, K_, ST);
-  cudaFuncSetAttribute(k_residual_fused<NV, NT, I_, J_, K_, ST, FT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)sm);
-  k_residual_fused<NV, NT, I_, J_, K_, ST, FT><<<g, NT, sm, st>>>(b->db, b->prm, level);
+  cudaFuncSetAttribute(k_residual_fused<NV, NT, I_, J_, K_, ST, FT, ALT>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k_residual_fused<NV, NT, I_, J_, K_, ST, FT, ALT><<<g, NT, sm, st>>>(b->db, b->prm, level);
 }
 
 template <int NV, int NT>
@@ -219,9 +219,11 @@ void launch_residual_fused_t(cudaStream_t st, dim3 g, const BlockCtx* b, int lev
   // the form the autotuner chose for this block (512 threads only): tile
   // shape, and the stencil staged in shared memory or not
   const int sh = NT == 512 ? b->res_shape : 0;
-  // a coarse level's face fluxes in FP32 (unstaged tiles; Roe with XXTRAP
-  // only: the other schemes and XXTRAA run their FP64 face code)
-  if (level > 1 && b->prm.res_fp32 && b->prm.flux == FF_FLUX_ROE && !b->prm.xxtral) {
+  // another IFLUX scheme, XXTRAA or JAMESON: the kernel with those variants
+  // compiled in, in the default 32x4x4 unstaged form
+  if (residual_alt(b->prm, level)) return launch_residual_fused_s<NV, NT, 32, 4, 4, false, double, true>(st, b, level);
+  // a coarse level's face fluxes in FP32 (unstaged tiles; Roe with XXTRAP)
+  if (level > 1 && b->prm.res_fp32) {
     const int s3 = sh % RES_NSHAPE;
     if (s3 == 1) return launch_residual_fused_s<NV, NT, 16, 8, 4, false, float>(st, b, level);
     if (s3 == 2) return launch_residual_fused_s<NV, NT, 8, 8, 8, false, float>(st, b, level);
@@ -406,7 +408,7 @@ bool res_batch_ok(Ctx* c) {
   const bool sst = c->tops[0]->prm.iturb >= 3;
   if (res_threads(sst) != 512) return false;
   for (auto* b : c->tops)
-    if ((b->prm.iturb >= 3) != sst) return false;
+    if ((b->prm.iturb >= 3) != sst || residual_alt(b->prm, 1)) return false;
   return true;
 }
 
@@ -558,7 +560,14 @@ int setup_lines(Ctx* c, BlockCtx* b) {
   lg.ntiles = lg.ntj * lg.ntk;
   const int nv = b->prm.iturb >= 3 ? 7 : 5;
   if (c->device < 0 || c->device >= kMaxDev) return fail(c, FF_ERR_ARG, "device id");
-  for (int cs = 16; cs >= 1; cs /= 2) {
+  // FINFLO_LINES_CS caps the cluster size (16 by default): smaller clusters
+  // let more blocks' sweeps run side by side in a multi-block cycle
+  static const int cs_max = [] {
+    const char* e = getenv("FINFLO_LINES_CS");
+    const int v = e ? atoi(e) : 16;
+    return (v == 1 || v == 2 || v == 4 || v == 8) ? v : 16;
+  }();
+  for (int cs = cs_max; cs >= 1; cs /= 2) {
     int csz = min(cs, lg.ntiles);
     int tpc = (lg.ntiles + csz - 1) / csz;
     int ng = min(tpc, LMAX_TPC);

@@ -630,7 +630,10 @@ __global__ void k_scalard(DevBlock b) {
 // sq (optional): RO, U, V, W, P of cell L in a staged stencil, variable v
 // at sq[v * vs], the cells along the face normal es apart.  T = float: a
 // coarse level's face in FP32 (loads converted, fluxes in FP32).
-template <typename T>
+// ALT = false compiles out the selectable variants (the other IFLUX schemes,
+// XXTRAA, JAMESON) for the residual kernels of the plain Roe/XXTRAP case:
+// their code would raise the register count of every face.
+template <typename T, bool ALT = true>
 FF_DI void face_flux(const DevBlock& b, const ff_params& p, int dir, size_t L, int m, int t1, int t2,
                      int level, T f[5], const double* sq = nullptr, int es = 0, int vs = 0) {
   const int S = dir == 1 ? 1 : (dir == 2 ? b.is : b.il);
@@ -661,7 +664,7 @@ FF_DI void face_flux(const DevBlock& b, const ff_params& p, int dir, size_t L, i
     f[0] = f[1] = f[2] = f[3] = f[4] = T(0.);
   }
   const int ao = 4 * (dir - 1);
-  if constexpr (sizeof(T) == sizeof(double)) {
+  if constexpr (ALT && sizeof(T) == sizeof(double)) {
     if (p.flux != FF_FLUX_ROE) {   // the other IFLUX schemes (FLUCYC res3c.f:7890-7990)
       alt_flux<5>(b, p, dir, L, S, intem, 1, f);
       return;
@@ -688,7 +691,7 @@ FF_DI void face_flux(const DevBlock& b, const ff_params& p, int dir, size_t L, i
   // RO and P of cell L2 (L itself for k faces) are in the stencil
   T cl[4] = {T(__ldg(b.a[FF_DRDP] + L2)), T(__ldg(b.a[FF_DRDH] + L2)), dir == 3 ? q[0][2] : q[0][1],
              dir == 3 ? q[4][2] : q[4][1]};
-  if constexpr (sizeof(T) == sizeof(double)) {
+  if constexpr (ALT && sizeof(T) == sizeof(double)) {
     if (p.xxtral) {   // XXTRAA over the cells' extents along the normal
       const double* D = b.a[FF_D1 + dir - 1];
       const double dd[4] = {__ldg(D + L - 2 * S), __ldg(D + L - S), __ldg(D + L), __ldg(D + L + S)};

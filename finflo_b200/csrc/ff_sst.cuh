@@ -412,7 +412,7 @@ FF_DI void wall_flux_ke(const DevBlock& b, const ff_params& p, size_t II, int S,
 // FLUXKE; BOTSKE on walls).
 // sq (optional): the seven MUSCL variables of cell L in a staged stencil,
 // variable v at sq[v * vs], the cells along the face normal es apart.
-template <typename T>
+template <typename T, bool ALT = true>
 FF_DI void face_flux_ke(const DevBlock& b, const ff_params& p, int dir, size_t L, int m, int t1, int t2,
                         int level, T f[7], const double* sq = nullptr, int es = 0, int vs = 0) {
   const int S = dir == 1 ? 1 : (dir == 2 ? b.is : b.il);
@@ -440,7 +440,7 @@ FF_DI void face_flux_ke(const DevBlock& b, const ff_params& p, int dir, size_t L
 #pragma unroll
   for (int v = 0; v < 7; v++) f[v] = T(0.);
   bool alt = false;
-  if constexpr (sizeof(T) == sizeof(double)) {
+  if constexpr (ALT && sizeof(T) == sizeof(double)) {
     if (p.flux != FF_FLUX_ROE) {   // KT or H-CUSP (RESIKE res3c.f:7017-7036)
       alt_flux<7>(b, p, dir, L, S, intem, intet, f);
       alt = true;
@@ -470,7 +470,7 @@ FF_DI void face_flux_ke(const DevBlock& b, const ff_params& p, int dir, size_t L
                dir == 3 ? q[4][2] : q[4][1]};
     const int ao = 4 * (dir - 1);
     bool done = false;
-    if constexpr (sizeof(T) == sizeof(double)) {
+    if constexpr (ALT && sizeof(T) == sizeof(double)) {
       if (p.xxtral) {   // XXTRAA over the cells' extents along the normal
         const double* D = b.a[FF_D1 + dir - 1];
         const double dd[4] = {__ldg(D + L - 2 * S), __ldg(D + L - S), __ldg(D + L), __ldg(D + L + S)};
@@ -505,7 +505,7 @@ FF_DI void face_flux_ke(const DevBlock& b, const ff_params& p, int dir, size_t L
     f[1] = fv[1] + f[1]; f[2] = fv[2] + f[2]; f[3] = fv[3] + f[3];
     f[4] = f4 + f[4]; f[5] = frk + f[5]; f[6] = feps + f[6];
   }
-  if constexpr (sizeof(T) == sizeof(double)) {   // JAMESON after the viscous and Roe fluxes
+  if constexpr (ALT && sizeof(T) == sizeof(double)) {   // JAMESON after the viscous and Roe fluxes
     if (!alt && level == 1 && (p.rjk2 > 0. || p.rjk4 > 0.)) jst_flux(b, p, L, S, f);
   }
 }
@@ -590,7 +590,7 @@ __global__ void __launch_bounds__(NT, RES_MIN_CTAS * 128 / NT) k_residual_sst(De
 //
 // FT = float: the face fluxes of a coarse level in FP32 (the cells' sums
 // of their faces and the result stay FP64).
-template <int NV, int NT, int TI_, int TJ_, int TK_, bool STAGE = false, typename FT = double>
+template <int NV, int NT, int TI_, int TJ_, int TK_, bool STAGE = false, typename FT = double, bool ALT = false>
 FF_DI void residual_tile(const DevBlock& b, const ff_params& p, int level, int i0, int j0, int k0,
                          double* res_smem) {
   constexpr int TI = TI_, TJ = TJ_, TK = TK_;
@@ -630,8 +630,8 @@ FF_DI void residual_tile(const DevBlock& b, const ff_params& p, int level, int i
       sq = sQ + ((fk + 2) * BJ + (fj + 2)) * BI + (fi + 2);
       es = dir == 1 ? 1 : (dir == 2 ? BI : BI * BJ);
     }
-    if constexpr (NV == 7) face_flux_ke(b, p, dir, ix(b, I, J, K), m, t1, t2, level, fl, sq, es, BOX);
-    else face_flux(b, p, dir, ix(b, I, J, K), m, t1, t2, level, fl, sq, es, BOX);
+    if constexpr (NV == 7) face_flux_ke<FT, ALT>(b, p, dir, ix(b, I, J, K), m, t1, t2, level, fl, sq, es, BOX);
+    else face_flux<FT, ALT>(b, p, dir, ix(b, I, J, K), m, t1, t2, level, fl, sq, es, BOX);
 #pragma unroll
     for (int v = 0; v < NV; v++) sF[v][f] = double(fl[v]);
   }
@@ -654,11 +654,19 @@ FF_DI void residual_tile(const DevBlock& b, const ff_params& p, int level, int i
   }
 }
 
-template <int NV, int NT, int TI_ = TI, int TJ_ = TJ, int TK_ = TK, bool STAGE = false, typename FT = double>
+// ALT: the selectable variants compiled in (the other IFLUX schemes, XXTRAA,
+// JAMESON); the plain Roe/XXTRAP forms leave them out.
+template <int NV, int NT, int TI_ = TI, int TJ_ = TJ, int TK_ = TK, bool STAGE = false, typename FT = double,
+          bool ALT = false>
 __global__ void __launch_bounds__(NT, RES_MIN_CTAS * 128 / NT) k_residual_fused(DevBlock b, ff_params p, int level) {
   extern __shared__ double res_smem[];
-  residual_tile<NV, NT, TI_, TJ_, TK_, STAGE, FT>(b, p, level, blockIdx.x * TI_, blockIdx.y * TJ_,
-                                                  blockIdx.z * TK_, res_smem);
+  residual_tile<NV, NT, TI_, TJ_, TK_, STAGE, FT, ALT>(b, p, level, blockIdx.x * TI_, blockIdx.y * TJ_,
+                                                       blockIdx.z * TK_, res_smem);
+}
+
+// Whether a block's residual on `level` needs the selectable variants.
+inline bool residual_alt(const ff_params& p, int level) {
+  return p.flux != FF_FLUX_ROE || p.xxtral || (level == 1 && (p.rjk2 > 0. || p.rjk4 > 0.));
 }
 
 // The same residual for several blocks in one launch: a block work-list of
