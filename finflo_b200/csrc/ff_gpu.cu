@@ -28,16 +28,21 @@ struct BlockCtx {
   ff_patch* d_patch = nullptr;
   std::vector<ff_patch> h_patch;
   ff_params prm{};
-  // LU-SGS data in the sweep layout (SW_N x ns) and the increments in it
-  // (7 x ns), FP64 or FP32 as the block's lusgs_fp32 asks
+  // LU-SGS data in the sweep layout (SW_N x ns) of the upper (sw) and the
+  // lower (swl) sweep, and the increments in it (7 x ns), FP64 or FP32 as
+  // the block's lusgs_fp32 asks.  sw_static: the metric-only part of both
+  // layouts is filled (1 FP64, 2 FP32; 0 after the metrics change).
   double* sw = nullptr;
+  double* swl = nullptr;
   double* dwp = nullptr;
+  int sw_static = 0;
   // DDADI kernel form per direction (index 1..3 = i, j, k): index into
   // DD_CFG, or -1 for one thread per line; the tuner's time of the chosen
   // form per direction
   int dd_cfg[4] = {0, 0, 0, 0};
   float dd_ms[4] = {0.f, 0.f, 0.f, 0.f};
   float* sw32 = nullptr;
+  float* swl32 = nullptr;
   float* dwp32 = nullptr;
   size_t ns = 0;
   unsigned long long* d_red = nullptr;   // per-block reduction word (FUN1KO CDMAX)
@@ -412,19 +417,27 @@ bool res_batch_ok(Ctx* c) {
   return true;
 }
 
+// The sweep-layout buffer of one sweep (upper = 1: the first, CORRGS
+// order; 0: PREDGS), FP64 or FP32.
+inline double* swd(const BlockCtx* b, int upper) { return upper ? b->sw : b->swl; }
+inline float* swf(const BlockCtx* b, int upper) { return upper ? b->sw32 : b->swl32; }
+
 // Sweep-layout buffers in the block's LU-SGS precision (the other
 // precision's are freed).
 int alloc_sweep(Ctx* c, BlockCtx* b) {
   const size_t ns = b->ns;
+  b->sw_static = 0;
   if (b->prm.lusgs_fp32) {
-    cudaFree(b->sw); cudaFree(b->dwp);
-    b->sw = nullptr; b->dwp = nullptr;
+    cudaFree(b->sw); cudaFree(b->swl); cudaFree(b->dwp);
+    b->sw = nullptr; b->swl = nullptr; b->dwp = nullptr;
     if (!b->sw32) CK(cudaMalloc(&b->sw32, sizeof(float) * SW_N * ns));
+    if (!b->swl32) CK(cudaMalloc(&b->swl32, sizeof(float) * SW_N * ns));
     if (!b->dwp32) CK(cudaMalloc(&b->dwp32, sizeof(float) * 7 * ns));
   } else {
-    cudaFree(b->sw32); cudaFree(b->dwp32);
-    b->sw32 = nullptr; b->dwp32 = nullptr;
+    cudaFree(b->sw32); cudaFree(b->swl32); cudaFree(b->dwp32);
+    b->sw32 = nullptr; b->swl32 = nullptr; b->dwp32 = nullptr;
     if (!b->sw) CK(cudaMalloc(&b->sw, sizeof(double) * SW_N * ns));
+    if (!b->swl) CK(cudaMalloc(&b->swl, sizeof(double) * SW_N * ns));
     if (!b->dwp) CK(cudaMalloc(&b->dwp, sizeof(double) * 7 * ns));
   }
   return 0;
@@ -455,15 +468,15 @@ int coop_sweep_n(Ctx* c, BlockCtx* b, int upper, bool fp32, int threads) {
   cudaError_t e;
   const bool ke = b->prm.iturb >= 3;   // seven equations (k-omega)
   if (!fp32) {
-    e = ke ? cudaLaunchKernelEx(&cfg, k_lusgs_sweep<double, 7>, b->db, (const double*)b->sw, b->dwp, upper,
-                                c->d_bar, c->d_err)
-           : cudaLaunchKernelEx(&cfg, k_lusgs_sweep<double, 5>, b->db, (const double*)b->sw, b->dwp, upper,
-                                c->d_bar, c->d_err);
+    e = ke ? cudaLaunchKernelEx(&cfg, k_lusgs_sweep<double, 7>, b->db, (const double*)swd(b, upper), b->dwp,
+                                upper, c->d_bar, c->d_err)
+           : cudaLaunchKernelEx(&cfg, k_lusgs_sweep<double, 5>, b->db, (const double*)swd(b, upper), b->dwp,
+                                upper, c->d_bar, c->d_err);
   } else {
-    e = ke ? cudaLaunchKernelEx(&cfg, k_lusgs_sweep<float, 7>, b->db, (const float*)b->sw32, b->dwp32, upper,
-                                c->d_bar, c->d_err)
-           : cudaLaunchKernelEx(&cfg, k_lusgs_sweep<float, 5>, b->db, (const float*)b->sw32, b->dwp32, upper,
-                                c->d_bar, c->d_err);
+    e = ke ? cudaLaunchKernelEx(&cfg, k_lusgs_sweep<float, 7>, b->db, (const float*)swf(b, upper), b->dwp32,
+                                upper, c->d_bar, c->d_err)
+           : cudaLaunchKernelEx(&cfg, k_lusgs_sweep<float, 5>, b->db, (const float*)swf(b, upper), b->dwp32,
+                                upper, c->d_bar, c->d_err);
   }
   if (e != cudaSuccess) return fail(c, FF_ERR_CUDA, "cooperative sweep launch", e);
   c->nlaunch++;
@@ -510,11 +523,11 @@ int lines_sweep(Ctx* c, BlockCtx* b, int upper, bool fp32) {
   }
   cudaError_t e;
   if (nv == 7)
-    e = fp32 ? launch_lines<float, 7>(&cfg, b, b->sw32, b->dwp32, upper, stage)
-             : launch_lines<double, 7>(&cfg, b, b->sw, b->dwp, upper, stage);
+    e = fp32 ? launch_lines<float, 7>(&cfg, b, swf(b, upper), b->dwp32, upper, stage)
+             : launch_lines<double, 7>(&cfg, b, swd(b, upper), b->dwp, upper, stage);
   else
-    e = fp32 ? launch_lines<float, 5>(&cfg, b, b->sw32, b->dwp32, upper, stage)
-             : launch_lines<double, 5>(&cfg, b, b->sw, b->dwp, upper, stage);
+    e = fp32 ? launch_lines<float, 5>(&cfg, b, swf(b, upper), b->dwp32, upper, stage)
+             : launch_lines<double, 5>(&cfg, b, swd(b, upper), b->dwp, upper, stage);
   if (e != cudaSuccess) return fail(c, FF_ERR_CUDA, "cluster sweep launch", e);
   c->nlaunch++;
   return 0;
@@ -675,7 +688,7 @@ int lines_batch_launch(Ctx* c, const std::vector<BlockCtx*>& v, int upper) {
       BlockCtx* b = part[n];
       lb.upper[n] = upper ? (b->prm.predgs_full ? 3 : 1) : 0;
       lb.lg[n] = geoms[n];
-      lb.sw[n] = fp32 ? (const void*)b->sw32 : (const void*)b->sw;
+      lb.sw[n] = fp32 ? (const void*)swf(b, upper) : (const void*)swd(b, upper);
       lb.dwp[n] = fp32 ? (void*)b->dwp32 : (void*)b->dwp;
       lb.b[n] = b->db;
     }
@@ -753,11 +766,11 @@ int pipe_sweep(Ctx* c, BlockCtx* b, int upper, bool fp32) {
   cfg.numAttrs = 1;
   cudaError_t e;
   if (nv == 7)
-    e = fp32 ? pipe_launch_tk<float, 7>(&cfg, b, b->sw32, b->dwp32, upper, c->d_err)
-             : pipe_launch_tk<double, 7>(&cfg, b, b->sw, b->dwp, upper, c->d_err);
+    e = fp32 ? pipe_launch_tk<float, 7>(&cfg, b, swf(b, upper), b->dwp32, upper, c->d_err)
+             : pipe_launch_tk<double, 7>(&cfg, b, swd(b, upper), b->dwp, upper, c->d_err);
   else
-    e = fp32 ? pipe_launch_tk<float, 5>(&cfg, b, b->sw32, b->dwp32, upper, c->d_err)
-             : pipe_launch_tk<double, 5>(&cfg, b, b->sw, b->dwp, upper, c->d_err);
+    e = fp32 ? pipe_launch_tk<float, 5>(&cfg, b, swf(b, upper), b->dwp32, upper, c->d_err)
+             : pipe_launch_tk<double, 5>(&cfg, b, swd(b, upper), b->dwp, upper, c->d_err);
   if (e != cudaSuccess) return fail(c, FF_ERR_CUDA, "pipelined sweep launch", e);
   c->nlaunch++;
   return 0;
@@ -847,13 +860,40 @@ int setup_pipe(Ctx* c, BlockCtx* b) {
   return 0;
 }
 
+// The metric-only part of both sweep layouts (k_sweep_static), once per
+// block and precision and again after the metrics change.  Inside a stream
+// capture the fill goes into the graph and the layouts stay marked unfilled.
+void sweep_static(Ctx* c, BlockCtx* b, bool fp32) {
+  const int want = fp32 ? 2 : 1;
+  if (b->sw_static == want) return;
+  for (int up = 0; up < 2; up++) {
+    if (fp32) k_sweep_static<float><<<nblk((long)b->ns, 128), 128, 0, c->stream>>>(b->db, swf(b, up), up);
+    else k_sweep_static<double><<<nblk((long)b->ns, 128), 128, 0, c->stream>>>(b->db, swd(b, up), up);
+    c->nlaunch++;
+  }
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(c->stream, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone) b->sw_static = want;
+}
+
+// The metrics of a block changed: its sweep layouts' static part is stale,
+// and so is every captured graph that skipped refilling it.
+void metrics_changed(Ctx* c, BlockCtx* b) {
+  b->sw_static = 0;
+  for (auto* x : c->blocks)
+    if (x->graph) { cudaGraphExecDestroy(x->graph); x->graph = nullptr; }
+  for (auto& g : c->phase_graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  if (c->mb_graph) { cudaGraphExecDestroy(c->mb_graph); c->mb_graph = nullptr; }
+}
+
 // Sweep data of one sweep in the sweep layout (and, for upper = 1, the
 // right-hand side copied into it).
 void sweep_coef(Ctx* c, BlockCtx* b, int upper, bool fp32) {
+  sweep_static(c, b, fp32);
   if (fp32)
-    k_sweep_coef<float><<<nblk((long)b->ns, 128), 128, 0, c->stream>>>(b->db, b->prm, b->sw32, b->dwp32, upper);
+    k_sweep_coef<float><<<nblk((long)b->ns, 128), 128, 0, c->stream>>>(b->db, b->prm, swf(b, upper), b->dwp32, upper);
   else
-    k_sweep_coef<double><<<nblk((long)b->ns, 128), 128, 0, c->stream>>>(b->db, b->prm, b->sw, b->dwp, upper);
+    k_sweep_coef<double><<<nblk((long)b->ns, 128), 128, 0, c->stream>>>(b->db, b->prm, swd(b, upper), b->dwp, upper);
   c->nlaunch++;
 }
 
@@ -1795,7 +1835,7 @@ int ff_destroy(void* ctx) {
   for (auto* b : c->blocks) {
     if (b->graph) cudaGraphExecDestroy(b->graph);
     cudaFree(b->base); cudaFree(b->d_patch);
-    cudaFree(b->sw); cudaFree(b->dwp); cudaFree(b->sw32); cudaFree(b->dwp32);
+    cudaFree(b->sw); cudaFree(b->swl); cudaFree(b->dwp); cudaFree(b->sw32); cudaFree(b->swl32); cudaFree(b->dwp32);
     cudaFree(b->d_red);
     delete b;
   }
@@ -1923,6 +1963,7 @@ int ff_upload(void* ctx, int blk, int slot, const double* host) {
   BlockCtx* b = getb(c, blk);
   if (!b || slot < 0 || slot >= FF_NSLOTS || !host) return fail(c, FF_ERR_ARG, "ff_upload");
   CK(cudaMemcpyAsync(b->db.a[slot], host, sizeof(double) * b->ntot, cudaMemcpyHostToDevice, c->stream));
+  if (slot >= FF_A1 && slot <= FF_VOL && b->sw_static) metrics_changed(c, b);
   return 0;
 }
 
@@ -2074,6 +2115,7 @@ int ff_block_metrics(void* ctx, int blk, const double* xyz) {
   Ctx* c = (Ctx*)ctx;
   BlockCtx* b = getb(c, blk);
   if (!b || !xyz) return fail(c, FF_ERR_ARG, "ff_block_metrics");
+  metrics_changed(c, b);
   const GridDims g{b->imax + 1, b->jmax + 1, b->kmax + 1};
   const size_t nn = (size_t)g.ni * g.nj * g.nk, ne = (size_t)(g.ni + 4) * (g.nj + 4) * (g.nk + 4);
   double *dn = nullptr, *de = nullptr;
@@ -2100,6 +2142,7 @@ int ff_block_metrics_levels(void* ctx, int blk, int nlev, const double* xyz) {
   std::vector<BlockCtx*> lv;
   for (BlockCtx* x = b; x && (int)lv.size() < nlev; x = x->coarse) lv.push_back(x);
   if ((int)lv.size() != nlev) return fail(c, FF_ERR_ARG, "ff_block_metrics_levels: fewer linked levels than nlev");
+  for (BlockCtx* x : lv) metrics_changed(c, x);
   const int ng = 2 << (nlev - 1);
   const GridDims g{b->imax + 1, b->jmax + 1, b->kmax + 1};
   const size_t nn = (size_t)g.ni * g.nj * g.nk;

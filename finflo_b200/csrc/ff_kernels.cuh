@@ -926,9 +926,41 @@ __global__ void k_lusgs_coef(DevBlock b, ff_params p, CT* coef, int upper) {
   coef[12 * nt + N] = (CT)cc.fdiag;
 }
 
-// All data of one sweep in the sweep layout (see sw_index), and for the
-// first sweep (upper = 1) the right-hand side DRO..DE(,DRK,DEPS) copied into
-// dwp in the same layout and type.
+// The static part of one sweep's layout (see sw_index): the face frames of
+// the three products (the face normal and its SURFVECTS tangents), the
+// areas and the volume -- the metrics only, written once per block.
+template <typename CT>
+__global__ void k_sweep_static(DevBlock b, CT* sw, int upper) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t row = (size_t)(b.imax + b.jmax - 1) * b.jmax;
+  if (t >= row * b.kmax) return;
+  const int K = (int)(t / row) + 1;
+  const int r = (int)(t % row), J = r % b.jmax + 1, I = r / b.jmax + 2 - J;
+  if (I < 1 || I > b.imax) return;
+  const size_t ns = sw_size(b.imax, b.jmax, b.kmax), S = sw_index(b, I, J, K);
+  const size_t N = ix(b, I, J, K);
+  const int IS = b.is, IL = b.il;
+  const int st[3] = {1, IS, IL};
+  sw[SW_VOL * ns + S] = (CT)__ldg(b.a[FF_VOL] + N);
+  sw[SW_A1 * ns + S] = (CT)__ldg(b.a[FF_A1] + (upper ? N + 1 : N));
+  sw[SW_A2 * ns + S] = (CT)__ldg(b.a[FF_A2] + (upper ? N + IS : N));
+  sw[SW_A3 * ns + S] = (CT)__ldg(b.a[FF_A3] + (upper ? N + IL : N));
+  for (int d = 0; d < 3; d++) {
+    const int ao = 4 * d;
+    size_t fN = upper ? N : N + st[d];   // the face the product in direction d crosses
+    CT nx = (CT)__ldg(b.a[FF_A1XA + ao] + fN), ny = (CT)__ldg(b.a[FF_A1YA + ao] + fN),
+       nz = (CT)__ldg(b.a[FF_A1ZA + ao] + fN);
+    CT a21, a22, a23, a31, a32, a33;
+    surfvects(nx, ny, nz, a21, a22, a23, a31, a32, a33);
+    const CT f[9] = {nx, ny, nz, a21, a22, a23, a31, a32, a33};
+    for (int q = 0; q < 9; q++) sw[(SW_F + 9 * d + q) * ns + S] = f[q];
+  }
+}
+
+// The state-dependent part of one sweep's layout (see sw_index; the static
+// part is k_sweep_static's), and for the first sweep (upper = 1) the
+// right-hand side DRO..DE(,DRK,DEPS) copied into dwp in the same layout and
+// type.
 template <typename CT>
 __global__ void k_sweep_coef(DevBlock b, ff_params p, CT* sw, CT* dwp, int upper) {
   // one thread per slot of the sweep layout, in slot order, so that the
@@ -944,16 +976,10 @@ __global__ void k_sweep_coef(DevBlock b, ff_params p, CT* sw, CT* dwp, int upper
   lusgs_cell_coef(b, p, I, J, K, upper, cc);
   const size_t ns = sw_size(b.imax, b.jmax, b.kmax), S = sw_index(b, I, J, K);
   const size_t N = ix(b, I, J, K);
-  const int IS = b.is, IL = b.il;
-  const int st[3] = {1, IS, IL};
   sw[SW_DT1 * ns + S] = (CT)cc.dt1;
   sw[SW_SCINV * ns + S] = (CT)cc.scinv;
   sw[SW_SCINP * ns + S] = (CT)cc.scinp;
   sw[SW_FD * ns + S] = (CT)cc.fdiag;
-  sw[SW_VOL * ns + S] = (CT)__ldg(b.a[FF_VOL] + N);
-  sw[SW_A1 * ns + S] = (CT)__ldg(b.a[FF_A1] + (upper ? N + 1 : N));
-  sw[SW_A2 * ns + S] = (CT)__ldg(b.a[FF_A2] + (upper ? N + IS : N));
-  sw[SW_A3 * ns + S] = (CT)__ldg(b.a[FF_A3] + (upper ? N + IL : N));
   CT ro = (CT)__ldg(b.a[FF_RO] + N), c = (CT)__ldg(b.a[FF_C] + N);
   sw[SW_RO * ns + S] = ro;
   CT ypro = CT(1) / ro;
@@ -965,17 +991,8 @@ __global__ void k_sweep_coef(DevBlock b, ff_params p, CT* sw, CT* dwp, int upper
     sw[(SW_SC + 3) * ns + S] = CT(.667) * rk * (ypro * ypro) * drdh;
     sw[(SW_SC + 4) * ns + S] = CT(1) / (CT(1) + CT(.667) * rk * ypro * drdp);
   }
-  for (int d = 0; d < 3; d++) {
-    const int ao = 4 * d;
-    size_t fN = upper ? N : N + st[d];   // the face the product in direction d crosses
-    CT nx = (CT)__ldg(b.a[FF_A1XA + ao] + fN), ny = (CT)__ldg(b.a[FF_A1YA + ao] + fN),
-       nz = (CT)__ldg(b.a[FF_A1ZA + ao] + fN);
-    CT a21, a22, a23, a31, a32, a33;
-    surfvects(nx, ny, nz, a21, a22, a23, a31, a32, a33);
-    const CT f[9] = {nx, ny, nz, a21, a22, a23, a31, a32, a33};
-    for (int q = 0; q < 9; q++) sw[(SW_F + 9 * d + q) * ns + S] = f[q];
+  for (int d = 0; d < 3; d++)
     for (int e = 0; e < 3; e++) sw[(SW_L + 3 * d + e) * ns + S] = (CT)cc.x[d][e];
-  }
   if (upper) {
     const int nv = p.iturb >= 3 ? 7 : 5;
     for (int v = 0; v < nv; v++) dwp[v * ns + S] = (CT)b.a[FF_DRO + v][N];
