@@ -36,6 +36,10 @@ struct BlockCtx {
   double* swl = nullptr;
   double* dwp = nullptr;
   int sw_static = 0;
+  // a second stream of the block: the second sweep's coefficient pass runs
+  // on it beside the first sweep (fork / join events)
+  cudaStream_t aux = nullptr;
+  cudaEvent_t aux_fork = nullptr, aux_join = nullptr;
   // DDADI kernel form per direction (index 1..3 = i, j, k): index into
   // DD_CFG, or -1 for one thread per line; the tuner's time of the chosen
   // form per direction
@@ -913,7 +917,7 @@ constexpr int DD_PD = 4, DD_TPB = 32;
 // (lines per CTA, cells per chunk) of the producer/consumer kernels the
 // autotuner chooses from
 constexpr int DD_NCFG = 4;
-constexpr int DD_CFG[DD_NCFG][2] = {{32, 4}, {16, 4}, {16, 8}, {8, 8}};
+[[maybe_unused]] constexpr int DD_CFG[DD_NCFG][2] = {{32, 4}, {16, 4}, {16, 8}, {8, 8}};
 
 // The autotuner's choice per device, block shape, equation count and
 // precision, kept for the life of the process: a later context with a block
@@ -1201,8 +1205,29 @@ int st_imps(Ctx* c, BlockCtx* b, int level, bool divide_cp) {
     if ((rc = ddadi_sweeps(c, b))) return rc;
   } else {
     sweep_coef(c, b, 1, fp32);
-    if ((rc = sweep(c, b, 1, fp32))) return rc;
-    sweep_coef(c, b, 0, fp32);
+    if (b->use_lines || b->use_pipe) {
+      // the second sweep's coefficients (their own layout buffer; they read
+      // the state, which the first sweep does not change) beside the first
+      // sweep, whose one cluster leaves most SMs free.  Not beside the
+      // cooperative hyperplane sweep, which needs every CTA resident.
+      if (!b->aux) {
+        CK(cudaStreamCreateWithFlags(&b->aux, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&b->aux_fork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&b->aux_join, cudaEventDisableTiming));
+      }
+      cudaStream_t main = c->stream;
+      CK(cudaEventRecord(b->aux_fork, main));
+      CK(cudaStreamWaitEvent(b->aux, b->aux_fork, 0));
+      c->stream = b->aux;
+      sweep_coef(c, b, 0, fp32);
+      c->stream = main;
+      CK(cudaEventRecord(b->aux_join, b->aux));
+      if ((rc = sweep(c, b, 1, fp32))) return rc;
+      CK(cudaStreamWaitEvent(main, b->aux_join, 0));
+    } else {
+      if ((rc = sweep(c, b, 1, fp32))) return rc;
+      sweep_coef(c, b, 0, fp32);
+    }
     if ((rc = sweep(c, b, 0, fp32))) return rc;
     st_sweep_out(c, b);
   }
@@ -1837,6 +1862,7 @@ int ff_destroy(void* ctx) {
     cudaFree(b->base); cudaFree(b->d_patch);
     cudaFree(b->sw); cudaFree(b->swl); cudaFree(b->dwp); cudaFree(b->sw32); cudaFree(b->swl32); cudaFree(b->dwp32);
     cudaFree(b->d_red);
+    if (b->aux) { cudaStreamDestroy(b->aux); cudaEventDestroy(b->aux_fork); cudaEventDestroy(b->aux_join); }
     delete b;
   }
   drop_phase_graphs(c);

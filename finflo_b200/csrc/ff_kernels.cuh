@@ -102,6 +102,7 @@ FF_DI size_t face_cell(const DevBlock& b, const FaceG& f, int a, int c) {
   int pa1 = pa.r1a + t % n1, pa2 = pa.r2a + t / n1;                            \
   FaceG fg = face_g((b), pa.iface);                                            \
   int ls = fg.idir * fg.s;                                                     \
+  (void)ls;                                                                    \
   size_t L = face_cell((b), fg, pa1, pa2);
 
 // REFLEC turb3.f:5294: solid walls (viscous, wall at rest) and the inlet
@@ -169,7 +170,7 @@ __global__ void k_inlet_outlet(DevBlock b, ff_params p, int icycle) {
   bool inl = pa.ityp == FF_BC_INL && pa.ibtype == 4;
   bool out = pa.ityp == FF_BC_OUT && (pa.ibtype == 2 || pa.ibtype == 3);
   if (!inl && !out) return;
-  size_t II = L, II2 = L + ls, IM1 = L - ls, IM2 = IM1 - ls;
+  size_t II = L, IM1 = L - ls, IM2 = IM1 - ls;
   size_t IF1 = fg.idir == 1 ? II : II + fg.s;
   double *U = b.a[FF_U], *V = b.a[FF_V], *W = b.a[FF_W], *T = b.a[FF_TEMP], *RO = b.a[FF_RO];
   double *P = b.a[FF_P], *PD = b.a[FF_PDIFF], *E = b.a[FF_E], *RM = b.a[FF_RM], *RN = b.a[FF_RN];
