@@ -51,6 +51,12 @@ WORKLOADS = {
 # ncu capture of the same workload (profiles/k_residual_fused_sstmg128x64x64_full.md:
 # 244.2 MB read + 24.3 MB written).
 TRAFFIC = {"sst-mg": 271.2e6}
+# DRAM bytes (read + write) per cell of one FP64 line-wavefront LU-SGS sweep
+# (k_lusgs_lines<double,7,0>) in the multi-block cycle, from an ncu capture of
+# the same eight-block case at 256x128x64 cells (profiles/
+# k_lusgs_lines_large8blk_256x128x64_dram.md); a launch's traffic scales with
+# its block's cells
+SWEEP_TRAFFIC_PER_CELL = 557.8
 
 
 def build_case(wl, nodes=None):
@@ -639,7 +645,8 @@ def run_large(args):
         # the LU-SGS line-wavefront sweep; one lower sweep of the largest block, timed alone
         "roofline": {"bound": "hbm", "kernel": "k_lusgs_lines<double,7> (lower sweep, largest block)",
                      "achieved": achieved_sweep, "peak": peak, "peak_kind": pkind, "unit": "GB/s",
-                     "frac": achieved_sweep / peak, "traffic": None, "ms_per_launch": ms_sweep,
+                     "frac": achieved_sweep / peak,
+                     "traffic": None if fp32 else SWEEP_TRAFFIC_PER_CELL * fine_cells[big], "ms_per_launch": ms_sweep,
                      "bytes_per_cell": sweep_bpc, "cells": fine_cells[big]},
         "residual": {"kernel": "k_residual_fused<7,512> (largest block, alone)", "ms_per_launch": ms_res,
                      "tile": g.residual_shape(big * nlev),
