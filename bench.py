@@ -56,7 +56,7 @@ TRAFFIC = {"sst-mg": 271.2e6}
 # the same eight-block case at 256x128x64 cells (profiles/
 # k_lusgs_lines_large8blk_256x128x64_dram.md); a launch's traffic scales with
 # its block's cells
-SWEEP_TRAFFIC_PER_CELL = 557.8
+SWEEP_TRAFFIC_PER_CELL = 376.1
 
 
 def build_case(wl, nodes=None):

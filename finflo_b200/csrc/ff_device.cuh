@@ -286,9 +286,9 @@ FF_DI void jac_product_ke(T out[7], const T dw[7], T rk, T c, T ro, T drdp, T dr
 enum : int {
   SW_DT1 = 0, SW_SCINV, SW_SCINP, SW_FD, SW_VOL, SW_A1, SW_A2, SW_A3, SW_RO,
   SW_SC = 9,     // 5 scalars
-  SW_F = 14,     // 3 directions x 9 frame values (normal, SURFVECTS a21..a33)
-  SW_L = 41,     // 3 directions x 3 eigenvalue coefficients
-  SW_N = 50
+  SW_F = 14,     // 3 directions x the face's unit normal
+  SW_L = 23,     // 3 directions x 3 eigenvalue coefficients
+  SW_N = 32
 };
 
 __host__ __device__ inline size_t sw_size(int imax, int jmax, int kmax) {
@@ -302,15 +302,16 @@ FF_DI size_t sw_index(const DevBlock& b, int I, int J, int K) {
 // The product of one cell with its precomputed frame f[9] and scalars
 // sc = {ypro, roc, proc, drh, ydrp}: SYM1I/SYM1KE(diag(l) * SYI/SYIKE(dw)).
 template <typename T, int NV>
-FF_DI void nb_product_pre(T* out, const T* dw, const T f[9], const T sc[5], T ro, T l1, T l2, T l5) {
-  const T nx = f[0], ny = f[1], nz = f[2], a21 = f[3], a22 = f[4], a23 = f[5], a31 = f[6], a32 = f[7], a33 = f[8];
+FF_DI void nb_product_pre(T* out, const T* dw, const T f[3], const T sc[5], T ro, T l1, T l2, T l5) {
+  // The tangential part of SYM1I(diag * SYI(dw)): with {n, t1, t2}
+  // orthonormal (the normal and its SURFVECTS tangents), t1 (t1 . dw) +
+  // t2 (t2 . dw) = dw - n (n . dw), so only the normal is needed:
+  // out_m = n (x2i - l1 z2) + l1 dw_m, the same operator in fewer steps.
+  const T nx = f[0], ny = f[1], nz = f[2];
   const T ypro = sc[0], roc = sc[1], proc = sc[2];
   T z2 = nx * dw[1] + ny * dw[2] + nz * dw[3];
-  T z3 = a21 * dw[1] + a22 * dw[2] + a23 * dw[3];
-  T z4 = a31 * dw[1] + a32 * dw[2] + a33 * dw[3];
   T w1 = l1 * (dw[0] - ypro * dw[4]);
   T w2 = l2 * (roc * z2 + dw[4]);
-  T w3 = l1 * z3, w4 = l1 * z4;
   T w5 = l5 * (-roc * z2 + dw[4]);
   T pc2 = T(.5) * ypro;
   T dh = w1 + pc2 * (w2 + w5);
@@ -324,9 +325,10 @@ FF_DI void nb_product_pre(T* out, const T* dw, const T f[9], const T sc[5], T ro
     out[5] = w6;
     out[6] = l1 * dw[6];
   }
-  out[1] = nx * x2i + a21 * w3 + a31 * w4;
-  out[2] = ny * x2i + a22 * w3 + a32 * w4;
-  out[3] = nz * x2i + a23 * w3 + a33 * w4;
+  const T g = x2i - l1 * z2;
+  out[1] = nx * g + l1 * dw[1];
+  out[2] = ny * g + l1 * dw[2];
+  out[3] = nz * g + l1 * dw[3];
 }
 
 // One neighbour's product for NV = 5 (laminar) or 7 (k-omega) equations.

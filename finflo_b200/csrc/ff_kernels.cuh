@@ -927,9 +927,9 @@ __global__ void k_lusgs_coef(DevBlock b, ff_params p, CT* coef, int upper) {
   coef[12 * nt + N] = (CT)cc.fdiag;
 }
 
-// The static part of one sweep's layout (see sw_index): the face frames of
-// the three products (the face normal and its SURFVECTS tangents), the
-// areas and the volume -- the metrics only, written once per block.
+// The static part of one sweep's layout (see sw_index): the unit normals
+// of the three products' faces, the areas and the volume -- the metrics
+// only, written once per block.
 template <typename CT>
 __global__ void k_sweep_static(DevBlock b, CT* sw, int upper) {
   const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -949,12 +949,9 @@ __global__ void k_sweep_static(DevBlock b, CT* sw, int upper) {
   for (int d = 0; d < 3; d++) {
     const int ao = 4 * d;
     size_t fN = upper ? N : N + st[d];   // the face the product in direction d crosses
-    CT nx = (CT)__ldg(b.a[FF_A1XA + ao] + fN), ny = (CT)__ldg(b.a[FF_A1YA + ao] + fN),
-       nz = (CT)__ldg(b.a[FF_A1ZA + ao] + fN);
-    CT a21, a22, a23, a31, a32, a33;
-    surfvects(nx, ny, nz, a21, a22, a23, a31, a32, a33);
-    const CT f[9] = {nx, ny, nz, a21, a22, a23, a31, a32, a33};
-    for (int q = 0; q < 9; q++) sw[(SW_F + 9 * d + q) * ns + S] = f[q];
+    sw[(SW_F + 3 * d + 0) * ns + S] = (CT)__ldg(b.a[FF_A1XA + ao] + fN);
+    sw[(SW_F + 3 * d + 1) * ns + S] = (CT)__ldg(b.a[FF_A1YA + ao] + fN);
+    sw[(SW_F + 3 * d + 2) * ns + S] = (CT)__ldg(b.a[FF_A1ZA + ao] + fN);
   }
 }
 
@@ -1120,11 +1117,11 @@ __global__ void k_lusgs_sweep(DevBlock b, const CT* __restrict__ sw, CT* dwp, in
           continue;
         }
         const size_t nb = upper ? S + off[d] : S - off[d];
-        CT x[NV], f[9], sc[5], l[3];
+        CT x[NV], f[3], sc[5], l[3];
 #pragma unroll
         for (int v = 0; v < NV; v++) x[v] = __ldcg(dwp + v * ns + nb);
 #pragma unroll
-        for (int c = 0; c < 9; c++) f[c] = __ldg(sw + (SW_F + 9 * d + c) * ns + nb);
+        for (int c = 0; c < 3; c++) f[c] = __ldg(sw + (SW_F + 3 * d + c) * ns + nb);
 #pragma unroll
         for (int c = 0; c < (NV == 7 ? 5 : 3); c++) sc[c] = __ldg(sw + (SW_SC + c) * ns + nb);
 #pragma unroll
@@ -1755,9 +1752,9 @@ FF_DI void lines_body(const DevBlock& b, const CT* __restrict__ sw, CT* dwp, int
       const CT ro = NV == 7 ? cd_(SW_RO) : CT(0);
 #pragma unroll
       for (int d = 0; d < 3; d++) {
-        CT f[9], l[3];
+        CT f[3], l[3];
 #pragma unroll
-        for (int c = 0; c < 9; c++) f[c] = cd_(SW_F + 9 * d + c);
+        for (int c = 0; c < 3; c++) f[c] = cd_(SW_F + 3 * d + c);
 #pragma unroll
         for (int e = 0; e < 3; e++) l[e] = cd_(SW_L + 3 * d + e);
         CT out[NV];

@@ -186,9 +186,9 @@ __global__ void __launch_bounds__(PTJ* TK) k_lusgs_pipe(DevBlock b, const CT* __
       const CT ro = NV == 7 ? cd_(SW_RO) : CT(0);
 #pragma unroll
       for (int d = 0; d < 3; d++) {
-        CT f[9], l[3], out[NV];
+        CT f[3], l[3], out[NV];
 #pragma unroll
-        for (int c = 0; c < 9; c++) f[c] = cd_(SW_F + 9 * d + c);
+        for (int c = 0; c < 3; c++) f[c] = cd_(SW_F + 3 * d + c);
 #pragma unroll
         for (int e = 0; e < 3; e++) l[e] = cd_(SW_L + 3 * d + e);
         nb_product_pre<CT, NV>(out, res, f, sc, ro, l[0], l[1], l[2]);

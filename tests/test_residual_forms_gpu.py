@@ -1,7 +1,8 @@
 """Every residual form the autotuner chooses from -- tile shapes 32x4x4,
 16x8x4, 8x8x8 cells, each with the face stencils read from global memory
-or staged in shared memory -- gives the same residual, bit for bit, and
-that residual matches the oracle's (1e-12 of max(|R|, S) per cell).  The
+or staged in shared memory -- gives the same residual to rounding (1e-14;
+each kernel instantiation forms its own fused multiply-adds), and that
+residual matches the oracle's (1e-12 of max(|R|, S) per cell).  The
 block sizes are not multiples of the tiles, so partial tiles and the
 stencil halo at the block's ghost layers are covered."""
 import numpy as np
@@ -56,5 +57,7 @@ def test_residual_forms_agree_and_match_oracle(gpu_lib, sst, monkeypatch):
     dims = (38, 20, 11)      # 37 x 19 x 10 cells
     res = [_residual(f, sst, dims, monkeypatch) for f in range(6)]
     for f in range(1, 6):
-        for n in res[0]:
-            np.testing.assert_array_equal(res[f][n], res[0][n], err_msg=f"form {f} {n}")
+        for n in res[0]:   # rounding-level: each instantiation contracts its own multiply-adds
+            scale = np.abs(res[0][n]).max()
+            np.testing.assert_allclose(res[f][n], res[0][n], rtol=1e-14, atol=1e-14 * scale,
+                                       err_msg=f"form {f} {n}")
