@@ -727,6 +727,11 @@ WARM_SST_NAME = ("learned warm start: k-omega SST bump channel 128x64x64 cells (
                  "V-cycle, INTER=1, CFL 1, Mach U[0.5,0.65]; solver solutions (seed 3) train the network (5 "
                  "refinement levels, k and omega as logs); held-out Mach points (seed 4); FP64 LU-SGS from the "
                  "free stream vs FP32 LU-SGS (every level) from the free stream and from the prediction")
+WARM_SST5_NAME = ("learned warm start, config-5 geometry: k-omega SST spanwise-varying bump (amplitude "
+                  "0.1(1+0.5 sin 2 pi z), z in [0,1], slip spanwise faces) as one 128x64x64-cell block, Re=5e6, "
+                  "first cell 2e-6, 3-level V-cycle, INTER=1, CFL 1, Mach U[0.5,0.65]; solver solutions (seed 3) "
+                  "train the network; held-out Mach points (seed 4); FP64 LU-SGS from the free stream vs FP32 "
+                  "LU-SGS (every level) from the free stream and from the prediction")
 
 
 def run_warmstart(args):
@@ -738,10 +743,10 @@ def run_warmstart(args):
     import torch
     torch.cuda.set_device(local)
     from finflo_b200 import warmstart as wsm
-    spec = wsm.SST if args.ws_family == "sst" else wsm.BUMP
+    spec = {"sst": wsm.SST, "sst5": wsm.SST5}.get(args.ws_family, wsm.BUMP)
     logs = []
     r = wsm.run_config(ntrain=args.ws_train, ntest=args.ws_test, cycles=args.ws_cycles, steps=args.ws_steps,
-                       tol_decades=args.ws_decades, log=logs.append, ddadi_arms=args.ws_family != "sst",
+                       tol_decades=args.ws_decades, log=logs.append, ddadi_arms=args.ws_family == "bump",
                        spec=spec, batch=min(16, args.ws_train), max_cycles=args.ws_max_cycles or None)
     if rank != 0:
         return 0
@@ -751,7 +756,7 @@ def run_warmstart(args):
         "ms_per_step": 1e3 * r["t_train"] / args.ws_steps, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "bf16 network / f32 LU-SGS / f64 residual",
         "data": "synthetic (seeded parameter points; training fields generated by the solver)",
-        "config": {"workload": WARM_NAME if args.ws_family != "sst" else WARM_SST_NAME,
+        "config": {"workload": {"sst": WARM_SST_NAME, "sst5": WARM_SST5_NAME}.get(args.ws_family, WARM_NAME),
                    "ntrain": args.ws_train, "ntest": args.ws_test,
                    "training_cycles": args.ws_cycles, "training_steps": args.ws_steps,
                    "parallelism": f"replicas x{ws_}"},
@@ -804,8 +809,9 @@ def main():
     ap.add_argument("--ws-cycles", type=int, default=2000)
     ap.add_argument("--ws-steps", type=int, default=6000)
     ap.add_argument("--ws-decades", type=float, default=2.0)
-    ap.add_argument("--ws-family", default="bump", choices=["bump", "sst"],
-                    help="warm start: the laminar bump family (Mach, amplitude) or the SST V-cycle case (Mach)")
+    ap.add_argument("--ws-family", default="bump", choices=["bump", "sst", "sst5"],
+                    help="warm start: the laminar bump family (Mach, amplitude), the SST V-cycle case (Mach) or "
+                         "the config-5 geometry as one block (Mach)")
     ap.add_argument("--ws-max-cycles", type=int, default=0)
     ap.add_argument("--blocks", default="4,3,2", help="block arrangement of the box workload")
     args = ap.parse_args()

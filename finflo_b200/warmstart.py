@@ -56,6 +56,8 @@ class Spec:
     inter: int = 3
     cfl: float = 2.0
     turbulence: str = None
+    span_amp: float = 0.0               # spanwise bump variation a(z) = amp (1 + span_amp sin 2 pi z)
+    zlen: float = 0.5                   # spanwise extent
 
     @property
     def grid(self):
@@ -81,6 +83,18 @@ BUMP = Spec("laminar bump channel 64x32x32 cells, Re 1e4, Mach U[0.3,0.8], ampli
 SST = Spec("k-omega SST bump channel 128x64x64 cells, Re 1e6, first cell 2e-6, 3-level V-cycle, Mach U[0.5,0.65]",
            root=(4, 2, 2), levels=5, nvar=7, params=("mach",), ranges=((0.5, 0.65),), nodes=(129, 65, 65), nlev=3,
            reynolds=1e6, h1=2e-6, noise=1e-3, inter=1, cfl=1.0, turbulence="sst")
+
+# the config-5 geometry (the spanwise-varying bump, amplitude
+# 0.1 (1 + 0.5 sin 2 pi z) on z in [0, 1], k-omega SST, Re 5e6, first cell
+# 2e-6, 3-level V-cycles, INTER=1, CFL 1) as one 128x64x64-cell block with
+# slip spanwise faces, over a Mach sweep below the transonic pocket; the
+# family the network is retrained on for config 5 (32 solutions), at the
+# single-block size the solves fit in (the 16.8 M-cell eight-block case
+# itself costs ~2 min of GPU per solution)
+SST5 = Spec("config-5 geometry: k-omega SST spanwise-varying bump 128x64x64 cells, amplitude 0.1(1+0.5 sin 2 pi z), "
+            "z in [0,1], Re 5e6, first cell 2e-6, 3-level V-cycle, Mach U[0.5,0.65]",
+            root=(4, 2, 2), levels=5, nvar=7, params=("mach",), ranges=((0.5, 0.65),), nodes=(129, 65, 65), nlev=3,
+            reynolds=5e6, h1=2e-6, noise=1e-3, inter=1, cfl=1.0, turbulence="sst", span_amp=0.5, zlen=1.0)
 
 # the config-4 family's sizes, kept as module constants
 ROOT, LEVELS, NVAR = BUMP.root, BUMP.levels, BUMP.nvar
@@ -417,7 +431,7 @@ def make_case(pv, seed=0, lusgs_fp32=False, ddadi=False, spec=BUMP):
                                          amp=kw.get("amp", spec.amp), reynolds=spec.reynolds, h1=spec.h1,
                                          noise=spec.noise, seed=seed, inter=spec.inter, cfl=spec.cfl,
                                          cfll=spec.cfl, lusgs_fp32=lusgs_fp32, coarse_fp32=lusgs_fp32,
-                                         turbulence=spec.turbulence)
+                                         turbulence=spec.turbulence, span_amp=spec.span_amp, zlen=spec.zlen)
     for q in prms:
         q.ddadi = int(ddadi)
         q.predgs_full = 1
