@@ -629,8 +629,9 @@ def run_large(args):
     line = {
         "metric": "cell-iters/s", "value": value, "unit": "cell-iters/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64 residual / " + ("f32" if fp32 else "f64") + " LU-SGS"
-        + (" (coarse levels: f32 face fluxes and LU-SGS)" if args.coarse_fp32 and not fp32 else ""),
+        "vs_baseline": None, "dtype": "f64 residual / " + ("f32" if fp32 else "f64")
+        + (" DDADI" if args.ddadi else " LU-SGS")
+        + (" (coarse levels: f32 face fluxes and implicit stage)" if args.coarse_fp32 and not fp32 else ""),
         "data": "synthetic (seeded block cuts and free-stream noise)",
         "config": {"workload": LARGE_NAME.format(cells="x".join(map(str, cells)), prec="FP32" if fp32 else "FP64")
                    + (", DDADI implicit stage (LUSGS=0)" if args.ddadi else "")
