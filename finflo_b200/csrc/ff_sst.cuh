@@ -222,28 +222,27 @@ FF_DI void roe_flux_ke(const T q[7][4], T nx, T ny, T nz, T area, int intem, int
     if (fabs(dpp) >= T(1.e-2) * (ppi + pmi)) dedph = (eip + elr - eim - erl) / dpp;
     if (fabs(drr) >= T(1.e-2) * (roip + roim)) dedrh = (eip + erl - eim - elr) / drr;
   }
-  T a21, a22, a23, a31, a32, a33;
-  surfvects(nx, ny, nz, a21, a22, a23, a31, a32, a33);
+  // normal velocities; the tangential parts as Cartesian vectors (the
+  // SURFVECTS tangents t1, t2 only ever appear as t1 t1' + t2 t2' = I - n n')
   T ur = nx * rmip + ny * rnip + nz * rwip;
-  T vr = a21 * rmip + a22 * rnip + a23 * rwip;
-  T wr = a31 * rmip + a32 * rnip + a33 * rwip;
   T ul = nx * rmim + ny * rnim + nz * rwim;
-  T vl = a21 * rmim + a22 * rnim + a23 * rwim;
-  T wl = a31 * rmim + a32 * rnim + a33 * rwim;
+  const T txr = rmip - ur * nx, tyr = rnip - ur * ny, tzr = rwip - ur * nz;
+  const T txl = rmim - ul * nx, tyl = rnim - ul * ny, tzl = rwim - ul * nz;
   T rkipi = dmax(T(0.001) * T(p.rklim), rkip), reipi = dmax(T(0.001) * T(p.epslim), reip);
   T rkimi = dmax(T(0.001) * T(p.rklim), rkim), reimi = dmax(T(0.001) * T(p.epslim), reim);
   T rkr = rkipi * ypror, rkl = rkimi * yprol;
-  T eir = eip + T(.5) * (ur * ur + vr * vr + wr * wr) + rkr;
-  T eil = eim + T(.5) * (ul * ul + vl * vl + wl * wl) + rkl;
+  T eir = eip + T(.5) * (rmip * rmip + rnip * rnip + rwip * rwip) + rkr;
+  T eil = eim + T(.5) * (rmim * rmim + rnim * rnim + rwim * rwim) + rkl;
   T pr = ppi, pl = pmi, pkr = T(.6667) * rkipi, pkl = T(.6667) * rkimi;
   T epsr = reipi * ypror, epsl = reimi * yprol;
   T hr = eir + pr * ypror, hl = eil + yprol * pl;
   T rohat = sqrt(roip * roim), yproh = rcp(rohat);
   T sqrl = rcp(roim + rohat), cql = roim * sqrl, cqr = T(1.) - cql;
-  T uhat = cqr * ur + cql * ul, vhat = cqr * vr + cql * vl, what = cqr * wr + cql * wl;
+  T uhat = cqr * ur + cql * ul;
+  const T thx = cqr * txr + cql * txl, thy = cqr * tyr + cql * tyl, thz = cqr * tzr + cql * tzl;
   T hhat = cqr * hr + cql * hl, ehat = cqr * eip + cql * eim;
   T rkhat = cqr * rkr + cql * rkl, epshat = cqr * epsr + cql * epsl;
-  T phat = rohat * (hhat - ehat - T(.5) * (uhat * uhat + vhat * vhat + what * what) - rkhat);
+  T phat = rohat * (hhat - ehat - T(.5) * (uhat * uhat + thx * thx + thy * thy + thz * thz) - rkhat);
   phat = dmin(dmax(pr, pl), phat);
   phat = dmax(dmin(pr, pl), phat);
   T drdhh = rcp(dedrh - phat * (yproh * yproh));
@@ -261,7 +260,7 @@ FF_DI void roe_flux_ke(const T q[7][4], T nx, T ny, T nz, T area, int intem, int
   T alfa1 = T(.5) * (dp + rohat * chat * du) * pchat2;
   T alfa2 = T(.5) * (dp - rohat * chat * du) * pchat2;
   T alfa3 = dro - dp * pchat2;
-  T alfa4 = rohat * (vr - vl), alfa5 = rohat * (wr - wl), alfa6 = rohat * dk, alfa7 = rohat * (epsr - epsl);
+  T alfa6 = rohat * dk, alfa7 = rohat * (epsr - epsl);
   T rl1h = uhat + chat, rl2h = uhat - chat, rl3h = uhat;
   T rl1 = fabs(rl1h), rl2 = fabs(rl2h), rl3 = fabs(rl3h);
   if (p.entropy_fix) {
@@ -278,18 +277,22 @@ FF_DI void roe_flux_ke(const T q[7][4], T nx, T ny, T nz, T area, int intem, int
   T ha = T(.5) * area;
   T f1 = ha * (roucr + roucl - damp);
   T f2 = ha * (roucr * ur + pr + pkr + roucl * ul + pl + pkl - (damp * uhat + (rl1 * alfa1 - rl2 * alfa2) * chat));
-  T f3 = ha * (roucr * vr + roucl * vl - damp * vhat - rl3 * alfa4);
-  T f4 = ha * (roucr * wr + roucl * wl - damp * what - rl3 * alfa5);
+  // the tangential momentum flux as a vector (f3, f4 of the reference's
+  // rotated frame) and its jump term of the energy flux
+  const T rr = rl3 * rohat;
+  const T ftx = ha * (roucr * txr + roucl * txl - damp * thx - rr * (txr - txl));
+  const T fty = ha * (roucr * tyr + roucl * tyl - damp * thy - rr * (tyr - tyl));
+  const T ftz = ha * (roucr * tzr + roucl * tzl - damp * thz - rr * (tzr - tzl));
+  const T tj = rr * ((txr - txl) * thx + (tyr - tyl) * thy + (tzr - tzl) * thz);
   T f5 = ha * (roucr * (hr + pkr * ypror) + roucl * (hl + pkl * yprol) - damp * hhat -
-               ((rl1 * alfa1 - rl2 * alfa2) * uhat * chat - rl3 * alfa3 * rohat * (chat * chat) * pdpde +
-                rl3 * alfa4 * vhat + rl3 * alfa5 * what) +
+               ((rl1 * alfa1 - rl2 * alfa2) * uhat * chat - rl3 * alfa3 * rohat * (chat * chat) * pdpde + tj) +
                rl3 * alfa6 * (T(1.) - T(.6667) * rohat * pdpde));
   T f6 = ha * (roucr * rkr + roucl * rkl - damp * rkhat - rl3 * alfa6);
   T f7 = ha * (roucr * epsr + roucl * epsl - damp * epshat - rl3 * alfa7);
   f[0] += f1;
-  f[1] += nx * f2 + a21 * f3 + a31 * f4;
-  f[2] += ny * f2 + a22 * f3 + a32 * f4;
-  f[3] += nz * f2 + a23 * f3 + a33 * f4;
+  f[1] += nx * f2 + ftx;
+  f[2] += ny * f2 + fty;
+  f[3] += nz * f2 + ftz;
   f[4] += f5;
   f[5] += f6;
   f[6] += f7;
