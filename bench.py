@@ -49,8 +49,8 @@ WORKLOADS = {
 
 # DRAM bytes (read + write) of one launch of the dominant kernel, from one
 # ncu capture of the same workload (profiles/k_residual_fused_sstmg128x64x64_full.md:
-# 244.2 MB read + 24.3 MB written).
-TRAFFIC = {"sst-mg": 271.2e6}
+# 244.6 MB read + 25.4 MB written, 16x8x4-cell tiles).
+TRAFFIC = {"sst-mg": 270.0e6}
 # DRAM bytes (read + write) per cell of one FP64 line-wavefront LU-SGS sweep
 # (k_lusgs_lines<double,7,0>) in the multi-block cycle, from an ncu capture of
 # the same eight-block case at 256x128x64 cells (profiles/
